@@ -1,0 +1,119 @@
+// Device-side descriptors of one pipeline launch, filled by the host runtime
+// (dq_runtime.cu) from the public IR (include/dogqc_b200.h) and passed to the
+// pipeline kernel as one __grid_constant__ parameter.
+#pragma once
+#include <stdint.h>
+#include "../../include/dogqc_b200.h"
+
+namespace dq {
+
+constexpr int kThreads = 256;          // pipeline kernel block size
+constexpr int kMaxStages = 4;          // tile staging depth
+constexpr int kMaxRes = 8;             // resources one pipeline touches
+constexpr int kMaxStr = 4;             // string columns per pipeline
+constexpr int kMaxStash = 24;          // values carried by one heavy work item
+constexpr uint64_t kEmpty = ~0ull;     // empty tag of every hash table
+
+// status bits written by device code
+enum : int32_t {
+  kErrHtFull = 1,
+  kErrTimeout = 2,
+  kErrOverflow = 4,
+  kErrBadOp = 8,
+  kErrAggSpill = 16,     // informational: a CTA-local aggregation table spilled
+};
+
+struct DevCol {           // staged fixed-width column
+  const uint8_t* ptr;
+  int32_t width;
+  int32_t smem_off;       // offset inside one stage buffer
+};
+
+struct DevStr {           // string column, read in place
+  const uint8_t* chars;
+  const uint64_t* offsets;
+  int32_t width;          // > 0: fixed-width strings
+  int32_t pad;
+};
+
+struct DevSlot {
+  int8_t kind, level, ctype, width;
+  int16_t src, res;
+  int32_t smem_off;       // REG: offset inside the level's register area
+  int32_t stash;          // index in a heavy item's stash (-1: not carried)
+};
+
+struct DevRes {
+  int32_t kind;           // dq_res_kind
+  int32_t nkeys;
+  int8_t key_ctype[DQ_MAX_KEYS];
+  int32_t packed;         // keys packed into the 64-bit tag
+  int32_t words;          // 64-bit words per slot (tag + keys + payload/aggs)
+  int32_t key_word;       // first key word (hashed keys only)
+  int32_t val_word;       // first payload / accumulator word
+  uint64_t cap;           // slots (UNIQUE/AGG), buckets (MULTI), rows (OUTPUT)
+  uint64_t* slots;        // UNIQUE/AGG: cap+1 slots (last = tag ~0 key)
+  uint32_t* counts;       // MULTI
+  uint32_t* offsets;      // MULTI (cap+1)
+  int32_t npay;
+  int32_t naggs;
+  int8_t pay_ctype[DQ_MAX_PAY];
+  int8_t pay_width[DQ_MAX_PAY];
+  int8_t agg_red[DQ_MAX_AGGS];
+  uint8_t* pay[DQ_MAX_PAY];   // MULTI payload columns / OUTPUT columns
+  uint64_t* cursor;       // OUTPUT row cursor
+  int32_t smem_slots;     // AGG: CTA-local table slots (0: global only)
+  int32_t smem_off;       // AGG: offset of the CTA-local table
+};
+
+struct DevHeavy {         // deferred wide expansion ranges
+  uint64_t* items;        // cap * words
+  uint32_t* count;
+  uint64_t* unit_prefix;  // work-unit prefix over items (heavy mode)
+  uint32_t cap;
+  int32_t words;          // 2 + number of stashed values
+  int32_t nstash;
+  int32_t op;             // index of the EXPAND op the items belong to
+  uint64_t threshold;     // ranges longer than this are deferred
+};
+
+struct DevPipe {
+  int64_t nrows;
+  const uint64_t* nrows_dev;   // row count produced on the device (temp tables)
+  int32_t source_kind;         // dq_source_kind
+  int32_t source_res;
+  int32_t tile;                // rows per tile (multiple of 16)
+  int32_t nstage;
+  int32_t stage_bytes;
+  int32_t exp_cap;             // rows per expansion chunk
+  int32_t use_tma;
+  int32_t mode;                // 0: tiles, 1: heavy work units
+  int32_t ncols;
+  DevCol cols[DQ_MAX_COLS];
+  int32_t nstr;
+  DevStr strs[kMaxStr];
+  int32_t nslots;
+  DevSlot slots[DQ_MAX_SLOTS];
+  int32_t nops;
+  dq_op ops[DQ_MAX_OPS];
+  int16_t lists[DQ_MAX_LIST];
+  int32_t nres;
+  DevRes res[kMaxRes];
+  const uint8_t* patterns;     // concatenated LIKE patterns / string constants
+  int32_t pat_off[DQ_MAX_PATTERNS + 1];
+  DevHeavy heavy;
+  // shared-memory layout (bytes)
+  int32_t off_stage;
+  int32_t off_reg[DQ_MAX_LEVELS];
+  int32_t off_sel[DQ_MAX_LEVELS];
+  int32_t off_par[DQ_MAX_LEVELS];
+  int32_t off_match[DQ_MAX_LEVELS];
+  int32_t off_exp;             // expansion bookkeeping (off, cnt, pos) per level-0 row
+  int32_t off_stash;
+  int32_t smem_bytes;
+  int32_t* status;
+  uint32_t* tile_counter;      // dynamic tile scheduler
+  uint64_t* scratch_ll;        // misc device counters
+};
+
+}  // namespace dq

@@ -1,0 +1,293 @@
+"""Seeded synthetic workloads: tables, plans and plan configs.
+
+Four pipeline shapes, sized at ``scale=1.0`` as follows:
+
+* ``c0`` scan-filter-aggregate over one 6,000,000-row table (TPC-H Q1 shape):
+  filter ``shipdate <= max-90``, group by two char flags (6 groups), exact
+  64-bit sums of quantity, price, ``price*(100-disc)`` and
+  ``price*(100-disc)*(100+tax)``, a count, and averages derived from them.
+* ``c1`` FK-PK hash join + aggregate: a 1,500,000-row dimension (unique keys,
+  a permutation of 1..1.5M) filtered on ``segment == 1`` (20%), probed by a
+  6,000,000-row fact table, grouped by ``nation`` (25 groups).
+* ``c2`` divergent expansion: a 10,000,000-row multimap build side with Zipf(1.0)
+  keys over 100,000 values, probed by 16,777,216 uniform keys over 200,000
+  values (about half miss), followed by 4 filters (90/50/10/1%) on build-side
+  columns, then a count and a 64-bit sum.
+* ``c3`` three-way star join: 60,000,000 fact rows against dimensions of
+  1,500,000 / 200,000 / 10,000 rows with 50% / ~20% (``LIKE '%word%'``
+  disjunction on a 25-byte string) / 100% filters, grouped by the 1.5M-key
+  dimension.
+
+TPC-H data is not available here; these seeded tables have TPC-H-like shapes,
+value ranges and distributions.  Each generator is deterministic in its seed
+(numpy ``Philox``), so the device engine, the CPU oracle and the reference's own
+generated pipeline all see identical bytes.
+
+Plan builders take the algebra object and the scalar/type/reduction namespaces
+as arguments, so the same function builds the plan with this package's front end
+or with the reference's (``oracle/ref_harness.py``).
+"""
+import math
+from collections import namedtuple
+
+import numpy as np
+
+from dogqc_b200.database import Database, StringColumn, Table
+from dogqc_b200.types import Type
+
+BASE_SEED = 20261203
+EPOCH_1992 = 8035          # 1992-01-01 as days since 1970-01-01
+DATE_RANGE = 2557          # 1992-01-01 .. 1998-12-31
+
+Workload = namedtuple("Workload", "name db build_plan description")
+
+
+def _rng(seed):
+    return np.random.Generator(np.random.Philox(seed))
+
+
+def _n(base, scale, minimum=1):
+    return max(minimum, int(round(base * scale)))
+
+
+# ---------------------------------------------------------------- c0 ----------
+
+def gen_c0(scale=1.0, seed=BASE_SEED + 0):
+    n = _n(6_000_000, scale)
+    r = _rng(seed)
+    cols = {
+        "l_quantity": r.integers(1, 51, n, dtype=np.int32),
+        "l_extendedprice": r.integers(90_000, 10_500_001, n, dtype=np.int64).astype(np.uint64),
+        "l_discount": r.integers(0, 11, n, dtype=np.int32),
+        "l_tax": r.integers(0, 9, n, dtype=np.int32),
+        "l_shipdate": (EPOCH_1992 + r.integers(0, DATE_RANGE, n)).astype(np.uint32),
+        "l_returnflag": np.frombuffer(b"ANR", dtype=np.int8)[r.integers(0, 3, n)],
+        "l_linestatus": np.frombuffer(b"FO", dtype=np.int8)[r.integers(0, 2, n)],
+    }
+    types = {"l_quantity": Type.INT, "l_extendedprice": Type.FLOAT, "l_discount": Type.INT,
+             "l_tax": Type.INT, "l_shipdate": Type.DATE, "l_returnflag": Type.CHAR,
+             "l_linestatus": Type.CHAR}
+    return Database([Table("lineitem", cols, types)])
+
+
+def plan_c0(alg, scal, Type, Reduction, cutoff=EPOCH_1992 + DATE_RANGE - 1 - 90):
+    sel = alg.selection(
+        scal.SmallerEqualExpr(scal.AttrExpr("l_shipdate"), scal.ConstExpr(str(cutoff), Type.DATE)),
+        alg.scan("lineitem"))
+    disc = alg.map("disc_price",
+                   scal.MulExpr(scal.AttrExpr("l_extendedprice"),
+                                scal.SubExpr(scal.ConstExpr("100", Type.INT), scal.AttrExpr("l_discount"))),
+                   sel)
+    charge = alg.map("charge",
+                     scal.MulExpr(scal.AttrExpr("disc_price"),
+                                  scal.AddExpr(scal.ConstExpr("100", Type.INT), scal.AttrExpr("l_tax"))),
+                     disc)
+    agg = alg.aggregation(
+        ["l_returnflag", "l_linestatus"],
+        [(Reduction.SUM, "l_quantity", "sum_qty"),
+         (Reduction.SUM, "l_extendedprice", "sum_base_price"),
+         (Reduction.SUM, "disc_price", "sum_disc_price"),
+         (Reduction.SUM, "charge", "sum_charge"),
+         (Reduction.AVG, "l_quantity", "avg_qty"),
+         (Reduction.AVG, "l_extendedprice", "avg_price"),
+         (Reduction.AVG, "l_discount", "avg_disc"),
+         (Reduction.COUNT, "", "count_order")],
+        charge)
+    cfg = {sel.opId: {"selectivity": (cutoff - EPOCH_1992 + 1) / DATE_RANGE},
+           agg.opId: {"numgroups": 6}}
+    return agg, cfg
+
+
+# ---------------------------------------------------------------- c1 ----------
+
+def gen_c1(scale=1.0, seed=BASE_SEED + 1):
+    nd = _n(1_500_000, scale)
+    nf = _n(6_000_000, scale)
+    r = _rng(seed)
+    dim = {
+        "d_key": (r.permutation(nd) + 1).astype(np.int32),
+        "d_segment": r.integers(0, 5, nd, dtype=np.int32),
+        "d_nation": r.integers(0, 25, nd, dtype=np.int32),
+    }
+    fact = {
+        "f_fk": r.integers(1, nd + 1, nf, dtype=np.int32),
+        "f_measure": r.integers(1_000, 10_000_001, nf, dtype=np.int64).astype(np.uint64),
+    }
+    return Database([
+        Table("dim", dim, {"d_key": Type.INT, "d_segment": Type.INT, "d_nation": Type.INT}),
+        Table("fact", fact, {"f_fk": Type.INT, "f_measure": Type.FLOAT}),
+    ])
+
+
+def plan_c1(alg, scal, Type, Reduction, segment=1):
+    sel = alg.selection(scal.EqualsExpr(scal.AttrExpr("d_segment"), scal.ConstExpr(str(segment), Type.INT)),
+                        alg.scan("dim"))
+    join = alg.join(("d_key", "f_fk"), sel, alg.scan("fact"))
+    agg = alg.aggregation(["d_nation"],
+                          [(Reduction.SUM, "f_measure", "sum_measure"),
+                           (Reduction.COUNT, "", "cnt")],
+                          join)
+    cfg = {sel.opId: {"selectivity": 0.2},
+           join.opId: {"multimatch": False, "selectivity": 0.2},
+           agg.opId: {"numgroups": 25}}
+    return agg, cfg
+
+
+# ---------------------------------------------------------------- c2 ----------
+
+def zipf_keys(r, n, distinct, s=1.0):
+    """``n`` keys in ``1..distinct`` with P(rank k) ~ 1/k^s and permuted labels.
+
+    Follows the construction of the reference's join-data generator
+    (query/datagen/zipfdist.c:295-355): a cumulative distribution over ranks,
+    a uniform draw mapped through it, and a random permutation from ranks to key
+    labels.
+    """
+    ranks = np.arange(1, distinct + 1, dtype=np.float64)
+    p = 1.0 / np.power(ranks, s)
+    cdf = np.cumsum(p)
+    cdf /= cdf[-1]
+    labels = (r.permutation(distinct) + 1).astype(np.int32)
+    u = r.random(n)
+    idx = np.searchsorted(cdf, u, side="left")
+    np.minimum(idx, distinct - 1, out=idx)
+    return labels[idx]
+
+
+def gen_c2(scale=1.0, seed=BASE_SEED + 2, distinct=None, probe_range=None, probe_lo=1):
+    nb = _n(10_000_000, scale)
+    npr = _n(16_777_216, scale)
+    distinct = distinct or _n(100_000, scale, 16)
+    probe_range = probe_range or 2 * distinct
+    r = _rng(seed)
+    build = {"r_key": zipf_keys(r, nb, distinct)}
+    for i in range(1, 5):
+        build["r_f%d" % i] = r.integers(0, 100, nb, dtype=np.int32)
+    build["r_measure"] = r.integers(1, 1_000_001, nb, dtype=np.int64).astype(np.uint64)
+    probe = {"s_key": r.integers(probe_lo, probe_lo + probe_range, npr, dtype=np.int32)}
+    btypes = {"r_key": Type.INT, "r_f1": Type.INT, "r_f2": Type.INT, "r_f3": Type.INT,
+              "r_f4": Type.INT, "r_measure": Type.FLOAT}
+    return Database([Table("r_build", build, btypes),
+                     Table("s_probe", probe, {"s_key": Type.INT})])
+
+
+C2_THRESHOLDS = (90, 50, 10, 1)
+
+
+def plan_c2(alg, scal, Type, Reduction, thresholds=C2_THRESHOLDS):
+    join = alg.join(("r_key", "s_key"), alg.scan("r_build"), alg.scan("s_probe"))
+    node = join
+    cfg = {join.opId: {"selectivity": 50.0}}
+    for i, t in enumerate(thresholds, start=1):
+        node = alg.selection(scal.SmallerExpr(scal.AttrExpr("r_f%d" % i), scal.ConstExpr(str(t), Type.INT)),
+                             node)
+        cfg[node.opId] = {"selectivity": t / 100.0}
+    agg = alg.aggregation([], [(Reduction.COUNT, "", "cnt"),
+                               (Reduction.SUM, "r_measure", "sum_measure")], node)
+    return agg, cfg
+
+
+# ---------------------------------------------------------------- c3 ----------
+
+def vocabulary(seed=BASE_SEED + 3, size=90, length=4):
+    """``size`` distinct lowercase words of ``length`` letters (seeded)."""
+    r = _rng(seed + 1000)
+    words = []
+    seen = set()
+    letters = np.frombuffer(b"abcdefghijklmnopqrstuvwxyz", dtype=np.uint8)
+    while len(words) < size:
+        w = bytes(letters[r.integers(0, 26, length)])
+        if w not in seen:
+            seen.add(w)
+            words.append(w)
+    return words
+
+
+C3_WIDTH = 25
+
+
+def gen_c3(scale=1.0, seed=BASE_SEED + 3):
+    n1 = _n(1_500_000, scale)
+    n2 = _n(200_000, scale)
+    n3 = _n(10_000, scale)
+    nf = _n(60_000_000, scale)
+    r = _rng(seed)
+    vocab = np.array([list(w) for w in vocabulary(seed)], dtype=np.uint8)   # 90 x 4
+    d1 = {"d1_key": (r.permutation(n1) + 1).astype(np.int32),
+          "d1_attr": r.integers(0, 100, n1, dtype=np.int32)}
+    pick = r.integers(0, len(vocab), (n2, 5))
+    text = np.full((n2, C3_WIDTH), ord(" "), dtype=np.uint8)
+    for j in range(5):
+        text[:, 5 * j:5 * j + 4] = vocab[pick[:, j]]
+    d2 = {"d2_key": (r.permutation(n2) + 1).astype(np.int32),
+          "d2_text": StringColumn.fixed(text)}
+    d3 = {"d3_key": (r.permutation(n3) + 1).astype(np.int32),
+          "d3_attr": r.integers(0, 100, n3, dtype=np.int32)}
+    fact = {"f_fk1": r.integers(1, n1 + 1, nf, dtype=np.int32),
+            "f_fk2": r.integers(1, n2 + 1, nf, dtype=np.int32),
+            "f_fk3": r.integers(1, n3 + 1, nf, dtype=np.int32),
+            "f_price": r.integers(90_000, 10_500_001, nf, dtype=np.int64).astype(np.uint64),
+            "f_disc": r.integers(0, 11, nf, dtype=np.int32)}
+    return Database([
+        Table("dim1", d1, {"d1_key": Type.INT, "d1_attr": Type.INT}),
+        Table("dim2", d2, {"d2_key": Type.INT, "d2_text": Type.STRING}),
+        Table("dim3", d3, {"d3_key": Type.INT, "d3_attr": Type.INT}),
+        Table("fact", fact, {"f_fk1": Type.INT, "f_fk2": Type.INT, "f_fk3": Type.INT,
+                             "f_price": Type.FLOAT, "f_disc": Type.INT}),
+    ])
+
+
+def c3_patterns(seed=BASE_SEED + 3, nwords=4):
+    """The LIKE patterns: ``nwords`` vocabulary words; 4 words give
+    P(match) = 1 - (86/90)^5 ~= 20.3% for 5-word strings."""
+    words = vocabulary(seed)
+    return ["%" + w.decode() + "%" for w in words[:nwords]]
+
+
+def plan_c3(alg, scal, Type, Reduction, patterns=None, d1_cut=50, d3_cut=100):
+    patterns = patterns or c3_patterns()
+    s1 = alg.selection(scal.SmallerExpr(scal.AttrExpr("d1_attr"), scal.ConstExpr(str(d1_cut), Type.INT)),
+                       alg.scan("dim1"))
+    like = scal.LikeExpr(scal.AttrExpr("d2_text"), scal.ConstExpr(patterns[0], Type.STRING))
+    for p in patterns[1:]:
+        like = scal.OrExpr(like, scal.LikeExpr(scal.AttrExpr("d2_text"), scal.ConstExpr(p, Type.STRING)))
+    s2 = alg.selection(like, alg.scan("dim2"))
+    s3 = alg.selection(scal.SmallerExpr(scal.AttrExpr("d3_attr"), scal.ConstExpr(str(d3_cut), Type.INT)),
+                       alg.scan("dim3"))
+    j3 = alg.join(("d3_key", "f_fk3"), s3, alg.scan("fact"))
+    j2 = alg.join(("d2_key", "f_fk2"), s2, j3)
+    j1 = alg.join(("d1_key", "f_fk1"), s1, j2)
+    m = alg.map("disc_price",
+                scal.MulExpr(scal.AttrExpr("f_price"),
+                             scal.SubExpr(scal.ConstExpr("100", Type.INT), scal.AttrExpr("f_disc"))),
+                j1)
+    agg = alg.aggregation(["d1_key"],
+                          [(Reduction.SUM, "f_price", "sum_price"),
+                           (Reduction.SUM, "disc_price", "sum_disc_price"),
+                           (Reduction.COUNT, "", "cnt")],
+                          m)
+    sel_like = 1.0 - (1.0 - len(patterns) / 90.0) ** 5
+    cfg = {s1.opId: {"selectivity": d1_cut / 100.0},
+           s2.opId: {"selectivity": sel_like},
+           s3.opId: {"selectivity": d3_cut / 100.0},
+           j3.opId: {"multimatch": False, "selectivity": 1.0},
+           j2.opId: {"multimatch": False, "selectivity": sel_like},
+           j1.opId: {"multimatch": False, "selectivity": sel_like * d1_cut / 100.0},
+           agg.opId: {"numgroups": 1_000_000}}
+    return agg, cfg
+
+
+GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3}
+PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3}
+
+
+def build(name, alg, scale=1.0, **kw):
+    """Build workload ``name``'s plan with this package's front end."""
+    import dogqc_b200.scalar as scal
+    from dogqc_b200.relational import Reduction
+    return PLANS[name](alg, scal, Type, Reduction, **kw)
+
+
+def algorithmic_bytes(db, tables):
+    """Bytes of the named tables' columns at stored width."""
+    return sum(db[t].nbytes for t in tables)

@@ -1,0 +1,264 @@
+/*
+ * dogqc_b200 — C ABI of the B200 execution backend for DogQC relational plans.
+ *
+ * The reference has no runtime library: its Python translator emits one CUDA
+ * source file per query whose generated main() maps column files, allocates
+ * device memory, launches the pipeline kernels and prints the result
+ * (dogqc/codegen.py:121-159, dogqc/cudaTranslator.py:31-101).  This header is the
+ * boundary that replaces that generated host program.  A caller (the Python
+ * Backend in dogqc_b200/backend.py, or any FFI binding) registers device-resident
+ * tables, hands a lowered plan (the IR below) to dq_plan_prepare, runs it with
+ * dq_plan_execute and reads result columns.  Every entry point returns a status
+ * (0 = OK, negative dq_status on error, message in dq_last_error); nothing calls
+ * exit() or prints, unlike the reference's ERROR macro (dogqc/include/util.h:1-5)
+ * and device printf on full hash tables (dogqc/include/hashing.cuh:96,117,267).
+ *
+ * Plain C types only: no CUDA or torch types appear in the signatures (streams
+ * are passed as void*).
+ */
+#ifndef DOGQC_B200_H
+#define DOGQC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DQ_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- status -- */
+typedef enum {
+    DQ_OK = 0,
+    DQ_ERR_INVALID = -1,     /* bad argument                                   */
+    DQ_ERR_CUDA = -2,        /* CUDA runtime error                             */
+    DQ_ERR_OOM = -3,         /* device allocation failed                       */
+    DQ_ERR_HT_FULL = -4,     /* a hash table stayed full after resizing        */
+    DQ_ERR_TIMEOUT = -5,     /* a bounded device wait gave up                  */
+    DQ_ERR_BAD_IR = -6,      /* plan IR failed validation                      */
+    DQ_ERR_ADMISSION = -7,   /* serving: query rejected by the memory budget   */
+    DQ_ERR_NOT_FOUND = -8,   /* unknown table / column / ticket                */
+    DQ_ERR_OVERFLOW = -9,    /* an output stayed larger than its allocation    */
+    DQ_ERR_UNSUPPORTED = -10 /* plan uses a feature this build does not have   */
+} dq_status;
+
+/* C value types of columns and plan values.  They mirror the reference's type
+ * map (dogqc/codegen.py:37-45) with decimals in exact 64-bit integers:
+ * INT -> I32, DATE -> U32, CHAR -> I8, FLOAT/DOUBLE -> U64, STRING -> STR.    */
+typedef enum {
+    DQ_I8 = 1, DQ_I32 = 2, DQ_U32 = 3, DQ_I64 = 4, DQ_U64 = 5, DQ_STR = 6
+} dq_ctype;
+
+typedef struct dq_ctx dq_ctx;
+typedef struct dq_plan dq_plan;
+typedef struct dq_result dq_result;
+
+typedef struct {
+    int32_t abi_version;        /* DQ_ABI_VERSION                               */
+    int32_t device;             /* CUDA device ordinal                          */
+    uint64_t memory_budget;     /* bytes the context may hold (0 = no limit)    */
+    int32_t block_threads;      /* pipeline kernel block size (0 = default 256) */
+    int32_t tile_rows;          /* rows per tile (0 = default)                  */
+    int32_t ctas_per_sm;        /* persistent CTAs per SM (0 = default)         */
+    int32_t flags;              /* DQ_CFG_* bits                                */
+} dq_config;
+
+#define DQ_CFG_NO_TMA      1    /* stage tiles with plain loads instead of TMA */
+#define DQ_CFG_NO_GRAPH    2    /* do not capture CUDA graphs                  */
+
+/* ------------------------------------------------------------- contexts -- */
+int dq_init(const dq_config* cfg, dq_ctx** out);
+void dq_shutdown(dq_ctx* ctx);
+const char* dq_last_error(dq_ctx* ctx);      /* NULL ctx: last init error      */
+int dq_version(void);
+
+/* --------------------------------------------------------------- tables -- */
+/* One column to register.  Fixed-width types: `data` holds nrows values.
+ * Strings: `data` is the char heap of `nchars` bytes and `offsets` holds
+ * nrows+1 byte offsets (the reference's size_t offsets + char heap,
+ * dogqc/cudaTranslator.py:263-269); with `width` > 0 every string has that
+ * length and `offsets` may be NULL.                                          */
+typedef struct {
+    const char* name;
+    int32_t ctype;              /* dq_ctype                                     */
+    int32_t width;              /* string width for fixed-width strings, else 0 */
+    const void* data;
+    const uint64_t* offsets;
+    uint64_t nchars;
+} dq_column;
+
+#define DQ_TABLE_DEVICE_DATA 1  /* pointers are device memory (else host)      */
+
+/* Copies the columns into library-owned, padded device memory (replacing a
+ * table of the same name).                                                   */
+int dq_table_register(dq_ctx* ctx, const char* name, int32_t ncols, const dq_column* cols,
+                      int64_t nrows, int32_t flags);
+/* Overwrites the values of an existing table's columns with the same types and
+ * row count from host memory (pinned memory gives full copy bandwidth).  The
+ * copies are queued on `stream` (NULL: the context stream).                  */
+int dq_table_update(dq_ctx* ctx, const char* name, int32_t ncols, const dq_column* cols,
+                    int64_t nrows, void* stream);
+int dq_table_drop(dq_ctx* ctx, const char* name);
+int dq_table_rows(dq_ctx* ctx, const char* name, int64_t* nrows);
+
+/* ------------------------------------------------------------------ IR -- */
+/* A plan is a list of resources (hash tables, aggregation tables, outputs)
+ * and pipelines.  Each pipeline streams one source in tiles through a list of
+ * operators that read and write slots (values per row), ending in one sink.
+ * The Python Backend (dogqc_b200/lowering.py) produces this from the
+ * reference's resolved operator tree; the produce/consume translators it
+ * replaces are dogqc/cudaTranslator.py:333-668 and dogqc/hashJoins.py:12-681. */
+
+#define DQ_MAX_COLS    16
+#define DQ_MAX_SLOTS   64
+#define DQ_MAX_OPS     48
+#define DQ_MAX_LIST   192
+#define DQ_MAX_KEYS     4
+#define DQ_MAX_PAY     16
+#define DQ_MAX_AGGS    16
+#define DQ_MAX_LEVELS   3
+#define DQ_MAX_PATTERNS 8
+
+typedef enum {
+    DQ_SLOT_COL = 1,     /* source column, staged per tile (level 0)           */
+    DQ_SLOT_REG = 2,     /* computed value                                     */
+    DQ_SLOT_GATHER = 3,  /* multimap payload column at an expansion level      */
+    DQ_SLOT_AGGKEY = 4,  /* aggregation-table key (agg-scan source)            */
+    DQ_SLOT_AGGVAL = 5,  /* aggregation-table accumulator (agg-scan source)    */
+    DQ_SLOT_STR = 6      /* string source column (read in place)               */
+} dq_slot_kind;
+
+typedef struct {
+    int8_t kind;         /* dq_slot_kind                                        */
+    int8_t level;        /* expansion level the value lives on                  */
+    int8_t ctype;        /* dq_ctype                                            */
+    int8_t pad;
+    int16_t src;         /* COL/STR: pipeline column; GATHER: payload column;   */
+                         /* AGGKEY: key index; AGGVAL: aggregate index          */
+    int16_t res;         /* resource for GATHER/AGGKEY/AGGVAL                   */
+} dq_slot;
+
+typedef enum {
+    DQ_OP_ARITH = 1,     /* sub: dq_arith; dst = a (op) b in ctype             */
+    DQ_OP_CMP = 2,       /* sub: dq_cmp;   dst = (a cmp b) in ctype, as I32     */
+    DQ_OP_LOGIC = 3,     /* sub: dq_logic                                      */
+    DQ_OP_CAST = 4,      /* dst = (dst type) a                                 */
+    DQ_OP_SELECT = 5,    /* dst = a ? b : c (CASE arm)                         */
+    DQ_OP_LIKE = 6,      /* dst = a LIKE pattern[res]                          */
+    DQ_OP_STREQ = 7,     /* dst = a == pattern[res] (string constant)          */
+    DQ_OP_FILTER = 10,   /* keep rows with a != 0                              */
+    DQ_OP_PROBE = 11,    /* unique-HT probe (res); sub: dq_join                */
+    DQ_OP_EXPAND = 12,   /* multimap probe (res) opening level+1               */
+    DQ_OP_AGG = 20,      /* sink: aggregate into res                           */
+    DQ_OP_BUILD = 21,    /* sink: insert into unique HT res                    */
+    DQ_OP_MM_COUNT = 22, /* sink: multimap bucket counts                       */
+    DQ_OP_MM_SCATTER = 23, /* sink: multimap payload scatter                   */
+    DQ_OP_EMIT = 24      /* sink: append rows to output res                    */
+} dq_op_kind;
+
+typedef enum { DQ_ADD = 1, DQ_SUB = 2, DQ_MUL = 3, DQ_DIV = 4, DQ_MOD = 5 } dq_arith;
+typedef enum { DQ_EQ = 1, DQ_NE = 2, DQ_LT = 3, DQ_LE = 4, DQ_GT = 5, DQ_GE = 6 } dq_cmp;
+typedef enum { DQ_AND = 1, DQ_OR = 2, DQ_NOT = 3 } dq_logic;
+typedef enum { DQ_JOIN_INNER = 1, DQ_JOIN_SEMI = 2, DQ_JOIN_ANTI = 3 } dq_join;
+typedef enum { DQ_RED_SUM = 1, DQ_RED_COUNT = 2, DQ_RED_MIN = 3, DQ_RED_MAX = 4 } dq_reduction;
+
+#define DQ_OPF_B_IMM 1   /* operand b is `imm` (in the op's ctype)              */
+#define DQ_OPF_A_IMM 2   /* operand a is `imm`                                  */
+
+typedef struct {
+    int16_t kind;        /* dq_op_kind                                          */
+    int16_t sub;         /* dq_arith / dq_cmp / dq_logic / dq_join              */
+    int16_t dst, a, b, c;/* slot indices (-1 if unused)                         */
+    int8_t ctype;        /* computation type                                    */
+    int8_t flags;        /* DQ_OPF_*                                            */
+    int16_t res;         /* resource or pattern index                           */
+    int16_t list, nlist; /* keys (probe/build/agg) or emitted slots             */
+    int16_t list2, nlist2; /* payload destinations / sources, agg inputs      */
+    int16_t pad;
+    int64_t imm;
+} dq_op;
+
+typedef enum {
+    DQ_RES_UNIQUE = 1,   /* unique join hash table (multimatch = False)        */
+    DQ_RES_MULTI = 2,    /* multimap: bucket counts/offsets + payload columns  */
+    DQ_RES_AGG = 3,      /* aggregation table                                  */
+    DQ_RES_OUTPUT = 4    /* materialised rows (result or temp table)           */
+} dq_res_kind;
+
+typedef struct {
+    int32_t kind;                    /* dq_res_kind                             */
+    int32_t nkeys;
+    int8_t key_ctype[DQ_MAX_KEYS];
+    int32_t npay;                    /* UNIQUE/MULTI payload; OUTPUT columns    */
+    int8_t pay_ctype[DQ_MAX_PAY];
+    int32_t naggs;
+    int8_t agg_red[DQ_MAX_AGGS];     /* dq_reduction                            */
+    int64_t capacity;                /* slots / buckets / rows (from estimates) */
+    int64_t group_hint;              /* AGG: estimated groups                   */
+    const char* name;                /* OUTPUT: temp-table name or NULL         */
+} dq_resource;
+
+typedef enum {
+    DQ_SRC_TABLE = 1,    /* registered table                                    */
+    DQ_SRC_OUTPUT = 2,   /* rows of an OUTPUT resource (temp table)             */
+    DQ_SRC_AGG = 3       /* occupied slots of an AGG resource                   */
+} dq_source_kind;
+
+typedef struct {
+    int32_t source_kind;             /* dq_source_kind                          */
+    int32_t source_res;              /* OUTPUT / AGG resource                   */
+    const char* table;               /* DQ_SRC_TABLE                            */
+    int32_t ncols;
+    const char* cols[DQ_MAX_COLS];   /* TABLE: column names; OUTPUT: indices as */
+                                     /* decimal strings                         */
+    int32_t nslots;
+    dq_slot slots[DQ_MAX_SLOTS];
+    int32_t nops;
+    dq_op ops[DQ_MAX_OPS];
+    int32_t nlist;
+    int16_t lists[DQ_MAX_LIST];
+    int32_t npatterns;
+    const char* patterns[DQ_MAX_PATTERNS];  /* LIKE patterns / string constants */
+    int32_t compact;                 /* 1: compact after every filter / probe   */
+} dq_pipeline;
+
+typedef struct {
+    int32_t abi_version;
+    int32_t nres;
+    const dq_resource* res;
+    int32_t npipes;
+    const dq_pipeline* pipes;        /* executed in order                       */
+    int32_t result_res;              /* OUTPUT resource returned as the result  */
+} dq_plan_desc;
+
+/* -------------------------------------------------------------- plans -- */
+int dq_plan_prepare(dq_ctx* ctx, const dq_plan_desc* desc, dq_plan** out);
+/* Runs every pipeline in order on `stream` (NULL: the context stream) and
+ * returns a new result.  Resources are reset at the start of each run.       */
+int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out);
+void dq_plan_free(dq_plan* plan);
+
+/* Device time of the last execute (CUDA events on the launching stream):
+ * total, and the longest pipeline kernel with its index.                     */
+typedef struct {
+    double total_ms;
+    double max_pipeline_ms;
+    int32_t max_pipeline;
+    int32_t kernel_launches;         /* kernels launched by the last execute    */
+    double pipeline_ms[DQ_MAX_OPS];
+} dq_plan_timing;
+int dq_plan_timing_get(dq_plan* plan, dq_plan_timing* out);
+
+/* ------------------------------------------------------------ results -- */
+int dq_result_rows(dq_result* r, int64_t* nrows);
+int dq_result_ncols(dq_result* r, int32_t* ncols);
+/* Host pointer to column `col` (nrows values of its C type; strings as
+ * nrows (start,end) byte offsets into `dq_result_heap`).                      */
+int dq_result_column(dq_result* r, int32_t col, int32_t* ctype, const void** data);
+void dq_result_free(dq_result* r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,18 @@
+"""Canonical form of a result set (test infrastructure).
+
+Results are compared as multisets: rows (tuples of Python ints; chars as their
+byte value) are sorted lexicographically and hashed.  Row order and column
+widths do not enter the checksum.
+"""
+import hashlib
+
+
+def canonical_rows(rows):
+    return sorted(tuple(int(v) for v in r) for r in rows)
+
+
+def canonical_checksum(rows):
+    h = hashlib.sha256()
+    for r in canonical_rows(rows):
+        h.update((",".join(str(v) for v in r) + "\n").encode())
+    return h.hexdigest()

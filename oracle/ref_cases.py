@@ -1,0 +1,29 @@
+"""Cases on which the reference's own generated pipeline pins the oracle.
+
+Test infrastructure (oracle side): nothing in the product imports this module.
+
+Each case names a workload (``dogqc_b200.workloads``), a scale, plan-builder
+keyword arguments and reference-compiler knobs.  ``ref_harness.py`` turns every
+case into a reference-generated ``.cu`` compiled for sm_100a; ``ref_run.py`` runs
+those binaries on a GPU host over tables generated from the same seeds, and
+``tests/golden/make_golden.py`` converts their outputs into committed fixtures.
+"""
+
+CASES = {
+    # small cases: full result sets are committed as fixtures
+    "c0_s": dict(workload="c0", scale=0.001),
+    "c1_s": dict(workload="c1", scale=0.001),
+    "c2_s": dict(workload="c2", scale=0.0005, pushdown=False),
+    "c2_s_pd": dict(workload="c2", scale=0.0005, pushdown=True),
+    "c3_s": dict(workload="c3", scale=0.0002),
+    "c0_lr": dict(workload="c0", scale=0.001, buffers="selection"),
+    # edge cases
+    "c0_empty": dict(workload="c0", scale=0.001, plan_kw=dict(cutoff=0)),
+    "c1_nomatch": dict(workload="c1", scale=0.001, plan_kw=dict(segment=9)),
+    "c2_nomatch": dict(workload="c2", scale=0.0005, gen_kw=dict(probe_lo=51)),
+    # full sizes: row counts, checksums and (small) full results are committed
+    "c0": dict(workload="c0", scale=1.0),
+    "c1": dict(workload="c1", scale=1.0),
+    "c2": dict(workload="c2", scale=1.0, pushdown=True),
+    "c3": dict(workload="c3", scale=1.0),
+}

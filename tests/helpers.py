@@ -1,0 +1,26 @@
+"""Shared test helpers: golden fixtures and plan construction."""
+import json
+import os
+
+from dogqc_b200 import workloads
+from dogqc_b200.relational import RelationalAlgebra
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden(case):
+    with open(os.path.join(GOLDEN, "ref_%s.json" % case)) as f:
+        return json.load(f)
+
+
+def golden_cases():
+    return sorted(f[4:-5] for f in os.listdir(GOLDEN) if f.startswith("ref_") and f.endswith(".json"))
+
+
+def make_case(spec):
+    """Database and resolved plan (this package's front end) for a golden case spec."""
+    db = workloads.GENERATORS[spec["workload"]](spec["scale"], **spec.get("gen_kw", {}))
+    alg = RelationalAlgebra(db)
+    plan, cfg = workloads.build(spec["workload"], alg, **spec.get("plan_kw", {}))
+    plan = alg.resolveAlgebraPlan(plan, cfg)
+    return db, alg, plan
