@@ -1,0 +1,363 @@
+"""Benchmark: FK-PK hash join + aggregation on one B200 (or N replicas).
+
+Workload (the configuration the headline metric is quoted on): a 1,500,000-row
+dimension with unique int32 keys filtered on ``segment == 1`` (20%) and built
+into a hash table, probed by a 6,000,000-row fact table (int32 FK + int64
+measure), grouped by ``nation`` (25 groups) with an exact 64-bit sum and a count.
+Seeded synthetic data with those shapes (no TPC-H data here).
+
+A step is one execution of the whole plan (dimension build pipeline, fact probe
++ aggregate pipeline, aggregation output pipeline).  ``value`` counts the input
+rows of both tables per second of device time (CUDA events on the engine's
+stream), inputs resident in HBM; the inputs (90 MB) fit in L2, so a 256 MB buffer
+is written between steps.  ``e2e`` runs the same plan through the public API
+with the input columns copied from pinned host memory every step and the result
+read back, timed on the host.  ``roofline`` is for the dominant kernel (the fact
+probe pipeline).  ``--impl reference`` times the CPU oracle (numpy restatement of
+the reference's semantics), partitioned over all host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SCALE = 1.0
+WORKLOAD = "c1"
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+METRIC = "rows/s (FK-PK hash join + aggregate pipeline, input rows of both tables per second)"
+CONFIG = {"workload": "fk_pk_join_agg", "dim_rows": 1_500_000, "fact_rows": 6_000_000,
+          "dim_filter": "segment == 1 (20%)", "groups": 25, "l2": "256 MB flush between steps",
+          "parallelism": "replicas"}
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def load_profile_traffic():
+    """DRAM bytes per launch of the probe kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(WORKLOAD, {}).get("probe_pipeline_dram_bytes")
+    except Exception:
+        return None
+
+
+class ClockSampler(object):
+    """nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, maxmhz, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                maxmhz = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        mhz.sort()
+        return {"sm_mhz": mhz[len(mhz) // 2] if mhz else None, "sm_max_mhz": maxmhz,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=300))
+    return world, rank, local
+
+
+def dist_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_plan(db):
+    from dogqc_b200 import workloads
+    from dogqc_b200.relational import RelationalAlgebra
+    alg = RelationalAlgebra(db)
+    plan, cfg = workloads.build(WORKLOAD, alg)
+    return alg.resolveAlgebraPlan(plan, cfg)
+
+
+# ------------------------------------------------------------------ our arm --
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    from dogqc_b200 import workloads
+    from dogqc_b200.engine import Engine
+
+    torch.cuda.set_device(local)
+    db = workloads.GENERATORS[WORKLOAD](SCALE)
+    plan = build_plan(db)
+    rows_per_step = sum(t.size for t in db.tables.values())
+    fact_bytes = db["fact"].nbytes
+    engine = Engine(local)
+    engine.register_database(db)
+    p = engine.prepare(plan)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def step():
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        res = p.execute()
+        return res, p.timing()
+
+    for _ in range(args.warmup):
+        res, _ = step()
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    total_ms, probe_ms, launches = 0.0, 0.0, 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            res, t = step()
+            total_ms += t["total_ms"]
+            probe_ms += t["pipeline_ms"][1]
+            launches += t["kernel_launches"]
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    total_ms = dist_max(total_ms, world)
+    probe_ms = dist_max(probe_ms, world)
+    ms_per_step = total_ms / args.steps
+    value = rows_per_step * world / (ms_per_step / 1e3)
+
+    # end to end: host columns (pinned) -> device, execute, result back
+    pinned = {}
+    for tname, table in db.tables.items():
+        for cname, col in table.columns.items():
+            arr = np.ascontiguousarray(col)
+            t = torch.from_numpy(arr.view(np.uint8)).pin_memory()
+            pinned[(tname, cname)] = (t, arr.dtype)
+
+    class PinnedTable(object):
+        def __init__(self, table):
+            self.name = table.name
+            self.size = table.size
+            self.types = table.types
+            self.columns = {c: pinned[(table.name, c)][0].numpy().view(pinned[(table.name, c)][1])
+                            for c in table.columns}
+
+    ptables = [PinnedTable(t) for t in db.tables.values()]
+    h2d = sum(t.nbytes for t in db.tables.values())
+    d2h_rows = res.nrows
+    d2h = sum(c.nbytes for c in res.columns) + 12
+    for _ in range(2):
+        for pt in ptables:
+            engine.update_table(pt)
+        p.execute()
+    dist_barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for pt in ptables:
+            engine.update_table(pt)
+        r2 = p.execute()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = dist_max(e2e_s, world)
+    assert r2.nrows == d2h_rows
+    e2e_value = rows_per_step * world * args.steps / e2e_s
+
+    peak, peak_kind = hbm_peak()
+    probe_avg_s = probe_ms / args.steps / 1e3
+    achieved = fact_bytes / probe_avg_s / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+        "config": CONFIG,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": load_profile_traffic(),
+                     "kernel": "pipeline_kernel (fact probe + aggregate)",
+                     "algorithmic_bytes": fact_bytes, "avg_ms": probe_avg_s * 1e3,
+                     "peak_source": "%s hbm_gbs (burst copy)" % peak_kind},
+        "plan": {"algorithmic_bytes": sum(t.nbytes for t in db.tables.values()),
+                 "avg_ms": ms_per_step,
+                 "frac": sum(t.nbytes for t in db.tables.values()) / (ms_per_step / 1e3) / 1e9 / peak},
+        "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(db, plan)
+    engine.close()
+    return out
+
+
+# ------------------------------------------------------------ CPU baselines --
+
+_WORKER_DB = {}
+
+
+def _oracle_partition(args):
+    """Worker: evaluate the plan over one slice of the fact table."""
+    lo, hi = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from evaluator import run_plan
+    from dogqc_b200 import workloads
+    from dogqc_b200.database import Database, Table
+    if "db" not in _WORKER_DB:
+        _WORKER_DB["db"] = workloads.GENERATORS[WORKLOAD](SCALE)
+    db = _WORKER_DB["db"]
+    fact = db["fact"]
+    part = Table("fact", {c: v[lo:hi] for c, v in fact.columns.items()}, fact.types)
+    db2 = Database([db["dim"], part])
+    plan = build_plan(db2)
+    t0 = time.perf_counter()
+    names, rows = run_plan(db2, plan)
+    return names, rows, time.perf_counter() - t0
+
+
+def merge_partials(rows):
+    """Merge per-partition (nation, sum, count) rows: wrapping 64/32-bit adds."""
+    acc = {}
+    for key, s, c in rows:
+        a = acc.setdefault(key, [0, 0])
+        a[0] = (a[0] + s) % (1 << 64)
+        a[1] = (a[1] + c) % (1 << 32)
+    out = []
+    for k, (s, c) in acc.items():
+        out.append((k, s, c - (1 << 32) if c >= 1 << 31 else c))
+    return out
+
+
+def cpu_baseline(db, plan, repeats=2):
+    """Single-threaded oracle over the full workload (bounded: a few seconds per run)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from evaluator import run_plan
+    rows = sum(t.size for t in db.tables.values())
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        run_plan(db, plan)
+    dt = time.perf_counter() - t0
+    return {"value": rows * repeats / dt, "unit": "rows/s", "cores": 1, "kind": "port",
+            "sample": "%d full runs of the workload (%d input rows each) through the numpy oracle"
+                      % (repeats, rows)}
+
+
+def run_reference(args, world, rank):
+    """The CPU oracle over all host cores: the fact table is split into one slice
+    per core, each worker evaluates the plan on its slice, partial aggregates
+    are merged."""
+    import multiprocessing as mp
+    if rank != 0:
+        return None
+    from dogqc_b200 import workloads
+    db = workloads.GENERATORS[WORKLOAD](SCALE)
+    nfact, ndim = db["fact"].size, db["dim"].size
+    cores = os.cpu_count() or 1
+    bounds = [(nfact * i // cores, nfact * (i + 1) // cores) for i in range(cores)]
+    ctx = mp.get_context("spawn")
+    times = []
+    with ctx.Pool(cores) as pool:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            parts = pool.map(_oracle_partition, bounds)
+            merged = merge_partials([r for _, rows, _ in parts for r in rows])
+            dt = time.perf_counter() - t0
+            worker = max(w for _, _, w in parts)
+            if i >= args.warmup:
+                times.append(worker)
+    # each step: every worker generates its tables, then evaluates; the timed part
+    # is the evaluation (the slowest worker)
+    step_s = sum(times) / len(times)
+    value = (nfact + ndim) / step_s
+    return {
+        "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
+        "config": CONFIG, "impl": "reference",
+        "cpu_baseline": {"kind": "port", "cores": cores, "value": value, "unit": "rows/s",
+                         "sample": "full workload per step; fact table split over %d processes, "
+                                   "dimension built by each; %d groups merged" % (cores, len(merged))},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out = run_ours(args, world, rank, local)
+    if rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

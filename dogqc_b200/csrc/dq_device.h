@@ -108,7 +108,8 @@ struct DevPipe {
   int32_t off_sel[DQ_MAX_LEVELS];
   int32_t off_par[DQ_MAX_LEVELS];
   int32_t off_match[DQ_MAX_LEVELS];
-  int32_t off_exp;             // expansion bookkeeping (off, cnt, pos) per level-0 row
+  int32_t off_exp;             // expansion bookkeeping (off, cnt, pos) per parent level
+  int32_t off_flags;           // per-row probe results
   int32_t off_stash;
   int32_t smem_bytes;
   int32_t* status;

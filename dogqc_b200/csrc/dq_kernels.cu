@@ -1,0 +1,1283 @@
+// Pipeline kernels of the B200 backend (sm_100a).
+//
+// One persistent kernel executes one pipeline of a plan: it streams the source
+// in tiles of `tile` rows, staged from HBM into shared memory with TMA bulk
+// copies (cp.async.bulk + mbarrier, multi-stage), and runs the pipeline's
+// operator list over each tile column-wise:
+//
+//   * expression ops evaluate for every selected row and write a register slot;
+//   * filters and probes keep a subset of rows: the tile's selection vector is
+//     compacted block-wide (warp ballot/popc + one scan), so every later op
+//     runs on full warps.  This is the lane-refill idea of the reference
+//     (dogqc/cudaDivergenceBuffer.py:11-283) applied at tile granularity;
+//   * a multimap probe opens an expansion level: the (row, match) pairs of the
+//     tile are produced in chunks of `tile` pairs and the rest of the pipeline
+//     runs once per chunk.  This generalises the reference's warp-level
+//     push-down expansion (dogqc/hashJoins.py:599-681) to the whole CTA; ranges
+//     longer than a threshold are deferred to a second launch in which all CTAs
+//     split them (the skewed heads of Zipf build sides);
+//   * the sink (aggregate / build / emit) ends the list.
+//
+// Values are carried as canonical 64-bit words: sign-extended for signed C
+// types, zero-extended for unsigned ones, and every operation computes in the C
+// type the lowering assigned (usual arithmetic conversions, wrap-around).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dq_device.h"
+
+namespace dq {
+
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxItems = 8;                 // tile <= kThreads * kMaxItems
+constexpr long long kSpinLimit = 1ll << 28;  // bound of every device wait
+constexpr uint64_t kBusy = ~0ull - 1;        // aggregation slot being claimed
+
+// ------------------------------------------------------------------ values --
+
+__device__ __forceinline__ uint64_t canon(uint64_t v, int t) {
+  switch (t) {
+    case DQ_I8: return (uint64_t)(int64_t)(int8_t)v;
+    case DQ_I32: return (uint64_t)(int64_t)(int32_t)v;
+    case DQ_U32: return (uint64_t)(uint32_t)v;
+    default: return v;
+  }
+}
+
+__device__ __forceinline__ bool is_signed(int t) { return t == DQ_I8 || t == DQ_I32 || t == DQ_I64; }
+
+__device__ __forceinline__ uint64_t ld(const uint8_t* p, int w) {
+  switch (w) {
+    case 1: return *p;
+    case 2: return *reinterpret_cast<const uint16_t*>(p);
+    case 4: return *reinterpret_cast<const uint32_t*>(p);
+    default: return *reinterpret_cast<const uint64_t*>(p);
+  }
+}
+
+__device__ __forceinline__ void st(uint8_t* p, int w, uint64_t v) {
+  switch (w) {
+    case 1: *p = (uint8_t)v; break;
+    case 2: *reinterpret_cast<uint16_t*>(p) = (uint16_t)v; break;
+    case 4: *reinterpret_cast<uint32_t*>(p) = (uint32_t)v; break;
+    default: *reinterpret_cast<uint64_t*>(p) = v; break;
+  }
+}
+
+// MurmurHash3 64-bit finaliser (Appleby), used for every hash table.
+__device__ __forceinline__ uint64_t fmix64(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdull;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ull;
+  k ^= k >> 33;
+  return k;
+}
+
+// Maps a 64-bit hash onto [0, cap) without a division (multiply-high range
+// reduction).
+__device__ __forceinline__ uint64_t reduce_range(uint64_t h, uint64_t cap) { return __umul64hi(h, cap); }
+
+__device__ uint64_t arith(int sub, int t, uint64_t a, uint64_t b) {
+  a = canon(a, t);
+  b = canon(b, t);
+  uint64_t r = 0;
+  switch (sub) {
+    case DQ_ADD: r = a + b; break;
+    case DQ_SUB: r = a - b; break;
+    case DQ_MUL: r = a * b; break;
+    case DQ_DIV:
+    case DQ_MOD: {
+      if (b == 0) return 0;  // undefined in C; defined as 0 here
+      bool div = sub == DQ_DIV;
+      if (t == DQ_I32) {
+        int32_t x = (int32_t)a, y = (int32_t)b;
+        if (y == -1) r = div ? (uint64_t)(uint32_t)(0u - (uint32_t)x) : 0;
+        else r = (uint64_t)(uint32_t)(div ? x / y : x % y);
+      } else if (t == DQ_U32) {
+        uint32_t x = (uint32_t)a, y = (uint32_t)b;
+        r = div ? x / y : x % y;
+      } else if (t == DQ_I64) {
+        int64_t x = (int64_t)a, y = (int64_t)b;
+        if (y == -1) r = div ? 0ull - a : 0;
+        else r = (uint64_t)(div ? x / y : x % y);
+      } else {
+        r = div ? a / b : a % b;
+      }
+      break;
+    }
+  }
+  return canon(r, t);
+}
+
+__device__ __forceinline__ bool compare(int sub, int t, uint64_t a, uint64_t b) {
+  a = canon(a, t);
+  b = canon(b, t);
+  if (is_signed(t)) {
+    int64_t x = (int64_t)a, y = (int64_t)b;
+    switch (sub) {
+      case DQ_EQ: return x == y;
+      case DQ_NE: return x != y;
+      case DQ_LT: return x < y;
+      case DQ_LE: return x <= y;
+      case DQ_GT: return x > y;
+      default: return x >= y;
+    }
+  }
+  switch (sub) {
+    case DQ_EQ: return a == b;
+    case DQ_NE: return a != b;
+    case DQ_LT: return a < b;
+    case DQ_LE: return a <= b;
+    case DQ_GT: return a > b;
+    default: return a >= b;
+  }
+}
+
+// LIKE with the reference matcher's exact semantics (util.cuh:144-199):
+// prefix, then suffix, then infixes left to right; '_' matches any byte; reads
+// one past the end of the string or pattern see a zero byte.
+__device__ bool like_match(const uint8_t* s, int ls, const uint8_t* p, int lp) {
+  auto S = [&](int i) -> int { return (i >= 0 && i < ls) ? s[i] : 0; };
+  auto P = [&](int i) -> int { return (i >= 0 && i < lp) ? p[i] : 0; };
+  auto cmp = [](int c, int l) { return c == l || l == '_'; };
+  int l_in_start = 0, l_in_end = lp, s_in_start = 0, s_in_end = ls, l_pos = 0;
+  if (P(0) != '%') {
+    int s_pos = 0;
+    l_pos = 0;
+    while (l_pos < lp && s_pos < ls && P(l_pos) != '%') {
+      if (!cmp(S(s_pos), P(l_pos))) return false;
+      ++l_pos;
+      ++s_pos;
+    }
+    l_in_start = l_pos;
+    s_in_start = s_pos;
+  }
+  if (P(lp - 1) != '%') {
+    int s_pos = ls - 1;
+    l_pos = lp - 1;
+    while (l_pos >= 0 && s_pos >= 0 && P(l_pos) != '%') {
+      if (!cmp(S(s_pos), P(l_pos))) return false;
+      --l_pos;
+      --s_pos;
+    }
+    l_in_end = l_pos;
+    s_in_end = s_pos + 1;
+  }
+  if (l_in_start < l_in_end) {
+    l_pos = l_in_start + 1;
+    int s_pos = s_in_start;
+    while (s_pos < s_in_end && l_pos < l_in_end) {
+      int l_tr = l_pos, s_tr = s_pos;
+      while (cmp(S(s_tr), P(l_tr)) && s_tr < s_in_end) {
+        ++l_tr;
+        if (P(l_tr) == '%') {
+          ++l_tr;
+          l_pos = l_tr;
+          s_pos = s_tr;
+          break;
+        }
+        ++s_tr;
+      }
+      ++s_pos;
+    }
+  }
+  return l_pos >= l_in_end;
+}
+
+// ------------------------------------------------------------ CTA state --
+
+struct Cta {
+  uint8_t* smem;
+  const uint8_t* stage;                 // staged columns of the current tile
+  int64_t tile_start;                   // first source row of the tile
+  int heavy;                            // executing deferred expansion units
+  uint8_t* reg[DQ_MAX_LEVELS];
+  uint16_t* sel[DQ_MAX_LEVELS];
+  uint16_t* par[DQ_MAX_LEVELS];
+  uint32_t* match[DQ_MAX_LEVELS];
+  uint32_t* eoff[DQ_MAX_LEVELS];        // expansion bookkeeping per parent level
+  uint32_t* ecnt[DQ_MAX_LEVELS];
+  uint32_t* epos[DQ_MAX_LEVELS];
+  uint8_t* flags;                       // per-row probe results
+  uint64_t* stash;
+};
+
+__shared__ int32_t s_scan[kMaxItems * kWarps + 64];
+__shared__ uint64_t s_bcast[8];
+
+__device__ __forceinline__ void set_status(const DevPipe& P, int32_t bits) { atomicOr(P.status, bits); }
+
+__device__ __forceinline__ int slot_row(const Cta& c, int slot_level, int level, int row) {
+  for (int l = level; l > slot_level; --l) row = c.par[l][row];
+  return row;
+}
+
+__device__ __forceinline__ const DevStr& str_of(const DevPipe& P, int s) { return P.strs[P.slots[s].src]; }
+
+__device__ __forceinline__ void read_str(const DevPipe& P, const Cta& c, int s, int level, int row,
+                                         const uint8_t*& ptr, int& len) {
+  const DevSlot& sl = P.slots[s];
+  int r = slot_row(c, sl.level, level, row);
+  const DevStr& d = P.strs[sl.src];
+  int64_t g = c.tile_start + r;
+  if (d.width > 0) {
+    ptr = d.chars + g * d.width;
+    len = d.width;
+  } else {
+    uint64_t a = d.offsets[g], b = d.offsets[g + 1];
+    ptr = d.chars + a;
+    len = (int)(b - a);
+  }
+}
+
+__device__ __forceinline__ uint64_t read_slot(const DevPipe& P, const Cta& c, int s, int level, int row) {
+  const DevSlot& sl = P.slots[s];
+  if (c.heavy && sl.level == 0) return c.stash[sl.stash];
+  int r = slot_row(c, sl.level, level, row);
+  uint64_t raw;
+  switch (sl.kind) {
+    case DQ_SLOT_COL:
+      raw = ld(c.stage + P.cols[sl.src].smem_off + (size_t)r * sl.width, sl.width);
+      break;
+    case DQ_SLOT_REG:
+      raw = ld(c.reg[sl.level] + sl.smem_off + (size_t)r * sl.width, sl.width);
+      break;
+    case DQ_SLOT_GATHER: {
+      uint32_t m = c.match[sl.level][r];
+      raw = ld(P.res[sl.res].pay[sl.src] + (size_t)m * sl.width, sl.width);
+      break;
+    }
+    case DQ_SLOT_AGGKEY: {
+      const DevRes& R = P.res[sl.res];
+      uint64_t idx = (uint64_t)(c.tile_start + r);
+      const uint64_t* slot = R.slots + idx * R.words;
+      if (R.packed) {
+        uint64_t tag = slot[0];
+        if (idx == R.cap) tag = kEmpty;  // the slot reserved for the all-ones key
+        raw = (R.nkeys == 1 && (R.key_ctype[0] == DQ_I64 || R.key_ctype[0] == DQ_U64))
+                  ? tag : (tag >> (32 * sl.src)) & 0xffffffffull;
+      } else {
+        raw = slot[R.key_word + sl.src];
+      }
+      break;
+    }
+    case DQ_SLOT_AGGVAL: {
+      const DevRes& R = P.res[sl.res];
+      uint64_t idx = (uint64_t)(c.tile_start + r);
+      raw = R.slots[idx * R.words + R.val_word + sl.src];
+      break;
+    }
+    default:
+      raw = 0;
+  }
+  return canon(raw, sl.ctype);
+}
+
+__device__ __forceinline__ void write_reg(const DevPipe& P, const Cta& c, int s, int row, uint64_t v) {
+  const DevSlot& sl = P.slots[s];
+  st(c.reg[sl.level] + sl.smem_off + (size_t)row * sl.width, sl.width, canon(v, sl.ctype));
+}
+
+// ------------------------------------------------------------ compaction --
+
+// Keeps the selection entries whose predicate holds; order preserving.
+// Element i of the selection is handled by thread (i % kThreads); all threads
+// must call this with the same n.
+template <class Keep>
+__device__ int compact(uint16_t* sel, int n, Keep keep) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int items = (n + kThreads - 1) / kThreads;
+  uint16_t v[kMaxItems];
+  uint32_t bal[kMaxItems];
+  bool kp[kMaxItems];
+#pragma unroll
+  for (int k = 0; k < kMaxItems; ++k) {
+    kp[k] = false;
+    bal[k] = 0;
+    v[k] = 0;
+    if (k < items) {
+      int i = tid + k * kThreads;
+      if (i < n) {
+        v[k] = sel[i];
+        kp[k] = keep(v[k]);
+      }
+      bal[k] = __ballot_sync(0xffffffffu, kp[k]);
+      if (lane == 0) s_scan[k * kWarps + warp] = __popc(bal[k]);
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int total_n = items * kWarps;
+    int carry = 0;
+    for (int base = 0; base < total_n; base += 32) {
+      int x = (base + lane < total_n) ? s_scan[base + lane] : 0;
+      int incl = x;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (base + lane < total_n) s_scan[base + lane] = carry + incl - x;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0) s_scan[kMaxItems * kWarps] = carry;
+  }
+  __syncthreads();
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < kMaxItems; ++k)
+    if (k < items && kp[k]) sel[s_scan[k * kWarps + warp] + __popc(bal[k] & lt)] = v[k];
+  int total = s_scan[kMaxItems * kWarps];
+  __syncthreads();
+  return total;
+}
+
+// Exclusive block scan of one value per thread; returns the total.
+__device__ uint32_t block_exclusive_scan(uint32_t x, uint32_t& excl) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_scan[warp] = (int32_t)incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < kWarps ? (uint32_t)s_scan[lane] : 0;
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < kWarps) s_scan[32 + lane] = (int32_t)(wi - w);
+    if (lane == kWarps - 1) s_scan[63] = (int32_t)wi;
+  }
+  __syncthreads();
+  excl = (uint32_t)s_scan[32 + warp] + incl - x;
+  uint32_t total = (uint32_t)s_scan[63];
+  __syncthreads();
+  return total;
+}
+
+// ------------------------------------------------------------- hashing --
+
+__device__ __forceinline__ void key_values(const DevPipe& P, const Cta& c, const DevRes& R, int list,
+                                           int nlist, int level, int row, uint64_t* k) {
+  for (int i = 0; i < nlist; ++i) k[i] = canon(read_slot(P, c, P.lists[list + i], level, row), R.key_ctype[i]);
+}
+
+// Packed tag (exact key) or 63-bit hash tag for wide keys.
+__device__ __forceinline__ uint64_t key_tag(const DevRes& R, const uint64_t* k) {
+  if (R.packed) {
+    if (R.nkeys == 0) return 0;
+    if (R.nkeys == 1 && (R.key_ctype[0] == DQ_I64 || R.key_ctype[0] == DQ_U64)) return k[0];
+    uint64_t t = (uint32_t)k[0];
+    if (R.nkeys > 1) t |= (uint64_t)(uint32_t)k[1] << 32;
+    return t;
+  }
+  uint64_t h = 0x9e3779b97f4a7c15ull;
+  for (int i = 0; i < R.nkeys; ++i) h = fmix64(h ^ k[i]) + 0x632be59bd9b4e019ull * (i + 1);
+  return fmix64(h) & 0x7fffffffffffffffull;
+}
+
+__device__ __forceinline__ uint64_t multimap_hash(const uint64_t* k, int n) {
+  uint64_t h = 0x9e3779b97f4a7c15ull;
+  for (int i = 0; i < n; ++i) h = fmix64(h ^ k[i]) + 0x632be59bd9b4e019ull * (i + 1);
+  return fmix64(h);
+}
+
+// Unique join table: returns slot index or -1.
+__device__ int64_t unique_find(const DevRes& R, uint64_t tag, const uint64_t* k) {
+  if (R.packed && tag == kEmpty) return R.slots[R.cap * R.words] == 0 ? (int64_t)R.cap : -1;
+  uint64_t idx = reduce_range(fmix64(tag), R.cap);
+  for (uint64_t n = 0; n < R.cap; ++n) {
+    const uint64_t* s = R.slots + idx * R.words;
+    uint64_t t = s[0];
+    if (t == kEmpty) return -1;
+    if (t == tag) {
+      bool eq = true;
+      if (!R.packed)
+        for (int i = 0; i < R.nkeys; ++i) eq &= s[R.key_word + i] == k[i];
+      if (eq) return (int64_t)idx;
+    }
+    idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+  }
+  return -1;
+}
+
+// Inserts the key; returns the slot to write the payload to, or -1 if the key
+// was present already (first insert wins) or the table is full.
+__device__ int64_t unique_insert(const DevPipe& P, const DevRes& R, uint64_t tag, const uint64_t* k) {
+  if (R.packed && tag == kEmpty) {
+    uint64_t old = atomicCAS((unsigned long long*)(R.slots + R.cap * R.words), kEmpty, 0ull);
+    return old == kEmpty ? (int64_t)R.cap : -1;
+  }
+  uint64_t idx = reduce_range(fmix64(tag), R.cap);
+  for (uint64_t n = 0; n < R.cap; ++n) {
+    uint64_t* s = R.slots + idx * R.words;
+    uint64_t old = atomicCAS((unsigned long long*)s, kEmpty, tag);
+    if (old == kEmpty) {
+      if (!R.packed)
+        for (int i = 0; i < R.nkeys; ++i) s[R.key_word + i] = k[i];
+      return (int64_t)idx;
+    }
+    if (old == tag && R.packed) return -1;
+    idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+  }
+  set_status(P, kErrHtFull);
+  return -1;
+}
+
+// Aggregation table (global): find or claim the group's slot.
+__device__ int64_t agg_slot_global(const DevPipe& P, const DevRes& R, uint64_t tag, const uint64_t* k) {
+  if (R.nkeys == 0) return 0;  // one group, always at slot 0
+  if (R.packed) {
+    if (tag == kEmpty) {
+      atomicCAS((unsigned long long*)(R.slots + R.cap * R.words), kEmpty, 0ull);
+      return (int64_t)R.cap;
+    }
+    uint64_t idx = reduce_range(fmix64(tag), R.cap);
+    for (uint64_t n = 0; n < R.cap; ++n) {
+      uint64_t* s = R.slots + idx * R.words;
+      uint64_t t = *(volatile uint64_t*)s;
+      if (t == tag) return (int64_t)idx;
+      if (t == kEmpty) {
+        uint64_t old = atomicCAS((unsigned long long*)s, kEmpty, tag);
+        if (old == kEmpty || old == tag) return (int64_t)idx;
+      }
+      idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+    }
+    set_status(P, kErrHtFull);
+    return -1;
+  }
+  // wide keys: claim with a busy marker, publish keys, then the tag
+  uint64_t idx = reduce_range(fmix64(tag), R.cap);
+  for (uint64_t n = 0; n < R.cap; ++n) {
+    uint64_t* s = R.slots + idx * R.words;
+    uint64_t t = *(volatile uint64_t*)s;
+    if (t == kEmpty) {
+      uint64_t old = atomicCAS((unsigned long long*)s, kEmpty, kBusy);
+      if (old == kEmpty) {
+        for (int i = 0; i < R.nkeys; ++i) s[R.key_word + i] = k[i];
+        __threadfence();
+        atomicExch((unsigned long long*)s, tag);
+        return (int64_t)idx;
+      }
+      t = old;
+    }
+    long long spins = 0;
+    while (t == kBusy && spins < kSpinLimit) {
+      t = *(volatile uint64_t*)s;
+      ++spins;
+    }
+    if (t == kBusy) {
+      set_status(P, kErrTimeout);
+      return -1;
+    }
+    if (t == tag) {
+      __threadfence();
+      bool eq = true;
+      for (int i = 0; i < R.nkeys; ++i) eq &= ((volatile uint64_t*)s)[R.key_word + i] == k[i];
+      if (eq) return (int64_t)idx;
+    }
+    idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+  }
+  set_status(P, kErrHtFull);
+  return -1;
+}
+
+__device__ __forceinline__ void accumulate(uint64_t* acc, int red, uint64_t v) {
+  switch (red) {
+    case DQ_RED_SUM: atomicAdd((unsigned long long*)acc, v); break;
+    case DQ_RED_COUNT: atomicAdd((unsigned long long*)acc, 1ull); break;
+    case DQ_RED_MIN: atomicMin((unsigned long long*)acc, v); break;
+    case DQ_RED_MAX: atomicMax((unsigned long long*)acc, v); break;
+  }
+}
+
+__device__ __forceinline__ uint64_t red_init(int red) { return red == DQ_RED_MIN ? ~0ull : 0ull; }
+
+// CTA-local aggregation table in shared memory: (ns+1) tags then accumulators.
+struct LocalAgg {
+  uint64_t* tags;
+  uint64_t* acc;
+  int ns;
+};
+
+__device__ __forceinline__ LocalAgg local_agg(const DevPipe& P, const Cta& c, const DevRes& R) {
+  LocalAgg a;
+  a.ns = R.smem_slots;
+  a.tags = reinterpret_cast<uint64_t*>(c.smem + R.smem_off);
+  a.acc = a.tags + (a.ns + 1);
+  return a;
+}
+
+__device__ int local_slot(const LocalAgg& a, uint64_t tag, int nkeys) {
+  if (nkeys == 0) {
+    a.tags[0] = 0;  // mark the single group present
+    return 0;
+  }
+  if (tag == kEmpty) {
+    atomicCAS((unsigned long long*)&a.tags[a.ns], kEmpty, 0ull);
+    return a.ns;
+  }
+  uint32_t idx = (uint32_t)reduce_range(fmix64(tag), (uint64_t)a.ns);
+  for (int n = 0; n < a.ns; ++n) {
+    uint64_t t = *(volatile uint64_t*)&a.tags[idx];
+    if (t == tag) return (int)idx;
+    if (t == kEmpty) {
+      uint64_t old = atomicCAS((unsigned long long*)&a.tags[idx], kEmpty, tag);
+      if (old == kEmpty || old == tag) return (int)idx;
+    }
+    idx = (idx + 1 == (uint32_t)a.ns) ? 0 : idx + 1;
+  }
+  return -1;
+}
+
+// ---------------------------------------------------------------- ops --
+
+struct Level {
+  int level;   // current expansion level
+  int n;       // selected rows at this level
+};
+
+__device__ void op_expr(const DevPipe& P, const Cta& c, const dq_op& op, const Level& L) {
+  const uint16_t* sel = c.sel[L.level];
+  for (int i = threadIdx.x; i < L.n; i += kThreads) {
+    int row = sel[i];
+    uint64_t r = 0;
+    switch (op.kind) {
+      case DQ_OP_ARITH: {
+        uint64_t a = (op.flags & DQ_OPF_A_IMM) ? (uint64_t)op.imm : read_slot(P, c, op.a, L.level, row);
+        uint64_t b = (op.flags & DQ_OPF_B_IMM) ? (uint64_t)op.imm : read_slot(P, c, op.b, L.level, row);
+        r = arith(op.sub, op.ctype, a, b);
+        break;
+      }
+      case DQ_OP_CMP: {
+        uint64_t a = (op.flags & DQ_OPF_A_IMM) ? (uint64_t)op.imm : read_slot(P, c, op.a, L.level, row);
+        uint64_t b = (op.flags & DQ_OPF_B_IMM) ? (uint64_t)op.imm : read_slot(P, c, op.b, L.level, row);
+        r = compare(op.sub, op.ctype, a, b);
+        break;
+      }
+      case DQ_OP_LOGIC: {
+        uint64_t a = read_slot(P, c, op.a, L.level, row);
+        if (op.sub == DQ_NOT) {
+          r = a == 0;
+        } else {
+          uint64_t b = read_slot(P, c, op.b, L.level, row);
+          r = op.sub == DQ_AND ? (a != 0 && b != 0) : (a != 0 || b != 0);
+        }
+        break;
+      }
+      case DQ_OP_CAST:
+        r = canon((op.flags & DQ_OPF_A_IMM) ? (uint64_t)op.imm : read_slot(P, c, op.a, L.level, row), op.ctype);
+        break;
+      case DQ_OP_SELECT: {
+        uint64_t cond = read_slot(P, c, op.a, L.level, row);
+        if (cond) r = (op.flags & DQ_OPF_B_IMM) ? (uint64_t)op.imm : read_slot(P, c, op.b, L.level, row);
+        else r = op.c >= 0 ? read_slot(P, c, op.c, L.level, row) : read_slot(P, c, op.dst, L.level, row);
+        r = canon(r, op.ctype);
+        break;
+      }
+      case DQ_OP_LIKE:
+      case DQ_OP_STREQ: {
+        const uint8_t* s;
+        int ls;
+        read_str(P, c, op.a, L.level, row, s, ls);
+        const uint8_t* p = P.patterns + P.pat_off[op.res];
+        int lp = P.pat_off[op.res + 1] - P.pat_off[op.res];
+        if (op.kind == DQ_OP_LIKE) {
+          r = like_match(s, ls, p, lp);
+        } else {
+          bool eq = ls == lp;
+          for (int j = 0; eq && j < ls; ++j) eq = s[j] == p[j];
+          r = eq;
+        }
+        break;
+      }
+    }
+    write_reg(P, c, op.dst, row, r);
+  }
+}
+
+// Unique-table probe: payload copied into register slots, then compaction.
+__device__ int op_probe(const DevPipe& P, const Cta& c, const dq_op& op, const Level& L) {
+  const DevRes& R = P.res[op.res];
+  const uint16_t* sel = c.sel[L.level];
+  uint8_t* found = c.flags;
+  for (int i = threadIdx.x; i < L.n; i += kThreads) {
+    int row = sel[i];
+    uint64_t k[DQ_MAX_KEYS];
+    key_values(P, c, R, op.list, op.nlist, L.level, row, k);
+    uint64_t tag = key_tag(R, k);
+    int64_t s = unique_find(R, tag, k);
+    found[row] = s >= 0;
+    if (s >= 0 && op.sub == DQ_JOIN_INNER) {
+      const uint64_t* pay = R.slots + (uint64_t)s * R.words + R.val_word;
+      for (int j = 0; j < op.nlist2; ++j) {
+        int d = P.lists[op.list2 + j];
+        if (d >= 0) write_reg(P, c, d, row, pay[j]);
+      }
+    }
+  }
+  __syncthreads();
+  const bool anti = op.sub == DQ_JOIN_ANTI;
+  return compact(c.sel[L.level], L.n, [&](int row) { return anti ? found[row] == 0 : found[row] != 0; });
+}
+
+__device__ void op_build(const DevPipe& P, const Cta& c, const dq_op& op, const Level& L) {
+  const DevRes& R = P.res[op.res];
+  const uint16_t* sel = c.sel[L.level];
+  for (int i = threadIdx.x; i < L.n; i += kThreads) {
+    int row = sel[i];
+    uint64_t k[DQ_MAX_KEYS];
+    key_values(P, c, R, op.list, op.nlist, L.level, row, k);
+    int64_t s = unique_insert(P, R, key_tag(R, k), k);
+    if (s >= 0) {
+      uint64_t* pay = R.slots + (uint64_t)s * R.words + R.val_word;
+      for (int j = 0; j < op.nlist2; ++j) pay[j] = read_slot(P, c, P.lists[op.list2 + j], L.level, row);
+    }
+  }
+}
+
+__device__ void op_mm(const DevPipe& P, const Cta& c, const dq_op& op, const Level& L) {
+  const DevRes& R = P.res[op.res];
+  const uint16_t* sel = c.sel[L.level];
+  for (int i = threadIdx.x; i < L.n; i += kThreads) {
+    int row = sel[i];
+    uint64_t k[DQ_MAX_KEYS];
+    key_values(P, c, R, op.list, op.nlist, L.level, row, k);
+    uint64_t b = reduce_range(multimap_hash(k, op.nlist), R.cap);
+    if (op.kind == DQ_OP_MM_COUNT) {
+      atomicAdd(&R.counts[b], 1u);
+    } else {
+      uint32_t pos = R.offsets[b] + atomicAdd(&R.counts[b], 1u);
+      for (int j = 0; j < op.nlist2; ++j)
+        st(R.pay[j] + (size_t)pos * R.pay_width[j], R.pay_width[j],
+           read_slot(P, c, P.lists[op.list2 + j], L.level, row));
+    }
+  }
+}
+
+__device__ void op_agg(const DevPipe& P, const Cta& c, const dq_op& op, const Level& L) {
+  const DevRes& R = P.res[op.res];
+  const uint16_t* sel = c.sel[L.level];
+  const bool local = R.smem_slots > 0;
+  LocalAgg la;
+  if (local) la = local_agg(P, c, R);
+  for (int i = threadIdx.x; i < L.n; i += kThreads) {
+    int row = sel[i];
+    uint64_t k[DQ_MAX_KEYS];
+    key_values(P, c, R, op.list, op.nlist, L.level, row, k);
+    uint64_t tag = key_tag(R, k);
+    uint64_t* acc = nullptr;
+    if (local) {
+      int s = local_slot(la, tag, R.nkeys);
+      if (s >= 0) acc = la.acc + (size_t)s * R.naggs;
+    }
+    if (!acc) {
+      int64_t g = agg_slot_global(P, R, tag, k);
+      if (g < 0) continue;
+      acc = R.slots + (uint64_t)g * R.words + R.val_word;
+    }
+    for (int j = 0; j < R.naggs; ++j) {
+      int src = P.lists[op.list2 + j];
+      uint64_t v = src >= 0 ? read_slot(P, c, src, L.level, row) : 1;
+      accumulate(acc + j, R.agg_red[j], v);
+    }
+  }
+}
+
+__device__ void op_emit(const DevPipe& P, const Cta& c, const dq_op& op, const Level& L) {
+  const DevRes& R = P.res[op.res];
+  const uint16_t* sel = c.sel[L.level];
+  if (threadIdx.x == 0) s_bcast[0] = L.n ? atomicAdd((unsigned long long*)R.cursor, (unsigned long long)L.n) : 0;
+  __syncthreads();
+  uint64_t base = s_bcast[0];
+  __syncthreads();
+  if (base + L.n > R.cap) set_status(P, kErrOverflow);
+  for (int i = threadIdx.x; i < L.n; i += kThreads) {
+    uint64_t pos = base + i;
+    if (pos >= R.cap) break;
+    int row = sel[i];
+    for (int j = 0; j < op.nlist; ++j)
+      st(R.pay[j] + pos * R.pay_width[j], R.pay_width[j], read_slot(P, c, P.lists[op.list + j], L.level, row));
+  }
+}
+
+// ------------------------------------------------------------ expansion --
+
+struct Frame {
+  int op;          // EXPAND op index
+  int level;       // parent level
+  int pn;          // selected parent rows
+  uint32_t total;  // pairs of the parent selection
+  uint32_t next;   // first pair of the next chunk
+};
+
+// Sets up an expansion over the selected rows of level L: ranges, deferral of
+// wide ranges, and the exclusive scan of range lengths.  Returns total pairs.
+__device__ uint32_t expand_setup(const DevPipe& P, const Cta& c, const dq_op& op, const Level& L) {
+  const DevRes& R = P.res[op.res];
+  const uint16_t* sel = c.sel[L.level];
+  const int tid = threadIdx.x;
+  const bool defer = L.level == 0 && P.heavy.cap > 0 && !c.heavy;
+  // each thread owns a contiguous run of selection entries
+  const int per = (L.n + kThreads - 1) / kThreads;
+  const int i0 = min(tid * per, L.n), i1 = min(i0 + per, L.n);
+  uint32_t* eoff = c.eoff[L.level];
+  uint32_t* ecnt = c.ecnt[L.level];
+  uint32_t* epos = c.epos[L.level];
+  uint32_t local = 0;
+  for (int i = i0; i < i1; ++i) {
+    int row = sel[i];
+    uint64_t k[DQ_MAX_KEYS];
+    key_values(P, c, R, op.list, op.nlist, L.level, row, k);
+    uint64_t b = reduce_range(multimap_hash(k, op.nlist), R.cap);
+    uint32_t cnt = R.counts[b];
+    uint32_t off = cnt ? R.offsets[b] : 0;
+    if (defer && cnt > P.heavy.threshold) {
+      uint32_t slot = atomicAdd(P.heavy.count, 1u);
+      if (slot < P.heavy.cap) {
+        uint64_t* it = P.heavy.items + (size_t)slot * P.heavy.words;
+        it[0] = off;
+        it[1] = cnt;
+        int j = 0;
+        for (int s = 0; s < P.nslots && j < P.heavy.nstash; ++s)
+          if (P.slots[s].stash >= 0) it[2 + P.slots[s].stash] = read_slot(P, c, s, 0, row), ++j;
+        cnt = 0;
+      }
+    }
+    eoff[i] = off;
+    ecnt[i] = cnt;
+    local += cnt;
+  }
+  uint32_t excl;
+  uint32_t total = block_exclusive_scan(local, excl);
+  for (int i = i0; i < i1; ++i) {
+    epos[i] = excl;
+    excl += ecnt[i];
+  }
+  __syncthreads();
+  return total;
+}
+
+// Produces pairs [base, base+n) of the expansion as level L+1 rows, checks the
+// build keys, and returns the number of matching rows.
+__device__ int expand_chunk(const DevPipe& P, const Cta& c, const dq_op& op, int parent_level, int parent_n,
+                            uint32_t base, int n) {
+  const int tid = threadIdx.x;
+  const int lv = parent_level + 1;
+  const uint16_t* psel = c.sel[parent_level];
+  const int per = (n + kThreads - 1) / kThreads;
+  const int j0 = min(tid * per, n), j1 = min(j0 + per, n);
+  const uint32_t* eoff = c.eoff[parent_level];
+  const uint32_t* ecnt = c.ecnt[parent_level];
+  const uint32_t* epos = c.epos[parent_level];
+  if (j0 < j1) {
+    uint32_t g = base + j0;
+    // last parent whose first pair is <= g
+    int lo = 0, hi = parent_n;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (epos[mid] <= g) lo = mid + 1;
+      else hi = mid;
+    }
+    int i = lo - 1;
+    for (int j = j0; j < j1; ++j, ++g) {
+      while (g >= epos[i] + ecnt[i]) ++i;
+      c.par[lv][j] = psel[i];
+      c.match[lv][j] = eoff[i] + (g - epos[i]);
+      c.sel[lv][j] = (uint16_t)j;
+    }
+  }
+  __syncthreads();
+  // key check: build keys are payload columns gathered at the new level
+  return compact(c.sel[lv], n, [&](int row) {
+    bool eq = true;
+    for (int q = 0; q < op.nlist; ++q) {
+      uint64_t pk = read_slot(P, c, P.lists[op.list + q], lv, row);
+      uint64_t bk = read_slot(P, c, P.lists[op.list2 + q], lv, row);
+      int t = P.res[op.res].key_ctype[q];
+      eq &= canon(pk, t) == canon(bk, t);
+    }
+    return eq;
+  });
+}
+
+// Runs ops [start, nops) over the current selection; handles expansion frames.
+__device__ void run_ops(const DevPipe& P, Cta& c, int start, Level L) {
+  Frame fr[DQ_MAX_LEVELS];
+  int depth = 0;
+  int k = start;
+  while (true) {
+    if (k >= P.nops) {
+      // resume the innermost expansion that still has chunks
+      bool resumed = false;
+      while (depth > 0) {
+        Frame& f = fr[depth - 1];
+        if (f.next < f.total) {
+          uint32_t n = min((uint32_t)P.exp_cap, f.total - f.next);
+          int got = expand_chunk(P, c, P.ops[f.op], f.level, f.pn, f.next, (int)n);
+          f.next += n;
+          L.level = f.level + 1;
+          L.n = got;
+          k = f.op + 1;
+          resumed = true;
+          break;
+        }
+        --depth;
+      }
+      if (!resumed) return;
+      continue;
+    }
+    const dq_op& op = P.ops[k];
+    switch (op.kind) {
+      case DQ_OP_ARITH:
+      case DQ_OP_CMP:
+      case DQ_OP_LOGIC:
+      case DQ_OP_CAST:
+      case DQ_OP_SELECT:
+      case DQ_OP_LIKE:
+      case DQ_OP_STREQ:
+        op_expr(P, c, op, L);
+        __syncthreads();
+        ++k;
+        break;
+      case DQ_OP_FILTER: {
+        L.n = compact(c.sel[L.level], L.n,
+                      [&](int row) { return read_slot(P, c, op.a, L.level, row) != 0; });
+        ++k;
+        break;
+      }
+      case DQ_OP_PROBE:
+        L.n = op_probe(P, c, op, L);
+        ++k;
+        break;
+      case DQ_OP_EXPAND: {
+        if (L.level + 1 >= DQ_MAX_LEVELS) {
+          set_status(P, kErrBadOp);
+          return;
+        }
+        uint32_t total;
+        if (c.heavy && L.level == 0) {
+          total = c.ecnt[0][0];  // prepared by the heavy-unit loop
+        } else {
+          total = expand_setup(P, c, op, L);
+        }
+        fr[depth].op = k;
+        fr[depth].level = L.level;
+        fr[depth].pn = L.n;
+        fr[depth].total = total;
+        fr[depth].next = 0;
+        ++depth;
+        k = P.nops;  // the resume logic produces the first chunk
+        break;
+      }
+      case DQ_OP_AGG:
+        op_agg(P, c, op, L);
+        __syncthreads();
+        k = P.nops;
+        break;
+      case DQ_OP_BUILD:
+        op_build(P, c, op, L);
+        __syncthreads();
+        k = P.nops;
+        break;
+      case DQ_OP_MM_COUNT:
+      case DQ_OP_MM_SCATTER:
+        op_mm(P, c, op, L);
+        __syncthreads();
+        k = P.nops;
+        break;
+      case DQ_OP_EMIT:
+        op_emit(P, c, op, L);
+        __syncthreads();
+        k = P.nops;
+        break;
+      default:
+        set_status(P, kErrBadOp);
+        return;
+    }
+  }
+}
+
+// ------------------------------------------------------------- staging --
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(phase)
+      : "memory");
+  return done != 0;
+}
+
+// Bounded wait; on exhaustion flags a timeout (the data is then not used).
+__device__ __forceinline__ bool mbar_wait(const DevPipe& P, uint64_t* bar, uint32_t phase) {
+  for (long long i = 0; i < (1ll << 24); ++i)
+    if (mbar_try_wait(bar, phase)) return true;
+  set_status(P, kErrTimeout);
+  return false;
+}
+
+__device__ __forceinline__ int64_t source_rows(const DevPipe& P) {
+  return P.nrows_dev ? (int64_t)*P.nrows_dev : P.nrows;
+}
+
+// Issues the copies of tile `t` into stage buffer `dst` (thread 0 only).
+__device__ void stage_issue(const DevPipe& P, uint8_t* dst, int64_t t, int64_t nrows, uint64_t* bar) {
+  const int64_t start = t * P.tile;
+  const int64_t rows = min((int64_t)P.tile, nrows - start);
+  uint32_t total = 0;
+  for (int i = 0; i < P.ncols; ++i) total += (uint32_t)((rows * P.cols[i].width + 15) & ~15ll);
+  mbar_expect_tx(bar, total);
+  for (int i = 0; i < P.ncols; ++i) {
+    const DevCol& col = P.cols[i];
+    uint32_t bytes = (uint32_t)((rows * col.width + 15) & ~15ll);
+    tma_load_1d(dst + col.smem_off, col.ptr + start * col.width, bytes, bar);
+  }
+}
+
+// Plain cooperative copy of a tile (used when TMA staging is disabled).
+__device__ void stage_plain(const DevPipe& P, uint8_t* dst, int64_t t, int64_t nrows) {
+  const int64_t start = t * P.tile;
+  const int64_t rows = min((int64_t)P.tile, nrows - start);
+  for (int i = 0; i < P.ncols; ++i) {
+    const DevCol& col = P.cols[i];
+    int64_t bytes = (rows * col.width + 15) & ~15ll;
+    const uint4* s = reinterpret_cast<const uint4*>(col.ptr + start * col.width);
+    uint4* d = reinterpret_cast<uint4*>(dst + col.smem_off);
+    for (int64_t j = threadIdx.x; j < bytes / 16; j += kThreads) d[j] = s[j];
+  }
+}
+
+// ----------------------------------------------------------- the kernel --
+
+__device__ void init_cta(const DevPipe& P, Cta& c, uint8_t* smem) {
+  c.smem = smem;
+  c.heavy = P.mode == 1;
+  for (int l = 0; l < DQ_MAX_LEVELS; ++l) {
+    c.reg[l] = smem + P.off_reg[l];
+    c.sel[l] = reinterpret_cast<uint16_t*>(smem + P.off_sel[l]);
+    c.par[l] = reinterpret_cast<uint16_t*>(smem + P.off_par[l]);
+    c.match[l] = reinterpret_cast<uint32_t*>(smem + P.off_match[l]);
+  }
+  for (int l = 0; l < DQ_MAX_LEVELS; ++l) {
+    c.eoff[l] = reinterpret_cast<uint32_t*>(smem + P.off_exp) + (size_t)l * 3 * P.tile;
+    c.ecnt[l] = c.eoff[l] + P.tile;
+    c.epos[l] = c.ecnt[l] + P.tile;
+  }
+  c.flags = smem + P.off_flags;
+  c.stash = reinterpret_cast<uint64_t*>(smem + P.off_stash);
+  c.stage = smem + P.off_stage;
+  c.tile_start = 0;
+  // CTA-local aggregation tables
+  for (int r = 0; r < P.nres; ++r) {
+    const DevRes& R = P.res[r];
+    if (R.kind == DQ_RES_AGG && R.smem_slots > 0) {
+      LocalAgg a = local_agg(P, c, R);
+      for (int i = threadIdx.x; i <= a.ns; i += kThreads) a.tags[i] = kEmpty;
+      for (int i = threadIdx.x; i < (a.ns + 1) * R.naggs; i += kThreads) a.acc[i] = red_init(R.agg_red[i % R.naggs]);
+    }
+  }
+  __syncthreads();
+}
+
+__device__ void flush_local_aggs(const DevPipe& P, Cta& c) {
+  __syncthreads();
+  for (int r = 0; r < P.nres; ++r) {
+    const DevRes& R = P.res[r];
+    if (R.kind != DQ_RES_AGG || R.smem_slots <= 0) continue;
+    LocalAgg a = local_agg(P, c, R);
+    for (int i = threadIdx.x; i <= a.ns; i += kThreads) {
+      uint64_t tag = a.tags[i];
+      if (tag == kEmpty) continue;
+      if (i == a.ns) tag = kEmpty;  // the all-ones key
+      int64_t g = R.nkeys == 0 ? 0 : agg_slot_global(P, R, tag, nullptr);
+      if (g < 0) continue;
+      uint64_t* acc = R.slots + (uint64_t)g * R.words + R.val_word;
+      for (int j = 0; j < R.naggs; ++j) {
+        uint64_t v = a.acc[(size_t)i * R.naggs + j];
+        int red = R.agg_red[j];
+        if (red == DQ_RED_COUNT) atomicAdd((unsigned long long*)(acc + j), v);
+        else accumulate(acc + j, red, v);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 2) pipeline_kernel(const __grid_constant__ DevPipe P) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t s_mbar[kMaxStages];
+  __shared__ int64_t s_tile[kMaxStages];
+  // an earlier pipeline of this run overflowed a table: the host re-runs the
+  // plan with larger tables, so skip the work (probing a full table is slow)
+  if (*(volatile int32_t*)P.status & (kErrHtFull | kErrTimeout)) return;
+  Cta c;
+  init_cta(P, c, smem);
+  const int tid = threadIdx.x;
+
+  if (P.mode == 1) {
+    // deferred expansion ranges: work units of exp_cap pairs
+    const uint32_t nitems = min(*P.heavy.count, P.heavy.cap);
+    const uint64_t units = P.heavy.unit_prefix[nitems];
+    const dq_op& op = P.ops[P.heavy.op];
+    while (true) {
+      if (tid == 0) s_bcast[1] = atomicAdd(P.tile_counter, 1u);
+      __syncthreads();
+      uint64_t u = s_bcast[1];
+      __syncthreads();
+      if (u >= units) break;
+      int lo = 0, hi = (int)nitems;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (P.heavy.unit_prefix[mid + 1] <= u) lo = mid + 1;
+        else hi = mid;
+      }
+      const uint64_t* it = P.heavy.items + (size_t)lo * P.heavy.words;
+      uint64_t chunk = u - P.heavy.unit_prefix[lo];
+      uint64_t off = it[0] + chunk * P.exp_cap;
+      uint64_t len = min((uint64_t)P.exp_cap, it[1] - chunk * P.exp_cap);
+      for (int s = tid; s < P.heavy.nstash; s += kThreads) c.stash[s] = it[2 + s];
+      if (tid == 0) {
+        c.sel[0][0] = 0;
+        c.eoff[0][0] = (uint32_t)off;
+        c.ecnt[0][0] = (uint32_t)len;
+        c.epos[0][0] = 0;
+      }
+      __syncthreads();
+      Level L{0, 1};
+      run_ops(P, c, P.heavy.op, L);
+      (void)op;
+      __syncthreads();
+    }
+    flush_local_aggs(P, c);
+    return;
+  }
+
+  const int64_t nrows = source_rows(P);
+  const int64_t ntiles = (nrows + P.tile - 1) / P.tile;
+  const bool staged = P.ncols > 0;
+  const bool tma = staged && P.use_tma;
+
+  if (tma) {
+    if (tid == 0) {
+      for (int s = 0; s < P.nstage; ++s) mbar_init(&s_mbar[s], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      for (int s = 0; s < P.nstage; ++s) {
+        int64_t t = atomicAdd(P.tile_counter, 1u);
+        s_tile[s] = t;
+        if (t < ntiles) stage_issue(P, smem + P.off_stage + s * P.stage_bytes, t, nrows, &s_mbar[s]);
+      }
+    }
+    __syncthreads();
+  }
+
+  uint32_t phase_bits = 0;
+  for (int64_t iter = 0;; ++iter) {
+    const int s = tma ? (int)(iter % P.nstage) : 0;
+    int64_t t;
+    if (tma) {
+      t = s_tile[s];
+    } else {
+      if (tid == 0) s_bcast[1] = atomicAdd(P.tile_counter, 1u);
+      __syncthreads();
+      t = (int64_t)s_bcast[1];
+      __syncthreads();
+    }
+    if (t >= ntiles) break;
+    c.stage = smem + P.off_stage + s * P.stage_bytes;
+    c.tile_start = t * P.tile;
+    const int rows = (int)min((int64_t)P.tile, nrows - c.tile_start);
+    if (tma) {
+      mbar_wait(P, &s_mbar[s], (phase_bits >> s) & 1u);
+      phase_bits ^= 1u << s;
+    } else if (staged) {
+      stage_plain(P, smem + P.off_stage, t, nrows);
+      __syncthreads();
+    }
+    // initial selection: every row of the tile (occupied slots for AGG sources)
+    for (int i = tid; i < rows; i += kThreads) c.sel[0][i] = (uint16_t)i;
+    __syncthreads();
+    Level L{0, rows};
+    if (P.source_kind == DQ_SRC_AGG && P.res[P.source_res].nkeys > 0) {
+      const DevRes& R = P.res[P.source_res];
+      L.n = compact(c.sel[0], rows, [&](int row) {
+        return R.slots[(uint64_t)(c.tile_start + row) * R.words] != kEmpty;
+      });
+    }
+    run_ops(P, c, 0, L);
+    __syncthreads();
+    if (tma && tid == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      int64_t nt = atomicAdd(P.tile_counter, 1u);
+      s_tile[s] = nt;
+      if (nt < ntiles) stage_issue(P, smem + P.off_stage + s * P.stage_bytes, nt, nrows, &s_mbar[s]);
+    }
+    __syncthreads();
+  }
+  flush_local_aggs(P, c);
+}
+
+// ------------------------------------------------------- helper kernels --
+
+// Fills aggregation tables: tags empty, accumulators at their initial values.
+__global__ void agg_init_kernel(uint64_t* slots, uint64_t nslots, int words, int val_word, int naggs,
+                                uint64_t red_packed) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nslots * words;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t w = i % words;
+    uint64_t v = kEmpty;
+    if ((int)w >= val_word && (int)w < val_word + naggs) {
+      int red = (int)((red_packed >> (4 * (w - val_word))) & 15);
+      v = red_init(red);
+    }
+    slots[i] = v;
+  }
+}
+
+// Multimap bucket offsets: exclusive scan of counts in three passes.
+constexpr int kScanItems = 8;
+constexpr int kScanChunk = kThreads * kScanItems;
+
+__global__ void mm_scan_partials(const uint32_t* counts, uint64_t n, uint32_t* partials) {
+  uint64_t base = (uint64_t)blockIdx.x * kScanChunk;
+  uint32_t sum = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    uint64_t i = base + (uint64_t)k * kThreads + threadIdx.x;
+    if (i < n) sum += counts[i];
+  }
+  uint32_t excl;
+  uint32_t total = block_exclusive_scan(sum, excl);
+  if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+__global__ void mm_scan_top(uint32_t* partials, int nblocks) {
+  uint32_t carry = 0;
+  for (int base = 0; base < nblocks; base += kThreads) {
+    int i = base + threadIdx.x;
+    uint32_t x = i < nblocks ? partials[i] : 0;
+    uint32_t excl;
+    uint32_t total = block_exclusive_scan(x, excl);
+    if (i < nblocks) partials[i] = carry + excl;
+    carry += total;
+  }
+}
+
+__global__ void mm_scan_final(uint32_t* counts, uint32_t* offsets, uint64_t n, const uint32_t* partials) {
+  uint64_t base = (uint64_t)blockIdx.x * kScanChunk;
+  uint64_t i0 = base + (uint64_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t sum = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = (i0 + k < n) ? counts[i0 + k] : 0;
+    sum += v[k];
+  }
+  uint32_t excl;
+  block_exclusive_scan(sum, excl);
+  uint32_t run = partials[blockIdx.x] + excl;
+  for (int k = 0; k < kScanItems; ++k) {
+    if (i0 + k < n) {
+      offsets[i0 + k] = run;
+      counts[i0 + k] = 0;
+    }
+    run += v[k];
+  }
+}
+
+// Work-unit prefix over deferred expansion items (one block).
+__global__ void heavy_prefix_kernel(const uint64_t* items, const uint32_t* count, uint32_t cap, int words,
+                                    uint64_t exp_cap, uint64_t* prefix) {
+  const uint32_t n = min(*count, cap);
+  uint64_t carry = 0;
+  for (uint32_t base = 0; base < n || base == 0; base += kThreads) {
+    uint32_t i = base + threadIdx.x;
+    uint32_t u = i < n ? (uint32_t)((items[(size_t)i * words + 1] + exp_cap - 1) / exp_cap) : 0;
+    uint32_t excl;
+    uint32_t total = block_exclusive_scan(u, excl);
+    if (i < n) prefix[i] = carry + excl;
+    carry += total;
+    if (base + kThreads >= n) break;
+  }
+  if (threadIdx.x == 0) prefix[n] = carry;
+}
+
+}  // namespace dq
+
+// ------------------------------------------------------ host-side launchers --
+
+namespace dq {
+
+cudaError_t launch_pipeline(const DevPipe& P, int grid, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(pipeline_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem_bytes);
+  if (e != cudaSuccess) return e;
+  pipeline_kernel<<<grid, kThreads, P.smem_bytes, stream>>>(P);
+  return cudaGetLastError();
+}
+
+int pipeline_occupancy(int smem_bytes) {
+  int blocks = 0;
+  cudaFuncSetAttribute(pipeline_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, pipeline_kernel, kThreads, smem_bytes);
+  return blocks;
+}
+
+cudaError_t launch_agg_init(uint64_t* slots, uint64_t nslots, int words, int val_word, int naggs,
+                            const int8_t* reds, cudaStream_t stream) {
+  uint64_t packed = 0;
+  for (int j = 0; j < naggs && j < 16; ++j) packed |= (uint64_t)(reds[j] & 15) << (4 * j);
+  uint64_t total = nslots * words;
+  uint64_t want = (total + 255) / 256;
+  int grid = (int)(want < 148ull * 16 ? want : 148ull * 16);
+  if (grid < 1) grid = 1;
+  agg_init_kernel<<<grid, 256, 0, stream>>>(slots, nslots, words, val_word, naggs, packed);
+  return cudaGetLastError();
+}
+
+size_t mm_scan_scratch_words(uint64_t n) { return (n + kScanChunk - 1) / kScanChunk + 1; }
+
+cudaError_t launch_mm_scan(uint32_t* counts, uint32_t* offsets, uint64_t n, uint32_t* partials,
+                           cudaStream_t stream, int* launches) {
+  int nblocks = (int)((n + kScanChunk - 1) / kScanChunk);
+  if (nblocks < 1) nblocks = 1;
+  mm_scan_partials<<<nblocks, kThreads, 0, stream>>>(counts, n, partials);
+  mm_scan_top<<<1, kThreads, 0, stream>>>(partials, nblocks);
+  mm_scan_final<<<nblocks, kThreads, 0, stream>>>(counts, offsets, n, partials);
+  *launches += 3;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_heavy_prefix(const DevHeavy& H, uint64_t exp_cap, cudaStream_t stream) {
+  heavy_prefix_kernel<<<1, kThreads, 0, stream>>>(H.items, H.count, H.cap, H.words, exp_cap, H.unit_prefix);
+  return cudaGetLastError();
+}
+
+}  // namespace dq

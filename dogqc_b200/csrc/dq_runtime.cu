@@ -1,0 +1,941 @@
+// Host runtime behind the C ABI (include/dogqc_b200.h).
+//
+// It owns device memory for registered tables and for every plan's resources,
+// turns the plan IR into pipeline launch descriptors (shared-memory layout,
+// resource layouts, tile sizes, persistent grid size), and executes a plan as
+// a stream-ordered sequence of launches.  Where the reference's generated
+// main() re-allocates, copies and frees everything per query and times launches
+// with std::clock (dogqc/codegen.py:121-159, dogqc/code.py:4-26), this runtime
+// keeps tables and hash tables resident, resets them with memsets, and times
+// launches with CUDA events on the launching stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/dogqc_b200.h"
+#include "dq_device.h"
+
+namespace dq {
+cudaError_t launch_pipeline(const DevPipe& P, int grid, cudaStream_t stream);
+int pipeline_occupancy(int smem_bytes);
+cudaError_t launch_agg_init(uint64_t* slots, uint64_t nslots, int words, int val_word, int naggs,
+                            const int8_t* reds, cudaStream_t stream);
+size_t mm_scan_scratch_words(uint64_t n);
+cudaError_t launch_mm_scan(uint32_t* counts, uint32_t* offsets, uint64_t n, uint32_t* partials,
+                           cudaStream_t stream, int* launches);
+cudaError_t launch_heavy_prefix(const DevHeavy& H, uint64_t exp_cap, cudaStream_t stream);
+}  // namespace dq
+
+using namespace dq;
+
+namespace {
+
+std::string g_init_error;
+
+struct DqError : std::runtime_error {
+  int code;
+  DqError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define DQ_CUDA(expr)                                                                        \
+  do {                                                                                       \
+    cudaError_t _e = (expr);                                                                 \
+    if (_e != cudaSuccess)                                                                   \
+      throw DqError(_e == cudaErrorMemoryAllocation ? DQ_ERR_OOM : DQ_ERR_CUDA,              \
+                    std::string(#expr) + ": " + cudaGetErrorString(_e));                     \
+  } while (0)
+
+int ctype_width(int t) {
+  switch (t) {
+    case DQ_I8: return 1;
+    case DQ_I32:
+    case DQ_U32: return 4;
+    case DQ_I64:
+    case DQ_U64: return 8;
+    default: return 0;
+  }
+}
+
+uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+
+// Device buffer with 256 bytes of tail padding: tile copies round their size up
+// to 16 bytes and may read past the last row.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void alloc(size_t b) {
+    release();
+    bytes = b;
+    DQ_CUDA(cudaMalloc(&ptr, align_up(b, 256) + 256));
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
+struct ColRec {
+  std::string name;
+  int ctype = 0;
+  int width = 0;       // bytes per value, or string width for fixed strings
+  uint64_t nchars = 0;
+  std::shared_ptr<DevBuf> data;
+  std::shared_ptr<DevBuf> offsets;
+};
+
+struct TableRec {
+  int64_t nrows = 0;
+  std::vector<ColRec> cols;
+  const ColRec* find(const char* n) const {
+    for (auto& c : cols)
+      if (c.name == n) return &c;
+    return nullptr;
+  }
+};
+
+}  // namespace
+
+struct dq_ctx {
+  dq_config cfg{};
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  std::mutex mu;
+  std::map<std::string, TableRec> tables;
+};
+
+struct ResRec {
+  dq_resource desc{};
+  std::string name;
+  DevRes dev{};
+  DevBuf slots, counts, offsets, cursor, scan_scratch;
+  std::vector<std::unique_ptr<DevBuf>> pay;
+  uint64_t pay_rows = 0;
+};
+
+struct PipeRec {
+  dq_pipeline desc{};
+  std::vector<std::string> col_names;
+  std::vector<std::string> patterns;
+  DevPipe dev{};
+  int grid = 1;
+  int expand_op = -1;       // level-0 expansion op with deferral
+  DevBuf pattern_buf, heavy_items, heavy_count, heavy_prefix;
+  bool mm_count = false;    // sink is a multimap count: bucket scan follows
+  int mm_res = -1;
+  int staged_cols = 0;
+};
+
+struct dq_result {
+  int64_t nrows = 0;
+  std::vector<int> ctypes;
+  std::vector<std::vector<uint8_t>> cols;
+};
+
+struct dq_plan {
+  dq_ctx* ctx = nullptr;
+  std::vector<std::unique_ptr<ResRec>> res;
+  std::vector<std::unique_ptr<PipeRec>> pipes;
+  int result_res = -1;
+  DevBuf status, counters;
+  dq_plan_timing timing{};
+  std::vector<cudaEvent_t> events;
+};
+
+namespace {
+
+int fail(dq_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->error = msg;
+  else g_init_error = msg;
+  return code;
+}
+
+template <class F>
+int guarded(dq_ctx* ctx, F f) {
+  try {
+    return f();
+  } catch (const DqError& e) {
+    return fail(ctx, e.code, e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, DQ_ERR_OOM, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(ctx, DQ_ERR_INVALID, e.what());
+  }
+}
+
+void upload_column(dq_ctx* ctx, ColRec& rec, const dq_column& c, int64_t nrows, bool device_src,
+                   cudaStream_t stream) {
+  cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (c.ctype == DQ_STR) {
+    uint64_t nchars = c.width > 0 ? (uint64_t)c.width * nrows : c.nchars;
+    if (!rec.data) rec.data = std::make_shared<DevBuf>();
+    if (rec.data->bytes != nchars || !rec.data->ptr) rec.data->alloc(nchars);
+    if (nchars) DQ_CUDA(cudaMemcpyAsync(rec.data->ptr, c.data, nchars, kind, stream));
+    rec.nchars = nchars;
+    if (c.width <= 0) {
+      if (!c.offsets) throw DqError(DQ_ERR_INVALID, "variable-width string column " + rec.name + " needs offsets");
+      if (!rec.offsets) rec.offsets = std::make_shared<DevBuf>();
+      size_t ob = (size_t)(nrows + 1) * 8;
+      if (rec.offsets->bytes != ob || !rec.offsets->ptr) rec.offsets->alloc(ob);
+      DQ_CUDA(cudaMemcpyAsync(rec.offsets->ptr, c.offsets, ob, kind, stream));
+    }
+  } else {
+    size_t b = (size_t)nrows * ctype_width(c.ctype);
+    if (!rec.data) rec.data = std::make_shared<DevBuf>();
+    if (rec.data->bytes != b || !rec.data->ptr) rec.data->alloc(b);
+    if (b) DQ_CUDA(cudaMemcpyAsync(rec.data->ptr, c.data, b, kind, stream));
+  }
+}
+
+bool keys_packed(int nkeys, const int8_t* kt) {
+  if (nkeys == 0) return true;
+  if (nkeys == 1) return true;
+  if (nkeys == 2) return ctype_width(kt[0]) <= 4 && ctype_width(kt[1]) <= 4;
+  return false;
+}
+
+// ------------------------------------------------------------- resources --
+
+void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
+  const dq_resource& d = r.desc;
+  DevRes& R = r.dev;
+  memset(&R, 0, sizeof(R));
+  R.kind = d.kind;
+  R.nkeys = d.nkeys;
+  for (int i = 0; i < DQ_MAX_KEYS; ++i) R.key_ctype[i] = d.key_ctype[i];
+  R.npay = d.npay;
+  R.naggs = d.naggs;
+  for (int i = 0; i < DQ_MAX_PAY; ++i) {
+    R.pay_ctype[i] = d.pay_ctype[i];
+    R.pay_width[i] = (int8_t)ctype_width(d.pay_ctype[i]);
+  }
+  for (int i = 0; i < DQ_MAX_AGGS; ++i) R.agg_red[i] = d.agg_red[i];
+  if (d.nkeys < 0 || d.nkeys > DQ_MAX_KEYS || d.npay < 0 || d.npay > DQ_MAX_PAY || d.naggs < 0 ||
+      d.naggs > DQ_MAX_AGGS)
+    throw DqError(DQ_ERR_BAD_IR, "resource sizes out of range");
+  uint64_t cap = (uint64_t)std::max<int64_t>(d.capacity, 1);
+  switch (d.kind) {
+    case DQ_RES_UNIQUE:
+    case DQ_RES_AGG: {
+      R.packed = keys_packed(d.nkeys, d.key_ctype);
+      R.key_word = 1;
+      R.val_word = 1 + (R.packed ? 0 : d.nkeys);
+      R.words = R.val_word + (d.kind == DQ_RES_UNIQUE ? d.npay : d.naggs);
+      cap = std::max<uint64_t>(cap, 16);
+      R.cap = cap;
+      r.slots.alloc((cap + 1) * R.words * 8);
+      R.slots = r.slots.as<uint64_t>();
+      if (d.kind == DQ_RES_AGG && R.packed) {
+        uint64_t want = std::max<int64_t>(d.group_hint, 1) * 2;
+        uint64_t ns = 16;
+        while (ns < want) ns <<= 1;
+        uint64_t bytes = (ns + 1) * (1 + d.naggs) * 8;
+        if (d.nkeys == 0) ns = 1, bytes = 2 * (1 + d.naggs) * 8;
+        R.smem_slots = bytes <= 24 * 1024 ? (int)ns : 0;
+      }
+      break;
+    }
+    case DQ_RES_MULTI: {
+      R.cap = cap;
+      r.counts.alloc(cap * 4);
+      r.offsets.alloc((cap + 1) * 4);
+      R.counts = r.counts.as<uint32_t>();
+      R.offsets = r.offsets.as<uint32_t>();
+      r.scan_scratch.alloc(mm_scan_scratch_words(cap) * 4);
+      r.pay_rows = (uint64_t)std::max<int64_t>(build_rows_bound, 1);
+      r.pay.clear();
+      for (int j = 0; j < d.npay; ++j) {
+        r.pay.emplace_back(new DevBuf());
+        r.pay.back()->alloc(r.pay_rows * ctype_width(d.pay_ctype[j]));
+        R.pay[j] = r.pay.back()->as<uint8_t>();
+      }
+      break;
+    }
+    case DQ_RES_OUTPUT: {
+      R.cap = cap;
+      r.cursor.alloc(8);
+      R.cursor = r.cursor.as<uint64_t>();
+      r.pay.clear();
+      for (int j = 0; j < d.npay; ++j) {
+        if (d.pay_ctype[j] == DQ_STR) throw DqError(DQ_ERR_UNSUPPORTED, "string output columns");
+        r.pay.emplace_back(new DevBuf());
+        r.pay.back()->alloc(cap * ctype_width(d.pay_ctype[j]));
+        R.pay[j] = r.pay.back()->as<uint8_t>();
+      }
+      break;
+    }
+    default:
+      throw DqError(DQ_ERR_BAD_IR, "unknown resource kind");
+  }
+}
+
+// ------------------------------------------------------------- pipelines --
+
+void slot_reads(const dq_pipeline& d, const dq_op& op, std::vector<int>& out) {
+  auto add = [&](int s) {
+    if (s >= 0) out.push_back(s);
+  };
+  auto add_list = [&](int list, int n) {
+    for (int i = 0; i < n; ++i) add(d.lists[list + i]);
+  };
+  switch (op.kind) {
+    case DQ_OP_ARITH:
+    case DQ_OP_CMP:
+    case DQ_OP_CAST:
+      if (!(op.flags & DQ_OPF_A_IMM)) add(op.a);
+      if (op.kind != DQ_OP_CAST && !(op.flags & DQ_OPF_B_IMM)) add(op.b);
+      break;
+    case DQ_OP_LOGIC:
+      add(op.a);
+      if (op.sub != DQ_NOT) add(op.b);
+      break;
+    case DQ_OP_SELECT:
+      add(op.a);
+      if (!(op.flags & DQ_OPF_B_IMM)) add(op.b);
+      add(op.c >= 0 ? op.c : op.dst);
+      break;
+    case DQ_OP_LIKE:
+    case DQ_OP_STREQ:
+    case DQ_OP_FILTER:
+      add(op.a);
+      break;
+    case DQ_OP_PROBE:
+    case DQ_OP_EXPAND:
+    case DQ_OP_MM_COUNT:
+      add_list(op.list, op.nlist);
+      if (op.kind == DQ_OP_EXPAND) add_list(op.list2, op.nlist2);
+      break;
+    case DQ_OP_AGG:
+    case DQ_OP_BUILD:
+    case DQ_OP_MM_SCATTER:
+      add_list(op.list, op.nlist);
+      add_list(op.list2, op.nlist2);
+      break;
+    case DQ_OP_EMIT:
+      add_list(op.list, op.nlist);
+      break;
+  }
+}
+
+void validate_pipeline(const dq_pipeline& d, int nres) {
+  if (d.nslots < 0 || d.nslots > DQ_MAX_SLOTS || d.nops <= 0 || d.nops > DQ_MAX_OPS || d.nlist < 0 ||
+      d.nlist > DQ_MAX_LIST || d.ncols < 0 || d.ncols > DQ_MAX_COLS || d.npatterns < 0 ||
+      d.npatterns > DQ_MAX_PATTERNS)
+    throw DqError(DQ_ERR_BAD_IR, "pipeline sizes out of range");
+  auto slot_ok = [&](int s) { return s >= -1 && s < d.nslots; };
+  for (int i = 0; i < d.nops; ++i) {
+    const dq_op& op = d.ops[i];
+    if (!slot_ok(op.dst) || !slot_ok(op.a) || !slot_ok(op.b) || !slot_ok(op.c))
+      throw DqError(DQ_ERR_BAD_IR, "op slot out of range");
+    if (op.nlist < 0 || op.nlist2 < 0 || op.list < 0 || op.list2 < 0 || op.list + op.nlist > d.nlist ||
+        op.list2 + op.nlist2 > d.nlist)
+      throw DqError(DQ_ERR_BAD_IR, "op list out of range");
+    bool sink = op.kind >= DQ_OP_AGG;
+    if (sink != (i == d.nops - 1)) throw DqError(DQ_ERR_BAD_IR, "the sink must be the last op");
+    if ((op.kind == DQ_OP_PROBE || op.kind == DQ_OP_EXPAND || sink) && (op.res < 0 || op.res >= nres))
+      throw DqError(DQ_ERR_BAD_IR, "op resource out of range");
+    if ((op.kind == DQ_OP_LIKE || op.kind == DQ_OP_STREQ) && (op.res < 0 || op.res >= d.npatterns))
+      throw DqError(DQ_ERR_BAD_IR, "pattern index out of range");
+    if (op.nlist > DQ_MAX_KEYS && (op.kind == DQ_OP_PROBE || op.kind == DQ_OP_EXPAND || op.kind == DQ_OP_BUILD ||
+                                    op.kind == DQ_OP_AGG || op.kind == DQ_OP_MM_COUNT || op.kind == DQ_OP_MM_SCATTER))
+      throw DqError(DQ_ERR_BAD_IR, "too many keys");
+  }
+  for (int i = 0; i < d.nlist; ++i)
+    if (!slot_ok(d.lists[i])) throw DqError(DQ_ERR_BAD_IR, "list entry out of range");
+  for (int s = 0; s < d.nslots; ++s) {
+    const dq_slot& sl = d.slots[s];
+    if (sl.level < 0 || sl.level >= DQ_MAX_LEVELS) throw DqError(DQ_ERR_BAD_IR, "slot level out of range");
+    if (sl.ctype < DQ_I8 || sl.ctype > DQ_STR) throw DqError(DQ_ERR_BAD_IR, "slot type out of range");
+    if ((sl.kind == DQ_SLOT_COL || sl.kind == DQ_SLOT_STR) && (sl.src < 0 || sl.src >= d.ncols))
+      throw DqError(DQ_ERR_BAD_IR, "slot column out of range");
+    if ((sl.kind == DQ_SLOT_GATHER || sl.kind == DQ_SLOT_AGGKEY || sl.kind == DQ_SLOT_AGGVAL) &&
+        (sl.res < 0 || sl.res >= nres))
+      throw DqError(DQ_ERR_BAD_IR, "slot resource out of range");
+  }
+}
+
+void setup_pipeline(dq_plan* plan, PipeRec& p) {
+  dq_ctx* ctx = plan->ctx;
+  const dq_pipeline& d = p.desc;
+  DevPipe& P = p.dev;
+  memset(&P, 0, sizeof(P));
+  validate_pipeline(d, (int)plan->res.size());
+
+  const int tile = ctx->cfg.tile_rows > 0 ? ctx->cfg.tile_rows : 1024;
+  if (tile % 16 || tile > kThreads * 8 || tile < 32) throw DqError(DQ_ERR_INVALID, "tile_rows must be a multiple of 16 in [32, 2048]");
+  P.tile = tile;
+  P.exp_cap = tile;
+  P.use_tma = !(ctx->cfg.flags & DQ_CFG_NO_TMA);
+  P.source_kind = d.source_kind;
+  P.source_res = d.source_res;
+  P.status = plan->status.as<int32_t>();
+
+  // resources: the pipeline sees the plan's resources under the same indices
+  if (plan->res.size() > (size_t)kMaxRes) throw DqError(DQ_ERR_UNSUPPORTED, "more than 8 resources in a plan");
+  P.nres = (int)plan->res.size();
+  for (size_t i = 0; i < plan->res.size(); ++i) P.res[i] = plan->res[i]->dev;
+
+  // source columns
+  std::vector<int> col_map(d.ncols, -1);  // pipeline column -> staged / string index
+  const TableRec* table = nullptr;
+  if (d.source_kind == DQ_SRC_TABLE) {
+    auto it = ctx->tables.find(d.table ? d.table : "");
+    if (it == ctx->tables.end()) throw DqError(DQ_ERR_NOT_FOUND, std::string("unknown table ") + (d.table ? d.table : "(null)"));
+    table = &it->second;
+    P.nrows = table->nrows;
+  } else if (d.source_kind == DQ_SRC_OUTPUT) {
+    if (d.source_res < 0 || d.source_res >= (int)plan->res.size() || plan->res[d.source_res]->desc.kind != DQ_RES_OUTPUT)
+      throw DqError(DQ_ERR_BAD_IR, "bad temp-table source");
+    P.nrows_dev = plan->res[d.source_res]->dev.cursor;
+  } else if (d.source_kind == DQ_SRC_AGG) {
+    if (d.source_res < 0 || d.source_res >= (int)plan->res.size() || plan->res[d.source_res]->desc.kind != DQ_RES_AGG)
+      throw DqError(DQ_ERR_BAD_IR, "bad aggregation source");
+    const DevRes& ar = plan->res[d.source_res]->dev;
+    P.nrows = ar.nkeys == 0 ? 1 : (int64_t)ar.cap + 1;  // no grouping: exactly one row
+  } else {
+    throw DqError(DQ_ERR_BAD_IR, "bad source kind");
+  }
+  int off = 0;
+  for (int i = 0; i < d.ncols; ++i) {
+    const char* cname = d.cols[i];
+    if (d.source_kind == DQ_SRC_TABLE) {
+      const ColRec* c = table->find(cname ? cname : "");
+      if (!c) throw DqError(DQ_ERR_NOT_FOUND, std::string("unknown column ") + (cname ? cname : "(null)"));
+      if (c->ctype == DQ_STR) {
+        if (P.nstr >= kMaxStr) throw DqError(DQ_ERR_UNSUPPORTED, "too many string columns");
+        DevStr& s = P.strs[P.nstr];
+        s.chars = c->data->as<uint8_t>();
+        s.offsets = c->offsets ? c->offsets->as<uint64_t>() : nullptr;
+        s.width = c->width;
+        col_map[i] = P.nstr++;
+      } else {
+        DevCol& dc = P.cols[P.ncols];
+        dc.ptr = c->data->as<uint8_t>();
+        dc.width = ctype_width(c->ctype);
+        dc.smem_off = off;
+        off += (int)align_up((uint64_t)tile * dc.width, 16);
+        col_map[i] = P.ncols++;
+      }
+    } else if (d.source_kind == DQ_SRC_OUTPUT) {
+      int j = atoi(cname ? cname : "-1");
+      const ResRec& o = *plan->res[d.source_res];
+      if (j < 0 || j >= o.desc.npay) throw DqError(DQ_ERR_BAD_IR, "bad temp-table column");
+      DevCol& dc = P.cols[P.ncols];
+      dc.ptr = o.dev.pay[j];
+      dc.width = ctype_width(o.desc.pay_ctype[j]);
+      dc.smem_off = off;
+      off += (int)align_up((uint64_t)tile * dc.width, 16);
+      col_map[i] = P.ncols++;
+    }
+  }
+  P.stage_bytes = off;
+  p.staged_cols = P.ncols;
+
+  // slots and register areas
+  int reg_bytes[DQ_MAX_LEVELS] = {0, 0, 0};
+  int nlevels = 1;
+  P.nslots = d.nslots;
+  for (int s = 0; s < d.nslots; ++s) {
+    const dq_slot& sl = d.slots[s];
+    DevSlot& ds = P.slots[s];
+    ds.kind = sl.kind;
+    ds.level = sl.level;
+    ds.ctype = sl.ctype;
+    ds.src = sl.src;
+    ds.res = sl.res;
+    ds.stash = -1;
+    nlevels = std::max(nlevels, (int)sl.level + 1);
+    switch (sl.kind) {
+      case DQ_SLOT_COL:
+        if (col_map[sl.src] < 0 || d.source_kind == DQ_SRC_AGG) throw DqError(DQ_ERR_BAD_IR, "COL slot on a non-staged column");
+        ds.src = (int16_t)col_map[sl.src];
+        ds.width = (int8_t)P.cols[ds.src].width;
+        break;
+      case DQ_SLOT_STR:
+        if (col_map[sl.src] < 0) throw DqError(DQ_ERR_BAD_IR, "STR slot on a bad column");
+        ds.src = (int16_t)col_map[sl.src];
+        ds.width = 0;
+        break;
+      case DQ_SLOT_REG:
+        ds.width = (int8_t)ctype_width(sl.ctype);
+        if (!ds.width) throw DqError(DQ_ERR_UNSUPPORTED, "string registers");
+        ds.smem_off = reg_bytes[sl.level];
+        reg_bytes[sl.level] += (int)align_up((uint64_t)tile * ds.width, 16);
+        break;
+      case DQ_SLOT_GATHER: {
+        const ResRec& r = *plan->res[sl.res];
+        if (r.desc.kind != DQ_RES_MULTI || sl.src < 0 || sl.src >= r.desc.npay) throw DqError(DQ_ERR_BAD_IR, "bad GATHER slot");
+        if (sl.level < 1) throw DqError(DQ_ERR_BAD_IR, "GATHER slot on level 0");
+        ds.width = (int8_t)ctype_width(r.desc.pay_ctype[sl.src]);
+        break;
+      }
+      case DQ_SLOT_AGGKEY:
+      case DQ_SLOT_AGGVAL:
+        if (d.source_kind != DQ_SRC_AGG || sl.res != d.source_res) throw DqError(DQ_ERR_BAD_IR, "aggregation slot outside its scan");
+        ds.width = 8;
+        break;
+      default:
+        throw DqError(DQ_ERR_BAD_IR, "bad slot kind");
+    }
+  }
+  // ops, lists, patterns
+  P.nops = d.nops;
+  for (int i = 0; i < d.nops; ++i) P.ops[i] = d.ops[i];
+  for (int i = 0; i < d.nlist; ++i) P.lists[i] = d.lists[i];
+  p.patterns.clear();
+  std::string cat;
+  for (int i = 0; i < d.npatterns; ++i) {
+    P.pat_off[i] = (int32_t)cat.size();
+    cat += d.patterns[i] ? d.patterns[i] : "";
+  }
+  P.pat_off[d.npatterns] = (int32_t)cat.size();
+  if (!cat.empty()) {
+    p.pattern_buf.alloc(cat.size());
+    DQ_CUDA(cudaMemcpy(p.pattern_buf.ptr, cat.data(), cat.size(), cudaMemcpyHostToDevice));
+    P.patterns = p.pattern_buf.as<uint8_t>();
+  }
+  const dq_op& sink = d.ops[d.nops - 1];
+  p.mm_count = sink.kind == DQ_OP_MM_COUNT;
+  p.mm_res = p.mm_count ? sink.res : -1;
+  for (int i = 0; i < d.nops; ++i)
+    if (d.ops[i].kind == DQ_OP_EXPAND) nlevels = std::max(nlevels, 2);
+
+  // deferred wide expansion ranges for the first level-0 expansion
+  p.expand_op = -1;
+  for (int i = 0; i < d.nops; ++i) {
+    const dq_op& op = d.ops[i];
+    if (op.kind != DQ_OP_EXPAND) continue;
+    bool level0 = true;
+    for (int q = 0; q < op.nlist; ++q) level0 &= d.slots[d.lists[op.list + q]].level == 0;
+    if (!level0) break;
+    std::vector<int> reads;
+    for (int j = i; j < d.nops; ++j) slot_reads(d, d.ops[j], reads);
+    std::vector<int> stash;
+    bool ok = true;
+    for (int s : reads) {
+      if (d.slots[s].level != 0) continue;
+      if (d.slots[s].kind == DQ_SLOT_STR) ok = false;
+      if (std::find(stash.begin(), stash.end(), s) == stash.end()) stash.push_back(s);
+    }
+    if (!ok || (int)stash.size() > kMaxStash) break;
+    for (size_t q = 0; q < stash.size(); ++q) P.slots[stash[q]].stash = (int)q;
+    p.expand_op = i;
+    DevHeavy& H = P.heavy;
+    H.nstash = (int)stash.size();
+    H.words = 2 + H.nstash;
+    int64_t rows = P.nrows_dev ? 1 << 20 : P.nrows;
+    H.cap = (uint32_t)std::min<int64_t>(std::max<int64_t>(rows, 1), 1 << 20);
+    H.op = i;
+    H.threshold = ctx->cfg.defer_threshold > 0 ? (uint64_t)ctx->cfg.defer_threshold : (uint64_t)tile * 8;
+    p.heavy_items.alloc((size_t)H.cap * H.words * 8);
+    p.heavy_count.alloc(8);
+    p.heavy_prefix.alloc(((size_t)H.cap + 1) * 8);
+    H.items = p.heavy_items.as<uint64_t>();
+    H.count = p.heavy_count.as<uint32_t>();
+    H.unit_prefix = p.heavy_prefix.as<uint64_t>();
+    break;
+  }
+
+  // shared-memory layout
+  int base = 0;
+  auto take = [&](int bytes) {
+    int o = base;
+    base += (int)align_up(bytes, 16);
+    return o;
+  };
+  P.nstage = p.staged_cols ? 3 : 1;
+  for (int l = 0; l < DQ_MAX_LEVELS; ++l) P.off_reg[l] = P.off_sel[l] = P.off_par[l] = P.off_match[l] = 0;
+  for (int l = 0; l < nlevels; ++l) {
+    P.off_reg[l] = take(reg_bytes[l]);
+    P.off_sel[l] = take(tile * 2);
+    if (l > 0) {
+      P.off_par[l] = take(tile * 2);
+      P.off_match[l] = take(tile * 4);
+    }
+  }
+  P.off_exp = take(std::max(1, nlevels - 1) * 3 * tile * 4);
+  P.off_flags = take(tile);
+  P.off_stash = take(kMaxStash * 8);
+  for (int r = 0; r < P.nres; ++r) {
+    DevRes& R = P.res[r];
+    if (R.kind == DQ_RES_AGG && R.smem_slots > 0) {
+      bool used = sink.kind == DQ_OP_AGG && sink.res == r;
+      if (used) R.smem_off = take((R.smem_slots + 1) * (1 + R.naggs) * 8);
+      else R.smem_slots = 0;
+    } else if (R.kind == DQ_RES_AGG) {
+      R.smem_slots = 0;
+    }
+  }
+  const int fixed = base;
+  const int max_smem = 227 * 1024 - 2048;
+  while (P.nstage > 1 && fixed + P.nstage * P.stage_bytes > max_smem) --P.nstage;
+  if (fixed + P.nstage * P.stage_bytes > max_smem)
+    throw DqError(DQ_ERR_UNSUPPORTED, "pipeline needs more shared memory than a CTA has; lower tile_rows");
+  P.off_stage = fixed;
+  P.smem_bytes = fixed + P.nstage * P.stage_bytes;
+  int occ = pipeline_occupancy(P.smem_bytes);
+  if (occ < 1) throw DqError(DQ_ERR_UNSUPPORTED, "pipeline kernel cannot be resident with this shared memory");
+  int want = ctx->cfg.ctas_per_sm > 0 ? std::min(ctx->cfg.ctas_per_sm, occ) : occ;
+  p.grid = ctx->sms * want;
+}
+
+void free_events(dq_plan* plan) {
+  for (auto e : plan->events) cudaEventDestroy(e);
+  plan->events.clear();
+}
+
+// One execution of all pipelines; returns the device status word.
+int run_once(dq_plan* plan, cudaStream_t st) {
+  dq_ctx* ctx = plan->ctx;
+  int launches = 0;
+  const size_t np = plan->pipes.size();
+  if (plan->events.size() != 2 * np + 2) {
+    free_events(plan);
+    for (size_t i = 0; i < 2 * np + 2; ++i) {
+      cudaEvent_t e;
+      DQ_CUDA(cudaEventCreate(&e));
+      plan->events.push_back(e);
+    }
+  }
+  DQ_CUDA(cudaEventRecord(plan->events[0], st));
+  DQ_CUDA(cudaMemsetAsync(plan->status.ptr, 0, 4, st));
+  DQ_CUDA(cudaMemsetAsync(plan->counters.ptr, 0, plan->counters.bytes, st));
+  for (auto& rp : plan->res) {
+    ResRec& r = *rp;
+    switch (r.desc.kind) {
+      case DQ_RES_UNIQUE:
+        DQ_CUDA(cudaMemsetAsync(r.slots.ptr, 0xff, r.slots.bytes, st));
+        break;
+      case DQ_RES_AGG:
+        DQ_CUDA(launch_agg_init(r.dev.slots, r.dev.cap + 1, r.dev.words, r.dev.val_word, r.dev.naggs, r.dev.agg_red, st));
+        ++launches;
+        break;
+      case DQ_RES_MULTI:
+        DQ_CUDA(cudaMemsetAsync(r.counts.ptr, 0, r.counts.bytes, st));
+        break;
+      case DQ_RES_OUTPUT:
+        DQ_CUDA(cudaMemsetAsync(r.cursor.ptr, 0, 8, st));
+        break;
+    }
+  }
+  uint32_t* counters = plan->counters.as<uint32_t>();
+  for (size_t i = 0; i < np; ++i) {
+    PipeRec& p = *plan->pipes[i];
+    p.dev.tile_counter = counters + 2 * i;
+    DQ_CUDA(cudaEventRecord(plan->events[1 + 2 * i], st));
+    if (p.expand_op >= 0) DQ_CUDA(cudaMemsetAsync(p.heavy_count.ptr, 0, 8, st));
+    DQ_CUDA(launch_pipeline(p.dev, p.grid, st));
+    ++launches;
+    if (p.expand_op >= 0) {
+      DQ_CUDA(launch_heavy_prefix(p.dev.heavy, (uint64_t)p.dev.exp_cap, st));
+      DevPipe H = p.dev;
+      H.mode = 1;
+      H.tile_counter = counters + 2 * i + 1;
+      DQ_CUDA(launch_pipeline(H, p.grid, st));
+      launches += 2;
+    }
+    if (p.mm_count) {
+      ResRec& r = *plan->res[p.mm_res];
+      DQ_CUDA(launch_mm_scan(r.dev.counts, r.dev.offsets, r.dev.cap, r.scan_scratch.as<uint32_t>(), st, &launches));
+    }
+    DQ_CUDA(cudaEventRecord(plan->events[2 + 2 * i], st));
+  }
+  DQ_CUDA(cudaEventRecord(plan->events[2 * np + 1], st));
+  int32_t status = 0;
+  DQ_CUDA(cudaMemcpyAsync(&status, plan->status.ptr, 4, cudaMemcpyDeviceToHost, st));
+  DQ_CUDA(cudaStreamSynchronize(st));
+  float ms = 0;
+  dq_plan_timing& T = plan->timing;
+  memset(&T, 0, sizeof(T));
+  cudaEventElapsedTime(&ms, plan->events[0], plan->events[2 * np + 1]);
+  T.total_ms = ms;
+  T.max_pipeline = -1;
+  for (size_t i = 0; i < np && i < (size_t)DQ_MAX_OPS; ++i) {
+    cudaEventElapsedTime(&ms, plan->events[1 + 2 * i], plan->events[2 + 2 * i]);
+    T.pipeline_ms[i] = ms;
+    if (ms > T.max_pipeline_ms) {
+      T.max_pipeline_ms = ms;
+      T.max_pipeline = (int)i;
+    }
+  }
+  T.kernel_launches = launches;
+  (void)ctx;
+  return status;
+}
+
+// Re-derives every pipeline's copy of the resource descriptors.
+void refresh_pipelines(dq_plan* plan) {
+  for (auto& pp : plan->pipes) setup_pipeline(plan, *pp);
+}
+
+}  // namespace
+
+// ====================================================================== ABI ==
+
+extern "C" {
+
+int dq_version(void) { return DQ_ABI_VERSION; }
+
+const char* dq_last_error(dq_ctx* ctx) { return ctx ? ctx->error.c_str() : g_init_error.c_str(); }
+
+int dq_init(const dq_config* cfg, dq_ctx** out) {
+  if (!out) return fail(nullptr, DQ_ERR_INVALID, "null output");
+  *out = nullptr;
+  return guarded(nullptr, [&]() {
+    std::unique_ptr<dq_ctx> ctx(new dq_ctx());
+    if (cfg) {
+      if (cfg->abi_version != DQ_ABI_VERSION) throw DqError(DQ_ERR_INVALID, "ABI version mismatch");
+      ctx->cfg = *cfg;
+    }
+    ctx->device = ctx->cfg.device;
+    int n = 0;
+    DQ_CUDA(cudaGetDeviceCount(&n));
+    if (ctx->device < 0 || ctx->device >= n) throw DqError(DQ_ERR_INVALID, "no such CUDA device");
+    DQ_CUDA(cudaSetDevice(ctx->device));
+    DQ_CUDA(cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    DQ_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    *out = ctx.release();
+    return (int)DQ_OK;
+  });
+}
+
+void dq_shutdown(dq_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  ctx->tables.clear();
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+int dq_table_register(dq_ctx* ctx, const char* name, int32_t ncols, const dq_column* cols, int64_t nrows,
+                      int32_t flags) {
+  if (!ctx || !name || (ncols > 0 && !cols) || nrows < 0 || ncols < 0) return fail(ctx, DQ_ERR_INVALID, "bad table arguments");
+  return guarded(ctx, [&]() {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DQ_CUDA(cudaSetDevice(ctx->device));
+    TableRec t;
+    t.nrows = nrows;
+    for (int i = 0; i < ncols; ++i) {
+      const dq_column& c = cols[i];
+      if (!c.name || c.ctype < DQ_I8 || c.ctype > DQ_STR) throw DqError(DQ_ERR_INVALID, "bad column descriptor");
+      if (nrows > 0 && !c.data) throw DqError(DQ_ERR_INVALID, std::string("column ") + c.name + " has no data");
+      ColRec rec;
+      rec.name = c.name;
+      rec.ctype = c.ctype;
+      rec.width = c.ctype == DQ_STR ? c.width : ctype_width(c.ctype);
+      upload_column(ctx, rec, c, nrows, flags & DQ_TABLE_DEVICE_DATA, ctx->stream);
+      t.cols.push_back(std::move(rec));
+    }
+    DQ_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->tables[name] = std::move(t);
+    return (int)DQ_OK;
+  });
+}
+
+int dq_table_update(dq_ctx* ctx, const char* name, int32_t ncols, const dq_column* cols, int64_t nrows,
+                    void* stream) {
+  if (!ctx || !name || !cols) return fail(ctx, DQ_ERR_INVALID, "bad table arguments");
+  return guarded(ctx, [&]() {
+    auto it = ctx->tables.find(name);
+    if (it == ctx->tables.end()) throw DqError(DQ_ERR_NOT_FOUND, std::string("unknown table ") + name);
+    TableRec& t = it->second;
+    if (t.nrows != nrows) throw DqError(DQ_ERR_INVALID, "row count differs from the registered table");
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    for (int i = 0; i < ncols; ++i) {
+      ColRec* rec = nullptr;
+      for (auto& c : t.cols)
+        if (c.name == cols[i].name) rec = &c;
+      if (!rec || rec->ctype != cols[i].ctype) throw DqError(DQ_ERR_INVALID, std::string("column mismatch ") + cols[i].name);
+      if (rec->ctype == DQ_STR) throw DqError(DQ_ERR_UNSUPPORTED, "updating string columns");
+      DQ_CUDA(cudaMemcpyAsync(rec->data->ptr, cols[i].data, (size_t)nrows * ctype_width(rec->ctype),
+                              cudaMemcpyHostToDevice, st));
+    }
+    return (int)DQ_OK;
+  });
+}
+
+int dq_table_drop(dq_ctx* ctx, const char* name) {
+  if (!ctx || !name) return fail(ctx, DQ_ERR_INVALID, "bad arguments");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->tables.erase(name)) return fail(ctx, DQ_ERR_NOT_FOUND, std::string("unknown table ") + name);
+  return DQ_OK;
+}
+
+int dq_table_rows(dq_ctx* ctx, const char* name, int64_t* nrows) {
+  if (!ctx || !name || !nrows) return fail(ctx, DQ_ERR_INVALID, "bad arguments");
+  auto it = ctx->tables.find(name);
+  if (it == ctx->tables.end()) return fail(ctx, DQ_ERR_NOT_FOUND, std::string("unknown table ") + name);
+  *nrows = it->second.nrows;
+  return DQ_OK;
+}
+
+int dq_plan_prepare(dq_ctx* ctx, const dq_plan_desc* desc, dq_plan** out) {
+  if (!ctx || !desc || !out) return fail(ctx, DQ_ERR_INVALID, "bad arguments");
+  *out = nullptr;
+  return guarded(ctx, [&]() {
+    if (desc->abi_version != DQ_ABI_VERSION) throw DqError(DQ_ERR_BAD_IR, "IR version mismatch");
+    if (desc->nres < 0 || desc->npipes <= 0 || (desc->nres && !desc->res) || !desc->pipes)
+      throw DqError(DQ_ERR_BAD_IR, "empty plan");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DQ_CUDA(cudaSetDevice(ctx->device));
+    std::unique_ptr<dq_plan> plan(new dq_plan());
+    plan->ctx = ctx;
+    plan->status.alloc(4);
+    plan->counters.alloc(8 * (size_t)desc->npipes);
+    // row bound for multimap payloads: rows of the source of the pipeline that scatters into it
+    std::vector<int64_t> bound(desc->nres, 1);
+    for (int i = 0; i < desc->npipes; ++i) {
+      const dq_pipeline& d = desc->pipes[i];
+      if (d.nops <= 0 || d.nops > DQ_MAX_OPS) throw DqError(DQ_ERR_BAD_IR, "bad op count");
+      const dq_op& sink = d.ops[d.nops - 1];
+      if ((sink.kind == DQ_OP_MM_SCATTER || sink.kind == DQ_OP_MM_COUNT) && sink.res >= 0 && sink.res < desc->nres) {
+        int64_t rows = 1 << 20;
+        if (d.source_kind == DQ_SRC_TABLE && d.table) {
+          auto it = ctx->tables.find(d.table);
+          if (it != ctx->tables.end()) rows = it->second.nrows;
+        } else if (d.source_kind == DQ_SRC_OUTPUT && d.source_res >= 0 && d.source_res < desc->nres) {
+          rows = desc->res[d.source_res].capacity;
+        }
+        bound[sink.res] = std::max(bound[sink.res], rows);
+      }
+    }
+    for (int i = 0; i < desc->nres; ++i) {
+      std::unique_ptr<ResRec> r(new ResRec());
+      r->desc = desc->res[i];
+      r->name = desc->res[i].name ? desc->res[i].name : "";
+      r->desc.name = nullptr;
+      setup_resource(plan.get(), *r, bound[i]);
+      plan->res.push_back(std::move(r));
+    }
+    for (int i = 0; i < desc->npipes; ++i) {
+      std::unique_ptr<PipeRec> p(new PipeRec());
+      p->desc = desc->pipes[i];
+      // keep string arguments alive
+      for (int c = 0; c < p->desc.ncols; ++c) p->col_names.push_back(p->desc.cols[c] ? p->desc.cols[c] : "");
+      for (int c = 0; c < p->desc.ncols; ++c) p->desc.cols[c] = p->col_names[c].c_str();
+      p->desc.table = nullptr;
+      std::string tname = desc->pipes[i].table ? desc->pipes[i].table : "";
+      p->col_names.push_back(tname);
+      p->desc.table = p->col_names.back().c_str();
+      for (int c = 0; c < p->desc.npatterns; ++c) p->patterns.push_back(p->desc.patterns[c] ? p->desc.patterns[c] : "");
+      for (int c = 0; c < p->desc.npatterns; ++c) p->desc.patterns[c] = p->patterns[c].c_str();
+      plan->pipes.push_back(std::move(p));
+    }
+    // the col_names vector may have reallocated: re-point
+    for (auto& p : plan->pipes) {
+      for (int c = 0; c < p->desc.ncols; ++c) p->desc.cols[c] = p->col_names[c].c_str();
+      p->desc.table = p->col_names.back().c_str();
+      for (int c = 0; c < p->desc.npatterns; ++c) p->desc.patterns[c] = p->patterns[c].c_str();
+    }
+    refresh_pipelines(plan.get());
+    plan->result_res = desc->result_res;
+    if (plan->result_res < 0 || plan->result_res >= desc->nres || plan->res[plan->result_res]->desc.kind != DQ_RES_OUTPUT)
+      throw DqError(DQ_ERR_BAD_IR, "result must be an OUTPUT resource");
+    *out = plan.release();
+    return (int)DQ_OK;
+  });
+}
+
+int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out) {
+  if (!plan || !out) return DQ_ERR_INVALID;
+  dq_ctx* ctx = plan->ctx;
+  *out = nullptr;
+  return guarded(ctx, [&]() {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DQ_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    int status = 0;
+    for (int attempt = 0;; ++attempt) {
+      status = run_once(plan, st);
+      if (status == 0) break;
+      if (attempt >= 8 || (status & (kErrTimeout | kErrBadOp)))
+        throw DqError(status & kErrTimeout ? DQ_ERR_TIMEOUT
+                      : status & kErrHtFull ? DQ_ERR_HT_FULL
+                      : status & kErrOverflow ? DQ_ERR_OVERFLOW : DQ_ERR_BAD_IR,
+                      "device status " + std::to_string(status));
+      // grow what overflowed and run again (the results of a failed run are discarded)
+      for (auto& rp : plan->res) {
+        ResRec& r = *rp;
+        if ((status & kErrHtFull) && (r.desc.kind == DQ_RES_UNIQUE || r.desc.kind == DQ_RES_AGG)) {
+          r.desc.capacity = (int64_t)r.dev.cap * 4;
+          setup_resource(plan, r, 1);
+        }
+        if ((status & kErrOverflow) && r.desc.kind == DQ_RES_OUTPUT) {
+          uint64_t need = 0;
+          DQ_CUDA(cudaMemcpy(&need, r.cursor.ptr, 8, cudaMemcpyDeviceToHost));
+          if (need > r.dev.cap) {
+            r.desc.capacity = (int64_t)need;
+            setup_resource(plan, r, 1);
+          }
+        }
+      }
+      refresh_pipelines(plan);
+    }
+    ResRec& o = *plan->res[plan->result_res];
+    uint64_t n = 0;
+    DQ_CUDA(cudaMemcpy(&n, o.cursor.ptr, 8, cudaMemcpyDeviceToHost));
+    std::unique_ptr<dq_result> res(new dq_result());
+    res->nrows = (int64_t)n;
+    for (int j = 0; j < o.desc.npay; ++j) {
+      int w = ctype_width(o.desc.pay_ctype[j]);
+      res->ctypes.push_back(o.desc.pay_ctype[j]);
+      res->cols.emplace_back((size_t)n * w);
+      if (n) DQ_CUDA(cudaMemcpyAsync(res->cols.back().data(), o.dev.pay[j], (size_t)n * w, cudaMemcpyDeviceToHost, st));
+    }
+    DQ_CUDA(cudaStreamSynchronize(st));
+    *out = res.release();
+    return (int)DQ_OK;
+  });
+}
+
+void dq_plan_free(dq_plan* plan) {
+  if (!plan) return;
+  cudaSetDevice(plan->ctx->device);
+  free_events(plan);
+  delete plan;
+}
+
+int dq_plan_timing_get(dq_plan* plan, dq_plan_timing* out) {
+  if (!plan || !out) return DQ_ERR_INVALID;
+  *out = plan->timing;
+  return DQ_OK;
+}
+
+int dq_result_rows(dq_result* r, int64_t* nrows) {
+  if (!r || !nrows) return DQ_ERR_INVALID;
+  *nrows = r->nrows;
+  return DQ_OK;
+}
+
+int dq_result_ncols(dq_result* r, int32_t* ncols) {
+  if (!r || !ncols) return DQ_ERR_INVALID;
+  *ncols = (int32_t)r->cols.size();
+  return DQ_OK;
+}
+
+int dq_result_column(dq_result* r, int32_t col, int32_t* ctype, const void** data) {
+  if (!r || col < 0 || col >= (int32_t)r->cols.size() || !ctype || !data) return DQ_ERR_INVALID;
+  *ctype = r->ctypes[col];
+  *data = r->cols[col].data();
+  return DQ_OK;
+}
+
+void dq_result_free(dq_result* r) { delete r; }
+
+}  // extern "C"

@@ -1,0 +1,179 @@
+"""Python handle on the CUDA engine (``libdogqc_b200.so``).
+
+``Engine`` owns one ``dq_ctx`` (one device, one stream), registers tables and
+prepares plans; ``Plan.execute`` runs a plan and returns a ``Result`` of numpy
+columns.  Everything here goes through the C ABI; there is no CPU path.
+"""
+import ctypes as C
+
+import numpy as np
+
+from dogqc_b200 import _lib as L
+from dogqc_b200.database import StringColumn
+from dogqc_b200.lowering import NP_DTYPE, Lowering, lang_type
+
+
+class Result(object):
+    """A materialised result: column names, C types and numpy arrays."""
+
+    def __init__(self, names, ctypes_, columns, nrows):
+        self.names = list(names)
+        self.ctypes = list(ctypes_)
+        self.columns = columns
+        self.nrows = int(nrows)
+
+    def rows(self):
+        if self.nrows == 0:
+            return []
+        return list(zip(*[c.tolist() for c in self.columns]))
+
+    def column(self, name):
+        return self.columns[self.names.index(name)]
+
+    def format_sample(self, limit=10):
+        """The reference's console summary (cudaTranslator.py:607-643)."""
+        out = ["", "Result: %i tuples" % self.nrows]
+        for i in range(min(limit, self.nrows)):
+            parts = []
+            for n, t, c in zip(self.names, self.ctypes, self.columns):
+                v = c[i]
+                if t == L.I8:
+                    s = chr(int(v) & 0xFF)
+                elif t == L.U64:
+                    s = "%10d" % int(v)
+                elif t == L.U32:
+                    s = "%10d" % int(v)
+                else:
+                    s = "%8d" % int(v)
+                parts.append("%s: %s" % (n, s))
+            out.append("  ".join(parts) + "  ")
+        if self.nrows > limit:
+            out.append("[...]")
+        return "\n".join(out) + "\n"
+
+
+class Plan(object):
+    def __init__(self, engine, lowering):
+        self.engine = engine
+        self.lowering = lowering
+        desc, keep = lowering.ir()
+        handle = C.c_void_p()
+        L.check(L.lib().dq_plan_prepare(engine.ctx, C.byref(desc), C.byref(handle)), engine.ctx)
+        self.handle = handle
+
+    def execute(self, stream=None):
+        lib = L.lib()
+        res = C.c_void_p()
+        L.check(lib.dq_plan_execute(self.handle, stream, C.byref(res)), self.engine.ctx)
+        try:
+            n = C.c_int64()
+            nc = C.c_int32()
+            L.check(lib.dq_result_rows(res, C.byref(n)))
+            L.check(lib.dq_result_ncols(res, C.byref(nc)))
+            cols, types = [], []
+            for j in range(nc.value):
+                t = C.c_int32()
+                ptr = C.c_void_p()
+                L.check(lib.dq_result_column(res, j, C.byref(t), C.byref(ptr)))
+                dt = np.dtype(NP_DTYPE[t.value])
+                if n.value:
+                    buf = (C.c_uint8 * (n.value * dt.itemsize)).from_address(ptr.value)
+                    cols.append(np.frombuffer(buf, dtype=dt).copy())
+                else:
+                    cols.append(np.zeros(0, dtype=dt))
+                types.append(t.value)
+        finally:
+            lib.dq_result_free(res)
+        return Result(self.lowering.result_names, types, cols, n.value)
+
+    def timing(self):
+        t = L.dq_plan_timing()
+        L.check(L.lib().dq_plan_timing_get(self.handle, C.byref(t)))
+        return {"total_ms": t.total_ms, "max_pipeline_ms": t.max_pipeline_ms,
+                "max_pipeline": t.max_pipeline, "kernel_launches": t.kernel_launches,
+                "pipeline_ms": [t.pipeline_ms[i] for i in range(len(self.lowering.pipes))]}
+
+    def free(self):
+        if self.handle:
+            L.lib().dq_plan_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Engine(object):
+    """One device context.  ``register_database`` uploads host tables once."""
+
+    def __init__(self, device=0, tile_rows=0, ctas_per_sm=0, flags=0, defer_threshold=0):
+        cfg = L.dq_config()
+        cfg.abi_version = L.ABI_VERSION
+        cfg.device = device
+        cfg.tile_rows = tile_rows
+        cfg.ctas_per_sm = ctas_per_sm
+        cfg.flags = flags
+        cfg.defer_threshold = defer_threshold
+        handle = C.c_void_p()
+        L.check(L.lib().dq_init(C.byref(cfg), C.byref(handle)))
+        self.ctx = handle
+        self.registered = {}
+
+    @staticmethod
+    def _columns(table):
+        cols, keep = [], []
+        for name, col in table.columns.items():
+            c = L.dq_column()
+            nb = name.encode()
+            keep.append(nb)
+            c.name = nb
+            t = lang_type(table.types[name])
+            c.ctype = {"i8": L.I8, "i32": L.I32, "u32": L.U32, "u64": L.U64, "str": L.STR}[t]
+            if isinstance(col, StringColumn):
+                keep += [col.chars, col.offsets]
+                c.width = col.width
+                c.data = col.chars.ctypes.data if len(col.chars) else None
+                c.offsets = col.offsets.ctypes.data
+                c.nchars = len(col.chars)
+            else:
+                arr = np.ascontiguousarray(col)
+                keep.append(arr)
+                c.data = arr.ctypes.data if len(arr) else None
+            cols.append(c)
+        arr = (L.dq_column * max(len(cols), 1))(*cols)
+        return arr, len(cols), keep
+
+    def register_table(self, table):
+        arr, n, keep = self._columns(table)
+        L.check(L.lib().dq_table_register(self.ctx, table.name.encode(), n, arr, table.size, 0), self.ctx)
+        self.registered[table.name] = table
+
+    def register_database(self, db, force=False):
+        for name, table in db.tables.items():
+            if force or self.registered.get(name) is not table:
+                self.register_table(table)
+
+    def update_table(self, table, stream=None):
+        """Copy new host values of a registered table's columns to the device."""
+        arr, n, keep = self._columns(table)
+        L.check(L.lib().dq_table_update(self.ctx, table.name.encode(), n, arr, table.size, stream), self.ctx)
+
+    def prepare(self, plan, options=None):
+        lowering = plan if isinstance(plan, Lowering) else Lowering(plan, options)
+        return Plan(self, lowering)
+
+    def close(self):
+        if self.ctx:
+            L.lib().dq_shutdown(self.ctx)
+            self.ctx = None
+
+
+_default = {}
+
+
+def default_engine(device=0):
+    if device not in _default:
+        _default[device] = Engine(device)
+    return _default[device]

@@ -1,0 +1,699 @@
+"""Lowering of a resolved DogQC plan into the backend's pipeline IR.
+
+The reference turns the operator tree into CUDA source with a produce/consume
+walk (dogqc/cudaTranslator.py:31-89, translatorBase.py:6-63): a scan opens a
+kernel, each operator appends code, a hash-join build or an aggregation closes
+the kernel, and the parent continues in a new one.  This module does the same
+walk but emits the IR of include/dogqc_b200.h: for every pipeline a source, the
+slots (typed values per row), an operator list and one sink, plus the hash
+tables and outputs the pipelines share.  The kernels that execute the IR are
+hand-written (dogqc_b200/csrc/dq_kernels.cu); nothing here generates code.
+
+Pipeline breaking follows the reference:
+
+* Scan -> new pipeline over the table (only columns that are read are staged);
+* Selection -> FILTER on the lowered condition (translator :353-366);
+* Map -> expression ops whose result is converted to the attribute's C type
+  (:402-422);
+* EquiJoin -> the build child is produced first into a BUILD sink (unique hash
+  table, ``multimatch=False``, hashJoins.py:95-109) or into a multimap built by
+  a count pass, a bucket scan and a scatter pass over the same build pipeline
+  (hashJoins.py:214-240, codegen.py:60-66); the probe child then continues with
+  PROBE or EXPAND (hashJoins.py:113-153, 465-681);
+* Aggregation -> AGG sink, then a new pipeline scanning the aggregation table,
+  computing AVG = SUM / (ULL)COUNT (cudaTranslator.py:431-525);
+* Materialize -> EMIT sink into an output (result or temp table, :582-616).
+
+Expression typing follows C: char promotes to int, the usual arithmetic
+conversions pick int / unsigned / long / unsigned long long, comparisons yield
+int, and a map's value is converted to its attribute's C type
+(codegen.py:37-45: INT->int, DATE->unsigned, CHAR->char, FLOAT/DOUBLE->ULL).
+"""
+import ctypes as C
+
+from dogqc_b200 import _lib as L
+
+
+class Unsupported(NotImplementedError):
+    """The plan uses an operator or expression this backend does not execute."""
+
+
+LANG = {"INT": "i32", "DATE": "u32", "CHAR": "i8", "FLOAT": "u64", "DOUBLE": "u64", "STRING": "str"}
+CT = {"i8": L.I8, "i32": L.I32, "u32": L.U32, "i64": L.I64, "u64": L.U64, "str": L.STR}
+NP_DTYPE = {L.I8: "int8", L.I32: "int32", L.U32: "uint32", L.I64: "int64", L.U64: "uint64"}
+
+
+def _tname(t):
+    return t.name if hasattr(t, "name") else str(t)
+
+
+def lang_type(relational_type):
+    n = _tname(relational_type)
+    if n not in LANG:
+        raise Unsupported("no C type for attribute type %s" % n)
+    return LANG[n]
+
+
+def _promote(t):
+    return "i32" if t == "i8" else t
+
+
+def common_type(a, b):
+    a, b = _promote(a), _promote(b)
+    if "u64" in (a, b):
+        return "u64"
+    if "i64" in (a, b):
+        return "i64"
+    if "u32" in (a, b):
+        return "u32"
+    return "i32"
+
+
+def _wrap(v, t):
+    """Two's-complement value of v in C type t, as a Python int (signed for i*)."""
+    bits = {"i8": 8, "i32": 32, "u32": 32, "i64": 64, "u64": 64}[t]
+    v &= (1 << bits) - 1
+    if t.startswith("i") and v >= 1 << (bits - 1):
+        v -= 1 << bits
+    return v
+
+
+def _imm64(v):
+    """Immediate as the int64 bit pattern the device reads."""
+    v &= (1 << 64) - 1
+    return v - (1 << 64) if v >= 1 << 63 else v
+
+
+class Imm(object):
+    def __init__(self, value, ctype):
+        self.value = value
+        self.ctype = ctype
+
+
+class Pattern(object):
+    def __init__(self, data):
+        self.data = data
+
+
+class Res(object):
+    def __init__(self, kind, **kw):
+        self.kind = kind
+        self.nkeys = kw.get("nkeys", 0)
+        self.key_ctype = kw.get("key_ctype", [])
+        self.pay_ctype = kw.get("pay_ctype", [])
+        self.agg_red = kw.get("agg_red", [])
+        self.capacity = int(kw.get("capacity", 1024))
+        self.group_hint = int(kw.get("group_hint", 0))
+        self.name = kw.get("name")
+        self.columns = kw.get("columns", [])
+
+
+class Pipe(object):
+    """One pipeline under construction."""
+
+    def __init__(self, source_kind, table=None, source_res=-1):
+        self.source_kind = source_kind
+        self.table = table
+        self.source_res = source_res
+        self.cols = []          # source columns (names or output indices)
+        self.slots = []         # dicts: kind, level, ctype, src, res
+        self.ops = []           # dicts
+        self.lists = []
+        self.patterns = []
+        self.att = {}           # attribute id -> slot index
+        self.level = 0
+        self.lazy = {}          # attribute id -> callable creating its slot
+
+    def slot(self, kind, level, ctype, src=0, res=-1):
+        self.slots.append(dict(kind=kind, level=level, ctype=ctype, src=src, res=res))
+        if len(self.slots) > L.MAX_SLOTS:
+            raise Unsupported("pipeline needs more than %d slots" % L.MAX_SLOTS)
+        return len(self.slots) - 1
+
+    def reg(self, ctype):
+        return self.slot(L.SLOT_REG, self.level, ctype)
+
+    def col(self, name):
+        if name not in self.cols:
+            self.cols.append(name)
+        return self.cols.index(name)
+
+    def op(self, kind, **kw):
+        d = dict(kind=kind, sub=0, dst=-1, a=-1, b=-1, c=-1, ctype=0, flags=0, res=-1,
+                 list=0, nlist=0, list2=0, nlist2=0, imm=0)
+        d.update(kw)
+        self.ops.append(d)
+        if len(self.ops) > L.MAX_OPS:
+            raise Unsupported("pipeline needs more than %d ops" % L.MAX_OPS)
+        return d
+
+    def list_(self, items):
+        start = len(self.lists)
+        self.lists.extend(items)
+        if len(self.lists) > L.MAX_LIST:
+            raise Unsupported("pipeline lists exceed %d entries" % L.MAX_LIST)
+        return start, len(items)
+
+    def pattern(self, data):
+        if data in self.patterns:
+            return self.patterns.index(data)
+        self.patterns.append(data)
+        if len(self.patterns) > L.MAX_PATTERNS:
+            raise Unsupported("more than %d string constants in a pipeline" % L.MAX_PATTERNS)
+        return len(self.patterns) - 1
+
+    def attr_slot(self, attr):
+        if attr.id not in self.att:
+            if attr.id in self.lazy:
+                self.att[attr.id] = self.lazy.pop(attr.id)()
+            else:
+                raise Unsupported("attribute %s (%d) is not available in this pipeline" % (attr.name, attr.id))
+        return self.att[attr.id]
+
+    def clone_for_rebuild(self):
+        """Fresh copy of the source part (used to run a build pipeline twice)."""
+        return Pipe(self.source_kind, self.table, self.source_res)
+
+
+class Lowering(object):
+    """Lowers resolved plan roots; ``ir()`` returns the ctypes plan description."""
+
+    def __init__(self, plan, options=None):
+        self.roots = plan if isinstance(plan, list) else [plan]
+        self.options = dict(options or {})
+        self.res = []
+        self.pipes = []
+        self.result_res = -1
+        self.result_names = []
+        self.result_types = []
+        self.temp = {}
+        self.parent = {}
+        self.joins = {}   # id(EquiJoin node) -> build information
+        for r in self.roots:
+            self._link(r, None)
+        for r in self.roots:
+            self.produce(r)
+        if self.result_res < 0:
+            raise Unsupported("plan has no result materialisation")
+
+    # -- tree helpers ------------------------------------------------------------
+    def _link(self, node, parent):
+        self.parent[id(node)] = parent
+        for ch in self._children(node):
+            self._link(ch, node)
+
+    @staticmethod
+    def _children(node):
+        k = type(node).__name__
+        if k in ("Selection", "Map", "Aggregation", "Projection", "Materialize"):
+            return [node.child]
+        if k in ("EquiJoin", "CrossJoin"):
+            return [node.leftChild, node.rightChild]
+        return []
+
+    def new_res(self, res):
+        self.res.append(res)
+        return len(self.res) - 1
+
+    # -- produce / consume -------------------------------------------------------
+    def produce(self, node):
+        k = type(node).__name__
+        if k == "Scan":
+            self.scan(node)
+        elif k in ("Selection", "Map", "Projection", "Materialize", "Aggregation"):
+            self.produce(node.child)
+        elif k == "EquiJoin":
+            self.produce_join(node)
+        elif k == "CrossJoin":
+            raise Unsupported("cross joins (nested loops) are not executed by this backend")
+        else:
+            raise Unsupported("operator %s" % k)
+
+    def consume(self, node, child, pipe):
+        """Continue ``pipe`` (which delivers ``child``'s rows) at ``node``."""
+        k = type(node).__name__
+        if k == "Selection":
+            self.filter(pipe, node.condition)
+            self.consume_parent(node, pipe)
+        elif k == "Map":
+            v = self.expr(pipe, node.expression)
+            want = lang_type(node.mapAttr.dataType)
+            pipe.att[node.mapAttr.id] = self.materialize_value(pipe, v, want)
+            self.consume_parent(node, pipe)
+        elif k == "Projection":
+            self.consume_parent(node, pipe)
+        elif k == "EquiJoin":
+            if child is node.leftChild:
+                self.join_build_sink(node, pipe)
+            else:
+                self.join_probe(node, pipe)
+                self.consume_parent(node, pipe)
+        elif k == "Aggregation":
+            self.aggregate(node, pipe)
+        elif k == "Materialize":
+            self.materialize(node, pipe)
+        else:
+            raise Unsupported("operator %s" % k)
+
+    def consume_parent(self, node, pipe):
+        parent = self.parent[id(node)]
+        if parent is None:
+            raise Unsupported("plan root %s is not a materialisation" % type(node).__name__)
+        self.consume(parent, node, pipe)
+
+    # -- scans -------------------------------------------------------------------
+    def scan(self, node):
+        if node.isTempScan:
+            rid = self.temp[node.table["name"]]
+            r = self.res[rid]
+            pipe = Pipe(L.SRC_OUTPUT, source_res=rid)
+            for id, a in node.outRelation.items():
+                j = r.columns.index(a.sourceId)
+                pipe.lazy[id] = self._lazy_col(pipe, str(j), r.pay_ctype[j])
+        else:
+            pipe = Pipe(L.SRC_TABLE, table=node.table["name"])
+            for id, a in node.outRelation.items():
+                pipe.lazy[id] = self._lazy_col(pipe, a.name, lang_type(a.dataType))
+        self._scan_node = node
+        self.consume_parent(node, pipe)
+
+    @staticmethod
+    def _lazy_col(pipe, name, ctype):
+        def make():
+            c = pipe.col(name)
+            if ctype == "str":
+                return pipe.slot(L.SLOT_STR, 0, "str", src=c)
+            return pipe.slot(L.SLOT_COL, 0, ctype, src=c)
+        return make
+
+    # -- expressions -------------------------------------------------------------
+    def const(self, e):
+        t = _tname(e.type)
+        tok = e.token
+        if t == "STRING":
+            return Pattern(tok.encode() if isinstance(tok, str) else bytes(tok))
+        if t == "CHAR":
+            return Imm(_wrap(ord(tok[0]), "i8"), "i8")
+        if t == "FLOAT":
+            raise Unsupported("FLOAT constants are not exact (the reference emits (float)%s); use INT" % tok)
+        try:
+            v = int(tok)
+        except ValueError:
+            raise Unsupported("non-integer constant %r is not exact" % tok)
+        return Imm(v, "i32" if -(1 << 31) <= v < (1 << 31) else "i64")
+
+    def ctype_of(self, pipe, v):
+        if isinstance(v, Imm):
+            return v.ctype
+        if isinstance(v, Pattern):
+            return "strconst"
+        return pipe.slots[v]["ctype"]
+
+    def materialize_value(self, pipe, v, ctype):
+        """A slot holding v converted to ctype."""
+        if isinstance(v, Pattern):
+            raise Unsupported("string values as map results")
+        if not isinstance(v, Imm) and pipe.slots[v]["ctype"] == ctype:
+            return v
+        if ctype == "str":
+            raise Unsupported("string-valued maps")
+        d = pipe.reg(ctype)
+        if isinstance(v, Imm):
+            pipe.op(L.OP_CAST, dst=d, ctype=CT[ctype], flags=L.OPF_A_IMM, imm=_imm64(_wrap(v.value, ctype)))
+        else:
+            pipe.op(L.OP_CAST, dst=d, a=v, ctype=CT[ctype])
+        return d
+
+    def binary_operands(self, pipe, a, b, t):
+        """Operand fields for an op computing in t; at most one immediate."""
+        kw = {}
+        if isinstance(a, Imm) and isinstance(b, Imm):
+            a = self.materialize_value(pipe, a, t)
+        if isinstance(a, Imm):
+            kw.update(flags=L.OPF_A_IMM, imm=_imm64(_wrap(a.value, t)), b=b)
+        elif isinstance(b, Imm):
+            kw.update(flags=L.OPF_B_IMM, imm=_imm64(_wrap(b.value, t)), a=a)
+        else:
+            kw.update(a=a, b=b)
+        return kw
+
+    ARITH = {"AddExpr": L.ADD, "SubExpr": L.SUB, "MulExpr": L.MUL, "DivExpr": L.DIV}
+    CMPS = {"EqualsExpr": L.EQ, "SmallerExpr": L.LT, "SmallerEqualExpr": L.LE,
+            "LargerExpr": L.GT, "LargerEqualExpr": L.GE}
+
+    def expr(self, pipe, e):
+        """Lower scalar expression e; returns a slot index, Imm or Pattern."""
+        k = type(e).__name__
+        if k == "AttrExpr":
+            return pipe.attr_slot(e.attr)
+        if k == "ConstExpr":
+            return self.const(e)
+        if k in self.ARITH:
+            a = self.expr(pipe, e.leftChild)
+            b = self.expr(pipe, e.rightChild)
+            t = common_type(self.ctype_of(pipe, a), self.ctype_of(pipe, b))
+            d = pipe.reg(t)
+            pipe.op(L.OP_ARITH, sub=self.ARITH[k], dst=d, ctype=CT[t], **self.binary_operands(pipe, a, b, t))
+            return d
+        if k in self.CMPS:
+            a = self.expr(pipe, e.leftChild)
+            b = self.expr(pipe, e.rightChild)
+            ta, tb = self.ctype_of(pipe, a), self.ctype_of(pipe, b)
+            if "str" in (ta, tb) or "strconst" in (ta, tb):
+                if k != "EqualsExpr":
+                    raise Unsupported("ordering comparisons on strings")
+                if ta == "strconst":
+                    a, b = b, a
+                    ta, tb = tb, ta
+                if ta != "str" or tb != "strconst":
+                    raise Unsupported("string equality needs an attribute and a constant")
+                d = pipe.reg("i32")
+                pipe.op(L.OP_STREQ, dst=d, a=a, res=pipe.pattern(b.data))
+                return d
+            t = common_type(ta, tb)
+            d = pipe.reg("i32")
+            pipe.op(L.OP_CMP, sub=self.CMPS[k], dst=d, ctype=CT[t], **self.binary_operands(pipe, a, b, t))
+            return d
+        if k in ("AndExpr", "OrExpr"):
+            a = self.as_slot(pipe, self.expr(pipe, e.leftChild))
+            b = self.as_slot(pipe, self.expr(pipe, e.rightChild))
+            d = pipe.reg("i32")
+            pipe.op(L.OP_LOGIC, sub=L.AND if k == "AndExpr" else L.OR, dst=d, a=a, b=b)
+            return d
+        if k == "NotExpr":
+            a = self.as_slot(pipe, self.expr(pipe, e.child))
+            d = pipe.reg("i32")
+            pipe.op(L.OP_LOGIC, sub=L.NOT, dst=d, a=a)
+            return d
+        if k == "LikeExpr":
+            s = self.expr(pipe, e.leftChild)
+            p = self.expr(pipe, e.rightChild)
+            if not isinstance(p, Pattern) or self.ctype_of(pipe, s) != "str":
+                raise Unsupported("LIKE needs a string attribute and a constant pattern")
+            d = pipe.reg("i32")
+            pipe.op(L.OP_LIKE, dst=d, a=s, res=pipe.pattern(p.data))
+            return d
+        if k == "ExtractExpr":
+            a = self.expr(pipe, e.child)
+            t = common_type(self.ctype_of(pipe, a), "i32")
+            ext = _tname(e.extract)
+            if ext == "YEAR":
+                steps = [(L.DIV, 10000)]
+            elif ext == "DAY":
+                steps = [(L.MOD, 100)]
+            else:
+                steps = [(L.DIV, 100), (L.MOD, 100)]
+            for sub, c in steps:
+                d = pipe.reg(t)
+                pipe.op(L.OP_ARITH, sub=sub, dst=d, ctype=CT[t], **self.binary_operands(pipe, a, Imm(c, "i32"), t))
+                a = d
+            return a
+        if k == "CaseExpr":
+            d = pipe.reg("u64")
+            if e.exprElse is not None:
+                ev = self.expr(pipe, e.exprElse)
+                self._cast_into(pipe, d, ev, "u64")
+            else:
+                pipe.op(L.OP_CAST, dst=d, ctype=CT["u64"], flags=L.OPF_A_IMM, imm=0)
+            for w, th in reversed(e.exprListWhenThen):
+                c = self.as_slot(pipe, self.expr(pipe, w))
+                tv = self.expr(pipe, th)
+                kw = dict(dst=d, a=c, c=d, ctype=CT["u64"])
+                if isinstance(tv, Imm):
+                    kw.update(flags=L.OPF_B_IMM, imm=_imm64(_wrap(tv.value, "u64")))
+                else:
+                    kw.update(b=tv)
+                pipe.op(L.OP_SELECT, **kw)
+            return d
+        raise Unsupported("scalar expression %s" % k)
+
+    def _cast_into(self, pipe, d, v, t):
+        if isinstance(v, Imm):
+            pipe.op(L.OP_CAST, dst=d, ctype=CT[t], flags=L.OPF_A_IMM, imm=_imm64(_wrap(v.value, t)))
+        else:
+            pipe.op(L.OP_CAST, dst=d, a=v, ctype=CT[t])
+
+    def as_slot(self, pipe, v):
+        if isinstance(v, Imm):
+            return self.materialize_value(pipe, v, _promote(v.ctype))
+        if isinstance(v, Pattern):
+            raise Unsupported("string constant used as a value")
+        return v
+
+    def filter(self, pipe, condition):
+        v = self.expr(pipe, condition)
+        if isinstance(v, Imm):
+            if v.value != 0:
+                return
+            v = self.materialize_value(pipe, v, "i32")
+        pipe.op(L.OP_FILTER, a=v)
+
+    # -- joins -------------------------------------------------------------------
+    def produce_join(self, node):
+        if self.joins.get(id(node), {}).get("built"):
+            # a second pass over an enclosing build pipeline: this join's own
+            # table exists already, only its probe side is produced again
+            self.produce(node.rightChild)
+            return
+        jt = _tname(node.joinType)
+        if jt == "OUTER":
+            raise Unsupported("outer joins are not executed by this backend")
+        if node.conditions is not None:
+            raise Unsupported("equi-joins with extra non-equality conditions")
+        bk = list(node.buildKeyAttributes.values())
+        pk = list(node.probeKeyAttributes.values())
+        if len(bk) > L.MAX_KEYS:
+            raise Unsupported("more than %d join keys" % L.MAX_KEYS)
+        key_types = []
+        for b, p in zip(bk, pk):
+            tb, tp = lang_type(b.dataType), lang_type(p.dataType)
+            if "str" in (tb, tp):
+                raise Unsupported("string join keys")
+            key_types.append(common_type(tb, tp))
+        build_atts = list(node.leftChild.outRelation.values())
+        unique = not getattr(node, "multimatch", True) or jt in ("SEMI", "ANTI")
+        est = max(int(node.leftChild.tupleNum), 1)
+        cap = max(int(est * float(getattr(node, "htSizeFactor", 2.0))), 16)
+        if jt in ("SEMI", "ANTI"):
+            build_atts = []
+        if unique:
+            payload = [lang_type(a.dataType) for a in build_atts]
+            if any(t == "str" for t in payload):
+                raise Unsupported("string attributes in join payloads")
+            rid = self.new_res(Res(L.RES_UNIQUE, nkeys=len(bk), key_ctype=key_types, pay_ctype=payload,
+                                   capacity=cap))
+            info = dict(res=rid, unique=True, bk=bk, pk=pk, build_atts=build_atts, passes=["build"])
+        else:
+            keys_in_payload = [build_atts.index(b) if b in build_atts else -1 for b in bk]
+            atts = list(build_atts)
+            for i, b in enumerate(bk):
+                if keys_in_payload[i] < 0:
+                    atts.append(b)
+            payload = [lang_type(a.dataType) for a in atts]
+            if any(t == "str" for t in payload):
+                raise Unsupported("string attributes in join payloads")
+            if len(payload) > L.MAX_PAY:
+                raise Unsupported("more than %d payload attributes" % L.MAX_PAY)
+            rid = self.new_res(Res(L.RES_MULTI, nkeys=len(bk), key_ctype=key_types, pay_ctype=payload,
+                                   capacity=cap))
+            info = dict(res=rid, unique=False, bk=bk, pk=pk, build_atts=atts, passes=["count", "scatter"])
+        self.joins[id(node)] = info
+        for p in info["passes"]:
+            info["pass"] = p
+            self.produce(node.leftChild)
+        info["built"] = True
+        self.produce(node.rightChild)
+
+    def join_build_sink(self, node, pipe):
+        info = self.joins[id(node)]
+        keys = [pipe.attr_slot(a) for a in info["bk"]]
+        kl, kn = pipe.list_(keys)
+        if info["unique"]:
+            pl, pn = pipe.list_([pipe.attr_slot(a) for a in info["build_atts"]])
+            pipe.op(L.OP_BUILD, res=info["res"], list=kl, nlist=kn, list2=pl, nlist2=pn)
+        elif info["pass"] == "count":
+            pipe.op(L.OP_MM_COUNT, res=info["res"], list=kl, nlist=kn)
+        else:
+            pl, pn = pipe.list_([pipe.attr_slot(a) for a in info["build_atts"]])
+            pipe.op(L.OP_MM_SCATTER, res=info["res"], list=kl, nlist=kn, list2=pl, nlist2=pn)
+        self.finish(pipe)
+
+    def join_probe(self, node, pipe):
+        info = self.joins[id(node)]
+        jt = _tname(node.joinType)
+        keys = [pipe.attr_slot(a) for a in info["pk"]]
+        kl, kn = pipe.list_(keys)
+        if info["unique"]:
+            dsts = []
+            for a in info["build_atts"]:
+                s = pipe.reg(lang_type(a.dataType))
+                pipe.att[a.id] = s
+                dsts.append(s)
+            pl, pn = pipe.list_(dsts)
+            sub = {"INNER": L.JOIN_INNER, "SEMI": L.JOIN_SEMI, "ANTI": L.JOIN_ANTI}[jt]
+            pipe.op(L.OP_PROBE, sub=sub, res=info["res"], list=kl, nlist=kn, list2=pl, nlist2=pn)
+        else:
+            if pipe.level + 1 >= L.MAX_LEVELS:
+                raise Unsupported("more than %d nested multimatch joins in one pipeline" % (L.MAX_LEVELS - 1))
+            lv = pipe.level + 1
+            gathers = []
+            for j, a in enumerate(info["build_atts"]):
+                s = pipe.slot(L.SLOT_GATHER, lv, lang_type(a.dataType), src=j, res=info["res"])
+                pipe.att[a.id] = s
+                gathers.append(s)
+            bkeys = [gathers[info["build_atts"].index(b)] for b in info["bk"]]
+            bl, bn = pipe.list_(bkeys)
+            pipe.op(L.OP_EXPAND, res=info["res"], list=kl, nlist=kn, list2=bl, nlist2=bn)
+            pipe.level = lv
+
+    # -- aggregation -------------------------------------------------------------
+    RED = {"SUM": L.RED_SUM, "AVG": L.RED_SUM, "COUNT": L.RED_COUNT, "MIN": L.RED_MIN, "MAX": L.RED_MAX}
+
+    def aggregate(self, node, pipe):
+        groups = list(node.groupAttributes.values())
+        if len(groups) > L.MAX_KEYS:
+            raise Unsupported("more than %d grouping attributes" % L.MAX_KEYS)
+        gtypes = [lang_type(g.dataType) for g in groups]
+        if "str" in gtypes:
+            raise Unsupported("grouping by strings")
+        aggs = [(id, inId, _tname(red)) for id, (inId, red) in node.aggregateTuples.items()]
+        if len(aggs) > L.MAX_AGGS:
+            raise Unsupported("more than %d aggregates" % L.MAX_AGGS)
+        numgroups = max(int(getattr(node, "numgroups", 1)), 1)
+        cap = max(2 * numgroups, 1024) if groups else 1
+        rid = self.new_res(Res(L.RES_AGG, nkeys=len(groups), key_ctype=gtypes,
+                               agg_red=[self.RED[r] for _, _, r in aggs], capacity=cap, group_hint=numgroups))
+        kl, kn = pipe.list_([pipe.attr_slot(g) for g in groups])
+        inputs = []
+        for id, inId, red in aggs:
+            if red == "COUNT":
+                inputs.append(-1)
+            else:
+                a = node.aggregateInAttributes[inId]
+                if lang_type(a.dataType) == "str":
+                    raise Unsupported("aggregating strings")
+                inputs.append(pipe.attr_slot(a))
+        il, inn = pipe.list_(inputs)
+        pipe.op(L.OP_AGG, res=rid, list=kl, nlist=kn, list2=il, nlist2=inn)
+        self.finish(pipe)
+        # the aggregation table becomes the source of the next pipeline
+        out = Pipe(L.SRC_AGG, source_res=rid)
+        for j, g in enumerate(groups):
+            out.att[g.id] = out.slot(L.SLOT_AGGKEY, 0, gtypes[j], src=j, res=rid)
+        count_slot = None
+        for j, (id, inId, red) in enumerate(aggs):
+            t = "i32" if red == "COUNT" else "u64"
+            out.att[id] = out.slot(L.SLOT_AGGVAL, 0, t, src=j, res=rid)
+            if red == "COUNT":
+                count_slot = out.att[id]
+        for id, (inId, red) in node.aggregateTuples.items():
+            if _tname(red) == "AVG":
+                d = out.reg("u64")
+                out.op(L.OP_ARITH, sub=L.DIV, dst=d, a=out.att[id], b=count_slot, ctype=L.U64)
+                out.att[id] = d
+        self.consume_parent(node, out)
+
+    # -- materialisation ---------------------------------------------------------
+    def materialize(self, node, pipe):
+        atts = list(node.outRelation.values())
+        types = [lang_type(a.dataType) for a in atts]
+        if "str" in types:
+            raise Unsupported("string result columns")
+        temp = _tname(node.matType) == "TEMPTABLE"
+        cap = max(int(getattr(node, "tupleNum", 0)), 1024)
+        if type(node.child).__name__ == "Aggregation":
+            cap = max(cap, self.res[pipe.source_res].capacity + 1)
+        rid = self.new_res(Res(L.RES_OUTPUT, pay_ctype=types, capacity=cap,
+                               name=node.table["name"] if temp else None,
+                               columns=[a.id for a in atts]))
+        sl, sn = pipe.list_([pipe.attr_slot(a) for a in atts])
+        pipe.op(L.OP_EMIT, res=rid, list=sl, nlist=sn)
+        self.finish(pipe)
+        if temp:
+            self.temp[node.table["name"]] = rid
+        else:
+            self.result_res = rid
+            self.result_names = [a.name for a in atts]
+            self.result_types = [CT[t] for t in types]
+
+    def finish(self, pipe):
+        self.pipes.append(pipe)
+
+    # -- IR ----------------------------------------------------------------------
+    def ir(self):
+        """ctypes ``dq_plan_desc`` plus the objects that keep its memory alive."""
+        keep = []
+        res_arr = (L.dq_resource * max(len(self.res), 1))()
+        for i, r in enumerate(self.res):
+            d = res_arr[i]
+            d.kind = r.kind
+            d.nkeys = r.nkeys
+            for j, t in enumerate(r.key_ctype):
+                d.key_ctype[j] = CT[t]
+            d.npay = len(r.pay_ctype)
+            for j, t in enumerate(r.pay_ctype):
+                d.pay_ctype[j] = CT[t] if isinstance(t, str) else t
+            d.naggs = len(r.agg_red)
+            for j, red in enumerate(r.agg_red):
+                d.agg_red[j] = red
+            d.capacity = r.capacity
+            d.group_hint = r.group_hint
+            if r.name:
+                b = r.name.encode()
+                keep.append(b)
+                d.name = b
+        pipe_arr = (L.dq_pipeline * len(self.pipes))()
+        for i, p in enumerate(self.pipes):
+            d = pipe_arr[i]
+            d.source_kind = p.source_kind
+            d.source_res = p.source_res
+            if p.table:
+                b = p.table.encode()
+                keep.append(b)
+                d.table = b
+            if len(p.cols) > L.MAX_COLS:
+                raise Unsupported("pipeline reads more than %d columns" % L.MAX_COLS)
+            d.ncols = len(p.cols)
+            for j, c in enumerate(p.cols):
+                b = c.encode()
+                keep.append(b)
+                d.cols[j] = b
+            d.nslots = len(p.slots)
+            for j, s in enumerate(p.slots):
+                ds = d.slots[j]
+                ds.kind, ds.level, ds.ctype = s["kind"], s["level"], CT[s["ctype"]]
+                ds.src, ds.res = s["src"], s["res"]
+            d.nops = len(p.ops)
+            for j, o in enumerate(p.ops):
+                do = d.ops[j]
+                for f in ("kind", "sub", "dst", "a", "b", "c", "ctype", "flags", "res", "list", "nlist",
+                          "list2", "nlist2", "imm"):
+                    setattr(do, f, o[f])
+            d.nlist = len(p.lists)
+            for j, v in enumerate(p.lists):
+                d.lists[j] = v
+            d.npatterns = len(p.patterns)
+            for j, pat in enumerate(p.patterns):
+                keep.append(pat)
+                d.patterns[j] = pat
+            d.compact = 1
+        desc = L.dq_plan_desc()
+        desc.abi_version = L.ABI_VERSION
+        desc.nres = len(self.res)
+        desc.res = res_arr
+        desc.npipes = len(self.pipes)
+        desc.pipes = pipe_arr
+        desc.result_res = self.result_res
+        keep += [res_arr, pipe_arr]
+        return desc, keep
+
+    def describe(self):
+        """Readable summary of the lowered plan (for logs and tests)."""
+        lines = []
+        for i, r in enumerate(self.res):
+            lines.append("res %d kind=%d keys=%s pay=%s aggs=%s cap=%d" % (
+                i, r.kind, r.key_ctype, r.pay_ctype, r.agg_red, r.capacity))
+        for i, p in enumerate(self.pipes):
+            lines.append("pipe %d src=%d table=%s cols=%s slots=%d ops=%s" % (
+                i, p.source_kind, p.table, p.cols, len(p.slots), [o["kind"] for o in p.ops]))
+        return "\n".join(lines)

@@ -62,6 +62,9 @@ typedef struct {
     int32_t tile_rows;          /* rows per tile (0 = default)                  */
     int32_t ctas_per_sm;        /* persistent CTAs per SM (0 = default)         */
     int32_t flags;              /* DQ_CFG_* bits                                */
+    int32_t defer_threshold;    /* expansion ranges longer than this many pairs */
+                                /* are split across CTAs (0 = 8 tiles)          */
+    int32_t reserved;
 } dq_config;
 
 #define DQ_CFG_NO_TMA      1    /* stage tiles with plain loads instead of TMA */

@@ -1,0 +1,79 @@
+"""Host-side lowering of every workload plan into the pipeline IR (no GPU)."""
+import pytest
+
+from dogqc_b200 import _lib as L
+from dogqc_b200 import workloads
+from dogqc_b200.lowering import Lowering, Unsupported, common_type
+from dogqc_b200.relational import RelationalAlgebra
+
+SCALES = {"c0": 0.001, "c1": 0.001, "c2": 0.0005, "c3": 0.0002}
+
+
+@pytest.mark.parametrize("name", sorted(SCALES))
+def test_workload_lowers(name):
+    db = workloads.GENERATORS[name](SCALES[name])
+    alg = RelationalAlgebra(db)
+    plan, cfg = workloads.build(name, alg)
+    plan = alg.resolveAlgebraPlan(plan, cfg)
+    lw = Lowering(plan)
+    desc, keep = lw.ir()
+    assert desc.npipes == len(lw.pipes) >= 2
+    for p in lw.pipes:
+        assert p.ops[-1]["kind"] >= L.OP_AGG
+    sinks = [p.ops[-1]["kind"] for p in lw.pipes]
+    if name == "c2":
+        assert sinks[:2] == [L.OP_MM_COUNT, L.OP_MM_SCATTER]
+        assert any(o["kind"] == L.OP_EXPAND for o in lw.pipes[2].ops)
+    if name == "c1":
+        assert sinks == [L.OP_BUILD, L.OP_AGG, L.OP_EMIT]
+    assert lw.result_names
+
+
+def test_c_conversions():
+    assert common_type("i8", "i8") == "i32"
+    assert common_type("i32", "u32") == "u32"
+    assert common_type("u32", "i64") == "i64"
+    assert common_type("i32", "u64") == "u64"
+
+
+def test_float_constants_rejected():
+    import dogqc_b200.scalar as scal
+    from dogqc_b200.types import Type
+    db = workloads.gen_c0(0.0001)
+    alg = RelationalAlgebra(db)
+    plan = alg.map("x", scal.MulExpr(scal.AttrExpr("l_extendedprice"), scal.ConstExpr("0.5", Type.FLOAT)),
+                   alg.scan("lineitem"))
+    plan = alg.resolveAlgebraPlan(plan, {})
+    with pytest.raises(Unsupported):
+        Lowering(plan)
+
+
+def test_reference_front_end_trees_lower(tmp_path):
+    """The backend accepts trees built with the reference's own classes."""
+    import os
+    import sys
+    import types as pytypes
+    ref = os.environ.get("DOGQC_REFERENCE", "/root/reference")
+    if not os.path.isdir(os.path.join(ref, "dogqc")):
+        pytest.skip("reference source tree not present")
+    sys.path.insert(0, ref)
+    try:
+        import dogqc.scalarAlgebra as rscal
+        from dogqc.relationalAlgebra import RelationalAlgebra as RAlg, Reduction as RRed
+        from dogqc.types import Type as RType
+    finally:
+        sys.path.remove(ref)
+    db = workloads.gen_c1(0.001)
+    schema = {}
+    for t, e in db.schema.items():
+        e = dict(e)
+        e["attributes"] = type(e["attributes"])((a, RType[ty.name]) for a, ty in e["attributes"].items())
+        schema[t] = e
+    alg = RAlg(pytypes.SimpleNamespace(schema=schema))
+    plan, cfg = workloads.plan_c1(alg, rscal, RType, RRed)
+    plan = alg.resolveAlgebraPlan(plan, cfg)
+    ours = RelationalAlgebra(db)
+    p2, c2 = workloads.build("c1", ours)
+    p2 = ours.resolveAlgebraPlan(p2, c2)
+    a, b = Lowering(plan), Lowering(p2)
+    assert a.describe() == b.describe()
