@@ -56,59 +56,57 @@ def load_profile_traffic():
 
 
 class ClockSampler(object):
-    """nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML every few
+    milliseconds while the timed region runs (the counters nvidia-smi reports as
+    clocks.sm and clocks_event_reasons.*)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
-    def __init__(self, device):
+    def __init__(self, device, period=0.002):
         self.device = device
-        self.proc = None
-        self.lines = []
+        self.period = period
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self.nvml = None
+        self.stop = threading.Event()
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.nvml = pynvml
+            self.thread = threading.Thread(target=self._run, daemon=True)
             self.thread.start()
         except Exception:
-            self.proc = None
+            self.nvml = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        nv = self.nvml
+        while not self.stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, mask in self.REASONS.items():
+                    if bits & mask:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        self.stop.set()
+        if self.nvml:
+            self.thread.join(timeout=2)
 
     def summary(self):
-        mhz, maxmhz, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                mhz.append(float(parts[1]))
-                maxmhz = float(parts[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        mhz.sort()
-        return {"sm_mhz": mhz[len(mhz) // 2] if mhz else None, "sm_max_mhz": maxmhz,
-                "reasons": sorted(reasons), "samples": len(mhz)}
+        mhz = sorted(self.samples)
+        return {"sm_mhz": mhz[len(mhz) // 2] if mhz else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(mhz), "source": "nvml"}
 
 
 def dist_setup():
@@ -158,7 +156,7 @@ def run_ours(args, world, rank, local):
     plan = build_plan(db)
     rows_per_step = sum(t.size for t in db.tables.values())
     fact_bytes = db["fact"].nbytes
-    engine = Engine(local)
+    engine = Engine(local, tile_rows=args.tile_rows, ctas_per_sm=args.ctas_per_sm, flags=args.engine_flags)
     engine.register_database(db)
     p = engine.prepare(plan)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -207,20 +205,22 @@ def run_ours(args, world, rank, local):
     h2d = sum(t.nbytes for t in db.tables.values())
     d2h_rows = res.nrows
     d2h = sum(c.nbytes for c in res.columns) + 12
-    for _ in range(2):
-        for pt in ptables:
-            engine.update_table(pt)
-        p.execute()
-    dist_barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for pt in ptables:
-            engine.update_table(pt)
-        r2 = p.execute()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = dist_max(e2e_s, world)
-    assert r2.nrows == d2h_rows
-    e2e_value = rows_per_step * world * args.steps / e2e_s
+    e2e_value = None
+    if not args.no_e2e:
+        for _ in range(2):
+            for pt in ptables:
+                engine.update_table(pt)
+            p.execute()
+        dist_barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            for pt in ptables:
+                engine.update_table(pt)
+            r2 = p.execute()
+        e2e_s = time.perf_counter() - t0
+        e2e_s = dist_max(e2e_s, world)
+        assert r2.nrows == d2h_rows
+        e2e_value = rows_per_step * world * args.steps / e2e_s
 
     peak, peak_kind = hbm_peak()
     probe_avg_s = probe_ms / args.steps / 1e3
@@ -345,8 +345,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--tile-rows", type=int, default=0, help="engine tile size (0: default)")
+    ap.add_argument("--ctas-per-sm", type=int, default=0, help="persistent CTAs per SM (0: occupancy)")
+    ap.add_argument("--engine-flags", type=int, default=0, help="DQ_CFG_* bits")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="workload size factor (profiling only; the bench line is quoted at 1.0)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global SCALE
+    SCALE = args.scale
     world, rank, local = dist_setup()
     if args.impl == "reference":
         out = run_reference(args, world, rank)

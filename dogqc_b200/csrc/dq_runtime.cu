@@ -134,7 +134,8 @@ struct PipeRec {
   std::vector<std::string> col_names;
   std::vector<std::string> patterns;
   DevPipe dev{};
-  int grid = 1;
+  int grid = 1;             // CTAs of a tile launch (at most one per tile)
+  int grid_full = 1;        // persistent grid (SMs x resident CTAs)
   int expand_op = -1;       // level-0 expansion op with deferral
   DevBuf pattern_buf, heavy_items, heavy_count, heavy_prefix;
   bool mm_count = false;    // sink is a multimap count: bucket scan follows
@@ -592,7 +593,12 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   int occ = pipeline_occupancy(P.smem_bytes);
   if (occ < 1) throw DqError(DQ_ERR_UNSUPPORTED, "pipeline kernel cannot be resident with this shared memory");
   int want = ctx->cfg.ctas_per_sm > 0 ? std::min(ctx->cfg.ctas_per_sm, occ) : occ;
-  p.grid = ctx->sms * want;
+  p.grid_full = ctx->sms * want;
+  p.grid = p.grid_full;
+  if (!P.nrows_dev) {  // no more CTAs than tiles
+    int64_t ntiles = (P.nrows + tile - 1) / tile;
+    p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(p.grid_full, ntiles));
+  }
 }
 
 void free_events(dq_plan* plan) {
@@ -647,7 +653,7 @@ int run_once(dq_plan* plan, cudaStream_t st) {
       DevPipe H = p.dev;
       H.mode = 1;
       H.tile_counter = counters + 2 * i + 1;
-      DQ_CUDA(launch_pipeline(H, p.grid, st));
+      DQ_CUDA(launch_pipeline(H, p.grid_full, st));
       launches += 2;
     }
     if (p.mm_count) {

@@ -477,6 +477,11 @@ class Lowering(object):
         if jt in ("SEMI", "ANTI"):
             build_atts = []
         if unique:
+            packed = len(bk) == 1 or (len(bk) == 2 and all(t in ("i8", "i32", "u32") for t in key_types))
+            if packed:
+                # the packed tag is the exact key: build keys that no operator above
+                # the join reads need not be stored in the payload
+                build_atts = [a for a in build_atts if not (a in bk and a.lastUse <= node.opId)]
             payload = [lang_type(a.dataType) for a in build_atts]
             if any(t == "str" for t in payload):
                 raise Unsupported("string attributes in join payloads")
