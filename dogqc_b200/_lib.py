@@ -91,9 +91,21 @@ class dq_plan_timing(C.Structure):
                 ("kernel_launches", C.c_int32), ("pipeline_ms", C.c_double * MAX_OPS)]
 
 
+NOALLOC_MAX_BUILD_ROWS = 262144
+NOALLOC_MAX_GROUPS = 4096
+
+
+class dq_join_agg_args(C.Structure):
+    _fields_ = [("build_key", C.c_void_p), ("build_filter", C.c_void_p), ("filter_value", C.c_int32),
+                ("build_group", C.c_void_p), ("build_rows", C.c_int64), ("probe_key", C.c_void_p),
+                ("probe_value", C.c_void_p), ("probe_rows", C.c_int64), ("out_group", C.c_void_p),
+                ("out_sum", C.c_void_p), ("out_count", C.c_void_p), ("out_ngroups", C.c_void_p),
+                ("max_groups", C.c_int32)]
+
+
 def check_layout():
     """Sizes the C compiler gives these structs on x86-64 (LP64)."""
-    expect = {dq_config: 40, dq_column: 40, dq_slot: 8, dq_op: 40, dq_resource: 80}
+    expect = {dq_config: 40, dq_column: 40, dq_slot: 8, dq_op: 40, dq_resource: 80, dq_join_agg_args: 104}
     for t, n in expect.items():
         if C.sizeof(t) != n:
             raise AssertionError("%s is %d bytes, header implies %d" % (t.__name__, C.sizeof(t), n))
@@ -124,6 +136,7 @@ EXPORTS = {
     "dq_result_ncols": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "dq_result_column": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_void_p)]),
     "dq_result_free": (None, [C.c_void_p]),
+    "dq_join_agg_noalloc": (C.c_int, [C.POINTER(dq_join_agg_args), C.c_void_p]),
 }
 
 

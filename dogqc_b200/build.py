@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libdogqc_b200.so")
-SOURCES = ["dq_kernels.cu", "dq_runtime.cu"]
+SOURCES = ["dq_kernels.cu", "dq_runtime.cu", "dq_noalloc.cu"]
 HEADERS = ["dq_device.h", os.path.join("..", "..", "include", "dogqc_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

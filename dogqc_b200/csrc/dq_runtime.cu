@@ -40,6 +40,15 @@ namespace {
 
 std::string g_init_error;
 
+}  // namespace
+
+namespace dq_internal {
+// Error text for entry points without a context (read with dq_last_error(NULL)).
+void set_global_error(const std::string& msg) { g_init_error = msg; }
+}  // namespace dq_internal
+
+namespace {
+
 struct DqError : std::runtime_error {
   int code;
   DqError(int c, const std::string& m) : std::runtime_error(m), code(c) {}

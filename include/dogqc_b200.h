@@ -261,6 +261,53 @@ int dq_result_ncols(dq_result* r, int32_t* ncols);
 int dq_result_column(dq_result* r, int32_t col, int32_t* ctype, const void** data);
 void dq_result_free(dq_result* r);
 
+/* ------------------------------------------------- allocation-free join -- */
+/* No counterpart in the reference (whose generated programs allocate every
+ * buffer with cudaMalloc).  For callers that cannot allocate device memory
+ * themselves -- code inside a host program that owns all device memory through
+ * its own pool, plugins whose allocator must account for every byte, paths on
+ * which cudaMalloc/cudaFree would synchronise the device -- this entry point
+ * runs the FK-PK join + grouped SUM/COUNT plan
+ *     aggregation([group], [SUM(value), COUNT])(
+ *       join(build.key = probe.key, selection(build.filter == filter_value, build), probe))
+ * with no allocation at all: its hash table and group table live in one
+ * statically sized device array (about 8.2 MB) that every GPU loading this
+ * library holds until the process exits.  The caller passes device pointers for
+ * all inputs and outputs and the stream to launch on.
+ *   - Limits: build_rows <= DQ_NOALLOC_MAX_BUILD_ROWS, max_groups <=
+ *     DQ_NOALLOC_MAX_GROUPS; larger requests return DQ_ERR_INVALID with a
+ *     message in dq_last_error(NULL).
+ *   - out_group/out_sum/out_count must hold max_groups entries; *out_ngroups
+ *     receives the number of groups, or -1 when they did not fit.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - Every call reuses the same array and clears what must start empty, so
+ *     calls whose work overlaps on the GPU (different streams or threads)
+ *     race; serialise them.
+ *   - Runs on the calling thread's current device.  Returns without
+ *     synchronising; results are ready when the stream reaches them.       */
+#define DQ_NOALLOC_MAX_BUILD_ROWS 262144
+#define DQ_NOALLOC_MAX_GROUPS 4096
+
+typedef struct {
+    const int32_t* build_key;       /* unique join keys of the build side       */
+    const int32_t* build_filter;    /* rows with build_filter == filter_value   */
+    int32_t filter_value;
+    const int32_t* build_group;     /* grouping value carried to the output     */
+    int64_t build_rows;
+    const int32_t* probe_key;       /* foreign keys of the probe side           */
+    const uint64_t* probe_value;    /* summed per group                         */
+    int64_t probe_rows;
+    int32_t* out_group;
+    uint64_t* out_sum;
+    int32_t* out_count;
+    int64_t* out_ngroups;
+    int32_t max_groups;
+} dq_join_agg_args;
+
+int dq_join_agg_noalloc(const dq_join_agg_args* args, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
