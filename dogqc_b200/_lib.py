@@ -40,7 +40,7 @@ OPF_B_IMM, OPF_A_IMM = 1, 2
 RES_UNIQUE, RES_MULTI, RES_AGG, RES_OUTPUT = 1, 2, 3, 4
 SRC_TABLE, SRC_OUTPUT, SRC_AGG = 1, 2, 3
 TABLE_DEVICE_DATA = 1
-CFG_NO_TMA, CFG_NO_GRAPH = 1, 2
+CFG_NO_TMA, CFG_NO_GRAPH, CFG_ROW_KERNEL = 1, 2, 4
 
 
 class dq_config(C.Structure):

@@ -492,7 +492,7 @@ __device__ int64_t agg_slot_global(const DevPipe& P, const DevRes& R, uint64_t t
 __device__ __forceinline__ void accumulate(uint64_t* acc, int red, uint64_t v) {
   switch (red) {
     case DQ_RED_SUM: atomicAdd((unsigned long long*)acc, v); break;
-    case DQ_RED_COUNT: atomicAdd((unsigned long long*)acc, 1ull); break;
+    case DQ_RED_COUNT: atomicAdd((unsigned long long*)acc, v); break;  // v rows (1 per row)
     case DQ_RED_MIN: atomicMin((unsigned long long*)acc, v); break;
     case DQ_RED_MAX: atomicMax((unsigned long long*)acc, v); break;
   }
@@ -1147,6 +1147,441 @@ __global__ void __launch_bounds__(kThreads, 2) pipeline_kernel(const __grid_cons
   flush_local_aggs(P, c);
 }
 
+// ------------------------------------------------------ row-at-a-time kernel --
+//
+// Pipelines without a multimap expansion run row-at-a-time: each warp carries
+// 32 rows of a staged tile through the whole operator list, with one active
+// flag per lane, and leaves as soon as no lane of the warp is active.  There is
+// no per-operator barrier, compaction or shared-memory slot traffic for
+// columns: staged columns are read in place, computed values live in a
+// per-thread shared-memory register area.  Tiles are staged exactly as for the
+// tile kernel (bulk copies on an mbarrier, three tiles ahead).
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t s_cas64(uint32_t a, uint64_t cmp, uint64_t val) {
+  uint64_t old;
+  asm volatile("atom.shared.cas.b64 %0, [%1], %2, %3;" : "=l"(old) : "r"(a), "l"(cmp), "l"(val) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void s_merge(uint32_t a, int red, uint64_t v) {
+  switch (red) {
+    case DQ_RED_SUM:
+    case DQ_RED_COUNT: asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); break;
+    case DQ_RED_MIN: asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); break;
+    case DQ_RED_MAX: asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); break;
+  }
+}
+
+// Exact reduction of one aggregate over the lanes in `in` (all 32 lanes call
+// it).  64-bit sums are split into 22-bit limbs so the 32-bit warp reductions
+// cannot overflow; min/max reduce the high words, then the low words of the
+// lanes holding the extreme high word.
+__device__ __forceinline__ uint64_t warp_reduce(int red, bool in, uint64_t v, unsigned grp) {
+  switch (red) {
+    case DQ_RED_COUNT:
+      return (uint64_t)__popc(grp);
+    case DQ_RED_SUM: {
+      uint32_t l0 = __reduce_add_sync(0xffffffffu, in ? (uint32_t)(v & 0x3fffff) : 0u);
+      uint32_t l1 = __reduce_add_sync(0xffffffffu, in ? (uint32_t)((v >> 22) & 0x3fffff) : 0u);
+      uint32_t l2 = __reduce_add_sync(0xffffffffu, in ? (uint32_t)(v >> 44) : 0u);
+      return (uint64_t)l0 + ((uint64_t)l1 << 22) + ((uint64_t)l2 << 44);
+    }
+    case DQ_RED_MIN: {
+      uint32_t hi = __reduce_min_sync(0xffffffffu, in ? (uint32_t)(v >> 32) : 0xffffffffu);
+      uint32_t lo = __reduce_min_sync(0xffffffffu, (in && (uint32_t)(v >> 32) == hi) ? (uint32_t)v : 0xffffffffu);
+      return ((uint64_t)hi << 32) | lo;
+    }
+    default: {
+      uint32_t hi = __reduce_max_sync(0xffffffffu, in ? (uint32_t)(v >> 32) : 0u);
+      uint32_t lo = __reduce_max_sync(0xffffffffu, (in && (uint32_t)(v >> 32) == hi) ? (uint32_t)v : 0u);
+      return ((uint64_t)hi << 32) | lo;
+    }
+  }
+}
+
+struct Row {
+  const DevPipe* P;
+  const uint8_t* stage;   // staged columns of the tile
+  uint64_t* regs;         // register area: value of register r of this thread at regs[r * kThreads]
+  int64_t tile_start;
+  int row;                // row within the tile
+};
+
+__device__ __forceinline__ uint64_t rget(const Row& x, int s) {
+  const DevPipe& P = *x.P;
+  const DevSlot& sl = P.slots[s];
+  switch (sl.kind) {
+    case DQ_SLOT_COL:
+      return canon(ld(x.stage + P.cols[sl.src].smem_off + (size_t)x.row * sl.width, sl.width), sl.ctype);
+    case DQ_SLOT_REG:
+      return x.regs[(size_t)sl.smem_off * kThreads];
+    case DQ_SLOT_AGGKEY: {
+      const DevRes& R = P.res[sl.res];
+      uint64_t idx = (uint64_t)(x.tile_start + x.row);
+      const uint64_t* slot = R.slots + idx * R.words;
+      uint64_t raw;
+      if (R.packed) {
+        uint64_t tag = slot[0];
+        if (idx == R.cap) tag = kEmpty;
+        raw = (R.nkeys == 1 && (R.key_ctype[0] == DQ_I64 || R.key_ctype[0] == DQ_U64))
+                  ? tag : (tag >> (32 * sl.src)) & 0xffffffffull;
+      } else {
+        raw = slot[R.key_word + sl.src];
+      }
+      return canon(raw, sl.ctype);
+    }
+    case DQ_SLOT_AGGVAL: {
+      const DevRes& R = P.res[sl.res];
+      uint64_t idx = (uint64_t)(x.tile_start + x.row);
+      return canon(R.slots[idx * R.words + R.val_word + sl.src], sl.ctype);
+    }
+    default:
+      return 0;
+  }
+}
+
+__device__ __forceinline__ void rput(const Row& x, int s, uint64_t v) {
+  const DevSlot& sl = x.P->slots[s];
+  x.regs[(size_t)sl.smem_off * kThreads] = canon(v, sl.ctype);
+}
+
+__device__ __forceinline__ void rstr(const Row& x, int s, const uint8_t*& ptr, int& len) {
+  const DevPipe& P = *x.P;
+  const DevStr& d = P.strs[P.slots[s].src];
+  int64_t g = x.tile_start + x.row;
+  if (d.width > 0) {
+    ptr = d.chars + g * d.width;
+    len = d.width;
+  } else {
+    uint64_t a = d.offsets[g], b = d.offsets[g + 1];
+    ptr = d.chars + a;
+    len = (int)(b - a);
+  }
+}
+
+__device__ __forceinline__ uint64_t rop(const Row& x, const dq_op& op, int which) {
+  if (which == 0) return (op.flags & DQ_OPF_A_IMM) ? (uint64_t)op.imm : rget(x, op.a);
+  return (op.flags & DQ_OPF_B_IMM) ? (uint64_t)op.imm : rget(x, op.b);
+}
+
+__device__ __forceinline__ void rkeys(const Row& x, const DevRes& R, int list, int n, uint64_t* k) {
+  const DevPipe& P = *x.P;
+  for (int i = 0; i < n; ++i) k[i] = canon(rget(x, P.lists[list + i]), R.key_ctype[i]);
+}
+
+// CTA-local aggregation table through shared-memory atomics.
+__device__ __forceinline__ int row_local_slot(uint64_t* tags, int ns, uint64_t tag, int nkeys) {
+  if (nkeys == 0) {
+    tags[0] = 0;
+    return 0;
+  }
+  if (tag == kEmpty) {
+    s_cas64(saddr(&tags[ns]), kEmpty, 0ull);
+    return ns;
+  }
+  uint32_t idx = (uint32_t)reduce_range(fmix64(tag), (uint64_t)ns);
+  for (int n = 0; n < ns; ++n) {
+    uint64_t t = ((volatile uint64_t*)tags)[idx];
+    if (t == tag) return (int)idx;
+    if (t == kEmpty) {
+      uint64_t old = s_cas64(saddr(&tags[idx]), kEmpty, tag);
+      if (old == kEmpty || old == tag) return (int)idx;
+    }
+    idx = (idx + 1 == (uint32_t)ns) ? 0 : idx + 1;
+  }
+  return -1;
+}
+
+__device__ void row_agg(const Row& x, const dq_op& op, bool act, uint8_t* smem) {
+  const DevPipe& P = *x.P;
+  const DevRes& R = P.res[op.res];
+  const int naggs = R.naggs;
+  uint64_t k[DQ_MAX_KEYS];
+  uint64_t tag = 0;
+  if (act) {
+    rkeys(x, R, op.list, op.nlist, k);
+    tag = key_tag(R, k);
+  }
+  const bool local = R.smem_slots > 0;
+  uint64_t* tags = local ? reinterpret_cast<uint64_t*>(smem + R.smem_off) : nullptr;
+  const int ns = R.smem_slots;
+  uint64_t* acc_base = local ? tags + (ns + 1) : nullptr;
+  const unsigned active = __ballot_sync(0xffffffffu, act);
+  const int lane = threadIdx.x & 31;
+  if (local && __popc(active) >= 12) {
+    // many rows, few groups: pre-aggregate the warp's rows per distinct key and
+    // merge each group once
+    unsigned todo = active;
+    while (todo) {
+      const int leader = __ffs(todo) - 1;
+      const uint64_t lt = __shfl_sync(0xffffffffu, tag, leader);
+      const bool in = act && tag == lt;
+      const unsigned grp = __ballot_sync(0xffffffffu, in);
+      int s = -1;
+      if (lane == leader) s = row_local_slot(tags, ns, lt, R.nkeys);
+      s = __shfl_sync(0xffffffffu, s, leader);
+      int64_t g = -1;
+      if (s < 0 && lane == leader) g = agg_slot_global(P, R, lt, k);
+      for (int j = 0; j < naggs; ++j) {
+        const int src = P.lists[op.list2 + j];
+        const uint64_t v = (in && src >= 0) ? rget(x, src) : 1;
+        const uint64_t r = warp_reduce(R.agg_red[j], in, v, grp);
+        if (lane == leader) {
+          if (s >= 0) s_merge(saddr(acc_base + (size_t)s * naggs + j), R.agg_red[j], r);
+          else if (g >= 0) accumulate(R.slots + (uint64_t)g * R.words + R.val_word + j, R.agg_red[j], r);
+        }
+      }
+      todo &= ~grp;
+    }
+    return;
+  }
+  if (!act) return;
+  if (local) {
+    int s = row_local_slot(tags, ns, tag, R.nkeys);
+    if (s >= 0) {
+      for (int j = 0; j < naggs; ++j) {
+        const int src = P.lists[op.list2 + j];
+        s_merge(saddr(acc_base + (size_t)s * naggs + j), R.agg_red[j], src >= 0 ? rget(x, src) : 1);
+      }
+      return;
+    }
+  }
+  int64_t g = agg_slot_global(P, R, tag, k);
+  if (g < 0) return;
+  uint64_t* acc = R.slots + (uint64_t)g * R.words + R.val_word;
+  for (int j = 0; j < naggs; ++j) {
+    const int src = P.lists[op.list2 + j];
+    accumulate(acc + j, R.agg_red[j], src >= 0 ? rget(x, src) : 1);
+  }
+}
+
+__device__ void row_emit(const Row& x, const dq_op& op, bool act) {
+  const DevPipe& P = *x.P;
+  const DevRes& R = P.res[op.res];
+  const unsigned active = __ballot_sync(0xffffffffu, act);
+  if (!active) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(active) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd((unsigned long long*)R.cursor, (unsigned long long)__popc(active));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (!act) return;
+  const uint64_t pos = base + __popc(active & ((1u << lane) - 1u));
+  if (pos >= R.cap) {
+    set_status(P, kErrOverflow);
+    return;
+  }
+  for (int j = 0; j < op.nlist; ++j) st(R.pay[j] + pos * R.pay_width[j], R.pay_width[j], rget(x, P.lists[op.list + j]));
+}
+
+// Runs the operator list for the calling warp's 32 rows.
+__device__ void row_ops(Row& x, bool act, uint8_t* smem) {
+  const DevPipe& P = *x.P;
+  for (int k = 0; k < P.nops; ++k) {
+    if (!__any_sync(0xffffffffu, act)) return;
+    const dq_op& op = P.ops[k];
+    switch (op.kind) {
+      case DQ_OP_ARITH:
+        if (act) rput(x, op.dst, arith(op.sub, op.ctype, rop(x, op, 0), rop(x, op, 1)));
+        break;
+      case DQ_OP_CMP:
+        if (act) rput(x, op.dst, compare(op.sub, op.ctype, rop(x, op, 0), rop(x, op, 1)));
+        break;
+      case DQ_OP_LOGIC:
+        if (act) {
+          uint64_t a = rget(x, op.a);
+          uint64_t r;
+          if (op.sub == DQ_NOT) r = a == 0;
+          else if (op.sub == DQ_AND) r = a != 0 && rget(x, op.b) != 0;
+          else r = a != 0 || rget(x, op.b) != 0;
+          rput(x, op.dst, r);
+        }
+        break;
+      case DQ_OP_CAST:
+        if (act) rput(x, op.dst, canon(rop(x, op, 0), op.ctype));
+        break;
+      case DQ_OP_SELECT:
+        if (act) {
+          uint64_t r = rget(x, op.a) ? rop(x, op, 1) : rget(x, op.c >= 0 ? op.c : op.dst);
+          rput(x, op.dst, canon(r, op.ctype));
+        }
+        break;
+      case DQ_OP_LIKE:
+      case DQ_OP_STREQ:
+        if (act) {
+          const uint8_t* s;
+          int ls;
+          rstr(x, op.a, s, ls);
+          const uint8_t* p = P.patterns + P.pat_off[op.res];
+          const int lp = P.pat_off[op.res + 1] - P.pat_off[op.res];
+          bool r;
+          if (op.kind == DQ_OP_LIKE) {
+            r = like_match(s, ls, p, lp);
+          } else {
+            r = ls == lp;
+            for (int j = 0; r && j < ls; ++j) r = s[j] == p[j];
+          }
+          rput(x, op.dst, r);
+        }
+        break;
+      case DQ_OP_FILTER:
+        if (act) act = rget(x, op.a) != 0;
+        break;
+      case DQ_OP_PROBE:
+        if (act) {
+          const DevRes& R = P.res[op.res];
+          uint64_t kv[DQ_MAX_KEYS];
+          rkeys(x, R, op.list, op.nlist, kv);
+          int64_t s = unique_find(R, key_tag(R, kv), kv);
+          if (op.sub == DQ_JOIN_ANTI) {
+            act = s < 0;
+          } else {
+            act = s >= 0;
+            if (act && op.sub == DQ_JOIN_INNER) {
+              const uint64_t* pay = R.slots + (uint64_t)s * R.words + R.val_word;
+              for (int j = 0; j < op.nlist2; ++j) {
+                int d = P.lists[op.list2 + j];
+                if (d >= 0) rput(x, d, pay[j]);
+              }
+            }
+          }
+        }
+        break;
+      case DQ_OP_AGG:
+        row_agg(x, op, act, smem);
+        return;
+      case DQ_OP_BUILD:
+        if (act) {
+          const DevRes& R = P.res[op.res];
+          uint64_t kv[DQ_MAX_KEYS];
+          rkeys(x, R, op.list, op.nlist, kv);
+          int64_t s = unique_insert(P, R, key_tag(R, kv), kv);
+          if (s >= 0) {
+            uint64_t* pay = R.slots + (uint64_t)s * R.words + R.val_word;
+            for (int j = 0; j < op.nlist2; ++j) pay[j] = rget(x, P.lists[op.list2 + j]);
+          }
+        }
+        return;
+      case DQ_OP_MM_COUNT:
+      case DQ_OP_MM_SCATTER:
+        if (act) {
+          const DevRes& R = P.res[op.res];
+          uint64_t kv[DQ_MAX_KEYS];
+          rkeys(x, R, op.list, op.nlist, kv);
+          uint64_t b = reduce_range(multimap_hash(kv, op.nlist), R.cap);
+          if (op.kind == DQ_OP_MM_COUNT) {
+            atomicAdd(&R.counts[b], 1u);
+          } else {
+            uint32_t pos = R.offsets[b] + atomicAdd(&R.counts[b], 1u);
+            for (int j = 0; j < op.nlist2; ++j)
+              st(R.pay[j] + (size_t)pos * R.pay_width[j], R.pay_width[j], rget(x, P.lists[op.list2 + j]));
+          }
+        }
+        return;
+      case DQ_OP_EMIT:
+        row_emit(x, op, act);
+        return;
+      default:
+        if (act) set_status(P, kErrBadOp);
+        return;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 3) row_kernel(const __grid_constant__ DevPipe Pk) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t s_mbar[kMaxStages];
+  if (*(volatile int32_t*)Pk.status & (kErrHtFull | kErrTimeout)) return;
+  // the descriptor is indexed with runtime values in every operator: keep it in
+  // shared memory rather than reading the parameter space through pointers
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(&Pk);
+    uint4* dst = reinterpret_cast<uint4*>(smem);
+    for (int i = threadIdx.x; i < (int)(sizeof(DevPipe) / 16); i += kThreads) dst[i] = src[i];
+  }
+  __syncthreads();
+  const DevPipe& P = *reinterpret_cast<const DevPipe*>(smem);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // CTA-local aggregation tables
+  for (int r = 0; r < P.nres; ++r) {
+    const DevRes& R = P.res[r];
+    if (R.kind == DQ_RES_AGG && R.smem_slots > 0) {
+      uint64_t* tags = reinterpret_cast<uint64_t*>(smem + R.smem_off);
+      uint64_t* acc = tags + (R.smem_slots + 1);
+      for (int i = tid; i <= R.smem_slots; i += kThreads) tags[i] = kEmpty;
+      for (int i = tid; i < (R.smem_slots + 1) * R.naggs; i += kThreads) acc[i] = red_init(R.agg_red[i % R.naggs]);
+    }
+  }
+  Row x;
+  x.P = &P;
+  x.regs = reinterpret_cast<uint64_t*>(smem + P.off_reg[0]) + tid;
+  const int64_t nrows = source_rows(P);
+  const int64_t ntiles = (nrows + P.tile - 1) / P.tile;
+  const bool staged = P.ncols > 0;
+  const bool tma = staged && P.use_tma;
+  const int64_t first = blockIdx.x, stride = gridDim.x;
+  if (tma && tid == 0) {
+    for (int s = 0; s < P.nstage; ++s) mbar_init(&s_mbar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int s = 0; s < P.nstage; ++s) {
+      int64_t t = first + s * stride;
+      if (t < ntiles) stage_issue(P, smem + P.off_stage + s * P.stage_bytes, t, nrows, &s_mbar[s]);
+    }
+  }
+  __syncthreads();
+  const bool agg_src = P.source_kind == DQ_SRC_AGG && P.res[P.source_res].nkeys > 0;
+  uint32_t phase_bits = 0;
+  for (int64_t k = 0;; ++k) {
+    const int64_t t = first + k * stride;
+    if (t >= ntiles) break;
+    const int s = tma ? (int)(k % P.nstage) : 0;
+    x.stage = smem + P.off_stage + s * P.stage_bytes;
+    x.tile_start = t * P.tile;
+    const int rows = (int)min((int64_t)P.tile, nrows - x.tile_start);
+    if (tma) {
+      mbar_wait(P, &s_mbar[s], (phase_bits >> s) & 1u);
+      phase_bits ^= 1u << s;
+    } else if (staged) {
+      stage_plain(P, smem + P.off_stage, t, nrows);
+      __syncthreads();
+    }
+    for (int base = warp * 32; base < rows; base += kThreads) {
+      x.row = base + lane;
+      bool act = x.row < rows;
+      if (act && agg_src) {
+        const DevRes& R = P.res[P.source_res];
+        act = R.slots[(uint64_t)(x.tile_start + x.row) * R.words] != kEmpty;
+      }
+      row_ops(x, act, smem);
+    }
+    __syncthreads();
+    if (tma && tid == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      int64_t nt = first + (k + P.nstage) * stride;
+      if (nt < ntiles) stage_issue(P, smem + P.off_stage + s * P.stage_bytes, nt, nrows, &s_mbar[s]);
+    }
+  }
+  // merge the CTA-local aggregation tables
+  __syncthreads();
+  for (int r = 0; r < P.nres; ++r) {
+    const DevRes& R = P.res[r];
+    if (R.kind != DQ_RES_AGG || R.smem_slots <= 0) continue;
+    const uint64_t* tags = reinterpret_cast<const uint64_t*>(smem + R.smem_off);
+    const uint64_t* acc = tags + (R.smem_slots + 1);
+    for (int i = tid; i <= R.smem_slots; i += kThreads) {
+      uint64_t tag = tags[i];
+      if (tag == kEmpty) continue;
+      if (i == R.smem_slots) tag = kEmpty;
+      int64_t g = R.nkeys == 0 ? 0 : agg_slot_global(P, R, tag, nullptr);
+      if (g < 0) continue;
+      uint64_t* dst = R.slots + (uint64_t)g * R.words + R.val_word;
+      for (int j = 0; j < R.naggs; ++j) accumulate(dst + j, R.agg_red[j], acc[(size_t)i * R.naggs + j]);
+    }
+  }
+}
+
 // ------------------------------------------------------- helper kernels --
 
 // Fills aggregation tables: tags empty, accumulators at their initial values.
@@ -1241,6 +1676,21 @@ cudaError_t launch_pipeline(const DevPipe& P, int grid, cudaStream_t stream) {
   if (e != cudaSuccess) return e;
   pipeline_kernel<<<grid, kThreads, P.smem_bytes, stream>>>(P);
   return cudaGetLastError();
+}
+
+cudaError_t launch_row(const DevPipe& P, int grid, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, P.smem_bytes);
+  if (e != cudaSuccess) return e;
+  row_kernel<<<grid, kThreads, P.smem_bytes, stream>>>(P);
+  return cudaGetLastError();
+}
+
+int row_occupancy(int smem_bytes) {
+  int blocks = 0;
+  if (cudaFuncSetAttribute(row_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes) != cudaSuccess)
+    return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, row_kernel, kThreads, smem_bytes);
+  return blocks;
 }
 
 int pipeline_occupancy(int smem_bytes) {

@@ -26,6 +26,8 @@
 namespace dq {
 cudaError_t launch_pipeline(const DevPipe& P, int grid, cudaStream_t stream);
 int pipeline_occupancy(int smem_bytes);
+cudaError_t launch_row(const DevPipe& P, int grid, cudaStream_t stream);
+int row_occupancy(int smem_bytes);
 cudaError_t launch_agg_init(uint64_t* slots, uint64_t nslots, int words, int val_word, int naggs,
                             const int8_t* reds, cudaStream_t stream);
 size_t mm_scan_scratch_words(uint64_t n);
@@ -145,6 +147,7 @@ struct PipeRec {
   DevPipe dev{};
   int grid = 1;             // CTAs of a tile launch (at most one per tile)
   int grid_full = 1;        // persistent grid (SMs x resident CTAs)
+  bool row = false;         // runs on the row kernel
   int expand_op = -1;       // level-0 expansion op with deferral
   DevBuf pattern_buf, heavy_items, heavy_count, heavy_prefix;
   bool mm_count = false;    // sink is a multimap count: bucket scan follows
@@ -562,6 +565,11 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     break;
   }
 
+  // row kernel (on request) for pipelines without a multimap expansion
+  p.row = (ctx->cfg.flags & DQ_CFG_ROW_KERNEL) != 0;
+  for (int i = 0; i < d.nops; ++i)
+    if (d.ops[i].kind == DQ_OP_EXPAND) p.row = false;
+
   // shared-memory layout
   int base = 0;
   auto take = [&](int bytes) {
@@ -571,17 +579,27 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   };
   P.nstage = p.staged_cols ? 3 : 1;
   for (int l = 0; l < DQ_MAX_LEVELS; ++l) P.off_reg[l] = P.off_sel[l] = P.off_par[l] = P.off_match[l] = 0;
-  for (int l = 0; l < nlevels; ++l) {
-    P.off_reg[l] = take(reg_bytes[l]);
-    P.off_sel[l] = take(tile * 2);
-    if (l > 0) {
-      P.off_par[l] = take(tile * 2);
-      P.off_match[l] = take(tile * 4);
+  if (p.row) {
+    // the launch descriptor first (the row kernel copies it there), then one
+    // 8-byte register per thread for every computed value
+    base = (int)align_up(sizeof(DevPipe), 16);
+    int nreg = 0;
+    for (int s = 0; s < P.nslots; ++s)
+      if (P.slots[s].kind == DQ_SLOT_REG) P.slots[s].smem_off = nreg++;
+    P.off_reg[0] = take(std::max(nreg, 1) * kThreads * 8);
+  } else {
+    for (int l = 0; l < nlevels; ++l) {
+      P.off_reg[l] = take(reg_bytes[l]);
+      P.off_sel[l] = take(tile * 2);
+      if (l > 0) {
+        P.off_par[l] = take(tile * 2);
+        P.off_match[l] = take(tile * 4);
+      }
     }
+    P.off_exp = take(std::max(1, nlevels - 1) * 3 * tile * 4);
+    P.off_flags = take(tile);
+    P.off_stash = take(kMaxStash * 8);
   }
-  P.off_exp = take(std::max(1, nlevels - 1) * 3 * tile * 4);
-  P.off_flags = take(tile);
-  P.off_stash = take(kMaxStash * 8);
   for (int r = 0; r < P.nres; ++r) {
     DevRes& R = P.res[r];
     if (R.kind == DQ_RES_AGG && R.smem_slots > 0) {
@@ -599,7 +617,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     throw DqError(DQ_ERR_UNSUPPORTED, "pipeline needs more shared memory than a CTA has; lower tile_rows");
   P.off_stage = fixed;
   P.smem_bytes = fixed + P.nstage * P.stage_bytes;
-  int occ = pipeline_occupancy(P.smem_bytes);
+  int occ = p.row ? row_occupancy(P.smem_bytes) : pipeline_occupancy(P.smem_bytes);
   if (occ < 1) throw DqError(DQ_ERR_UNSUPPORTED, "pipeline kernel cannot be resident with this shared memory");
   int want = ctx->cfg.ctas_per_sm > 0 ? std::min(ctx->cfg.ctas_per_sm, occ) : occ;
   p.grid_full = ctx->sms * want;
@@ -655,7 +673,7 @@ int run_once(dq_plan* plan, cudaStream_t st) {
     p.dev.tile_counter = counters + 2 * i;
     DQ_CUDA(cudaEventRecord(plan->events[1 + 2 * i], st));
     if (p.expand_op >= 0) DQ_CUDA(cudaMemsetAsync(p.heavy_count.ptr, 0, 8, st));
-    DQ_CUDA(launch_pipeline(p.dev, p.grid, st));
+    DQ_CUDA(p.row ? launch_row(p.dev, p.grid, st) : launch_pipeline(p.dev, p.grid, st));
     ++launches;
     if (p.expand_op >= 0) {
       DQ_CUDA(launch_heavy_prefix(p.dev.heavy, (uint64_t)p.dev.exp_cap, st));

@@ -69,6 +69,8 @@ typedef struct {
 
 #define DQ_CFG_NO_TMA      1    /* stage tiles with plain loads instead of TMA */
 #define DQ_CFG_NO_GRAPH    2    /* do not capture CUDA graphs                  */
+#define DQ_CFG_ROW_KERNEL  4    /* run pipelines without a multimap expansion  */
+                                /* on the row-at-a-time kernel                 */
 
 /* ------------------------------------------------------------- contexts -- */
 int dq_init(const dq_config* cfg, dq_ctx** out);

@@ -154,3 +154,21 @@ def test_backend_drop_in(engine):
     b.compile("c0")
     res = b.execute(quiet=True)
     assert canonical_checksum(res.rows()) == golden("c0_s")["checksum"]
+
+
+@pytest.mark.parametrize("name,scale", [("c0", 0.001), ("c1", 0.001), ("c3", 0.0002)])
+def test_tile_kernel_matches_row_kernel(engine, name, scale):
+    """Pipelines without expansion can run on the row kernel; it must give
+    the same results as the default tile kernel."""
+    from dogqc_b200 import _lib as L
+    from dogqc_b200.engine import Engine
+    db, plan = _plan(name, scale)
+    want = canonical_rows(run_plan(db, plan)[1])
+    e = Engine(0, flags=L.CFG_ROW_KERNEL)
+    try:
+        res, _ = run_engine(e, db, plan)
+    finally:
+        e.close()
+    assert canonical_rows(res.rows()) == want
+    res2, _ = run_engine(engine, db, plan)
+    assert canonical_rows(res2.rows()) == want
