@@ -40,7 +40,7 @@ OPF_B_IMM, OPF_A_IMM = 1, 2
 RES_UNIQUE, RES_MULTI, RES_AGG, RES_OUTPUT = 1, 2, 3, 4
 SRC_TABLE, SRC_OUTPUT, SRC_AGG = 1, 2, 3
 TABLE_DEVICE_DATA = 1
-CFG_NO_TMA, CFG_NO_GRAPH, CFG_ROW_KERNEL = 1, 2, 4
+CFG_NO_TMA, CFG_NO_GRAPH, CFG_ROW_KERNEL, CFG_NO_JIT, CFG_OFFLINE = 1, 2, 4, 8, 16
 
 
 class dq_config(C.Structure):
@@ -131,6 +131,7 @@ EXPORTS = {
     "dq_plan_prepare": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_desc), C.POINTER(C.c_void_p)]),
     "dq_plan_execute": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dq_plan_free": (None, [C.c_void_p]),
+    "dq_plan_source": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
     "dq_plan_timing_get": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_timing)]),
     "dq_result_rows": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "dq_result_ncols": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),

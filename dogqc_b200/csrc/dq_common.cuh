@@ -1,0 +1,431 @@
+// Device helpers shared by the prebuilt pipeline kernels (dq_kernels.cu) and
+// the per-pipeline kernels generated at plan preparation (dq_jit.cu compiles
+// them with NVRTC and embeds this file as an in-memory header).  Keeping one
+// copy of the value semantics, hashing and table probing makes every kernel
+// of a plan agree on table layouts and results.
+//
+// Values are carried as canonical 64-bit words: sign-extended for signed C
+// types, zero-extended for unsigned ones, and every operation computes in the C
+// type the lowering assigned (usual arithmetic conversions, wrap-around).
+#pragma once
+#include "dq_device.h"
+
+namespace dq {
+
+constexpr long long kSpinLimit = 1ll << 28;  // bound of every device wait
+constexpr uint64_t kBusy = ~0ull - 1;        // aggregation slot being claimed
+constexpr unsigned kFull = 0xffffffffu;
+
+// ------------------------------------------------------------------ values --
+
+__device__ __forceinline__ uint64_t canon(uint64_t v, int t) {
+  switch (t) {
+    case DQ_I8: return (uint64_t)(int64_t)(int8_t)v;
+    case DQ_I32: return (uint64_t)(int64_t)(int32_t)v;
+    case DQ_U32: return (uint64_t)(uint32_t)v;
+    default: return v;
+  }
+}
+
+__device__ __forceinline__ bool is_signed(int t) { return t == DQ_I8 || t == DQ_I32 || t == DQ_I64; }
+
+__device__ __forceinline__ uint64_t ld(const uint8_t* p, int w) {
+  switch (w) {
+    case 1: return *p;
+    case 2: return *reinterpret_cast<const uint16_t*>(p);
+    case 4: return *reinterpret_cast<const uint32_t*>(p);
+    default: return *reinterpret_cast<const uint64_t*>(p);
+  }
+}
+
+__device__ __forceinline__ void st(uint8_t* p, int w, uint64_t v) {
+  switch (w) {
+    case 1: *p = (uint8_t)v; break;
+    case 2: *reinterpret_cast<uint16_t*>(p) = (uint16_t)v; break;
+    case 4: *reinterpret_cast<uint32_t*>(p) = (uint32_t)v; break;
+    default: *reinterpret_cast<uint64_t*>(p) = v; break;
+  }
+}
+
+// MurmurHash3 64-bit finaliser (Appleby), used for every hash table.
+__device__ __forceinline__ uint64_t fmix64(uint64_t k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdull;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ull;
+  k ^= k >> 33;
+  return k;
+}
+
+// Maps a 64-bit hash onto [0, cap) without a division (multiply-high range
+// reduction).
+__device__ __forceinline__ uint64_t reduce_range(uint64_t h, uint64_t cap) { return __umul64hi(h, cap); }
+
+__device__ __forceinline__ uint64_t arith(int sub, int t, uint64_t a, uint64_t b) {
+  a = canon(a, t);
+  b = canon(b, t);
+  uint64_t r = 0;
+  switch (sub) {
+    case DQ_ADD: r = a + b; break;
+    case DQ_SUB: r = a - b; break;
+    case DQ_MUL: r = a * b; break;
+    case DQ_DIV:
+    case DQ_MOD: {
+      if (b == 0) return 0;  // undefined in C; defined as 0 here
+      bool div = sub == DQ_DIV;
+      if (t == DQ_I32) {
+        int32_t x = (int32_t)a, y = (int32_t)b;
+        if (y == -1) r = div ? (uint64_t)(uint32_t)(0u - (uint32_t)x) : 0;
+        else r = (uint64_t)(uint32_t)(div ? x / y : x % y);
+      } else if (t == DQ_U32) {
+        uint32_t x = (uint32_t)a, y = (uint32_t)b;
+        r = div ? x / y : x % y;
+      } else if (t == DQ_I64) {
+        int64_t x = (int64_t)a, y = (int64_t)b;
+        if (y == -1) r = div ? 0ull - a : 0;
+        else r = (uint64_t)(div ? x / y : x % y);
+      } else {
+        r = div ? a / b : a % b;
+      }
+      break;
+    }
+  }
+  return canon(r, t);
+}
+
+__device__ __forceinline__ bool compare(int sub, int t, uint64_t a, uint64_t b) {
+  a = canon(a, t);
+  b = canon(b, t);
+  if (is_signed(t)) {
+    int64_t x = (int64_t)a, y = (int64_t)b;
+    switch (sub) {
+      case DQ_EQ: return x == y;
+      case DQ_NE: return x != y;
+      case DQ_LT: return x < y;
+      case DQ_LE: return x <= y;
+      case DQ_GT: return x > y;
+      default: return x >= y;
+    }
+  }
+  switch (sub) {
+    case DQ_EQ: return a == b;
+    case DQ_NE: return a != b;
+    case DQ_LT: return a < b;
+    case DQ_LE: return a <= b;
+    case DQ_GT: return a > b;
+    default: return a >= b;
+  }
+}
+
+// LIKE with the reference matcher's exact semantics (util.cuh:144-199):
+// prefix, then suffix, then infixes left to right; '_' matches any byte; reads
+// one past the end of the string or pattern see a zero byte.
+__device__ __noinline__ bool like_match(const uint8_t* s, int ls, const uint8_t* p, int lp) {
+  auto S = [&](int i) -> int { return (i >= 0 && i < ls) ? s[i] : 0; };
+  auto P = [&](int i) -> int { return (i >= 0 && i < lp) ? p[i] : 0; };
+  auto cmp = [](int c, int l) { return c == l || l == '_'; };
+  int l_in_start = 0, l_in_end = lp, s_in_start = 0, s_in_end = ls, l_pos = 0;
+  if (P(0) != '%') {
+    int s_pos = 0;
+    l_pos = 0;
+    while (l_pos < lp && s_pos < ls && P(l_pos) != '%') {
+      if (!cmp(S(s_pos), P(l_pos))) return false;
+      ++l_pos;
+      ++s_pos;
+    }
+    l_in_start = l_pos;
+    s_in_start = s_pos;
+  }
+  if (P(lp - 1) != '%') {
+    int s_pos = ls - 1;
+    l_pos = lp - 1;
+    while (l_pos >= 0 && s_pos >= 0 && P(l_pos) != '%') {
+      if (!cmp(S(s_pos), P(l_pos))) return false;
+      --l_pos;
+      --s_pos;
+    }
+    l_in_end = l_pos;
+    s_in_end = s_pos + 1;
+  }
+  if (l_in_start < l_in_end) {
+    l_pos = l_in_start + 1;
+    int s_pos = s_in_start;
+    while (s_pos < s_in_end && l_pos < l_in_end) {
+      int l_tr = l_pos, s_tr = s_pos;
+      while (cmp(S(s_tr), P(l_tr)) && s_tr < s_in_end) {
+        ++l_tr;
+        if (P(l_tr) == '%') {
+          ++l_tr;
+          l_pos = l_tr;
+          s_pos = s_tr;
+          break;
+        }
+        ++s_tr;
+      }
+      ++s_pos;
+    }
+  }
+  return l_pos >= l_in_end;
+}
+
+// String value of row g of a string column.
+__device__ __forceinline__ void str_at(const DevStr& d, int64_t g, const uint8_t*& ptr, int& len) {
+  if (d.width > 0) {
+    ptr = d.chars + g * d.width;
+    len = d.width;
+  } else {
+    uint64_t a = d.offsets[g], b = d.offsets[g + 1];
+    ptr = d.chars + a;
+    len = (int)(b - a);
+  }
+}
+
+__device__ __forceinline__ bool str_eq(const uint8_t* s, int ls, const uint8_t* p, int lp) {
+  bool eq = ls == lp;
+  for (int j = 0; eq && j < ls; ++j) eq = s[j] == p[j];
+  return eq;
+}
+
+// ------------------------------------------------------------ pipelines --
+
+__device__ __forceinline__ void set_status(const DevPipe& P, int32_t bits) { atomicOr(P.status, bits); }
+
+// Rows of the pipeline's source.  A temp table's row count is its cursor,
+// which an overflowing emit may have advanced past the capacity: the rows
+// beyond it were never written (the plan is re-run with a larger table).
+__device__ __forceinline__ int64_t source_rows(const DevPipe& P) {
+  if (!P.nrows_dev) return P.nrows;
+  uint64_t n = *P.nrows_dev;
+  if (P.source_res >= 0 && n > P.res[P.source_res].cap) n = P.res[P.source_res].cap;
+  return (int64_t)n;
+}
+
+// ------------------------------------------------------------- hashing --
+
+// Packed tag (exact key) or 63-bit hash tag for wide keys.
+__device__ __forceinline__ uint64_t key_tag(const DevRes& R, const uint64_t* k) {
+  if (R.packed) {
+    if (R.nkeys == 0) return 0;
+    if (R.nkeys == 1 && (R.key_ctype[0] == DQ_I64 || R.key_ctype[0] == DQ_U64)) return k[0];
+    uint64_t t = (uint32_t)k[0];
+    if (R.nkeys > 1) t |= (uint64_t)(uint32_t)k[1] << 32;
+    return t;
+  }
+  uint64_t h = 0x9e3779b97f4a7c15ull;
+  for (int i = 0; i < R.nkeys; ++i) h = fmix64(h ^ k[i]) + 0x632be59bd9b4e019ull * (i + 1);
+  return fmix64(h) & 0x7fffffffffffffffull;
+}
+
+__device__ __forceinline__ uint64_t multimap_hash(const uint64_t* k, int n) {
+  uint64_t h = 0x9e3779b97f4a7c15ull;
+  for (int i = 0; i < n; ++i) h = fmix64(h ^ k[i]) + 0x632be59bd9b4e019ull * (i + 1);
+  return fmix64(h);
+}
+
+// Unique join table: returns slot index or -1.
+__device__ __forceinline__ int64_t unique_find(const DevRes& R, uint64_t tag, const uint64_t* k) {
+  if (R.packed && tag == kEmpty) return R.slots[R.cap * R.words] == 0 ? (int64_t)R.cap : -1;
+  uint64_t idx = reduce_range(fmix64(tag), R.cap);
+  for (uint64_t n = 0; n < R.cap; ++n) {
+    const uint64_t* s = R.slots + idx * R.words;
+    uint64_t t = s[0];
+    if (t == kEmpty) return -1;
+    if (t == tag) {
+      bool eq = true;
+      if (!R.packed)
+        for (int i = 0; i < R.nkeys; ++i) eq &= s[R.key_word + i] == k[i];
+      if (eq) return (int64_t)idx;
+    }
+    idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+  }
+  return -1;
+}
+
+// Inserts the key; returns the slot to write the payload to, or -1 if the key
+// was present already (first insert wins) or the table is full.
+__device__ __forceinline__ int64_t unique_insert(const DevPipe& P, const DevRes& R, uint64_t tag,
+                                                 const uint64_t* k) {
+  if (R.packed && tag == kEmpty) {
+    uint64_t old = atomicCAS((unsigned long long*)(R.slots + R.cap * R.words), kEmpty, 0ull);
+    return old == kEmpty ? (int64_t)R.cap : -1;
+  }
+  uint64_t idx = reduce_range(fmix64(tag), R.cap);
+  for (uint64_t n = 0; n < R.cap; ++n) {
+    uint64_t* s = R.slots + idx * R.words;
+    uint64_t old = atomicCAS((unsigned long long*)s, kEmpty, tag);
+    if (old == kEmpty) {
+      if (!R.packed)
+        for (int i = 0; i < R.nkeys; ++i) s[R.key_word + i] = k[i];
+      return (int64_t)idx;
+    }
+    if (old == tag && R.packed) return -1;
+    idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+  }
+  set_status(P, kErrHtFull);
+  return -1;
+}
+
+// Aggregation table (global): find or claim the group's slot.
+__device__ __noinline__ int64_t agg_slot_global(const DevPipe& P, const DevRes& R, uint64_t tag,
+                                                const uint64_t* k) {
+  if (R.nkeys == 0) return 0;  // one group, always at slot 0
+  if (R.packed) {
+    if (tag == kEmpty) {
+      atomicCAS((unsigned long long*)(R.slots + R.cap * R.words), kEmpty, 0ull);
+      return (int64_t)R.cap;
+    }
+    uint64_t idx = reduce_range(fmix64(tag), R.cap);
+    for (uint64_t n = 0; n < R.cap; ++n) {
+      uint64_t* s = R.slots + idx * R.words;
+      uint64_t t = *(volatile uint64_t*)s;
+      if (t == tag) return (int64_t)idx;
+      if (t == kEmpty) {
+        uint64_t old = atomicCAS((unsigned long long*)s, kEmpty, tag);
+        if (old == kEmpty || old == tag) return (int64_t)idx;
+      }
+      idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+    }
+    set_status(P, kErrHtFull);
+    return -1;
+  }
+  // wide keys: claim with a busy marker, publish keys, then the tag
+  uint64_t idx = reduce_range(fmix64(tag), R.cap);
+  for (uint64_t n = 0; n < R.cap; ++n) {
+    uint64_t* s = R.slots + idx * R.words;
+    uint64_t t = *(volatile uint64_t*)s;
+    if (t == kEmpty) {
+      uint64_t old = atomicCAS((unsigned long long*)s, kEmpty, kBusy);
+      if (old == kEmpty) {
+        for (int i = 0; i < R.nkeys; ++i) s[R.key_word + i] = k[i];
+        __threadfence();
+        atomicExch((unsigned long long*)s, tag);
+        return (int64_t)idx;
+      }
+      t = old;
+    }
+    long long spins = 0;
+    while (t == kBusy && spins < kSpinLimit) {
+      t = *(volatile uint64_t*)s;
+      ++spins;
+    }
+    if (t == kBusy) {
+      set_status(P, kErrTimeout);
+      return -1;
+    }
+    if (t == tag) {
+      __threadfence();
+      bool eq = true;
+      for (int i = 0; i < R.nkeys; ++i) eq &= ((volatile uint64_t*)s)[R.key_word + i] == k[i];
+      if (eq) return (int64_t)idx;
+    }
+    idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+  }
+  set_status(P, kErrHtFull);
+  return -1;
+}
+
+// Merges v into a global accumulator.  COUNT accumulators add v (1 per row,
+// or a partial count when a CTA-local table is merged).
+__device__ __forceinline__ void accumulate(uint64_t* acc, int red, uint64_t v) {
+  switch (red) {
+    case DQ_RED_SUM: atomicAdd((unsigned long long*)acc, v); break;
+    case DQ_RED_COUNT: atomicAdd((unsigned long long*)acc, v); break;
+    case DQ_RED_MIN: atomicMin((unsigned long long*)acc, v); break;
+    case DQ_RED_MAX: atomicMax((unsigned long long*)acc, v); break;
+  }
+}
+
+__device__ __forceinline__ uint64_t red_init(int red) { return red == DQ_RED_MIN ? ~0ull : 0ull; }
+
+// Combines two partial aggregates (on the canonical 64-bit words).
+__device__ __forceinline__ uint64_t red_combine(int red, uint64_t a, uint64_t b) {
+  switch (red) {
+    case DQ_RED_MIN: return a < b ? a : b;
+    case DQ_RED_MAX: return a > b ? a : b;
+    default: return a + b;
+  }
+}
+
+// ------------------------------------------------------- shared memory --
+
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t s_cas64(uint32_t a, uint64_t cmp, uint64_t val) {
+  uint64_t old;
+  asm volatile("atom.shared.cas.b64 %0, [%1], %2, %3;" : "=l"(old) : "r"(a), "l"(cmp), "l"(val) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void s_merge(uint32_t a, int red, uint64_t v) {
+  switch (red) {
+    case DQ_RED_SUM:
+    case DQ_RED_COUNT: asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); break;
+    case DQ_RED_MIN: asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); break;
+    case DQ_RED_MAX: asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); break;
+  }
+}
+
+// Exact reduction of one aggregate over the lanes in `in` (all 32 lanes call
+// it).  64-bit sums are split into 22-bit limbs so the 32-bit warp reductions
+// cannot overflow; min/max reduce the high words, then the low words of the
+// lanes holding the extreme high word.
+__device__ __forceinline__ uint64_t warp_reduce(int red, bool in, uint64_t v, unsigned grp) {
+  switch (red) {
+    case DQ_RED_COUNT:
+      return (uint64_t)__popc(grp);
+    case DQ_RED_SUM: {
+      uint32_t l0 = __reduce_add_sync(kFull, in ? (uint32_t)(v & 0x3fffff) : 0u);
+      uint32_t l1 = __reduce_add_sync(kFull, in ? (uint32_t)((v >> 22) & 0x3fffff) : 0u);
+      uint32_t l2 = __reduce_add_sync(kFull, in ? (uint32_t)(v >> 44) : 0u);
+      return (uint64_t)l0 + ((uint64_t)l1 << 22) + ((uint64_t)l2 << 44);
+    }
+    case DQ_RED_MIN: {
+      uint32_t hi = __reduce_min_sync(kFull, in ? (uint32_t)(v >> 32) : 0xffffffffu);
+      uint32_t lo = __reduce_min_sync(kFull, (in && (uint32_t)(v >> 32) == hi) ? (uint32_t)v : 0xffffffffu);
+      return ((uint64_t)hi << 32) | lo;
+    }
+    default: {
+      uint32_t hi = __reduce_max_sync(kFull, in ? (uint32_t)(v >> 32) : 0u);
+      uint32_t lo = __reduce_max_sync(kFull, (in && (uint32_t)(v >> 32) == hi) ? (uint32_t)v : 0u);
+      return ((uint64_t)hi << 32) | lo;
+    }
+  }
+}
+
+// Warp reduction of a partial aggregate every lane holds (all lanes take part).
+__device__ __forceinline__ uint64_t warp_reduce_all(int red, uint64_t v) {
+  if (red == DQ_RED_COUNT) red = DQ_RED_SUM;
+  return warp_reduce(red, true, v, kFull);
+}
+
+// CTA-local aggregation table through shared-memory atomics: ns slots plus
+// one for the all-ones packed key; returns the slot or -1 when full.
+__device__ __forceinline__ int local_group_slot(uint64_t* tags, int ns, uint64_t tag, int nkeys) {
+  if (nkeys == 0) {
+    tags[0] = 0;
+    return 0;
+  }
+  if (tag == kEmpty) {
+    s_cas64(saddr(&tags[ns]), kEmpty, 0ull);
+    return ns;
+  }
+  uint32_t idx = (uint32_t)reduce_range(fmix64(tag), (uint64_t)ns);
+  for (int n = 0; n < ns; ++n) {
+    uint64_t t = ((volatile uint64_t*)tags)[idx];
+    if (t == tag) return (int)idx;
+    if (t == kEmpty) {
+      uint64_t old = s_cas64(saddr(&tags[idx]), kEmpty, tag);
+      if (old == kEmpty || old == tag) return (int)idx;
+    }
+    idx = (idx + 1 == (uint32_t)ns) ? 0 : idx + 1;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
+  uint32_t lo = __shfl_sync(kFull, (uint32_t)v, src);
+  uint32_t hi = __shfl_sync(kFull, (uint32_t)(v >> 32), src);
+  return ((uint64_t)hi << 32) | lo;
+}
+
+}  // namespace dq

@@ -1,0 +1,892 @@
+// Per-pipeline kernel generator and NVRTC compiler (host code).
+//
+// A generated pipeline kernel processes one row per lane and keeps every
+// value in registers: the ops of the pipeline become straight-line code, so
+// the per-row cost is the work of the ops themselves, not the interpretation
+// of an op list.  The structure of every kernel:
+//
+//   * a grid-stride loop over the source, `rows_per_thread` rows per thread
+//     per step (row = base + u * 256 + thread), with the staged columns of all
+//     of them loaded before any is processed (coalesced, independent loads);
+//   * filters and probes clear a lane's `act` flag; when no lane of a warp is
+//     active the warp skips to its next row;
+//   * a multimap probe (EXPAND) is distributed over the warp, the reference's
+//     warp-level push-down expansion (dogqc/hashJoins.py:599-681): the lanes'
+//     match ranges are scanned, then the warp walks the concatenated
+//     (row, match) pairs 32 at a time, each lane taking one pair and the
+//     parent row's values by shuffle.  Ranges longer than a threshold are
+//     handed to a second kernel in which whole CTAs split them;
+//   * aggregation is pre-combined where the group count allows: in registers
+//     for a single group, in a CTA-local shared-memory table whose
+//     accumulators are replicated 16 ways (lane % 16) so that lanes of one warp
+//     do not collide on hot groups, and in the global table otherwise;
+//   * emits reserve output rows once per warp (ballot + one atomic).
+//
+// Table layouts, hashing and value semantics are the shared helpers of
+// dq_common.cuh, embedded with the other device headers as in-memory headers.
+#include "dq_jit.h"
+
+#include <nvrtc.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "dq_jit_embed.inc"  // kEmbedCount, kEmbedNames[], kEmbedText[] (written by build.py)
+
+namespace dq {
+namespace jit {
+namespace {
+
+constexpr int kCopies = 16;                 // accumulator replicas of the striped local table
+constexpr int kStripedMax = 48 * 1024;      // shared memory the striped table may take
+constexpr int kBlock = kThreads;
+
+const char* ct_name(int t) {
+  switch (t) {
+    case DQ_I8: return "DQ_I8";
+    case DQ_I32: return "DQ_I32";
+    case DQ_U32: return "DQ_U32";
+    case DQ_I64: return "DQ_I64";
+    default: return "DQ_U64";
+  }
+}
+
+const char* red_name(int r) {
+  switch (r) {
+    case DQ_RED_SUM: return "DQ_RED_SUM";
+    case DQ_RED_COUNT: return "DQ_RED_COUNT";
+    case DQ_RED_MIN: return "DQ_RED_MIN";
+    default: return "DQ_RED_MAX";
+  }
+}
+
+const char* arith_name(int s) {
+  switch (s) {
+    case DQ_ADD: return "DQ_ADD";
+    case DQ_SUB: return "DQ_SUB";
+    case DQ_MUL: return "DQ_MUL";
+    case DQ_DIV: return "DQ_DIV";
+    default: return "DQ_MOD";
+  }
+}
+
+const char* cmp_name(int s) {
+  switch (s) {
+    case DQ_EQ: return "DQ_EQ";
+    case DQ_NE: return "DQ_NE";
+    case DQ_LT: return "DQ_LT";
+    case DQ_LE: return "DQ_LE";
+    case DQ_GT: return "DQ_GT";
+    default: return "DQ_GE";
+  }
+}
+
+const char* uint_type(int w) {
+  switch (w) {
+    case 1: return "uint8_t";
+    case 2: return "uint16_t";
+    case 4: return "uint32_t";
+    default: return "uint64_t";
+  }
+}
+
+std::string lit(uint64_t v) {
+  char b[40];
+  snprintf(b, sizeof b, "0x%llxull", (unsigned long long)v);
+  return b;
+}
+
+std::string num(long long v) { return std::to_string(v); }
+
+// Slots an op reads (same rule as the runtime's validation).
+void op_reads(const DevPipe& P, const dq_op& op, std::vector<int>& out) {
+  auto add = [&](int s) {
+    if (s >= 0) out.push_back(s);
+  };
+  auto add_list = [&](int list, int n) {
+    for (int i = 0; i < n; ++i) add(P.lists[list + i]);
+  };
+  switch (op.kind) {
+    case DQ_OP_ARITH:
+    case DQ_OP_CMP:
+    case DQ_OP_CAST:
+      if (!(op.flags & DQ_OPF_A_IMM)) add(op.a);
+      if (op.kind != DQ_OP_CAST && !(op.flags & DQ_OPF_B_IMM)) add(op.b);
+      break;
+    case DQ_OP_LOGIC:
+      add(op.a);
+      if (op.sub != DQ_NOT) add(op.b);
+      break;
+    case DQ_OP_SELECT:
+      add(op.a);
+      if (!(op.flags & DQ_OPF_B_IMM)) add(op.b);
+      add(op.c >= 0 ? op.c : op.dst);
+      break;
+    case DQ_OP_LIKE:
+    case DQ_OP_STREQ:
+    case DQ_OP_FILTER:
+      add(op.a);
+      break;
+    case DQ_OP_PROBE:
+    case DQ_OP_EXPAND:
+    case DQ_OP_MM_COUNT:
+      add_list(op.list, op.nlist);
+      if (op.kind == DQ_OP_EXPAND) add_list(op.list2, op.nlist2);
+      break;
+    case DQ_OP_AGG:
+    case DQ_OP_BUILD:
+    case DQ_OP_MM_SCATTER:
+      add_list(op.list, op.nlist);
+      add_list(op.list2, op.nlist2);
+      break;
+    case DQ_OP_EMIT:
+      add_list(op.list, op.nlist);
+      break;
+  }
+}
+
+enum AggMode { AGG_NONE, AGG_REGS, AGG_STRIPED, AGG_LOCAL, AGG_GLOBAL };
+
+struct Gen {
+  const DevPipe& P;
+  int expand_op;
+  std::string o;
+  int ind = 0;
+  int uid = 0;
+  std::vector<std::string> var;  // slot -> C variable holding its canonical value
+  std::string row;               // level-0 row index of the current lane
+  AggMode agg = AGG_NONE;
+  int agg_res = -1;
+  int ns = 0;                    // local table slots (without the all-ones slot)
+  int copies = 1;
+  int U = 1;
+  int smem = 0;
+
+  Gen(const DevPipe& p, int e) : P(p), expand_op(e), var(p.nslots) {}
+
+  void L(const std::string& s) {
+    o.append((size_t)ind * 2, ' ');
+    o += s;
+    o += '\n';
+  }
+  std::string fresh(const char* b) { return std::string(b) + num(uid++); }
+  const DevSlot& slot(int s) const { return P.slots[s]; }
+  std::string V(int s) const {
+    if (s < 0 || s >= P.nslots || var[s].empty()) throw Error("generated code reads an undefined slot " + num(s));
+    return var[s];
+  }
+  std::string res(int r) const { return "P.res[" + num(r) + "]"; }
+  std::string operand(const dq_op& op, int which) const {
+    if (which == 0) return (op.flags & DQ_OPF_A_IMM) ? lit((uint64_t)op.imm) : V(op.a);
+    return (op.flags & DQ_OPF_B_IMM) ? lit((uint64_t)op.imm) : V(op.b);
+  }
+  std::string assign(int dst, const std::string& expr, int op_ctype) const {
+    return V(dst) + " = canon(canon(" + expr + ", " + ct_name(op_ctype) + "), " + ct_name(slot(dst).ctype) + ");";
+  }
+
+  // keys of a resource from a slot list, canonicalised to the key types
+  std::string keys(const dq_op& op, int r, int list, int n) {
+    std::string k = fresh("kk");
+    L("uint64_t " + k + "[" + num(std::max(n, 1)) + "];");
+    for (int i = 0; i < n; ++i)
+      L(k + "[" + num(i) + "] = canon(" + V(P.lists[list + i]) + ", " + ct_name(P.res[r].key_ctype[i]) + ");");
+    (void)op;
+    return k;
+  }
+
+  void declare_regs(int level) {
+    for (int s = 0; s < P.nslots; ++s)
+      if (slot(s).kind == DQ_SLOT_REG && slot(s).level == level) {
+        var[s] = "v" + num(s);
+        L("uint64_t " + var[s] + " = 0;");
+      }
+  }
+
+  void skip_if_idle(const std::string& act, const std::string& exit) {
+    L("if (!__any_sync(kFull, " + act + ")) " + exit);
+  }
+
+  // ---------------------------------------------------------------- ops --
+  void ops_from(int k, int level, const std::string& act, const std::string& exit) {
+    for (; k < P.nops; ++k) {
+      const dq_op& op = P.ops[k];
+      switch (op.kind) {
+        case DQ_OP_ARITH:
+          L(assign(op.dst, std::string("arith(") + arith_name(op.sub) + ", " + ct_name(op.ctype) + ", " +
+                               operand(op, 0) + ", " + operand(op, 1) + ")", op.ctype));
+          break;
+        case DQ_OP_CMP:
+          L(assign(op.dst, std::string("(uint64_t)compare(") + cmp_name(op.sub) + ", " + ct_name(op.ctype) + ", " +
+                               operand(op, 0) + ", " + operand(op, 1) + ")", DQ_U64));
+          break;
+        case DQ_OP_LOGIC:
+          if (op.sub == DQ_NOT) L(assign(op.dst, "(uint64_t)(" + V(op.a) + " == 0ull)", DQ_U64));
+          else
+            L(assign(op.dst, "(uint64_t)(" + V(op.a) + (op.sub == DQ_AND ? " != 0ull && " : " != 0ull || ") +
+                                 V(op.b) + " != 0ull)", DQ_U64));
+          break;
+        case DQ_OP_CAST:
+          L(assign(op.dst, operand(op, 0), op.ctype));
+          break;
+        case DQ_OP_SELECT: {
+          std::string prev = V(op.c >= 0 ? op.c : op.dst);
+          L(assign(op.dst, "(" + V(op.a) + " ? " + operand(op, 1) + " : " + prev + ")", op.ctype));
+          break;
+        }
+        case DQ_OP_LIKE:
+        case DQ_OP_STREQ: {
+          const DevSlot& sl = slot(op.a);
+          if (sl.kind != DQ_SLOT_STR) throw Error("string op on a non-string slot");
+          L(V(op.dst) + " = 0;");
+          L("if (" + act + ") {");
+          ++ind;
+          L("const uint8_t* sp_; int sn_;");
+          L("str_at(P.strs[" + num(sl.src) + "], " + row + ", sp_, sn_);");
+          std::string pat = "P.patterns + P.pat_off[" + num(op.res) + "]";
+          std::string plen = "P.pat_off[" + num(op.res + 1) + "] - P.pat_off[" + num(op.res) + "]";
+          L(V(op.dst) + std::string(" = (uint64_t)") + (op.kind == DQ_OP_LIKE ? "like_match" : "str_eq") +
+            "(sp_, sn_, " + pat + ", " + plen + ");");
+          --ind;
+          L("}");
+          break;
+        }
+        case DQ_OP_FILTER:
+          L(act + " = " + act + " && (" + V(op.a) + " != 0ull);");
+          skip_if_idle(act, exit);
+          break;
+        case DQ_OP_PROBE:
+          probe(op, act);
+          skip_if_idle(act, exit);
+          break;
+        case DQ_OP_EXPAND:
+          expand(k, level, act);
+          return;
+        case DQ_OP_AGG:
+          sink_agg(op, act);
+          return;
+        case DQ_OP_BUILD:
+          sink_build(op, act);
+          return;
+        case DQ_OP_MM_COUNT:
+        case DQ_OP_MM_SCATTER:
+          sink_mm(op, act);
+          return;
+        case DQ_OP_EMIT:
+          sink_emit(op, act);
+          return;
+        default:
+          throw Error("op kind " + num(op.kind) + " has no generated form");
+      }
+    }
+  }
+
+  void probe(const dq_op& op, const std::string& act) {
+    const int r = op.res;
+    const DevRes& R = P.res[r];
+    std::string s = fresh("ps");
+    L("int64_t " + s + " = -1;");
+    L("if (" + act + ") {");
+    ++ind;
+    std::string k = keys(op, r, op.list, op.nlist);
+    L(s + " = unique_find(" + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
+    if (op.sub == DQ_JOIN_INNER && op.nlist2 > 0) {
+      L("if (" + s + " >= 0) {");
+      ++ind;
+      L("const uint64_t* pay_ = " + res(r) + ".slots + (uint64_t)" + s + " * " + num(R.words) + " + " +
+        num(R.val_word) + ";");
+      for (int j = 0; j < op.nlist2; ++j) {
+        int d = P.lists[op.list2 + j];
+        if (d >= 0) L(V(d) + " = canon(pay_[" + num(j) + "], " + ct_name(slot(d).ctype) + ");");
+      }
+      --ind;
+      L("}");
+    }
+    --ind;
+    L("}");
+    if (op.sub == DQ_JOIN_ANTI) L(act + " = " + act + " && " + s + " < 0;");
+    else L(act + " = " + act + " && " + s + " >= 0;");
+  }
+
+  // live values of parent levels that ops k.. read
+  std::vector<int> live_after(int k, int level) {
+    std::vector<int> reads;
+    for (int j = k; j < P.nops; ++j) op_reads(P, P.ops[j], reads);
+    std::vector<int> live;
+    for (int s : reads) {
+      if (slot(s).level > level || slot(s).kind == DQ_SLOT_STR) continue;
+      if (std::find(live.begin(), live.end(), s) == live.end()) live.push_back(s);
+    }
+    std::sort(live.begin(), live.end());
+    return live;
+  }
+
+  bool reads_strings_after(int k) {
+    std::vector<int> reads;
+    for (int j = k; j < P.nops; ++j) op_reads(P, P.ops[j], reads);
+    for (int s : reads)
+      if (slot(s).kind == DQ_SLOT_STR) return true;
+    return false;
+  }
+
+  // gathers of level `lv` (the key columns first), key check, rest of the ops
+  void pairs(int k, int lv, const std::string& a, const std::string& m, const std::string& exit) {
+    const dq_op& op = P.ops[k];
+    declare_regs(lv);
+    auto gather = [&](int s) {
+      const DevSlot& g = slot(s);
+      var[s] = "v" + num(s) + "_" + num(uid++);
+      L("const uint64_t " + var[s] + " = " + a + " ? canon(ld(" + res(g.res) + ".pay[" + num(g.src) + "] + (uint64_t)" + m +
+        " * " + num(g.width) + ", " + num(g.width) + "), " + ct_name(g.ctype) + ") : 0ull;");
+    };
+    for (int q = 0; q < op.nlist2; ++q) {
+      int s = P.lists[op.list2 + q];
+      if (s >= 0 && slot(s).kind == DQ_SLOT_GATHER && slot(s).level == lv) gather(s);
+    }
+    for (int q = 0; q < op.nlist; ++q) {
+      int t = P.res[op.res].key_ctype[q];
+      L(a + " = " + a + " && canon(" + V(P.lists[op.list + q]) + ", " + ct_name(t) + ") == canon(" +
+        V(P.lists[op.list2 + q]) + ", " + ct_name(t) + ");");
+    }
+    skip_if_idle(a, exit);
+    for (int s = 0; s < P.nslots; ++s)
+      if (slot(s).kind == DQ_SLOT_GATHER && slot(s).level == lv && var[s].empty()) gather(s);
+    ops_from(k + 1, lv, a, exit);
+  }
+
+  void expand(int k, int level, const std::string& act) {
+    const dq_op& op = P.ops[k];
+    const int r = op.res;
+    const std::string id = num(uid++);
+    const std::string eo = "eo" + id, ec = "ec" + id, ei = "ei" + id, et = "et" + id, eb = "eb" + id,
+                      q = "eq" + id, sl = "es" + id, m = "em" + id, a = "ea" + id;
+    L("{");
+    ++ind;
+    L("uint32_t " + eo + " = 0u, " + ec + " = 0u;");
+    L("if (" + act + ") {");
+    ++ind;
+    std::string kk = keys(op, r, op.list, op.nlist);
+    L("const uint64_t b_ = reduce_range(multimap_hash(" + kk + ", " + num(op.nlist) + "), " + res(r) + ".cap);");
+    L(ec + " = " + res(r) + ".counts[b_];");
+    L(eo + " = " + ec + " ? " + res(r) + ".offsets[b_] : 0u;");
+    if (k == expand_op && level == 0) {
+      L("if (" + ec + " > P.heavy.threshold) {");
+      ++ind;
+      L("const uint32_t hs_ = atomicAdd(P.heavy.count, 1u);");
+      L("if (hs_ < P.heavy.cap) {");
+      ++ind;
+      L("uint64_t* it_ = P.heavy.items + (size_t)hs_ * P.heavy.words;");
+      L("it_[0] = " + eo + ";");
+      L("it_[1] = " + ec + ";");
+      for (int s = 0; s < P.nslots; ++s)
+        if (slot(s).stash >= 0) L("it_[" + num(2 + slot(s).stash) + "] = " + V(s) + ";");
+      L(ec + " = 0u;");
+      --ind;
+      L("}");
+      --ind;
+      L("}");
+    }
+    --ind;
+    L("}");
+    L("uint32_t " + ei + " = " + ec + ";");
+    L("#pragma unroll");
+    L("for (int d_ = 1; d_ < 32; d_ <<= 1) {");
+    L("  const uint32_t t_ = __shfl_up_sync(kFull, " + ei + ", d_);");
+    L("  if (lane >= d_) " + ei + " += t_;");
+    L("}");
+    L("const uint32_t " + et + " = __shfl_sync(kFull, " + ei + ", 31);");
+    L("for (uint32_t " + eb + " = 0; " + eb + " < " + et + "; " + eb + " += 32u) {");
+    ++ind;
+    L("const uint32_t " + q + " = " + eb + " + (uint32_t)lane;");
+    L("int " + sl + " = 0;");
+    L("#pragma unroll");
+    L("for (int s_ = 16; s_ > 0; s_ >>= 1)");
+    L("  if (__shfl_sync(kFull, " + ei + ", " + sl + " + s_ - 1) <= " + q + ") " + sl + " += s_;");
+    L("const uint32_t " + m + " = __shfl_sync(kFull, " + eo + ", " + sl + ") + (" + q + " - (__shfl_sync(kFull, " +
+      ei + ", " + sl + ") - __shfl_sync(kFull, " + ec + ", " + sl + ")));");
+    L("bool " + a + " = " + q + " < " + et + ";");
+    for (int s : live_after(k, level)) {
+      std::string nv = "v" + num(s) + "_" + num(uid++);
+      L("uint64_t " + nv + " = shfl64(" + V(s) + ", " + sl + ");");
+      var[s] = nv;
+    }
+    if (reads_strings_after(k + 1)) {
+      std::string nr = fresh("row");
+      L("const int64_t " + nr + " = (int64_t)shfl64((uint64_t)" + row + ", " + sl + ");");
+      row = nr;
+    }
+    pairs(k, level + 1, a, m, "continue;");
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+  }
+
+  // ---------------------------------------------------------------- sinks --
+  void sink_agg(const dq_op& op, const std::string& act) {
+    const int r = op.res;
+    const DevRes& R = P.res[r];
+    std::vector<std::string> vals;
+    for (int j = 0; j < R.naggs; ++j) {
+      int src = P.lists[op.list2 + j];
+      vals.push_back(R.agg_red[j] == DQ_RED_COUNT || src < 0 ? std::string("1ull") : V(src));
+    }
+    if (agg == AGG_REGS) {
+      L("if (" + act + ") {");
+      for (int j = 0; j < R.naggs; ++j)
+        L("  acc" + num(j) + " = red_combine(" + red_name(R.agg_red[j]) + ", acc" + num(j) + ", " + vals[j] + ");");
+      L("}");
+      return;
+    }
+    L("if (" + act + ") {");
+    ++ind;
+    std::string k = keys(op, r, op.list, op.nlist);
+    L("const uint64_t tag_ = key_tag(" + res(r) + ", " + k + ");");
+    auto global = [&]() {
+      L("const int64_t g_ = agg_slot_global(P, " + res(r) + ", tag_, " + k + ");");
+      L("if (g_ >= 0) {");
+      ++ind;
+      L("uint64_t* a_ = " + res(r) + ".slots + (uint64_t)g_ * " + num(R.words) + " + " + num(R.val_word) + ";");
+      for (int j = 0; j < R.naggs; ++j)
+        L("accumulate(a_ + " + num(j) + ", " + red_name(R.agg_red[j]) + ", " + vals[j] + ");");
+      --ind;
+      L("}");
+    };
+    if (agg == AGG_GLOBAL) {
+      global();
+    } else {
+      L("const int s_ = local_group_slot(ltags, " + num(ns) + ", tag_, " + num(R.nkeys) + ");");
+      L("if (s_ >= 0) {");
+      ++ind;
+      for (int j = 0; j < R.naggs; ++j) {
+        std::string idx = agg == AGG_STRIPED
+                              ? "((s_ * " + num(R.naggs) + " + " + num(j) + ") * " + num(kCopies) + " + (lane & " +
+                                    num(kCopies - 1) + "))"
+                              : "(s_ * " + num(R.naggs) + " + " + num(j) + ")";
+        L("s_merge(saddr(lacc + " + idx + "), " + red_name(R.agg_red[j]) + ", " + vals[j] + ");");
+      }
+      --ind;
+      L("} else {");
+      ++ind;
+      global();
+      --ind;
+      L("}");
+    }
+    --ind;
+    L("}");
+  }
+
+  void sink_build(const dq_op& op, const std::string& act) {
+    const int r = op.res;
+    const DevRes& R = P.res[r];
+    L("if (" + act + ") {");
+    ++ind;
+    std::string k = keys(op, r, op.list, op.nlist);
+    L("const int64_t s_ = unique_insert(P, " + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
+    if (op.nlist2 > 0) {
+      L("if (s_ >= 0) {");
+      ++ind;
+      L("uint64_t* pay_ = " + res(r) + ".slots + (uint64_t)s_ * " + num(R.words) + " + " + num(R.val_word) + ";");
+      for (int j = 0; j < op.nlist2; ++j) L("pay_[" + num(j) + "] = " + V(P.lists[op.list2 + j]) + ";");
+      --ind;
+      L("}");
+    }
+    --ind;
+    L("}");
+  }
+
+  void sink_mm(const dq_op& op, const std::string& act) {
+    const int r = op.res;
+    const DevRes& R = P.res[r];
+    L("if (" + act + ") {");
+    ++ind;
+    std::string k = keys(op, r, op.list, op.nlist);
+    L("const uint64_t b_ = reduce_range(multimap_hash(" + k + ", " + num(op.nlist) + "), " + res(r) + ".cap);");
+    if (op.kind == DQ_OP_MM_COUNT) {
+      L("atomicAdd(&" + res(r) + ".counts[b_], 1u);");
+    } else {
+      L("const uint32_t pos_ = " + res(r) + ".offsets[b_] + atomicAdd(&" + res(r) + ".counts[b_], 1u);");
+      for (int j = 0; j < op.nlist2; ++j) {
+        int w = R.pay_width[j];
+        L("st(" + res(r) + ".pay[" + num(j) + "] + (size_t)pos_ * " + num(w) + ", " + num(w) + ", " +
+          V(P.lists[op.list2 + j]) + ");");
+      }
+    }
+    --ind;
+    L("}");
+  }
+
+  void sink_emit(const dq_op& op, const std::string& act) {
+    const int r = op.res;
+    const DevRes& R = P.res[r];
+    L("{");
+    ++ind;
+    L("const unsigned am_ = __ballot_sync(kFull, " + act + ");");
+    L("if (am_) {");
+    ++ind;
+    L("const int ld_ = __ffs(am_) - 1;");
+    L("unsigned long long b_ = 0;");
+    L("if (lane == ld_) b_ = atomicAdd((unsigned long long*)" + res(r) + ".cursor, (unsigned long long)__popc(am_));");
+    L("b_ = __shfl_sync(kFull, b_, ld_);");
+    L("if (" + act + ") {");
+    ++ind;
+    L("const uint64_t pos_ = b_ + __popc(am_ & ((1u << lane) - 1u));");
+    L("if (pos_ >= " + res(r) + ".cap) {");
+    L("  set_status(P, kErrOverflow);");
+    L("} else {");
+    ++ind;
+    for (int j = 0; j < op.nlist; ++j) {
+      int w = R.pay_width[j];
+      L("st(" + res(r) + ".pay[" + num(j) + "] + pos_ * " + num(w) + ", " + num(w) + ", " + V(P.lists[op.list + j]) +
+        ");");
+    }
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+  }
+
+  // --------------------------------------------------------- aggregation --
+  void choose_agg() {
+    const dq_op& sink = P.ops[P.nops - 1];
+    if (sink.kind != DQ_OP_AGG) return;
+    agg_res = sink.res;
+    const DevRes& R = P.res[agg_res];
+    if (R.nkeys == 0) {
+      agg = AGG_REGS;
+      return;
+    }
+    ns = R.smem_slots;
+    if (ns <= 0 || !R.packed) {
+      agg = AGG_GLOBAL;
+      ns = 0;
+      return;
+    }
+    const int tags = (ns + 1) * 8;
+    const int striped = (ns + 1) * R.naggs * 8 * kCopies;
+    if (tags + striped <= kStripedMax) {
+      agg = AGG_STRIPED;
+      copies = kCopies;
+    } else {
+      agg = AGG_LOCAL;
+      copies = 1;
+    }
+    smem = tags + (ns + 1) * R.naggs * 8 * copies;
+  }
+
+  uint64_t min_mask() const {
+    const DevRes& R = P.res[agg_res];
+    uint64_t mask = 0;
+    for (int j = 0; j < R.naggs; ++j)
+      if (R.agg_red[j] == DQ_RED_MIN) mask |= 1ull << j;
+    return mask;
+  }
+
+  void agg_init() {
+    if (agg == AGG_NONE || agg == AGG_GLOBAL) return;
+    const DevRes& R = P.res[agg_res];
+    if (agg == AGG_REGS) {
+      for (int j = 0; j < R.naggs; ++j)
+        L("uint64_t acc" + num(j) + " = red_init(" + red_name(R.agg_red[j]) + ");");
+      return;
+    }
+    L("uint64_t* ltags = reinterpret_cast<uint64_t*>(smem);");
+    L("uint64_t* lacc = ltags + " + num(ns + 1) + ";");
+    L("for (int i = tid; i <= " + num(ns) + "; i += " + num(kBlock) + ") ltags[i] = kEmpty;");
+    L("for (int i = tid; i < " + num((ns + 1) * R.naggs * copies) + "; i += " + num(kBlock) + ")");
+    L("  lacc[i] = ((" + lit(min_mask()) + " >> ((i / " + num(copies) + ") % " + num(R.naggs) +
+      ")) & 1ull) ? ~0ull : 0ull;");
+    L("__syncthreads();");
+  }
+
+  void agg_flush() {
+    if (agg == AGG_NONE || agg == AGG_GLOBAL) return;
+    const DevRes& R = P.res[agg_res];
+    const std::string rr = res(agg_res);
+    if (agg == AGG_REGS) {
+      for (int j = 0; j < R.naggs; ++j) {
+        L("{");
+        L("  const uint64_t w_ = warp_reduce_all(" + std::string(red_name(R.agg_red[j])) + ", acc" + num(j) + ");");
+        L("  if (lane == 0) accumulate(" + rr + ".slots + " + num(R.val_word + j) + ", " + red_name(R.agg_red[j]) +
+          ", w_);");
+        L("}");
+      }
+      return;
+    }
+    uint64_t packed_reds = 0;
+    for (int j = 0; j < R.naggs; ++j) packed_reds |= (uint64_t)(R.agg_red[j] & 15) << (4 * j);
+    L("__syncthreads();");
+    L("for (int i = tid; i < " + num((ns + 1) * R.naggs) + "; i += " + num(kBlock) + ") {");
+    ++ind;
+    L("const int s_ = i / " + num(R.naggs) + ", j_ = i % " + num(R.naggs) + ";");
+    L("uint64_t tg_ = ltags[s_];");
+    L("if (tg_ == kEmpty) continue;");
+    L("if (s_ == " + num(ns) + ") tg_ = kEmpty;  // the all-ones key");
+    L("const int red_ = (int)((" + lit(packed_reds) + " >> (4 * j_)) & 15ull);");
+    L("uint64_t v_ = lacc[i * " + num(copies) + "];");
+    if (copies > 1) L("for (int c_ = 1; c_ < " + num(copies) + "; ++c_) v_ = red_combine(red_, v_, lacc[i * " +
+                      num(copies) + " + c_]);");
+    L("const int64_t g_ = agg_slot_global(P, " + rr + ", tg_, nullptr);");
+    L("if (g_ >= 0) accumulate(" + rr + ".slots + (uint64_t)g_ * " + num(R.words) + " + " + num(R.val_word) +
+      " + j_, red_, v_);");
+    --ind;
+    L("}");
+  }
+
+  void prologue(const char* name) {
+    L(std::string("extern \"C\" __global__ void __launch_bounds__(") + num(kBlock) + ") " + name +
+      "(const __grid_constant__ DevPipe P) {");
+    ++ind;
+    L("extern __shared__ __align__(16) uint8_t smem[];");
+    L("if (*(volatile int32_t*)P.status & (kErrHtFull | kErrTimeout)) return;");
+    L("const int tid = threadIdx.x, lane = tid & 31;");
+    L("(void)smem;");
+    L("(void)lane;");
+    agg_init();
+  }
+
+  void epilogue() {
+    agg_flush();
+    --ind;
+    L("}");
+  }
+
+  // ----------------------------------------------------------- kernels --
+  void main_kernel() {
+    prologue("dq_main");
+    const bool agg_src = P.source_kind == DQ_SRC_AGG;
+    std::vector<int> cols;  // staged columns read by COL slots
+    for (int s = 0; s < P.nslots; ++s)
+      if (slot(s).kind == DQ_SLOT_COL && std::find(cols.begin(), cols.end(), slot(s).src) == cols.end())
+        cols.push_back(slot(s).src);
+    L("const int64_t nrows = source_rows(P);");
+    L("const int64_t span = " + num((long long)kBlock * U) + ";");
+    L("for (int64_t base = (int64_t)blockIdx.x * span; base < nrows; base += (int64_t)gridDim.x * span) {");
+    ++ind;
+    for (int c : cols) L("uint64_t c" + num(c) + "[" + num(U) + "];");
+    if (!cols.empty()) {
+      L("#pragma unroll");
+      L("for (int u = 0; u < " + num(U) + "; ++u) {");
+      ++ind;
+      L("const int64_t r_ = base + u * " + num(kBlock) + " + tid;");
+      L("const bool in_ = r_ < nrows;");
+      for (int c : cols) {
+        int w = P.cols[c].width;
+        L("c" + num(c) + "[u] = in_ ? (uint64_t)reinterpret_cast<const " + uint_type(w) + "*>(P.cols[" + num(c) +
+          "].ptr)[r_] : 0ull;");
+      }
+      --ind;
+      L("}");
+    }
+    L("#pragma unroll");
+    L("for (int u = 0; u < " + num(U) + "; ++u) {");
+    ++ind;
+    L("const int64_t row = base + u * " + num(kBlock) + " + tid;");
+    L("bool act = row < nrows;");
+    row = "row";
+    if (agg_src) {
+      const int sr = P.source_res;
+      const DevRes& R = P.res[sr];
+      if (R.nkeys > 0) L("if (act) act = " + res(sr) + ".slots[(uint64_t)row * " + num(R.words) + "] != kEmpty;");
+    }
+    for (int s = 0; s < P.nslots; ++s) {
+      const DevSlot& sl = slot(s);
+      if (sl.kind == DQ_SLOT_COL) {
+        var[s] = "v" + num(s);
+        L("const uint64_t " + var[s] + " = canon(c" + num(sl.src) + "[u], " + ct_name(sl.ctype) + ");");
+      } else if (sl.kind == DQ_SLOT_AGGKEY || sl.kind == DQ_SLOT_AGGVAL) {
+        const DevRes& R = P.res[sl.res];
+        var[s] = "v" + num(s);
+        L("uint64_t " + var[s] + " = 0;");
+        L("if (row < nrows) {");
+        ++ind;
+        L("const uint64_t* as_ = " + res(sl.res) + ".slots + (uint64_t)row * " + num(R.words) + ";");
+        if (sl.kind == DQ_SLOT_AGGVAL) {
+          L(var[s] + " = canon(as_[" + num(R.val_word + sl.src) + "], " + ct_name(sl.ctype) + ");");
+        } else if (R.packed) {
+          L("const uint64_t t_ = (uint64_t)row == " + res(sl.res) + ".cap ? kEmpty : as_[0];");
+          bool wide = R.nkeys == 1 && (R.key_ctype[0] == DQ_I64 || R.key_ctype[0] == DQ_U64);
+          L(var[s] + " = canon(" + (wide ? std::string("t_") : "(t_ >> " + num(32 * sl.src) + ") & 0xffffffffull") +
+            ", " + ct_name(sl.ctype) + ");");
+        } else {
+          L(var[s] + " = canon(as_[" + num(R.key_word + sl.src) + "], " + ct_name(sl.ctype) + ");");
+        }
+        --ind;
+        L("}");
+      }
+    }
+    declare_regs(0);
+    L("do {");
+    ++ind;
+    ops_from(0, 0, "act", "break;");
+    --ind;
+    L("} while (0);");
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+    epilogue();
+  }
+
+  void heavy_kernel() {
+    const dq_op& op = P.ops[expand_op];
+    (void)op;
+    std::fill(var.begin(), var.end(), std::string());
+    prologue("dq_heavy");
+    L("__shared__ uint32_t s_unit;");
+    L("const uint32_t nitems = *P.heavy.count < P.heavy.cap ? *P.heavy.count : P.heavy.cap;");
+    L("const uint64_t units = P.heavy.unit_prefix[nitems];");
+    L("for (;;) {");
+    ++ind;
+    L("if (tid == 0) s_unit = atomicAdd(P.tile_counter, 1u);");
+    L("__syncthreads();");
+    L("const uint64_t unit = s_unit;");
+    L("__syncthreads();");
+    L("if (unit >= units) break;");
+    L("int lo = 0, hi = (int)nitems;");
+    L("while (lo < hi) {");
+    L("  const int mid = (lo + hi) >> 1;");
+    L("  if (P.heavy.unit_prefix[mid + 1] <= unit) lo = mid + 1; else hi = mid;");
+    L("}");
+    L("const uint64_t* it = P.heavy.items + (size_t)lo * P.heavy.words;");
+    L("const uint64_t chunk = unit - P.heavy.unit_prefix[lo];");
+    L("const uint64_t off = it[0] + chunk * (uint64_t)P.exp_cap;");
+    L("const uint64_t rem = it[1] - chunk * (uint64_t)P.exp_cap;");
+    L("const uint32_t len = (uint32_t)(rem < (uint64_t)P.exp_cap ? rem : (uint64_t)P.exp_cap);");
+    for (int s = 0; s < P.nslots; ++s)
+      if (slot(s).stash >= 0) {
+        var[s] = "h" + num(s);
+        L("const uint64_t " + var[s] + " = it[" + num(2 + slot(s).stash) + "];");
+      }
+    L("for (uint32_t pb = 0; pb < len; pb += " + num(kBlock) + "u) {");
+    ++ind;
+    L("const uint32_t q = pb + (uint32_t)tid;");
+    L("bool a = q < len;");
+    L("const uint32_t m = (uint32_t)off + q;");
+    row = "";
+    pairs(expand_op, 1, "a", "m", "continue;");
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+    epilogue();
+  }
+};
+
+}  // namespace
+
+Program generate(const DevPipe& P, int expand_op) {
+  Gen g(P, expand_op);
+  bool has_expand = false;
+  for (int i = 0; i < P.nops; ++i) has_expand |= P.ops[i].kind == DQ_OP_EXPAND;
+  g.U = (has_expand || P.source_kind == DQ_SRC_AGG) ? 1 : 4;
+  g.choose_agg();
+  g.o = "// generated pipeline kernel (dogqc_b200)\n#include \"dq_common.cuh\"\nusing namespace dq;\n\n";
+  g.main_kernel();
+  Program prog;
+  if (expand_op >= 0) {
+    g.o += "\n";
+    g.heavy_kernel();
+    prog.heavy = true;
+  }
+  prog.source = g.o;
+  prog.smem_bytes = g.smem;
+  prog.rows_per_thread = g.U;
+  return prog;
+}
+
+// ------------------------------------------------------------- compiler --
+
+namespace {
+
+struct Entry {
+  std::vector<char> cubin;
+  std::string log;
+  cudaLibrary_t lib = nullptr;
+  cudaKernel_t main = nullptr, heavy = nullptr;
+};
+
+std::mutex g_mu;
+std::map<std::string, std::unique_ptr<Entry>> g_cache;
+
+const char* kStdint =
+    "#pragma once\n"
+    "typedef signed char int8_t; typedef short int16_t; typedef int int32_t; typedef long long int64_t;\n"
+    "typedef unsigned char uint8_t; typedef unsigned short uint16_t; typedef unsigned int uint32_t;\n"
+    "typedef unsigned long long uint64_t;\n";
+const char* kStddef = "#pragma once\ntypedef unsigned long size_t; typedef long ptrdiff_t;\n";
+
+void nvrtc_check(nvrtcResult r, const char* what) {
+  if (r != NVRTC_SUCCESS) throw Error(std::string(what) + ": " + nvrtcGetErrorString(r));
+}
+
+void build(Entry& e, const std::string& src) {
+  std::vector<const char*> hdrs, names;
+  for (int i = 0; i < kEmbedCount; ++i) {
+    hdrs.push_back(kEmbedText[i]);
+    names.push_back(kEmbedNames[i]);
+  }
+  hdrs.push_back(kStdint);
+  names.push_back("stdint.h");
+  hdrs.push_back(kStddef);
+  names.push_back("stddef.h");
+  nvrtcProgram prog;
+  nvrtc_check(nvrtcCreateProgram(&prog, src.c_str(), "dq_pipeline.cu", (int)hdrs.size(), hdrs.data(), names.data()),
+              "nvrtcCreateProgram");
+  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-lineinfo",
+                        "--ptxas-options=-v"};
+  nvrtcResult r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
+  size_t n = 0;
+  nvrtcGetProgramLogSize(prog, &n);
+  e.log.assign(n, '\0');
+  if (n) nvrtcGetProgramLog(prog, &e.log[0]);
+  while (!e.log.empty() && e.log.back() == '\0') e.log.pop_back();
+  if (r != NVRTC_SUCCESS) {
+    nvrtcDestroyProgram(&prog);
+    throw Error("generated pipeline kernel failed to compile:\n" + e.log);
+  }
+  size_t cb = 0;
+  nvrtc_check(nvrtcGetCUBINSize(prog, &cb), "nvrtcGetCUBINSize");
+  e.cubin.resize(cb);
+  nvrtc_check(nvrtcGetCUBIN(prog, e.cubin.data()), "nvrtcGetCUBIN");
+  nvrtcDestroyProgram(&prog);
+}
+
+}  // namespace
+
+Kernels compile(const Program& prog, bool load) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  std::unique_ptr<Entry>& slot = g_cache[prog.source];
+  if (!slot) {
+    std::unique_ptr<Entry> e(new Entry());
+    build(*e, prog.source);
+    slot = std::move(e);
+  }
+  Entry& e = *slot;
+  if (load && !e.lib) {
+    cudaError_t err = cudaLibraryLoadData(&e.lib, e.cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
+    if (err != cudaSuccess) {
+      e.lib = nullptr;
+      throw Error(std::string("loading a generated pipeline kernel: ") + cudaGetErrorString(err));
+    }
+    err = cudaLibraryGetKernel(&e.main, e.lib, "dq_main");
+    if (err == cudaSuccess && prog.heavy) err = cudaLibraryGetKernel(&e.heavy, e.lib, "dq_heavy");
+    if (err != cudaSuccess) throw Error(std::string("generated kernel entry: ") + cudaGetErrorString(err));
+  }
+  Kernels k;
+  k.main = e.main;
+  k.heavy = e.heavy;
+  k.log = e.log;
+  return k;
+}
+
+}  // namespace jit
+}  // namespace dq

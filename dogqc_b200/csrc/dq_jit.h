@@ -1,0 +1,49 @@
+// Per-pipeline kernels generated at plan preparation (host side).
+//
+// The reference compiles every query: its translator writes one CUDA source per
+// query and runs nvcc on it (dogqc/cudaTranslator.py, dogqc/codegen.py,
+// dogqc/code.py).  This backend does the same per pipeline of the lowered plan,
+// in process: dq_jit.cu turns a pipeline descriptor into straight-line CUDA
+// (values in registers, one row per lane, warp-cooperative expansion and
+// aggregation), compiles it with NVRTC for sm_100a and loads the cubin with
+// the runtime's library API.  Compiled programs are cached by source text, so
+// re-preparing a plan or growing its tables does not recompile.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "dq_device.h"
+
+namespace dq {
+namespace jit {
+
+struct Error : std::runtime_error {
+  explicit Error(const std::string& m) : std::runtime_error(m) {}
+};
+
+struct Program {
+  std::string source;
+  int smem_bytes = 0;        // dynamic shared memory of both kernels
+  int rows_per_thread = 1;   // rows one thread takes per grid-stride step
+  bool heavy = false;        // second kernel for deferred expansion ranges
+};
+
+struct Kernels {
+  cudaKernel_t main = nullptr;
+  cudaKernel_t heavy = nullptr;
+  std::string log;           // compiler log (register and spill report)
+};
+
+// Source of the kernels for one pipeline.  `P` is the launch descriptor the
+// runtime filled (resource layouts, slots with their staged-column indices,
+// stash indices); `expand_op` is the expansion whose wide ranges are deferred
+// to the second kernel (-1: none).
+Program generate(const DevPipe& P, int expand_op);
+
+// Compiles the program (cached by source text) and, with `load`, loads it.
+Kernels compile(const Program& prog, bool load);
+
+}  // namespace jit
+}  // namespace dq

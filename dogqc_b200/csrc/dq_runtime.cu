@@ -22,6 +22,7 @@
 
 #include "../../include/dogqc_b200.h"
 #include "dq_device.h"
+#include "dq_jit.h"
 
 namespace dq {
 cudaError_t launch_pipeline(const DevPipe& P, int grid, cudaStream_t stream);
@@ -77,6 +78,16 @@ int ctype_width(int t) {
 
 uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 
+// Set while an offline context (DQ_CFG_OFFLINE) registers tables or prepares
+// plans: buffers then record their size but take no device memory.
+thread_local bool t_offline = false;
+
+struct OfflineScope {
+  bool prev;
+  explicit OfflineScope(bool on) : prev(t_offline) { t_offline = on; }
+  ~OfflineScope() { t_offline = prev; }
+};
+
 // Device buffer with 256 bytes of tail padding: tile copies round their size up
 // to 16 bytes and may read past the last row.
 struct DevBuf {
@@ -89,6 +100,7 @@ struct DevBuf {
   void alloc(size_t b) {
     release();
     bytes = b;
+    if (t_offline) return;
     DQ_CUDA(cudaMalloc(&ptr, align_up(b, 256) + 256));
   }
   void release() {
@@ -124,6 +136,7 @@ struct TableRec {
 struct dq_ctx {
   dq_config cfg{};
   int device = 0;
+  bool offline = false;     // DQ_CFG_OFFLINE: no device, plans are compiled only
   int sms = 148;
   cudaStream_t stream = nullptr;
   std::string error;
@@ -148,6 +161,9 @@ struct PipeRec {
   int grid = 1;             // CTAs of a tile launch (at most one per tile)
   int grid_full = 1;        // persistent grid (SMs x resident CTAs)
   bool row = false;         // runs on the row kernel
+  bool jit = false;         // runs on its generated kernel
+  jit::Program prog;        // generated source and launch shape
+  jit::Kernels kernels;
   int expand_op = -1;       // level-0 expansion op with deferral
   DevBuf pattern_buf, heavy_items, heavy_count, heavy_prefix;
   bool mm_count = false;    // sink is a multimap count: bucket scan follows
@@ -185,6 +201,8 @@ int guarded(dq_ctx* ctx, F f) {
     return f();
   } catch (const DqError& e) {
     return fail(ctx, e.code, e.what());
+  } catch (const jit::Error& e) {
+    return fail(ctx, DQ_ERR_CUDA, e.what());
   } catch (const std::bad_alloc&) {
     return fail(ctx, DQ_ERR_OOM, "host allocation failed");
   } catch (const std::exception& e) {
@@ -195,6 +213,11 @@ int guarded(dq_ctx* ctx, F f) {
 void upload_column(dq_ctx* ctx, ColRec& rec, const dq_column& c, int64_t nrows, bool device_src,
                    cudaStream_t stream) {
   cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (ctx->offline) {  // sizes only
+    if (!rec.data) rec.data = std::make_shared<DevBuf>();
+    if (c.ctype == DQ_STR && c.width <= 0 && !rec.offsets) rec.offsets = std::make_shared<DevBuf>();
+    return;
+  }
   if (c.ctype == DQ_STR) {
     uint64_t nchars = c.width > 0 ? (uint64_t)c.width * nrows : c.nchars;
     if (!rec.data) rec.data = std::make_shared<DevBuf>();
@@ -520,7 +543,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   P.pat_off[d.npatterns] = (int32_t)cat.size();
   if (!cat.empty()) {
     p.pattern_buf.alloc(cat.size());
-    DQ_CUDA(cudaMemcpy(p.pattern_buf.ptr, cat.data(), cat.size(), cudaMemcpyHostToDevice));
+    if (!ctx->offline) DQ_CUDA(cudaMemcpy(p.pattern_buf.ptr, cat.data(), cat.size(), cudaMemcpyHostToDevice));
     P.patterns = p.pattern_buf.as<uint8_t>();
   }
   const dq_op& sink = d.ops[d.nops - 1];
@@ -617,15 +640,39 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     throw DqError(DQ_ERR_UNSUPPORTED, "pipeline needs more shared memory than a CTA has; lower tile_rows");
   P.off_stage = fixed;
   P.smem_bytes = fixed + P.nstage * P.stage_bytes;
-  int occ = p.row ? row_occupancy(P.smem_bytes) : pipeline_occupancy(P.smem_bytes);
+
+  // generated kernel (default), else the prebuilt tile or row kernel
+  p.jit = !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL));
+  int occ = 1;
+  int64_t rows_per_cta = tile;
+  if (p.jit) {
+    p.prog = jit::generate(P, p.expand_op);
+    p.kernels = jit::compile(p.prog, !ctx->offline);
+    rows_per_cta = (int64_t)kThreads * p.prog.rows_per_thread;
+    if (!ctx->offline) {
+      const void* fn = (const void*)p.kernels.main;
+      DQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, p.prog.smem_bytes));
+      DQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, p.prog.smem_bytes));
+      if (p.kernels.heavy)
+        DQ_CUDA(cudaFuncSetAttribute((const void*)p.kernels.heavy, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     p.prog.smem_bytes));
+    }
+  } else if (!ctx->offline) {
+    occ = p.row ? row_occupancy(P.smem_bytes) : pipeline_occupancy(P.smem_bytes);
+  }
   if (occ < 1) throw DqError(DQ_ERR_UNSUPPORTED, "pipeline kernel cannot be resident with this shared memory");
   int want = ctx->cfg.ctas_per_sm > 0 ? std::min(ctx->cfg.ctas_per_sm, occ) : occ;
   p.grid_full = ctx->sms * want;
   p.grid = p.grid_full;
-  if (!P.nrows_dev) {  // no more CTAs than tiles
-    int64_t ntiles = (P.nrows + tile - 1) / tile;
-    p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(p.grid_full, ntiles));
+  if (!P.nrows_dev) {  // no more CTAs than row blocks
+    int64_t blocks = (P.nrows + rows_per_cta - 1) / rows_per_cta;
+    p.grid = (int)std::max<int64_t>(1, std::min<int64_t>(p.grid_full, blocks));
   }
+}
+
+cudaError_t launch_generated(cudaKernel_t k, const DevPipe& P, int grid, int smem, cudaStream_t st) {
+  void* args[] = {(void*)&P};
+  return cudaLaunchKernel((const void*)k, dim3(grid), dim3(kThreads), args, (size_t)smem, st);
 }
 
 void free_events(dq_plan* plan) {
@@ -673,14 +720,16 @@ int run_once(dq_plan* plan, cudaStream_t st) {
     p.dev.tile_counter = counters + 2 * i;
     DQ_CUDA(cudaEventRecord(plan->events[1 + 2 * i], st));
     if (p.expand_op >= 0) DQ_CUDA(cudaMemsetAsync(p.heavy_count.ptr, 0, 8, st));
-    DQ_CUDA(p.row ? launch_row(p.dev, p.grid, st) : launch_pipeline(p.dev, p.grid, st));
+    if (p.jit) DQ_CUDA(launch_generated(p.kernels.main, p.dev, p.grid, p.prog.smem_bytes, st));
+    else DQ_CUDA(p.row ? launch_row(p.dev, p.grid, st) : launch_pipeline(p.dev, p.grid, st));
     ++launches;
     if (p.expand_op >= 0) {
       DQ_CUDA(launch_heavy_prefix(p.dev.heavy, (uint64_t)p.dev.exp_cap, st));
       DevPipe H = p.dev;
       H.mode = 1;
       H.tile_counter = counters + 2 * i + 1;
-      DQ_CUDA(launch_pipeline(H, p.grid_full, st));
+      if (p.jit) DQ_CUDA(launch_generated(p.kernels.heavy, H, p.grid_full, p.prog.smem_bytes, st));
+      else DQ_CUDA(launch_pipeline(H, p.grid_full, st));
       launches += 2;
     }
     if (p.mm_count) {
@@ -737,6 +786,11 @@ int dq_init(const dq_config* cfg, dq_ctx** out) {
       ctx->cfg = *cfg;
     }
     ctx->device = ctx->cfg.device;
+    if (ctx->cfg.flags & DQ_CFG_OFFLINE) {
+      ctx->offline = true;  // 148 SMs assumed for launch shapes; nothing touches a device
+      *out = ctx.release();
+      return (int)DQ_OK;
+    }
     int n = 0;
     DQ_CUDA(cudaGetDeviceCount(&n));
     if (ctx->device < 0 || ctx->device >= n) throw DqError(DQ_ERR_INVALID, "no such CUDA device");
@@ -750,6 +804,10 @@ int dq_init(const dq_config* cfg, dq_ctx** out) {
 
 void dq_shutdown(dq_ctx* ctx) {
   if (!ctx) return;
+  if (ctx->offline) {
+    delete ctx;
+    return;
+  }
   cudaSetDevice(ctx->device);
   ctx->tables.clear();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -761,7 +819,8 @@ int dq_table_register(dq_ctx* ctx, const char* name, int32_t ncols, const dq_col
   if (!ctx || !name || (ncols > 0 && !cols) || nrows < 0 || ncols < 0) return fail(ctx, DQ_ERR_INVALID, "bad table arguments");
   return guarded(ctx, [&]() {
     std::lock_guard<std::mutex> lk(ctx->mu);
-    DQ_CUDA(cudaSetDevice(ctx->device));
+    OfflineScope offline(ctx->offline);
+    if (!ctx->offline) DQ_CUDA(cudaSetDevice(ctx->device));
     TableRec t;
     t.nrows = nrows;
     for (int i = 0; i < ncols; ++i) {
@@ -775,7 +834,7 @@ int dq_table_register(dq_ctx* ctx, const char* name, int32_t ncols, const dq_col
       upload_column(ctx, rec, c, nrows, flags & DQ_TABLE_DEVICE_DATA, ctx->stream);
       t.cols.push_back(std::move(rec));
     }
-    DQ_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (!ctx->offline) DQ_CUDA(cudaStreamSynchronize(ctx->stream));
     ctx->tables[name] = std::move(t);
     return (int)DQ_OK;
   });
@@ -826,7 +885,8 @@ int dq_plan_prepare(dq_ctx* ctx, const dq_plan_desc* desc, dq_plan** out) {
     if (desc->nres < 0 || desc->npipes <= 0 || (desc->nres && !desc->res) || !desc->pipes)
       throw DqError(DQ_ERR_BAD_IR, "empty plan");
     std::lock_guard<std::mutex> lk(ctx->mu);
-    DQ_CUDA(cudaSetDevice(ctx->device));
+    OfflineScope offline(ctx->offline);
+    if (!ctx->offline) DQ_CUDA(cudaSetDevice(ctx->device));
     std::unique_ptr<dq_plan> plan(new dq_plan());
     plan->ctx = ctx;
     plan->status.alloc(4);
@@ -890,6 +950,7 @@ int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out) {
   dq_ctx* ctx = plan->ctx;
   *out = nullptr;
   return guarded(ctx, [&]() {
+    if (ctx->offline) throw DqError(DQ_ERR_UNSUPPORTED, "an offline context compiles plans but cannot execute them");
     std::lock_guard<std::mutex> lk(ctx->mu);
     DQ_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
@@ -939,9 +1000,29 @@ int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out) {
 
 void dq_plan_free(dq_plan* plan) {
   if (!plan) return;
+  if (plan->ctx->offline) {
+    delete plan;
+    return;
+  }
   cudaSetDevice(plan->ctx->device);
   free_events(plan);
   delete plan;
+}
+
+int dq_plan_source(dq_plan* plan, int32_t pipe, char* buf, int64_t cap, int64_t* len) {
+  if (!plan || !len || cap < 0 || (cap > 0 && !buf)) return DQ_ERR_INVALID;
+  if (pipe < 0 || pipe >= (int32_t)plan->pipes.size()) return fail(plan->ctx, DQ_ERR_INVALID, "no such pipeline");
+  const PipeRec& p = *plan->pipes[pipe];
+  if (!p.jit) return fail(plan->ctx, DQ_ERR_NOT_FOUND, "pipeline runs on a prebuilt kernel");
+  std::string text = p.prog.source;
+  if (!p.kernels.log.empty()) text += "\n/* compiler report:\n" + p.kernels.log + "\n*/\n";
+  *len = (int64_t)text.size();
+  if (cap > 0) {
+    size_t n = std::min<size_t>((size_t)cap - 1, text.size());
+    memcpy(buf, text.data(), n);
+    buf[n] = '\0';
+  }
+  return DQ_OK;
 }
 
 int dq_plan_timing_get(dq_plan* plan, dq_plan_timing* out) {

@@ -86,6 +86,19 @@ class Plan(object):
             lib.dq_result_free(res)
         return Result(self.lowering.result_names, types, cols, n.value)
 
+    def source(self, pipe):
+        """Generated CUDA source of pipeline ``pipe`` with the compiler's
+        register report (None when the pipeline runs on a prebuilt kernel)."""
+        lib = L.lib()
+        n = C.c_int64()
+        st = lib.dq_plan_source(self.handle, pipe, None, 0, C.byref(n))
+        if st == L.ERR_NOT_FOUND:
+            return None
+        L.check(st, self.engine.ctx)
+        buf = C.create_string_buffer(n.value + 1)
+        L.check(lib.dq_plan_source(self.handle, pipe, buf, n.value + 1, C.byref(n)), self.engine.ctx)
+        return buf.value.decode()
+
     def timing(self):
         t = L.dq_plan_timing()
         L.check(L.lib().dq_plan_timing_get(self.handle, C.byref(t)))

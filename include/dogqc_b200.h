@@ -71,6 +71,11 @@ typedef struct {
 #define DQ_CFG_NO_GRAPH    2    /* do not capture CUDA graphs                  */
 #define DQ_CFG_ROW_KERNEL  4    /* run pipelines without a multimap expansion  */
                                 /* on the row-at-a-time kernel                 */
+#define DQ_CFG_NO_JIT      8    /* run every pipeline on the prebuilt tile      */
+                                /* kernel instead of a generated one           */
+#define DQ_CFG_OFFLINE     16   /* no device: tables are metadata only, plans   */
+                                /* are lowered and their kernels compiled but  */
+                                /* cannot execute (ahead-of-time checking)     */
 
 /* ------------------------------------------------------------- contexts -- */
 int dq_init(const dq_config* cfg, dq_ctx** out);
@@ -238,7 +243,17 @@ typedef struct {
 } dq_plan_desc;
 
 /* -------------------------------------------------------------- plans -- */
+/* Validates the IR, lays out the plan's tables and, unless DQ_CFG_NO_JIT or
+ * DQ_CFG_ROW_KERNEL is set, generates one CUDA kernel per pipeline and
+ * compiles it for sm_100a (NVRTC, in process; cached by source text).  This is
+ * the step where the reference writes and compiles its query source
+ * (dogqc/cudaTranslator.py:31-101, dogqc/code.py:4-26).                      */
 int dq_plan_prepare(dq_ctx* ctx, const dq_plan_desc* desc, dq_plan** out);
+/* Generated CUDA source of pipeline `pipe` followed by the compiler's
+ * register report, NUL-terminated into buf (at most cap bytes); *len is the
+ * full length.  DQ_ERR_NOT_FOUND when the pipeline runs on a prebuilt kernel.
+ * The counterpart of the reference's generated query file.                 */
+int dq_plan_source(dq_plan* plan, int32_t pipe, char* buf, int64_t cap, int64_t* len);
 /* Runs every pipeline in order on `stream` (NULL: the context stream) and
  * returns a new result.  Resources are reset at the start of each run.       */
 int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out);
