@@ -61,6 +61,21 @@ __device__ __forceinline__ uint64_t fmix64(uint64_t k) {
 // reduction).
 __device__ __forceinline__ uint64_t reduce_range(uint64_t h, uint64_t cap) { return __umul64hi(h, cap); }
 
+// Home slot of a 64-bit tag in a table of `cap` slots (cap < 2^32): the high
+// word of a multiplicative (Fibonacci) hash, range-reduced by a multiply-high.
+// Every hash table of a plan places keys with this function.
+__device__ __forceinline__ uint32_t slot_of(uint64_t tag, uint32_t cap) {
+  const uint32_t h = (uint32_t)((tag * 0x9e3779b97f4a7c15ull) >> 32);
+  return __umulhi(h, cap);
+}
+
+// Bucket of a multimap key (n key values) among `cap` buckets.
+__device__ __forceinline__ uint32_t bucket_of(const uint64_t* k, int n, uint32_t cap) {
+  uint64_t h = n > 0 ? k[0] : 0;
+  for (int i = 1; i < n; ++i) h = (h ^ (h >> 29)) * 0xbf58476d1ce4e5b9ull + k[i];
+  return slot_of(h, cap);
+}
+
 __device__ __forceinline__ uint64_t arith(int sub, int t, uint64_t a, uint64_t b) {
   a = canon(a, t);
   b = canon(b, t);
@@ -216,16 +231,10 @@ __device__ __forceinline__ uint64_t key_tag(const DevRes& R, const uint64_t* k) 
   return fmix64(h) & 0x7fffffffffffffffull;
 }
 
-__device__ __forceinline__ uint64_t multimap_hash(const uint64_t* k, int n) {
-  uint64_t h = 0x9e3779b97f4a7c15ull;
-  for (int i = 0; i < n; ++i) h = fmix64(h ^ k[i]) + 0x632be59bd9b4e019ull * (i + 1);
-  return fmix64(h);
-}
-
 // Unique join table: returns slot index or -1.
 __device__ __forceinline__ int64_t unique_find(const DevRes& R, uint64_t tag, const uint64_t* k) {
   if (R.packed && tag == kEmpty) return R.slots[R.cap * R.words] == 0 ? (int64_t)R.cap : -1;
-  uint64_t idx = reduce_range(fmix64(tag), R.cap);
+  uint64_t idx = slot_of(tag, (uint32_t)R.cap);
   for (uint64_t n = 0; n < R.cap; ++n) {
     const uint64_t* s = R.slots + idx * R.words;
     uint64_t t = s[0];
@@ -249,7 +258,7 @@ __device__ __forceinline__ int64_t unique_insert(const DevPipe& P, const DevRes&
     uint64_t old = atomicCAS((unsigned long long*)(R.slots + R.cap * R.words), kEmpty, 0ull);
     return old == kEmpty ? (int64_t)R.cap : -1;
   }
-  uint64_t idx = reduce_range(fmix64(tag), R.cap);
+  uint64_t idx = slot_of(tag, (uint32_t)R.cap);
   for (uint64_t n = 0; n < R.cap; ++n) {
     uint64_t* s = R.slots + idx * R.words;
     uint64_t old = atomicCAS((unsigned long long*)s, kEmpty, tag);
@@ -274,7 +283,7 @@ __device__ __noinline__ int64_t agg_slot_global(const DevPipe& P, const DevRes& 
       atomicCAS((unsigned long long*)(R.slots + R.cap * R.words), kEmpty, 0ull);
       return (int64_t)R.cap;
     }
-    uint64_t idx = reduce_range(fmix64(tag), R.cap);
+    uint64_t idx = slot_of(tag, (uint32_t)R.cap);
     for (uint64_t n = 0; n < R.cap; ++n) {
       uint64_t* s = R.slots + idx * R.words;
       uint64_t t = *(volatile uint64_t*)s;
@@ -289,7 +298,7 @@ __device__ __noinline__ int64_t agg_slot_global(const DevPipe& P, const DevRes& 
     return -1;
   }
   // wide keys: claim with a busy marker, publish keys, then the tag
-  uint64_t idx = reduce_range(fmix64(tag), R.cap);
+  uint64_t idx = slot_of(tag, (uint32_t)R.cap);
   for (uint64_t n = 0; n < R.cap; ++n) {
     uint64_t* s = R.slots + idx * R.words;
     uint64_t t = *(volatile uint64_t*)s;
@@ -409,7 +418,7 @@ __device__ __forceinline__ int local_group_slot(uint64_t* tags, int ns, uint64_t
     s_cas64(saddr(&tags[ns]), kEmpty, 0ull);
     return ns;
   }
-  uint32_t idx = (uint32_t)reduce_range(fmix64(tag), (uint64_t)ns);
+  uint32_t idx = slot_of(tag, (uint32_t)ns);
   for (int n = 0; n < ns; ++n) {
     uint64_t t = ((volatile uint64_t*)tags)[idx];
     if (t == tag) return (int)idx;

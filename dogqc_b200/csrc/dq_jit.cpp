@@ -42,9 +42,9 @@ namespace dq {
 namespace jit {
 namespace {
 
-constexpr int kCopies = 16;                 // accumulator replicas of the striped local table
-constexpr int kStripedMax = 48 * 1024;      // shared memory the striped table may take
+constexpr int kStripedMax = 48 * 1024;      // shared memory the striped local table may take
 constexpr int kBlock = kThreads;
+constexpr int kWarpBuf = 64;                // rows one warp's divergence buffer holds
 
 const char* ct_name(int t) {
   switch (t) {
@@ -166,8 +166,31 @@ struct Gen {
   int copies = 1;
   int U = 1;
   int smem = 0;
+  int refill = -1;               // op after which lanes are refilled (-1: none)
+  int nbuf = 0;                  // values per row in the warp buffers
+  int buf_off = 0;               // shared-memory offset of the warp buffers
 
   Gen(const DevPipe& p, int e) : P(p), expand_op(e), var(p.nslots) {}
+
+  static bool narrow(int t) { return t == DQ_I8 || t == DQ_I32 || t == DQ_U32; }
+
+  // Tag of a packed-key table (the value key_tag computes), from a slot list.
+  std::string packed_tag(int r, int list, int n) {
+    const DevRes& R = P.res[r];
+    std::string t = fresh("tg");
+    auto key = [&](int i) { return "canon(" + V(P.lists[list + i]) + ", " + ct_name(R.key_ctype[i]) + ")"; };
+    if (n == 0) L("const uint64_t " + t + " = 0ull;");
+    else if (n == 1 && !narrow(R.key_ctype[0])) L("const uint64_t " + t + " = " + key(0) + ";");
+    else if (n == 1) L("const uint64_t " + t + " = (uint64_t)(uint32_t)" + key(0) + ";");
+    else L("const uint64_t " + t + " = (uint64_t)(uint32_t)" + key(0) + " | ((uint64_t)(uint32_t)" + key(1) + " << 32);");
+    return t;
+  }
+
+  // Whether a packed tag can equal the empty marker (all ones).
+  bool tag_can_be_empty(int r) const {
+    const DevRes& R = P.res[r];
+    return !(R.nkeys == 1 && narrow(R.key_ctype[0])) && R.nkeys > 0;
+  }
 
   void L(const std::string& s) {
     o.append((size_t)ind * 2, ' ');
@@ -258,10 +281,18 @@ struct Gen {
         case DQ_OP_FILTER:
           L(act + " = " + act + " && (" + V(op.a) + " != 0ull);");
           skip_if_idle(act, exit);
+          if (k == refill && level == 0) {
+            refill_lanes(k, act);
+            return;
+          }
           break;
         case DQ_OP_PROBE:
           probe(op, act);
           skip_if_idle(act, exit);
+          if (k == refill && level == 0) {
+            refill_lanes(k, act);
+            return;
+          }
           break;
         case DQ_OP_EXPAND:
           expand(k, level, act);
@@ -292,8 +323,34 @@ struct Gen {
     L("int64_t " + s + " = -1;");
     L("if (" + act + ") {");
     ++ind;
-    std::string k = keys(op, r, op.list, op.nlist);
-    L(s + " = unique_find(" + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
+    if (R.packed && R.nkeys > 0) {
+      // packed keys: the tag is the key; linear probing with a 32-bit index
+      const std::string tg = packed_tag(r, op.list, op.nlist);
+      const std::string W = num(R.words);
+      const bool ext = tag_can_be_empty(r);
+      L("const uint64_t* const ht_ = " + res(r) + ".slots;");
+      L("const uint32_t hc_ = (uint32_t)" + res(r) + ".cap;");
+      if (ext) {
+        L("if (" + tg + " == kEmpty) {");
+        L("  if (ht_[(uint64_t)hc_ * " + W + "] == 0ull) " + s + " = (int64_t)hc_;");
+        L("} else {");
+        ++ind;
+      }
+      L("uint32_t i_ = slot_of(" + tg + ", hc_);");
+      L("for (uint32_t n_ = 0; n_ < hc_; ++n_) {");
+      L("  const uint64_t t_ = ht_[(uint64_t)i_ * " + W + "];");
+      L("  if (t_ == " + tg + ") { " + s + " = (int64_t)i_; break; }");
+      L("  if (t_ == kEmpty) break;");
+      L("  i_ = (i_ + 1u == hc_) ? 0u : i_ + 1u;");
+      L("}");
+      if (ext) {
+        --ind;
+        L("}");
+      }
+    } else {
+      std::string k = keys(op, r, op.list, op.nlist);
+      L(s + " = unique_find(" + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
+    }
     if (op.sub == DQ_JOIN_INNER && op.nlist2 > 0) {
       L("if (" + s + " >= 0) {");
       ++ind;
@@ -370,7 +427,7 @@ struct Gen {
     L("if (" + act + ") {");
     ++ind;
     std::string kk = keys(op, r, op.list, op.nlist);
-    L("const uint64_t b_ = reduce_range(multimap_hash(" + kk + ", " + num(op.nlist) + "), " + res(r) + ".cap);");
+    L("const uint32_t b_ = bucket_of(" + kk + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap);");
     L(ec + " = " + res(r) + ".counts[b_];");
     L(eo + " = " + ec + " ? " + res(r) + ".offsets[b_] : 0u;");
     if (k == expand_op && level == 0) {
@@ -445,7 +502,8 @@ struct Gen {
     L("if (" + act + ") {");
     ++ind;
     std::string k = keys(op, r, op.list, op.nlist);
-    L("const uint64_t tag_ = key_tag(" + res(r) + ", " + k + ");");
+    if (R.packed) L("const uint64_t tag_ = " + packed_tag(r, op.list, op.nlist) + ";");
+    else L("const uint64_t tag_ = key_tag(" + res(r) + ", " + k + ");");
     auto global = [&]() {
       L("const int64_t g_ = agg_slot_global(P, " + res(r) + ", tag_, " + k + ");");
       L("if (g_ >= 0) {");
@@ -464,8 +522,8 @@ struct Gen {
       ++ind;
       for (int j = 0; j < R.naggs; ++j) {
         std::string idx = agg == AGG_STRIPED
-                              ? "((s_ * " + num(R.naggs) + " + " + num(j) + ") * " + num(kCopies) + " + (lane & " +
-                                    num(kCopies - 1) + "))"
+                              ? "((s_ * " + num(R.naggs) + " + " + num(j) + ") * " + num(copies) + " + (lane & " +
+                                    num(copies - 1) + "))"
                               : "(s_ * " + num(R.naggs) + " + " + num(j) + ")";
         L("s_merge(saddr(lacc + " + idx + "), " + red_name(R.agg_red[j]) + ", " + vals[j] + ");");
       }
@@ -505,7 +563,7 @@ struct Gen {
     L("if (" + act + ") {");
     ++ind;
     std::string k = keys(op, r, op.list, op.nlist);
-    L("const uint64_t b_ = reduce_range(multimap_hash(" + k + ", " + num(op.nlist) + "), " + res(r) + ".cap);");
+    L("const uint32_t b_ = bucket_of(" + k + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap);");
     if (op.kind == DQ_OP_MM_COUNT) {
       L("atomicAdd(&" + res(r) + ".counts[b_], 1u);");
     } else {
@@ -570,16 +628,100 @@ struct Gen {
       ns = 0;
       return;
     }
+    // replicate the accumulators per lane (32 copies: lanes of a warp never
+    // collide) or per half-warp (16) when the table allows, else one copy
     const int tags = (ns + 1) * 8;
-    const int striped = (ns + 1) * R.naggs * 8 * kCopies;
-    if (tags + striped <= kStripedMax) {
-      agg = AGG_STRIPED;
-      copies = kCopies;
-    } else {
-      agg = AGG_LOCAL;
-      copies = 1;
-    }
+    agg = AGG_LOCAL;
+    copies = 1;
+    for (int c : {32, 16})
+      if (tags + (ns + 1) * R.naggs * 8 * c <= kStripedMax) {
+        agg = AGG_STRIPED;
+        copies = c;
+        break;
+      }
     smem = tags + (ns + 1) * R.naggs * 8 * copies;
+  }
+
+  // Lane refill after op `k`: only when later ops do enough per-row work to
+  // pay for buffering the live values.
+  void choose_refill(int k) {
+    refill = -1;
+    if (k < 0 || k >= P.nops || P.source_kind == DQ_SRC_AGG) return;
+    const dq_op& op = P.ops[k];
+    if (op.kind != DQ_OP_FILTER && op.kind != DQ_OP_PROBE) return;
+    for (int j = 0; j < k; ++j)
+      if (P.ops[j].kind == DQ_OP_EXPAND) return;
+    bool heavy = false;
+    for (int j = k + 1; j < P.nops; ++j) {
+      const int kind = P.ops[j].kind;
+      heavy |= kind == DQ_OP_PROBE || kind == DQ_OP_EXPAND || kind == DQ_OP_LIKE || kind == DQ_OP_STREQ ||
+               kind == DQ_OP_BUILD || kind == DQ_OP_MM_COUNT || kind == DQ_OP_MM_SCATTER || kind == DQ_OP_EMIT ||
+               (kind == DQ_OP_AGG && agg != AGG_REGS);
+    }
+    if (!heavy) return;
+    refill = k;
+    nbuf = (int)live_after(k + 1, 0).size() + (reads_strings_after(k + 1) ? 1 : 0);
+    if (nbuf == 0) nbuf = 1;
+    buf_off = (smem + 15) / 16 * 16;
+    smem = buf_off + (kBlock / 32) * kWarpBuf * nbuf * 8;
+  }
+
+  // Appends the active lanes' live values to the warp's buffer, then drains
+  // it 32 rows at a time (and the remainder after the warp's last rows)
+  // through ops k+1.. with every lane busy.  Called inside the row body's
+  // do-while, which it closes and reopens.
+  void refill_lanes(int k, const std::string& act) {
+    std::vector<int> live = live_after(k + 1, 0);
+    const bool need_row = reads_strings_after(k + 1);
+    const std::string B = num(kWarpBuf);
+    L("{");
+    ++ind;
+    L("const unsigned bm_ = __ballot_sync(kFull, " + act + ");");
+    L("if (" + act + ") {");
+    ++ind;
+    L("const int p_ = wn + __popc(bm_ & ((1u << lane) - 1u));");
+    int j = 0;
+    for (int s : live) L("wb[" + num(j++ * kWarpBuf) + " + p_] = " + V(s) + ";");
+    if (need_row) L("wb[" + num(j * kWarpBuf) + " + p_] = (uint64_t)" + row + ";");
+    --ind;
+    L("}");
+    L("wn += __popc(bm_);");
+    --ind;
+    L("}");
+    --ind;
+    L("} while (0);");
+    L("__syncwarp();");
+    L("const bool last_ = base + (int64_t)gridDim.x * span >= nrows && u == " + num(U - 1) + ";");
+    L("while (wn >= 32 || (last_ && wn > 0)) {");
+    ++ind;
+    L("bool ra = lane < wn;");
+    j = 0;
+    for (int s : live) {
+      std::string nv = "b" + num(s) + "_" + num(uid++);
+      L("uint64_t " + nv + " = wb[" + num(j++ * kWarpBuf) + " + lane];");
+      var[s] = nv;
+    }
+    if (need_row) {
+      row = fresh("brow");
+      L("const int64_t " + row + " = (int64_t)wb[" + num(j * kWarpBuf) + " + lane];");
+    }
+    L("__syncwarp();");
+    L("if (lane + 32 < wn) {");
+    for (int q = 0; q < nbuf; ++q)
+      L("  wb[" + num(q * kWarpBuf) + " + lane] = wb[" + num(q * kWarpBuf) + " + lane + 32];");
+    L("}");
+    L("__syncwarp();");
+    L("wn = wn > 32 ? wn - 32 : 0;");
+    L("do {");
+    ++ind;
+    ops_from(k + 1, 0, "ra", "break;");
+    --ind;
+    L("} while (0);");
+    --ind;
+    L("}");
+    L("do {");
+    ++ind;
+    (void)B;
   }
 
   uint64_t min_mask() const {
@@ -669,6 +811,11 @@ struct Gen {
         cols.push_back(slot(s).src);
     L("const int64_t nrows = source_rows(P);");
     L("const int64_t span = " + num((long long)kBlock * U) + ";");
+    if (refill >= 0) {
+      L("uint64_t* const wb = reinterpret_cast<uint64_t*>(smem + " + num(buf_off) + ") + (tid >> 5) * " +
+        num(kWarpBuf * nbuf) + ";  // this warp's refill buffer");
+      L("int wn = 0;  // rows in it");
+    }
     L("for (int64_t base = (int64_t)blockIdx.x * span; base < nrows; base += (int64_t)gridDim.x * span) {");
     ++ind;
     for (int c : cols) L("uint64_t c" + num(c) + "[" + num(U) + "];");
@@ -783,12 +930,13 @@ struct Gen {
 
 }  // namespace
 
-Program generate(const DevPipe& P, int expand_op) {
+Program generate(const DevPipe& P, int expand_op, int refill_op) {
   Gen g(P, expand_op);
   bool has_expand = false;
   for (int i = 0; i < P.nops; ++i) has_expand |= P.ops[i].kind == DQ_OP_EXPAND;
   g.U = (has_expand || P.source_kind == DQ_SRC_AGG) ? 1 : 4;
   g.choose_agg();
+  g.choose_refill(refill_op);
   g.o = "// generated pipeline kernel (dogqc_b200)\n#include \"dq_common.cuh\"\nusing namespace dq;\n\n";
   g.main_kernel();
   Program prog;

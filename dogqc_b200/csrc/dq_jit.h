@@ -39,8 +39,9 @@ struct Kernels {
 // Source of the kernels for one pipeline.  `P` is the launch descriptor the
 // runtime filled (resource layouts, slots with their staged-column indices,
 // stash indices); `expand_op` is the expansion whose wide ranges are deferred
-// to the second kernel (-1: none).
-Program generate(const DevPipe& P, int expand_op);
+// to the second kernel (-1: none); `refill_op` is the selective filter or
+// probe after which the warps refill their lanes from a buffer (-1: none).
+Program generate(const DevPipe& P, int expand_op, int refill_op);
 
 // Compiles the program (cached by source text) and, with `load`, loads it.
 Kernels compile(const Program& prog, bool load);

@@ -227,7 +227,7 @@ __device__ int local_slot(const LocalAgg& a, uint64_t tag, int nkeys) {
     atomicCAS((unsigned long long*)&a.tags[a.ns], kEmpty, 0ull);
     return a.ns;
   }
-  uint32_t idx = (uint32_t)reduce_range(fmix64(tag), (uint64_t)a.ns);
+  uint32_t idx = slot_of(tag, (uint32_t)a.ns);
   for (int n = 0; n < a.ns; ++n) {
     uint64_t t = *(volatile uint64_t*)&a.tags[idx];
     if (t == tag) return (int)idx;
@@ -353,7 +353,7 @@ __device__ void op_mm(const DevPipe& P, const Cta& c, const dq_op& op, const Lev
     int row = sel[i];
     uint64_t k[DQ_MAX_KEYS];
     key_values(P, c, R, op.list, op.nlist, L.level, row, k);
-    uint64_t b = reduce_range(multimap_hash(k, op.nlist), R.cap);
+    uint64_t b = bucket_of(k, op.nlist, (uint32_t)R.cap);
     if (op.kind == DQ_OP_MM_COUNT) {
       atomicAdd(&R.counts[b], 1u);
     } else {
@@ -439,7 +439,7 @@ __device__ uint32_t expand_setup(const DevPipe& P, const Cta& c, const dq_op& op
     int row = sel[i];
     uint64_t k[DQ_MAX_KEYS];
     key_values(P, c, R, op.list, op.nlist, L.level, row, k);
-    uint64_t b = reduce_range(multimap_hash(k, op.nlist), R.cap);
+    uint64_t b = bucket_of(k, op.nlist, (uint32_t)R.cap);
     uint32_t cnt = R.counts[b];
     uint32_t off = cnt ? R.offsets[b] : 0;
     if (defer && cnt > P.heavy.threshold) {
@@ -1093,7 +1093,7 @@ __device__ void row_ops(Row& x, bool act, uint8_t* smem) {
           const DevRes& R = P.res[op.res];
           uint64_t kv[DQ_MAX_KEYS];
           rkeys(x, R, op.list, op.nlist, kv);
-          uint64_t b = reduce_range(multimap_hash(kv, op.nlist), R.cap);
+          uint64_t b = bucket_of(kv, op.nlist, (uint32_t)R.cap);
           if (op.kind == DQ_OP_MM_COUNT) {
             atomicAdd(&R.counts[b], 1u);
           } else {

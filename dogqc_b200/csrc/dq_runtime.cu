@@ -646,7 +646,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   int occ = 1;
   int64_t rows_per_cta = tile;
   if (p.jit) {
-    p.prog = jit::generate(P, p.expand_op);
+    p.prog = jit::generate(P, p.expand_op, d.compact - 1);
     p.kernels = jit::compile(p.prog, !ctx->offline);
     rows_per_cta = (int64_t)kThreads * p.prog.rows_per_thread;
     if (!ctx->offline) {

@@ -43,6 +43,28 @@ CT = {"i8": L.I8, "i32": L.I32, "u32": L.U32, "i64": L.I64, "u64": L.U64, "str":
 NP_DTYPE = {L.I8: "int8", L.I32: "int32", L.U32: "uint32", L.I64: "int64", L.U64: "uint64"}
 
 
+class _Op(dict):
+    """One IR op (its fields), plus the plan's estimate of the fraction of rows
+    that pass it (filters and probes), which places the lane refill."""
+    sel = 1.0
+
+
+# A filter or probe whose estimated pass fraction is at most this refills the
+# lanes of the generated kernel before the rest of the pipeline.
+REFILL_SELECTIVITY = 0.5
+
+
+def refill_point(ops):
+    """1 + index of the first level-0 filter/probe that passes at most
+    REFILL_SELECTIVITY of its rows (the ``compact`` field of dq_pipeline), or 0."""
+    for k, o in enumerate(ops):
+        if o["kind"] == L.OP_EXPAND:
+            break
+        if o["kind"] in (L.OP_FILTER, L.OP_PROBE) and getattr(o, "sel", 1.0) <= REFILL_SELECTIVITY:
+            return k + 1
+    return 0
+
+
 def _tname(t):
     return t.name if hasattr(t, "name") else str(t)
 
@@ -139,8 +161,8 @@ class Pipe(object):
         return self.cols.index(name)
 
     def op(self, kind, **kw):
-        d = dict(kind=kind, sub=0, dst=-1, a=-1, b=-1, c=-1, ctype=0, flags=0, res=-1,
-                 list=0, nlist=0, list2=0, nlist2=0, imm=0)
+        d = _Op(kind=kind, sub=0, dst=-1, a=-1, b=-1, c=-1, ctype=0, flags=0, res=-1,
+                list=0, nlist=0, list2=0, nlist2=0, imm=0)
         d.update(kw)
         self.ops.append(d)
         if len(self.ops) > L.MAX_OPS:
@@ -233,7 +255,7 @@ class Lowering(object):
         """Continue ``pipe`` (which delivers ``child``'s rows) at ``node``."""
         k = type(node).__name__
         if k == "Selection":
-            self.filter(pipe, node.condition)
+            self.filter(pipe, node.condition, getattr(node, "selectivity", 1.0))
             self.consume_parent(node, pipe)
         elif k == "Map":
             v = self.expr(pipe, node.expression)
@@ -440,13 +462,13 @@ class Lowering(object):
             raise Unsupported("string constant used as a value")
         return v
 
-    def filter(self, pipe, condition):
+    def filter(self, pipe, condition, selectivity=1.0):
         v = self.expr(pipe, condition)
         if isinstance(v, Imm):
             if v.value != 0:
                 return
             v = self.materialize_value(pipe, v, "i32")
-        pipe.op(L.OP_FILTER, a=v)
+        pipe.op(L.OP_FILTER, a=v).sel = selectivity
 
     # -- joins -------------------------------------------------------------------
     def produce_join(self, node):
@@ -536,7 +558,10 @@ class Lowering(object):
                 dsts.append(s)
             pl, pn = pipe.list_(dsts)
             sub = {"INNER": L.JOIN_INNER, "SEMI": L.JOIN_SEMI, "ANTI": L.JOIN_ANTI}[jt]
-            pipe.op(L.OP_PROBE, sub=sub, res=info["res"], list=kl, nlist=kn, list2=pl, nlist2=pn)
+            op = pipe.op(L.OP_PROBE, sub=sub, res=info["res"], list=kl, nlist=kn, list2=pl, nlist2=pn)
+            # fraction of probe rows that find a match (the plan's estimate)
+            probe_rows = max(getattr(node.rightChild, "tupleNum", 0), 1)
+            op.sel = min(1.0, getattr(node, "tupleNum", probe_rows) / float(probe_rows))
         else:
             if pipe.level + 1 >= L.MAX_LEVELS:
                 raise Unsupported("more than %d nested multimatch joins in one pipeline" % (L.MAX_LEVELS - 1))
@@ -681,7 +706,7 @@ class Lowering(object):
             for j, pat in enumerate(p.patterns):
                 keep.append(pat)
                 d.patterns[j] = pat
-            d.compact = 1
+            d.compact = refill_point(p.ops)
         desc = L.dq_plan_desc()
         desc.abi_version = L.ABI_VERSION
         desc.nres = len(self.res)

@@ -230,7 +230,10 @@ typedef struct {
     int16_t lists[DQ_MAX_LIST];
     int32_t npatterns;
     const char* patterns[DQ_MAX_PATTERNS];  /* LIKE patterns / string constants */
-    int32_t compact;                 /* 1: compact after every filter / probe   */
+    int32_t compact;                 /* k > 0: generated kernels refill lanes   */
+                                     /* after op k-1 (a selective filter or    */
+                                     /* probe); 0: no refill.  The tile kernel */
+                                     /* compacts after every filter and probe. */
 } dq_pipeline;
 
 typedef struct {
