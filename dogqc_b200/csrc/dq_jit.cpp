@@ -166,6 +166,8 @@ struct Gen {
   int copies = 1;
   int U = 1;
   int smem = 0;
+  std::string pay_reg;           // probe payload already loaded with its tag
+  int min_blocks = 0;            // __launch_bounds__ minimum CTAs per SM (0: none)
   int refill = -1;               // op after which lanes are refilled (-1: none)
   int nbuf = 0;                  // values per row in the warp buffers
   int buf_off = 0;               // shared-memory offset of the warp buffers
@@ -330,19 +332,52 @@ struct Gen {
       const bool ext = tag_can_be_empty(r);
       L("const uint64_t* const ht_ = " + res(r) + ".slots;");
       L("const uint32_t hc_ = (uint32_t)" + res(r) + ".cap;");
+      if (R.words == 2 && op.sub == DQ_JOIN_INNER && op.nlist2 > 0 && P.lists[op.list2] >= 0)
+        L("uint64_t pv_ = 0;");
       if (ext) {
         L("if (" + tg + " == kEmpty) {");
         L("  if (ht_[(uint64_t)hc_ * " + W + "] == 0ull) " + s + " = (int64_t)hc_;");
         L("} else {");
         ++ind;
       }
-      L("uint32_t i_ = slot_of(" + tg + ", hc_);");
-      L("for (uint32_t n_ = 0; n_ < hc_; ++n_) {");
-      L("  const uint64_t t_ = ht_[(uint64_t)i_ * " + W + "];");
-      L("  if (t_ == " + tg + ") { " + s + " = (int64_t)i_; break; }");
-      L("  if (t_ == kEmpty) break;");
-      L("  i_ = (i_ + 1u == hc_) ? 0u : i_ + 1u;");
-      L("}");
+      if (R.words <= 2) {
+        // aligned slot pairs (the slot count is even): slot p_ before the home
+        // slot can only match, not end the walk; with one payload word the
+        // payload arrives with its tag
+        L("uint32_t p_ = slot_of(" + tg + ", hc_);");
+        L("bool odd_ = (p_ & 1u) != 0u;");
+        L("p_ &= ~1u;");
+        L("for (uint32_t n_ = 0; n_ < hc_; n_ += 2u) {");
+        ++ind;
+        std::string t0, t1, p0, p1;
+        if (R.words == 2) {
+          L("const ulonglong2 a_ = __ldg(reinterpret_cast<const ulonglong2*>(ht_ + (uint64_t)p_ * 2));");
+          L("const ulonglong2 b_ = __ldg(reinterpret_cast<const ulonglong2*>(ht_ + (uint64_t)p_ * 2 + 2));");
+          t0 = "a_.x", t1 = "b_.x", p0 = "a_.y", p1 = "b_.y";
+        } else {
+          L("const ulonglong2 a_ = __ldg(reinterpret_cast<const ulonglong2*>(ht_ + p_));");
+          t0 = "a_.x", t1 = "a_.y";
+        }
+        const bool with_pay = R.words == 2 && op.sub == DQ_JOIN_INNER && op.nlist2 > 0 && P.lists[op.list2] >= 0;
+        L("if (" + t0 + " == " + tg + ") { " + s + " = (int64_t)p_;" + (with_pay ? " pv_ = " + p0 + ";" : "") +
+          " break; }");
+        L("if (" + t1 + " == " + tg + ") { " + s + " = (int64_t)p_ + 1;" + (with_pay ? " pv_ = " + p1 + ";" : "") +
+          " break; }");
+        L("if ((!odd_ && " + t0 + " == kEmpty) || " + t1 + " == kEmpty) break;");
+        L("odd_ = false;");
+        L("p_ = (p_ + 2u == hc_) ? 0u : p_ + 2u;");
+        --ind;
+        L("}");
+        if (with_pay) pay_reg = "pv_";
+      } else {
+        L("uint32_t i_ = slot_of(" + tg + ", hc_);");
+        L("for (uint32_t n_ = 0; n_ < hc_; ++n_) {");
+        L("  const uint64_t t_ = ht_[(uint64_t)i_ * " + W + "];");
+        L("  if (t_ == " + tg + ") { " + s + " = (int64_t)i_; break; }");
+        L("  if (t_ == kEmpty) break;");
+        L("  i_ = (i_ + 1u == hc_) ? 0u : i_ + 1u;");
+        L("}");
+      }
       if (ext) {
         --ind;
         L("}");
@@ -351,7 +386,13 @@ struct Gen {
       std::string k = keys(op, r, op.list, op.nlist);
       L(s + " = unique_find(" + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
     }
-    if (op.sub == DQ_JOIN_INNER && op.nlist2 > 0) {
+    if (!pay_reg.empty()) {
+      // the payload came with the tag (the all-ones key's slot is read here)
+      int d = P.lists[op.list2];
+      L("if (" + s + " >= 0) " + V(d) + " = canon(" + s + " == (int64_t)hc_ ? ht_[(uint64_t)hc_ * 2 + 1] : pv_, " +
+        ct_name(slot(d).ctype) + ");");
+      pay_reg.clear();
+    } else if (op.sub == DQ_JOIN_INNER && op.nlist2 > 0) {
       L("if (" + s + " >= 0) {");
       ++ind;
       L("const uint64_t* pay_ = " + res(r) + ".slots + (uint64_t)" + s + " * " + num(R.words) + " + " +
@@ -784,8 +825,8 @@ struct Gen {
   }
 
   void prologue(const char* name) {
-    L(std::string("extern \"C\" __global__ void __launch_bounds__(") + num(kBlock) + ") " + name +
-      "(const __grid_constant__ DevPipe P) {");
+    L(std::string("extern \"C\" __global__ void __launch_bounds__(") + num(kBlock) +
+      (min_blocks > 0 ? ", " + num(min_blocks) : std::string()) + ") " + name + "(const __grid_constant__ DevPipe P) {");
     ++ind;
     L("extern __shared__ __align__(16) uint8_t smem[];");
     L("if (*(volatile int32_t*)P.status & (kErrHtFull | kErrTimeout)) return;");
@@ -934,7 +975,11 @@ Program generate(const DevPipe& P, int expand_op, int refill_op) {
   Gen g(P, expand_op);
   bool has_expand = false;
   for (int i = 0; i < P.nops; ++i) has_expand |= P.ops[i].kind == DQ_OP_EXPAND;
-  g.U = (has_expand || P.source_kind == DQ_SRC_AGG) ? 1 : 4;
+  g.U = (has_expand || P.source_kind == DQ_SRC_AGG) ? 1 : 2;
+  // tuning knobs: rows per thread and step, minimum resident CTAs per SM
+  if (const char* e = getenv("DQ_JIT_ROWS"))
+    if (!has_expand && P.source_kind != DQ_SRC_AGG) g.U = std::min(8, std::max(1, atoi(e)));
+  if (const char* e = getenv("DQ_JIT_MIN_BLOCKS")) g.min_blocks = std::min(8, std::max(0, atoi(e)));
   g.choose_agg();
   g.choose_refill(refill_op);
   g.o = "// generated pipeline kernel (dogqc_b200)\n#include \"dq_common.cuh\"\nusing namespace dq;\n\n";

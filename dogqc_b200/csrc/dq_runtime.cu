@@ -273,7 +273,13 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       R.key_word = 1;
       R.val_word = 1 + (R.packed ? 0 : d.nkeys);
       R.words = R.val_word + (d.kind == DQ_RES_UNIQUE ? d.npay : d.naggs);
+      // join tables get twice the slots the plan asks for (a load factor of at
+      // most 1/4 with the reference's default size factor 2): most probes of a
+      // selective join miss, and a miss walks to the next empty slot.  An even
+      // slot count lets probes read aligned slot pairs.
+      if (d.kind == DQ_RES_UNIQUE) cap = (cap * 2 + 1) & ~1ull;
       cap = std::max<uint64_t>(cap, 16);
+      if (cap >= 0xffffffffull) throw DqError(DQ_ERR_UNSUPPORTED, "hash tables hold fewer than 2^32 slots");
       R.cap = cap;
       r.slots.alloc((cap + 1) * R.words * 8);
       R.slots = r.slots.as<uint64_t>();
@@ -288,6 +294,7 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       break;
     }
     case DQ_RES_MULTI: {
+      if (cap >= 0xffffffffull) throw DqError(DQ_ERR_UNSUPPORTED, "multimaps hold fewer than 2^32 buckets");
       R.cap = cap;
       r.counts.alloc(cap * 4);
       r.offsets.alloc((cap + 1) * 4);
