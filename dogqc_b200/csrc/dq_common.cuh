@@ -47,6 +47,25 @@ __device__ __forceinline__ void st(uint8_t* p, int w, uint64_t v) {
   }
 }
 
+template <class T>
+__device__ __forceinline__ T ld_plain(const T* p) { return *p; }
+
+// Read-only (non-coherent) load of a w-byte value: for data a kernel does not
+// write, such as a multimap payload during the probe.
+__device__ __forceinline__ uint64_t ldg_w(const uint8_t* p, int w) {
+  switch (w) {
+    case 1: return __ldg(p);
+    case 2: return __ldg(reinterpret_cast<const uint16_t*>(p));
+    case 4: return __ldg(reinterpret_cast<const uint32_t*>(p));
+    default: return __ldg(reinterpret_cast<const unsigned long long*>(p));
+  }
+}
+
+// One 32-byte read-only load (four 64-bit words; p 32-byte aligned).
+__device__ __forceinline__ void ld_nc_32B(const uint64_t* p, uint64_t& a, uint64_t& b, uint64_t& c, uint64_t& d) {
+  asm volatile("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
+}
+
 // MurmurHash3 64-bit finaliser (Appleby), used for every hash table.
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {
   k ^= k >> 33;

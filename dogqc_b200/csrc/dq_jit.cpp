@@ -167,10 +167,13 @@ struct Gen {
   int U = 1;
   int smem = 0;
   std::string pay_reg;           // probe payload already loaded with its tag
+  std::vector<int> prefetch;     // probes whose first slot pair is loaded early
+  std::map<int, std::string> pending;  // gathered slots not loaded yet -> match index
   int min_blocks = 0;            // __launch_bounds__ minimum CTAs per SM (0: none)
   int refill = -1;               // op after which lanes are refilled (-1: none)
   int nbuf = 0;                  // values per row in the warp buffers
   int buf_off = 0;               // shared-memory offset of the warp buffers
+  std::string ldfn = "__ldcs";   // load function of streamed source columns
 
   Gen(const DevPipe& p, int e) : P(p), expand_op(e), var(p.nslots) {}
 
@@ -240,6 +243,15 @@ struct Gen {
   void ops_from(int k, int level, const std::string& act, const std::string& exit) {
     for (; k < P.nops; ++k) {
       const dq_op& op = P.ops[k];
+      if (!pending.empty()) {
+        std::vector<int> reads;
+        op_reads(P, op, reads);
+        if (op.kind == DQ_OP_EXPAND) {
+          std::vector<int> live = live_after(k, level);
+          reads.insert(reads.end(), live.begin(), live.end());
+        }
+        materialize(reads, act);
+      }
       switch (op.kind) {
         case DQ_OP_ARITH:
           L(assign(op.dst, std::string("arith(") + arith_name(op.sub) + ", " + ct_name(op.ctype) + ", " +
@@ -289,7 +301,7 @@ struct Gen {
           }
           break;
         case DQ_OP_PROBE:
-          probe(op, act);
+          probe(k, act);
           skip_if_idle(act, exit);
           if (k == refill && level == 0) {
             refill_lanes(k, act);
@@ -318,7 +330,60 @@ struct Gen {
     }
   }
 
-  void probe(const dq_op& op, const std::string& act) {
+  bool is_prefetched(int k) const {
+    return std::find(prefetch.begin(), prefetch.end(), k) != prefetch.end();
+  }
+
+  // Probes whose first slot pair is loaded together with the row's columns:
+  // packed-key join tables of at most two words, probed at level 0 before the
+  // lane refill, with keys read straight from source columns.
+  void choose_prefetch() {
+    prefetch.clear();
+    if (P.source_kind == DQ_SRC_AGG) return;
+    for (int k = 0; k < P.nops; ++k) {
+      const dq_op& op = P.ops[k];
+      if (op.kind == DQ_OP_EXPAND || (refill >= 0 && k > refill)) break;
+      if (op.kind != DQ_OP_PROBE) continue;
+      const DevRes& R = P.res[op.res];
+      if (!R.packed || R.nkeys == 0 || R.words > 2 || tag_can_be_empty(op.res)) continue;
+      bool cols = true;
+      for (int i = 0; i < op.nlist; ++i) cols &= slot(P.lists[op.list + i]).kind == DQ_SLOT_COL;
+      if (cols) prefetch.push_back(k);
+    }
+  }
+
+  // Issues the first pair loads of the prefetched probes for row u (inside
+  // the column-load loop, where c<col>[u] and in_ are defined).
+  void prefetch_loads() {
+    for (int k : prefetch) {
+      const dq_op& op = P.ops[k];
+      const int r = op.res;
+      const DevRes& R = P.res[r];
+      std::string key[2];
+      for (int i = 0; i < op.nlist && i < 2; ++i) {
+        const DevSlot& sl = slot(P.lists[op.list + i]);
+        key[i] = "canon(canon(c" + num(sl.src) + "[u], " + ct_name(sl.ctype) + "), " + ct_name(R.key_ctype[i]) + ")";
+      }
+      std::string tag = op.nlist == 1 ? (narrow(R.key_ctype[0]) ? "(uint64_t)(uint32_t)" + key[0] : key[0])
+                                      : "(uint64_t)(uint32_t)" + key[0] + " | ((uint64_t)(uint32_t)" + key[1] + " << 32)";
+      L("{");
+      ++ind;
+      L("const uint64_t* const ht_ = " + res(r) + ".slots;");
+      const std::string K = num(k);
+      L("const uint32_t p_ = slot_of(" + tag + ", (uint32_t)" + res(r) + ".cap) & ~" + num(4 / R.words - 1) + "u;");
+      L("if (in_) {");
+      L("  ld_nc_32B(ht_ + (uint64_t)p_ * " + num(R.words) + ", pw" + K + "_0[u], pw" + K + "_1[u], pw" + K + "_2[u], pw" +
+        K + "_3[u]);");
+      L("} else {");
+      L("  pw" + K + "_0[u] = pw" + K + "_1[u] = pw" + K + "_2[u] = pw" + K + "_3[u] = kEmpty;");
+      L("}");
+      --ind;
+      L("}");
+    }
+  }
+
+  void probe(int k, const std::string& act) {
+    const dq_op& op = P.ops[k];
     const int r = op.res;
     const DevRes& R = P.res[r];
     std::string s = fresh("ps");
@@ -341,31 +406,44 @@ struct Gen {
         ++ind;
       }
       if (R.words <= 2) {
-        // aligned slot pairs (the slot count is even): slot p_ before the home
-        // slot can only match, not end the walk; with one payload word the
-        // payload arrives with its tag
-        L("uint32_t p_ = slot_of(" + tg + ", hc_);");
-        L("bool odd_ = (p_ & 1u) != 0u;");
-        L("p_ &= ~1u;");
-        L("for (uint32_t n_ = 0; n_ < hc_; n_ += 2u) {");
-        ++ind;
-        std::string t0, t1, p0, p1;
-        if (R.words == 2) {
-          L("const ulonglong2 a_ = __ldg(reinterpret_cast<const ulonglong2*>(ht_ + (uint64_t)p_ * 2));");
-          L("const ulonglong2 b_ = __ldg(reinterpret_cast<const ulonglong2*>(ht_ + (uint64_t)p_ * 2 + 2));");
-          t0 = "a_.x", t1 = "b_.x", p0 = "a_.y", p1 = "b_.y";
-        } else {
-          L("const ulonglong2 a_ = __ldg(reinterpret_cast<const ulonglong2*>(ht_ + p_));");
-          t0 = "a_.x", t1 = "a_.y";
-        }
+        // aligned 32-byte groups (two slots with a payload word, four tags
+        // otherwise; the slot count divides by 4) read in one load.  Slots of
+        // the first group before the home slot can only match, not end the
+        // walk.  A prefetched probe takes its first group from the load issued
+        // with the row's columns.
+        const bool pf = is_prefetched(k);
+        const int G = 4 / R.words;
+        const std::string Gs = num(G);
         const bool with_pay = R.words == 2 && op.sub == DQ_JOIN_INNER && op.nlist2 > 0 && P.lists[op.list2] >= 0;
-        L("if (" + t0 + " == " + tg + ") { " + s + " = (int64_t)p_;" + (with_pay ? " pv_ = " + p0 + ";" : "") +
-          " break; }");
-        L("if (" + t1 + " == " + tg + ") { " + s + " = (int64_t)p_ + 1;" + (with_pay ? " pv_ = " + p1 + ";" : "") +
-          " break; }");
-        L("if ((!odd_ && " + t0 + " == kEmpty) || " + t1 + " == kEmpty) break;");
-        L("odd_ = false;");
-        L("p_ = (p_ + 2u == hc_) ? 0u : p_ + 2u;");
+        L("uint32_t p_ = slot_of(" + tg + ", hc_);");
+        L("uint32_t f_ = p_ & " + num(G - 1) + "u;");
+        L("p_ -= f_;");
+        if (pf) {
+          L("uint64_t w0_ = pw" + num(k) + "_0[u], w1_ = pw" + num(k) + "_1[u], w2_ = pw" + num(k) + "_2[u], w3_ = pw" +
+            num(k) + "_3[u];");
+        } else {
+          L("uint64_t w0_, w1_, w2_, w3_;");
+          L("ld_nc_32B(ht_ + (uint64_t)p_ * " + W + ", w0_, w1_, w2_, w3_);");
+        }
+        L("for (uint32_t n_ = 0;;) {");
+        ++ind;
+        if (R.words == 2) {
+          L("if (w0_ == " + tg + ") { " + s + " = (int64_t)p_;" + (with_pay ? " pv_ = w1_;" : "") + " break; }");
+          L("if (w2_ == " + tg + ") { " + s + " = (int64_t)p_ + 1;" + (with_pay ? " pv_ = w3_;" : "") + " break; }");
+          L("if ((f_ == 0u && w0_ == kEmpty) || w2_ == kEmpty) break;");
+        } else {
+          L("if (w0_ == " + tg + ") { " + s + " = (int64_t)p_; break; }");
+          L("if (w1_ == " + tg + ") { " + s + " = (int64_t)p_ + 1; break; }");
+          L("if (w2_ == " + tg + ") { " + s + " = (int64_t)p_ + 2; break; }");
+          L("if (w3_ == " + tg + ") { " + s + " = (int64_t)p_ + 3; break; }");
+          L("if ((f_ == 0u && w0_ == kEmpty) || (f_ <= 1u && w1_ == kEmpty) || (f_ <= 2u && w2_ == kEmpty) || "
+            "w3_ == kEmpty) break;");
+        }
+        L("f_ = 0u;");
+        L("p_ = (p_ + " + Gs + "u == hc_) ? 0u : p_ + " + Gs + "u;");
+        L("n_ += " + Gs + "u;");
+        L("if (n_ >= hc_) break;");
+        L("ld_nc_32B(ht_ + (uint64_t)p_ * " + W + ", w0_, w1_, w2_, w3_);");
         --ind;
         L("}");
         if (with_pay) pay_reg = "pv_";
@@ -432,27 +510,46 @@ struct Gen {
   }
 
   // gathers of level `lv` (the key columns first), key check, rest of the ops
+  // Loads a gathered multimap payload value of match `m` for the active lanes.
+  void gather(int s, const std::string& act, const std::string& m) {
+    const DevSlot& g = slot(s);
+    var[s] = "v" + num(s) + "_" + num(uid++);
+    L("const uint64_t " + var[s] + " = " + act + " ? canon(ldg_w(" + res(g.res) + ".pay[" + num(g.src) +
+      "] + (uint64_t)" + m + " * " + num(g.width) + ", " + num(g.width) + "), " + ct_name(g.ctype) + ") : 0ull;");
+  }
+
+  // Gathers the pending payload values the given slots need (lanes that a
+  // filter has dropped since the expansion do not load them).
+  void materialize(const std::vector<int>& slots, const std::string& act) {
+    for (int s : slots) {
+      auto it = pending.find(s);
+      if (it == pending.end()) continue;
+      const std::string m = it->second;
+      pending.erase(it);
+      gather(s, act, m);
+    }
+  }
+
+  // Gathers of level `lv`, all issued together (one round trip per chunk of
+  // pairs: the hot buckets of a skewed build side are L2-resident, so the
+  // latency of dependent loads, not their bytes, bounds the expansion), key
+  // check, rest of the ops.  The `pending` mechanism (load at first read)
+  // stays available for slots a generator variant wants to defer.
   void pairs(int k, int lv, const std::string& a, const std::string& m, const std::string& exit) {
     const dq_op& op = P.ops[k];
     declare_regs(lv);
-    auto gather = [&](int s) {
-      const DevSlot& g = slot(s);
-      var[s] = "v" + num(s) + "_" + num(uid++);
-      L("const uint64_t " + var[s] + " = " + a + " ? canon(ld(" + res(g.res) + ".pay[" + num(g.src) + "] + (uint64_t)" + m +
-        " * " + num(g.width) + ", " + num(g.width) + "), " + ct_name(g.ctype) + ") : 0ull;");
-    };
     for (int q = 0; q < op.nlist2; ++q) {
       int s = P.lists[op.list2 + q];
-      if (s >= 0 && slot(s).kind == DQ_SLOT_GATHER && slot(s).level == lv) gather(s);
+      if (s >= 0 && slot(s).kind == DQ_SLOT_GATHER && slot(s).level == lv && var[s].empty()) gather(s, a, m);
     }
+    for (int s = 0; s < P.nslots; ++s)
+      if (slot(s).kind == DQ_SLOT_GATHER && slot(s).level == lv && var[s].empty()) gather(s, a, m);
     for (int q = 0; q < op.nlist; ++q) {
       int t = P.res[op.res].key_ctype[q];
       L(a + " = " + a + " && canon(" + V(P.lists[op.list + q]) + ", " + ct_name(t) + ") == canon(" +
         V(P.lists[op.list2 + q]) + ", " + ct_name(t) + ");");
     }
     skip_if_idle(a, exit);
-    for (int s = 0; s < P.nslots; ++s)
-      if (slot(s).kind == DQ_SLOT_GATHER && slot(s).level == lv && var[s].empty()) gather(s);
     ops_from(k + 1, lv, a, exit);
   }
 
@@ -546,7 +643,45 @@ struct Gen {
     if (R.packed) L("const uint64_t tag_ = " + packed_tag(r, op.list, op.nlist) + ";");
     else L("const uint64_t tag_ = key_tag(" + res(r) + ", " + k + ");");
     auto global = [&]() {
-      L("const int64_t g_ = agg_slot_global(P, " + res(r) + ", tag_, " + k + ");");
+      if (R.packed) {
+        // agg_slot_global's packed-key claim, inline: find the tag or claim an
+        // empty slot with a compare-and-swap; the all-ones key has its own slot
+        const std::string W = num(R.words);
+        L("int64_t g_ = -1;");
+        L("{");
+        ++ind;
+        L("uint64_t* const gs_ = " + res(r) + ".slots;");
+        L("const uint32_t gc_ = (uint32_t)" + res(r) + ".cap;");
+        if (tag_can_be_empty(r)) {
+          L("if (tag_ == kEmpty) {");
+          L("  atomicCAS((unsigned long long*)(gs_ + (uint64_t)gc_ * " + W + "), kEmpty, 0ull);");
+          L("  g_ = (int64_t)gc_;");
+          L("} else {");
+          ++ind;
+        }
+        L("uint32_t i_ = slot_of(tag_, gc_);");
+        L("for (uint32_t n_ = 0; n_ < gc_; ++n_) {");
+        ++ind;
+        L("uint64_t* const s_ = gs_ + (uint64_t)i_ * " + W + ";");
+        L("const uint64_t t_ = *(volatile uint64_t*)s_;");
+        L("if (t_ == tag_) { g_ = (int64_t)i_; break; }");
+        L("if (t_ == kEmpty) {");
+        L("  const uint64_t o_ = atomicCAS((unsigned long long*)s_, kEmpty, tag_);");
+        L("  if (o_ == kEmpty || o_ == tag_) { g_ = (int64_t)i_; break; }");
+        L("}");
+        L("i_ = (i_ + 1u == gc_) ? 0u : i_ + 1u;");
+        --ind;
+        L("}");
+        L("if (g_ < 0) set_status(P, kErrHtFull);");
+        if (tag_can_be_empty(r)) {
+          --ind;
+          L("}");
+        }
+        --ind;
+        L("}");
+      } else {
+        L("const int64_t g_ = agg_slot_global(P, " + res(r) + ", tag_, " + k + ");");
+      }
       L("if (g_ >= 0) {");
       ++ind;
       L("uint64_t* a_ = " + res(r) + ".slots + (uint64_t)g_ * " + num(R.words) + " + " + num(R.val_word) + ";");
@@ -599,16 +734,29 @@ struct Gen {
   }
 
   void sink_mm(const dq_op& op, const std::string& act) {
+    // lanes of a warp that hit the same bucket (the hot keys of a skewed build
+    // side) take one atomic per bucket: the lowest such lane adds the group's
+    // size, the others their rank within the group
     const int r = op.res;
     const DevRes& R = P.res[r];
+    L("uint32_t b_ = 0xffffffffu;");
     L("if (" + act + ") {");
     ++ind;
     std::string k = keys(op, r, op.list, op.nlist);
-    L("const uint32_t b_ = bucket_of(" + k + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap);");
+    L("b_ = bucket_of(" + k + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap);");
+    --ind;
+    L("}");
+    L("const unsigned peers_ = __match_any_sync(kFull, b_);");
+    L("if (" + act + ") {");
+    ++ind;
+    L("const int lead_ = __ffs(peers_) - 1;");
     if (op.kind == DQ_OP_MM_COUNT) {
-      L("atomicAdd(&" + res(r) + ".counts[b_], 1u);");
+      L("if (lane == lead_) atomicAdd(&" + res(r) + ".counts[b_], (uint32_t)__popc(peers_));");
     } else {
-      L("const uint32_t pos_ = " + res(r) + ".offsets[b_] + atomicAdd(&" + res(r) + ".counts[b_], 1u);");
+      L("uint32_t at_ = 0;");
+      L("if (lane == lead_) at_ = atomicAdd(&" + res(r) + ".counts[b_], (uint32_t)__popc(peers_));");
+      L("at_ = __shfl_sync(peers_, at_, lead_);");
+      L("const uint32_t pos_ = " + res(r) + ".offsets[b_] + at_ + (uint32_t)__popc(peers_ & ((1u << lane) - 1u));");
       for (int j = 0; j < op.nlist2; ++j) {
         int w = R.pay_width[j];
         L("st(" + res(r) + ".pay[" + num(j) + "] + (size_t)pos_ * " + num(w) + ", " + num(w) + ", " +
@@ -842,6 +990,69 @@ struct Gen {
     L("}");
   }
 
+  // <dst><col>[0..U) for the thread's U consecutive rows of the step starting
+  // at `base_expr`: whole rows of every column in vector loads when the step
+  // is complete (columns are 256-byte aligned), else per row.  Source columns
+  // are streamed once: evict-first loads keep the join tables resident in L2.
+  void col_loads(const std::vector<int>& cols, const std::string& dst, const std::string& base_expr) {
+    L("{");
+    ++ind;
+    L("const int64_t r0_ = " + base_expr + " + (int64_t)tid * " + num(U) + ";");
+    L("if (r0_ + " + num(U) + " <= nrows) {");
+    ++ind;
+    for (int c : cols) vector_load(c, dst);
+    --ind;
+    L("} else {");
+    ++ind;
+    L("#pragma unroll");
+    L("for (int u = 0; u < " + num(U) + "; ++u) {");
+    L("  const bool in_ = r0_ + u < nrows;");
+    for (int c : cols) {
+      int w = P.cols[c].width;
+      L("  " + dst + num(c) + "[u] = in_ ? (uint64_t)" + ldfn + "(reinterpret_cast<const " + uint_type(w) + "*>(P.cols[" +
+        num(c) + "].ptr) + r0_ + u) : 0ull;");
+    }
+    L("}");
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+  }
+
+  // <dst><col>[0..U) from U consecutive rows starting at r0_ (in bounds): loads
+  // of up to 16 bytes, split into the column's values.
+  void vector_load(int c, const std::string& dst) {
+    const int w = P.cols[c].width;
+    const int total = U * w;
+    const int chunk = std::min(16, total);
+    const int n = total / chunk;
+    const char* T = chunk == 16 ? "uint4" : chunk == 8 ? "uint2" : uint_type(chunk);
+    const std::string base_ptr = "reinterpret_cast<const " + std::string(T) + "*>(P.cols[" + num(c) + "].ptr + r0_ * " +
+                                 num(w) + ")";
+    std::vector<std::string> words;  // 32-bit words of the loaded bytes (or narrower chunks)
+    for (int q = 0; q < n; ++q) {
+      std::string x = "x" + num(c) + "_" + num(q);
+      L("const " + std::string(T) + " " + x + " = " + ldfn + "(" + base_ptr + " + " + num(q) + ");");
+      if (chunk == 16) {
+        for (const char* f : {".x", ".y", ".z", ".w"}) words.push_back(x + f);
+      } else if (chunk == 8) {
+        words.push_back(x + ".x");
+        words.push_back(x + ".y");
+      } else {
+        words.push_back("(uint32_t)" + x);
+      }
+    }
+    for (int u = 0; u < U; ++u) {
+      std::string v;
+      const int byte = u * w;
+      if (w == 8) v = "((uint64_t)" + words[byte / 4] + " | ((uint64_t)" + words[byte / 4 + 1] + " << 32))";
+      else if (w == 4) v = "(uint64_t)" + words[byte / 4];
+      else if (chunk < 4) v = "(uint64_t)((" + words[0] + " >> " + num(8 * byte) + ") & " + (w == 2 ? "0xffffu" : "0xffu") + ")";
+      else v = "(uint64_t)((" + words[byte / 4] + " >> " + num(8 * (byte % 4)) + ") & " + (w == 2 ? "0xffffu" : "0xffu") + ")";
+      L(dst + num(c) + "[" + num(u) + "] = " + v + ";");
+    }
+  }
+
   // ----------------------------------------------------------- kernels --
   void main_kernel() {
     prologue("dq_main");
@@ -857,27 +1068,32 @@ struct Gen {
         num(kWarpBuf * nbuf) + ";  // this warp's refill buffer");
       L("int wn = 0;  // rows in it");
     }
+    for (int c : cols) L("uint64_t c" + num(c) + "[" + num(U) + "];");
+    if (!cols.empty()) col_loads(cols, "c", "(int64_t)blockIdx.x * span");
     L("for (int64_t base = (int64_t)blockIdx.x * span; base < nrows; base += (int64_t)gridDim.x * span) {");
     ++ind;
-    for (int c : cols) L("uint64_t c" + num(c) + "[" + num(U) + "];");
+    for (int k : prefetch) {
+      for (int q = 0; q < 4; ++q) L("uint64_t pw" + num(k) + "_" + num(q) + "[" + num(U) + "];");
+    }
     if (!cols.empty()) {
-      L("#pragma unroll");
-      L("for (int u = 0; u < " + num(U) + "; ++u) {");
-      ++ind;
-      L("const int64_t r_ = base + u * " + num(kBlock) + " + tid;");
-      L("const bool in_ = r_ < nrows;");
-      for (int c : cols) {
-        int w = P.cols[c].width;
-        L("c" + num(c) + "[u] = in_ ? (uint64_t)reinterpret_cast<const " + uint_type(w) + "*>(P.cols[" + num(c) +
-          "].ptr)[r_] : 0ull;");
+      // the columns of the next step are loaded before this step's rows are
+      // processed, so their DRAM latency overlaps the probes of this step
+      for (int c : cols) L("uint64_t n" + num(c) + "[" + num(U) + "];");
+      col_loads(cols, "n", "base + (int64_t)gridDim.x * span");
+      if (!prefetch.empty()) {
+        L("#pragma unroll");
+        L("for (int u = 0; u < " + num(U) + "; ++u) {");
+        ++ind;
+        L("const bool in_ = base + (int64_t)tid * " + num(U) + " + u < nrows;");
+        prefetch_loads();
+        --ind;
+        L("}");
       }
-      --ind;
-      L("}");
     }
     L("#pragma unroll");
     L("for (int u = 0; u < " + num(U) + "; ++u) {");
     ++ind;
-    L("const int64_t row = base + u * " + num(kBlock) + " + tid;");
+    L("const int64_t row = base + (int64_t)tid * " + num(U) + " + u;");
     L("bool act = row < nrows;");
     row = "row";
     if (agg_src) {
@@ -919,6 +1135,12 @@ struct Gen {
     L("} while (0);");
     --ind;
     L("}");
+    if (!cols.empty()) {
+      L("#pragma unroll");
+      L("for (int u = 0; u < " + num(U) + "; ++u) {");
+      for (int c : cols) L("  c" + num(c) + "[u] = n" + num(c) + "[u];");
+      L("}");
+    }
     --ind;
     L("}");
     epilogue();
@@ -928,6 +1150,7 @@ struct Gen {
     const dq_op& op = P.ops[expand_op];
     (void)op;
     std::fill(var.begin(), var.end(), std::string());
+    pending.clear();
     prologue("dq_heavy");
     L("__shared__ uint32_t s_unit;");
     L("const uint32_t nitems = *P.heavy.count < P.heavy.cap ? *P.heavy.count : P.heavy.cap;");
@@ -975,13 +1198,33 @@ Program generate(const DevPipe& P, int expand_op, int refill_op) {
   Gen g(P, expand_op);
   bool has_expand = false;
   for (int i = 0; i < P.nops; ++i) has_expand |= P.ops[i].kind == DQ_OP_EXPAND;
-  g.U = (has_expand || P.source_kind == DQ_SRC_AGG) ? 1 : 2;
-  // tuning knobs: rows per thread and step, minimum resident CTAs per SM
+  g.U = (has_expand || P.source_kind == DQ_SRC_AGG) ? 1 : 4;
+  // tuning knobs: rows per thread and step (1, 2 or 4), minimum resident CTAs per SM
   if (const char* e = getenv("DQ_JIT_ROWS"))
-    if (!has_expand && P.source_kind != DQ_SRC_AGG) g.U = std::min(8, std::max(1, atoi(e)));
+    if (!has_expand && P.source_kind != DQ_SRC_AGG) {
+      int u = atoi(e);
+      g.U = u >= 4 ? 4 : u >= 2 ? 2 : 1;
+    }
   if (const char* e = getenv("DQ_JIT_MIN_BLOCKS")) g.min_blocks = std::min(8, std::max(0, atoi(e)));
+  if (const char* e = getenv("DQ_JIT_LOAD")) {
+    std::string s(e);
+    g.ldfn = s == "nc" ? "__ldg" : s == "plain" ? "ld_plain" : s == "lu" ? "__ldlu" : "__ldcs";
+  }
   g.choose_agg();
-  g.choose_refill(refill_op);
+  const char* no_refill = getenv("DQ_JIT_REFILL");
+  g.choose_refill(no_refill && atoi(no_refill) == 0 ? -1 : refill_op);
+  g.choose_prefetch();
+  const char* no_pf = getenv("DQ_JIT_PREFETCH");
+  if (no_pf && atoi(no_pf) == 0) g.prefetch.clear();
+  if (g.U == 4 && !getenv("DQ_JIT_ROWS")) {
+    // four rows per thread keep enough loads in flight for narrow pipelines;
+    // wide ones (many columns or several early probes) run out of registers
+    std::vector<int> cols;
+    for (int s = 0; s < P.nslots; ++s)
+      if (P.slots[s].kind == DQ_SLOT_COL && std::find(cols.begin(), cols.end(), P.slots[s].src) == cols.end())
+        cols.push_back(P.slots[s].src);
+    if (cols.size() > 3 || g.prefetch.size() > 1) g.U = 2;
+  }
   g.o = "// generated pipeline kernel (dogqc_b200)\n#include \"dq_common.cuh\"\nusing namespace dq;\n\n";
   g.main_kernel();
   Program prog;

@@ -275,9 +275,9 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       R.words = R.val_word + (d.kind == DQ_RES_UNIQUE ? d.npay : d.naggs);
       // join tables get twice the slots the plan asks for (a load factor of at
       // most 1/4 with the reference's default size factor 2): most probes of a
-      // selective join miss, and a miss walks to the next empty slot.  An even
-      // slot count lets probes read aligned slot pairs.
-      if (d.kind == DQ_RES_UNIQUE) cap = (cap * 2 + 1) & ~1ull;
+      // selective join miss, and a miss walks to the next empty slot.  A slot
+      // count divisible by 4 lets probes read aligned 32-byte slot groups.
+      if (d.kind == DQ_RES_UNIQUE) cap = (cap * 2 + 3) & ~3ull;
       cap = std::max<uint64_t>(cap, 16);
       if (cap >= 0xffffffffull) throw DqError(DQ_ERR_UNSUPPORTED, "hash tables hold fewer than 2^32 slots");
       R.cap = cap;
