@@ -9,12 +9,19 @@ Seeded synthetic data with those shapes (no TPC-H data here).
 A step is one execution of the whole plan (dimension build pipeline, fact probe
 + aggregate pipeline, aggregation output pipeline).  ``value`` counts the input
 rows of both tables per second of device time (CUDA events on the engine's
-stream), inputs resident in HBM; the inputs (90 MB) fit in L2, so a 256 MB buffer
-is written between steps.  ``e2e`` runs the same plan through the public API
-with the input columns copied from pinned host memory every step and the result
-read back, timed on the host.  ``roofline`` is for the dominant kernel (the fact
-probe pipeline).  ``--impl reference`` times the CPU oracle (numpy restatement of
-the reference's semantics), partitioned over all host cores.
+stream), inputs resident in HBM; the inputs (90 MB) fit in L2, so between steps
+a 256 MB buffer is written and another 256 MB read (the read writes the dirty
+flush lines back before the timed region).  ``e2e`` runs the same plan through
+the public API with the input columns copied from pinned host memory every step
+and the result read back, timed on the host.  ``roofline`` is for the dominant
+kernel (the slowest pipeline: the fact probe), its algorithmic bytes the columns
+it reads; ``traffic`` is its DRAM bytes from the committed ncu summary
+(profiles/traffic.json).  ``--impl reference`` times the CPU oracle (numpy
+restatement of the reference's semantics), partitioned over all host cores.
+
+``--workload c0|c2|c3`` measures the other configurations the same way (scan-
+filter-aggregate, divergent multimap expansion, three-way star join) for the
+per-pipeline table; the headline line is the default ``c1``.
 """
 import argparse
 import json
@@ -33,8 +40,24 @@ PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 METRIC = "rows/s (FK-PK hash join + aggregate pipeline, input rows of both tables per second)"
 CONFIG = {"workload": "fk_pk_join_agg", "dim_rows": 1_500_000, "fact_rows": 6_000_000,
-          "dim_filter": "segment == 1 (20%)", "groups": 25, "l2": "256 MB flush between steps",
+          "dim_filter": "segment == 1 (20%)", "groups": 25, "l2": "256 MB write + 256 MB read between steps (inputs evicted)",
           "parallelism": "replicas"}
+# the other configurations (parity-test cases; measured with --workload for the
+# per-pipeline roofline table)
+WORKLOADS = {
+    "c0": ("rows/s (scan-filter-aggregate pipeline, input rows per second)",
+           {"workload": "scan_filter_agg", "rows": 6_000_000, "filter": "shipdate <= max-90",
+            "groups": 6, "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c1": (METRIC, CONFIG),
+    "c2": ("rows/s (multimap build + divergent expansion, input rows of both tables per second)",
+           {"workload": "divergent_expansion", "build_rows": 10_000_000, "probe_rows": 16_777_216,
+            "build_keys": "zipf(1.0) over 100,000", "probe_keys": "uniform over 200,000",
+            "filters": "90/50/10/1%", "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c3": ("rows/s (three-way star join + 1M-group aggregate, input rows per second)",
+           {"workload": "star_join_high_cardinality", "fact_rows": 60_000_000,
+            "dim_rows": [1_500_000, 200_000, 10_000], "groups": "~1,000,000",
+            "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+}
 
 
 def hbm_peak():
@@ -46,13 +69,39 @@ def hbm_peak():
 
 
 def load_profile_traffic():
-    """DRAM bytes per launch of the probe kernel from the committed ncu summary."""
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(WORKLOAD, {}).get("probe_pipeline_dram_bytes")
+            return json.load(f).get(WORKLOAD, {}).get("dram_bytes_per_launch")
     except Exception:
         return None
+
+
+def pipeline_bytes(db, lowering, i):
+    """Algorithmic bytes of pipeline i: every column it reads, once, at stored width."""
+    pipe = lowering.pipes[i]
+    if not pipe.table:
+        return 0
+    from dogqc_b200.database import StringColumn
+    table = db[pipe.table]
+    total = 0
+    for c in pipe.cols:
+        col = table.columns[c]
+        if isinstance(col, StringColumn):  # fixed-width strings are read without offsets
+            total += col.chars.nbytes + (0 if col.width else col.offsets.nbytes)
+        else:
+            total += col.nbytes
+    return total
+
+
+def join_pairs(db):
+    """Matching (probe, build) key pairs of the divergent-expansion workload."""
+    import numpy as np
+    b = np.bincount(db["r_build"].columns["r_key"])
+    p = np.bincount(db["s_probe"].columns["s_key"])
+    n = min(len(b), len(p))
+    return int((b[:n].astype(np.int64) * p[:n].astype(np.int64)).sum())
 
 
 class ClockSampler(object):
@@ -155,14 +204,18 @@ def run_ours(args, world, rank, local):
     db = workloads.GENERATORS[WORKLOAD](SCALE)
     plan = build_plan(db)
     rows_per_step = sum(t.size for t in db.tables.values())
-    fact_bytes = db["fact"].nbytes
     engine = Engine(local, tile_rows=args.tile_rows, ctas_per_sm=args.ctas_per_sm, flags=args.engine_flags)
     engine.register_database(db)
     p = engine.prepare(plan)
+    npipes = len(p.lowering.pipes)
+    # L2 flush between steps: write 256 MB (evicts the inputs), then read another
+    # 256 MB, which writes the dirty flush lines back before the timed region
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    evict = torch.zeros(32 << 20, dtype=torch.int64, device="cuda")
 
     def step():
         flush.fill_(1)
+        evict.sum()
         torch.cuda.synchronize()
         res = p.execute()
         return res, p.timing()
@@ -171,42 +224,53 @@ def run_ours(args, world, rank, local):
         res, _ = step()
     dist_barrier(world)
     torch.cuda.synchronize()
-    total_ms, probe_ms, launches = 0.0, 0.0, 0
+    total_ms, launches = 0.0, 0
+    pipe_ms = [0.0] * npipes
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
             res, t = step()
             total_ms += t["total_ms"]
-            probe_ms += t["pipeline_ms"][1]
+            for i in range(npipes):
+                pipe_ms[i] += t["pipeline_ms"][i]
             launches += t["kernel_launches"]
     torch.cuda.synchronize()
     dist_barrier(world)
     total_ms = dist_max(total_ms, world)
-    probe_ms = dist_max(probe_ms, world)
+    pipe_ms = [dist_max(x, world) for x in pipe_ms]
+    dom = max(range(npipes), key=lambda i: pipe_ms[i])   # the dominant pipeline kernel
+    probe_ms = pipe_ms[dom]
+    fact_bytes = pipeline_bytes(db, p.lowering, dom)
     ms_per_step = total_ms / args.steps
     value = rows_per_step * world / (ms_per_step / 1e3)
 
-    # end to end: host columns (pinned) -> device, execute, result back
-    pinned = {}
-    for tname, table in db.tables.items():
-        for cname, col in table.columns.items():
-            arr = np.ascontiguousarray(col)
-            t = torch.from_numpy(arr.view(np.uint8)).pin_memory()
-            pinned[(tname, cname)] = (t, arr.dtype)
-
-    class PinnedTable(object):
-        def __init__(self, table):
-            self.name = table.name
-            self.size = table.size
-            self.types = table.types
-            self.columns = {c: pinned[(table.name, c)][0].numpy().view(pinned[(table.name, c)][1])
-                            for c in table.columns}
-
-    ptables = [PinnedTable(t) for t in db.tables.values()]
-    h2d = sum(t.nbytes for t in db.tables.values())
+    # end to end: host columns (pinned) -> device, execute, result back.  String
+    # columns (a dimension's text) stay resident: the library does not update
+    # them in place, and they are not counted in the copied bytes.
+    from dogqc_b200.database import StringColumn
     d2h_rows = res.nrows
     d2h = sum(c.nbytes for c in res.columns) + 12
     e2e_value = None
+    h2d = 0
     if not args.no_e2e:
+        pinned = {}
+        for tname, table in db.tables.items():
+            for cname, col in table.columns.items():
+                if isinstance(col, StringColumn):
+                    continue
+                arr = np.ascontiguousarray(col)
+                t = torch.from_numpy(arr.view(np.uint8)).pin_memory()
+                pinned[(tname, cname)] = (t, arr.dtype)
+
+        class PinnedTable(object):
+            def __init__(self, table):
+                self.name = table.name
+                self.size = table.size
+                self.types = table.types
+                self.columns = {c: pinned[(table.name, c)][0].numpy().view(pinned[(table.name, c)][1])
+                                for c in table.columns if (table.name, c) in pinned}
+
+        ptables = [PinnedTable(t) for t in db.tables.values()]
+        h2d = sum(t.nbytes for t, _ in pinned.values())
         for _ in range(2):
             for pt in ptables:
                 engine.update_table(pt)
@@ -225,23 +289,31 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = hbm_peak()
     probe_avg_s = probe_ms / args.steps / 1e3
     achieved = fact_bytes / probe_avg_s / 1e9
+    plan_bytes = sum(pipeline_bytes(db, p.lowering, i) for i in range(npipes))
+    metric, config = WORKLOADS[WORKLOAD]
+    kernel = "dq_main (generated kernel of pipeline %d: %s)" % (dom, p.lowering.pipes[dom].table or "scan of a temp table")
+    if args.engine_flags & 12:
+        kernel = "prebuilt %s kernel of pipeline %d" % ("row" if args.engine_flags & 4 else "tile", dom)
     out = {
-        "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
-        "config": CONFIG,
+        "config": config,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": load_profile_traffic(),
-                     "kernel": "pipeline_kernel (fact probe + aggregate)",
+                     "kernel": kernel,
                      "algorithmic_bytes": fact_bytes, "avg_ms": probe_avg_s * 1e3,
                      "peak_source": "%s hbm_gbs (burst copy)" % peak_kind},
-        "plan": {"algorithmic_bytes": sum(t.nbytes for t in db.tables.values()),
-                 "avg_ms": ms_per_step,
-                 "frac": sum(t.nbytes for t in db.tables.values()) / (ms_per_step / 1e3) / 1e9 / peak},
+        "plan": {"algorithmic_bytes": plan_bytes, "avg_ms": ms_per_step,
+                 "frac": plan_bytes / (ms_per_step / 1e3) / 1e9 / peak,
+                 "pipeline_ms": [x / args.steps for x in pipe_ms]},
         "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
+    if WORKLOAD == "c2":
+        pairs = join_pairs(db)
+        out["join_pairs"] = {"pairs": pairs, "pairs_per_s": pairs * world / (ms_per_step / 1e3)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(db, plan)
     engine.close()
@@ -285,18 +357,27 @@ def merge_partials(rows):
     return out
 
 
-def cpu_baseline(db, plan, repeats=2):
-    """Single-threaded oracle over the full workload (bounded: a few seconds per run)."""
+def cpu_baseline(db, plan, repeats=2, max_rows=8_000_000):
+    """Single-threaded oracle over the workload (bounded: a few seconds per run;
+    workloads above `max_rows` input rows run on a proportionally smaller seeded
+    instance of the same shape)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from evaluator import run_plan
+    from dogqc_b200 import workloads
     rows = sum(t.size for t in db.tables.values())
+    what = "full runs of the workload"
+    if rows > max_rows:
+        scale = SCALE * max_rows / rows
+        db = workloads.GENERATORS[WORKLOAD](scale)
+        plan = build_plan(db)
+        rows = sum(t.size for t in db.tables.values())
+        what = "runs of the same workload at scale %.3f" % scale
     t0 = time.perf_counter()
     for _ in range(repeats):
         run_plan(db, plan)
     dt = time.perf_counter() - t0
     return {"value": rows * repeats / dt, "unit": "rows/s", "cores": 1, "kind": "port",
-            "sample": "%d full runs of the workload (%d input rows each) through the numpy oracle"
-                      % (repeats, rows)}
+            "sample": "%d %s (%d input rows each) through the numpy oracle" % (repeats, what, rows)}
 
 
 def run_reference(args, world, rank):
@@ -351,12 +432,20 @@ def main():
     ap.add_argument("--engine-flags", type=int, default=0, help="DQ_CFG_* bits")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="workload size factor (profiling only; the bench line is quoted at 1.0)")
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS),
+                    help="c1 (default): the FK-PK join the headline metric is quoted on; c0, c2, c3: "
+                         "the other configurations, for the per-pipeline table")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    global SCALE
+    global SCALE, WORKLOAD
     SCALE = args.scale
+    WORKLOAD = args.workload
     world, rank, local = dist_setup()
-    if args.impl == "reference":
+    if args.impl == "reference" and WORKLOAD != "c1":
+        out = {"impl": "reference", "unavailable": "the partitioned CPU reference arm covers the c1 workload; "
+                                                   "the others report cpu_baseline in the ours line"}
+        out = out if rank == 0 else None
+    elif args.impl == "reference":
         out = run_reference(args, world, rank)
     else:
         out = run_ours(args, world, rank, local)

@@ -61,9 +61,20 @@ __device__ __forceinline__ uint64_t ldg_w(const uint8_t* p, int w) {
   }
 }
 
-// One 32-byte read-only load (four 64-bit words; p 32-byte aligned).
+// 32 read-only bytes (four 64-bit words; p 32-byte aligned): one 256-bit load
+// where the compiler accepts it (CUDA 12.9 and later for sm_100a, signalled by
+// DQ_LD256), else two 128-bit loads of the same sector.
 __device__ __forceinline__ void ld_nc_32B(const uint64_t* p, uint64_t& a, uint64_t& b, uint64_t& c, uint64_t& d) {
+#if defined(DQ_LD256) && DQ_LD256
   asm volatile("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
+#else
+  const ulonglong2 x = __ldg(reinterpret_cast<const ulonglong2*>(p));
+  const ulonglong2 y = __ldg(reinterpret_cast<const ulonglong2*>(p) + 1);
+  a = x.x;
+  b = x.y;
+  c = y.x;
+  d = y.y;
+#endif
 }
 
 // MurmurHash3 64-bit finaliser (Appleby), used for every hash table.

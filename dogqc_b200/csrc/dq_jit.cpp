@@ -1277,14 +1277,20 @@ void build(Entry& e, const std::string& src) {
   nvrtcProgram prog;
   nvrtc_check(nvrtcCreateProgram(&prog, src.c_str(), "dq_pipeline.cu", (int)hdrs.size(), hdrs.data(), names.data()),
               "nvrtcCreateProgram");
+  // the NVRTC the process resolved (an application may have loaded an older
+  // one first): 256-bit loads for sm_100a need 12.9
+  int major = 0, minor = 0;
+  nvrtcVersion(&major, &minor);
+  const bool ld256 = major > 12 || (major == 12 && minor >= 9);
   const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-lineinfo",
-                        "--ptxas-options=-v"};
+                        "--ptxas-options=-v", ld256 ? "-DDQ_LD256=1" : "-DDQ_LD256=0"};
   nvrtcResult r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
   size_t n = 0;
   nvrtcGetProgramLogSize(prog, &n);
   e.log.assign(n, '\0');
   if (n) nvrtcGetProgramLog(prog, &e.log[0]);
   while (!e.log.empty() && e.log.back() == '\0') e.log.pop_back();
+  e.log = "NVRTC " + std::to_string(major) + "." + std::to_string(minor) + "\n" + e.log;
   if (r != NVRTC_SUCCESS) {
     nvrtcDestroyProgram(&prog);
     throw Error("generated pipeline kernel failed to compile:\n" + e.log);
