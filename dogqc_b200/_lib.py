@@ -91,6 +91,11 @@ class dq_plan_timing(C.Structure):
                 ("kernel_launches", C.c_int32), ("pipeline_ms", C.c_double * MAX_OPS)]
 
 
+class dq_tuning(C.Structure):
+    _fields_ = [("rows_per_thread", C.c_int32), ("block_threads", C.c_int32), ("refill", C.c_int32),
+                ("unique_slots_pct", C.c_int32), ("multi_buckets_pct", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+
 NOALLOC_MAX_BUILD_ROWS = 262144
 NOALLOC_MAX_GROUPS = 4096
 
@@ -105,7 +110,8 @@ class dq_join_agg_args(C.Structure):
 
 def check_layout():
     """Sizes the C compiler gives these structs on x86-64 (LP64)."""
-    expect = {dq_config: 40, dq_column: 40, dq_slot: 8, dq_op: 40, dq_resource: 80, dq_join_agg_args: 104}
+    expect = {dq_config: 40, dq_column: 40, dq_slot: 8, dq_op: 40, dq_resource: 80, dq_join_agg_args: 104,
+              dq_tuning: 32}
     for t, n in expect.items():
         if C.sizeof(t) != n:
             raise AssertionError("%s is %d bytes, header implies %d" % (t.__name__, C.sizeof(t), n))
@@ -138,6 +144,14 @@ EXPORTS = {
     "dq_result_column": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_void_p)]),
     "dq_result_free": (None, [C.c_void_p]),
     "dq_join_agg_noalloc": (C.c_int, [C.POINTER(dq_join_agg_args), C.c_void_p]),
+    "dq_plan_prepare_tuned": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_desc), C.POINTER(dq_tuning),
+                                        C.POINTER(C.c_void_p)]),
+    "dq_batch_prepare": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(dq_plan_desc), C.POINTER(dq_tuning),
+                                   C.POINTER(C.c_void_p)]),
+    "dq_batch_execute": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "dq_batch_timing_get": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_timing)]),
+    "dq_batch_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "dq_batch_free": (None, [C.c_void_p]),
 }
 
 

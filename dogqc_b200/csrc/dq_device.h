@@ -117,4 +117,37 @@ struct DevPipe {
   uint64_t* scratch_ll;        // misc device counters
 };
 
+// ---------------------------------------------------------------- batches --
+// A batch runs many instances of one plan shape: these descriptors let one
+// launch reset, scan or pack the per-instance buffers of all instances.
+
+struct BatchReset {       // one buffer to reset before a batch run
+  void* ptr;
+  uint64_t n;             // 64-bit words (kind 0), 32-bit words (kind 1), slots (kind 2)
+  uint64_t value;         // kinds 0 and 1
+  uint64_t reds;          // kind 2: 4 bits of dq_red_kind per aggregate
+  int32_t kind;           // 0: fill u64, 1: fill u32, 2: aggregation table
+  int32_t words;          // kind 2: words per slot
+  int32_t val_word;       // kind 2: first accumulator word
+  int32_t naggs;          // kind 2
+};
+
+struct BatchScanSeg {     // one multimap's bucket counts -> offsets
+  uint32_t* counts;
+  uint32_t* offsets;
+  uint64_t n;             // buckets
+  uint64_t block0;        // first scan block of this segment
+  uint64_t nblocks;
+};
+
+struct BatchPack {        // one output column of one instance
+  const uint8_t* src;
+  const uint64_t* cursor; // rows emitted (may exceed cap on overflow)
+  uint64_t cap;
+  uint64_t dst;           // byte offset in the packed buffer
+  uint64_t* rows_out;     // where the kernel records min(cursor, cap)
+  int32_t width;
+  int32_t pad;
+};
+
 }  // namespace dq

@@ -174,6 +174,10 @@ struct Gen {
   int nbuf = 0;                  // values per row in the warp buffers
   int buf_off = 0;               // shared-memory offset of the warp buffers
   std::string ldfn = "__ldcs";   // load function of streamed source columns
+  int block = kBlock;            // threads per CTA
+  bool batched = false;          // kernel over many instances of the plan
+  // whether the current step is the lane's last (the refill buffer drains then)
+  std::string last_step = "base + (int64_t)gridDim.x * span >= nrows";
 
   Gen(const DevPipe& p, int e) : P(p), expand_op(e), var(p.nslots) {}
 
@@ -812,7 +816,7 @@ struct Gen {
       return;
     }
     ns = R.smem_slots;
-    if (ns <= 0 || !R.packed) {
+    if (ns <= 0 || !R.packed || batched) {  // a batched kernel's items change instance
       agg = AGG_GLOBAL;
       ns = 0;
       return;
@@ -852,7 +856,7 @@ struct Gen {
     nbuf = (int)live_after(k + 1, 0).size() + (reads_strings_after(k + 1) ? 1 : 0);
     if (nbuf == 0) nbuf = 1;
     buf_off = (smem + 15) / 16 * 16;
-    smem = buf_off + (kBlock / 32) * kWarpBuf * nbuf * 8;
+    smem = buf_off + (block / 32) * kWarpBuf * nbuf * 8;
   }
 
   // Appends the active lanes' live values to the warp's buffer, then drains
@@ -880,7 +884,7 @@ struct Gen {
     --ind;
     L("} while (0);");
     L("__syncwarp();");
-    L("const bool last_ = base + (int64_t)gridDim.x * span >= nrows && u == " + num(U - 1) + ";");
+    L("const bool last_ = " + last_step + " && u == " + num(U - 1) + ";");
     L("while (wn >= 32 || (last_ && wn > 0)) {");
     ++ind;
     L("bool ra = lane < wn;");
@@ -931,8 +935,8 @@ struct Gen {
     }
     L("uint64_t* ltags = reinterpret_cast<uint64_t*>(smem);");
     L("uint64_t* lacc = ltags + " + num(ns + 1) + ";");
-    L("for (int i = tid; i <= " + num(ns) + "; i += " + num(kBlock) + ") ltags[i] = kEmpty;");
-    L("for (int i = tid; i < " + num((ns + 1) * R.naggs * copies) + "; i += " + num(kBlock) + ")");
+    L("for (int i = tid; i <= " + num(ns) + "; i += " + num(block) + ") ltags[i] = kEmpty;");
+    L("for (int i = tid; i < " + num((ns + 1) * R.naggs * copies) + "; i += " + num(block) + ")");
     L("  lacc[i] = ((" + lit(min_mask()) + " >> ((i / " + num(copies) + ") % " + num(R.naggs) +
       ")) & 1ull) ? ~0ull : 0ull;");
     L("__syncthreads();");
@@ -955,7 +959,7 @@ struct Gen {
     uint64_t packed_reds = 0;
     for (int j = 0; j < R.naggs; ++j) packed_reds |= (uint64_t)(R.agg_red[j] & 15) << (4 * j);
     L("__syncthreads();");
-    L("for (int i = tid; i < " + num((ns + 1) * R.naggs) + "; i += " + num(kBlock) + ") {");
+    L("for (int i = tid; i < " + num((ns + 1) * R.naggs) + "; i += " + num(block) + ") {");
     ++ind;
     L("const int s_ = i / " + num(R.naggs) + ", j_ = i % " + num(R.naggs) + ";");
     L("uint64_t tg_ = ltags[s_];");
@@ -973,7 +977,7 @@ struct Gen {
   }
 
   void prologue(const char* name) {
-    L(std::string("extern \"C\" __global__ void __launch_bounds__(") + num(kBlock) +
+    L(std::string("extern \"C\" __global__ void __launch_bounds__(") + num(block) +
       (min_blocks > 0 ? ", " + num(min_blocks) : std::string()) + ") " + name + "(const __grid_constant__ DevPipe P) {");
     ++ind;
     L("extern __shared__ __align__(16) uint8_t smem[];");
@@ -1056,13 +1060,9 @@ struct Gen {
   // ----------------------------------------------------------- kernels --
   void main_kernel() {
     prologue("dq_main");
-    const bool agg_src = P.source_kind == DQ_SRC_AGG;
-    std::vector<int> cols;  // staged columns read by COL slots
-    for (int s = 0; s < P.nslots; ++s)
-      if (slot(s).kind == DQ_SLOT_COL && std::find(cols.begin(), cols.end(), slot(s).src) == cols.end())
-        cols.push_back(slot(s).src);
+    std::vector<int> cols = source_cols();
     L("const int64_t nrows = source_rows(P);");
-    L("const int64_t span = " + num((long long)kBlock * U) + ";");
+    L("const int64_t span = " + num((long long)block * U) + ";");
     if (refill >= 0) {
       L("uint64_t* const wb = reinterpret_cast<uint64_t*>(smem + " + num(buf_off) + ") + (tid >> 5) * " +
         num(kWarpBuf * nbuf) + ";  // this warp's refill buffer");
@@ -1090,6 +1090,30 @@ struct Gen {
         L("}");
       }
     }
+    row_loop();
+    if (!cols.empty()) {
+      L("#pragma unroll");
+      L("for (int u = 0; u < " + num(U) + "; ++u) {");
+      for (int c : cols) L("  c" + num(c) + "[u] = n" + num(c) + "[u];");
+      L("}");
+    }
+    --ind;
+    L("}");
+    epilogue();
+  }
+
+  std::vector<int> source_cols() const {
+    std::vector<int> cols;  // staged columns read by COL slots
+    for (int s = 0; s < P.nslots; ++s)
+      if (slot(s).kind == DQ_SLOT_COL && std::find(cols.begin(), cols.end(), slot(s).src) == cols.end())
+        cols.push_back(slot(s).src);
+    return cols;
+  }
+
+  // The U rows of the thread in the current step: slot values, then the ops.
+  // Expects base, nrows, c<col>[u] (and the prefetched probe groups) in scope.
+  void row_loop() {
+    const bool agg_src = P.source_kind == DQ_SRC_AGG;
     L("#pragma unroll");
     L("for (int u = 0; u < " + num(U) + "; ++u) {");
     ++ind;
@@ -1135,15 +1159,64 @@ struct Gen {
     L("} while (0);");
     --ind;
     L("}");
-    if (!cols.empty()) {
-      L("#pragma unroll");
-      L("for (int u = 0; u < " + num(U) + "; ++u) {");
-      for (int c : cols) L("  c" + num(c) + "[u] = n" + num(c) + "[u];");
-      L("}");
+  }
+
+  // Many instances of the plan (same shape, own tables) in one launch: the
+  // work items are the row blocks of all instances (prefix bprefix over the
+  // instances); a CTA takes items grid-stride, binds the item's instance
+  // descriptor, drains its lane-refill buffer and flushes its aggregates at the
+  // end of every item.
+  void batch_kernel() {
+    L(std::string("extern \"C\" __global__ void __launch_bounds__(") + num(block) +
+      (min_blocks > 0 ? ", " + num(min_blocks) : std::string()) +
+      ") dq_batch_main(const DevPipe* __restrict__ Ps, const int64_t* __restrict__ bprefix, int ninst) {");
+    ++ind;
+    L("extern __shared__ __align__(16) uint8_t smem[];");
+    L("if (*(volatile int32_t*)Ps[0].status & (kErrHtFull | kErrTimeout)) return;");
+    L("const int tid = threadIdx.x, lane = tid & 31;");
+    L("(void)smem;");
+    L("(void)lane;");
+    L("const int64_t span = " + num((long long)block * U) + ";");
+    if (refill >= 0) {
+      L("uint64_t* const wb = reinterpret_cast<uint64_t*>(smem + " + num(buf_off) + ") + (tid >> 5) * " +
+        num(kWarpBuf * nbuf) + ";  // this warp's refill buffer");
+      L("int wn = 0;  // rows in it");
     }
+    L("const int64_t total = bprefix[ninst];");
+    L("for (int64_t blk = blockIdx.x; blk < total; blk += gridDim.x) {");
+    ++ind;
+    L("int lo = 0, hi = ninst;");
+    L("while (hi - lo > 1) {");
+    L("  const int mid = (lo + hi) >> 1;");
+    L("  if (bprefix[mid] <= blk) lo = mid; else hi = mid;");
+    L("}");
+    L("const DevPipe& P = Ps[lo];");
+    L("const int64_t nrows = source_rows(P);");
+    L("const int64_t base = (blk - bprefix[lo]) * span;");
+    agg_init();
+    std::vector<int> cols = source_cols();
+    for (int c : cols) L("uint64_t c" + num(c) + "[" + num(U) + "];");
+    for (int k : prefetch)
+      for (int q = 0; q < 4; ++q) L("uint64_t pw" + num(k) + "_" + num(q) + "[" + num(U) + "];");
+    if (!cols.empty()) {
+      col_loads(cols, "c", "base");
+      if (!prefetch.empty()) {
+        L("#pragma unroll");
+        L("for (int u = 0; u < " + num(U) + "; ++u) {");
+        ++ind;
+        L("const bool in_ = base + (int64_t)tid * " + num(U) + " + u < nrows;");
+        prefetch_loads();
+        --ind;
+        L("}");
+      }
+    }
+    last_step = "true";
+    row_loop();
+    agg_flush();
     --ind;
     L("}");
-    epilogue();
+    --ind;
+    L("}");
   }
 
   void heavy_kernel() {
@@ -1177,7 +1250,7 @@ struct Gen {
         var[s] = "h" + num(s);
         L("const uint64_t " + var[s] + " = it[" + num(2 + slot(s).stash) + "];");
       }
-    L("for (uint32_t pb = 0; pb < len; pb += " + num(kBlock) + "u) {");
+    L("for (uint32_t pb = 0; pb < len; pb += " + num(block) + "u) {");
     ++ind;
     L("const uint32_t q = pb + (uint32_t)tid;");
     L("bool a = q < len;");
@@ -1194,17 +1267,18 @@ struct Gen {
 
 }  // namespace
 
-Program generate(const DevPipe& P, int expand_op, int refill_op) {
-  Gen g(P, expand_op);
+Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t) {
+  Gen g(P, t.batched ? -1 : expand_op);
+  g.batched = t.batched;
+  if (t.block == 128 || t.block == 256 || t.block == 512) g.block = t.block;
   bool has_expand = false;
   for (int i = 0; i < P.nops; ++i) has_expand |= P.ops[i].kind == DQ_OP_EXPAND;
   g.U = (has_expand || P.source_kind == DQ_SRC_AGG) ? 1 : 4;
   // tuning knobs: rows per thread and step (1, 2 or 4), minimum resident CTAs per SM
-  if (const char* e = getenv("DQ_JIT_ROWS"))
-    if (!has_expand && P.source_kind != DQ_SRC_AGG) {
-      int u = atoi(e);
-      g.U = u >= 4 ? 4 : u >= 2 ? 2 : 1;
-    }
+  int rows = t.rows_per_thread;
+  if (const char* e = getenv("DQ_JIT_ROWS")) rows = atoi(e);
+  if (rows > 0 && !has_expand && P.source_kind != DQ_SRC_AGG) g.U = rows >= 4 ? 4 : rows >= 2 ? 2 : 1;
+  if (t.refill < 0) refill_op = -1;
   if (const char* e = getenv("DQ_JIT_MIN_BLOCKS")) g.min_blocks = std::min(8, std::max(0, atoi(e)));
   if (const char* e = getenv("DQ_JIT_LOAD")) {
     std::string s(e);
@@ -1216,7 +1290,7 @@ Program generate(const DevPipe& P, int expand_op, int refill_op) {
   g.choose_prefetch();
   const char* no_pf = getenv("DQ_JIT_PREFETCH");
   if (no_pf && atoi(no_pf) == 0) g.prefetch.clear();
-  if (g.U == 4 && !getenv("DQ_JIT_ROWS")) {
+  if (g.U == 4 && rows <= 0) {
     // four rows per thread keep enough loads in flight for narrow pipelines;
     // wide ones (many columns or several early probes) run out of registers
     std::vector<int> cols;
@@ -1226,8 +1300,17 @@ Program generate(const DevPipe& P, int expand_op, int refill_op) {
     if (cols.size() > 3 || g.prefetch.size() > 1) g.U = 2;
   }
   g.o = "// generated pipeline kernel (dogqc_b200)\n#include \"dq_common.cuh\"\nusing namespace dq;\n\n";
-  g.main_kernel();
   Program prog;
+  prog.block = g.block;
+  if (t.batched) {
+    g.batch_kernel();
+    prog.source = g.o;
+    prog.smem_bytes = g.smem;
+    prog.rows_per_thread = g.U;
+    prog.batched = true;
+    return prog;
+  }
+  g.main_kernel();
   if (expand_op >= 0) {
     g.o += "\n";
     g.heavy_kernel();
@@ -1319,7 +1402,7 @@ Kernels compile(const Program& prog, bool load) {
       e.lib = nullptr;
       throw Error(std::string("loading a generated pipeline kernel: ") + cudaGetErrorString(err));
     }
-    err = cudaLibraryGetKernel(&e.main, e.lib, "dq_main");
+    err = cudaLibraryGetKernel(&e.main, e.lib, prog.batched ? "dq_batch_main" : "dq_main");
     if (err == cudaSuccess && prog.heavy) err = cudaLibraryGetKernel(&e.heavy, e.lib, "dq_heavy");
     if (err != cudaSuccess) throw Error(std::string("generated kernel entry: ") + cudaGetErrorString(err));
   }

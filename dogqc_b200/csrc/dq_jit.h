@@ -27,7 +27,9 @@ struct Program {
   std::string source;
   int smem_bytes = 0;        // dynamic shared memory of both kernels
   int rows_per_thread = 1;   // rows one thread takes per grid-stride step
+  int block = kThreads;      // threads per CTA
   bool heavy = false;        // second kernel for deferred expansion ranges
+  bool batched = false;      // one kernel `dq_batch_main` over many instances
 };
 
 struct Kernels {
@@ -36,12 +38,21 @@ struct Kernels {
   std::string log;           // compiler log (register and spill report)
 };
 
+// Launch-shape choices an autotuner may override (0 / default: the
+// generator's own choice).
+struct Tuning {
+  bool batched = false;      // generate the many-instance kernel
+  int rows_per_thread = 0;   // 1, 2 or 4
+  int block = 0;             // 128, 256 or 512 threads per CTA
+  int refill = 0;            // -1: no lane refill; 0: the plan's refill point
+};
+
 // Source of the kernels for one pipeline.  `P` is the launch descriptor the
 // runtime filled (resource layouts, slots with their staged-column indices,
 // stash indices); `expand_op` is the expansion whose wide ranges are deferred
 // to the second kernel (-1: none); `refill_op` is the selective filter or
 // probe after which the warps refill their lanes from a buffer (-1: none).
-Program generate(const DevPipe& P, int expand_op, int refill_op);
+Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t = Tuning());
 
 // Compiles the program (cached by source text) and, with `load`, loads it.
 Kernels compile(const Program& prog, bool load);

@@ -1288,6 +1288,109 @@ __global__ void heavy_prefix_kernel(const uint64_t* items, const uint32_t* count
   if (threadIdx.x == 0) prefix[n] = carry;
 }
 
+// ------------------------------------------------------- batch helpers --
+
+// Resets every per-instance buffer of a batch in one launch; each CTA walks
+// all descriptors (starting at a rotated one) and strides over its share.
+__global__ void batch_reset_kernel(const BatchReset* ops, int nops) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (int k = 0; k < nops; ++k) {
+    const int o = (int)((blockIdx.x + (unsigned)k) % (unsigned)nops);
+    const BatchReset op = ops[o];
+    const uint64_t start = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (op.kind == 0) {
+      uint64_t* p = reinterpret_cast<uint64_t*>(op.ptr);
+      for (uint64_t i = start; i < op.n; i += stride) p[i] = op.value;
+    } else if (op.kind == 1) {
+      uint32_t* p = reinterpret_cast<uint32_t*>(op.ptr);
+      for (uint64_t i = start; i < op.n; i += stride) p[i] = (uint32_t)op.value;
+    } else {
+      uint64_t* p = reinterpret_cast<uint64_t*>(op.ptr);
+      const uint64_t total = op.n * (uint64_t)op.words;
+      for (uint64_t i = start; i < total; i += stride) {
+        const int w = (int)(i % (uint64_t)op.words);
+        uint64_t v = kEmpty;
+        if (w >= op.val_word && w < op.val_word + op.naggs) v = red_init((int)((op.reds >> (4 * (w - op.val_word))) & 15));
+        p[i] = v;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int batch_seg_of(const BatchScanSeg* segs, int nseg, uint64_t block) {
+  int lo = 0, hi = nseg;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (segs[mid].block0 <= block) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Segmented form of the three-pass multimap bucket scan: scan block b belongs to
+// the segment (multimap of one instance) whose block range holds b.
+__global__ void batch_scan_partials(const BatchScanSeg* segs, int nseg, uint32_t* partials) {
+  const uint64_t b = blockIdx.x;
+  const BatchScanSeg s = segs[batch_seg_of(segs, nseg, b)];
+  const uint64_t base = (b - s.block0) * kScanChunk;
+  uint32_t sum = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    const uint64_t i = base + (uint64_t)k * kThreads + threadIdx.x;
+    if (i < s.n) sum += s.counts[i];
+  }
+  uint32_t excl;
+  const uint32_t total = block_exclusive_scan(sum, excl);
+  if (threadIdx.x == 0) partials[b] = total;
+}
+
+__global__ void batch_scan_top(const BatchScanSeg* segs, uint32_t* partials) {
+  const BatchScanSeg s = segs[blockIdx.x];
+  uint32_t carry = 0;
+  for (uint64_t base = 0; base < s.nblocks; base += kThreads) {
+    const uint64_t i = base + threadIdx.x;
+    const uint32_t x = i < s.nblocks ? partials[s.block0 + i] : 0;
+    uint32_t excl;
+    const uint32_t total = block_exclusive_scan(x, excl);
+    if (i < s.nblocks) partials[s.block0 + i] = carry + excl;
+    carry += total;
+  }
+}
+
+__global__ void batch_scan_final(const BatchScanSeg* segs, int nseg, const uint32_t* partials) {
+  const uint64_t b = blockIdx.x;
+  const BatchScanSeg s = segs[batch_seg_of(segs, nseg, b)];
+  const uint64_t i0 = (b - s.block0) * kScanChunk + (uint64_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t sum = 0;
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = (i0 + k < s.n) ? s.counts[i0 + k] : 0;
+    sum += v[k];
+  }
+  uint32_t excl;
+  block_exclusive_scan(sum, excl);
+  uint32_t run = partials[b] + excl;
+  for (int k = 0; k < kScanItems; ++k) {
+    if (i0 + k < s.n) {
+      s.offsets[i0 + k] = run;
+      s.counts[i0 + k] = 0;
+    }
+    run += v[k];
+  }
+}
+
+// Copies every instance's output columns (the rows emitted, at most the
+// capacity) into one buffer that a single device-to-host copy returns.
+__global__ void batch_pack_kernel(const BatchPack* ops, int nops, uint8_t* dst) {
+  for (int o = blockIdx.x; o < nops; o += gridDim.x) {
+    const BatchPack op = ops[o];
+    uint64_t n = *op.cursor;
+    if (n > op.cap) n = op.cap;
+    const uint64_t bytes = n * (uint64_t)op.width;
+    for (uint64_t i = threadIdx.x; i < bytes; i += blockDim.x) dst[op.dst + i] = op.src[i];
+    if (threadIdx.x == 0 && op.rows_out) *op.rows_out = n;
+  }
+}
+
 }  // namespace dq
 
 // ------------------------------------------------------ host-side launchers --
@@ -1345,6 +1448,29 @@ cudaError_t launch_mm_scan(uint32_t* counts, uint32_t* offsets, uint64_t n, uint
   mm_scan_top<<<1, kThreads, 0, stream>>>(partials, nblocks);
   mm_scan_final<<<nblocks, kThreads, 0, stream>>>(counts, offsets, n, partials);
   *launches += 3;
+  return cudaGetLastError();
+}
+
+size_t batch_scan_blocks(uint64_t n) { return (size_t)((n + kScanChunk - 1) / kScanChunk); }
+
+cudaError_t launch_batch_reset(const BatchReset* ops, int nops, int sms, cudaStream_t stream) {
+  if (nops <= 0) return cudaSuccess;
+  batch_reset_kernel<<<sms * 4, 256, 0, stream>>>(ops, nops);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_scan(const BatchScanSeg* segs, int nseg, uint64_t total_blocks, uint32_t* partials,
+                              cudaStream_t stream) {
+  if (nseg <= 0 || total_blocks == 0) return cudaSuccess;
+  batch_scan_partials<<<(unsigned)total_blocks, kThreads, 0, stream>>>(segs, nseg, partials);
+  batch_scan_top<<<nseg, kThreads, 0, stream>>>(segs, partials);
+  batch_scan_final<<<(unsigned)total_blocks, kThreads, 0, stream>>>(segs, nseg, partials);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_pack(const BatchPack* ops, int nops, uint8_t* dst, int sms, cudaStream_t stream) {
+  if (nops <= 0) return cudaSuccess;
+  batch_pack_kernel<<<sms * 2, 256, 0, stream>>>(ops, nops, dst);
   return cudaGetLastError();
 }
 

@@ -35,6 +35,11 @@ size_t mm_scan_scratch_words(uint64_t n);
 cudaError_t launch_mm_scan(uint32_t* counts, uint32_t* offsets, uint64_t n, uint32_t* partials,
                            cudaStream_t stream, int* launches);
 cudaError_t launch_heavy_prefix(const DevHeavy& H, uint64_t exp_cap, cudaStream_t stream);
+size_t batch_scan_blocks(uint64_t n);
+cudaError_t launch_batch_reset(const BatchReset* ops, int nops, int sms, cudaStream_t stream);
+cudaError_t launch_batch_scan(const BatchScanSeg* segs, int nseg, uint64_t total_blocks, uint32_t* partials,
+                              cudaStream_t stream);
+cudaError_t launch_batch_pack(const BatchPack* ops, int nops, uint8_t* dst, int sms, cudaStream_t stream);
 }  // namespace dq
 
 using namespace dq;
@@ -177,14 +182,62 @@ struct dq_result {
   std::vector<std::vector<uint8_t>> cols;
 };
 
+// How a plan is laid out: standalone (the default) or as one instance of a
+// batch, with the join-table sizing an autotuner may change.
+struct PlanOpts {
+  bool batch_member = false;  // no standalone kernels, no deferred expansion
+  int unique_pct = 200;       // join-table slots, % of the plan's capacity
+  int multi_pct = 100;        // multimap buckets, % of the plan's capacity
+  jit::Tuning tuning;
+};
+
 struct dq_plan {
   dq_ctx* ctx = nullptr;
+  PlanOpts opts;
   std::vector<std::unique_ptr<ResRec>> res;
   std::vector<std::unique_ptr<PipeRec>> pipes;
   int result_res = -1;
   DevBuf status, counters;
   dq_plan_timing timing{};
   std::vector<cudaEvent_t> events;
+};
+
+// One pipeline of a batch: a generated kernel over all instances.
+struct BatchStage {
+  jit::Program prog;
+  jit::Kernels kernels;
+  DevBuf descs;             // the instances' launch descriptors (DevPipe[ninst])
+  DevBuf bprefix;           // row blocks of the instances before each (int64[ninst + 1])
+  int grid = 1;
+  bool mm_scan = false;     // a multimap count: the bucket scan of every instance follows
+  DevBuf segs, partials;
+  int nsegs = 0;
+  uint64_t scan_blocks = 0;
+};
+
+struct dq_batch {
+  dq_ctx* ctx = nullptr;
+  int ninst = 0;
+  std::vector<std::unique_ptr<dq_plan>> inst;
+  std::vector<std::unique_ptr<BatchStage>> stages;
+  DevBuf status, resets, packs, packed, rows;
+  int nresets = 0, npacks = 0;
+  size_t packed_bytes = 0;
+  std::vector<std::vector<uint64_t>> col_off;   // [instance][column] offset in the packed buffer
+  uint8_t* host = nullptr;                      // pinned: packed columns, rows per instance, status
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  dq_plan_timing timing{};
+  int launches = 0;
+  jit::Tuning tuning;
+  ~dq_batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (host) cudaFreeHost(host);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
 };
 
 namespace {
@@ -277,7 +330,7 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       // most 1/4 with the reference's default size factor 2): most probes of a
       // selective join miss, and a miss walks to the next empty slot.  A slot
       // count divisible by 4 lets probes read aligned 32-byte slot groups.
-      if (d.kind == DQ_RES_UNIQUE) cap = (cap * 2 + 3) & ~3ull;
+      if (d.kind == DQ_RES_UNIQUE) cap = (cap * (uint64_t)std::max(plan->opts.unique_pct, 25) / 100 + 3) & ~3ull;
       cap = std::max<uint64_t>(cap, 16);
       if (cap >= 0xffffffffull) throw DqError(DQ_ERR_UNSUPPORTED, "hash tables hold fewer than 2^32 slots");
       R.cap = cap;
@@ -294,6 +347,7 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       break;
     }
     case DQ_RES_MULTI: {
+      cap = std::max<uint64_t>(1, cap * (uint64_t)std::max(plan->opts.multi_pct, 10) / 100);
       if (cap >= 0xffffffffull) throw DqError(DQ_ERR_UNSUPPORTED, "multimaps hold fewer than 2^32 buckets");
       R.cap = cap;
       r.counts.alloc(cap * 4);
@@ -561,7 +615,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
 
   // deferred wide expansion ranges for the first level-0 expansion
   p.expand_op = -1;
-  for (int i = 0; i < d.nops; ++i) {
+  for (int i = 0; i < d.nops && !plan->opts.batch_member; ++i) {
     const dq_op& op = d.ops[i];
     if (op.kind != DQ_OP_EXPAND) continue;
     bool level0 = true;
@@ -649,17 +703,19 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   P.smem_bytes = fixed + P.nstage * P.stage_bytes;
 
   // generated kernel (default), else the prebuilt tile or row kernel
-  p.jit = !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL));
+  p.jit = !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) && !plan->opts.batch_member;
   int occ = 1;
   int64_t rows_per_cta = tile;
-  if (p.jit) {
-    p.prog = jit::generate(P, p.expand_op, d.compact - 1);
+  if (plan->opts.batch_member) {
+    // the batch launches its own many-instance kernels
+  } else if (p.jit) {
+    p.prog = jit::generate(P, p.expand_op, d.compact - 1, plan->opts.tuning);
     p.kernels = jit::compile(p.prog, !ctx->offline);
-    rows_per_cta = (int64_t)kThreads * p.prog.rows_per_thread;
+    rows_per_cta = (int64_t)p.prog.block * p.prog.rows_per_thread;
     if (!ctx->offline) {
       const void* fn = (const void*)p.kernels.main;
       DQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, p.prog.smem_bytes));
-      DQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kThreads, p.prog.smem_bytes));
+      DQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, p.prog.block, p.prog.smem_bytes));
       if (p.kernels.heavy)
         DQ_CUDA(cudaFuncSetAttribute((const void*)p.kernels.heavy, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      p.prog.smem_bytes));
@@ -677,9 +733,9 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   }
 }
 
-cudaError_t launch_generated(cudaKernel_t k, const DevPipe& P, int grid, int smem, cudaStream_t st) {
+cudaError_t launch_generated(cudaKernel_t k, const DevPipe& P, int grid, int block, int smem, cudaStream_t st) {
   void* args[] = {(void*)&P};
-  return cudaLaunchKernel((const void*)k, dim3(grid), dim3(kThreads), args, (size_t)smem, st);
+  return cudaLaunchKernel((const void*)k, dim3(grid), dim3(block), args, (size_t)smem, st);
 }
 
 void free_events(dq_plan* plan) {
@@ -727,7 +783,7 @@ int run_once(dq_plan* plan, cudaStream_t st) {
     p.dev.tile_counter = counters + 2 * i;
     DQ_CUDA(cudaEventRecord(plan->events[1 + 2 * i], st));
     if (p.expand_op >= 0) DQ_CUDA(cudaMemsetAsync(p.heavy_count.ptr, 0, 8, st));
-    if (p.jit) DQ_CUDA(launch_generated(p.kernels.main, p.dev, p.grid, p.prog.smem_bytes, st));
+    if (p.jit) DQ_CUDA(launch_generated(p.kernels.main, p.dev, p.grid, p.prog.block, p.prog.smem_bytes, st));
     else DQ_CUDA(p.row ? launch_row(p.dev, p.grid, st) : launch_pipeline(p.dev, p.grid, st));
     ++launches;
     if (p.expand_op >= 0) {
@@ -735,7 +791,7 @@ int run_once(dq_plan* plan, cudaStream_t st) {
       DevPipe H = p.dev;
       H.mode = 1;
       H.tile_counter = counters + 2 * i + 1;
-      if (p.jit) DQ_CUDA(launch_generated(p.kernels.heavy, H, p.grid_full, p.prog.smem_bytes, st));
+      if (p.jit) DQ_CUDA(launch_generated(p.kernels.heavy, H, p.grid_full, p.prog.block, p.prog.smem_bytes, st));
       else DQ_CUDA(launch_pipeline(H, p.grid_full, st));
       launches += 2;
     }
@@ -771,6 +827,279 @@ int run_once(dq_plan* plan, cudaStream_t st) {
 // Re-derives every pipeline's copy of the resource descriptors.
 void refresh_pipelines(dq_plan* plan) {
   for (auto& pp : plan->pipes) setup_pipeline(plan, *pp);
+}
+
+// Lays out a plan's resources and pipelines (the caller holds the context lock
+// and has made the device current).
+std::unique_ptr<dq_plan> make_plan(dq_ctx* ctx, const dq_plan_desc* desc, const PlanOpts& opts) {
+  if (desc->abi_version != DQ_ABI_VERSION) throw DqError(DQ_ERR_BAD_IR, "IR version mismatch");
+  if (desc->nres < 0 || desc->npipes <= 0 || (desc->nres && !desc->res) || !desc->pipes)
+    throw DqError(DQ_ERR_BAD_IR, "empty plan");
+  std::unique_ptr<dq_plan> plan(new dq_plan());
+  plan->ctx = ctx;
+  plan->opts = opts;
+  plan->status.alloc(4);
+  plan->counters.alloc(8 * (size_t)desc->npipes);
+  // row bound for multimap payloads: rows of the source of the pipeline that scatters into it
+  std::vector<int64_t> bound(desc->nres, 1);
+  for (int i = 0; i < desc->npipes; ++i) {
+    const dq_pipeline& d = desc->pipes[i];
+    if (d.nops <= 0 || d.nops > DQ_MAX_OPS) throw DqError(DQ_ERR_BAD_IR, "bad op count");
+    const dq_op& sink = d.ops[d.nops - 1];
+    if ((sink.kind == DQ_OP_MM_SCATTER || sink.kind == DQ_OP_MM_COUNT) && sink.res >= 0 && sink.res < desc->nres) {
+      int64_t rows = 1 << 20;
+      if (d.source_kind == DQ_SRC_TABLE && d.table) {
+        auto it = ctx->tables.find(d.table);
+        if (it != ctx->tables.end()) rows = it->second.nrows;
+      } else if (d.source_kind == DQ_SRC_OUTPUT && d.source_res >= 0 && d.source_res < desc->nres) {
+        rows = desc->res[d.source_res].capacity;
+      }
+      bound[sink.res] = std::max(bound[sink.res], rows);
+    }
+  }
+  for (int i = 0; i < desc->nres; ++i) {
+    std::unique_ptr<ResRec> r(new ResRec());
+    r->desc = desc->res[i];
+    r->name = desc->res[i].name ? desc->res[i].name : "";
+    r->desc.name = nullptr;
+    setup_resource(plan.get(), *r, bound[i]);
+    plan->res.push_back(std::move(r));
+  }
+  for (int i = 0; i < desc->npipes; ++i) {
+    std::unique_ptr<PipeRec> p(new PipeRec());
+    p->desc = desc->pipes[i];
+    // keep string arguments alive
+    for (int c = 0; c < p->desc.ncols; ++c) p->col_names.push_back(p->desc.cols[c] ? p->desc.cols[c] : "");
+    for (int c = 0; c < p->desc.ncols; ++c) p->desc.cols[c] = p->col_names[c].c_str();
+    p->desc.table = nullptr;
+    std::string tname = desc->pipes[i].table ? desc->pipes[i].table : "";
+    p->col_names.push_back(tname);
+    p->desc.table = p->col_names.back().c_str();
+    for (int c = 0; c < p->desc.npatterns; ++c) p->patterns.push_back(p->desc.patterns[c] ? p->desc.patterns[c] : "");
+    for (int c = 0; c < p->desc.npatterns; ++c) p->desc.patterns[c] = p->patterns[c].c_str();
+    plan->pipes.push_back(std::move(p));
+  }
+  // the col_names vector may have reallocated: re-point
+  for (auto& p : plan->pipes) {
+    for (int c = 0; c < p->desc.ncols; ++c) p->desc.cols[c] = p->col_names[c].c_str();
+    p->desc.table = p->col_names.back().c_str();
+    for (int c = 0; c < p->desc.npatterns; ++c) p->desc.patterns[c] = p->patterns[c].c_str();
+  }
+  refresh_pipelines(plan.get());
+  plan->result_res = desc->result_res;
+  if (plan->result_res < 0 || plan->result_res >= desc->nres || plan->res[plan->result_res]->desc.kind != DQ_RES_OUTPUT)
+    throw DqError(DQ_ERR_BAD_IR, "result must be an OUTPUT resource");
+  return plan;
+}
+
+// Grows the tables a failed run overflowed (device status bits) and re-derives
+// the pipelines' descriptors.
+void grow_plan(dq_plan* plan, int status) {
+  for (auto& rp : plan->res) {
+    ResRec& r = *rp;
+    if ((status & kErrHtFull) && (r.desc.kind == DQ_RES_UNIQUE || r.desc.kind == DQ_RES_AGG)) {
+      // four times the slots (join tables are sized at unique_pct of the capacity)
+      const int64_t pct = r.desc.kind == DQ_RES_UNIQUE ? std::max(plan->opts.unique_pct, 25) : 100;
+      r.desc.capacity = (int64_t)r.dev.cap * 4 * 100 / pct;
+      setup_resource(plan, r, 1);
+    }
+    if ((status & kErrOverflow) && r.desc.kind == DQ_RES_OUTPUT) {
+      uint64_t need = 0;
+      DQ_CUDA(cudaMemcpy(&need, r.cursor.ptr, 8, cudaMemcpyDeviceToHost));
+      if (need > r.dev.cap) {
+        r.desc.capacity = (int64_t)need;
+        setup_resource(plan, r, 1);
+      }
+    }
+  }
+  refresh_pipelines(plan);
+}
+
+void throw_status(int status) {
+  throw DqError(status & kErrTimeout ? DQ_ERR_TIMEOUT
+                : status & kErrHtFull ? DQ_ERR_HT_FULL
+                : status & kErrOverflow ? DQ_ERR_OVERFLOW : DQ_ERR_BAD_IR,
+                "device status " + std::to_string(status));
+}
+
+jit::Tuning tuning_of(const dq_tuning* t) {
+  jit::Tuning j;
+  if (t) {
+    j.rows_per_thread = t->rows_per_thread;
+    j.block = t->block_threads;
+    j.refill = t->refill;
+  }
+  return j;
+}
+
+PlanOpts opts_of(const dq_tuning* t) {
+  PlanOpts o;
+  o.tuning = tuning_of(t);
+  if (t && t->unique_slots_pct > 0) o.unique_pct = t->unique_slots_pct;
+  if (t && t->multi_buckets_pct > 0) o.multi_pct = t->multi_buckets_pct;
+  return o;
+}
+
+// ---------------------------------------------------------------- batches --
+
+template <class T>
+void upload(DevBuf& buf, const std::vector<T>& v) {
+  buf.alloc(std::max<size_t>(v.size(), 1) * sizeof(T));
+  if (!v.empty()) DQ_CUDA(cudaMemcpy(buf.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+
+// (Re)builds the batch's kernels, descriptors and CUDA graph from its
+// instance plans (after preparation and after tables grew).
+void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
+  dq_ctx* ctx = b->ctx;
+  const dq_plan& first = *b->inst[0];
+  const size_t np = first.pipes.size();
+  b->stages.clear();
+  b->launches = 0;
+  for (size_t p = 0; p < np; ++p) {
+    b->stages.emplace_back(new BatchStage());
+    BatchStage& S = *b->stages[p];
+    jit::Tuning t = tuning;
+    t.batched = true;
+    const PipeRec& p0 = *first.pipes[p];
+    S.prog = jit::generate(p0.dev, -1, p0.desc.compact - 1, t);
+    for (int i = 1; i < b->ninst; ++i) {
+      const PipeRec& pi = *b->inst[i]->pipes[p];
+      if (jit::generate(pi.dev, -1, pi.desc.compact - 1, t).source != S.prog.source)
+        throw DqError(DQ_ERR_BAD_IR, "batch instance " + std::to_string(i) + " differs in shape from instance 0");
+    }
+    S.kernels = jit::compile(S.prog, true);
+    std::vector<DevPipe> descs(b->ninst);
+    std::vector<int64_t> prefix(b->ninst + 1, 0);
+    const int64_t span = (int64_t)S.prog.block * S.prog.rows_per_thread;
+    for (int i = 0; i < b->ninst; ++i) {
+      const dq_plan& pl = *b->inst[i];
+      descs[i] = pl.pipes[p]->dev;
+      descs[i].status = b->status.as<int32_t>();
+      int64_t rows = descs[i].nrows;
+      if (descs[i].nrows_dev) rows = (int64_t)pl.res[descs[i].source_res]->dev.cap;  // temp table: its capacity
+      prefix[i + 1] = prefix[i] + (rows + span - 1) / span;
+    }
+    upload(S.descs, descs);
+    upload(S.bprefix, prefix);
+    const void* fn = (const void*)S.kernels.main;
+    DQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, S.prog.smem_bytes));
+    int occ = 0;
+    DQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, S.prog.block, S.prog.smem_bytes));
+    if (occ < 1) throw DqError(DQ_ERR_UNSUPPORTED, "batched pipeline kernel cannot be resident");
+    S.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->sms * occ, prefix[b->ninst]));
+    S.mm_scan = p0.mm_count;
+    if (S.mm_scan) {
+      std::vector<BatchScanSeg> segs(b->ninst);
+      uint64_t blocks = 0;
+      for (int i = 0; i < b->ninst; ++i) {
+        const DevRes& R = b->inst[i]->res[p0.mm_res]->dev;
+        segs[i].counts = R.counts;
+        segs[i].offsets = R.offsets;
+        segs[i].n = R.cap;
+        segs[i].block0 = blocks;
+        segs[i].nblocks = batch_scan_blocks(R.cap);
+        blocks += segs[i].nblocks;
+      }
+      upload(S.segs, segs);
+      S.partials.alloc(std::max<uint64_t>(blocks, 1) * 4);
+      S.nsegs = b->ninst;
+      S.scan_blocks = blocks;
+    }
+  }
+  // resets of every instance's tables, in one launch
+  std::vector<BatchReset> resets;
+  for (int i = 0; i < b->ninst; ++i)
+    for (auto& rp : b->inst[i]->res) {
+      const ResRec& r = *rp;
+      BatchReset op{};
+      switch (r.desc.kind) {
+        case DQ_RES_UNIQUE:
+          op.ptr = r.dev.slots, op.n = (r.dev.cap + 1) * r.dev.words, op.value = kEmpty, op.kind = 0;
+          break;
+        case DQ_RES_AGG:
+          op.ptr = r.dev.slots, op.n = r.dev.cap + 1, op.kind = 2, op.words = r.dev.words;
+          op.val_word = r.dev.val_word, op.naggs = r.dev.naggs;
+          for (int j = 0; j < r.dev.naggs && j < 16; ++j) op.reds |= (uint64_t)(r.dev.agg_red[j] & 15) << (4 * j);
+          break;
+        case DQ_RES_MULTI:
+          op.ptr = r.dev.counts, op.n = r.dev.cap, op.value = 0, op.kind = 1;
+          break;
+        case DQ_RES_OUTPUT:
+          op.ptr = r.dev.cursor, op.n = 1, op.value = 0, op.kind = 0;
+          break;
+      }
+      resets.push_back(op);
+    }
+  upload(b->resets, resets);
+  b->nresets = (int)resets.size();
+  // results: every instance's output columns packed into one buffer
+  std::vector<BatchPack> packs;
+  b->col_off.assign(b->ninst, std::vector<uint64_t>());
+  uint64_t off = 0;
+  b->rows.alloc((size_t)b->ninst * 8);
+  for (int i = 0; i < b->ninst; ++i) {
+    const ResRec& o = *b->inst[i]->res[b->inst[i]->result_res];
+    for (int j = 0; j < o.desc.npay; ++j) {
+      BatchPack pk{};
+      pk.src = o.dev.pay[j];
+      pk.cursor = o.dev.cursor;
+      pk.cap = o.dev.cap;
+      pk.width = ctype_width(o.desc.pay_ctype[j]);
+      pk.dst = off;
+      pk.rows_out = j == 0 ? b->rows.as<uint64_t>() + i : nullptr;
+      b->col_off[i].push_back(off);
+      off += align_up(o.dev.cap * (uint64_t)pk.width, 16);
+      packs.push_back(pk);
+    }
+    if (o.desc.npay == 0) throw DqError(DQ_ERR_BAD_IR, "batch results need at least one column");
+  }
+  upload(b->packs, packs);
+  b->npacks = (int)packs.size();
+  b->packed_bytes = std::max<uint64_t>(off, 16);
+  b->packed.alloc(b->packed_bytes);
+  if (b->host) cudaFreeHost(b->host);
+  b->host = nullptr;
+  DQ_CUDA(cudaMallocHost((void**)&b->host, b->packed_bytes + (size_t)b->ninst * 8 + 16));
+  // the whole run as one CUDA graph
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  DQ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaSuccess;
+  auto rec = [&](cudaError_t e) {
+    if (err == cudaSuccess && e != cudaSuccess) err = e;
+  };
+  rec(cudaMemsetAsync(b->status.ptr, 0, 4, st));
+  rec(launch_batch_reset(b->resets.as<BatchReset>(), b->nresets, ctx->sms, st));
+  int launches = 1;
+  for (auto& Sp : b->stages) {
+    BatchStage& S = *Sp;
+    const DevPipe* d = S.descs.as<DevPipe>();
+    const int64_t* pre = S.bprefix.as<int64_t>();
+    int n = b->ninst;
+    void* args[] = {(void*)&d, (void*)&pre, (void*)&n};
+    rec(cudaLaunchKernel((const void*)S.kernels.main, dim3(S.grid), dim3(S.prog.block), args,
+                         (size_t)S.prog.smem_bytes, st));
+    ++launches;
+    if (S.mm_scan) {
+      rec(launch_batch_scan(S.segs.as<BatchScanSeg>(), S.nsegs, S.scan_blocks, S.partials.as<uint32_t>(), st));
+      launches += 3;
+    }
+  }
+  rec(launch_batch_pack(b->packs.as<BatchPack>(), b->npacks, b->packed.as<uint8_t>(), ctx->sms, st));
+  ++launches;
+  rec(cudaMemcpyAsync(b->host, b->packed.ptr, b->packed_bytes, cudaMemcpyDeviceToHost, st));
+  rec(cudaMemcpyAsync(b->host + b->packed_bytes, b->rows.ptr, (size_t)b->ninst * 8, cudaMemcpyDeviceToHost, st));
+  rec(cudaMemcpyAsync(b->host + b->packed_bytes + (size_t)b->ninst * 8, b->status.ptr, 4, cudaMemcpyDeviceToHost, st));
+  cudaGraph_t g = nullptr;
+  cudaError_t end = cudaStreamEndCapture(st, &g);
+  DQ_CUDA(err);
+  DQ_CUDA(end);
+  b->graph = g;
+  DQ_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  b->launches = launches;
 }
 
 }  // namespace
@@ -894,59 +1223,7 @@ int dq_plan_prepare(dq_ctx* ctx, const dq_plan_desc* desc, dq_plan** out) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     OfflineScope offline(ctx->offline);
     if (!ctx->offline) DQ_CUDA(cudaSetDevice(ctx->device));
-    std::unique_ptr<dq_plan> plan(new dq_plan());
-    plan->ctx = ctx;
-    plan->status.alloc(4);
-    plan->counters.alloc(8 * (size_t)desc->npipes);
-    // row bound for multimap payloads: rows of the source of the pipeline that scatters into it
-    std::vector<int64_t> bound(desc->nres, 1);
-    for (int i = 0; i < desc->npipes; ++i) {
-      const dq_pipeline& d = desc->pipes[i];
-      if (d.nops <= 0 || d.nops > DQ_MAX_OPS) throw DqError(DQ_ERR_BAD_IR, "bad op count");
-      const dq_op& sink = d.ops[d.nops - 1];
-      if ((sink.kind == DQ_OP_MM_SCATTER || sink.kind == DQ_OP_MM_COUNT) && sink.res >= 0 && sink.res < desc->nres) {
-        int64_t rows = 1 << 20;
-        if (d.source_kind == DQ_SRC_TABLE && d.table) {
-          auto it = ctx->tables.find(d.table);
-          if (it != ctx->tables.end()) rows = it->second.nrows;
-        } else if (d.source_kind == DQ_SRC_OUTPUT && d.source_res >= 0 && d.source_res < desc->nres) {
-          rows = desc->res[d.source_res].capacity;
-        }
-        bound[sink.res] = std::max(bound[sink.res], rows);
-      }
-    }
-    for (int i = 0; i < desc->nres; ++i) {
-      std::unique_ptr<ResRec> r(new ResRec());
-      r->desc = desc->res[i];
-      r->name = desc->res[i].name ? desc->res[i].name : "";
-      r->desc.name = nullptr;
-      setup_resource(plan.get(), *r, bound[i]);
-      plan->res.push_back(std::move(r));
-    }
-    for (int i = 0; i < desc->npipes; ++i) {
-      std::unique_ptr<PipeRec> p(new PipeRec());
-      p->desc = desc->pipes[i];
-      // keep string arguments alive
-      for (int c = 0; c < p->desc.ncols; ++c) p->col_names.push_back(p->desc.cols[c] ? p->desc.cols[c] : "");
-      for (int c = 0; c < p->desc.ncols; ++c) p->desc.cols[c] = p->col_names[c].c_str();
-      p->desc.table = nullptr;
-      std::string tname = desc->pipes[i].table ? desc->pipes[i].table : "";
-      p->col_names.push_back(tname);
-      p->desc.table = p->col_names.back().c_str();
-      for (int c = 0; c < p->desc.npatterns; ++c) p->patterns.push_back(p->desc.patterns[c] ? p->desc.patterns[c] : "");
-      for (int c = 0; c < p->desc.npatterns; ++c) p->desc.patterns[c] = p->patterns[c].c_str();
-      plan->pipes.push_back(std::move(p));
-    }
-    // the col_names vector may have reallocated: re-point
-    for (auto& p : plan->pipes) {
-      for (int c = 0; c < p->desc.ncols; ++c) p->desc.cols[c] = p->col_names[c].c_str();
-      p->desc.table = p->col_names.back().c_str();
-      for (int c = 0; c < p->desc.npatterns; ++c) p->desc.patterns[c] = p->patterns[c].c_str();
-    }
-    refresh_pipelines(plan.get());
-    plan->result_res = desc->result_res;
-    if (plan->result_res < 0 || plan->result_res >= desc->nres || plan->res[plan->result_res]->desc.kind != DQ_RES_OUTPUT)
-      throw DqError(DQ_ERR_BAD_IR, "result must be an OUTPUT resource");
+    std::unique_ptr<dq_plan> plan = make_plan(ctx, desc, PlanOpts());
     *out = plan.release();
     return (int)DQ_OK;
   });
@@ -971,22 +1248,7 @@ int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out) {
                       : status & kErrOverflow ? DQ_ERR_OVERFLOW : DQ_ERR_BAD_IR,
                       "device status " + std::to_string(status));
       // grow what overflowed and run again (the results of a failed run are discarded)
-      for (auto& rp : plan->res) {
-        ResRec& r = *rp;
-        if ((status & kErrHtFull) && (r.desc.kind == DQ_RES_UNIQUE || r.desc.kind == DQ_RES_AGG)) {
-          r.desc.capacity = (int64_t)r.dev.cap * 4;
-          setup_resource(plan, r, 1);
-        }
-        if ((status & kErrOverflow) && r.desc.kind == DQ_RES_OUTPUT) {
-          uint64_t need = 0;
-          DQ_CUDA(cudaMemcpy(&need, r.cursor.ptr, 8, cudaMemcpyDeviceToHost));
-          if (need > r.dev.cap) {
-            r.desc.capacity = (int64_t)need;
-            setup_resource(plan, r, 1);
-          }
-        }
-      }
-      refresh_pipelines(plan);
+      grow_plan(plan, status);
     }
     ResRec& o = *plan->res[plan->result_res];
     uint64_t n = 0;
@@ -1058,5 +1320,106 @@ int dq_result_column(dq_result* r, int32_t col, int32_t* ctype, const void** dat
 }
 
 void dq_result_free(dq_result* r) { delete r; }
+
+int dq_plan_prepare_tuned(dq_ctx* ctx, const dq_plan_desc* desc, const dq_tuning* tuning, dq_plan** out) {
+  if (!ctx || !desc || !out) return fail(ctx, DQ_ERR_INVALID, "bad arguments");
+  *out = nullptr;
+  return guarded(ctx, [&]() {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    OfflineScope offline(ctx->offline);
+    if (!ctx->offline) DQ_CUDA(cudaSetDevice(ctx->device));
+    *out = make_plan(ctx, desc, opts_of(tuning)).release();
+    return (int)DQ_OK;
+  });
+}
+
+// --------------------------------------------------------------- batches --
+
+int dq_batch_prepare(dq_ctx* ctx, int32_t ninst, const dq_plan_desc* descs, const dq_tuning* tuning, dq_batch** out) {
+  if (!ctx || !descs || !out || ninst <= 0) return fail(ctx, DQ_ERR_INVALID, "bad arguments");
+  *out = nullptr;
+  return guarded(ctx, [&]() {
+    if (ctx->offline) throw DqError(DQ_ERR_UNSUPPORTED, "an offline context cannot hold batches");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DQ_CUDA(cudaSetDevice(ctx->device));
+    std::unique_ptr<dq_batch> b(new dq_batch());
+    b->ctx = ctx;
+    b->ninst = ninst;
+    b->tuning = tuning_of(tuning);
+    PlanOpts o = opts_of(tuning);
+    o.batch_member = true;
+    for (int i = 0; i < ninst; ++i) {
+      b->inst.push_back(make_plan(ctx, &descs[i], o));
+      if (b->inst[i]->pipes.size() != b->inst[0]->pipes.size() || b->inst[i]->res.size() != b->inst[0]->res.size())
+        throw DqError(DQ_ERR_BAD_IR, "batch instance " + std::to_string(i) + " differs in shape from instance 0");
+    }
+    b->status.alloc(4);
+    DQ_CUDA(cudaEventCreate(&b->ev0));
+    DQ_CUDA(cudaEventCreate(&b->ev1));
+    build_batch(b.get(), b->tuning, ctx->stream);
+    *out = b.release();
+    return (int)DQ_OK;
+  });
+}
+
+int dq_batch_execute(dq_batch* b, void* stream, dq_result** results) {
+  if (!b || !results) return DQ_ERR_INVALID;
+  dq_ctx* ctx = b->ctx;
+  return guarded(ctx, [&]() {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DQ_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    int32_t status = 0;
+    for (int attempt = 0;; ++attempt) {
+      DQ_CUDA(cudaEventRecord(b->ev0, st));
+      DQ_CUDA(cudaGraphLaunch(b->exec, st));
+      DQ_CUDA(cudaEventRecord(b->ev1, st));
+      DQ_CUDA(cudaStreamSynchronize(st));
+      memcpy(&status, b->host + b->packed_bytes + (size_t)b->ninst * 8, 4);
+      if (status == 0) break;
+      if (attempt >= 8 || (status & (kErrTimeout | kErrBadOp))) throw_status(status);
+      for (auto& pl : b->inst) grow_plan(pl.get(), status);
+      build_batch(b, b->tuning, st);
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+    memset(&b->timing, 0, sizeof(b->timing));
+    b->timing.total_ms = ms;
+    b->timing.max_pipeline = -1;
+    b->timing.kernel_launches = b->launches;
+    const uint64_t* rows = reinterpret_cast<const uint64_t*>(b->host + b->packed_bytes);
+    for (int i = 0; i < b->ninst; ++i) {
+      const ResRec& o = *b->inst[i]->res[b->inst[i]->result_res];
+      std::unique_ptr<dq_result> res(new dq_result());
+      res->nrows = (int64_t)rows[i];
+      for (int j = 0; j < o.desc.npay; ++j) {
+        const int w = ctype_width(o.desc.pay_ctype[j]);
+        res->ctypes.push_back(o.desc.pay_ctype[j]);
+        const uint8_t* src = b->host + b->col_off[i][j];
+        res->cols.emplace_back(src, src + (size_t)rows[i] * w);
+      }
+      results[i] = res.release();
+    }
+    return (int)DQ_OK;
+  });
+}
+
+int dq_batch_timing_get(dq_batch* b, dq_plan_timing* out) {
+  if (!b || !out) return DQ_ERR_INVALID;
+  *out = b->timing;
+  return DQ_OK;
+}
+
+int dq_batch_size(dq_batch* b, int32_t* ninst) {
+  if (!b || !ninst) return DQ_ERR_INVALID;
+  *ninst = b->ninst;
+  return DQ_OK;
+}
+
+void dq_batch_free(dq_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->ctx->device);
+  delete b;
+}
 
 }  // extern "C"

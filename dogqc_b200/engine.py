@@ -52,39 +52,60 @@ class Result(object):
         return "\n".join(out) + "\n"
 
 
+def _take_result(res, names):
+    """Copies a dq_result into a Result and frees it."""
+    lib = L.lib()
+    try:
+        n = C.c_int64()
+        nc = C.c_int32()
+        L.check(lib.dq_result_rows(res, C.byref(n)))
+        L.check(lib.dq_result_ncols(res, C.byref(nc)))
+        cols, types = [], []
+        for j in range(nc.value):
+            t = C.c_int32()
+            ptr = C.c_void_p()
+            L.check(lib.dq_result_column(res, j, C.byref(t), C.byref(ptr)))
+            dt = np.dtype(NP_DTYPE[t.value])
+            if n.value:
+                buf = (C.c_uint8 * (n.value * dt.itemsize)).from_address(ptr.value)
+                cols.append(np.frombuffer(buf, dtype=dt).copy())
+            else:
+                cols.append(np.zeros(0, dtype=dt))
+            types.append(t.value)
+    finally:
+        lib.dq_result_free(res)
+    return Result(names, types, cols, n.value)
+
+
+def make_tuning(tuning):
+    """A dq_tuning from a dict (keys are the struct's fields) or None."""
+    if tuning is None:
+        return None
+    if isinstance(tuning, L.dq_tuning):
+        return tuning
+    t = L.dq_tuning()
+    for k, v in dict(tuning).items():
+        setattr(t, k, int(v))
+    return t
+
+
 class Plan(object):
-    def __init__(self, engine, lowering):
+    def __init__(self, engine, lowering, tuning=None):
         self.engine = engine
         self.lowering = lowering
         desc, keep = lowering.ir()
         handle = C.c_void_p()
-        L.check(L.lib().dq_plan_prepare(engine.ctx, C.byref(desc), C.byref(handle)), engine.ctx)
+        t = make_tuning(tuning)
+        if t is None:
+            L.check(L.lib().dq_plan_prepare(engine.ctx, C.byref(desc), C.byref(handle)), engine.ctx)
+        else:
+            L.check(L.lib().dq_plan_prepare_tuned(engine.ctx, C.byref(desc), C.byref(t), C.byref(handle)), engine.ctx)
         self.handle = handle
 
     def execute(self, stream=None):
-        lib = L.lib()
         res = C.c_void_p()
-        L.check(lib.dq_plan_execute(self.handle, stream, C.byref(res)), self.engine.ctx)
-        try:
-            n = C.c_int64()
-            nc = C.c_int32()
-            L.check(lib.dq_result_rows(res, C.byref(n)))
-            L.check(lib.dq_result_ncols(res, C.byref(nc)))
-            cols, types = [], []
-            for j in range(nc.value):
-                t = C.c_int32()
-                ptr = C.c_void_p()
-                L.check(lib.dq_result_column(res, j, C.byref(t), C.byref(ptr)))
-                dt = np.dtype(NP_DTYPE[t.value])
-                if n.value:
-                    buf = (C.c_uint8 * (n.value * dt.itemsize)).from_address(ptr.value)
-                    cols.append(np.frombuffer(buf, dtype=dt).copy())
-                else:
-                    cols.append(np.zeros(0, dtype=dt))
-                types.append(t.value)
-        finally:
-            lib.dq_result_free(res)
-        return Result(self.lowering.result_names, types, cols, n.value)
+        L.check(L.lib().dq_plan_execute(self.handle, stream, C.byref(res)), self.engine.ctx)
+        return _take_result(res, self.lowering.result_names)
 
     def source(self, pipe):
         """Generated CUDA source of pipeline ``pipe`` with the compiler's
@@ -109,6 +130,50 @@ class Plan(object):
     def free(self):
         if self.handle:
             L.lib().dq_plan_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Batch(object):
+    """Many instances of one plan shape executed together (dq_batch_*): one
+    generated kernel per pipeline over all instances, under one CUDA graph.
+    ``lowerings`` are the instances' lowered plans, each naming its own tables."""
+
+    def __init__(self, engine, lowerings, tuning=None):
+        self.engine = engine
+        self.lowerings = list(lowerings)
+        irs = [lw.ir() for lw in self.lowerings]
+        self._keep = irs
+        arr = (L.dq_plan_desc * len(irs))(*[d for d, _ in irs])
+        self._arr = arr
+        handle = C.c_void_p()
+        t = make_tuning(tuning)
+        L.check(L.lib().dq_batch_prepare(engine.ctx, len(irs), arr, C.byref(t) if t is not None else None,
+                                         C.byref(handle)), engine.ctx)
+        self.handle = handle
+
+    def __len__(self):
+        return len(self.lowerings)
+
+    def execute(self, stream=None):
+        n = len(self.lowerings)
+        out = (C.c_void_p * n)()
+        L.check(L.lib().dq_batch_execute(self.handle, stream, out), self.engine.ctx)
+        return [_take_result(C.c_void_p(out[i]), self.lowerings[i].result_names) for i in range(n)]
+
+    def timing(self):
+        t = L.dq_plan_timing()
+        L.check(L.lib().dq_batch_timing_get(self.handle, C.byref(t)))
+        return {"total_ms": t.total_ms, "kernel_launches": t.kernel_launches}
+
+    def free(self):
+        if self.handle:
+            L.lib().dq_batch_free(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -173,9 +238,13 @@ class Engine(object):
         arr, n, keep = self._columns(table)
         L.check(L.lib().dq_table_update(self.ctx, table.name.encode(), n, arr, table.size, stream), self.ctx)
 
-    def prepare(self, plan, options=None):
+    def prepare(self, plan, options=None, tuning=None):
+        """``tuning``: dq_tuning fields as a dict (see dogqc_b200.autotune)."""
         lowering = plan if isinstance(plan, Lowering) else Lowering(plan, options)
-        return Plan(self, lowering)
+        return Plan(self, lowering, tuning)
+
+    def prepare_batch(self, lowerings, tuning=None):
+        return Batch(self, lowerings, tuning)
 
     def close(self):
         if self.ctx:

@@ -53,6 +53,7 @@ typedef enum {
 typedef struct dq_ctx dq_ctx;
 typedef struct dq_plan dq_plan;
 typedef struct dq_result dq_result;
+typedef struct dq_batch dq_batch;
 
 typedef struct {
     int32_t abi_version;        /* DQ_ABI_VERSION                               */
@@ -272,6 +273,38 @@ typedef struct {
     double pipeline_ms[DQ_MAX_OPS];
 } dq_plan_timing;
 int dq_plan_timing_get(dq_plan* plan, dq_plan_timing* out);
+
+/* ------------------------------------------------------------- tuning -- */
+/* Launch-shape and table-sizing choices an autotuner sets (0: the backend's
+ * default).  The reference fixes these in its generator (grid 920-1024 x 128,
+ * dogqc/kernel.py:10-11; htSizeFactor 2.0, dogqc/hashJoins.py:43; lane-refill
+ * threshold 28 of 32, dogqc/cudaDivergenceBuffer.py:15).                     */
+typedef struct {
+    int32_t rows_per_thread;         /* 1, 2 or 4 consecutive rows per thread   */
+    int32_t block_threads;           /* 128, 256 or 512 (batched kernels)       */
+    int32_t refill;                  /* -1: no lane refill; 0: the plan's own   */
+    int32_t unique_slots_pct;        /* join-table slots, % of the plan's       */
+                                     /* capacity (default 200)                  */
+    int32_t multi_buckets_pct;       /* multimap buckets, % (default 100)       */
+    int32_t reserved[3];
+} dq_tuning;
+int dq_plan_prepare_tuned(dq_ctx* ctx, const dq_plan_desc* desc, const dq_tuning* tuning, dq_plan** out);
+
+/* ------------------------------------------------------------ batches -- */
+/* Many instances of one plan shape (same pipelines and ops; own tables and
+ * capacities), such as the partitions of a workload or many small queries,
+ * run together: one generated kernel per pipeline walks the row blocks of all
+ * instances, one launch resets all their tables, one segmented scan builds all
+ * their multimaps, and the whole run (resets, pipelines, scans, result pack
+ * and the device-to-host copy) is a captured CUDA graph replayed per execute.
+ * No counterpart in the reference, which launches every query separately.  */
+int dq_batch_prepare(dq_ctx* ctx, int32_t ninst, const dq_plan_desc* descs, const dq_tuning* tuning,
+                     dq_batch** out);
+/* results: ninst new results, one per instance, in instance order           */
+int dq_batch_execute(dq_batch* batch, void* stream, dq_result** results);
+int dq_batch_timing_get(dq_batch* batch, dq_plan_timing* out);  /* total_ms: the graph */
+int dq_batch_size(dq_batch* batch, int32_t* ninst);
+void dq_batch_free(dq_batch* batch);
 
 /* ------------------------------------------------------------ results -- */
 int dq_result_rows(dq_result* r, int64_t* nrows);
