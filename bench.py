@@ -419,6 +419,120 @@ def run_reference(args, world, rank):
     }
 
 
+# ------------------------------------------------- batched and served forms --
+
+def run_batched(args, world, rank, local):
+    """256 divergent-expansion instances (row counts log-uniform in 2^10..2^20)
+    in one batch (one generated kernel per pipeline, one CUDA graph) against the
+    same instances executed as plain plans one after the other."""
+    import numpy as np
+    import torch
+    from dogqc_b200 import autotune, batch
+    from dogqc_b200.engine import Engine
+    torch.cuda.set_device(local)
+    n = 256
+    insts = batch.make_instances("c2", n)
+    rows = sum(i.input_rows for i in insts)
+    engine = Engine(local)
+    batch.register(engine, insts)
+    tuning, tuned = None, None
+    if args.autotune:
+        tuning, t_best, log = autotune.tune_batch(engine, [i.lowering for i in insts])
+        tuned = {"tuning": tuning, "candidates": len(log), "best_ms": t_best * 1e3}
+    b = batch.prepare_batch(engine, insts, tuning)
+    for _ in range(args.warmup):
+        res = b.execute()
+    dist_barrier(world)
+    ms = []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            b.execute()
+            ms.append(b.timing()["total_ms"])
+    step_ms = dist_max(float(np.mean(ms)), world)
+    from dogqc_b200 import serve
+    plans = batch.prepare_one_by_one(engine, insts)
+    order = [(0.0, i) for i in range(n)]
+    keyed = {i: p for i, p in enumerate(plans)}
+    serve.sequence(engine, insts, order, keyed)
+    seq = []
+    for _ in range(max(1, args.steps // 4)):
+        per, wall, _ = serve.sequence(engine, insts, order, keyed)
+        seq.append(wall)
+    one_ms = float(np.median(seq)) * 1e3
+    parity = all(sorted(p.execute().rows()) == sorted(r.rows()) for p, r in zip(plans, res))
+    out = {
+        "metric": "instances/s (256 divergent-expansion instances, one batch)", "value": n * world / (step_ms / 1e3),
+        "unit": "instances/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "divergent_expansion_x256", "instances": n, "rows": "log-uniform 2^10..2^20 probe rows",
+                   "input_rows": rows, "parallelism": "replicas"},
+        "rows_per_s": rows * world / (step_ms / 1e3),
+        "one_by_one": {"ms": one_ms, "instances_per_s": n / (one_ms / 1e3),
+                       "how": "the same instances as plain plans, executed one after the other from native code"},
+        "speedup_vs_one_by_one": one_ms / step_ms,
+        "parity_with_one_by_one": parity,
+        "gpu_launches": b.timing()["kernel_launches"] * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if tuned:
+        out["autotune"] = tuned
+    b.free()
+    for p in plans:
+        p.free()
+    engine.close()
+    return out
+
+
+def run_served(args, world, rank, local):
+    """The served mixed stream: queries of the c0-c3 shapes over small resident
+    tables, replayed through the request server (native submit/collect) closed
+    loop and at Poisson rates, against the same requests run one at a time."""
+    import torch
+    from dogqc_b200 import serve
+    from dogqc_b200.engine import Engine
+    torch.cuda.set_device(local)
+    sizes = tuple(float(x) for x in args.served_sizes.split(","))
+    qs = serve.make_queries(sizes=sizes)
+    engine = Engine(local)
+    serve.register(engine, qs)
+    n = 2000
+    sched = serve.arrivals(n, None, qs, seed=5)
+    _, _, plans = serve.sequence(engine, qs, sched[:200])
+    per, wall1, plans = serve.sequence(engine, qs, sched, plans)
+    one = {"queries_per_s": n / wall1, "p50_ms": serve.percentile(per, .5), "p99_ms": serve.percentile(per, .99)}
+    srv = serve.Server(engine, slots=args.slots)
+    serve.warm(srv, qs, args.slots)
+    with ClockSampler(local) as clocks:
+        infos, wall = serve.replay(srv, qs, sched)
+    tot = [i["total_ms"] for i in infos]
+    rates = []
+    for rate in (100, 1000, 5000):
+        sch = serve.arrivals(min(4000, max(300, rate)), rate, qs, seed=9)
+        inf, w = serve.replay(srv, qs, sch)
+        t = [i["total_ms"] for i in inf]
+        rates.append({"offered_qps": rate, "achieved_qps": len(sch) / w, "p50_ms": serve.percentile(t, .5),
+                      "p99_ms": serve.percentile(t, .99)})
+    st = srv.stats()
+    srv.stop()
+    for p in plans.values():
+        p.free()
+    engine.close()
+    value = n / wall
+    return {
+        "metric": "queries/s (served mixed stream of c0-c3 queries, closed loop)", "value": value,
+        "unit": "queries/s", "n_gpus": world, "steps": n, "warmup": 2, "ms_per_step": wall * 1e3 / n,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "served_mixed_stream", "shapes": ["c0", "c1", "c2", "c3"], "sizes": list(sizes),
+                   "slots": args.slots, "requests": n, "memory_budget_gb": 150, "parallelism": "replicas"},
+        "p50_ms": serve.percentile(tot, .5), "p99_ms": serve.percentile(tot, .99),
+        "one_at_a_time": one, "speedup_vs_one_at_a_time": value / one["queries_per_s"],
+        "poisson": rates, "memory_peak_bytes": st["memory_peak"],
+        "clocks": clocks.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -432,16 +546,25 @@ def main():
     ap.add_argument("--engine-flags", type=int, default=0, help="DQ_CFG_* bits")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="workload size factor (profiling only; the bench line is quoted at 1.0)")
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS),
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["c2x256", "c4"],
                     help="c1 (default): the FK-PK join the headline metric is quoted on; c0, c2, c3: "
-                         "the other configurations, for the per-pipeline table")
+                         "the other configurations, for the per-pipeline table; c2x256: the batched form; "
+                         "c4: the served mixed stream")
+    ap.add_argument("--autotune", action="store_true", help="c2x256: pick the batch's tuning by measurement")
+    ap.add_argument("--slots", type=int, default=4, help="c4: requests in flight on the device")
+    ap.add_argument("--served-sizes", default="0.0005,0.002,0.01",
+                    help="c4: table sizes of the query mix, as fractions of the configurations' rows")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global SCALE, WORKLOAD
     SCALE = args.scale
     WORKLOAD = args.workload
     world, rank, local = dist_setup()
-    if args.impl == "reference" and WORKLOAD != "c1":
+    if args.impl == "ours" and WORKLOAD == "c2x256":
+        out = run_batched(args, world, rank, local)
+    elif args.impl == "ours" and WORKLOAD == "c4":
+        out = run_served(args, world, rank, local)
+    elif args.impl == "reference" and WORKLOAD != "c1":
         out = {"impl": "reference", "unavailable": "the partitioned CPU reference arm covers the c1 workload; "
                                                    "the others report cpu_baseline in the ours line"}
         out = out if rank == 0 else None

@@ -96,6 +96,22 @@ class dq_tuning(C.Structure):
                 ("unique_slots_pct", C.c_int32), ("multi_buckets_pct", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
+class dq_server_config(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("pool_per_query", C.c_int32), ("memory_budget", C.c_uint64),
+                ("reserved", C.c_int32 * 4)]
+
+
+class dq_request_info(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("run_ms", C.c_double), ("total_ms", C.c_double), ("bytes", C.c_uint64),
+                ("status", C.c_int32), ("kernel_launches", C.c_int32)]
+
+
+class dq_server_stats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("memory_in_use", C.c_uint64), ("memory_peak", C.c_uint64), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("span_ms", C.c_double)]
+
+
 NOALLOC_MAX_BUILD_ROWS = 262144
 NOALLOC_MAX_GROUPS = 4096
 
@@ -111,7 +127,7 @@ class dq_join_agg_args(C.Structure):
 def check_layout():
     """Sizes the C compiler gives these structs on x86-64 (LP64)."""
     expect = {dq_config: 40, dq_column: 40, dq_slot: 8, dq_op: 40, dq_resource: 80, dq_join_agg_args: 104,
-              dq_tuning: 32}
+              dq_tuning: 32, dq_server_config: 32, dq_request_info: 40, dq_server_stats: 72}
     for t, n in expect.items():
         if C.sizeof(t) != n:
             raise AssertionError("%s is %d bytes, header implies %d" % (t.__name__, C.sizeof(t), n))
@@ -152,6 +168,15 @@ EXPORTS = {
     "dq_batch_timing_get": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_timing)]),
     "dq_batch_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "dq_batch_free": (None, [C.c_void_p]),
+    "dq_server_start": (C.c_int, [C.c_void_p, C.POINTER(dq_server_config), C.POINTER(C.c_void_p)]),
+    "dq_server_submit": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_desc), C.POINTER(C.c_uint64)]),
+    "dq_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_void_p), C.POINTER(dq_request_info)]),
+    "dq_server_stats_get": (C.c_int, [C.c_void_p, C.POINTER(dq_server_stats)]),
+    "dq_server_stop": (None, [C.c_void_p]),
+    "dq_server_replay": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(dq_plan_desc), C.c_int64,
+                                   C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(dq_request_info)]),
+    "dq_plan_run_sequence": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int64, C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_double)]),
 }
 
 

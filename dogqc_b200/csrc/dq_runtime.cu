@@ -11,13 +11,18 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/dogqc_b200.h"
@@ -744,8 +749,9 @@ void free_events(dq_plan* plan) {
 }
 
 // One execution of all pipelines; returns the device status word.
-int run_once(dq_plan* plan, cudaStream_t st) {
-  dq_ctx* ctx = plan->ctx;
+// Enqueues one execution of all pipelines on `st`, ending with the copy of the
+// device status word to `host_status`; returns the kernels launched.
+int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status) {
   int launches = 0;
   const size_t np = plan->pipes.size();
   if (plan->events.size() != 2 * np + 2) {
@@ -802,9 +808,13 @@ int run_once(dq_plan* plan, cudaStream_t st) {
     DQ_CUDA(cudaEventRecord(plan->events[2 + 2 * i], st));
   }
   DQ_CUDA(cudaEventRecord(plan->events[2 * np + 1], st));
-  int32_t status = 0;
-  DQ_CUDA(cudaMemcpyAsync(&status, plan->status.ptr, 4, cudaMemcpyDeviceToHost, st));
-  DQ_CUDA(cudaStreamSynchronize(st));
+  DQ_CUDA(cudaMemcpyAsync(host_status, plan->status.ptr, 4, cudaMemcpyDeviceToHost, st));
+  return launches;
+}
+
+// Device times of the last completed execution (its events have completed).
+void collect_timing(dq_plan* plan, int launches) {
+  const size_t np = plan->pipes.size();
   float ms = 0;
   dq_plan_timing& T = plan->timing;
   memset(&T, 0, sizeof(T));
@@ -820,8 +830,47 @@ int run_once(dq_plan* plan, cudaStream_t st) {
     }
   }
   T.kernel_launches = launches;
-  (void)ctx;
+}
+
+// One execution of all pipelines; returns the device status word.
+int run_once(dq_plan* plan, cudaStream_t st) {
+  int32_t status = 0;
+  const int launches = enqueue_run(plan, st, &status);
+  DQ_CUDA(cudaStreamSynchronize(st));
+  collect_timing(plan, launches);
   return status;
+}
+
+// Copies a completed execution's result (OUTPUT resource) to the host.
+dq_result* read_result(dq_plan* plan, cudaStream_t st) {
+  ResRec& o = *plan->res[plan->result_res];
+  uint64_t n = 0;
+  DQ_CUDA(cudaMemcpyAsync(&n, o.cursor.ptr, 8, cudaMemcpyDeviceToHost, st));
+  DQ_CUDA(cudaStreamSynchronize(st));
+  if (n > o.dev.cap) n = o.dev.cap;
+  std::unique_ptr<dq_result> res(new dq_result());
+  res->nrows = (int64_t)n;
+  for (int j = 0; j < o.desc.npay; ++j) {
+    int w = ctype_width(o.desc.pay_ctype[j]);
+    res->ctypes.push_back(o.desc.pay_ctype[j]);
+    res->cols.emplace_back((size_t)n * w);
+    if (n) DQ_CUDA(cudaMemcpyAsync(res->cols.back().data(), o.dev.pay[j], (size_t)n * w, cudaMemcpyDeviceToHost, st));
+  }
+  DQ_CUDA(cudaStreamSynchronize(st));
+  return res.release();
+}
+
+// Device bytes a plan holds (its tables, intermediates and scratch).
+uint64_t plan_bytes(const dq_plan* plan) {
+  uint64_t b = plan->status.bytes + plan->counters.bytes;
+  for (auto& rp : plan->res) {
+    const ResRec& r = *rp;
+    b += r.slots.bytes + r.counts.bytes + r.offsets.bytes + r.cursor.bytes + r.scan_scratch.bytes;
+    for (auto& p : r.pay) b += p->bytes;
+  }
+  for (auto& pp : plan->pipes)
+    b += pp->pattern_buf.bytes + pp->heavy_items.bytes + pp->heavy_count.bytes + pp->heavy_prefix.bytes;
+  return b;
 }
 
 // Re-derives every pipeline's copy of the resource descriptors.
@@ -1250,19 +1299,7 @@ int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out) {
       // grow what overflowed and run again (the results of a failed run are discarded)
       grow_plan(plan, status);
     }
-    ResRec& o = *plan->res[plan->result_res];
-    uint64_t n = 0;
-    DQ_CUDA(cudaMemcpy(&n, o.cursor.ptr, 8, cudaMemcpyDeviceToHost));
-    std::unique_ptr<dq_result> res(new dq_result());
-    res->nrows = (int64_t)n;
-    for (int j = 0; j < o.desc.npay; ++j) {
-      int w = ctype_width(o.desc.pay_ctype[j]);
-      res->ctypes.push_back(o.desc.pay_ctype[j]);
-      res->cols.emplace_back((size_t)n * w);
-      if (n) DQ_CUDA(cudaMemcpyAsync(res->cols.back().data(), o.dev.pay[j], (size_t)n * w, cudaMemcpyDeviceToHost, st));
-    }
-    DQ_CUDA(cudaStreamSynchronize(st));
-    *out = res.release();
+    *out = read_result(plan, st);
     return (int)DQ_OK;
   });
 }
@@ -1420,6 +1457,664 @@ void dq_batch_free(dq_batch* b) {
   if (!b) return;
   cudaSetDevice(b->ctx->device);
   delete b;
+}
+
+}  // extern "C"
+
+// ================================================================= serving ==
+//
+// A request loop on its own thread.  Requests carry a plan IR over registered
+// (resident) tables; the loop keeps prepared plans pooled per distinct request,
+// so a repeated query reuses its tables and compiled kernels.  It admits the
+// oldest waiting request when a device slot (a CUDA stream) is free and the
+// request's estimated table and intermediate bytes fit the memory budget next
+// to the plans already held (idle pooled plans are freed first to make room),
+// enqueues the request's pipelines on that stream without waiting, and turns
+// completed slots into results.  Requests that arrive while others run are
+// admitted as soon as a slot and memory free up, and their kernels overlap on
+// the device with the running ones.
+
+namespace {
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// A deep copy of a request's IR (the caller's arrays and strings may go away
+// after submit) and the key that identifies the query.
+struct DescCopy {
+  std::vector<dq_resource> res;
+  std::vector<dq_pipeline> pipes;
+  std::deque<std::string> strs;
+  dq_plan_desc d{};
+  std::string key;
+  const char* keep(const char* s) {
+    if (!s) return nullptr;
+    strs.emplace_back(s);
+    return strs.back().c_str();
+  }
+};
+
+std::shared_ptr<DescCopy> copy_desc(const dq_plan_desc* in) {
+  if (!in || in->abi_version != DQ_ABI_VERSION || in->npipes <= 0 || !in->pipes || in->nres < 0 ||
+      (in->nres > 0 && !in->res))
+    throw DqError(DQ_ERR_BAD_IR, "bad plan descriptor");
+  std::shared_ptr<DescCopy> c(new DescCopy());
+  c->res.assign(in->res, in->res + in->nres);
+  c->pipes.assign(in->pipes, in->pipes + in->npipes);
+  std::string key;
+  for (auto& r : c->res) {
+    dq_resource z = r;
+    z.name = nullptr;
+    key.append(reinterpret_cast<const char*>(&z), sizeof(z));
+    r.name = c->keep(r.name);
+  }
+  for (auto& p : c->pipes) {
+    if (p.ncols < 0 || p.ncols > DQ_MAX_COLS || p.npatterns < 0 || p.npatterns > DQ_MAX_PATTERNS)
+      throw DqError(DQ_ERR_BAD_IR, "pipeline sizes out of range");
+    dq_pipeline z = p;
+    z.table = nullptr;
+    for (int j = 0; j < DQ_MAX_COLS; ++j) z.cols[j] = nullptr;
+    for (int j = 0; j < DQ_MAX_PATTERNS; ++j) z.patterns[j] = nullptr;
+    key.append(reinterpret_cast<const char*>(&z), sizeof(z));
+    p.table = c->keep(p.table);
+    key += p.table ? p.table : "";
+    key.push_back('\0');
+    for (int j = 0; j < p.ncols; ++j) {
+      p.cols[j] = c->keep(p.cols[j]);
+      key += p.cols[j] ? p.cols[j] : "";
+      key.push_back('\0');
+    }
+    for (int j = 0; j < p.npatterns; ++j) {
+      p.patterns[j] = c->keep(p.patterns[j]);
+      key += p.patterns[j] ? p.patterns[j] : "";
+      key.push_back('\0');
+    }
+  }
+  c->d = *in;
+  c->d.res = c->res.data();
+  c->d.pipes = c->pipes.data();
+  c->key = std::move(key);
+  return c;
+}
+
+// Device bytes a request's plan will hold, from its IR (before preparing it).
+uint64_t estimate_bytes(dq_ctx* ctx, const dq_plan_desc& d) {
+  uint64_t b = 4096;
+  for (int i = 0; i < d.nres; ++i) {
+    const dq_resource& r = d.res[i];
+    const uint64_t cap = (uint64_t)std::max<int64_t>(r.capacity, 16);
+    const bool packed = r.nkeys <= 1 || (r.nkeys == 2 && ctype_width(r.key_ctype[0]) <= 4 && ctype_width(r.key_ctype[1]) <= 4);
+    const uint64_t keyw = packed ? 0 : r.nkeys;
+    uint64_t widths = 0;
+    for (int j = 0; j < r.npay && j < DQ_MAX_PAY; ++j) widths += ctype_width(r.pay_ctype[j]);
+    switch (r.kind) {
+      case DQ_RES_UNIQUE: b += (2 * cap + 1) * (1 + keyw + r.npay) * 8; break;
+      case DQ_RES_AGG: b += (cap + 1) * (1 + keyw + r.naggs) * 8; break;
+      case DQ_RES_MULTI: {
+        uint64_t rows = cap;
+        for (int p = 0; p < d.npipes; ++p) {
+          const dq_pipeline& pp = d.pipes[p];
+          const dq_op& sink = pp.ops[std::max(pp.nops - 1, 0)];
+          if (sink.kind == DQ_OP_MM_SCATTER && sink.res == i && pp.table) {
+            auto it = ctx->tables.find(pp.table);
+            if (it != ctx->tables.end()) rows = (uint64_t)it->second.nrows;
+          }
+        }
+        b += cap * 8 + rows * widths + 256;
+        break;
+      }
+      case DQ_RES_OUTPUT: b += cap * widths + 256; break;
+    }
+  }
+  return b;
+}
+
+struct SrvReq {
+  uint64_t id = 0;
+  std::shared_ptr<DescCopy> desc;
+  uint64_t est = 0;
+  double t_submit = 0, t_dispatch = 0, t_done = 0;
+  dq_result* result = nullptr;
+  int status = DQ_OK;
+  std::string error;
+  bool done = false;
+  int attempts = 0;                 // executions after tables grew
+  dq_request_info info{};
+};
+
+// Outputs up to this size are copied back inside a pooled plan's CUDA graph
+// (at full capacity, into pinned memory); larger ones are read after the run.
+constexpr uint64_t kGraphOutMax = 16ull << 20;
+
+struct PoolEntry {
+  std::unique_ptr<dq_plan> plan;
+  uint64_t bytes = 0;
+  bool busy = false;
+  int32_t* host_status = nullptr;   // pinned
+  // the whole run (resets, pipelines, status, row count and result columns
+  // copied back) as one graph: one launch per request
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint8_t* host_out = nullptr;      // pinned: row count, then the columns
+  std::vector<uint64_t> col_off;
+  int launches = 0;
+  bool no_graph = false;
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (host_out) cudaFreeHost(host_out);
+    exec = nullptr;
+    graph = nullptr;
+    host_out = nullptr;
+  }
+  ~PoolEntry() {
+    drop_graph();
+    if (host_status) cudaFreeHost(host_status);
+  }
+};
+
+// Captures a pooled plan's run and result copies into a graph (no graph for
+// outputs above kGraphOutMax).
+void srv_build_graph(PoolEntry* pe, cudaStream_t st) {
+  pe->drop_graph();
+  dq_plan* plan = pe->plan.get();
+  const ResRec& o = *plan->res[plan->result_res];
+  uint64_t bytes = 16;
+  pe->col_off.clear();
+  for (int j = 0; j < o.desc.npay; ++j) {
+    pe->col_off.push_back(bytes);
+    bytes = align_up(bytes + o.dev.cap * (uint64_t)ctype_width(o.desc.pay_ctype[j]), 16);
+  }
+  if (bytes > kGraphOutMax) {
+    pe->no_graph = true;
+    return;
+  }
+  DQ_CUDA(cudaMallocHost((void**)&pe->host_out, bytes));
+  DQ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaError_t err = cudaSuccess;
+  try {
+    pe->launches = enqueue_run(plan, st, pe->host_status);
+  } catch (const DqError&) {
+    err = cudaErrorUnknown;
+  }
+  auto rec = [&](cudaError_t e) {
+    if (err == cudaSuccess && e != cudaSuccess) err = e;
+  };
+  rec(cudaMemcpyAsync(pe->host_out, o.cursor.ptr, 8, cudaMemcpyDeviceToHost, st));
+  for (int j = 0; j < o.desc.npay; ++j)
+    rec(cudaMemcpyAsync(pe->host_out + pe->col_off[j], o.dev.pay[j],
+                        o.dev.cap * (uint64_t)ctype_width(o.desc.pay_ctype[j]), cudaMemcpyDeviceToHost, st));
+  cudaGraph_t g = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(st, &g);
+  pe->graph = g;
+  DQ_CUDA(err);
+  DQ_CUDA(end);
+  DQ_CUDA(cudaGraphInstantiate(&pe->exec, pe->graph, 0));
+}
+
+dq_result* srv_graph_result(PoolEntry* pe) {
+  const ResRec& o = *pe->plan->res[pe->plan->result_res];
+  uint64_t n = 0;
+  memcpy(&n, pe->host_out, 8);
+  if (n > o.dev.cap) n = o.dev.cap;
+  std::unique_ptr<dq_result> res(new dq_result());
+  res->nrows = (int64_t)n;
+  for (int j = 0; j < o.desc.npay; ++j) {
+    const int w = ctype_width(o.desc.pay_ctype[j]);
+    res->ctypes.push_back(o.desc.pay_ctype[j]);
+    const uint8_t* src = pe->host_out + pe->col_off[j];
+    res->cols.emplace_back(src, src + (size_t)n * w);
+  }
+  return res.release();
+}
+
+struct SrvSlot {
+  cudaStream_t st = nullptr;
+  cudaEvent_t done = nullptr;
+  SrvReq* req = nullptr;
+  PoolEntry* pe = nullptr;
+  int launches = 0;
+};
+
+}  // namespace
+
+struct dq_server {
+  dq_ctx* ctx = nullptr;
+  dq_server_config cfg{};
+  std::mutex mu;                    // requests, pending queue, statistics
+  std::condition_variable cv;
+  std::deque<SrvReq*> pending;
+  std::unordered_map<uint64_t, std::unique_ptr<SrvReq>> reqs;
+  uint64_t next_id = 1;
+  // owned by the worker thread
+  std::unordered_map<std::string, std::vector<std::unique_ptr<PoolEntry>>> pool;
+  std::vector<SrvSlot> slots;
+  uint64_t mem = 0;
+  // statistics (under mu)
+  uint64_t submitted = 0, completed = 0, failed = 0, mem_peak = 0, mem_now = 0;
+  std::vector<double> lat;
+  double t_first = 0, t_last = 0;
+  bool stop = false;
+  std::thread worker;
+};
+
+namespace {
+
+void srv_finish(dq_server* s, SrvReq* r, int status, const std::string& err, dq_result* res) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  r->status = status;
+  r->error = err;
+  r->result = res;
+  r->t_done = now_ms();
+  r->done = true;
+  r->info.status = status;
+  r->info.total_ms = r->t_done - r->t_submit;
+  r->info.queue_ms = r->t_dispatch > 0 ? r->t_dispatch - r->t_submit : r->info.total_ms;
+  r->info.run_ms = r->t_dispatch > 0 ? r->t_done - r->t_dispatch : 0;
+  if (status == DQ_OK) {
+    ++s->completed;
+    s->lat.push_back(r->info.total_ms);
+  } else {
+    ++s->failed;
+  }
+  s->t_last = r->t_done;
+  s->mem_now = s->mem;
+  s->mem_peak = std::max(s->mem_peak, s->mem);
+  s->cv.notify_all();
+}
+
+// Frees idle pooled plans (other than those of `keep`) until `need` more bytes
+// fit the budget; returns whether they fit.
+bool srv_make_room(dq_server* s, uint64_t need, const std::string& keep) {
+  for (auto& kv : s->pool) {
+    if (s->mem + need <= s->cfg.memory_budget) break;
+    if (kv.first == keep) continue;
+    auto& v = kv.second;
+    for (size_t i = 0; i < v.size() && s->mem + need > s->cfg.memory_budget;) {
+      if (!v[i]->busy) {
+        s->mem -= v[i]->bytes;
+        v.erase(v.begin() + i);
+      } else {
+        ++i;
+      }
+    }
+  }
+  return s->mem + need <= s->cfg.memory_budget;
+}
+
+// A prepared plan for the request: an idle one of the same query, else a new
+// one if the budget allows.  nullptr: wait; throws: the request fails.
+PoolEntry* srv_acquire(dq_server* s, SrvReq* r) {
+  auto& v = s->pool[r->desc->key];
+  for (auto& e : v)
+    if (!e->busy) {
+      e->busy = true;
+      return e.get();
+    }
+  if (!srv_make_room(s, r->est, r->desc->key)) {
+    bool any_busy = false;
+    for (auto& kv : s->pool)
+      for (auto& e : kv.second) any_busy |= e->busy;
+    if (!any_busy) throw DqError(DQ_ERR_ADMISSION, "request needs more device memory than the server's budget");
+    return nullptr;
+  }
+  std::unique_ptr<PoolEntry> e(new PoolEntry());
+  e->plan = make_plan(s->ctx, &r->desc->d, PlanOpts());
+  e->bytes = plan_bytes(e->plan.get());
+  DQ_CUDA(cudaMallocHost((void**)&e->host_status, 4));
+  s->mem += e->bytes;
+  e->busy = true;
+  v.push_back(std::move(e));
+  return v.back().get();
+}
+
+void srv_release(dq_server* s, SrvReq* r, PoolEntry* pe) {
+  pe->busy = false;
+  auto& v = s->pool[r->desc->key];
+  int idle = 0;
+  for (auto& e : v) idle += !e->busy;
+  if (idle > s->cfg.pool_per_query)
+    for (size_t i = 0; i < v.size(); ++i)
+      if (v[i].get() == pe) {
+        s->mem -= pe->bytes;
+        v.erase(v.begin() + i);
+        break;
+      }
+}
+
+void srv_dispatch(dq_server* s, SrvSlot& slot, SrvReq* r, PoolEntry* pe) {
+  slot.req = r;
+  slot.pe = pe;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->t_dispatch = now_ms();
+    r->info.bytes = pe->bytes;
+  }
+  if (!pe->exec && !pe->no_graph) srv_build_graph(pe, slot.st);
+  if (pe->exec) {
+    DQ_CUDA(cudaGraphLaunch(pe->exec, slot.st));
+    slot.launches = pe->launches;
+  } else {
+    slot.launches = enqueue_run(pe->plan.get(), slot.st, pe->host_status);
+  }
+  DQ_CUDA(cudaEventRecord(slot.done, slot.st));
+}
+
+// A slot whose event completed: its result, or a re-run after growing the
+// tables that overflowed.
+void srv_complete(dq_server* s, SrvSlot& slot) {
+  SrvReq* r = slot.req;
+  PoolEntry* pe = slot.pe;
+  const int32_t status = *pe->host_status;
+  if (status != 0 && !(status & (kErrTimeout | kErrBadOp)) && r->attempts < 8) {
+    ++r->attempts;
+    const uint64_t before = pe->bytes;
+    grow_plan(pe->plan.get(), status);
+    pe->bytes = plan_bytes(pe->plan.get());
+    s->mem = s->mem - before + pe->bytes;
+    r->info.kernel_launches += slot.launches;
+    pe->drop_graph();  // the tables moved: capture again
+    pe->no_graph = false;
+    srv_build_graph(pe, slot.st);
+    if (pe->exec) {
+      DQ_CUDA(cudaGraphLaunch(pe->exec, slot.st));
+      slot.launches = pe->launches;
+    } else {
+      slot.launches = enqueue_run(pe->plan.get(), slot.st, pe->host_status);
+    }
+    DQ_CUDA(cudaEventRecord(slot.done, slot.st));
+    return;
+  }
+  slot.req = nullptr;
+  slot.pe = nullptr;
+  if (status != 0) {
+    srv_release(s, r, pe);
+    srv_finish(s, r, status & kErrTimeout ? DQ_ERR_TIMEOUT : DQ_ERR_BAD_IR, "device status " + std::to_string(status),
+               nullptr);
+    return;
+  }
+  r->info.kernel_launches += slot.launches;
+  dq_result* res;
+  if (pe->exec) {
+    res = srv_graph_result(pe);
+  } else {
+    collect_timing(pe->plan.get(), slot.launches);
+    res = read_result(pe->plan.get(), slot.st);
+  }
+  srv_release(s, r, pe);
+  srv_finish(s, r, DQ_OK, "", res);
+}
+
+void srv_loop(dq_server* s) {
+  cudaSetDevice(s->ctx->device);
+  for (;;) {
+    bool busy = false, progressed = false;
+    {
+      std::lock_guard<std::mutex> lk(s->ctx->mu);
+      // completions
+      for (auto& slot : s->slots) {
+        if (!slot.req) continue;
+        busy = true;
+        const cudaError_t q = cudaEventQuery(slot.done);
+        if (q == cudaErrorNotReady) continue;
+        progressed = true;
+        SrvReq* r = slot.req;
+        try {
+          if (q != cudaSuccess) throw DqError(DQ_ERR_CUDA, std::string("request execution: ") + cudaGetErrorString(q));
+          srv_complete(s, slot);
+        } catch (const DqError& e) {
+          if (slot.pe) srv_release(s, r, slot.pe);
+          slot.req = nullptr;
+          slot.pe = nullptr;
+          srv_finish(s, r, e.code, e.what(), nullptr);
+        } catch (const std::exception& e) {
+          if (slot.pe) srv_release(s, r, slot.pe);
+          slot.req = nullptr;
+          slot.pe = nullptr;
+          srv_finish(s, r, DQ_ERR_CUDA, e.what(), nullptr);
+        }
+      }
+      // admissions, oldest first, while a slot and memory are free
+      for (auto& slot : s->slots) {
+        if (slot.req) continue;
+        SrvReq* r = nullptr;
+        {
+          std::lock_guard<std::mutex> lk2(s->mu);
+          if (s->pending.empty()) break;
+          r = s->pending.front();
+        }
+        PoolEntry* pe = nullptr;
+        try {
+          pe = srv_acquire(s, r);
+          if (!pe) break;
+          {
+            std::lock_guard<std::mutex> lk2(s->mu);
+            s->pending.pop_front();
+            s->mem_peak = std::max(s->mem_peak, s->mem);
+            s->mem_now = s->mem;
+          }
+          srv_dispatch(s, slot, r, pe);
+        } catch (const DqError& e) {
+          {
+            std::lock_guard<std::mutex> lk2(s->mu);
+            if (!s->pending.empty() && s->pending.front() == r) s->pending.pop_front();
+          }
+          if (pe) srv_release(s, r, pe);
+          slot.req = nullptr;
+          slot.pe = nullptr;
+          srv_finish(s, r, e.code, e.what(), nullptr);
+        } catch (const std::exception& e) {
+          {
+            std::lock_guard<std::mutex> lk2(s->mu);
+            if (!s->pending.empty() && s->pending.front() == r) s->pending.pop_front();
+          }
+          if (pe) srv_release(s, r, pe);
+          slot.req = nullptr;
+          slot.pe = nullptr;
+          srv_finish(s, r, DQ_ERR_CUDA, e.what(), nullptr);
+        }
+        progressed = true;
+        busy = true;
+      }
+    }
+    if (progressed) continue;
+    if (busy) {
+      std::this_thread::sleep_for(std::chrono::microseconds(4));
+      continue;
+    }
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->stop && s->pending.empty()) break;
+    if (s->pending.empty()) s->cv.wait_for(lk, std::chrono::milliseconds(2));
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int dq_server_start(dq_ctx* ctx, const dq_server_config* cfg, dq_server** out) {
+  if (!ctx || !out) return fail(ctx, DQ_ERR_INVALID, "bad arguments");
+  *out = nullptr;
+  return guarded(ctx, [&]() {
+    if (ctx->offline) throw DqError(DQ_ERR_UNSUPPORTED, "an offline context cannot serve");
+    std::unique_ptr<dq_server> s(new dq_server());
+    s->ctx = ctx;
+    if (cfg) s->cfg = *cfg;
+    if (s->cfg.slots <= 0) s->cfg.slots = 8;
+    if (s->cfg.slots > 64) s->cfg.slots = 64;
+    if (s->cfg.pool_per_query <= 0) s->cfg.pool_per_query = s->cfg.slots;  // no plan churn: freeing synchronises the device
+    if (s->cfg.memory_budget == 0) s->cfg.memory_budget = 150ull << 30;
+    {
+      std::lock_guard<std::mutex> lk(ctx->mu);
+      DQ_CUDA(cudaSetDevice(ctx->device));
+      s->slots.resize(s->cfg.slots);
+      for (auto& slot : s->slots) {
+        DQ_CUDA(cudaStreamCreateWithFlags(&slot.st, cudaStreamNonBlocking));
+        DQ_CUDA(cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming));
+      }
+    }
+    dq_server* raw = s.get();
+    s->worker = std::thread(srv_loop, raw);
+    *out = s.release();
+    return (int)DQ_OK;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+uint64_t srv_submit(dq_server* s, const std::shared_ptr<DescCopy>& desc, uint64_t est) {
+  std::unique_ptr<SrvReq> r(new SrvReq());
+  r->desc = desc;
+  r->est = est;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stop) throw DqError(DQ_ERR_INVALID, "server is stopping");
+  r->id = s->next_id++;
+  r->t_submit = now_ms();
+  if (s->submitted == 0) s->t_first = r->t_submit;
+  ++s->submitted;
+  const uint64_t id = r->id;
+  s->pending.push_back(r.get());
+  s->reqs[id] = std::move(r);
+  s->cv.notify_all();
+  return id;
+}
+
+// Waits for a request; returns its status, fills *out and *info.
+int srv_wait(dq_server* s, uint64_t ticket, dq_result** out, dq_request_info* info) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return fail(s->ctx, DQ_ERR_NOT_FOUND, "unknown ticket");
+  SrvReq* r = it->second.get();
+  s->cv.wait(lk, [&]() { return r->done; });
+  const int status = r->status;
+  if (info) *info = r->info;
+  *out = r->result;
+  if (status != DQ_OK) s->ctx->error = r->error;
+  s->reqs.erase(it);
+  return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dq_server_submit(dq_server* s, const dq_plan_desc* desc, uint64_t* ticket) {
+  if (!s || !desc || !ticket) return DQ_ERR_INVALID;
+  return guarded(s->ctx, [&]() {
+    std::shared_ptr<DescCopy> d = copy_desc(desc);
+    uint64_t est;
+    {
+      std::lock_guard<std::mutex> lk(s->ctx->mu);
+      est = estimate_bytes(s->ctx, d->d);
+    }
+    *ticket = srv_submit(s, d, est);
+    return (int)DQ_OK;
+  });
+}
+
+int dq_server_replay(dq_server* s, int32_t nq, const dq_plan_desc* queries, int64_t nreq, const double* arrival_ms,
+                     const int32_t* query_of, dq_request_info* infos) {
+  if (!s || nq <= 0 || !queries || nreq < 0 || (nreq > 0 && (!arrival_ms || !query_of || !infos)))
+    return DQ_ERR_INVALID;
+  return guarded(s->ctx, [&]() {
+    std::vector<std::shared_ptr<DescCopy>> descs;
+    std::vector<uint64_t> est;
+    for (int q = 0; q < nq; ++q) descs.push_back(copy_desc(&queries[q]));
+    {
+      std::lock_guard<std::mutex> lk(s->ctx->mu);
+      for (auto& d : descs) est.push_back(estimate_bytes(s->ctx, d->d));
+    }
+    for (int64_t i = 0; i < nreq; ++i)
+      if (query_of[i] < 0 || query_of[i] >= nq) throw DqError(DQ_ERR_INVALID, "request names no query");
+    std::vector<uint64_t> tickets((size_t)nreq);
+    const double t0 = now_ms();
+    for (int64_t i = 0; i < nreq; ++i) {
+      const double target = t0 + arrival_ms[i];
+      for (double t = now_ms(); t < target; t = now_ms()) {
+        if (target - t > 0.3) std::this_thread::sleep_for(std::chrono::microseconds((int64_t)((target - t - 0.2) * 1e3)));
+      }
+      tickets[i] = srv_submit(s, descs[query_of[i]], est[query_of[i]]);
+    }
+    int first_error = DQ_OK;
+    for (int64_t i = 0; i < nreq; ++i) {
+      dq_result* res = nullptr;
+      const int st = srv_wait(s, tickets[i], &res, &infos[i]);
+      if (res) delete res;
+      if (st != DQ_OK && first_error == DQ_OK) first_error = st;
+    }
+    return first_error;
+  });
+}
+
+int dq_plan_run_sequence(dq_plan* const* plans, int32_t nplans, int64_t nreq, const int32_t* plan_of, double* ms_out) {
+  if (!plans || nplans <= 0 || nreq < 0 || (nreq > 0 && (!plan_of || !ms_out))) return DQ_ERR_INVALID;
+  for (int64_t i = 0; i < nreq; ++i) {
+    if (plan_of[i] < 0 || plan_of[i] >= nplans || !plans[plan_of[i]]) return DQ_ERR_INVALID;
+    const double t = now_ms();
+    dq_result* res = nullptr;
+    const int st = dq_plan_execute(plans[plan_of[i]], nullptr, &res);
+    if (st != DQ_OK) return st;
+    dq_result_free(res);
+    ms_out[i] = now_ms() - t;
+  }
+  return DQ_OK;
+}
+
+int dq_server_wait(dq_server* s, uint64_t ticket, dq_result** out, dq_request_info* info) {
+  if (!s || !out) return DQ_ERR_INVALID;
+  *out = nullptr;
+  return srv_wait(s, ticket, out, info);
+}
+
+int dq_server_stats_get(dq_server* s, dq_server_stats* out) {
+  if (!s || !out) return DQ_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(s->mu);
+  memset(out, 0, sizeof(*out));
+  out->submitted = s->submitted;
+  out->completed = s->completed;
+  out->failed = s->failed;
+  out->memory_in_use = s->mem_now;
+  out->memory_peak = s->mem_peak;
+  if (!s->lat.empty()) {
+    std::vector<double> v = s->lat;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double q) { return v[std::min(v.size() - 1, (size_t)(q * (v.size() - 1) + 0.5))]; };
+    out->p50_ms = pct(0.50);
+    out->p99_ms = pct(0.99);
+    double sum = 0;
+    for (double x : v) sum += x;
+    out->mean_ms = sum / v.size();
+  }
+  out->span_ms = s->t_last > s->t_first ? s->t_last - s->t_first : 0;
+  return DQ_OK;
+}
+
+void dq_server_stop(dq_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    s->cv.notify_all();
+  }
+  if (s->worker.joinable()) s->worker.join();
+  {
+    std::lock_guard<std::mutex> lk(s->ctx->mu);
+    cudaSetDevice(s->ctx->device);
+    for (auto& slot : s->slots) {
+      if (slot.st) cudaStreamSynchronize(slot.st);
+    }
+    s->pool.clear();
+    for (auto& slot : s->slots) {
+      if (slot.done) cudaEventDestroy(slot.done);
+      if (slot.st) cudaStreamDestroy(slot.st);
+    }
+  }
+  for (auto& kv : s->reqs)
+    if (kv.second->result) delete kv.second->result;
+  delete s;
 }
 
 }  // extern "C"

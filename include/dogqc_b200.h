@@ -306,6 +306,58 @@ int dq_batch_timing_get(dq_batch* batch, dq_plan_timing* out);  /* total_ms: the
 int dq_batch_size(dq_batch* batch, int32_t* ninst);
 void dq_batch_free(dq_batch* batch);
 
+/* ------------------------------------------------------------ serving -- */
+/* A request loop on its own thread over one context's resident tables.  A
+ * request is a plan IR; the server keeps prepared plans pooled per distinct
+ * request (tables, built hash tables and compiled kernels stay resident),
+ * admits the oldest waiting request when one of `slots` CUDA streams is free
+ * and its estimated table and intermediate bytes fit `memory_budget` beside
+ * the plans already held (idle pooled plans are freed to make room; a request
+ * larger than the whole budget fails with DQ_ERR_ADMISSION), and enqueues it
+ * without waiting, so that requests arriving while others run are admitted as
+ * slots and memory free up and their kernels overlap on the device.  No
+ * counterpart in the reference, which runs one query per process.          */
+typedef struct dq_server dq_server;
+typedef struct {
+    int32_t slots;                   /* requests in flight (streams); 0: 8      */
+    int32_t pool_per_query;          /* idle plans kept per request; 0: slots  */
+    uint64_t memory_budget;          /* bytes; 0: 150 GB                         */
+    int32_t reserved[4];
+} dq_server_config;
+typedef struct {
+    double queue_ms;                 /* submitted -> dispatched to a stream      */
+    double run_ms;                   /* dispatched -> result read                */
+    double total_ms;                 /* submitted -> result ready                */
+    uint64_t bytes;                  /* device bytes of the plan that ran it     */
+    int32_t status;                  /* dq_status of the request                 */
+    int32_t kernel_launches;
+} dq_request_info;
+typedef struct {
+    uint64_t submitted, completed, failed;
+    uint64_t memory_in_use, memory_peak;   /* bytes of pooled plans              */
+    double p50_ms, p99_ms, mean_ms;        /* total latency of completed requests */
+    double span_ms;                        /* first submit -> last completion    */
+} dq_server_stats;
+int dq_server_start(dq_ctx* ctx, const dq_server_config* cfg, dq_server** out);
+/* Copies the IR; the tables it names must stay registered until the request
+ * completes.                                                               */
+int dq_server_submit(dq_server* server, const dq_plan_desc* desc, uint64_t* ticket);
+/* Blocks until the request completes; returns its status; *out: its result. */
+int dq_server_wait(dq_server* server, uint64_t ticket, dq_result** out, dq_request_info* info);
+int dq_server_stats_get(dq_server* server, dq_server_stats* out);
+/* Measurement driver: submits request i (query `query_of[i]` of `queries`)
+ * at `arrival_ms[i]` after the call starts, from the calling thread, then
+ * waits for all of them; infos[i] receives each request's times (results are
+ * discarded).  Returns the first failed request's status, else DQ_OK.      */
+int dq_server_replay(dq_server* server, int32_t nq, const dq_plan_desc* queries, int64_t nreq,
+                     const double* arrival_ms, const int32_t* query_of, dq_request_info* infos);
+/* The one-at-a-time reference point: executes plans[plan_of[i]] for every i
+ * in order, each to completion (result read and freed); ms_out[i]: its time. */
+int dq_plan_run_sequence(dq_plan* const* plans, int32_t nplans, int64_t nreq, const int32_t* plan_of,
+                         double* ms_out);
+/* Finishes the waiting and running requests, then frees the server.        */
+void dq_server_stop(dq_server* server);
+
 /* ------------------------------------------------------------ results -- */
 int dq_result_rows(dq_result* r, int64_t* nrows);
 int dq_result_ncols(dq_result* r, int32_t* ncols);

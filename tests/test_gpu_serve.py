@@ -1,0 +1,100 @@
+"""Served form on the GPU: results are the same alone and in a concurrent mix,
+admission by memory, statistics."""
+import pytest
+
+from canonical import canonical_rows
+from evaluator import run_plan
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine():
+    from dogqc_b200.engine import Engine
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+@pytest.fixture(scope="module")
+def queries(engine):
+    from dogqc_b200 import serve
+    qs = serve.make_queries(sizes=(0.0005, 0.004))
+    serve.register(engine, qs)
+    return qs
+
+
+def test_results_same_alone_and_in_mix(engine, queries):
+    from dogqc_b200 import serve
+    want = [canonical_rows(run_plan(q.base_db, q.plan)[1]) for q in queries]
+    alone = []
+    for q in queries:
+        p = engine.prepare(q.lowering)
+        try:
+            alone.append(canonical_rows(p.execute().rows()))
+        finally:
+            p.free()
+    assert alone == want
+    srv = serve.Server(engine, slots=6)
+    try:
+        sched = serve.arrivals(48, None, queries, seed=7)   # all at once: maximal overlap
+        results, infos, wall, errors = serve.mixed_stream(srv, queries, sched)
+        assert not errors
+        for (at, qi), res in zip(sched, results):
+            assert canonical_rows(res.rows()) == want[qi]
+        st = srv.stats()
+        assert st["completed"] == 48 and st["failed"] == 0
+        assert st["p99_ms"] >= st["p50_ms"] > 0
+        assert all(i["total_ms"] >= i["queue_ms"] for i in infos)
+    finally:
+        srv.stop()
+
+
+def test_poisson_arrivals(engine, queries):
+    from dogqc_b200 import serve
+    srv = serve.Server(engine, slots=4)
+    try:
+        sched = serve.arrivals(30, 2000.0, queries, seed=11)
+        results, infos, wall, errors = serve.mixed_stream(srv, queries, sched)
+        assert not errors and len(results) == 30
+        assert srv.stats()["completed"] == 30
+    finally:
+        srv.stop()
+
+
+def test_admission_rejects_oversized_request(engine, queries):
+    from dogqc_b200 import _lib as L, serve
+    srv = serve.Server(engine, slots=2, memory_budget=64 << 10)
+    try:
+        t = srv.submit(queries[-1].lowering)
+        with pytest.raises(L.DqError) as ei:
+            srv.wait(t)
+        assert ei.value.status == L.ERR_ADMISSION
+    finally:
+        srv.stop()
+
+
+def test_tight_budget_evicts_and_completes(engine, queries):
+    """A budget that holds about one plan: requests wait for memory, idle plans
+    are freed, every request still completes with the right result."""
+    from dogqc_b200 import serve
+    want = {i: canonical_rows(run_plan(q.base_db, q.plan)[1]) for i, q in enumerate(queries)}
+    srv = serve.Server(engine, slots=4)
+    try:  # the device bytes of every query's plan
+        sched = [(0.0, i) for i in range(len(queries))]
+        _, infos, _, errors = serve.mixed_stream(srv, queries, sched)
+        assert not errors
+        need = max(i["bytes"] for i in infos)
+    finally:
+        srv.stop()
+    budget = need + need // 2
+    srv = serve.Server(engine, slots=4, memory_budget=budget)
+    try:
+        sched = serve.arrivals(16, None, queries, seed=3)
+        results, infos, wall, errors = serve.mixed_stream(srv, queries, sched)
+        assert not errors
+        for (at, qi), res in zip(sched, results):
+            assert canonical_rows(res.rows()) == want[qi]
+        assert srv.stats()["memory_peak"] <= budget
+    finally:
+        srv.stop()
