@@ -153,7 +153,9 @@ def warm(server, queries, slots, rounds=2):
     """Fills the server's plan pool: every query runs `slots` times at once,
     `rounds` times (preparing a pooled plan and capturing its graph is the slow
     first step of a query; a served stream then finds them ready)."""
-    sched = [(0.0, qi) for _ in range(slots) for qi in range(len(queries))]
+    # each query `slots` times in a row: with first-come admission that many
+    # copies of it run at once, so its pool holds a plan for every slot
+    sched = [(0.0, qi) for qi in range(len(queries)) for _ in range(slots)]
     for _ in range(rounds):
         replay(server, queries, sched)
 
