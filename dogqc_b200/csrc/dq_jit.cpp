@@ -201,6 +201,47 @@ struct Gen {
     return !(R.nkeys == 1 && narrow(R.key_ctype[0])) && R.nkeys > 0;
   }
 
+  // Declares `int64_t g_`: the global aggregation slot of packed tag `tag`
+  // (agg_slot_global's packed-key claim, inline: find the tag or claim an empty
+  // slot with a compare-and-swap; the all-ones key has its own slot).  Inline
+  // because a call needs an ABI stack frame in the calling kernel.
+  void packed_claim(int r, const std::string& tag) {
+    const DevRes& R = P.res[r];
+    const std::string W = num(R.words);
+    L("int64_t g_ = -1;");
+    L("{");
+    ++ind;
+    L("uint64_t* const gs_ = " + res(r) + ".slots;");
+    L("const uint32_t gc_ = (uint32_t)" + res(r) + ".cap;");
+    if (tag_can_be_empty(r)) {
+      L("if (" + tag + " == kEmpty) {");
+      L("  atomicCAS((unsigned long long*)(gs_ + (uint64_t)gc_ * " + W + "), kEmpty, 0ull);");
+      L("  g_ = (int64_t)gc_;");
+      L("} else {");
+      ++ind;
+    }
+    L("uint32_t i_ = slot_of(" + tag + ", gc_);");
+    L("for (uint32_t n_ = 0; n_ < gc_; ++n_) {");
+    ++ind;
+    L("uint64_t* const s_ = gs_ + (uint64_t)i_ * " + W + ";");
+    L("const uint64_t t_ = *(volatile uint64_t*)s_;");
+    L("if (t_ == " + tag + ") { g_ = (int64_t)i_; break; }");
+    L("if (t_ == kEmpty) {");
+    L("  const uint64_t o_ = atomicCAS((unsigned long long*)s_, kEmpty, " + tag + ");");
+    L("  if (o_ == kEmpty || o_ == " + tag + ") { g_ = (int64_t)i_; break; }");
+    L("}");
+    L("i_ = (i_ + 1u == gc_) ? 0u : i_ + 1u;");
+    --ind;
+    L("}");
+    L("if (g_ < 0) set_status(P, kErrHtFull);");
+    if (tag_can_be_empty(r)) {
+      --ind;
+      L("}");
+    }
+    --ind;
+    L("}");
+  }
+
   void L(const std::string& s) {
     o.append((size_t)ind * 2, ' ');
     o += s;
@@ -648,41 +689,7 @@ struct Gen {
     else L("const uint64_t tag_ = key_tag(" + res(r) + ", " + k + ");");
     auto global = [&]() {
       if (R.packed) {
-        // agg_slot_global's packed-key claim, inline: find the tag or claim an
-        // empty slot with a compare-and-swap; the all-ones key has its own slot
-        const std::string W = num(R.words);
-        L("int64_t g_ = -1;");
-        L("{");
-        ++ind;
-        L("uint64_t* const gs_ = " + res(r) + ".slots;");
-        L("const uint32_t gc_ = (uint32_t)" + res(r) + ".cap;");
-        if (tag_can_be_empty(r)) {
-          L("if (tag_ == kEmpty) {");
-          L("  atomicCAS((unsigned long long*)(gs_ + (uint64_t)gc_ * " + W + "), kEmpty, 0ull);");
-          L("  g_ = (int64_t)gc_;");
-          L("} else {");
-          ++ind;
-        }
-        L("uint32_t i_ = slot_of(tag_, gc_);");
-        L("for (uint32_t n_ = 0; n_ < gc_; ++n_) {");
-        ++ind;
-        L("uint64_t* const s_ = gs_ + (uint64_t)i_ * " + W + ";");
-        L("const uint64_t t_ = *(volatile uint64_t*)s_;");
-        L("if (t_ == tag_) { g_ = (int64_t)i_; break; }");
-        L("if (t_ == kEmpty) {");
-        L("  const uint64_t o_ = atomicCAS((unsigned long long*)s_, kEmpty, tag_);");
-        L("  if (o_ == kEmpty || o_ == tag_) { g_ = (int64_t)i_; break; }");
-        L("}");
-        L("i_ = (i_ + 1u == gc_) ? 0u : i_ + 1u;");
-        --ind;
-        L("}");
-        L("if (g_ < 0) set_status(P, kErrHtFull);");
-        if (tag_can_be_empty(r)) {
-          --ind;
-          L("}");
-        }
-        --ind;
-        L("}");
+        packed_claim(r, "tag_");
       } else {
         L("const int64_t g_ = agg_slot_global(P, " + res(r) + ", tag_, " + k + ");");
       }
@@ -969,7 +976,8 @@ struct Gen {
     L("uint64_t v_ = lacc[i * " + num(copies) + "];");
     if (copies > 1) L("for (int c_ = 1; c_ < " + num(copies) + "; ++c_) v_ = red_combine(red_, v_, lacc[i * " +
                       num(copies) + " + c_]);");
-    L("const int64_t g_ = agg_slot_global(P, " + rr + ", tg_, nullptr);");
+    if (R.packed) packed_claim(agg_res, "tg_");
+    else L("const int64_t g_ = agg_slot_global(P, " + rr + ", tg_, nullptr);");
     L("if (g_ >= 0) accumulate(" + rr + ".slots + (uint64_t)g_ * " + num(R.words) + " + " + num(R.val_word) +
       " + j_, red_, v_);");
     --ind;
@@ -1347,7 +1355,8 @@ void nvrtc_check(nvrtcResult r, const char* what) {
   if (r != NVRTC_SUCCESS) throw Error(std::string(what) + ": " + nvrtcGetErrorString(r));
 }
 
-void build(Entry& e, const std::string& src) {
+// One NVRTC compilation of `src`; false (log kept) when it does not compile.
+bool compile_once(const std::string& src, bool ld256, std::string& log, std::vector<char>& cubin) {
   std::vector<const char*> hdrs, names;
   for (int i = 0; i < kEmbedCount; ++i) {
     hdrs.push_back(kEmbedText[i]);
@@ -1360,29 +1369,35 @@ void build(Entry& e, const std::string& src) {
   nvrtcProgram prog;
   nvrtc_check(nvrtcCreateProgram(&prog, src.c_str(), "dq_pipeline.cu", (int)hdrs.size(), hdrs.data(), names.data()),
               "nvrtcCreateProgram");
-  // the NVRTC the process resolved (an application may have loaded an older
-  // one first): 256-bit loads for sm_100a need 12.9
-  int major = 0, minor = 0;
-  nvrtcVersion(&major, &minor);
-  const bool ld256 = major > 12 || (major == 12 && minor >= 9);
   const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-lineinfo",
                         "--ptxas-options=-v", ld256 ? "-DDQ_LD256=1" : "-DDQ_LD256=0"};
   nvrtcResult r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
   size_t n = 0;
   nvrtcGetProgramLogSize(prog, &n);
-  e.log.assign(n, '\0');
-  if (n) nvrtcGetProgramLog(prog, &e.log[0]);
-  while (!e.log.empty() && e.log.back() == '\0') e.log.pop_back();
-  e.log = "NVRTC " + std::to_string(major) + "." + std::to_string(minor) + "\n" + e.log;
+  log.assign(n, '\0');
+  if (n) nvrtcGetProgramLog(prog, &log[0]);
+  while (!log.empty() && log.back() == '\0') log.pop_back();
   if (r != NVRTC_SUCCESS) {
     nvrtcDestroyProgram(&prog);
-    throw Error("generated pipeline kernel failed to compile:\n" + e.log);
+    return false;
   }
   size_t cb = 0;
   nvrtc_check(nvrtcGetCUBINSize(prog, &cb), "nvrtcGetCUBINSize");
-  e.cubin.resize(cb);
-  nvrtc_check(nvrtcGetCUBIN(prog, e.cubin.data()), "nvrtcGetCUBIN");
+  cubin.resize(cb);
+  nvrtc_check(nvrtcGetCUBIN(prog, cubin.data()), "nvrtcGetCUBIN");
   nvrtcDestroyProgram(&prog);
+  return true;
+}
+
+void build(Entry& e, const std::string& src) {
+  // the NVRTC the process resolved (an application may have loaded an older
+  // one first): 256-bit loads for sm_100a need 12.9
+  int major = 0, minor = 0;
+  nvrtcVersion(&major, &minor);
+  const bool ld256 = major > 12 || (major == 12 && minor >= 9);
+  const bool ok = compile_once(src, ld256, e.log, e.cubin);
+  e.log = "NVRTC " + std::to_string(major) + "." + std::to_string(minor) + "\n" + e.log;
+  if (!ok) throw Error("generated pipeline kernel failed to compile:\n" + e.log);
 }
 
 }  // namespace

@@ -1,0 +1,63 @@
+"""CPU checks of the kernel generator: with DQ_CFG_OFFLINE a context needs no
+device, and preparing a plan generates and compiles (NVRTC, sm_100a) every
+pipeline's kernel.  Every workload shape compiles without register spills,
+under the default launch shape; the tunings the autotuner searches compile
+with at most a few spilled words (NVRTC 12.9's register allocation differs from
+nvcc's for some one-row-per-thread kernels)."""
+import re
+
+import pytest
+
+from dogqc_b200 import _lib as L
+from dogqc_b200 import workloads as W
+from dogqc_b200.engine import Engine
+from dogqc_b200.relational import RelationalAlgebra
+
+SCALE = 0.001
+
+
+@pytest.fixture(scope="module")
+def engine():
+    e = Engine(0, flags=L.CFG_OFFLINE)
+    yield e
+    e.close()
+
+
+def resolved(engine, name):
+    db = W.GENERATORS[name](SCALE)
+    alg = RelationalAlgebra(db)
+    plan, cfg = W.build(name, alg)
+    engine.register_database(db)
+    return alg.resolveAlgebraPlan(plan, cfg)
+
+
+def check_sources(plan, max_spill=0):
+    n = len(plan.lowering.pipes)
+    assert n >= 2
+    for i in range(n):
+        src = plan.source(i)
+        assert "dq_main" in src, i
+        assert "#include" in src
+        regs = [int(r) for r in re.findall(r"Used (\d+) registers", src)]
+        assert regs and max(regs) <= 128, (i, regs)
+        spills = [int(b) for b in re.findall(r"(\d+) bytes spill stores", src)]
+        assert spills and max(spills) <= max_spill, (i, spills)
+
+
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "c3"])
+def test_every_workload_compiles_offline(engine, name):
+    plan = engine.prepare(resolved(engine, name))
+    check_sources(plan)
+    with pytest.raises(L.DqError):
+        plan.execute()
+
+
+@pytest.mark.parametrize("tuning", [
+    {"rows_per_thread": 1, "block_threads": 128},
+    {"rows_per_thread": 2, "block_threads": 512, "refill": -1},
+    {"rows_per_thread": 4, "block_threads": 256, "unique_slots_pct": 400, "multi_buckets_pct": 50},
+])
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_tuned_launch_shapes_compile(engine, name, tuning):
+    plan = engine.prepare(resolved(engine, name), tuning=tuning)
+    check_sources(plan, max_spill=32)
