@@ -461,6 +461,24 @@ __device__ __forceinline__ int local_group_slot(uint64_t* tags, int ns, uint64_t
   return -1;
 }
 
+// CTA-local table of multimap buckets (the hot buckets of a skewed build side
+// land in it first): kHotSlots bucket ids, kEmpty32 when free.  Returns the
+// bucket's slot, claiming a free one in its window of kHotProbe slots, or -1.
+
+__device__ __forceinline__ int hot_slot(uint32_t* keys, uint32_t b) {
+  uint32_t idx = __umulhi(b * 0x9E3779B1u, (uint32_t)kHotSlots);
+  for (int n = 0; n < kHotProbe; ++n) {
+    const uint32_t k = ((volatile uint32_t*)keys)[idx];
+    if (k == b) return (int)idx;
+    if (k == kEmpty32) {
+      const uint32_t old = atomicCAS(&keys[idx], kEmpty32, b);
+      if (old == kEmpty32 || old == b) return (int)idx;
+    }
+    idx = (idx + 1) & (uint32_t)(kHotSlots - 1);
+  }
+  return -1;
+}
+
 __device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
   uint32_t lo = __shfl_sync(kFull, (uint32_t)v, src);
   uint32_t hi = __shfl_sync(kFull, (uint32_t)(v >> 32), src);

@@ -20,8 +20,10 @@ enum : int32_t {
   kErrTimeout = 2,
   kErrOverflow = 4,
   kErrBadOp = 8,
-  kErrAggSpill = 16,     // informational: a CTA-local aggregation table spilled
+  kInfoHeavyFull = 32,   // informational: deferred expansion items exceeded their
+                         // capacity; the rest ran in place (results stay exact)
 };
+constexpr int32_t kInfoMask = kInfoHeavyFull;
 
 struct DevCol {           // staged fixed-width column
   const uint8_t* ptr;
@@ -75,7 +77,26 @@ struct DevHeavy {         // deferred wide expansion ranges
   int32_t nstash;
   int32_t op;             // index of the EXPAND op the items belong to
   uint64_t threshold;     // ranges longer than this are deferred
+  // grouped mode (generated kernels): items whose probe rows matched the same
+  // range form a group, and a warp gathers a chunk of the range once for all
+  // of the group's items
+  int32_t grouped;
+  uint32_t gcap;          // group table slots
+  uint64_t* gkey;         // (range length << 32) | range offset; kEmpty: free
+  uint32_t* gcnt;         // items per group slot, then its scatter cursor
+  uint32_t* glist;        // claimed group slots, in claim order
+  uint32_t* ngroups;
+  uint32_t* gstart;       // item prefix over glist (ngroups + 1 entries)
+  uint64_t* sorted;       // the items' stashed values, grouped (cap * nstash)
 };
+
+constexpr int kGroupRows = 32;    // range rows per grouped work unit (a warp)
+constexpr int kGroupItems = 64;   // items per grouped work unit
+constexpr int kGroupThreshold = 128;  // grouped mode: ranges longer than this are deferred
+
+constexpr int kHotSlots = 512;         // CTA-local hot multimap buckets (generated kernels)
+constexpr int kHotProbe = 4;           // probe window in that table
+constexpr uint32_t kEmpty32 = 0xffffffffu;
 
 struct DevPipe {
   int64_t nrows;

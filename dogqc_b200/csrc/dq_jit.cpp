@@ -173,6 +173,9 @@ struct Gen {
   int refill = -1;               // op after which lanes are refilled (-1: none)
   int nbuf = 0;                  // values per row in the warp buffers
   int buf_off = 0;               // shared-memory offset of the warp buffers
+  int hot = 0;                   // multimap sink through the CTA's hot-bucket table:
+                                 // 1 count (flushed at the end), 2 scatter (per step)
+  int hot_off = 0;               // shared-memory offset of that table
   std::string ldfn = "__ldcs";   // load function of streamed source columns
   int block = kBlock;            // threads per CTA
   bool batched = false;          // kernel over many instances of the plan
@@ -581,14 +584,26 @@ struct Gen {
   // check, rest of the ops.  The `pending` mechanism (load at first read)
   // stays available for slots a generator variant wants to defer.
   void pairs(int k, int lv, const std::string& a, const std::string& m, const std::string& exit) {
+    gather_level(k, lv, a, m);
+    match_ops(k, lv, a, exit);
+  }
+
+  // The payload values of level `lv` for match `m` (the key columns first).
+  void gather_level(int k, int lv, const std::string& a, const std::string& m) {
     const dq_op& op = P.ops[k];
-    declare_regs(lv);
     for (int q = 0; q < op.nlist2; ++q) {
       int s = P.lists[op.list2 + q];
       if (s >= 0 && slot(s).kind == DQ_SLOT_GATHER && slot(s).level == lv && var[s].empty()) gather(s, a, m);
     }
     for (int s = 0; s < P.nslots; ++s)
       if (slot(s).kind == DQ_SLOT_GATHER && slot(s).level == lv && var[s].empty()) gather(s, a, m);
+  }
+
+  // Key check of a pair whose payload is gathered, then the ops after the
+  // expansion.
+  void match_ops(int k, int lv, const std::string& a, const std::string& exit) {
+    const dq_op& op = P.ops[k];
+    declare_regs(lv);
     for (int q = 0; q < op.nlist; ++q) {
       int t = P.res[op.res].key_ctype[q];
       L(a + " = " + a + " && canon(" + V(P.lists[op.list + q]) + ", " + ct_name(t) + ") == canon(" +
@@ -613,25 +628,62 @@ struct Gen {
     L("const uint32_t b_ = bucket_of(" + kk + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap);");
     L(ec + " = " + res(r) + ".counts[b_];");
     L(eo + " = " + ec + " ? " + res(r) + ".offsets[b_] : 0u;");
+    --ind;
+    L("}");
     if (k == expand_op && level == 0) {
-      L("if (" + ec + " > P.heavy.threshold) {");
+      // deferral of long ranges: one atomic per warp reserves the item slots
+      L("{");
       ++ind;
-      L("const uint32_t hs_ = atomicAdd(P.heavy.count, 1u);");
-      L("if (hs_ < P.heavy.cap) {");
+      L("const bool dw_ = " + ec + " > P.heavy.threshold;");
+      L("const unsigned dm_ = __ballot_sync(kFull, dw_);");
+      L("if (dm_) {");
+      ++ind;
+      L("const int dl_ = __ffs(dm_) - 1;");
+      L("uint32_t db_ = 0u;");
+      L("if (lane == dl_) db_ = atomicAdd(P.heavy.count, (uint32_t)__popc(dm_));");
+      L("db_ = __shfl_sync(kFull, db_, dl_);");
+      L("const uint32_t hs_ = db_ + (uint32_t)__popc(dm_ & ((1u << lane) - 1u));");
+      L("if (dw_ && hs_ < P.heavy.cap) {");
       ++ind;
       L("uint64_t* it_ = P.heavy.items + (size_t)hs_ * P.heavy.words;");
-      L("it_[0] = " + eo + ";");
-      L("it_[1] = " + ec + ";");
+      if (P.heavy.grouped) {
+        // the item joins the group of its range (claimed on first sight); an
+        // item whose claim fails is expanded here and carries kEmpty
+        L("const uint64_t gk_ = ((uint64_t)" + ec + " << 32) | " + eo + ";");
+        L("uint32_t g_ = slot_of(gk_, P.heavy.gcap);");
+        L("uint64_t gid_ = kEmpty;");
+        L("for (uint32_t n_ = 0; n_ < P.heavy.gcap; ++n_) {");
+        L("  const uint64_t t_ = *(volatile uint64_t*)(P.heavy.gkey + g_);");
+        L("  if (t_ == gk_) { gid_ = g_; break; }");
+        L("  if (t_ == kEmpty) {");
+        L("    const uint64_t o_ = atomicCAS((unsigned long long*)(P.heavy.gkey + g_), kEmpty, gk_);");
+        L("    if (o_ == kEmpty) { P.heavy.glist[atomicAdd(P.heavy.ngroups, 1u)] = g_; gid_ = g_; break; }");
+        L("    if (o_ == gk_) { gid_ = g_; break; }");
+        L("  }");
+        L("  g_ = (g_ + 1u == P.heavy.gcap) ? 0u : g_ + 1u;");
+        L("}");
+        L("it_[0] = gid_;");
+        L("if (gid_ != kEmpty) {");
+        ++ind;
+        L("atomicAdd(P.heavy.gcnt + gid_, 1u);");
+      } else {
+        L("it_[0] = " + eo + ";");
+        L("it_[1] = " + ec + ";");
+      }
       for (int s = 0; s < P.nslots; ++s)
         if (slot(s).stash >= 0) L("it_[" + num(2 + slot(s).stash) + "] = " + V(s) + ";");
       L(ec + " = 0u;");
+      if (P.heavy.grouped) {
+        --ind;
+        L("}");
+      }
+      --ind;
+      L("}");
       --ind;
       L("}");
       --ind;
       L("}");
     }
-    --ind;
-    L("}");
     L("uint32_t " + ei + " = " + ec + ";");
     L("#pragma unroll");
     L("for (int d_ = 1; d_ < 32; d_ <<= 1) {");
@@ -761,7 +813,41 @@ struct Gen {
     L("if (" + act + ") {");
     ++ind;
     L("const int lead_ = __ffs(peers_) - 1;");
-    if (op.kind == DQ_OP_MM_COUNT) {
+    if (hot == 1) {
+      L("if (lane == lead_) {");
+      L("  const int hs_ = hot_slot(hk_, b_);");
+      L("  if (hs_ >= 0) atomicAdd(&hc_[hs_], (uint32_t)__popc(peers_));");
+      L("  else atomicAdd(&" + res(r) + ".counts[b_], (uint32_t)__popc(peers_));");
+      L("}");
+    } else if (hot == 2) {
+      // the bucket's offset does not depend on the claim: load it first
+      L("const uint32_t ob_ = " + res(r) + ".offsets[b_];");
+      L("int hs_ = -1;");
+      L("uint32_t at_ = 0;");
+      L("if (lane == lead_) {");
+      L("  hs_ = hot_slot(hk_, b_);");
+      L("  at_ = atomicAdd(hs_ >= 0 ? &hc_[hs_] : &" + res(r) + ".counts[b_], (uint32_t)__popc(peers_));");
+      L("}");
+      L("hs_ = __shfl_sync(peers_, hs_, lead_);");
+      L("at_ = __shfl_sync(peers_, at_, lead_) + (uint32_t)__popc(peers_ & ((1u << lane) - 1u));");
+      L("if (hs_ >= 0) {");
+      ++ind;
+      L("hs_u[u] = hs_;");
+      L("hr_u[u] = ob_ + at_;");
+      for (int j = 0; j < op.nlist2; ++j)
+        if (hot_value(op, j, "u").empty()) L("hv" + num(j) + "_u[u] = " + V(P.lists[op.list2 + j]) + ";");
+      --ind;
+      L("} else {");
+      ++ind;
+      L("const uint32_t pos_ = ob_ + at_;");
+      for (int j = 0; j < op.nlist2; ++j) {
+        int w = R.pay_width[j];
+        L("st(" + res(r) + ".pay[" + num(j) + "] + (size_t)pos_ * " + num(w) + ", " + num(w) + ", " +
+          V(P.lists[op.list2 + j]) + ");");
+      }
+      --ind;
+      L("}");
+    } else if (op.kind == DQ_OP_MM_COUNT) {
       L("if (lane == lead_) atomicAdd(&" + res(r) + ".counts[b_], (uint32_t)__popc(peers_));");
     } else {
       L("uint32_t at_ = 0;");
@@ -864,6 +950,105 @@ struct Gen {
     if (nbuf == 0) nbuf = 1;
     buf_off = (smem + 15) / 16 * 16;
     smem = buf_off + (block / 32) * kWarpBuf * nbuf * 8;
+  }
+
+  // Multimap sinks of a skewed build side meet on a few buckets: a CTA-local
+  // table of buckets takes their counts (count pass) or ranks (scatter pass),
+  // so a hot bucket sees one global atomic per CTA (count) or per CTA and row
+  // step (scatter) instead of one per warp.  The scatter pass reserves ranges
+  // at the end of every row step behind block barriers, so it needs straight
+  // row steps: no lane refill, no expansion.
+  void choose_hot() {
+    hot = 0;
+    if (batched || P.nops == 0) return;
+    const int kind = P.ops[P.nops - 1].kind;
+    if (kind != DQ_OP_MM_COUNT && kind != DQ_OP_MM_SCATTER) return;
+    for (int j = 0; j < P.nops; ++j)
+      if (P.ops[j].kind == DQ_OP_EXPAND) return;
+    if (kind == DQ_OP_MM_SCATTER && refill >= 0) return;
+    hot = kind == DQ_OP_MM_COUNT ? 1 : 2;
+    hot_off = (smem + 15) / 16 * 16;
+    smem = hot_off + kHotSlots * 12;
+  }
+
+  void hot_init() {
+    if (!hot) return;
+    L("uint32_t* const hk_ = reinterpret_cast<uint32_t*>(smem + " + num(hot_off) + ");  // hot buckets");
+    L("uint32_t* const hc_ = hk_ + " + num(kHotSlots) + ";  // their counts (of this step when scattering)");
+    L("uint32_t* const hb_ = hc_ + " + num(kHotSlots) + ";  // their reserved range starts");
+    L("(void)hb_;");
+    L("for (int i = tid; i < " + num(kHotSlots) + "; i += " + num(block) + ") {");
+    L("  hk_[i] = kEmpty32;");
+    L("  hc_[i] = 0u;");
+    L("}");
+    L("__syncthreads();");
+  }
+
+  // Scatter pass: per-row state of the table rows of the current step.
+  void hot_step_begin() {
+    if (hot != 2) return;
+    const dq_op& op = P.ops[P.nops - 1];
+    L("int hs_u[" + num(U) + "];");
+    L("uint32_t hr_u[" + num(U) + "];  // bucket offset + rank in the step");
+    for (int j = 0; j < op.nlist2; ++j)
+      if (hot_value(op, j, "u").empty()) L("uint64_t hv" + num(j) + "_u[" + num(U) + "];");
+    L("#pragma unroll");
+    L("for (int u = 0; u < " + num(U) + "; ++u) hs_u[u] = -1;");
+  }
+
+  // Payload value j of a deferred table row in the scatter's last phase: a
+  // source column value is still in the step's column registers; anything else
+  // was kept in hv<j>_u (empty result).
+  std::string hot_value(const dq_op& op, int j, const std::string& u) {
+    const int s = P.lists[op.list2 + j];
+    if (s >= 0 && slot(s).kind == DQ_SLOT_COL)
+      return "canon(c" + num(slot(s).src) + "[" + u + "], " + ct_name(slot(s).ctype) + ")";
+    return std::string();
+  }
+
+  // Scatter pass: one global range per hot bucket of the step, then the
+  // table rows' payload at range start + rank.
+  void hot_step_end() {
+    if (hot != 2) return;
+    const dq_op& op = P.ops[P.nops - 1];
+    const int r = op.res;
+    const DevRes& R = P.res[r];
+    L("__syncthreads();");
+    L("for (int i = tid; i < " + num(kHotSlots) + "; i += " + num(block) + ") {");
+    L("  const uint32_t c_ = hc_[i];");
+    L("  if (c_) {");
+    L("    hb_[i] = atomicAdd(&" + res(r) + ".counts[hk_[i]], c_);");
+    L("    hc_[i] = 0u;");
+    L("  }");
+    L("}");
+    L("__syncthreads();");
+    L("#pragma unroll");
+    L("for (int u = 0; u < " + num(U) + "; ++u) {");
+    ++ind;
+    L("if (hs_u[u] >= 0) {");
+    ++ind;
+    L("const uint32_t pos_ = hb_[hs_u[u]] + hr_u[u];");
+    for (int j = 0; j < op.nlist2; ++j) {
+      int w = R.pay_width[j];
+      std::string v = hot_value(op, j, "u");
+      if (v.empty()) v = "hv" + num(j) + "_u[u]";
+      L("st(" + res(r) + ".pay[" + num(j) + "] + (size_t)pos_ * " + num(w) + ", " + num(w) + ", " + v + ");");
+    }
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+  }
+
+  // Count pass: the table's counts go to the global ones once per CTA.
+  void hot_flush() {
+    if (hot != 1) return;
+    const int r = P.ops[P.nops - 1].res;
+    L("__syncthreads();");
+    L("for (int i = tid; i < " + num(kHotSlots) + "; i += " + num(block) + ") {");
+    L("  const uint32_t c_ = hc_[i];");
+    L("  if (c_) atomicAdd(&" + res(r) + ".counts[hk_[i]], c_);");
+    L("}");
   }
 
   // Appends the active lanes' live values to the warp's buffer, then drains
@@ -1068,6 +1253,7 @@ struct Gen {
   // ----------------------------------------------------------- kernels --
   void main_kernel() {
     prologue("dq_main");
+    hot_init();
     std::vector<int> cols = source_cols();
     L("const int64_t nrows = source_rows(P);");
     L("const int64_t span = " + num((long long)block * U) + ";");
@@ -1098,7 +1284,9 @@ struct Gen {
         L("}");
       }
     }
+    hot_step_begin();
     row_loop();
+    hot_step_end();
     if (!cols.empty()) {
       L("#pragma unroll");
       L("for (int u = 0; u < " + num(U) + "; ++u) {");
@@ -1107,6 +1295,7 @@ struct Gen {
     }
     --ind;
     L("}");
+    hot_flush();
     epilogue();
   }
 
@@ -1227,9 +1416,92 @@ struct Gen {
     L("}");
   }
 
+  // Deferred items grouped by range: a warp's work unit is 32 rows of one
+  // group's range and up to kGroupItems of its items.  The rows' payload is
+  // gathered once; the items' carried values come 32 at a time in one load and
+  // are broadcast by shuffle, and every (item, row) pair runs the key check
+  // and the ops after the expansion.
+  void heavy_grouped_kernel() {
+    std::fill(var.begin(), var.end(), std::string());
+    pending.clear();
+    prologue("dq_heavy");
+    L("const uint32_t ng = *P.heavy.ngroups < P.heavy.gcap ? *P.heavy.ngroups : P.heavy.gcap;");
+    L("const uint64_t units = P.heavy.unit_prefix[ng];");
+    L("const int ns = P.heavy.nstash;");
+    L("(void)ns;");
+    // the warp's current group and its unit range stay in registers: the
+    // units of a long range come to the same warp in runs
+    L("uint32_t lo = 0;");
+    L("uint64_t ulo = 1, uhi = 0;");
+    L("for (;;) {");
+    ++ind;
+    L("uint32_t unit = 0;");
+    L("if (lane == 0) unit = atomicAdd(P.tile_counter, 1u);");
+    L("unit = __shfl_sync(kFull, unit, 0);");
+    L("if ((uint64_t)unit >= units) break;");
+    L("if ((uint64_t)unit < ulo || (uint64_t)unit >= uhi) {");
+    ++ind;
+    // 32-ary search of the unit prefix: every round the lanes read 32 evenly
+    // spaced entries of [a, b) and keep the segment that holds the unit
+    L("uint32_t a = 0, b = ng;");
+    L("while (b - a > 1u) {");
+    L("  const uint32_t st_ = (b - a + 31u) / 32u;");
+    L("  const uint32_t ix_ = a + (uint32_t)lane * st_;");
+    L("  const bool le_ = ix_ < b && P.heavy.unit_prefix[ix_] <= (uint64_t)unit;");
+    L("  const unsigned m_ = __ballot_sync(kFull, le_);");
+    L("  a = a + (uint32_t)(31 - __clz(m_)) * st_;");
+    L("  b = b < a + st_ ? b : a + st_;");
+    L("}");
+    L("lo = a;");
+    L("ulo = P.heavy.unit_prefix[lo];");
+    L("uhi = P.heavy.unit_prefix[lo + 1];");
+    --ind;
+    L("}");
+    L("const uint64_t gk = P.heavy.gkey[P.heavy.glist[lo]];");
+    L("const uint32_t len = (uint32_t)(gk >> 32);");
+    L("const uint32_t i0 = P.heavy.gstart[lo], ni = P.heavy.gstart[lo + 1] - i0;");
+    L("const uint32_t local = (uint32_t)((uint64_t)unit - ulo);");
+    L("const uint32_t rch = (len + " + num(kGroupRows - 1) + "u) / " + num(kGroupRows) + "u;");
+    L("const uint32_t q = (local % rch) * " + num(kGroupRows) + "u + (uint32_t)lane;");
+    L("const bool a0 = q < len;");
+    L("const uint32_t m = (uint32_t)gk + q;");
+    L("const uint32_t ib = (local / rch) * " + num(kGroupItems) + "u;");
+    L("const uint32_t ie = ni < ib + " + num(kGroupItems) + "u ? ni : ib + " + num(kGroupItems) + "u;");
+    row = "";
+    gather_level(expand_op, 1, "a0", "m");
+    L("for (uint32_t ix = ib; ix < ie; ix += 32u) {");
+    ++ind;
+    std::vector<std::pair<int, std::string>> carried;
+    for (int s = 0; s < P.nslots; ++s)
+      if (slot(s).stash >= 0) {
+        const std::string hl = "hl" + num(s);
+        L("const uint64_t " + hl + " = ix + lane < ie ? P.heavy.sorted[(size_t)(i0 + ix + lane) * ns + " +
+          num(slot(s).stash) + "] : 0ull;");
+        carried.emplace_back(s, hl);
+      }
+    L("const int nt = (int)(ie - ix < 32u ? ie - ix : 32u);");
+    L("for (int t = 0; t < nt; ++t) {");
+    ++ind;
+    for (auto& c : carried) {
+      var[c.first] = "h" + num(c.first);
+      L("const uint64_t " + var[c.first] + " = shfl64(" + c.second + ", t);");
+    }
+    L("bool a = a0;");
+    match_ops(expand_op, 1, "a", "continue;");
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+    epilogue();
+  }
+
   void heavy_kernel() {
-    const dq_op& op = P.ops[expand_op];
-    (void)op;
+    if (P.heavy.grouped) {
+      heavy_grouped_kernel();
+      return;
+    }
     std::fill(var.begin(), var.end(), std::string());
     pending.clear();
     prologue("dq_heavy");
@@ -1295,6 +1567,8 @@ Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t
   g.choose_agg();
   const char* no_refill = getenv("DQ_JIT_REFILL");
   g.choose_refill(no_refill && atoi(no_refill) == 0 ? -1 : refill_op);
+  const char* no_hot = getenv("DQ_JIT_HOT");
+  if (!(no_hot && atoi(no_hot) == 0)) g.choose_hot();
   g.choose_prefetch();
   const char* no_pf = getenv("DQ_JIT_PREFETCH");
   if (no_pf && atoi(no_pf) == 0) g.prefetch.clear();

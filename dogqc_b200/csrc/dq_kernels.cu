@@ -1223,7 +1223,7 @@ __global__ void agg_init_kernel(uint64_t* slots, uint64_t nslots, int words, int
 }
 
 // Multimap bucket offsets: exclusive scan of counts in three passes.
-constexpr int kScanItems = 8;
+constexpr int kScanItems = 16;
 constexpr int kScanChunk = kThreads * kScanItems;
 
 __global__ void mm_scan_partials(const uint32_t* counts, uint64_t n, uint32_t* partials) {
@@ -1238,43 +1238,90 @@ __global__ void mm_scan_partials(const uint32_t* counts, uint64_t n, uint32_t* p
   if (threadIdx.x == 0) partials[blockIdx.x] = total;
 }
 
+// Exclusive scan of the block partials (one block; 8 consecutive partials a
+// thread per round).
 __global__ void mm_scan_top(uint32_t* partials, int nblocks) {
+  constexpr int kPer = 8;
   uint32_t carry = 0;
-  for (int base = 0; base < nblocks; base += kThreads) {
-    int i = base + threadIdx.x;
-    uint32_t x = i < nblocks ? partials[i] : 0;
+  for (int base = 0; base < nblocks; base += kThreads * kPer) {
+    const int i0 = base + threadIdx.x * kPer;
+    uint32_t v[kPer];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      v[k] = i0 + k < nblocks ? partials[i0 + k] : 0u;
+      sum += v[k];
+    }
     uint32_t excl;
-    uint32_t total = block_exclusive_scan(x, excl);
-    if (i < nblocks) partials[i] = carry + excl;
+    const uint32_t total = block_exclusive_scan(sum, excl);
+    uint32_t run = carry + excl;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      if (i0 + k < nblocks) partials[i0 + k] = run;
+      run += v[k];
+    }
     carry += total;
   }
 }
 
+// Offsets of one chunk of buckets (kScanItems consecutive counts a thread, in
+// 16-byte vectors when the chunk is whole) and the counts reset to zero for the
+// scatter pass that follows.
 __global__ void mm_scan_final(uint32_t* counts, uint32_t* offsets, uint64_t n, const uint32_t* partials) {
-  uint64_t base = (uint64_t)blockIdx.x * kScanChunk;
-  uint64_t i0 = base + (uint64_t)threadIdx.x * kScanItems;
+  static_assert(kScanItems % 4 == 0, "vector path");
+  const uint64_t i0 = (uint64_t)blockIdx.x * kScanChunk + (uint64_t)threadIdx.x * kScanItems;
+  const bool whole = i0 + kScanItems <= n;
   uint32_t v[kScanItems];
   uint32_t sum = 0;
-  for (int k = 0; k < kScanItems; ++k) {
-    v[k] = (i0 + k < n) ? counts[i0 + k] : 0;
-    sum += v[k];
+  if (whole) {
+#pragma unroll
+    for (int k = 0; k < kScanItems; k += 4) {
+      const uint4 x = *reinterpret_cast<const uint4*>(counts + i0 + k);
+      v[k] = x.x;
+      v[k + 1] = x.y;
+      v[k + 2] = x.z;
+      v[k + 3] = x.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) v[k] = (i0 + k < n) ? counts[i0 + k] : 0;
   }
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) sum += v[k];
   uint32_t excl;
   block_exclusive_scan(sum, excl);
   uint32_t run = partials[blockIdx.x] + excl;
-  for (int k = 0; k < kScanItems; ++k) {
-    if (i0 + k < n) {
-      offsets[i0 + k] = run;
-      counts[i0 + k] = 0;
+  if (whole) {
+#pragma unroll
+    for (int k = 0; k < kScanItems; k += 4) {
+      uint4 o;
+      o.x = run;
+      run += v[k];
+      o.y = run;
+      run += v[k + 1];
+      o.z = run;
+      run += v[k + 2];
+      o.w = run;
+      run += v[k + 3];
+      *reinterpret_cast<uint4*>(offsets + i0 + k) = o;
+      *reinterpret_cast<uint4*>(counts + i0 + k) = make_uint4(0u, 0u, 0u, 0u);
     }
-    run += v[k];
+  } else {
+    for (int k = 0; k < kScanItems; ++k) {
+      if (i0 + k < n) {
+        offsets[i0 + k] = run;
+        counts[i0 + k] = 0;
+      }
+      run += v[k];
+    }
   }
 }
 
 // Work-unit prefix over deferred expansion items (one block).
 __global__ void heavy_prefix_kernel(const uint64_t* items, const uint32_t* count, uint32_t cap, int words,
-                                    uint64_t exp_cap, uint64_t* prefix) {
+                                    uint64_t exp_cap, uint64_t* prefix, int32_t* status) {
   const uint32_t n = min(*count, cap);
+  if (threadIdx.x == 0 && *count > cap) atomicOr(status, kInfoHeavyFull);
   uint64_t carry = 0;
   for (uint32_t base = 0; base < n || base == 0; base += kThreads) {
     uint32_t i = base + threadIdx.x;
@@ -1286,6 +1333,119 @@ __global__ void heavy_prefix_kernel(const uint64_t* items, const uint32_t* count
     if (base + kThreads >= n) break;
   }
   if (threadIdx.x == 0) prefix[n] = carry;
+}
+
+// Exclusive block scan of one 64-bit value per thread; returns the total.
+__device__ uint64_t block_exclusive_scan64(uint64_t x, uint64_t& excl) {
+  __shared__ uint64_t s_w[kThreads / 32 + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint64_t incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_w[warp] = incl;
+  __syncthreads();
+  if (tid == 0) {
+    uint64_t run = 0;
+    for (int w = 0; w < kThreads / 32; ++w) {
+      const uint64_t v = s_w[w];
+      s_w[w] = run;
+      run += v;
+    }
+    s_w[kThreads / 32] = run;
+  }
+  __syncthreads();
+  excl = s_w[warp] + incl - x;
+  const uint64_t total = s_w[kThreads / 32];
+  __syncthreads();
+  return total;
+}
+
+// Grouped deferred expansion, step 1 (all CTAs): per claimed group, its item
+// count and its work units (a group of `len` range rows and `cnt` items is
+// ceil(len / kGroupRows) x ceil(cnt / kGroupItems) units), written in place of
+// the two prefixes that step 2 computes.
+__global__ void heavy_group_units_kernel(DevHeavy H, int32_t* status) {
+  const uint32_t n = min(*H.ngroups, H.gcap);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && *H.count > H.cap) atomicOr(status, kInfoHeavyFull);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
+    const uint32_t g = H.glist[j];
+    const uint64_t len = H.gkey[g] >> 32;
+    const uint32_t cnt = H.gcnt[g];
+    H.gstart[j] = cnt;
+    H.unit_prefix[j] = ((len + kGroupRows - 1) / kGroupRows) * (uint64_t)((cnt + kGroupItems - 1) / kGroupItems);
+  }
+}
+
+// Grouped deferred expansion, step 2 (one block, 8 consecutive groups a
+// thread per round): exclusive prefixes of the items (each group's first
+// position in `sorted`, also its scatter cursor) and of the work units.
+// Totals of 2^32 units or more are refused (the unit counter is 32-bit): the
+// pipeline then reports kErrBadOp instead of running them.
+__global__ void heavy_group_prefix_kernel(DevHeavy H, int32_t* status) {
+  constexpr int kPer = 8;
+  const uint32_t n = min(*H.ngroups, H.gcap);
+  uint64_t ucarry = 0;
+  uint32_t icarry = 0;
+  for (uint32_t base = 0; base < n; base += kThreads * kPer) {
+    const uint32_t j0 = base + threadIdx.x * kPer;
+    uint32_t cnt[kPer];
+    uint64_t units[kPer];
+    uint32_t csum = 0;
+    uint64_t usum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const bool in = j0 + k < n;
+      cnt[k] = in ? H.gstart[j0 + k] : 0u;
+      units[k] = in ? H.unit_prefix[j0 + k] : 0ull;
+      csum += cnt[k];
+      usum += units[k];
+    }
+    uint32_t iexcl;
+    const uint32_t itot = block_exclusive_scan(csum, iexcl);
+    uint64_t uexcl;
+    const uint64_t utot = block_exclusive_scan64(usum, uexcl);
+    uint32_t irun = icarry + iexcl;
+    uint64_t urun = ucarry + uexcl;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      if (j0 + k < n) {
+        H.gstart[j0 + k] = irun;
+        H.gcnt[H.glist[j0 + k]] = irun;
+        H.unit_prefix[j0 + k] = urun;
+      }
+      irun += cnt[k];
+      urun += units[k];
+    }
+    icarry += itot;
+    ucarry += utot;
+  }
+  if (threadIdx.x == 0) {
+    H.gstart[n] = icarry;
+    if (ucarry >= (1ull << 32)) {
+      atomicOr(status, kErrBadOp);
+      ucarry = 0;
+    }
+    H.unit_prefix[n] = ucarry;
+  }
+}
+
+// Grouped deferred expansion, step 2: every item's stashed values move to its
+// group's next position in `sorted` (items whose group claim failed were not
+// deferred and carry kEmpty as their group).
+__global__ void heavy_group_scatter_kernel(DevHeavy H) {
+  const uint32_t n = min(*H.count, H.cap);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t* it = H.items + (size_t)i * H.words;
+    const uint64_t g = it[0];
+    if (g == kEmpty) continue;
+    const uint32_t pos = atomicAdd(H.gcnt + g, 1u);
+    for (int s = 0; s < H.nstash; ++s) H.sorted[(size_t)pos * H.nstash + s] = it[2 + s];
+  }
 }
 
 // ------------------------------------------------------- batch helpers --
@@ -1474,8 +1634,15 @@ cudaError_t launch_batch_pack(const BatchPack* ops, int nops, uint8_t* dst, int 
   return cudaGetLastError();
 }
 
-cudaError_t launch_heavy_prefix(const DevHeavy& H, uint64_t exp_cap, cudaStream_t stream) {
-  heavy_prefix_kernel<<<1, kThreads, 0, stream>>>(H.items, H.count, H.cap, H.words, exp_cap, H.unit_prefix);
+cudaError_t launch_heavy_prefix(const DevHeavy& H, uint64_t exp_cap, int32_t* status, cudaStream_t stream) {
+  heavy_prefix_kernel<<<1, kThreads, 0, stream>>>(H.items, H.count, H.cap, H.words, exp_cap, H.unit_prefix, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_heavy_group(const DevHeavy& H, int32_t* status, int sms, cudaStream_t stream) {
+  heavy_group_units_kernel<<<sms, 256, 0, stream>>>(H, status);
+  heavy_group_prefix_kernel<<<1, kThreads, 0, stream>>>(H, status);
+  heavy_group_scatter_kernel<<<sms * 2, 256, 0, stream>>>(H);
   return cudaGetLastError();
 }
 

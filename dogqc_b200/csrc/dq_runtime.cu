@@ -39,7 +39,8 @@ cudaError_t launch_agg_init(uint64_t* slots, uint64_t nslots, int words, int val
 size_t mm_scan_scratch_words(uint64_t n);
 cudaError_t launch_mm_scan(uint32_t* counts, uint32_t* offsets, uint64_t n, uint32_t* partials,
                            cudaStream_t stream, int* launches);
-cudaError_t launch_heavy_prefix(const DevHeavy& H, uint64_t exp_cap, cudaStream_t stream);
+cudaError_t launch_heavy_prefix(const DevHeavy& H, uint64_t exp_cap, int32_t* status, cudaStream_t stream);
+cudaError_t launch_heavy_group(const DevHeavy& H, int32_t* status, int sms, cudaStream_t stream);
 size_t batch_scan_blocks(uint64_t n);
 cudaError_t launch_batch_reset(const BatchReset* ops, int nops, int sms, cudaStream_t stream);
 cudaError_t launch_batch_scan(const BatchScanSeg* segs, int nseg, uint64_t total_blocks, uint32_t* partials,
@@ -175,7 +176,9 @@ struct PipeRec {
   jit::Program prog;        // generated source and launch shape
   jit::Kernels kernels;
   int expand_op = -1;       // level-0 expansion op with deferral
+  uint64_t heavy_cap = 0;   // deferred-item capacity grown after an overflow (0: default)
   DevBuf pattern_buf, heavy_items, heavy_count, heavy_prefix;
+  DevBuf heavy_gkey, heavy_gcnt, heavy_glist, heavy_gstart, heavy_sorted;  // grouped deferral
   bool mm_count = false;    // sink is a multimap count: bucket scan follows
   int mm_res = -1;
   int staged_cols = 0;
@@ -642,12 +645,37 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     H.nstash = (int)stash.size();
     H.words = 2 + H.nstash;
     int64_t rows = P.nrows_dev ? 1 << 20 : P.nrows;
-    H.cap = (uint32_t)std::min<int64_t>(std::max<int64_t>(rows, 1), 1 << 20);
+    H.cap = (uint32_t)std::min<int64_t>(std::max<int64_t>(rows, 1),
+                                        std::max<int64_t>(1 << 20, (int64_t)p.heavy_cap));
     H.op = i;
-    H.threshold = ctx->cfg.defer_threshold > 0 ? (uint64_t)ctx->cfg.defer_threshold : (uint64_t)tile * 8;
+    // generated kernels group the deferred items by range, so shorter ranges
+    // pay off there: a range is gathered once per 32-row chunk for all probe
+    // rows that matched it
+    H.grouped = !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) ? 1 : 0;
+    const uint64_t dflt = H.grouped ? (uint64_t)kGroupThreshold : (uint64_t)tile * 8;
+    H.threshold = ctx->cfg.defer_threshold > 0 ? (uint64_t)ctx->cfg.defer_threshold : dflt;
     p.heavy_items.alloc((size_t)H.cap * H.words * 8);
-    p.heavy_count.alloc(8);
-    p.heavy_prefix.alloc(((size_t)H.cap + 1) * 8);
+    p.heavy_count.alloc(8);  // item count, group count
+    size_t nprefix = (size_t)H.cap + 1;
+    if (H.grouped) {
+      // distinct ranges longer than the threshold: at most rows / (threshold + 1)
+      const uint64_t rows_bound = std::max<uint64_t>(plan->res[op.res]->pay_rows, 1);
+      const uint64_t groups = std::min<uint64_t>(H.cap, rows_bound / (H.threshold + 1) + 1);
+      H.gcap = (uint32_t)std::max<uint64_t>(64, 2 * groups);
+      p.heavy_gkey.alloc((size_t)H.gcap * 8);
+      p.heavy_gcnt.alloc((size_t)H.gcap * 4);
+      p.heavy_glist.alloc((size_t)H.gcap * 4);
+      p.heavy_gstart.alloc(((size_t)H.gcap + 1) * 4);
+      p.heavy_sorted.alloc((size_t)H.cap * std::max(H.nstash, 1) * 8);
+      H.gkey = p.heavy_gkey.as<uint64_t>();
+      H.gcnt = p.heavy_gcnt.as<uint32_t>();
+      H.glist = p.heavy_glist.as<uint32_t>();
+      H.ngroups = p.heavy_count.as<uint32_t>() + 1;
+      H.gstart = p.heavy_gstart.as<uint32_t>();
+      H.sorted = p.heavy_sorted.as<uint64_t>();
+      nprefix = std::max<size_t>(nprefix, (size_t)H.gcap + 1);
+    }
+    p.heavy_prefix.alloc(nprefix * 8);
     H.items = p.heavy_items.as<uint64_t>();
     H.count = p.heavy_count.as<uint32_t>();
     H.unit_prefix = p.heavy_prefix.as<uint64_t>();
@@ -788,12 +816,23 @@ int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status) {
     PipeRec& p = *plan->pipes[i];
     p.dev.tile_counter = counters + 2 * i;
     DQ_CUDA(cudaEventRecord(plan->events[1 + 2 * i], st));
-    if (p.expand_op >= 0) DQ_CUDA(cudaMemsetAsync(p.heavy_count.ptr, 0, 8, st));
+    if (p.expand_op >= 0) {
+      DQ_CUDA(cudaMemsetAsync(p.heavy_count.ptr, 0, 8, st));
+      if (p.dev.heavy.grouped) {
+        DQ_CUDA(cudaMemsetAsync(p.heavy_gkey.ptr, 0xff, p.heavy_gkey.bytes, st));
+        DQ_CUDA(cudaMemsetAsync(p.heavy_gcnt.ptr, 0, p.heavy_gcnt.bytes, st));
+      }
+    }
     if (p.jit) DQ_CUDA(launch_generated(p.kernels.main, p.dev, p.grid, p.prog.block, p.prog.smem_bytes, st));
     else DQ_CUDA(p.row ? launch_row(p.dev, p.grid, st) : launch_pipeline(p.dev, p.grid, st));
     ++launches;
     if (p.expand_op >= 0) {
-      DQ_CUDA(launch_heavy_prefix(p.dev.heavy, (uint64_t)p.dev.exp_cap, st));
+      if (p.dev.heavy.grouped) {
+        DQ_CUDA(launch_heavy_group(p.dev.heavy, p.dev.status, plan->ctx->sms, st));
+        launches += 2;  // units, prefix and scatter, in place of the item prefix
+      } else {
+        DQ_CUDA(launch_heavy_prefix(p.dev.heavy, (uint64_t)p.dev.exp_cap, p.dev.status, st));
+      }
       DevPipe H = p.dev;
       H.mode = 1;
       H.tile_counter = counters + 2 * i + 1;
@@ -868,8 +907,11 @@ uint64_t plan_bytes(const dq_plan* plan) {
     b += r.slots.bytes + r.counts.bytes + r.offsets.bytes + r.cursor.bytes + r.scan_scratch.bytes;
     for (auto& p : r.pay) b += p->bytes;
   }
-  for (auto& pp : plan->pipes)
+  for (auto& pp : plan->pipes) {
     b += pp->pattern_buf.bytes + pp->heavy_items.bytes + pp->heavy_count.bytes + pp->heavy_prefix.bytes;
+    b += pp->heavy_gkey.bytes + pp->heavy_gcnt.bytes + pp->heavy_glist.bytes + pp->heavy_gstart.bytes +
+         pp->heavy_sorted.bytes;
+  }
   return b;
 }
 
@@ -962,6 +1004,26 @@ void grow_plan(dq_plan* plan, int status) {
     }
   }
   refresh_pipelines(plan);
+}
+
+// After a run whose deferred expansion items overflowed (kInfoHeavyFull; its
+// results are exact, the overflowing rows were expanded in place, which is
+// slow for long ranges): twice the items the run wanted, for the runs that
+// follow.  Returns whether the plan's buffers moved.
+bool grow_heavy(dq_plan* plan) {
+  bool moved = false;
+  for (auto& pp : plan->pipes) {
+    PipeRec& p = *pp;
+    if (p.expand_op < 0) continue;
+    uint32_t n = 0;
+    DQ_CUDA(cudaMemcpy(&n, p.heavy_count.ptr, 4, cudaMemcpyDeviceToHost));
+    if (n > p.dev.heavy.cap) {
+      p.heavy_cap = std::min<uint64_t>(2ull * n, 0xffffffffull);
+      moved = true;
+    }
+  }
+  if (moved) refresh_pipelines(plan);
+  return moved;
 }
 
 void throw_status(int status) {
@@ -1290,6 +1352,10 @@ int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out) {
     int status = 0;
     for (int attempt = 0;; ++attempt) {
       status = run_once(plan, st);
+      if (status & kInfoMask) {
+        if (status & kInfoHeavyFull) grow_heavy(plan);
+        status &= ~kInfoMask;
+      }
       if (status == 0) break;
       if (attempt >= 8 || (status & (kErrTimeout | kErrBadOp)))
         throw DqError(status & kErrTimeout ? DQ_ERR_TIMEOUT
@@ -1806,7 +1872,12 @@ void srv_dispatch(dq_server* s, SrvSlot& slot, SrvReq* r, PoolEntry* pe) {
 void srv_complete(dq_server* s, SrvSlot& slot) {
   SrvReq* r = slot.req;
   PoolEntry* pe = slot.pe;
-  const int32_t status = *pe->host_status;
+  int32_t status = *pe->host_status;
+  bool regrow_heavy = false;
+  if (status & kInfoMask) {
+    regrow_heavy = (status & kInfoHeavyFull) != 0;
+    status &= ~kInfoMask;
+  }
   if (status != 0 && !(status & (kErrTimeout | kErrBadOp)) && r->attempts < 8) {
     ++r->attempts;
     const uint64_t before = pe->bytes;
@@ -1841,6 +1912,17 @@ void srv_complete(dq_server* s, SrvSlot& slot) {
   } else {
     collect_timing(pe->plan.get(), slot.launches);
     res = read_result(pe->plan.get(), slot.st);
+  }
+  if (regrow_heavy) {
+    // the result stands; later runs get the larger item capacity
+    const uint64_t before = pe->bytes;
+    if (grow_heavy(pe->plan.get())) {
+      pe->bytes = plan_bytes(pe->plan.get());
+      s->mem = s->mem - before + pe->bytes;
+      pe->drop_graph();
+      pe->no_graph = false;
+      srv_build_graph(pe, slot.st);
+    }
   }
   srv_release(s, r, pe);
   srv_finish(s, r, DQ_OK, "", res);
