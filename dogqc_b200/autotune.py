@@ -12,7 +12,8 @@ Knobs (the dq_tuning fields):
   rows_per_thread    consecutive rows one thread loads and processes per step
   block_threads      threads per CTA of the generated kernels
   refill             -1 turns the plan's lane refill off
-  unique_slots_pct   join-table slots as % of the plan's estimate (load factor)
+  unique_slots_pct   join-table slots as % of the plan's estimate (load factor;
+                     0 is the backend's size-dependent default)
   multi_buckets_pct  multimap buckets as % of the plan's estimate
 """
 import hashlib
@@ -23,8 +24,8 @@ KNOBS = [
     ("rows_per_thread", [1, 2, 4]),
     ("block_threads", [128, 256, 512]),
     ("refill", [0, -1]),
-    ("unique_slots_pct", [200, 400, 100]),
-    ("multi_buckets_pct", [100, 200, 50]),
+    ("unique_slots_pct", [0, 200, 400, 800]),
+    ("multi_buckets_pct", [100, 50, 25, 200]),
 ]
 
 _cache = {}

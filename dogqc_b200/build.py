@@ -85,7 +85,7 @@ def build(force=False, verbose=False):
             sys.stderr.write(r.stderr)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [_nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs, "-lnvrtc"]
+    cmd = [_nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs, "-lnvrtc", "-ldl"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n%s" % r.stderr[-4000:])

@@ -26,6 +26,7 @@
 // dq_common.cuh, embedded with the other device headers as in-memory headers.
 #include "dq_jit.h"
 
+#include <dlfcn.h>
 #include <nvrtc.h>
 
 #include <algorithm>
@@ -1625,8 +1626,65 @@ const char* kStdint =
     "typedef unsigned long long uint64_t;\n";
 const char* kStddef = "#pragma once\ntypedef unsigned long size_t; typedef long ptrdiff_t;\n";
 
+// The NVRTC that compiles generated kernels.  An application may have loaded
+// an older NVRTC into the process before this library (PyTorch loads its own);
+// the CUDA toolkit's library, when newer, is opened privately beside it (local
+// symbols, its own bindings first), since 256-bit loads for sm_100a need 12.9.
+struct NvrtcApi {
+  nvrtcResult (*version)(int*, int*);
+  nvrtcResult (*create)(nvrtcProgram*, const char*, const char*, int, const char* const*, const char* const*);
+  nvrtcResult (*compile)(nvrtcProgram, int, const char* const*);
+  nvrtcResult (*log_size)(nvrtcProgram, size_t*);
+  nvrtcResult (*log)(nvrtcProgram, char*);
+  nvrtcResult (*cubin_size)(nvrtcProgram, size_t*);
+  nvrtcResult (*cubin)(nvrtcProgram, char*);
+  nvrtcResult (*destroy)(nvrtcProgram*);
+  const char* (*error)(nvrtcResult);
+};
+
+bool open_nvrtc(const std::string& path, NvrtcApi& a) {
+  void* h = dlopen(path.c_str(), RTLD_NOW | RTLD_LOCAL | RTLD_DEEPBIND);
+  if (!h) return false;
+  auto sym = [&](const char* n) { return dlsym(h, n); };
+  a.version = reinterpret_cast<decltype(a.version)>(sym("nvrtcVersion"));
+  a.create = reinterpret_cast<decltype(a.create)>(sym("nvrtcCreateProgram"));
+  a.compile = reinterpret_cast<decltype(a.compile)>(sym("nvrtcCompileProgram"));
+  a.log_size = reinterpret_cast<decltype(a.log_size)>(sym("nvrtcGetProgramLogSize"));
+  a.log = reinterpret_cast<decltype(a.log)>(sym("nvrtcGetProgramLog"));
+  a.cubin_size = reinterpret_cast<decltype(a.cubin_size)>(sym("nvrtcGetCUBINSize"));
+  a.cubin = reinterpret_cast<decltype(a.cubin)>(sym("nvrtcGetCUBIN"));
+  a.destroy = reinterpret_cast<decltype(a.destroy)>(sym("nvrtcDestroyProgram"));
+  a.error = reinterpret_cast<decltype(a.error)>(sym("nvrtcGetErrorString"));
+  if (a.version && a.create && a.compile && a.log_size && a.log && a.cubin_size && a.cubin && a.destroy && a.error)
+    return true;
+  dlclose(h);
+  return false;
+}
+
+const NvrtcApi& nvrtc() {
+  static const NvrtcApi api = [] {
+    NvrtcApi linked = {&nvrtcVersion, &nvrtcCreateProgram, &nvrtcCompileProgram, &nvrtcGetProgramLogSize,
+                       &nvrtcGetProgramLog, &nvrtcGetCUBINSize, &nvrtcGetCUBIN, &nvrtcDestroyProgram,
+                       &nvrtcGetErrorString};
+    int maj = 0, min = 0;
+    linked.version(&maj, &min);
+    std::vector<std::string> roots;
+    for (const char* e : {"DQ_CUDA_HOME", "CUDA_HOME", "CUDA_PATH"})
+      if (const char* v = getenv(e)) roots.push_back(v);
+    roots.push_back("/usr/local/cuda");
+    for (const std::string& r : roots) {
+      NvrtcApi a;
+      if (!open_nvrtc(r + "/lib64/libnvrtc.so.12", a) && !open_nvrtc(r + "/lib64/libnvrtc.so", a)) continue;
+      int M = 0, m = 0;
+      if (a.version(&M, &m) == NVRTC_SUCCESS && (M > maj || (M == maj && m > min))) return a;
+    }
+    return linked;
+  }();
+  return api;
+}
+
 void nvrtc_check(nvrtcResult r, const char* what) {
-  if (r != NVRTC_SUCCESS) throw Error(std::string(what) + ": " + nvrtcGetErrorString(r));
+  if (r != NVRTC_SUCCESS) throw Error(std::string(what) + ": " + nvrtc().error(r));
 }
 
 // One NVRTC compilation of `src`; false (log kept) when it does not compile.
@@ -1641,25 +1699,25 @@ bool compile_once(const std::string& src, bool ld256, std::string& log, std::vec
   hdrs.push_back(kStddef);
   names.push_back("stddef.h");
   nvrtcProgram prog;
-  nvrtc_check(nvrtcCreateProgram(&prog, src.c_str(), "dq_pipeline.cu", (int)hdrs.size(), hdrs.data(), names.data()),
+  nvrtc_check(nvrtc().create(&prog, src.c_str(), "dq_pipeline.cu", (int)hdrs.size(), hdrs.data(), names.data()),
               "nvrtcCreateProgram");
   const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "-lineinfo",
                         "--ptxas-options=-v", ld256 ? "-DDQ_LD256=1" : "-DDQ_LD256=0"};
-  nvrtcResult r = nvrtcCompileProgram(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
+  nvrtcResult r = nvrtc().compile(prog, (int)(sizeof(opts) / sizeof(opts[0])), opts);
   size_t n = 0;
-  nvrtcGetProgramLogSize(prog, &n);
+  nvrtc().log_size(prog, &n);
   log.assign(n, '\0');
-  if (n) nvrtcGetProgramLog(prog, &log[0]);
+  if (n) nvrtc().log(prog, &log[0]);
   while (!log.empty() && log.back() == '\0') log.pop_back();
   if (r != NVRTC_SUCCESS) {
-    nvrtcDestroyProgram(&prog);
+    nvrtc().destroy(&prog);
     return false;
   }
   size_t cb = 0;
-  nvrtc_check(nvrtcGetCUBINSize(prog, &cb), "nvrtcGetCUBINSize");
+  nvrtc_check(nvrtc().cubin_size(prog, &cb), "nvrtcGetCUBINSize");
   cubin.resize(cb);
-  nvrtc_check(nvrtcGetCUBIN(prog, cubin.data()), "nvrtcGetCUBIN");
-  nvrtcDestroyProgram(&prog);
+  nvrtc_check(nvrtc().cubin(prog, cubin.data()), "nvrtcGetCUBIN");
+  nvrtc().destroy(&prog);
   return true;
 }
 
@@ -1667,7 +1725,7 @@ void build(Entry& e, const std::string& src) {
   // the NVRTC the process resolved (an application may have loaded an older
   // one first): 256-bit loads for sm_100a need 12.9
   int major = 0, minor = 0;
-  nvrtcVersion(&major, &minor);
+  nvrtc().version(&major, &minor);
   const bool ld256 = major > 12 || (major == 12 && minor >= 9);
   const bool ok = compile_once(src, ld256, e.log, e.cubin);
   e.log = "NVRTC " + std::to_string(major) + "." + std::to_string(minor) + "\n" + e.log;

@@ -162,7 +162,10 @@ struct ResRec {
   DevBuf slots, counts, offsets, cursor, scan_scratch;
   std::vector<std::unique_ptr<DevBuf>> pay;
   uint64_t pay_rows = 0;
+  int pct = 100;            // UNIQUE: slots as a percentage of the plan's capacity
 };
+
+constexpr uint64_t kL2TableBytes = 48ull << 20;  // join tables up to this size get extra slack
 
 struct PipeRec {
   dq_pipeline desc{};
@@ -194,7 +197,7 @@ struct dq_result {
 // batch, with the join-table sizing an autotuner may change.
 struct PlanOpts {
   bool batch_member = false;  // no standalone kernels, no deferred expansion
-  int unique_pct = 200;       // join-table slots, % of the plan's capacity
+  int unique_pct = 0;         // join-table slots, % of the plan's capacity (0: by size)
   int multi_pct = 100;        // multimap buckets, % of the plan's capacity
   jit::Tuning tuning;
 };
@@ -334,11 +337,18 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       R.key_word = 1;
       R.val_word = 1 + (R.packed ? 0 : d.nkeys);
       R.words = R.val_word + (d.kind == DQ_RES_UNIQUE ? d.npay : d.naggs);
-      // join tables get twice the slots the plan asks for (a load factor of at
-      // most 1/4 with the reference's default size factor 2): most probes of a
-      // selective join miss, and a miss walks to the next empty slot.  A slot
-      // count divisible by 4 lets probes read aligned 32-byte slot groups.
-      if (d.kind == DQ_RES_UNIQUE) cap = (cap * (uint64_t)std::max(plan->opts.unique_pct, 25) / 100 + 3) & ~3ull;
+      // join tables get more slots than the plan asks for: most probes of a
+      // selective join miss, a miss walks to the next empty slot, and a walk
+      // past the first 32-byte slot group is a second dependent load.  Four
+      // times (a load factor of at most 1/8 with the reference's default size
+      // factor 2) while the table stays small enough to live in L2 beside the
+      // probe's input stream, else twice.  A slot count divisible by 4 lets
+      // probes read aligned 32-byte slot groups.
+      if (d.kind == DQ_RES_UNIQUE) {
+        r.pct = plan->opts.unique_pct > 0 ? std::max(plan->opts.unique_pct, 25)
+                : cap * 4 * (uint64_t)R.words * 8 <= kL2TableBytes ? 400 : 200;
+        cap = (cap * (uint64_t)r.pct / 100 + 3) & ~3ull;
+      }
       cap = std::max<uint64_t>(cap, 16);
       if (cap >= 0xffffffffull) throw DqError(DQ_ERR_UNSUPPORTED, "hash tables hold fewer than 2^32 slots");
       R.cap = cap;
@@ -990,7 +1000,7 @@ void grow_plan(dq_plan* plan, int status) {
     ResRec& r = *rp;
     if ((status & kErrHtFull) && (r.desc.kind == DQ_RES_UNIQUE || r.desc.kind == DQ_RES_AGG)) {
       // four times the slots (join tables are sized at unique_pct of the capacity)
-      const int64_t pct = r.desc.kind == DQ_RES_UNIQUE ? std::max(plan->opts.unique_pct, 25) : 100;
+      const int64_t pct = r.desc.kind == DQ_RES_UNIQUE ? r.pct : 100;
       r.desc.capacity = (int64_t)r.dev.cap * 4 * 100 / pct;
       setup_resource(plan, r, 1);
     }

@@ -587,15 +587,29 @@ class Lowering(object):
         if "str" in gtypes:
             raise Unsupported("grouping by strings")
         aggs = [(id, inId, _tname(red)) for id, (inId, red) in node.aggregateTuples.items()]
-        if len(aggs) > L.MAX_AGGS:
+        # one accumulator per distinct (reduction, input): an AVG shares the SUM
+        # of its input with a SUM aggregate of the same attribute and divides by
+        # the COUNT (one is added when the query has none)
+        accs, acc_of = [], {}
+        for id, inId, red in aggs:
+            key = ("COUNT", None) if red == "COUNT" else (self.RED[red], inId)
+            if key not in acc_of:
+                acc_of[key] = len(accs)
+                accs.append(key)
+            acc_of[id] = acc_of[key]
+        if any(r == "AVG" for _, _, r in aggs) and ("COUNT", None) not in acc_of:
+            acc_of[("COUNT", None)] = len(accs)
+            accs.append(("COUNT", None))
+        if len(accs) > L.MAX_AGGS:
             raise Unsupported("more than %d aggregates" % L.MAX_AGGS)
         numgroups = max(int(getattr(node, "numgroups", 1)), 1)
         cap = max(2 * numgroups, 1024) if groups else 1
+        reds = [L.RED_COUNT if k[0] == "COUNT" else k[0] for k in accs]
         rid = self.new_res(Res(L.RES_AGG, nkeys=len(groups), key_ctype=gtypes,
-                               agg_red=[self.RED[r] for _, _, r in aggs], capacity=cap, group_hint=numgroups))
+                               agg_red=reds, capacity=cap, group_hint=numgroups))
         kl, kn = pipe.list_([pipe.attr_slot(g) for g in groups])
         inputs = []
-        for id, inId, red in aggs:
+        for red, inId in accs:
             if red == "COUNT":
                 inputs.append(-1)
             else:
@@ -610,17 +624,16 @@ class Lowering(object):
         out = Pipe(L.SRC_AGG, source_res=rid)
         for j, g in enumerate(groups):
             out.att[g.id] = out.slot(L.SLOT_AGGKEY, 0, gtypes[j], src=j, res=rid)
-        count_slot = None
-        for j, (id, inId, red) in enumerate(aggs):
-            t = "i32" if red == "COUNT" else "u64"
-            out.att[id] = out.slot(L.SLOT_AGGVAL, 0, t, src=j, res=rid)
-            if red == "COUNT":
-                count_slot = out.att[id]
-        for id, (inId, red) in node.aggregateTuples.items():
-            if _tname(red) == "AVG":
+        acc_slot = [out.slot(L.SLOT_AGGVAL, 0, "i32" if red == "COUNT" else "u64", src=j, res=rid)
+                    for j, (red, _) in enumerate(accs)]
+        count_slot = acc_slot[acc_of[("COUNT", None)]] if ("COUNT", None) in acc_of else None
+        for id, inId, red in aggs:
+            if red == "AVG":
                 d = out.reg("u64")
-                out.op(L.OP_ARITH, sub=L.DIV, dst=d, a=out.att[id], b=count_slot, ctype=L.U64)
+                out.op(L.OP_ARITH, sub=L.DIV, dst=d, a=acc_slot[acc_of[id]], b=count_slot, ctype=L.U64)
                 out.att[id] = d
+            else:
+                out.att[id] = acc_slot[acc_of[id]]
         self.consume_parent(node, out)
 
     # -- materialisation ---------------------------------------------------------

@@ -284,7 +284,8 @@ typedef struct {
     int32_t block_threads;           /* 128, 256 or 512 (batched kernels)       */
     int32_t refill;                  /* -1: no lane refill; 0: the plan's own   */
     int32_t unique_slots_pct;        /* join-table slots, % of the plan's       */
-                                     /* capacity (default 200)                  */
+                                     /* capacity (default 400 for tables of     */
+                                     /* up to 48 MB there, else 200)            */
     int32_t multi_buckets_pct;       /* multimap buckets, % (default 100)       */
     int32_t reserved[3];
 } dq_tuning;
