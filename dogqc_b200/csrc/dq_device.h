@@ -82,7 +82,10 @@ struct DevHeavy {         // deferred wide expansion ranges
   // of the group's items
   int32_t grouped;
   uint32_t gcap;          // group table slots
-  uint64_t* gkey;         // (range length << 32) | range offset; kEmpty: free
+  uint64_t* gkey;         // (instance << 32) | range offset; kEmpty: free.  A
+                          // range's offset identifies it within its instance
+                          // (plain plans: instance 0; batches: shared buffers)
+  uint32_t* glen;         // range length of a claimed group slot
   uint32_t* gcnt;         // items per group slot, then its scatter cursor
   uint32_t* glist;        // claimed group slots, in claim order
   uint32_t* ngroups;

@@ -177,6 +177,7 @@ struct Gen {
   int hot = 0;                   // multimap sink through the CTA's hot-bucket table:
                                  // 1 count (flushed at the end), 2 scatter (per step)
   int hot_off = 0;               // shared-memory offset of that table
+  std::string inst_expr = "0u";  // the instance a deferred item belongs to (batches)
   std::string ldfn = "__ldcs";   // load function of streamed source columns
   int block = kBlock;            // threads per CTA
   bool batched = false;          // kernel over many instances of the plan
@@ -650,7 +651,7 @@ struct Gen {
       if (P.heavy.grouped) {
         // the item joins the group of its range (claimed on first sight); an
         // item whose claim fails is expanded here and carries kEmpty
-        L("const uint64_t gk_ = ((uint64_t)" + ec + " << 32) | " + eo + ";");
+        L("const uint64_t gk_ = ((uint64_t)" + inst_expr + " << 32) | " + eo + ";");
         L("uint32_t g_ = slot_of(gk_, P.heavy.gcap);");
         L("uint64_t gid_ = kEmpty;");
         L("for (uint32_t n_ = 0; n_ < P.heavy.gcap; ++n_) {");
@@ -658,7 +659,12 @@ struct Gen {
         L("  if (t_ == gk_) { gid_ = g_; break; }");
         L("  if (t_ == kEmpty) {");
         L("    const uint64_t o_ = atomicCAS((unsigned long long*)(P.heavy.gkey + g_), kEmpty, gk_);");
-        L("    if (o_ == kEmpty) { P.heavy.glist[atomicAdd(P.heavy.ngroups, 1u)] = g_; gid_ = g_; break; }");
+        L("    if (o_ == kEmpty) {");
+        L("      P.heavy.glen[g_] = " + ec + ";");
+        L("      P.heavy.glist[atomicAdd(P.heavy.ngroups, 1u)] = g_;");
+        L("      gid_ = g_;");
+        L("      break;");
+        L("    }");
         L("    if (o_ == gk_) { gid_ = g_; break; }");
         L("  }");
         L("  g_ = (g_ + 1u == P.heavy.gcap) ? 0u : g_ + 1u;");
@@ -1391,6 +1397,7 @@ struct Gen {
     L("const DevPipe& P = Ps[lo];");
     L("const int64_t nrows = source_rows(P);");
     L("const int64_t base = (blk - bprefix[lo]) * span;");
+    inst_expr = "(uint32_t)lo";
     agg_init();
     std::vector<int> cols = source_cols();
     for (int c : cols) L("uint64_t c" + num(c) + "[" + num(U) + "];");
@@ -1425,10 +1432,27 @@ struct Gen {
   void heavy_grouped_kernel() {
     std::fill(var.begin(), var.end(), std::string());
     pending.clear();
-    prologue("dq_heavy");
-    L("const uint32_t ng = *P.heavy.ngroups < P.heavy.gcap ? *P.heavy.ngroups : P.heavy.gcap;");
-    L("const uint64_t units = P.heavy.unit_prefix[ng];");
-    L("const int ns = P.heavy.nstash;");
+    if (batched) {
+      // the instances share the deferral buffers; a unit binds its instance
+      L(std::string("extern \"C\" __global__ void __launch_bounds__(") + num(block) +
+        ") dq_batch_heavy(const DevPipe* __restrict__ Ps, int ninst) {");
+      ++ind;
+      L("extern __shared__ __align__(16) uint8_t smem[];");
+      L("if (*(volatile int32_t*)Ps[0].status & (kErrHtFull | kErrTimeout)) return;");
+      L("const int tid = threadIdx.x, lane = tid & 31;");
+      L("(void)smem;");
+      L("(void)tid;");
+      L("(void)ninst;");
+      L("const DevHeavy& H = Ps[0].heavy;");
+      L("uint32_t* const units_taken = Ps[0].tile_counter;");
+    } else {
+      prologue("dq_heavy");
+      L("const DevHeavy& H = P.heavy;");
+      L("uint32_t* const units_taken = P.tile_counter;");
+    }
+    L("const uint32_t ng = *H.ngroups < H.gcap ? *H.ngroups : H.gcap;");
+    L("const uint64_t units = H.unit_prefix[ng];");
+    L("const int ns = H.nstash;");
     L("(void)ns;");
     // the warp's current group and its unit range stay in registers: the
     // units of a long range come to the same warp in runs
@@ -1437,7 +1461,7 @@ struct Gen {
     L("for (;;) {");
     ++ind;
     L("uint32_t unit = 0;");
-    L("if (lane == 0) unit = atomicAdd(P.tile_counter, 1u);");
+    L("if (lane == 0) unit = atomicAdd(units_taken, 1u);");
     L("unit = __shfl_sync(kFull, unit, 0);");
     L("if ((uint64_t)unit >= units) break;");
     L("if ((uint64_t)unit < ulo || (uint64_t)unit >= uhi) {");
@@ -1448,19 +1472,25 @@ struct Gen {
     L("while (b - a > 1u) {");
     L("  const uint32_t st_ = (b - a + 31u) / 32u;");
     L("  const uint32_t ix_ = a + (uint32_t)lane * st_;");
-    L("  const bool le_ = ix_ < b && P.heavy.unit_prefix[ix_] <= (uint64_t)unit;");
+    L("  const bool le_ = ix_ < b && H.unit_prefix[ix_] <= (uint64_t)unit;");
     L("  const unsigned m_ = __ballot_sync(kFull, le_);");
     L("  a = a + (uint32_t)(31 - __clz(m_)) * st_;");
     L("  b = b < a + st_ ? b : a + st_;");
     L("}");
     L("lo = a;");
-    L("ulo = P.heavy.unit_prefix[lo];");
-    L("uhi = P.heavy.unit_prefix[lo + 1];");
+    L("ulo = H.unit_prefix[lo];");
+    L("uhi = H.unit_prefix[lo + 1];");
     --ind;
     L("}");
-    L("const uint64_t gk = P.heavy.gkey[P.heavy.glist[lo]];");
-    L("const uint32_t len = (uint32_t)(gk >> 32);");
-    L("const uint32_t i0 = P.heavy.gstart[lo], ni = P.heavy.gstart[lo + 1] - i0;");
+    L("const uint32_t gs = H.glist[lo];");
+    L("const uint64_t gk = H.gkey[gs];");
+    L("const uint32_t len = H.glen[gs];");
+    L("const uint32_t i0 = H.gstart[lo], ni = H.gstart[lo + 1] - i0;");
+    if (batched) {
+      // aggregates go to the unit's own instance: accumulated per unit
+      L("const DevPipe& P = Ps[(uint32_t)(gk >> 32)];");
+      agg_init();
+    }
     L("const uint32_t local = (uint32_t)((uint64_t)unit - ulo);");
     L("const uint32_t rch = (len + " + num(kGroupRows - 1) + "u) / " + num(kGroupRows) + "u;");
     L("const uint32_t q = (local % rch) * " + num(kGroupRows) + "u + (uint32_t)lane;");
@@ -1476,7 +1506,7 @@ struct Gen {
     for (int s = 0; s < P.nslots; ++s)
       if (slot(s).stash >= 0) {
         const std::string hl = "hl" + num(s);
-        L("const uint64_t " + hl + " = ix + lane < ie ? P.heavy.sorted[(size_t)(i0 + ix + lane) * ns + " +
+        L("const uint64_t " + hl + " = ix + lane < ie ? H.sorted[(size_t)(i0 + ix + lane) * ns + " +
           num(slot(s).stash) + "] : 0ull;");
         carried.emplace_back(s, hl);
       }
@@ -1493,9 +1523,15 @@ struct Gen {
     L("}");
     --ind;
     L("}");
+    if (batched) agg_flush();
     --ind;
     L("}");
-    epilogue();
+    if (batched) {
+      --ind;
+      L("}");
+    } else {
+      epilogue();
+    }
   }
 
   void heavy_kernel() {
@@ -1549,7 +1585,7 @@ struct Gen {
 }  // namespace
 
 Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t) {
-  Gen g(P, t.batched ? -1 : expand_op);
+  Gen g(P, expand_op);
   g.batched = t.batched;
   if (t.block == 128 || t.block == 256 || t.block == 512) g.block = t.block;
   bool has_expand = false;
@@ -1587,6 +1623,11 @@ Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t
   prog.block = g.block;
   if (t.batched) {
     g.batch_kernel();
+    if (expand_op >= 0) {
+      g.o += "\n";
+      g.heavy_kernel();
+      prog.heavy = true;
+    }
     prog.source = g.o;
     prog.smem_bytes = g.smem;
     prog.rows_per_thread = g.U;
@@ -1721,6 +1762,25 @@ bool compile_once(const std::string& src, bool ld256, std::string& log, std::vec
   return true;
 }
 
+// The generated lines around the first line a compiler message names.
+std::string source_excerpt(const std::string& src, const std::string& log) {
+  const std::string tag = "dq_pipeline.cu(";
+  const size_t at = log.find(tag);
+  if (at == std::string::npos) return std::string();
+  const int line = atoi(log.c_str() + at + tag.size());
+  std::string out = "\ngenerated source near line " + std::to_string(line) + ":\n";
+  int n = 1;
+  size_t pos = 0;
+  while (pos < src.size()) {
+    size_t end = src.find('\n', pos);
+    if (end == std::string::npos) end = src.size();
+    if (n >= line - 6 && n <= line + 3) out += std::to_string(n) + ": " + src.substr(pos, end - pos) + "\n";
+    pos = end + 1;
+    ++n;
+  }
+  return out;
+}
+
 void build(Entry& e, const std::string& src) {
   // the NVRTC the process resolved (an application may have loaded an older
   // one first): 256-bit loads for sm_100a need 12.9
@@ -1729,7 +1789,7 @@ void build(Entry& e, const std::string& src) {
   const bool ld256 = major > 12 || (major == 12 && minor >= 9);
   const bool ok = compile_once(src, ld256, e.log, e.cubin);
   e.log = "NVRTC " + std::to_string(major) + "." + std::to_string(minor) + "\n" + e.log;
-  if (!ok) throw Error("generated pipeline kernel failed to compile:\n" + e.log);
+  if (!ok) throw Error("generated pipeline kernel failed to compile:\n" + e.log + source_excerpt(src, e.log));
 }
 
 }  // namespace
@@ -1750,7 +1810,8 @@ Kernels compile(const Program& prog, bool load) {
       throw Error(std::string("loading a generated pipeline kernel: ") + cudaGetErrorString(err));
     }
     err = cudaLibraryGetKernel(&e.main, e.lib, prog.batched ? "dq_batch_main" : "dq_main");
-    if (err == cudaSuccess && prog.heavy) err = cudaLibraryGetKernel(&e.heavy, e.lib, "dq_heavy");
+    if (err == cudaSuccess && prog.heavy)
+      err = cudaLibraryGetKernel(&e.heavy, e.lib, prog.batched ? "dq_batch_heavy" : "dq_heavy");
     if (err != cudaSuccess) throw Error(std::string("generated kernel entry: ") + cudaGetErrorString(err));
   }
   Kernels k;

@@ -1373,7 +1373,7 @@ __global__ void heavy_group_units_kernel(DevHeavy H, int32_t* status) {
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += stride) {
     const uint32_t g = H.glist[j];
-    const uint64_t len = H.gkey[g] >> 32;
+    const uint64_t len = H.glen[g];
     const uint32_t cnt = H.gcnt[g];
     H.gstart[j] = cnt;
     H.unit_prefix[j] = ((len + kGroupRows - 1) / kGroupRows) * (uint64_t)((cnt + kGroupItems - 1) / kGroupItems);

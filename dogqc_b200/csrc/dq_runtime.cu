@@ -181,7 +181,7 @@ struct PipeRec {
   int expand_op = -1;       // level-0 expansion op with deferral
   uint64_t heavy_cap = 0;   // deferred-item capacity grown after an overflow (0: default)
   DevBuf pattern_buf, heavy_items, heavy_count, heavy_prefix;
-  DevBuf heavy_gkey, heavy_gcnt, heavy_glist, heavy_gstart, heavy_sorted;  // grouped deferral
+  DevBuf heavy_gkey, heavy_glen, heavy_gcnt, heavy_glist, heavy_gstart, heavy_sorted;  // grouped deferral
   bool mm_count = false;    // sink is a multimap count: bucket scan follows
   int mm_res = -1;
   int staged_cols = 0;
@@ -224,6 +224,10 @@ struct BatchStage {
   DevBuf segs, partials;
   int nsegs = 0;
   uint64_t scan_blocks = 0;
+  // deferred expansion shared by the instances (grouped by instance and range)
+  DevHeavy heavy{};
+  DevBuf h_items, h_count, h_prefix, h_gkey, h_glen, h_gcnt, h_glist, h_gstart, h_sorted, h_units;
+  int heavy_grid = 0;
 };
 
 struct dq_batch {
@@ -235,6 +239,7 @@ struct dq_batch {
   int nresets = 0, npacks = 0;
   size_t packed_bytes = 0;
   std::vector<std::vector<uint64_t>> col_off;   // [instance][column] offset in the packed buffer
+  uint64_t heavy_cap = 0;                       // deferred items, grown after an overflow
   uint8_t* host = nullptr;                      // pinned: packed columns, rows per instance, status
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -633,7 +638,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
 
   // deferred wide expansion ranges for the first level-0 expansion
   p.expand_op = -1;
-  for (int i = 0; i < d.nops && !plan->opts.batch_member; ++i) {
+  for (int i = 0; i < d.nops; ++i) {
     const dq_op& op = d.ops[i];
     if (op.kind != DQ_OP_EXPAND) continue;
     bool level0 = true;
@@ -661,9 +666,10 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     // generated kernels group the deferred items by range, so shorter ranges
     // pay off there: a range is gathered once per 32-row chunk for all probe
     // rows that matched it
-    H.grouped = !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) ? 1 : 0;
+    H.grouped = plan->opts.batch_member || !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) ? 1 : 0;
     const uint64_t dflt = H.grouped ? (uint64_t)kGroupThreshold : (uint64_t)tile * 8;
     H.threshold = ctx->cfg.defer_threshold > 0 ? (uint64_t)ctx->cfg.defer_threshold : dflt;
+    if (plan->opts.batch_member) break;  // the batch holds the buffers, shared by its instances
     p.heavy_items.alloc((size_t)H.cap * H.words * 8);
     p.heavy_count.alloc(8);  // item count, group count
     size_t nprefix = (size_t)H.cap + 1;
@@ -673,11 +679,13 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
       const uint64_t groups = std::min<uint64_t>(H.cap, rows_bound / (H.threshold + 1) + 1);
       H.gcap = (uint32_t)std::max<uint64_t>(64, 2 * groups);
       p.heavy_gkey.alloc((size_t)H.gcap * 8);
+      p.heavy_glen.alloc((size_t)H.gcap * 4);
       p.heavy_gcnt.alloc((size_t)H.gcap * 4);
       p.heavy_glist.alloc((size_t)H.gcap * 4);
       p.heavy_gstart.alloc(((size_t)H.gcap + 1) * 4);
       p.heavy_sorted.alloc((size_t)H.cap * std::max(H.nstash, 1) * 8);
       H.gkey = p.heavy_gkey.as<uint64_t>();
+      H.glen = p.heavy_glen.as<uint32_t>();
       H.gcnt = p.heavy_gcnt.as<uint32_t>();
       H.glist = p.heavy_glist.as<uint32_t>();
       H.ngroups = p.heavy_count.as<uint32_t>() + 1;
@@ -919,8 +927,8 @@ uint64_t plan_bytes(const dq_plan* plan) {
   }
   for (auto& pp : plan->pipes) {
     b += pp->pattern_buf.bytes + pp->heavy_items.bytes + pp->heavy_count.bytes + pp->heavy_prefix.bytes;
-    b += pp->heavy_gkey.bytes + pp->heavy_gcnt.bytes + pp->heavy_glist.bytes + pp->heavy_gstart.bytes +
-         pp->heavy_sorted.bytes;
+    b += pp->heavy_gkey.bytes + pp->heavy_glen.bytes + pp->heavy_gcnt.bytes + pp->heavy_glist.bytes +
+         pp->heavy_gstart.bytes + pp->heavy_sorted.bytes;
   }
   return b;
 }
@@ -1071,6 +1079,50 @@ void upload(DevBuf& buf, const std::vector<T>& v) {
 
 // (Re)builds the batch's kernels, descriptors and CUDA graph from its
 // instance plans (after preparation and after tables grew).
+// Deferred-expansion buffers of batch stage `p`, shared by all instances: items
+// of any instance, grouped by (instance, range).  Sized by the instances'
+// probe rows (at most 2^20 items, or what an overflow asked for) and their
+// build rows.
+void setup_batch_heavy(dq_batch* b, size_t p, BatchStage& S) {
+  const PipeRec& p0 = *b->inst[0]->pipes[p];
+  DevHeavy H = p0.dev.heavy;
+  int64_t rows = 0;
+  uint64_t build_rows = 0;
+  for (int i = 0; i < b->ninst; ++i) {
+    const dq_plan& pl = *b->inst[i];
+    const PipeRec& pi = *pl.pipes[p];
+    rows += pi.dev.nrows_dev ? (int64_t)pl.res[pi.dev.source_res]->dev.cap : pi.dev.nrows;
+    build_rows += std::max<uint64_t>(pl.res[pi.desc.ops[pi.expand_op].res]->pay_rows, 1);
+  }
+  H.grouped = 1;
+  H.cap = (uint32_t)std::min<int64_t>(std::max<int64_t>(rows, 1),
+                                      std::max<int64_t>(1 << 20, (int64_t)b->heavy_cap));
+  const uint64_t groups =
+      std::min<uint64_t>(H.cap, build_rows / (H.threshold + 1) + (uint64_t)b->ninst);
+  H.gcap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(64, 2 * groups), 0xfffffff0ull);
+  S.h_items.alloc((size_t)H.cap * H.words * 8);
+  S.h_count.alloc(8);
+  S.h_units.alloc(4);
+  S.h_gkey.alloc((size_t)H.gcap * 8);
+  S.h_glen.alloc((size_t)H.gcap * 4);
+  S.h_gcnt.alloc((size_t)H.gcap * 4);
+  S.h_glist.alloc((size_t)H.gcap * 4);
+  S.h_gstart.alloc(((size_t)H.gcap + 1) * 4);
+  S.h_sorted.alloc((size_t)H.cap * std::max(H.nstash, 1) * 8);
+  S.h_prefix.alloc((std::max<size_t>(H.cap, H.gcap) + 1) * 8);
+  H.items = S.h_items.as<uint64_t>();
+  H.count = S.h_count.as<uint32_t>();
+  H.ngroups = S.h_count.as<uint32_t>() + 1;
+  H.unit_prefix = S.h_prefix.as<uint64_t>();
+  H.gkey = S.h_gkey.as<uint64_t>();
+  H.glen = S.h_glen.as<uint32_t>();
+  H.gcnt = S.h_gcnt.as<uint32_t>();
+  H.glist = S.h_glist.as<uint32_t>();
+  H.gstart = S.h_gstart.as<uint32_t>();
+  H.sorted = S.h_sorted.as<uint64_t>();
+  S.heavy = H;
+}
+
 void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
   dq_ctx* ctx = b->ctx;
   const dq_plan& first = *b->inst[0];
@@ -1083,13 +1135,16 @@ void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
     jit::Tuning t = tuning;
     t.batched = true;
     const PipeRec& p0 = *first.pipes[p];
-    S.prog = jit::generate(p0.dev, -1, p0.desc.compact - 1, t);
+    S.prog = jit::generate(p0.dev, p0.expand_op, p0.desc.compact - 1, t);
     for (int i = 1; i < b->ninst; ++i) {
       const PipeRec& pi = *b->inst[i]->pipes[p];
-      if (jit::generate(pi.dev, -1, pi.desc.compact - 1, t).source != S.prog.source)
+      if (pi.expand_op != p0.expand_op ||
+          jit::generate(pi.dev, pi.expand_op, pi.desc.compact - 1, t).source != S.prog.source)
         throw DqError(DQ_ERR_BAD_IR, "batch instance " + std::to_string(i) + " differs in shape from instance 0");
     }
-    S.kernels = jit::compile(S.prog, true);
+    S.kernels = jit::compile(S.prog, !ctx->offline);
+    if (ctx->offline) continue;
+    if (p0.expand_op >= 0) setup_batch_heavy(b, p, S);
     std::vector<DevPipe> descs(b->ninst);
     std::vector<int64_t> prefix(b->ninst + 1, 0);
     const int64_t span = (int64_t)S.prog.block * S.prog.rows_per_thread;
@@ -1097,6 +1152,12 @@ void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
       const dq_plan& pl = *b->inst[i];
       descs[i] = pl.pipes[p]->dev;
       descs[i].status = b->status.as<int32_t>();
+      if (p0.expand_op >= 0) {
+        const uint64_t threshold = descs[i].heavy.threshold;
+        descs[i].heavy = S.heavy;
+        descs[i].heavy.threshold = threshold;
+        descs[i].tile_counter = S.h_units.as<uint32_t>();
+      }
       int64_t rows = descs[i].nrows;
       if (descs[i].nrows_dev) rows = (int64_t)pl.res[descs[i].source_res]->dev.cap;  // temp table: its capacity
       prefix[i + 1] = prefix[i] + (rows + span - 1) / span;
@@ -1109,6 +1170,13 @@ void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
     DQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, S.prog.block, S.prog.smem_bytes));
     if (occ < 1) throw DqError(DQ_ERR_UNSUPPORTED, "batched pipeline kernel cannot be resident");
     S.grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->sms * occ, prefix[b->ninst]));
+    if (S.kernels.heavy) {
+      const void* hf = (const void*)S.kernels.heavy;
+      DQ_CUDA(cudaFuncSetAttribute(hf, cudaFuncAttributeMaxDynamicSharedMemorySize, S.prog.smem_bytes));
+      int hocc = 0;
+      DQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&hocc, hf, S.prog.block, S.prog.smem_bytes));
+      S.heavy_grid = ctx->sms * std::max(hocc, 1);
+    }
     S.mm_scan = p0.mm_count;
     if (S.mm_scan) {
       std::vector<BatchScanSeg> segs(b->ninst);
@@ -1128,6 +1196,7 @@ void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
       S.scan_blocks = blocks;
     }
   }
+  if (ctx->offline) return;
   // resets of every instance's tables, in one launch
   std::vector<BatchReset> resets;
   for (int i = 0; i < b->ninst; ++i)
@@ -1201,9 +1270,22 @@ void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
     const int64_t* pre = S.bprefix.as<int64_t>();
     int n = b->ninst;
     void* args[] = {(void*)&d, (void*)&pre, (void*)&n};
+    if (S.kernels.heavy) {
+      rec(cudaMemsetAsync(S.h_count.ptr, 0, S.h_count.bytes, st));
+      rec(cudaMemsetAsync(S.h_units.ptr, 0, S.h_units.bytes, st));
+      rec(cudaMemsetAsync(S.h_gkey.ptr, 0xff, S.h_gkey.bytes, st));
+      rec(cudaMemsetAsync(S.h_gcnt.ptr, 0, S.h_gcnt.bytes, st));
+    }
     rec(cudaLaunchKernel((const void*)S.kernels.main, dim3(S.grid), dim3(S.prog.block), args,
                          (size_t)S.prog.smem_bytes, st));
     ++launches;
+    if (S.kernels.heavy) {
+      rec(launch_heavy_group(S.heavy, b->status.as<int32_t>(), ctx->sms, st));
+      void* hargs[] = {(void*)&d, (void*)&n};
+      rec(cudaLaunchKernel((const void*)S.kernels.heavy, dim3(S.heavy_grid), dim3(S.prog.block), hargs,
+                           (size_t)S.prog.smem_bytes, st));
+      launches += 4;
+    }
     if (S.mm_scan) {
       rec(launch_batch_scan(S.segs.as<BatchScanSeg>(), S.nsegs, S.scan_blocks, S.partials.as<uint32_t>(), st));
       launches += 3;
@@ -1452,9 +1534,9 @@ int dq_batch_prepare(dq_ctx* ctx, int32_t ninst, const dq_plan_desc* descs, cons
   if (!ctx || !descs || !out || ninst <= 0) return fail(ctx, DQ_ERR_INVALID, "bad arguments");
   *out = nullptr;
   return guarded(ctx, [&]() {
-    if (ctx->offline) throw DqError(DQ_ERR_UNSUPPORTED, "an offline context cannot hold batches");
     std::lock_guard<std::mutex> lk(ctx->mu);
-    DQ_CUDA(cudaSetDevice(ctx->device));
+    OfflineScope offline(ctx->offline);  // offline: the batch's kernels are compiled only
+    if (!ctx->offline) DQ_CUDA(cudaSetDevice(ctx->device));
     std::unique_ptr<dq_batch> b(new dq_batch());
     b->ctx = ctx;
     b->ninst = ninst;
@@ -1467,8 +1549,10 @@ int dq_batch_prepare(dq_ctx* ctx, int32_t ninst, const dq_plan_desc* descs, cons
         throw DqError(DQ_ERR_BAD_IR, "batch instance " + std::to_string(i) + " differs in shape from instance 0");
     }
     b->status.alloc(4);
-    DQ_CUDA(cudaEventCreate(&b->ev0));
-    DQ_CUDA(cudaEventCreate(&b->ev1));
+    if (!ctx->offline) {
+      DQ_CUDA(cudaEventCreate(&b->ev0));
+      DQ_CUDA(cudaEventCreate(&b->ev1));
+    }
     build_batch(b.get(), b->tuning, ctx->stream);
     *out = b.release();
     return (int)DQ_OK;
@@ -1479,6 +1563,7 @@ int dq_batch_execute(dq_batch* b, void* stream, dq_result** results) {
   if (!b || !results) return DQ_ERR_INVALID;
   dq_ctx* ctx = b->ctx;
   return guarded(ctx, [&]() {
+    if (ctx->offline) throw DqError(DQ_ERR_UNSUPPORTED, "an offline context compiles batches but cannot execute them");
     std::lock_guard<std::mutex> lk(ctx->mu);
     DQ_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
@@ -1489,6 +1574,21 @@ int dq_batch_execute(dq_batch* b, void* stream, dq_result** results) {
       DQ_CUDA(cudaEventRecord(b->ev1, st));
       DQ_CUDA(cudaStreamSynchronize(st));
       memcpy(&status, b->host + b->packed_bytes + (size_t)b->ninst * 8, 4);
+      if (status & kInfoHeavyFull) {
+        // this run's results stand; later runs get twice the deferred items
+        uint64_t want = 0;
+        for (auto& Sp : b->stages)
+          if (Sp->kernels.heavy) {
+            uint32_t n = 0;
+            DQ_CUDA(cudaMemcpy(&n, Sp->h_count.ptr, 4, cudaMemcpyDeviceToHost));
+            want = std::max<uint64_t>(want, 2ull * n);
+          }
+        b->heavy_cap = std::min<uint64_t>(std::max(want, 2 * std::max<uint64_t>(b->heavy_cap, 1 << 20)),
+                                          0xffffffffull);
+        status &= ~kInfoMask;
+        if (status == 0) build_batch(b, b->tuning, st);
+      }
+      status &= ~kInfoMask;
       if (status == 0) break;
       if (attempt >= 8 || (status & (kErrTimeout | kErrBadOp))) throw_status(status);
       for (auto& pl : b->inst) grow_plan(pl.get(), status);
@@ -1676,6 +1776,8 @@ struct PoolEntry {
   std::vector<uint64_t> col_off;
   int launches = 0;
   bool no_graph = false;
+  bool count_only = false;          // results too large to copy whole: the graph copies the
+                                    // row count, the rows follow after completion
   void drop_graph() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
@@ -1690,8 +1792,8 @@ struct PoolEntry {
   }
 };
 
-// Captures a pooled plan's run and result copies into a graph (no graph for
-// outputs above kGraphOutMax).
+// Captures a pooled plan's run and result copies into a graph (outputs whose
+// capacity exceeds kGraphOutMax: the row count only, the rows follow).
 void srv_build_graph(PoolEntry* pe, cudaStream_t st) {
   pe->drop_graph();
   dq_plan* plan = pe->plan.get();
@@ -1702,10 +1804,8 @@ void srv_build_graph(PoolEntry* pe, cudaStream_t st) {
     pe->col_off.push_back(bytes);
     bytes = align_up(bytes + o.dev.cap * (uint64_t)ctype_width(o.desc.pay_ctype[j]), 16);
   }
-  if (bytes > kGraphOutMax) {
-    pe->no_graph = true;
-    return;
-  }
+  pe->count_only = bytes > kGraphOutMax;
+  if (pe->count_only) bytes = 16;
   DQ_CUDA(cudaMallocHost((void**)&pe->host_out, bytes));
   DQ_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   cudaError_t err = cudaSuccess;
@@ -1718,18 +1818,20 @@ void srv_build_graph(PoolEntry* pe, cudaStream_t st) {
     if (err == cudaSuccess && e != cudaSuccess) err = e;
   };
   rec(cudaMemcpyAsync(pe->host_out, o.cursor.ptr, 8, cudaMemcpyDeviceToHost, st));
-  for (int j = 0; j < o.desc.npay; ++j)
-    rec(cudaMemcpyAsync(pe->host_out + pe->col_off[j], o.dev.pay[j],
-                        o.dev.cap * (uint64_t)ctype_width(o.desc.pay_ctype[j]), cudaMemcpyDeviceToHost, st));
+  if (!pe->count_only)
+    for (int j = 0; j < o.desc.npay; ++j)
+      rec(cudaMemcpyAsync(pe->host_out + pe->col_off[j], o.dev.pay[j],
+                          o.dev.cap * (uint64_t)ctype_width(o.desc.pay_ctype[j]), cudaMemcpyDeviceToHost, st));
   cudaGraph_t g = nullptr;
   const cudaError_t end = cudaStreamEndCapture(st, &g);
   pe->graph = g;
   DQ_CUDA(err);
   DQ_CUDA(end);
   DQ_CUDA(cudaGraphInstantiate(&pe->exec, pe->graph, 0));
+  DQ_CUDA(cudaGraphUpload(pe->exec, st));  // not at the first request's launch
 }
 
-dq_result* srv_graph_result(PoolEntry* pe) {
+dq_result* srv_graph_result(PoolEntry* pe, cudaStream_t st) {
   const ResRec& o = *pe->plan->res[pe->plan->result_res];
   uint64_t n = 0;
   memcpy(&n, pe->host_out, 8);
@@ -1739,9 +1841,15 @@ dq_result* srv_graph_result(PoolEntry* pe) {
   for (int j = 0; j < o.desc.npay; ++j) {
     const int w = ctype_width(o.desc.pay_ctype[j]);
     res->ctypes.push_back(o.desc.pay_ctype[j]);
-    const uint8_t* src = pe->host_out + pe->col_off[j];
-    res->cols.emplace_back(src, src + (size_t)n * w);
+    if (pe->count_only) {
+      res->cols.emplace_back((size_t)n * w);
+      if (n) DQ_CUDA(cudaMemcpyAsync(res->cols.back().data(), o.dev.pay[j], (size_t)n * w, cudaMemcpyDeviceToHost, st));
+    } else {
+      const uint8_t* src = pe->host_out + pe->col_off[j];
+      res->cols.emplace_back(src, src + (size_t)n * w);
+    }
   }
+  if (pe->count_only && n) DQ_CUDA(cudaStreamSynchronize(st));
   return res.release();
 }
 
@@ -1766,6 +1874,7 @@ struct dq_server {
   // owned by the worker thread
   std::unordered_map<std::string, std::vector<std::unique_ptr<PoolEntry>>> pool;
   std::vector<SrvSlot> slots;
+  cudaStream_t prep = nullptr;      // captures and uploads of pooled plans' graphs
   uint64_t mem = 0;
   // statistics (under mu)
   uint64_t submitted = 0, completed = 0, failed = 0, mem_peak = 0, mem_now = 0;
@@ -1835,14 +1944,27 @@ PoolEntry* srv_acquire(dq_server* s, SrvReq* r) {
     if (!any_busy) throw DqError(DQ_ERR_ADMISSION, "request needs more device memory than the server's budget");
     return nullptr;
   }
-  std::unique_ptr<PoolEntry> e(new PoolEntry());
-  e->plan = make_plan(s->ctx, &r->desc->d, PlanOpts());
-  e->bytes = plan_bytes(e->plan.get());
-  DQ_CUDA(cudaMallocHost((void**)&e->host_status, 4));
-  s->mem += e->bytes;
-  e->busy = true;
-  v.push_back(std::move(e));
-  return v.back().get();
+  auto prepare = [&]() {
+    std::unique_ptr<PoolEntry> e(new PoolEntry());
+    e->plan = make_plan(s->ctx, &r->desc->d, PlanOpts());
+    e->bytes = plan_bytes(e->plan.get());
+    DQ_CUDA(cudaMallocHost((void**)&e->host_status, 4));
+    s->mem += e->bytes;
+    v.push_back(std::move(e));
+    return v.back().get();
+  };
+  PoolEntry* got = prepare();
+  got->busy = true;
+  // the rest of the request's pool (a plan per slot, graphs captured), while
+  // this request pays for preparing one: concurrent copies of it later find a
+  // prepared plan instead of stalling the loop to prepare and capture one
+  const size_t want = std::min<size_t>((size_t)std::max(s->cfg.pool_per_query, 1), s->slots.size());
+  while (v.size() < want && s->mem + r->est <= s->cfg.memory_budget) {  // never evicts for this
+    PoolEntry* extra = prepare();
+    srv_build_graph(extra, s->prep);
+  }
+  if (v.size() > 1) DQ_CUDA(cudaStreamSynchronize(s->prep));
+  return got;
 }
 
 void srv_release(dq_server* s, SrvReq* r, PoolEntry* pe) {
@@ -1918,7 +2040,7 @@ void srv_complete(dq_server* s, SrvSlot& slot) {
   r->info.kernel_launches += slot.launches;
   dq_result* res;
   if (pe->exec) {
-    res = srv_graph_result(pe);
+    res = srv_graph_result(pe, slot.st);
   } else {
     collect_timing(pe->plan.get(), slot.launches);
     res = read_result(pe->plan.get(), slot.st);
@@ -2045,6 +2167,7 @@ int dq_server_start(dq_ctx* ctx, const dq_server_config* cfg, dq_server** out) {
         DQ_CUDA(cudaStreamCreateWithFlags(&slot.st, cudaStreamNonBlocking));
         DQ_CUDA(cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming));
       }
+      DQ_CUDA(cudaStreamCreateWithFlags(&s->prep, cudaStreamNonBlocking));
     }
     dq_server* raw = s.get();
     s->worker = std::thread(srv_loop, raw);
@@ -2198,11 +2321,13 @@ void dq_server_stop(dq_server* s) {
     for (auto& slot : s->slots) {
       if (slot.st) cudaStreamSynchronize(slot.st);
     }
+    if (s->prep) cudaStreamSynchronize(s->prep);
     s->pool.clear();
     for (auto& slot : s->slots) {
       if (slot.done) cudaEventDestroy(slot.done);
       if (slot.st) cudaStreamDestroy(slot.st);
     }
+    if (s->prep) cudaStreamDestroy(s->prep);
   }
   for (auto& kv : s->reqs)
     if (kv.second->result) delete kv.second->result;

@@ -61,3 +61,15 @@ def test_every_workload_compiles_offline(engine, name):
 def test_tuned_launch_shapes_compile(engine, name, tuning):
     plan = engine.prepare(resolved(engine, name), tuning=tuning)
     check_sources(plan, max_spill=32)
+
+
+@pytest.mark.parametrize("shape", ["c0", "c1", "c2", "c3"])
+def test_batches_compile_offline(engine, shape):
+    """A batch's many-instance kernels (the expansion's deferral and its
+    grouped heavy kernel included) compile without a device."""
+    from dogqc_b200 import batch
+    insts = batch.make_instances(shape, 3, lo=1 << 10, hi=1 << 12)
+    batch.register(engine, insts)
+    b = batch.prepare_batch(engine, insts, tuning={"rows_per_thread": 2})
+    with pytest.raises(L.DqError):
+        b.execute()
