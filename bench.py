@@ -34,6 +34,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from dogqc_b200 import replicas  # noqa: E402  (after the path insert)
+
 SCALE = 1.0
 WORKLOAD = "c1"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -159,29 +161,15 @@ class ClockSampler(object):
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=300))
-    return world, rank, local
+    return replicas.setup()
 
 
 def dist_max(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(x, world)
 
 
 def dist_barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    replicas.barrier(world)
 
 
 def build_plan(db):
@@ -574,9 +562,7 @@ def main():
         out = run_ours(args, world, rank, local)
     if rank == 0 and out is not None:
         print(json.dumps(out), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.teardown(world)
 
 
 if __name__ == "__main__":
