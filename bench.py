@@ -176,7 +176,7 @@ def build_plan(db):
     from dogqc_b200 import workloads
     from dogqc_b200.relational import RelationalAlgebra
     alg = RelationalAlgebra(db)
-    plan, cfg = workloads.build(WORKLOAD, alg)
+    plan, cfg = workloads.build(WORKLOAD, alg, scale=SCALE)
     return alg.resolveAlgebraPlan(plan, cfg)
 
 
@@ -484,19 +484,19 @@ def run_served(args, world, rank, local):
     qs = serve.make_queries(sizes=sizes)
     engine = Engine(local)
     serve.register(engine, qs)
-    n = 2000
+    n = 6000
     sched = serve.arrivals(n, None, qs, seed=5)
     _, _, plans = serve.sequence(engine, qs, sched[:200])
     per, wall1, plans = serve.sequence(engine, qs, sched, plans)
     one = {"queries_per_s": n / wall1, "p50_ms": serve.percentile(per, .5), "p99_ms": serve.percentile(per, .99)}
-    srv = serve.Server(engine, slots=args.slots)
+    srv = serve.Server(engine, slots=args.slots, batch_max=args.batch_max)
     serve.warm(srv, qs, args.slots)
     with ClockSampler(local) as clocks:
         infos, wall = serve.replay(srv, qs, sched)
     tot = [i["total_ms"] for i in infos]
     rates = []
-    for rate in (100, 1000, 5000):
-        sch = serve.arrivals(min(4000, max(300, rate)), rate, qs, seed=9)
+    for rate in (100, 1000, 5000, 10000, 20000, 40000):
+        sch = serve.arrivals(min(8000, max(300, rate // 4)), rate, qs, seed=9)
         inf, w = serve.replay(srv, qs, sch)
         t = [i["total_ms"] for i in inf]
         rates.append({"offered_qps": rate, "achieved_qps": len(sch) / w, "p50_ms": serve.percentile(t, .5),
@@ -513,7 +513,9 @@ def run_served(args, world, rank, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
         "data": "synthetic (seeded)",
         "config": {"workload": "served_mixed_stream", "shapes": ["c0", "c1", "c2", "c3"], "sizes": list(sizes),
-                   "slots": args.slots, "requests": n, "memory_budget_gb": 150, "parallelism": "replicas"},
+                   "slots": args.slots, "batch_max": args.batch_max or 16, "requests": n, "memory_budget_gb": 150,
+                   "parallelism": "replicas"},
+        "batches": {"launches": st["batches"], "requests": st["batched"]},
         "p50_ms": serve.percentile(tot, .5), "p99_ms": serve.percentile(tot, .99),
         "one_at_a_time": one, "speedup_vs_one_at_a_time": value / one["queries_per_s"],
         "poisson": rates, "memory_peak_bytes": st["memory_peak"],
@@ -539,7 +541,9 @@ def main():
                          "the other configurations, for the per-pipeline table; c2x256: the batched form; "
                          "c4: the served mixed stream")
     ap.add_argument("--autotune", action="store_true", help="c2x256: pick the batch's tuning by measurement")
-    ap.add_argument("--slots", type=int, default=4, help="c4: requests in flight on the device")
+    ap.add_argument("--slots", type=int, default=4, help="c4: launches in flight on the device (streams)")
+    ap.add_argument("--batch-max", type=int, default=0,
+                    help="c4: requests of one shape per launch (0: 16; 1: every request alone)")
     ap.add_argument("--served-sizes", default="0.0005,0.002,0.01",
                     help="c4: table sizes of the query mix, as fractions of the configurations' rows")
     args = ap.parse_args()

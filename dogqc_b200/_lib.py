@@ -98,7 +98,7 @@ class dq_tuning(C.Structure):
 
 class dq_server_config(C.Structure):
     _fields_ = [("slots", C.c_int32), ("pool_per_query", C.c_int32), ("memory_budget", C.c_uint64),
-                ("reserved", C.c_int32 * 4)]
+                ("batch_max", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class dq_request_info(C.Structure):
@@ -109,7 +109,8 @@ class dq_request_info(C.Structure):
 class dq_server_stats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("memory_in_use", C.c_uint64), ("memory_peak", C.c_uint64), ("p50_ms", C.c_double),
-                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("span_ms", C.c_double)]
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("span_ms", C.c_double),
+                ("batches", C.c_uint64), ("batched", C.c_uint64)]
 
 
 NOALLOC_MAX_BUILD_ROWS = 262144
@@ -127,7 +128,7 @@ class dq_join_agg_args(C.Structure):
 def check_layout():
     """Sizes the C compiler gives these structs on x86-64 (LP64)."""
     expect = {dq_config: 40, dq_column: 40, dq_slot: 8, dq_op: 40, dq_resource: 80, dq_join_agg_args: 104,
-              dq_tuning: 32, dq_server_config: 32, dq_request_info: 40, dq_server_stats: 72}
+              dq_tuning: 32, dq_server_config: 32, dq_request_info: 40, dq_server_stats: 88}
     for t, n in expect.items():
         if C.sizeof(t) != n:
             raise AssertionError("%s is %d bytes, header implies %d" % (t.__name__, C.sizeof(t), n))

@@ -43,7 +43,7 @@ class Instance(object):
         base = workloads.GENERATORS[shape](scale, seed=seed if seed is not None else SEED + 1 + index)
         self.base_db = base
         alg = RelationalAlgebra(base)
-        plan, cfg = workloads.build(shape, alg)
+        plan, cfg = workloads.build(shape, alg, scale=scale)
         self.plan = alg.resolveAlgebraPlan(plan, cfg)
         self.lowering = Lowering(self.plan)
         for p in self.lowering.pipes:

@@ -1756,6 +1756,7 @@ struct SrvReq {
   std::string error;
   bool done = false;
   int attempts = 0;                 // executions after tables grew
+  bool solo = false;                // runs alone (a batch it was in overflowed)
   dq_request_info info{};
 };
 
@@ -1853,12 +1854,84 @@ dq_result* srv_graph_result(PoolEntry* pe, cudaStream_t st) {
   return res.release();
 }
 
+// ------------------------------------------------------ continuous batching --
+// Waiting requests of one shape (the same generated batch kernels: same
+// pipelines and ops, any tables and sizes) run as one many-instance launch on
+// one slot, each on its own pooled plan: the batch kernels and helpers of
+// dq_batch_* over descriptors assembled per dispatch.
+
+struct SrvShape {                   // the batch kernels of one request shape
+  struct Stage {
+    jit::Program prog;
+    jit::Kernels kernels;
+    int occ = 1, hocc = 1;          // resident CTAs per SM (main, heavy kernel)
+    bool mm_scan = false;           // a multimap count: the bucket scans follow
+    int mm_res = -1;
+    int expand_op = -1;             // deferred expansion (heavy kernel)
+  };
+  std::vector<Stage> stages;
+};
+
+void grow(DevBuf& b, size_t n) {
+  if (b.bytes < n) b.alloc(n + n / 2);
+}
+
+struct HeavyBufs {                  // a slot's shared deferral buffers of one stage
+  DevBuf items, count, units, gkey, glen, gcnt, glist, gstart, sorted, prefix;
+  DevHeavy bind(const DevHeavy& proto, uint32_t cap, uint32_t gcap) {
+    DevHeavy H = proto;
+    H.grouped = 1;
+    H.cap = cap;
+    H.gcap = gcap;
+    grow(items, (size_t)cap * H.words * 8);
+    grow(count, 8);
+    grow(units, 4);
+    grow(gkey, (size_t)gcap * 8);
+    grow(glen, (size_t)gcap * 4);
+    grow(gcnt, (size_t)gcap * 4);
+    grow(glist, (size_t)gcap * 4);
+    grow(gstart, ((size_t)gcap + 1) * 4);
+    grow(sorted, (size_t)cap * std::max(H.nstash, 1) * 8);
+    grow(prefix, (std::max<size_t>(cap, gcap) + 1) * 8);
+    H.items = items.as<uint64_t>();
+    H.count = count.as<uint32_t>();
+    H.ngroups = count.as<uint32_t>() + 1;
+    H.unit_prefix = prefix.as<uint64_t>();
+    H.gkey = gkey.as<uint64_t>();
+    H.glen = glen.as<uint32_t>();
+    H.gcnt = gcnt.as<uint32_t>();
+    H.glist = glist.as<uint32_t>();
+    H.gstart = gstart.as<uint32_t>();
+    H.sorted = sorted.as<uint64_t>();
+    return H;
+  }
+};
+
+struct SrvBatch {                   // a slot's batch in flight and its scratch
+  std::vector<std::pair<SrvReq*, PoolEntry*>> members;
+  DevBuf params, packed, rows, status, partials;
+  uint8_t* host_params = nullptr;   // pinned staging of the descriptors
+  size_t host_params_cap = 0;
+  uint8_t* host_out = nullptr;      // pinned: packed columns, rows per member, status
+  size_t host_out_cap = 0;
+  std::vector<std::unique_ptr<HeavyBufs>> heavy;
+  std::vector<std::vector<uint64_t>> col_off;
+  size_t packed_bytes = 0;
+  int launches = 0;
+  ~SrvBatch() {
+    if (host_params) cudaFreeHost(host_params);
+    if (host_out) cudaFreeHost(host_out);
+  }
+};
+
 struct SrvSlot {
   cudaStream_t st = nullptr;
   cudaEvent_t done = nullptr;
-  SrvReq* req = nullptr;
+  SrvReq* req = nullptr;            // a request alone, or
   PoolEntry* pe = nullptr;
+  std::unique_ptr<SrvBatch> batch;  // a batch (members non-empty)
   int launches = 0;
+  bool busy() const { return req || (batch && !batch->members.empty()); }
 };
 
 }  // namespace
@@ -1873,6 +1946,9 @@ struct dq_server {
   uint64_t next_id = 1;
   // owned by the worker thread
   std::unordered_map<std::string, std::vector<std::unique_ptr<PoolEntry>>> pool;
+  std::unordered_map<std::string, SrvShape*> shape_of;   // request key -> its batch shape (null: alone)
+  std::unordered_map<std::string, std::unique_ptr<SrvShape>> shapes;
+  uint64_t batches = 0, batched = 0;
   std::vector<SrvSlot> slots;
   cudaStream_t prep = nullptr;      // captures and uploads of pooled plans' graphs
   uint64_t mem = 0;
@@ -1930,6 +2006,330 @@ bool srv_make_room(dq_server* s, uint64_t need, const std::string& keep) {
 
 // A prepared plan for the request: an idle one of the same query, else a new
 // one if the budget allows.  nullptr: wait; throws: the request fails.
+// The batch shape of a prepared plan: its pipelines' many-instance kernels
+// (generated, compiled on first sight of the shape), or null when the plan
+// runs alone (a prebuilt kernel, or a result too large for the packed copy).
+SrvShape* srv_shape(dq_server* s, dq_plan* plan) {
+  if (s->cfg.batch_max <= 1) return nullptr;
+  for (auto& pp : plan->pipes)
+    if (!pp->jit) return nullptr;
+  const ResRec& o = *plan->res[plan->result_res];
+  if (o.desc.npay == 0) return nullptr;
+  uint64_t out = 0;
+  for (int j = 0; j < o.desc.npay; ++j) out += o.dev.cap * (uint64_t)ctype_width(o.desc.pay_ctype[j]);
+  if (out > kGraphOutMax) return nullptr;
+  std::vector<jit::Program> progs;
+  std::string key;
+  for (auto& pp : plan->pipes) {
+    jit::Tuning t = plan->opts.tuning;
+    t.batched = true;
+    progs.push_back(jit::generate(pp->dev, pp->expand_op, pp->desc.compact - 1, t));
+    key += progs.back().source;
+    key.push_back('\1');
+  }
+  auto it = s->shapes.find(key);
+  if (it != s->shapes.end()) return it->second.get();
+  std::unique_ptr<SrvShape> sh(new SrvShape());
+  for (size_t p = 0; p < progs.size(); ++p) {
+    SrvShape::Stage st;
+    st.prog = progs[p];
+    st.kernels = jit::compile(st.prog, true);
+    const void* fn = (const void*)st.kernels.main;
+    DQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, st.prog.smem_bytes));
+    DQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&st.occ, fn, st.prog.block, st.prog.smem_bytes));
+    if (st.kernels.heavy) {
+      const void* hf = (const void*)st.kernels.heavy;
+      DQ_CUDA(cudaFuncSetAttribute(hf, cudaFuncAttributeMaxDynamicSharedMemorySize, st.prog.smem_bytes));
+      DQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&st.hocc, hf, st.prog.block, st.prog.smem_bytes));
+    }
+    if (st.occ < 1 || (st.kernels.heavy && st.hocc < 1)) return nullptr;
+    st.mm_scan = plan->pipes[p]->mm_count;
+    st.mm_res = plan->pipes[p]->mm_res;
+    st.expand_op = plan->pipes[p]->expand_op;
+    sh->stages.push_back(st);
+  }
+  SrvShape* raw = sh.get();
+  s->shapes[key] = std::move(sh);
+  return raw;
+}
+
+// Appends `n` bytes of `src` to a parameter blob at a 256-byte boundary; returns the offset.
+size_t blob_put(std::vector<uint8_t>& blob, const void* src, size_t n) {
+  const size_t off = align_up(blob.size(), 256);
+  blob.resize(off + n);
+  if (n) memcpy(blob.data() + off, src, n);
+  return off;
+}
+
+// One launch sequence for the batch's members on the slot's stream: resets of
+// all members' tables, every stage's many-instance kernel (with its shared
+// deferral and bucket scans), a pack of all results, one copy back.
+void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
+  SrvBatch& B = *slot.batch;
+  dq_ctx* ctx = s->ctx;
+  cudaStream_t st = slot.st;
+  const int K = (int)B.members.size();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    const double t = now_ms();
+    for (auto& m : B.members) {
+      m.first->t_dispatch = t;
+      m.first->info.bytes = m.second->bytes;
+    }
+  }
+  grow(B.status, 4);
+  grow(B.rows, (size_t)K * 8);
+  while (B.heavy.size() < sh->stages.size()) B.heavy.emplace_back(new HeavyBufs());
+  std::vector<uint8_t> blob;
+  struct StageArgs {
+    size_t descs = 0, bprefix = 0, segs = 0;
+    uint64_t blocks = 0, scan_blocks = 0;
+    int grid = 1;
+    DevHeavy heavy{};
+  };
+  std::vector<StageArgs> sa(sh->stages.size());
+  uint64_t max_scan_blocks = 0;
+  for (size_t p = 0; p < sh->stages.size(); ++p) {
+    const SrvShape::Stage& S = sh->stages[p];
+    std::vector<DevPipe> descs(K);
+    std::vector<int64_t> prefix(K + 1, 0);
+    const int64_t span = (int64_t)S.prog.block * S.prog.rows_per_thread;
+    int64_t rows_all = 0;
+    uint64_t build_rows = 0;
+    for (int i = 0; i < K; ++i) {
+      const dq_plan& pl = *B.members[i].second->plan;
+      const PipeRec& pi = *pl.pipes[p];
+      descs[i] = pi.dev;
+      descs[i].status = B.status.as<int32_t>();
+      const int64_t rows = pi.dev.nrows_dev ? (int64_t)pl.res[pi.dev.source_res]->dev.cap : pi.dev.nrows;
+      prefix[i + 1] = prefix[i] + (rows + span - 1) / span;
+      rows_all += rows;
+      if (S.expand_op >= 0) build_rows += std::max<uint64_t>(pl.res[pi.desc.ops[S.expand_op].res]->pay_rows, 1);
+    }
+    if (S.expand_op >= 0) {
+      const DevHeavy& proto = B.members[0].second->plan->pipes[p]->dev.heavy;
+      const uint32_t cap = (uint32_t)std::min<int64_t>(std::max<int64_t>(rows_all, 1), 1 << 20);
+      const uint64_t groups = std::min<uint64_t>(cap, build_rows / (proto.threshold + 1) + (uint64_t)K);
+      const uint32_t gcap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(64, 2 * groups), 0xfffffff0ull);
+      sa[p].heavy = B.heavy[p]->bind(proto, cap, gcap);
+      for (int i = 0; i < K; ++i) {
+        const uint64_t threshold = descs[i].heavy.threshold;
+        descs[i].heavy = sa[p].heavy;
+        descs[i].heavy.threshold = threshold;
+        descs[i].tile_counter = B.heavy[p]->units.as<uint32_t>();
+      }
+    }
+    sa[p].blocks = (uint64_t)prefix[K];
+    sa[p].grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)ctx->sms * S.occ, prefix[K]));
+    sa[p].descs = blob_put(blob, descs.data(), descs.size() * sizeof(DevPipe));
+    sa[p].bprefix = blob_put(blob, prefix.data(), prefix.size() * sizeof(int64_t));
+    if (S.mm_scan) {
+      std::vector<BatchScanSeg> segs(K);
+      uint64_t blocks = 0;
+      for (int i = 0; i < K; ++i) {
+        const DevRes& R = B.members[i].second->plan->res[S.mm_res]->dev;
+        segs[i].counts = R.counts;
+        segs[i].offsets = R.offsets;
+        segs[i].n = R.cap;
+        segs[i].block0 = blocks;
+        segs[i].nblocks = batch_scan_blocks(R.cap);
+        blocks += segs[i].nblocks;
+      }
+      sa[p].segs = blob_put(blob, segs.data(), segs.size() * sizeof(BatchScanSeg));
+      sa[p].scan_blocks = blocks;
+      max_scan_blocks = std::max(max_scan_blocks, blocks);
+    }
+  }
+  grow(B.partials, std::max<uint64_t>(max_scan_blocks, 1) * 4);
+  // resets and the result pack of every member
+  std::vector<BatchReset> resets;
+  std::vector<BatchPack> packs;
+  B.col_off.assign(K, std::vector<uint64_t>());
+  uint64_t off = 0;
+  for (int i = 0; i < K; ++i) {
+    const dq_plan& pl = *B.members[i].second->plan;
+    for (auto& rp : pl.res) {
+      const ResRec& r = *rp;
+      BatchReset op{};
+      switch (r.desc.kind) {
+        case DQ_RES_UNIQUE:
+          op.ptr = r.dev.slots, op.n = (r.dev.cap + 1) * r.dev.words, op.value = kEmpty, op.kind = 0;
+          break;
+        case DQ_RES_AGG:
+          op.ptr = r.dev.slots, op.n = r.dev.cap + 1, op.kind = 2, op.words = r.dev.words;
+          op.val_word = r.dev.val_word, op.naggs = r.dev.naggs;
+          for (int j = 0; j < r.dev.naggs && j < 16; ++j) op.reds |= (uint64_t)(r.dev.agg_red[j] & 15) << (4 * j);
+          break;
+        case DQ_RES_MULTI:
+          op.ptr = r.dev.counts, op.n = r.dev.cap, op.value = 0, op.kind = 1;
+          break;
+        case DQ_RES_OUTPUT:
+          op.ptr = r.dev.cursor, op.n = 1, op.value = 0, op.kind = 0;
+          break;
+      }
+      resets.push_back(op);
+    }
+    const ResRec& o = *pl.res[pl.result_res];
+    for (int j = 0; j < o.desc.npay; ++j) {
+      BatchPack pk{};
+      pk.src = o.dev.pay[j];
+      pk.cursor = o.dev.cursor;
+      pk.cap = o.dev.cap;
+      pk.width = ctype_width(o.desc.pay_ctype[j]);
+      pk.dst = off;
+      pk.rows_out = j == 0 ? B.rows.as<uint64_t>() + i : nullptr;
+      B.col_off[i].push_back(off);
+      off += align_up(o.dev.cap * (uint64_t)pk.width, 16);
+      packs.push_back(pk);
+    }
+  }
+  const size_t resets_off = blob_put(blob, resets.data(), resets.size() * sizeof(BatchReset));
+  const size_t packs_off = blob_put(blob, packs.data(), packs.size() * sizeof(BatchPack));
+  B.packed_bytes = std::max<uint64_t>(off, 16);
+  grow(B.packed, B.packed_bytes);
+  const size_t out_need = B.packed_bytes + (size_t)K * 8 + 16;
+  if (B.host_out_cap < out_need) {
+    if (B.host_out) cudaFreeHost(B.host_out);
+    B.host_out = nullptr;
+    B.host_out_cap = out_need + out_need / 2;
+    DQ_CUDA(cudaMallocHost((void**)&B.host_out, B.host_out_cap));
+  }
+  if (B.host_params_cap < blob.size()) {
+    if (B.host_params) cudaFreeHost(B.host_params);
+    B.host_params = nullptr;
+    B.host_params_cap = blob.size() + blob.size() / 2;
+    DQ_CUDA(cudaMallocHost((void**)&B.host_params, B.host_params_cap));
+  }
+  grow(B.params, blob.size());
+  memcpy(B.host_params, blob.data(), blob.size());
+  uint8_t* dev = B.params.as<uint8_t>();
+  int launches = 0;
+  DQ_CUDA(cudaMemcpyAsync(dev, B.host_params, blob.size(), cudaMemcpyHostToDevice, st));
+  DQ_CUDA(cudaMemsetAsync(B.status.ptr, 0, 4, st));
+  DQ_CUDA(launch_batch_reset(reinterpret_cast<const BatchReset*>(dev + resets_off), (int)resets.size(), ctx->sms, st));
+  ++launches;
+  for (size_t p = 0; p < sh->stages.size(); ++p) {
+    const SrvShape::Stage& S = sh->stages[p];
+    const DevPipe* d = reinterpret_cast<const DevPipe*>(dev + sa[p].descs);
+    const int64_t* pre = reinterpret_cast<const int64_t*>(dev + sa[p].bprefix);
+    int n = K;
+    if (S.expand_op >= 0) {
+      HeavyBufs& hb = *B.heavy[p];
+      DQ_CUDA(cudaMemsetAsync(hb.count.ptr, 0, 8, st));
+      DQ_CUDA(cudaMemsetAsync(hb.units.ptr, 0, 4, st));
+      DQ_CUDA(cudaMemsetAsync(hb.gkey.ptr, 0xff, (size_t)sa[p].heavy.gcap * 8, st));
+      DQ_CUDA(cudaMemsetAsync(hb.gcnt.ptr, 0, (size_t)sa[p].heavy.gcap * 4, st));
+    }
+    void* args[] = {(void*)&d, (void*)&pre, (void*)&n};
+    DQ_CUDA(cudaLaunchKernel((const void*)S.kernels.main, dim3(sa[p].grid), dim3(S.prog.block), args,
+                             (size_t)S.prog.smem_bytes, st));
+    ++launches;
+    if (S.expand_op >= 0) {
+      DQ_CUDA(launch_heavy_group(sa[p].heavy, B.status.as<int32_t>(), ctx->sms, st));
+      void* hargs[] = {(void*)&d, (void*)&n};
+      DQ_CUDA(cudaLaunchKernel((const void*)S.kernels.heavy, dim3(ctx->sms * S.hocc), dim3(S.prog.block), hargs,
+                               (size_t)S.prog.smem_bytes, st));
+      launches += 4;
+    }
+    if (S.mm_scan) {
+      DQ_CUDA(launch_batch_scan(reinterpret_cast<const BatchScanSeg*>(dev + sa[p].segs), K, sa[p].scan_blocks,
+                                B.partials.as<uint32_t>(), st));
+      launches += 3;
+    }
+  }
+  DQ_CUDA(launch_batch_pack(reinterpret_cast<const BatchPack*>(dev + packs_off), (int)packs.size(),
+                            B.packed.as<uint8_t>(), ctx->sms, st));
+  ++launches;
+  DQ_CUDA(cudaMemcpyAsync(B.host_out, B.packed.ptr, B.packed_bytes, cudaMemcpyDeviceToHost, st));
+  DQ_CUDA(cudaMemcpyAsync(B.host_out + B.packed_bytes, B.rows.ptr, (size_t)K * 8, cudaMemcpyDeviceToHost, st));
+  DQ_CUDA(cudaMemcpyAsync(B.host_out + B.packed_bytes + (size_t)K * 8, B.status.ptr, 4, cudaMemcpyDeviceToHost, st));
+  DQ_CUDA(cudaEventRecord(slot.done, st));
+  B.launches = launches;
+  std::lock_guard<std::mutex> lk(s->mu);
+  ++s->batches;
+  s->batched += (uint64_t)K;
+}
+
+void srv_finish(dq_server* s, SrvReq* r, int status, const std::string& err, dq_result* res);
+void srv_release(dq_server* s, SrvReq* r, PoolEntry* pe);
+
+// A completed batch: every member's result, or (a member's table overflowed)
+// every member back to the front of the queue to run alone, where tables grow.
+void srv_complete_batch(dq_server* s, SrvSlot& slot) {
+  SrvBatch& B = *slot.batch;
+  const int K = (int)B.members.size();
+  int32_t status = 0;
+  memcpy(&status, B.host_out + B.packed_bytes + (size_t)K * 8, 4);
+  status &= ~kInfoMask;
+  std::vector<std::pair<SrvReq*, PoolEntry*>> members;
+  members.swap(B.members);
+  if (status != 0) {
+    for (auto& m : members) srv_release(s, m.first, m.second);
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (auto it = members.rbegin(); it != members.rend(); ++it) {
+      it->first->solo = true;
+      it->first->t_dispatch = 0;
+      s->pending.push_front(it->first);
+    }
+    return;
+  }
+  const uint64_t* rows = reinterpret_cast<const uint64_t*>(B.host_out + B.packed_bytes);
+  for (int i = 0; i < K; ++i) {
+    SrvReq* r = members[i].first;
+    PoolEntry* pe = members[i].second;
+    const ResRec& o = *pe->plan->res[pe->plan->result_res];
+    std::unique_ptr<dq_result> res(new dq_result());
+    res->nrows = (int64_t)rows[i];
+    for (int j = 0; j < o.desc.npay; ++j) {
+      const int w = ctype_width(o.desc.pay_ctype[j]);
+      res->ctypes.push_back(o.desc.pay_ctype[j]);
+      const uint8_t* src = B.host_out + B.col_off[i][j];
+      res->cols.emplace_back(src, src + (size_t)rows[i] * w);
+    }
+    r->info.kernel_launches += B.launches;
+    srv_release(s, r, pe);
+    srv_finish(s, r, DQ_OK, "", res.release());
+  }
+}
+
+// Waiting requests of the shape of the oldest one that have an idle pooled
+// plan, up to batch_max, taken out of the queue (none when the oldest
+// request runs alone or its shape is not known yet).
+std::vector<std::pair<SrvReq*, PoolEntry*>> srv_take_batch(dq_server* s, SrvShape** shape) {
+  std::vector<std::pair<SrvReq*, PoolEntry*>> out;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->pending.empty() || s->cfg.batch_max <= 1) return out;
+  SrvReq* head = s->pending.front();
+  if (head->solo) return out;
+  auto sit = s->shape_of.find(head->desc->key);
+  if (sit == s->shape_of.end() || !sit->second) return out;
+  SrvShape* sh = sit->second;
+  size_t seen = 0;
+  for (auto it = s->pending.begin(); it != s->pending.end() && (int)out.size() < s->cfg.batch_max && seen < 1024;
+       ++seen) {
+    SrvReq* r = *it;
+    auto q = s->shape_of.find(r->desc->key);
+    PoolEntry* pe = nullptr;
+    if (!r->solo && q != s->shape_of.end() && q->second == sh) {
+      auto& v = s->pool[r->desc->key];
+      for (auto& e : v)
+        if (!e->busy) {
+          pe = e.get();
+          break;
+        }
+    }
+    if (!pe) {
+      ++it;
+      continue;
+    }
+    pe->busy = true;
+    out.emplace_back(r, pe);
+    it = s->pending.erase(it);
+  }
+  *shape = sh;
+  return out;
+}
+
 PoolEntry* srv_acquire(dq_server* s, SrvReq* r) {
   auto& v = s->pool[r->desc->key];
   for (auto& e : v)
@@ -1937,6 +2337,9 @@ PoolEntry* srv_acquire(dq_server* s, SrvReq* r) {
       e->busy = true;
       return e.get();
     }
+  // a full pool waits for one of its plans (preparing more on the loop stalls
+  // every slot, and the surplus would be freed later with a device sync)
+  if (!v.empty() && v.size() >= (size_t)std::max(s->cfg.pool_per_query, 1)) return nullptr;
   if (!srv_make_room(s, r->est, r->desc->key)) {
     bool any_busy = false;
     for (auto& kv : s->pool)
@@ -1953,12 +2356,14 @@ PoolEntry* srv_acquire(dq_server* s, SrvReq* r) {
     v.push_back(std::move(e));
     return v.back().get();
   };
+  const bool first = v.empty();
   PoolEntry* got = prepare();
   got->busy = true;
-  // the rest of the request's pool (a plan per slot, graphs captured), while
-  // this request pays for preparing one: concurrent copies of it later find a
-  // prepared plan instead of stalling the loop to prepare and capture one
-  const size_t want = std::min<size_t>((size_t)std::max(s->cfg.pool_per_query, 1), s->slots.size());
+  if (first && !s->shape_of.count(r->desc->key)) s->shape_of[r->desc->key] = srv_shape(s, got->plan.get());
+  // the rest of the request's pool (graphs captured), while this request pays
+  // for preparing one: concurrent copies of it later find a prepared plan
+  // instead of stalling the loop to prepare and capture one
+  const size_t want = (size_t)std::max(s->cfg.pool_per_query, 1);
   while (v.size() < want && s->mem + r->est <= s->cfg.memory_budget) {  // never evicts for this
     PoolEntry* extra = prepare();
     srv_build_graph(extra, s->prep);
@@ -2068,11 +2473,24 @@ void srv_loop(dq_server* s) {
       std::lock_guard<std::mutex> lk(s->ctx->mu);
       // completions
       for (auto& slot : s->slots) {
-        if (!slot.req) continue;
+        if (!slot.busy()) continue;
         busy = true;
         const cudaError_t q = cudaEventQuery(slot.done);
         if (q == cudaErrorNotReady) continue;
         progressed = true;
+        if (!slot.req) {  // a batch
+          if (q == cudaSuccess) {
+            srv_complete_batch(s, slot);
+          } else {
+            std::vector<std::pair<SrvReq*, PoolEntry*>> members;
+            members.swap(slot.batch->members);
+            for (auto& m : members) {
+              srv_release(s, m.first, m.second);
+              srv_finish(s, m.first, DQ_ERR_CUDA, std::string("batch execution: ") + cudaGetErrorString(q), nullptr);
+            }
+          }
+          continue;
+        }
         SrvReq* r = slot.req;
         try {
           if (q != cudaSuccess) throw DqError(DQ_ERR_CUDA, std::string("request execution: ") + cudaGetErrorString(q));
@@ -2089,9 +2507,47 @@ void srv_loop(dq_server* s) {
           srv_finish(s, r, DQ_ERR_CUDA, e.what(), nullptr);
         }
       }
-      // admissions, oldest first, while a slot and memory are free
+      // admissions, oldest first, while a slot and memory are free: the oldest
+      // request with the waiting requests of its shape as one batch when there
+      // are several, else alone
       for (auto& slot : s->slots) {
-        if (slot.req) continue;
+        if (slot.busy()) continue;
+        {
+          SrvShape* sh = nullptr;
+          std::vector<std::pair<SrvReq*, PoolEntry*>> take = srv_take_batch(s, &sh);
+          if (take.size() >= 2) {
+            if (!slot.batch) slot.batch.reset(new SrvBatch());
+            slot.batch->members = take;
+            try {
+              srv_dispatch_batch(s, slot, sh);
+            } catch (const std::exception& e) {
+              std::vector<std::pair<SrvReq*, PoolEntry*>> members;
+              members.swap(slot.batch->members);
+              for (auto& m : members) {
+                srv_release(s, m.first, m.second);
+                const DqError* de = dynamic_cast<const DqError*>(&e);
+                srv_finish(s, m.first, de ? de->code : DQ_ERR_CUDA, e.what(), nullptr);
+              }
+            }
+            progressed = true;
+            busy = true;
+            continue;
+          }
+          if (take.size() == 1) {  // alone, on the plan it took
+            try {
+              srv_dispatch(s, slot, take[0].first, take[0].second);
+            } catch (const std::exception& e) {
+              srv_release(s, take[0].first, take[0].second);
+              slot.req = nullptr;
+              slot.pe = nullptr;
+              const DqError* de = dynamic_cast<const DqError*>(&e);
+              srv_finish(s, take[0].first, de ? de->code : DQ_ERR_CUDA, e.what(), nullptr);
+            }
+            progressed = true;
+            busy = true;
+            continue;
+          }
+        }
         SrvReq* r = nullptr;
         {
           std::lock_guard<std::mutex> lk2(s->mu);
@@ -2157,7 +2613,9 @@ int dq_server_start(dq_ctx* ctx, const dq_server_config* cfg, dq_server** out) {
     if (cfg) s->cfg = *cfg;
     if (s->cfg.slots <= 0) s->cfg.slots = 8;
     if (s->cfg.slots > 64) s->cfg.slots = 64;
-    if (s->cfg.pool_per_query <= 0) s->cfg.pool_per_query = s->cfg.slots;  // no plan churn: freeing synchronises the device
+    // no plan churn (freeing synchronises the device); batches take several plans of a request
+    if (s->cfg.pool_per_query <= 0) s->cfg.pool_per_query = 2 * s->cfg.slots;
+    if (s->cfg.batch_max <= 0) s->cfg.batch_max = 16;
     if (s->cfg.memory_budget == 0) s->cfg.memory_budget = 150ull << 30;
     {
       std::lock_guard<std::mutex> lk(ctx->mu);
@@ -2304,6 +2762,8 @@ int dq_server_stats_get(dq_server* s, dq_server_stats* out) {
     out->mean_ms = sum / v.size();
   }
   out->span_ms = s->t_last > s->t_first ? s->t_last - s->t_first : 0;
+  out->batches = s->batches;
+  out->batched = s->batched;
   return DQ_OK;
 }
 

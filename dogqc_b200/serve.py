@@ -21,12 +21,15 @@ from dogqc_b200.engine import _take_result
 
 
 class Server(object):
-    def __init__(self, engine, slots=8, memory_budget=0, pool_per_query=2):
+    def __init__(self, engine, slots=4, memory_budget=0, pool_per_query=0, batch_max=0):
+        """``batch_max``: requests of one shape run as one launch (0: 16, 1:
+        every request alone); ``pool_per_query`` 0: twice ``slots``."""
         self.engine = engine
         cfg = L.dq_server_config()
         cfg.slots = slots
         cfg.memory_budget = int(memory_budget)
         cfg.pool_per_query = pool_per_query
+        cfg.batch_max = batch_max
         h = C.c_void_p()
         L.check(L.lib().dq_server_start(engine.ctx, C.byref(cfg), C.byref(h)), engine.ctx)
         self.handle = h
@@ -150,14 +153,16 @@ def replay(server, queries, schedule):
 
 
 def warm(server, queries, slots, rounds=2):
-    """Fills the server's plan pool: every query runs `slots` times at once,
-    `rounds` times (preparing a pooled plan and capturing its graph is the slow
-    first step of a query; a served stream then finds them ready)."""
-    # each query `slots` times in a row: with first-come admission that many
-    # copies of it run at once, so its pool holds a plan for every slot
+    """Prepares what a served stream needs before it is timed: every query's
+    plan pool (its first request prepares the whole pool and compiles the
+    batch kernels of its shape), then bursts of all queries at once, so the
+    slots' batch buffers have grown to the sizes the stream's batches take."""
     sched = [(0.0, qi) for qi in range(len(queries)) for _ in range(slots)]
     for _ in range(rounds):
         replay(server, queries, sched)
+    burst = [(0.0, qi) for _ in range(16 * slots) for qi in range(len(queries))]
+    for _ in range(rounds):
+        replay(server, queries, burst)
 
 
 def sequence(engine, queries, schedule, plans=None):

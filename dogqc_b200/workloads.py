@@ -244,7 +244,7 @@ def c3_patterns(seed=BASE_SEED + 3, nwords=4):
     return ["%" + w.decode() + "%" for w in words[:nwords]]
 
 
-def plan_c3(alg, scal, Type, Reduction, patterns=None, d1_cut=50, d3_cut=100):
+def plan_c3(alg, scal, Type, Reduction, patterns=None, d1_cut=50, d3_cut=100, numgroups=1_000_000):
     patterns = patterns or c3_patterns()
     s1 = alg.selection(scal.SmallerExpr(scal.AttrExpr("d1_attr"), scal.ConstExpr(str(d1_cut), Type.INT)),
                        alg.scan("dim1"))
@@ -273,7 +273,7 @@ def plan_c3(alg, scal, Type, Reduction, patterns=None, d1_cut=50, d3_cut=100):
            j3.opId: {"multimatch": False, "selectivity": 1.0},
            j2.opId: {"multimatch": False, "selectivity": sel_like},
            j1.opId: {"multimatch": False, "selectivity": sel_like * d1_cut / 100.0},
-           agg.opId: {"numgroups": 1_000_000}}
+           agg.opId: {"numgroups": numgroups}}
     return agg, cfg
 
 
@@ -282,9 +282,13 @@ PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3}
 
 
 def build(name, alg, scale=1.0, **kw):
-    """Build workload ``name``'s plan with this package's front end."""
+    """Build workload ``name``'s plan with this package's front end.  The
+    cardinality hints follow ``scale`` (c3's group count: one million at full
+    size), as an optimizer's estimate from the tables would."""
     import dogqc_b200.scalar as scal
     from dogqc_b200.relational import Reduction
+    if name == "c3" and "numgroups" not in kw:
+        kw["numgroups"] = max(1024, int(round(1_000_000 * scale)))
     return PLANS[name](alg, scal, Type, Reduction, **kw)
 
 

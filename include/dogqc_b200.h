@@ -316,14 +316,19 @@ void dq_batch_free(dq_batch* batch);
  * the plans already held (idle pooled plans are freed to make room; a request
  * larger than the whole budget fails with DQ_ERR_ADMISSION), and enqueues it
  * without waiting, so that requests arriving while others run are admitted as
- * slots and memory free up and their kernels overlap on the device.  No
+ * slots and memory free up and their kernels overlap on the device.
+ * Continuous batching: when a slot frees up, waiting requests of the oldest
+ * request's shape (the same pipelines and ops, any tables and sizes) that have
+ * an idle pooled plan run together as one many-instance launch on that slot,
+ * each on its own plan and tables (the batch kernels of dq_batch_*).  No
  * counterpart in the reference, which runs one query per process.          */
 typedef struct dq_server dq_server;
 typedef struct {
-    int32_t slots;                   /* requests in flight (streams); 0: 8      */
-    int32_t pool_per_query;          /* idle plans kept per request; 0: slots  */
+    int32_t slots;                   /* batches in flight (streams); 0: 8       */
+    int32_t pool_per_query;          /* plans kept per request; 0: twice slots  */
     uint64_t memory_budget;          /* bytes; 0: 150 GB                         */
-    int32_t reserved[4];
+    int32_t batch_max;               /* requests per launch; 0: 16, 1: alone    */
+    int32_t reserved[3];
 } dq_server_config;
 typedef struct {
     double queue_ms;                 /* submitted -> dispatched to a stream      */
@@ -338,6 +343,8 @@ typedef struct {
     uint64_t memory_in_use, memory_peak;   /* bytes of pooled plans              */
     double p50_ms, p99_ms, mean_ms;        /* total latency of completed requests */
     double span_ms;                        /* first submit -> last completion    */
+    uint64_t batches;                      /* launches that ran several requests */
+    uint64_t batched;                      /* requests that ran in them          */
 } dq_server_stats;
 int dq_server_start(dq_ctx* ctx, const dq_server_config* cfg, dq_server** out);
 /* Copies the IR; the tables it names must stay registered until the request

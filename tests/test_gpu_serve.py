@@ -98,3 +98,26 @@ def test_tight_budget_evicts_and_completes(engine, queries):
         assert srv.stats()["memory_peak"] <= budget
     finally:
         srv.stop()
+
+
+@pytest.mark.parametrize("batch_max", [8, 1])
+def test_continuous_batching_results(engine, queries, batch_max):
+    """Requests of one shape waiting together run as one many-instance launch
+    (batch_max > 1); every request's result still equals the oracle's."""
+    from dogqc_b200 import serve
+    want = [canonical_rows(run_plan(q.base_db, q.plan)[1]) for q in queries]
+    srv = serve.Server(engine, slots=2, batch_max=batch_max)
+    try:
+        serve.warm(srv, queries, 2, rounds=1)          # every request shape prepared
+        sched = serve.arrivals(96, None, queries, seed=13)
+        results, infos, wall, errors = serve.mixed_stream(srv, queries, sched)
+        assert not errors
+        for (at, qi), res in zip(sched, results):
+            assert canonical_rows(res.rows()) == want[qi]
+        st = srv.stats()
+        if batch_max > 1:
+            assert st["batches"] > 0 and st["batched"] >= 2 * st["batches"]
+        else:
+            assert st["batches"] == 0
+    finally:
+        srv.stop()
