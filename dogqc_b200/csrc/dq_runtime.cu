@@ -1717,6 +1717,7 @@ std::shared_ptr<DescCopy> copy_desc(const dq_plan_desc* in) {
 // Device bytes a request's plan will hold, from its IR (before preparing it).
 uint64_t estimate_bytes(dq_ctx* ctx, const dq_plan_desc& d) {
   uint64_t b = 4096;
+  std::vector<uint64_t> multi_rows(std::max(d.nres, 0), 0);
   for (int i = 0; i < d.nres; ++i) {
     const dq_resource& r = d.res[i];
     const uint64_t cap = (uint64_t)std::max<int64_t>(r.capacity, 16);
@@ -1725,7 +1726,12 @@ uint64_t estimate_bytes(dq_ctx* ctx, const dq_plan_desc& d) {
     uint64_t widths = 0;
     for (int j = 0; j < r.npay && j < DQ_MAX_PAY; ++j) widths += ctype_width(r.pay_ctype[j]);
     switch (r.kind) {
-      case DQ_RES_UNIQUE: b += (2 * cap + 1) * (1 + keyw + r.npay) * 8; break;
+      case DQ_RES_UNIQUE: {  // the sizing of setup_resource: 4x while that fits kL2TableBytes, else 2x
+        const uint64_t words = 1 + keyw + r.npay;
+        const uint64_t slots = cap * 4 * words * 8 <= kL2TableBytes ? 4 * cap : 2 * cap;
+        b += (slots + 4) * words * 8;
+        break;
+      }
       case DQ_RES_AGG: b += (cap + 1) * (1 + keyw + r.naggs) * 8; break;
       case DQ_RES_MULTI: {
         uint64_t rows = cap;
@@ -1738,9 +1744,36 @@ uint64_t estimate_bytes(dq_ctx* ctx, const dq_plan_desc& d) {
           }
         }
         b += cap * 8 + rows * widths + 256;
+        multi_rows[i] = rows;
         break;
       }
       case DQ_RES_OUTPUT: b += cap * widths + 256; break;
+    }
+  }
+  // deferred-expansion buffers of a pipeline that expands at level 0 (the
+  // sizing of setup_pipeline: items, their grouped copy, prefixes, group table)
+  for (int p = 0; p < d.npipes; ++p) {
+    const dq_pipeline& pp = d.pipes[p];
+    for (int k = 0; k < pp.nops; ++k) {
+      const dq_op& op = pp.ops[k];
+      if (op.kind != DQ_OP_EXPAND) continue;
+      std::vector<int> reads;
+      for (int j = k; j < pp.nops; ++j) slot_reads(pp, pp.ops[j], reads);
+      std::sort(reads.begin(), reads.end());
+      reads.erase(std::unique(reads.begin(), reads.end()), reads.end());
+      uint64_t stash = 0;
+      for (int sl : reads) stash += pp.slots[sl].level == 0 ? 1 : 0;
+      if (stash > (uint64_t)kMaxStash) break;
+      uint64_t rows = 1 << 20;
+      if (pp.table) {
+        auto it = ctx->tables.find(pp.table);
+        if (it != ctx->tables.end()) rows = std::min<uint64_t>(rows, std::max<int64_t>(it->second.nrows, 1));
+      }
+      const uint64_t built = op.res >= 0 && op.res < d.nres ? std::max<uint64_t>(multi_rows[op.res], 1) : rows;
+      const uint64_t gcap = std::max<uint64_t>(64, 2 * std::min<uint64_t>(rows, built / (kGroupThreshold + 1) + 1));
+      b += rows * (2 + stash) * 8 + rows * std::max<uint64_t>(stash, 1) * 8 + (std::max(rows, gcap) + 1) * 8 +
+           gcap * 24 + 4096;
+      break;
     }
   }
   return b;
@@ -1870,6 +1903,10 @@ struct SrvShape {                   // the batch kernels of one request shape
     int expand_op = -1;             // deferred expansion (heavy kernel)
   };
   std::vector<Stage> stages;
+  // the largest per-member needs seen: a slot's scratch is sized for a full
+  // batch of such members, so it grows while the shape's mix is first seen
+  // (growing frees device memory, which synchronises the device), not later
+  uint64_t member_out = 0, member_rows = 0, member_build = 0;
 };
 
 void grow(DevBuf& b, size_t n) {
@@ -2077,8 +2114,9 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
       m.first->info.bytes = m.second->bytes;
     }
   }
+  const uint64_t full = (uint64_t)std::max(s->cfg.batch_max, K);
   grow(B.status, 4);
-  grow(B.rows, (size_t)K * 8);
+  grow(B.rows, (size_t)full * 8);
   while (B.heavy.size() < sh->stages.size()) B.heavy.emplace_back(new HeavyBufs());
   std::vector<uint8_t> blob;
   struct StageArgs {
@@ -2104,13 +2142,24 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
       const int64_t rows = pi.dev.nrows_dev ? (int64_t)pl.res[pi.dev.source_res]->dev.cap : pi.dev.nrows;
       prefix[i + 1] = prefix[i] + (rows + span - 1) / span;
       rows_all += rows;
-      if (S.expand_op >= 0) build_rows += std::max<uint64_t>(pl.res[pi.desc.ops[S.expand_op].res]->pay_rows, 1);
+      if (S.expand_op >= 0) {
+        const uint64_t b = std::max<uint64_t>(pl.res[pi.desc.ops[S.expand_op].res]->pay_rows, 1);
+        build_rows += b;
+        sh->member_rows = std::max<uint64_t>(sh->member_rows, (uint64_t)std::max<int64_t>(rows, 1));
+        sh->member_build = std::max(sh->member_build, b);
+      }
     }
     if (S.expand_op >= 0) {
       const DevHeavy& proto = B.members[0].second->plan->pipes[p]->dev.heavy;
-      const uint32_t cap = (uint32_t)std::min<int64_t>(std::max<int64_t>(rows_all, 1), 1 << 20);
-      const uint64_t groups = std::min<uint64_t>(cap, build_rows / (proto.threshold + 1) + (uint64_t)K);
-      const uint32_t gcap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(64, 2 * groups), 0xfffffff0ull);
+      auto sizes = [&](uint64_t rows, uint64_t build, uint64_t k, uint32_t& cap, uint32_t& gcap) {
+        cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(rows, 1), 1 << 20);
+        const uint64_t groups = std::min<uint64_t>(cap, build / (proto.threshold + 1) + k);
+        gcap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(64, 2 * groups), 0xfffffff0ull);
+      };
+      uint32_t cap, gcap, cap_full, gcap_full;
+      sizes((uint64_t)rows_all, build_rows, (uint64_t)K, cap, gcap);
+      sizes(full * sh->member_rows, full * sh->member_build, full, cap_full, gcap_full);
+      B.heavy[p]->bind(proto, std::max(cap, cap_full), std::max(gcap, gcap_full));  // capacity for a full batch
       sa[p].heavy = B.heavy[p]->bind(proto, cap, gcap);
       for (int i = 0; i < K; ++i) {
         const uint64_t threshold = descs[i].heavy.threshold;
@@ -2140,7 +2189,6 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
       max_scan_blocks = std::max(max_scan_blocks, blocks);
     }
   }
-  grow(B.partials, std::max<uint64_t>(max_scan_blocks, 1) * 4);
   // resets and the result pack of every member
   std::vector<BatchReset> resets;
   std::vector<BatchPack> packs;
@@ -2170,6 +2218,7 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
       resets.push_back(op);
     }
     const ResRec& o = *pl.res[pl.result_res];
+    const uint64_t off0 = off;
     for (int j = 0; j < o.desc.npay; ++j) {
       BatchPack pk{};
       pk.src = o.dev.pay[j];
@@ -2182,13 +2231,17 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
       off += align_up(o.dev.cap * (uint64_t)pk.width, 16);
       packs.push_back(pk);
     }
+    sh->member_out = std::max(sh->member_out, off - off0);
   }
   const size_t resets_off = blob_put(blob, resets.data(), resets.size() * sizeof(BatchReset));
   const size_t packs_off = blob_put(blob, packs.data(), packs.size() * sizeof(BatchPack));
   B.packed_bytes = std::max<uint64_t>(off, 16);
-  grow(B.packed, B.packed_bytes);
-  const size_t out_need = B.packed_bytes + (size_t)K * 8 + 16;
-  if (B.host_out_cap < out_need) {
+  const uint64_t packed_full = std::max<uint64_t>(B.packed_bytes, full * sh->member_out);
+  const size_t blob_full = std::max<size_t>(blob.size(), (size_t)(blob.size() * full / (uint64_t)K) + 4096);
+  grow(B.packed, packed_full);
+  grow(B.partials, std::max<uint64_t>(max_scan_blocks, 1) * 4 * full / (uint64_t)K);
+  const size_t out_need = packed_full + (size_t)full * 8 + 16;
+  if (B.host_out_cap < B.packed_bytes + (size_t)K * 8 + 16) {
     if (B.host_out) cudaFreeHost(B.host_out);
     B.host_out = nullptr;
     B.host_out_cap = out_need + out_need / 2;
@@ -2197,10 +2250,10 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
   if (B.host_params_cap < blob.size()) {
     if (B.host_params) cudaFreeHost(B.host_params);
     B.host_params = nullptr;
-    B.host_params_cap = blob.size() + blob.size() / 2;
+    B.host_params_cap = blob_full + blob_full / 2;
     DQ_CUDA(cudaMallocHost((void**)&B.host_params, B.host_params_cap));
   }
-  grow(B.params, blob.size());
+  grow(B.params, blob_full);
   memcpy(B.host_params, blob.data(), blob.size());
   uint8_t* dev = B.params.as<uint8_t>();
   int launches = 0;
@@ -2340,7 +2393,9 @@ PoolEntry* srv_acquire(dq_server* s, SrvReq* r) {
   // a full pool waits for one of its plans (preparing more on the loop stalls
   // every slot, and the surplus would be freed later with a device sync)
   if (!v.empty() && v.size() >= (size_t)std::max(s->cfg.pool_per_query, 1)) return nullptr;
-  if (!srv_make_room(s, r->est, r->desc->key)) {
+  // the bytes of a plan of this request when one exists, else the estimate
+  const uint64_t need = v.empty() ? r->est : std::max(r->est, v.front()->bytes);
+  if (!srv_make_room(s, need, r->desc->key)) {
     bool any_busy = false;
     for (auto& kv : s->pool)
       for (auto& e : kv.second) any_busy |= e->busy;
@@ -2364,7 +2419,7 @@ PoolEntry* srv_acquire(dq_server* s, SrvReq* r) {
   // for preparing one: concurrent copies of it later find a prepared plan
   // instead of stalling the loop to prepare and capture one
   const size_t want = (size_t)std::max(s->cfg.pool_per_query, 1);
-  while (v.size() < want && s->mem + r->est <= s->cfg.memory_budget) {  // never evicts for this
+  while (v.size() < want && s->mem + std::max(r->est, got->bytes) <= s->cfg.memory_budget) {  // never evicts
     PoolEntry* extra = prepare();
     srv_build_graph(extra, s->prep);
   }
