@@ -503,6 +503,22 @@ def run_served(args, world, rank, local):
                       "p99_ms": serve.percentile(t, .99)})
     st = srv.stats()
     srv.stop()
+    # the same Poisson streams one request at a time: one slot, no batching
+    srv1 = serve.Server(engine, slots=1, batch_max=1)
+    serve.warm(srv1, qs, 1, rounds=1)
+    alone = []
+    for rate in (1000, 2500, 5000, 7500, 10000):
+        sch = serve.arrivals(min(8000, max(300, rate // 4)), rate, qs, seed=9)
+        inf, w = serve.replay(srv1, qs, sch)
+        t = [i["total_ms"] for i in inf]
+        alone.append({"offered_qps": rate, "achieved_qps": len(sch) / w, "p50_ms": serve.percentile(t, .5),
+                      "p99_ms": serve.percentile(t, .99)})
+    srv1.stop()
+
+    def best_rate(points, p99_ms=1.0):  # highest offered rate kept up with at p99 <= p99_ms
+        ok = [p["offered_qps"] for p in points
+              if p["p99_ms"] <= p99_ms and p["achieved_qps"] >= 0.95 * p["offered_qps"]]
+        return max(ok) if ok else 0
     for p in plans.values():
         p.free()
     engine.close()
@@ -518,7 +534,9 @@ def run_served(args, world, rank, local):
         "batches": {"launches": st["batches"], "requests": st["batched"]},
         "p50_ms": serve.percentile(tot, .5), "p99_ms": serve.percentile(tot, .99),
         "one_at_a_time": one, "speedup_vs_one_at_a_time": value / one["queries_per_s"],
-        "poisson": rates, "memory_peak_bytes": st["memory_peak"],
+        "poisson": rates, "poisson_one_at_a_time": alone,
+        "max_rate_at_p99_1ms": {"served": best_rate(rates), "one_at_a_time": best_rate(alone)},
+        "memory_peak_bytes": st["memory_peak"],
         "clocks": clocks.summary(),
     }
 
