@@ -395,10 +395,23 @@ __device__ __forceinline__ uint64_t s_cas64(uint32_t a, uint64_t cmp, uint64_t v
   return old;
 }
 
+// A 64-bit shared-memory sum kept as two 32-bit words: a 32-bit atomic add of
+// the low word returns the old word, whose wrap-around carries into the high
+// word together with the value's high part (exact mod 2^64 once all adds are
+// done).  64-bit shared-memory atomics run at about a third of the 32-bit rate
+// on sm_100a, and most summed values have a zero high word.
+__device__ __forceinline__ void s_add64(uint32_t a, uint64_t v) {
+  const uint32_t lo = (uint32_t)v;
+  uint32_t old;
+  asm volatile("atom.shared.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(a), "r"(lo) : "memory");
+  const uint32_t hi = (uint32_t)(v >> 32) + (old + lo < old ? 1u : 0u);
+  if (hi) asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(a + 4), "r"(hi) : "memory");
+}
+
 __device__ __forceinline__ void s_merge(uint32_t a, int red, uint64_t v) {
   switch (red) {
     case DQ_RED_SUM:
-    case DQ_RED_COUNT: asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); break;
+    case DQ_RED_COUNT: s_add64(a, v); break;
     case DQ_RED_MIN: asm volatile("red.shared.min.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); break;
     case DQ_RED_MAX: asm volatile("red.shared.max.u64 [%0], %1;" ::"r"(a), "l"(v) : "memory"); break;
   }
