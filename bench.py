@@ -491,8 +491,11 @@ def run_served(args, world, rank, local):
     one = {"queries_per_s": n / wall1, "p50_ms": serve.percentile(per, .5), "p99_ms": serve.percentile(per, .99)}
     srv = serve.Server(engine, slots=args.slots, batch_max=args.batch_max)
     serve.warm(srv, qs, args.slots)
+    runs = []
     with ClockSampler(local) as clocks:
-        infos, wall = serve.replay(srv, qs, sched)
+        for _ in range(3):  # closed-loop bursts; the median one is reported
+            runs.append(serve.replay(srv, qs, sched))
+    infos, wall = sorted(runs, key=lambda r: r[1])[1]
     tot = [i["total_ms"] for i in infos]
     rates = []
     for rate in (100, 1000, 5000, 10000, 20000, 40000):

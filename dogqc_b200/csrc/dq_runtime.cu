@@ -1097,8 +1097,8 @@ void setup_batch_heavy(dq_batch* b, size_t p, BatchStage& S) {
   H.grouped = 1;
   H.cap = (uint32_t)std::min<int64_t>(std::max<int64_t>(rows, 1),
                                       std::max<int64_t>(1 << 20, (int64_t)b->heavy_cap));
-  const uint64_t groups =
-      std::min<uint64_t>(H.cap, build_rows / (H.threshold + 1) + (uint64_t)b->ninst);
+  const uint64_t groups = std::min<uint64_t>(
+      H.cap, build_rows / (std::max<uint64_t>(H.threshold, kBatchGroupThreshold) + 1) + (uint64_t)b->ninst);
   H.gcap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(64, 2 * groups), 0xfffffff0ull);
   S.h_items.alloc((size_t)H.cap * H.words * 8);
   S.h_count.alloc(8);
@@ -1153,7 +1153,7 @@ void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
       descs[i] = pl.pipes[p]->dev;
       descs[i].status = b->status.as<int32_t>();
       if (p0.expand_op >= 0) {
-        const uint64_t threshold = descs[i].heavy.threshold;
+        const uint64_t threshold = std::max<uint64_t>(descs[i].heavy.threshold, kBatchGroupThreshold);
         descs[i].heavy = S.heavy;
         descs[i].heavy.threshold = threshold;
         descs[i].tile_counter = S.h_units.as<uint32_t>();
@@ -2153,7 +2153,8 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
       const DevHeavy& proto = B.members[0].second->plan->pipes[p]->dev.heavy;
       auto sizes = [&](uint64_t rows, uint64_t build, uint64_t k, uint32_t& cap, uint32_t& gcap) {
         cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(rows, 1), 1 << 20);
-        const uint64_t groups = std::min<uint64_t>(cap, build / (proto.threshold + 1) + k);
+        const uint64_t groups =
+            std::min<uint64_t>(cap, build / (std::max<uint64_t>(proto.threshold, kBatchGroupThreshold) + 1) + k);
         gcap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(64, 2 * groups), 0xfffffff0ull);
       };
       uint32_t cap, gcap, cap_full, gcap_full;
@@ -2162,7 +2163,7 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
       B.heavy[p]->bind(proto, std::max(cap, cap_full), std::max(gcap, gcap_full));  // capacity for a full batch
       sa[p].heavy = B.heavy[p]->bind(proto, cap, gcap);
       for (int i = 0; i < K; ++i) {
-        const uint64_t threshold = descs[i].heavy.threshold;
+        const uint64_t threshold = std::max<uint64_t>(descs[i].heavy.threshold, kBatchGroupThreshold);
         descs[i].heavy = sa[p].heavy;
         descs[i].heavy.threshold = threshold;
         descs[i].tile_counter = B.heavy[p]->units.as<uint32_t>();
