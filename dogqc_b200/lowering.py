@@ -52,6 +52,8 @@ class _Op(dict):
 # A filter or probe whose estimated pass fraction is at most this refills the
 # lanes of the generated kernel before the rest of the pipeline.
 REFILL_SELECTIVITY = 0.5
+L2_TABLE_BYTES = 48 << 20   # join tables the runtime gives 4x slots (they stay in L2)
+NARROW = ("i8", "i32", "u32")
 
 
 def refill_point(ops):
@@ -660,7 +662,43 @@ class Lowering(object):
             self.result_types = [CT[t] for t in types]
 
     def finish(self, pipe):
+        self.reorder_probes(pipe)
         self.pipes.append(pipe)
+
+    def probe_cost(self, op):
+        """Relative cost of one probe of a join table: 1 for a table that stays
+        L2-resident (the runtime's 4x slots fit L2_TABLE_BYTES), 2 otherwise."""
+        r = self.res[op["res"]]
+        packed = r.nkeys <= 1 or (r.nkeys == 2 and all(t in NARROW for t in r.key_ctype))
+        words = 1 + len(r.pay_ctype) + (0 if packed else r.nkeys)
+        return 1.0 if r.capacity * 4 * words * 8 <= L2_TABLE_BYTES else 2.0
+
+    def reorder_probes(self, pipe):
+        """Consecutive unique-key probes whose keys none of them produces are
+        independent filters (inner, semi or anti; results do not depend on
+        their order): ordered by cost / (1 - estimated pass rate), the cheap,
+        selective ones first, so later probes see fewer rows.  The reference
+        probes in plan order."""
+        ops = pipe.ops
+        i = 0
+        while i < len(ops):
+            if ops[i]["kind"] != L.OP_PROBE:
+                i += 1
+                continue
+            j = i
+            while j < len(ops) and ops[j]["kind"] == L.OP_PROBE:
+                j += 1
+            run = ops[i:j]
+            if len(run) > 1:
+                written = set()
+                for o in run:
+                    written.update(pipe.lists[o["list2"]:o["list2"] + o["nlist2"]])
+                if all(not set(pipe.lists[o["list"]:o["list"] + o["nlist"]]) & written for o in run):
+                    def rank(o):
+                        sel = getattr(o, "sel", 1.0)
+                        return self.probe_cost(o) / (1.0 - sel) if sel < 1.0 else float("inf")
+                    ops[i:j] = sorted(run, key=rank)
+            i = j
 
     # -- IR ----------------------------------------------------------------------
     def ir(self):
