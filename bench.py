@@ -59,6 +59,10 @@ WORKLOADS = {
            {"workload": "star_join_high_cardinality", "fact_rows": 60_000_000,
             "dim_rows": [1_500_000, 200_000, 10_000], "groups": "~1,000,000",
             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c5": ("rows/s (left outer join on a multimap + two aggregations, input rows of both tables per second)",
+           {"workload": "outer_join_two_aggregations", "customer_rows": 150_000, "order_rows": 1_500_000,
+            "orders_filter": "flag >= 2 (98%)", "customers_without_orders": "1/3",
+            "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
 }
 
 

@@ -95,7 +95,8 @@ struct DevHeavy {         // deferred wide expansion ranges
 
 constexpr int kGroupRows = 32;    // range rows per grouped work unit (a warp)
 constexpr int kGroupItems = 64;   // items per grouped work unit
-constexpr int kGroupThreshold = 8;     // grouped mode: ranges longer than this are deferred
+constexpr int kGroupThreshold = 128;   // grouped mode: ranges longer than this are deferred
+constexpr int kGroupThresholdLow = 8;  // ... once a run showed several probe rows per range
 constexpr int kBatchGroupThreshold = 128;  // the same in batches (their item buffers do not grow)
 
 constexpr int kHotSlots = 512;         // CTA-local hot multimap buckets (generated kernels)

@@ -180,6 +180,11 @@ struct PipeRec {
   jit::Kernels kernels;
   int expand_op = -1;       // level-0 expansion op with deferral
   uint64_t heavy_cap = 0;   // deferred-item capacity grown after an overflow (0: default)
+  uint64_t heavy_threshold = 0;       // adapted deferral threshold (0: the default)
+  uint32_t* heavy_stats = nullptr;    // pinned: items and groups of the last run
+  ~PipeRec() {
+    if (heavy_stats) cudaFreeHost(heavy_stats);
+  }
   DevBuf pattern_buf, heavy_items, heavy_count, heavy_prefix;
   DevBuf heavy_gkey, heavy_glen, heavy_gcnt, heavy_glist, heavy_gstart, heavy_sorted;  // grouped deferral
   bool mm_count = false;    // sink is a multimap count: bucket scan follows
@@ -667,8 +672,11 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     // pay off there: a range is gathered once per 32-row chunk for all probe
     // rows that matched it
     H.grouped = plan->opts.batch_member || !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) ? 1 : 0;
-    const uint64_t dflt = H.grouped ? (uint64_t)kGroupThreshold : (uint64_t)tile * 8;
+    const uint64_t dflt = H.grouped ? (p.heavy_threshold ? p.heavy_threshold : (uint64_t)kGroupThreshold)
+                                    : (uint64_t)tile * 8;
     H.threshold = ctx->cfg.defer_threshold > 0 ? (uint64_t)ctx->cfg.defer_threshold : dflt;
+    if (H.grouped && !p.heavy_stats && !ctx->offline && !plan->opts.batch_member)
+      DQ_CUDA(cudaMallocHost((void**)&p.heavy_stats, 8));
     if (plan->opts.batch_member) break;  // the batch holds the buffers, shared by its instances
     p.heavy_items.alloc((size_t)H.cap * H.words * 8);
     p.heavy_count.alloc(8);  // item count, group count
@@ -857,6 +865,7 @@ int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status) {
       if (p.jit) DQ_CUDA(launch_generated(p.kernels.heavy, H, p.grid_full, p.prog.block, p.prog.smem_bytes, st));
       else DQ_CUDA(launch_pipeline(H, p.grid_full, st));
       launches += 2;
+      if (p.heavy_stats) DQ_CUDA(cudaMemcpyAsync(p.heavy_stats, p.heavy_count.ptr, 8, cudaMemcpyDeviceToHost, st));
     }
     if (p.mm_count) {
       ResRec& r = *plan->res[p.mm_res];
@@ -1042,6 +1051,26 @@ bool grow_heavy(dq_plan* plan) {
   }
   if (moved) refresh_pipelines(plan);
   return moved;
+}
+
+// Deferral pays when several probe rows match the same range (its chunks are
+// gathered once for all of them); with one probe row per range it only adds
+// passes.  After a completed run: items per group of 4 or more lower a plan's
+// threshold to kGroupThresholdLow for the runs that follow, fewer than 2 raise
+// it back (the runs' results do not depend on it).
+void adapt_threshold(dq_plan* plan) {
+  if (plan->ctx->cfg.defer_threshold > 0) return;
+  for (auto& pp : plan->pipes) {
+    PipeRec& p = *pp;
+    if (p.expand_op < 0 || !p.heavy_stats || !p.dev.heavy.grouped) continue;
+    const uint64_t items = std::min<uint64_t>(p.heavy_stats[0], p.dev.heavy.cap), groups = p.heavy_stats[1];
+    if (groups == 0) continue;
+    uint64_t t = p.dev.heavy.threshold;
+    if (items >= 4 * groups) t = kGroupThresholdLow;
+    else if (items < 2 * groups) t = kGroupThreshold;
+    p.heavy_threshold = t;
+    p.dev.heavy.threshold = t;
+  }
 }
 
 void throw_status(int status) {
@@ -1448,7 +1477,10 @@ int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out) {
         if (status & kInfoHeavyFull) grow_heavy(plan);
         status &= ~kInfoMask;
       }
-      if (status == 0) break;
+      if (status == 0) {
+        adapt_threshold(plan);
+        break;
+      }
       if (attempt >= 8 || (status & (kErrTimeout | kErrBadOp)))
         throw DqError(status & kErrTimeout ? DQ_ERR_TIMEOUT
                       : status & kErrHtFull ? DQ_ERR_HT_FULL

@@ -481,7 +481,14 @@ class Lowering(object):
             return
         jt = _tname(node.joinType)
         if jt == "OUTER":
-            raise Unsupported("outer joins are not executed by this backend")
+            # The reference's outer join runs on its multimatch table only and
+            # yields the inner join's rows: an unmatched probe row's extra
+            # iteration repeats the key check on a foreign payload row and drops
+            # it (hashJoins.py:473-530, include/hashing.cuh:189-199); its unique
+            # table rejects the join type (hashJoins.py:95-109).
+            if not getattr(node, "multimatch", True):
+                raise Unsupported("outer joins on unique keys (the reference's unique hash table rejects them)")
+            jt = "INNER"
         if node.conditions is not None:
             raise Unsupported("equi-joins with extra non-equality conditions")
         bk = list(node.buildKeyAttributes.values())

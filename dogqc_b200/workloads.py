@@ -277,8 +277,44 @@ def plan_c3(alg, scal, Type, Reduction, patterns=None, d1_cut=50, d3_cut=100, nu
     return agg, cfg
 
 
-GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3}
-PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3}
+# ---------------------------------------------------------------- c5 ----------
+
+def gen_c5(scale=1.0, seed=BASE_SEED + 5):
+    """Customers and their orders (TPC-H Q13 shape): customer keys a
+    permutation of 1..n; every order belongs to a customer whose key is not a
+    multiple of 3, so a third of the customers have no orders."""
+    nc = _n(150_000, scale, 16)
+    no = _n(1_500_000, scale, 16)
+    r = _rng(seed)
+    cust = {"c_custkey": (r.permutation(nc) + 1).astype(np.int32),
+            "c_nation": r.integers(0, 25, nc, dtype=np.int32)}
+    with_orders = np.arange(1, nc + 1, dtype=np.int32)
+    with_orders = with_orders[with_orders % 3 != 0]
+    orders = {"o_orderkey": (r.permutation(no) + 1).astype(np.int32),
+              "o_custkey": with_orders[r.integers(0, len(with_orders), no)],
+              "o_flag": r.integers(0, 100, no, dtype=np.int32)}
+    return Database([Table("customer", cust, {"c_custkey": Type.INT, "c_nation": Type.INT}),
+                     Table("orders", orders, {"o_orderkey": Type.INT, "o_custkey": Type.INT, "o_flag": Type.INT})])
+
+
+def plan_c5(alg, scal, Type, Reduction, flag_cut=2, numgroups=150_000):
+    """Customers left outer join their (filtered) orders, the number of orders
+    per customer (COUNT of a build attribute: null rows count 0), then the
+    number of customers per order count (Q13's two aggregations)."""
+    ords = alg.selection(scal.LargerEqualExpr(scal.AttrExpr("o_flag"), scal.ConstExpr(str(flag_cut), Type.INT)),
+                         alg.scan("orders"))
+    j = alg.outerjoin(("o_custkey", "c_custkey"), None, ords, alg.scan("customer"))
+    per_cust = alg.aggregation(["c_custkey"], [(Reduction.COUNT, "o_orderkey", "c_count")], j)
+    dist = alg.aggregation(["c_count"], [(Reduction.COUNT, "", "custdist")], per_cust)
+    cfg = {ords.opId: {"selectivity": (100 - flag_cut) / 100.0},
+           j.opId: {"multimatch": True},
+           per_cust.opId: {"numgroups": numgroups},
+           dist.opId: {"numgroups": 64}}
+    return dist, cfg
+
+
+GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5}
+PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5}
 
 
 def build(name, alg, scale=1.0, **kw):
@@ -289,6 +325,8 @@ def build(name, alg, scale=1.0, **kw):
     from dogqc_b200.relational import Reduction
     if name == "c3" and "numgroups" not in kw:
         kw["numgroups"] = max(1024, int(round(1_000_000 * scale)))
+    if name == "c5" and "numgroups" not in kw:
+        kw["numgroups"] = max(1024, int(round(150_000 * scale)))
     return PLANS[name](alg, scal, Type, Reduction, **kw)
 
 

@@ -447,6 +447,19 @@ class Oracle(object):
 
     def equijoin(self, node):
         jt = tname(node.joinType)
+        if jt == "OUTER":
+            # The reference runs an outer join only on its multimatch hash table
+            # (its unique table rejects the join type, hashJoins.py:95-109).
+            # After a probe row's matches, the generated loop gives an unmatched
+            # row one more iteration (hashJoins.py:524-530), but that iteration
+            # runs the key check again on the payload at the row's offset
+            # (hashJoins.py:505-510; hashProbeMulti leaves the offset at 0 or at
+            # the range end, include/hashing.cuh:189-199), which fails: unmatched
+            # rows are dropped, matched rows have no nulls.  The result is the
+            # inner join's.
+            if not getattr(node, "multimatch", True):
+                raise NotImplementedError("outer join on a unique hash table")
+            jt = "INNER"
         if jt not in ("INNER", "SEMI", "ANTI"):
             raise NotImplementedError("join type %s" % jt)
         bk = list(node.buildKeyAttributes.values())

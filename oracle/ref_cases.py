@@ -21,6 +21,9 @@ CASES = {
     "c0_empty": dict(workload="c0", scale=0.001, plan_kw=dict(cutoff=0)),
     "c1_nomatch": dict(workload="c1", scale=0.001, plan_kw=dict(segment=9)),
     "c2_nomatch": dict(workload="c2", scale=0.0005, gen_kw=dict(probe_lo=51)),
+    # left outer join (customers without orders count 0), two aggregations
+    "c5_s": dict(workload="c5", scale=0.01),
+    "c5": dict(workload="c5", scale=1.0),
     # full sizes: row counts, checksums and (small) full results are committed
     "c0": dict(workload="c0", scale=1.0),
     "c1": dict(workload="c1", scale=1.0),

@@ -11,8 +11,8 @@ from canonical import canonical_checksum, canonical_rows
 from evaluator import run_plan
 from helpers import golden, golden_cases, make_case
 
-SMALL = [c for c in golden_cases() if golden(c)["spec"]["scale"] < 0.01]
-FULL_FAST = ["c0", "c1"]
+SMALL = [c for c in golden_cases() if golden(c)["spec"]["scale"] < 0.1]
+FULL_FAST = ["c0", "c1", "c5"]
 
 
 @pytest.mark.parametrize("case", SMALL)
