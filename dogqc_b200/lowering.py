@@ -249,9 +249,34 @@ class Lowering(object):
         elif k == "EquiJoin":
             self.produce_join(node)
         elif k == "CrossJoin":
-            raise Unsupported("cross joins (nested loops) are not executed by this backend")
+            self.produce_cross(node)
         else:
             raise Unsupported("operator %s" % k)
+
+    def produce_cross(self, node):
+        """Nested-loop join (cudaTranslator.py:369-397: the inner side, the left
+        child, materialised; every outer row loops over all of it with the
+        condition as the filter).  Lowered as a multimap without keys: one
+        bucket holds every inner row, the outer rows' expansion walks it, the
+        condition filters the pairs.  Outer rows share the one range, so the
+        grouped deferral reads each chunk of the inner rows once for all."""
+        if self.joins.get(id(node), {}).get("built"):
+            self.produce(node.rightChild)
+            return
+        atts = list(node.leftChild.outRelation.values())
+        payload = [lang_type(a.dataType) for a in atts]
+        if any(t == "str" for t in payload):
+            raise Unsupported("string attributes in nested-loop join inputs")
+        if len(payload) > L.MAX_PAY:
+            raise Unsupported("more than %d payload attributes" % L.MAX_PAY)
+        rid = self.new_res(Res(L.RES_MULTI, nkeys=0, key_ctype=[], pay_ctype=payload, capacity=1))
+        info = dict(res=rid, unique=False, bk=[], pk=[], build_atts=atts, passes=["count", "scatter"], cross=True)
+        self.joins[id(node)] = info
+        for p in info["passes"]:
+            info["pass"] = p
+            self.produce(node.leftChild)
+        info["built"] = True
+        self.produce(node.rightChild)
 
     def consume(self, node, child, pipe):
         """Continue ``pipe`` (which delivers ``child``'s rows) at ``node``."""
@@ -271,6 +296,13 @@ class Lowering(object):
                 self.join_build_sink(node, pipe)
             else:
                 self.join_probe(node, pipe)
+                self.consume_parent(node, pipe)
+        elif k == "CrossJoin":
+            if child is node.leftChild:
+                self.join_build_sink(node, pipe)
+            else:
+                self.join_probe(node, pipe)
+                self.filter(pipe, node.condition, getattr(node, "selectivity", 1.0))
                 self.consume_parent(node, pipe)
         elif k == "Aggregation":
             self.aggregate(node, pipe)

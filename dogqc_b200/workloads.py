@@ -293,7 +293,8 @@ def gen_c5(scale=1.0, seed=BASE_SEED + 5):
     orders = {"o_orderkey": (r.permutation(no) + 1).astype(np.int32),
               "o_custkey": with_orders[r.integers(0, len(with_orders), no)],
               "o_flag": r.integers(0, 100, no, dtype=np.int32)}
-    return Database([Table("customer", cust, {"c_custkey": Type.INT, "c_nation": Type.INT}),
+    cust["c_acctbal"] = r.integers(0, 10_000, nc, dtype=np.int32)   # drawn last: earlier columns unchanged
+    return Database([Table("customer", cust, {"c_custkey": Type.INT, "c_nation": Type.INT, "c_acctbal": Type.INT}),
                      Table("orders", orders, {"o_orderkey": Type.INT, "o_custkey": Type.INT, "o_flag": Type.INT})])
 
 
@@ -313,8 +314,21 @@ def plan_c5(alg, scal, Type, Reduction, flag_cut=2, numgroups=150_000):
     return dist, cfg
 
 
-GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5}
-PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5}
+def plan_c7(alg, scal, Type, Reduction):
+    """Customers whose balance exceeds the average balance (TPC-H Q22 shape):
+    the one-row average, nested-loop joined to every customer with the
+    comparison as the join condition, then counts and sums per nation."""
+    avg = alg.aggregation([], [(Reduction.AVG, "c_acctbal", "avg_bal")], alg.scan("customer"))
+    cj = alg.crossjoin(scal.LargerExpr(scal.AttrExpr("c_acctbal"), scal.AttrExpr("avg_bal")), avg,
+                       alg.scan("customer"))
+    agg = alg.aggregation(["c_nation"], [(Reduction.COUNT, "", "numcust"), (Reduction.SUM, "c_acctbal", "totbal")],
+                          cj)
+    cfg = {cj.opId: {"selectivity": 0.5}, agg.opId: {"numgroups": 25}}
+    return agg, cfg
+
+
+GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5, "c7": gen_c5}
+PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5, "c7": plan_c7}
 
 
 def build(name, alg, scale=1.0, **kw):

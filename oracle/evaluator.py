@@ -526,6 +526,9 @@ class Oracle(object):
             yield probe.take(np.nonzero(keep)[0])
 
     def crossjoin(self, node):
+        """Nested-loop join: every (inner, outer) pair that satisfies the
+        condition; the inner side is the left child, materialised, the outer
+        side streams (cudaTranslator.py:369-397)."""
         left = self.collect(node.leftChild)
         for right in self.stream(node.rightChild):
             total = left.n * right.n

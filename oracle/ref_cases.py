@@ -24,6 +24,9 @@ CASES = {
     # left outer join (customers without orders count 0), two aggregations
     "c5_s": dict(workload="c5", scale=0.01),
     "c5": dict(workload="c5", scale=1.0),
+    # nested-loop join with a one-row aggregate (Q22 shape)
+    "c7_s": dict(workload="c7", scale=0.01),
+    "c7": dict(workload="c7", scale=1.0),
     # full sizes: row counts, checksums and (small) full results are committed
     "c0": dict(workload="c0", scale=1.0),
     "c1": dict(workload="c1", scale=1.0),
