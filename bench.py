@@ -63,6 +63,10 @@ WORKLOADS = {
            {"workload": "nested_loop_join_scalar_subquery", "customer_rows": 150_000,
             "condition": "acctbal > avg(acctbal)", "groups": 25,
             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c8": ("rows/s (temp table written by one plan root, scanned and joined by another, input rows per second)",
+           {"workload": "temp_table_two_roots", "customer_rows": 150_000, "order_rows": 1_500_000,
+            "orders_filter": "flag < 50 (50%)", "customers_filter": "nation < 5 (20%)",
+            "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
     "c5": ("rows/s (left outer join on a multimap + two aggregations, input rows of both tables per second)",
            {"workload": "outer_join_two_aggregations", "customer_rows": 150_000, "order_rows": 1_500_000,
             "orders_filter": "flag >= 2 (98%)", "customers_without_orders": "1/3",

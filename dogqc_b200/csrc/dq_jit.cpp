@@ -1781,13 +1781,49 @@ std::string source_excerpt(const std::string& src, const std::string& log) {
   return out;
 }
 
+// Whether a ptxas report shows register spills in any function.
+bool spills(const std::string& log) {
+  const std::string tag = " bytes spill stores";
+  for (size_t i = log.find(tag); i != std::string::npos; i = log.find(tag, i + 1)) {
+    size_t b = i;
+    while (b > 0 && log[b - 1] >= '0' && log[b - 1] <= '9') --b;
+    if (b < i && std::stoll(log.substr(b, i - b)) > 0) return true;
+  }
+  return false;
+}
+
+// The source with every `__launch_bounds__(N)` made `__launch_bounds__(N, 1)`.
+std::string one_block_bounds(const std::string& src) {
+  std::string out;
+  const std::string tag = "__launch_bounds__(";
+  size_t pos = 0;
+  for (size_t i = src.find(tag); i != std::string::npos; i = src.find(tag, pos)) {
+    const size_t close = src.find(')', i);
+    out += src.substr(pos, close - pos);
+    if (src.substr(i, close - i).find(',') == std::string::npos) out += ", 1";
+    pos = close;
+  }
+  return out + src.substr(pos);
+}
+
 void build(Entry& e, const std::string& src) {
   // the NVRTC the process resolved (an application may have loaded an older
   // one first): 256-bit loads for sm_100a need 12.9
   int major = 0, minor = 0;
   nvrtc().version(&major, &minor);
   const bool ld256 = major > 12 || (major == 12 && minor >= 9);
-  const bool ok = compile_once(src, ld256, e.log, e.cubin);
+  bool ok = compile_once(src, ld256, e.log, e.cubin);
+  // With a block size alone in the launch bounds, ptxas may aim at more
+  // resident blocks than the kernel's registers allow and spill; a minimum of
+  // one block lets it keep the values in registers.  Kept when spill-free.
+  if (ok && spills(e.log)) {
+    std::string log2;
+    std::vector<char> cubin2;
+    if (compile_once(one_block_bounds(src), ld256, log2, cubin2) && !spills(log2)) {
+      e.log = "launch bounds with a minimum of one block per SM (spill-free)\n" + log2;
+      e.cubin.swap(cubin2);
+    }
+  }
   e.log = "NVRTC " + std::to_string(major) + "." + std::to_string(minor) + "\n" + e.log;
   if (!ok) throw Error("generated pipeline kernel failed to compile:\n" + e.log + source_excerpt(src, e.log));
 }

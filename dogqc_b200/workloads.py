@@ -327,8 +327,30 @@ def plan_c7(alg, scal, Type, Reduction):
     return agg, cfg
 
 
-GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5, "c7": gen_c5}
-PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5, "c7": plan_c7}
+def plan_c8(alg, scal, Type, Reduction, flag_cut=50, nation_cut=5):
+    """Two plan roots over a temp table (TPC-H Q15 shape): the first
+    materialises orders per customer (the filtered orders grouped by
+    customer), the second scans it, joins the customers of some nations
+    (unique keys) and counts customers per order count."""
+    ords = alg.selection(scal.SmallerExpr(scal.AttrExpr("o_flag"), scal.ConstExpr(str(flag_cut), Type.INT)),
+                         alg.scan("orders"))
+    per = alg.aggregation(["o_custkey"], [(Reduction.COUNT, "", "n_orders")], ords)
+    tmp = alg.createtemp("cust_orders", per)
+    cust = alg.selection(scal.SmallerExpr(scal.AttrExpr("c_nation"), scal.ConstExpr(str(nation_cut), Type.INT)),
+                         alg.scan("customer"))
+    j = alg.join(("o_custkey", "c_custkey"), alg.scan("cust_orders"), cust)
+    dist = alg.aggregation(["n_orders"], [(Reduction.COUNT, "", "customers")], j)
+    cfg = {ords.opId: {"selectivity": flag_cut / 100.0},
+           per.opId: {"numgroups": 100_000},
+           cust.opId: {"selectivity": nation_cut / 25.0},
+           j.opId: {"multimatch": False},
+           dist.opId: {"numgroups": 64}}
+    return [tmp, dist], cfg
+
+
+GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5, "c7": gen_c5, "c8": gen_c5}
+PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5, "c7": plan_c7,
+         "c8": plan_c8}
 
 
 def build(name, alg, scale=1.0, **kw):

@@ -27,6 +27,9 @@ CASES = {
     # nested-loop join with a one-row aggregate (Q22 shape)
     "c7_s": dict(workload="c7", scale=0.01),
     "c7": dict(workload="c7", scale=1.0),
+    # two plan roots: a temp table written by the first, scanned by the second
+    "c8_s": dict(workload="c8", scale=0.01),
+    "c8": dict(workload="c8", scale=1.0),
     # full sizes: row counts, checksums and (small) full results are committed
     "c0": dict(workload="c0", scale=1.0),
     "c1": dict(workload="c1", scale=1.0),

@@ -1,9 +1,9 @@
 """CPU checks of the kernel generator: with DQ_CFG_OFFLINE a context needs no
 device, and preparing a plan generates and compiles (NVRTC, sm_100a) every
 pipeline's kernel.  Every workload shape compiles without register spills,
-under the default launch shape; the tunings the autotuner searches compile
-with at most a few spilled words (NVRTC 12.9's register allocation differs from
-nvcc's for some one-row-per-thread kernels)."""
+under the default launch shape and under the tunings the autotuner searches (a
+kernel that spills is recompiled with a minimum of one block per SM in its
+launch bounds)."""
 import re
 
 import pytest
@@ -44,10 +44,10 @@ def check_sources(plan, max_spill=0):
         assert spills and max(spills) <= max_spill, (i, spills)
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2", "c3", "c5", "c7"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "c3", "c5", "c7", "c8"])
 def test_every_workload_compiles_offline(engine, name):
     plan = engine.prepare(resolved(engine, name))
-    check_sources(plan, max_spill=32 if name == "c7" else 0)
+    check_sources(plan)
     with pytest.raises(L.DqError):
         plan.execute()
 
@@ -60,7 +60,7 @@ def test_every_workload_compiles_offline(engine, name):
 @pytest.mark.parametrize("name", ["c1", "c2"])
 def test_tuned_launch_shapes_compile(engine, name, tuning):
     plan = engine.prepare(resolved(engine, name), tuning=tuning)
-    check_sources(plan, max_spill=32)
+    check_sources(plan)
 
 
 @pytest.mark.parametrize("shape", ["c0", "c1", "c2", "c3"])
