@@ -495,6 +495,176 @@ def run_batched(args, world, rank, local):
     return out
 
 
+TBL_BLOCK = 100_000
+TBL_WORDS = [b"carefully", b"final", b"deposits", b"furiously", b"regular", b"accounts", b"blithely",
+             b"ironic", b"packages", b"quickly", b"express", b"pending", b"requests", b"slyly", b"bold"]
+def tbl_fields():
+    from dogqc_b200 import _lib as L
+    dec = lambda n: (n, L.TEXT_DECIMAL, 2)  # noqa: E731
+    return [("l_orderkey", L.TEXT_INT), ("l_partkey", L.TEXT_INT), ("l_suppkey", L.TEXT_INT),
+            ("l_linenumber", L.TEXT_INT), ("l_quantity", L.TEXT_INT), dec("l_extendedprice"), dec("l_discount"),
+            dec("l_tax"), ("l_returnflag", L.TEXT_CHAR), ("l_linestatus", L.TEXT_CHAR),
+            ("l_shipdate", L.TEXT_DATE), ("l_commitdate", L.TEXT_DATE), ("l_receiptdate", L.TEXT_DATE),
+            ("l_shipinstruct", L.TEXT_STRING), ("l_shipmode", L.TEXT_STRING), ("l_comment", L.TEXT_STRING)]
+
+
+def tbl_text(rows, seed=20261203):
+    """lineitem as dbgen writes it (16 fields, each followed by '|', the types of
+    the reference's schema, query/schema/tpch.py:22-41): a block of
+    100,000 seeded lines repeated to ``rows`` lines.  Returns the text and the
+    expected sums of l_orderkey and l_extendedprice (cents)."""
+    import numpy as np
+    r = np.random.Generator(np.random.Philox(seed))
+    n = min(rows, TBL_BLOCK)
+    ok = r.integers(1, 6_000_000, n)
+    pk = r.integers(1, 200_000, n)
+    sk = r.integers(1, 10_000, n)
+    ln = r.integers(1, 8, n)
+    qty = r.integers(1, 51, n)
+    price = r.integers(90_000, 10_500_001, n)
+    disc = r.integers(0, 11, n)
+    tax = r.integers(0, 9, n)
+    rf = r.integers(0, 3, n)
+    ls = r.integers(0, 2, n)
+    day = r.integers(0, 2526, n)
+    nw = r.integers(2, 8, n)
+    words = r.integers(0, len(TBL_WORDS), (n, 8))
+    instr = [b"DELIVER IN PERSON", b"COLLECT COD", b"NONE", b"TAKE BACK RETURN"]
+    modes = [b"TRUCK", b"MAIL", b"REG AIR", b"AIR", b"FOB", b"RAIL", b"SHIP"]
+    im = r.integers(0, 4, n)
+    mm = r.integers(0, 7, n)
+
+    def date(d):
+        y, rem = 1992 + d // 365, d % 365
+        return b"%04d-%02d-%02d" % (y, rem // 28 % 12 + 1, rem % 28 + 1)
+    lines = []
+    for i in range(n):
+        d = int(day[i])
+        lines.append(b"%d|%d|%d|%d|%d|%d.%02d|0.%02d|0.%02d|%c|%c|%s|%s|%s|%s|%s|%s|\n" % (
+            ok[i], pk[i], sk[i], ln[i], qty[i], price[i] // 100, price[i] % 100, disc[i], tax[i],
+            b"ANR"[rf[i]], b"FO"[ls[i]], date(d), date(d + 30), date(d + 60), instr[im[i]], modes[mm[i]],
+            b" ".join(TBL_WORDS[int(w)] for w in words[i, :nw[i]])))
+    block = b"".join(lines)
+    reps, rest = divmod(rows, n)
+    text = block * reps + b"".join(lines[:rest])
+    sum_ok = int(ok.sum()) * reps + int(ok[:rest].sum())
+    sum_price = int(price.sum()) * reps + int(price[:rest].sum())
+    return text, sum_ok, sum_price
+
+
+def tbl_algorithmic_bytes(nbytes, rows):
+    """Bytes the parse kernel must move: the text, the line ends (8 B a row), the
+    fixed-width columns (5 ints, 3 decimals of 8 B, 2 chars, 3 dates) and the
+    (first byte, length) record of each of the 3 strings (12 B)."""
+    return nbytes + rows * (8 + 5 * 4 + 3 * 8 + 2 * 1 + 3 * 4 + 3 * 12)
+
+
+TBL_REF_ROWS = 2_000_000
+
+
+def tbl_cpu_baseline(fields):
+    """The reference's own importer (generated C++, compiled here by
+    oracle/build_ref_importer.py into oracle/_ref) on the first 2,000,000 lines
+    of the benchmark text, timed on the host; without that program, the Python
+    restatement of it on the first 3 MB."""
+    import shutil
+    import tempfile
+    refbin = os.path.join(ROOT, "oracle", "_ref", "tbl_import_lineitem_%d" % TBL_REF_ROWS)
+    if os.path.exists(refbin):
+        sample = tbl_text(TBL_REF_ROWS)[0]
+        work = tempfile.mkdtemp(prefix="dq_tbl_ref_")
+        try:
+            os.makedirs(os.path.join(work, "csv"))
+            os.makedirs(os.path.join(work, "mmdb"))
+            with open(os.path.join(work, "csv", "lineitem.tbl"), "wb") as fh:
+                fh.write(sample)
+            t0 = time.perf_counter()
+            subprocess.run([refbin], cwd=work, check=True, stdout=subprocess.DEVNULL)
+            dt = time.perf_counter() - t0
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+        return {"value": len(sample) / dt / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
+                "sample": "the first %d lines (%d bytes) of the same text through the reference's generated "
+                          "importer (its CSV reader, both passes, column files written), wall time" % (
+                              TBL_REF_ROWS, len(sample)), "seconds": dt}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import text_import
+    text = tbl_text(30_000)[0]
+    t0 = time.perf_counter()
+    text_import.parse(text, [(f[0], f[1]) + tuple(f[2:]) for f in fields])
+    dt = time.perf_counter() - t0
+    return {"value": len(text) / dt / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+            "sample": "30,000 lines (%d bytes) through the Python restatement of the reference's importer" % len(text)}
+
+
+def run_import(args, world, rank, local):
+    """Text import: lineitem in dbgen's .tbl layout (6,000,000 lines at scale 1,
+    about 750 MB) parsed into 16 device columns.  ``value``: text bytes per
+    second of device time, the text already in HBM (a device tensor; the call's
+    device timeline from its first phase to its last, host waits included);
+    ``e2e``: the same from pinned host memory, host wall time of the whole call."""
+    import numpy as np
+    import torch
+    from dogqc_b200 import _lib as L
+    from dogqc_b200.engine import Engine
+    torch.cuda.set_device(local)
+    rows = int(6_000_000 * SCALE)
+    text, sum_ok, sum_price = tbl_text(rows)
+    nbytes = len(text)
+    host = torch.frombuffer(bytearray(text), dtype=torch.uint8).pin_memory()
+    dev = host.cuda()
+    fields = tbl_fields()
+    engine = Engine(local)
+    for _ in range(args.warmup):
+        engine.import_text("lineitem", dev, fields)
+    replicas.barrier(world)
+    spans, parse = [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            n = engine.import_text("lineitem", dev, fields)
+            t = engine.import_timing()
+            spans.append(t["span_ms"])
+            parse.append(t["parse_ms"])
+    t = engine.import_timing()
+    step_ms = replicas.max_over_ranks(float(np.mean(spans)), world)
+    ok = engine.read_column("lineitem", "l_orderkey", L.I32).astype(np.int64).sum()
+    price = engine.read_column("lineitem", "l_extendedprice", L.I64).sum()
+    parity = bool(n == rows and int(ok) == sum_ok and int(price) == sum_price)
+    e2e = []
+    for _ in range(max(2, args.steps // 2)):
+        engine.import_text("lineitem", host, fields)
+        e2e.append(engine.import_timing()["call_ms"])
+    e2e_ms = float(np.median(e2e))
+    peak, peak_kind = hbm_peak()
+    alg = tbl_algorithmic_bytes(nbytes, rows)
+    parse_ms = float(np.mean(parse))
+    achieved = alg / (parse_ms / 1e3) / 1e9
+    out = {
+        "metric": "GB/s of .tbl text parsed into device columns (lineitem layout, 16 fields)",
+        "value": nbytes * world / (step_ms / 1e3) / 1e9, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded, dbgen layout)",
+        "config": {"workload": "tbl_import_lineitem", "rows": rows, "text_bytes": nbytes,
+                   "fields": "5 INT, 3 DECIMAL(2), 2 CHAR, 3 DATE, 3 STRING (the reference's lineitem schema)",
+                   "l2": "text %.0f MB > L2 (inputs larger than L2)" % (nbytes / 1e6), "parallelism": "replicas"},
+        "rows_per_s": rows * world / (step_ms / 1e3),
+        "phases_ms": {k: t[k] for k in ("copy_ms", "newline_ms", "line_end_ms", "parse_ms", "string_ms")},
+        "parity": parity,
+        "e2e": {"value": nbytes / (e2e_ms / 1e3) / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": 8 * (2 + 16), "ms": e2e_ms,
+                "how": "dq_table_import_text from pinned host memory, host wall time of the call"},
+        "roofline": {"bound": "hbm", "kernel": "imp_parse_kernel", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "algorithmic_bytes": alg, "traffic": None},
+        "gpu_launches": int(t["kernel_launches"]) * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = tbl_cpu_baseline(fields)
+    engine.close()
+    return out
+
+
 def run_served(args, world, rank, local):
     """The served mixed stream: queries of the c0-c3 shapes over small resident
     tables, replayed through the request server (native submit/collect) closed
@@ -580,7 +750,7 @@ def main():
     ap.add_argument("--engine-flags", type=int, default=0, help="DQ_CFG_* bits")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="workload size factor (profiling only; the bench line is quoted at 1.0)")
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["c2x256", "c4"],
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["c2x256", "c4", "tbl"],
                     help="c1 (default): the FK-PK join the headline metric is quoted on; c0, c2, c3: "
                          "the other configurations, for the per-pipeline table; c2x256: the batched form; "
                          "c4: the served mixed stream")
@@ -600,6 +770,8 @@ def main():
         out = run_batched(args, world, rank, local)
     elif args.impl == "ours" and WORKLOAD == "c4":
         out = run_served(args, world, rank, local)
+    elif args.impl == "ours" and WORKLOAD == "tbl":
+        out = run_import(args, world, rank, local)
     elif args.impl == "reference" and WORKLOAD != "c1":
         out = {"impl": "reference", "unavailable": "the partitioned CPU reference arm covers the c1 workload; "
                                                    "the others report cpu_baseline in the ours line"}

@@ -54,6 +54,20 @@ class dq_column(C.Structure):
                 ("offsets", C.c_void_p), ("nchars", C.c_uint64)]
 
 
+TEXT_INT, TEXT_DATE, TEXT_CHAR, TEXT_DECIMAL, TEXT_STRING, TEXT_SKIP, TEXT_FLOAT = 1, 2, 3, 4, 5, 6, 7
+
+
+class dq_text_field(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("kind", C.c_int32), ("scale", C.c_int32)]
+
+
+class dq_import_timing(C.Structure):
+    _fields_ = [("copy_ms", C.c_double), ("newline_ms", C.c_double), ("line_end_ms", C.c_double),
+                ("parse_ms", C.c_double), ("string_ms", C.c_double), ("call_ms", C.c_double),
+                ("span_ms", C.c_double),
+                ("kernel_launches", C.c_int64), ("nbytes", C.c_uint64)]
+
+
 class dq_slot(C.Structure):
     _fields_ = [("kind", C.c_int8), ("level", C.c_int8), ("ctype", C.c_int8), ("pad", C.c_int8),
                 ("src", C.c_int16), ("res", C.c_int16)]
@@ -128,7 +142,8 @@ class dq_join_agg_args(C.Structure):
 def check_layout():
     """Sizes the C compiler gives these structs on x86-64 (LP64)."""
     expect = {dq_config: 40, dq_column: 40, dq_slot: 8, dq_op: 40, dq_resource: 80, dq_join_agg_args: 104,
-              dq_tuning: 32, dq_server_config: 32, dq_request_info: 40, dq_server_stats: 88}
+              dq_tuning: 32, dq_server_config: 32, dq_request_info: 40, dq_server_stats: 88,
+              dq_text_field: 16, dq_import_timing: 72}
     for t, n in expect.items():
         if C.sizeof(t) != n:
             raise AssertionError("%s is %d bytes, header implies %d" % (t.__name__, C.sizeof(t), n))
@@ -151,6 +166,11 @@ EXPORTS = {
     "dq_table_update": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int32, C.POINTER(dq_column), C.c_int64, C.c_void_p]),
     "dq_table_drop": (C.c_int, [C.c_void_p, C.c_char_p]),
     "dq_table_rows": (C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_int64)]),
+    "dq_table_import_text": (C.c_int, [C.c_void_p, C.c_char_p, C.c_void_p, C.c_uint64, C.c_char, C.c_int32,
+                                       C.POINTER(dq_text_field), C.POINTER(C.c_int64)]),
+    "dq_table_import_timing_get": (C.c_int, [C.c_void_p, C.POINTER(dq_import_timing)]),
+    "dq_table_column_read": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_void_p, C.c_uint64,
+                                       C.c_void_p, C.POINTER(C.c_uint64)]),
     "dq_plan_prepare": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_desc), C.POINTER(C.c_void_p)]),
     "dq_plan_execute": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dq_plan_free": (None, [C.c_void_p]),

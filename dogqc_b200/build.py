@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libdogqc_b200.so")
-SOURCES = ["dq_kernels.cu", "dq_runtime.cu", "dq_noalloc.cu", "dq_jit.cpp"]
+SOURCES = ["dq_kernels.cu", "dq_import.cu", "dq_runtime.cu", "dq_noalloc.cu", "dq_jit.cpp"]
 HEADERS = ["dq_device.h", "dq_common.cuh", "dq_jit.h", os.path.join("..", "..", "include", "dogqc_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # in-memory headers of generated kernels: (include name, file)

@@ -176,4 +176,44 @@ struct BatchPack {        // one output column of one instance
   int32_t pad;
 };
 
+// ------------------------------------------------------------ text import --
+constexpr int kImpTile = 16384;       // text bytes per CTA in the newline passes (64 a thread)
+constexpr int kImpRows = 256;         // rows per CTA in the parse and string passes
+constexpr int kImpMaxFields = 64;
+
+// Field kinds (dq_text_kind) and the reasons a row is rejected.
+enum : int32_t { kTxtInt = 1, kTxtDate = 2, kTxtChar = 3, kTxtDecimal = 4, kTxtString = 5, kTxtSkip = 6,
+                 kTxtFloat = 7 };
+enum : int32_t { kImpTooFew = 1, kImpTooMany = 2, kImpNoDigit = 3, kImpOverflow = 4, kImpNotChar = 5,
+                 kImpShortDate = 6, kImpExponent = 7 };
+
+struct ImpField {
+  int32_t kind;
+  int32_t scale;          // decimal digits kept after the point
+  void* out;              // fixed-width column (nrows values)
+  int32_t str;            // string ordinal (kTxtString)
+  int32_t pad;
+};
+
+struct ImpArgs {
+  const uint8_t* text;    // padded with zeros to a multiple of kImpTile
+  uint64_t nbytes;
+  uint64_t nlines;        // newlines in the text
+  uint64_t nrows;         // nlines, plus one for a last line without a newline
+  const uint64_t* line_end;
+  uint64_t* err;          // min over bad rows of row << 16 | field << 8 | reason
+  uint64_t* spos;         // [nstr][nrows] first byte of each string
+  uint32_t* slen;         // [nstr][nrows] its length
+  uint64_t* bsum;         // [nstr][nblocks + 1] string bytes per parse block
+  uint64_t* boff;         // the same, exclusive prefix sums (total last)
+  uint64_t nblocks;
+  int32_t nfields;
+  int32_t nstr;
+  uint32_t delim;
+  int32_t pad;
+  ImpField f[kImpMaxFields];
+  uint64_t* soff[kImpMaxFields];  // string offsets (nrows + 1), by string ordinal
+  uint8_t* sheap[kImpMaxFields];  // string heaps
+};
+
 }  // namespace dq

@@ -1,0 +1,532 @@
+// Text import kernels (sm_100a): a table in the reference's .tbl layout parsed
+// on the device.
+//
+// The reference loads text on the host with generated C++ (dogqc/dbio.py:
+// 117-253) around a CSV reader (dogqc/include/csv.h): one row per line, fields
+// split at the delimiter, spaces trimmed, integers and floats parsed digit by
+// digit, dates through the schema's toDate (query/schema/tpch.py:9-20), and a
+// second pass over the file to fill the string heaps.  Here the whole text sits
+// in HBM and four passes run over it:
+//
+//   1. count:   each CTA counts the newlines of a 16 KB tile (64 bytes a
+//               thread, four 16-byte loads, a SIMD byte compare per word);
+//   2. scan:    one CTA turns the tile counts into each tile's first line;
+//   3. lines:   each CTA writes the byte positions of its newlines in order
+//               (a block scan over the threads' counts places them);
+//   4. parse:   one thread per row walks its line in 16-byte chunks held in
+//               registers: delimiters are found with a byte-compare mask,
+//               numbers are parsed as they stream past, strings are recorded
+//               as (first byte, length);
+//   5. strings: a prefix sum of the lengths (per-CTA sums from the parse pass,
+//               then one CTA per column) gives the offsets, and each warp
+//               copies the bytes of its 32 rows, coalesced on both sides.
+//
+// Every pass is a read of the text at most once from HBM (the parse pass
+// reads each chunk through L1); the algorithmic traffic is the text, the line
+// ends, and the columns written.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dq_device.h"
+
+namespace dq {
+namespace {
+
+constexpr int kImpThreads = 256;
+constexpr int kImpPerThread = kImpTile / kImpThreads;  // 64 bytes: four 16-byte chunks
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 8;
+
+// Bytes of `w` equal to those of `pat` as a 4-bit mask (byte k -> bit k).  The
+// 0/1 byte flags sit at bits 0, 8, 16, 24; the multiply moves them to bits
+// 24..27 without overlapping partial products.
+__device__ __forceinline__ uint32_t eq_nibble(uint32_t w, uint32_t pat) {
+  const uint32_t t = __vcmpeq4(w, pat) & 0x01010101u;
+  return (t * 0x01020408u) >> 24;
+}
+
+__device__ __forceinline__ uint32_t eq_mask16(const uint4& v, uint32_t pat) {
+  return eq_nibble(v.x, pat) | (eq_nibble(v.y, pat) << 4) | (eq_nibble(v.z, pat) << 8) |
+         (eq_nibble(v.w, pat) << 12);
+}
+
+__device__ __forceinline__ uint4 ld_chunk(const uint8_t* p) {
+  return __ldg(reinterpret_cast<const uint4*>(p));
+}
+
+// Exclusive block scan of one value per thread (any power-of-two block up to
+// 1024); returns the total.
+template <int kBlock, class T>
+__device__ T block_scan(T x, T& excl) {
+  constexpr int kW = kBlock / 32;
+  __shared__ T s_w[kW + 1];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  T incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_w[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    T v = lane < kW ? s_w[lane] : T(0);
+    T vi = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T y = __shfl_up_sync(0xffffffffu, vi, o);
+      if (lane >= o) vi += y;
+    }
+    if (lane < kW) s_w[lane] = vi - v;
+    if (lane == kW - 1) s_w[kW] = vi;
+  }
+  __syncthreads();
+  excl = s_w[warp] + incl - x;
+  const T total = s_w[kW];
+  __syncthreads();
+  return total;
+}
+
+// ------------------------------------------------------------ newlines --
+
+__global__ void __launch_bounds__(kImpThreads) imp_count_kernel(const uint8_t* text, uint64_t* tile_cnt) {
+  const uint8_t* p = text + (uint64_t)blockIdx.x * kImpTile + threadIdx.x * kImpPerThread;
+  uint32_t n = 0;
+#pragma unroll
+  for (int k = 0; k < kImpPerThread / 16; ++k) n += __popc(eq_mask16(ld_chunk(p + 16 * k), 0x0a0a0a0au));
+  uint32_t excl;
+  const uint32_t total = block_scan<kImpThreads>(n, excl);
+  if (threadIdx.x == 0) tile_cnt[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kImpThreads) imp_lines_kernel(const uint8_t* text, const uint64_t* tile_off,
+                                                                uint64_t* line_end) {
+  const uint64_t first = (uint64_t)blockIdx.x * kImpTile + threadIdx.x * kImpPerThread;
+  uint32_t m[kImpPerThread / 16];
+  uint32_t n = 0;
+#pragma unroll
+  for (int k = 0; k < kImpPerThread / 16; ++k) {
+    m[k] = eq_mask16(ld_chunk(text + first + 16 * k), 0x0a0a0a0au);
+    n += __popc(m[k]);
+  }
+  uint32_t excl;
+  block_scan<kImpThreads>(n, excl);
+  uint64_t at = tile_off[blockIdx.x] + excl;
+#pragma unroll
+  for (int k = 0; k < kImpPerThread / 16; ++k) {
+    uint32_t b = m[k];
+    while (b) {
+      line_end[at++] = first + 16 * k + (__ffs(b) - 1);
+      b &= b - 1;
+    }
+  }
+}
+
+// One CTA per segment: out[i] = in[0] + ... + in[i - 1], out[n] = the total.
+__global__ void __launch_bounds__(kScanThreads) imp_scan_kernel(const uint64_t* in, uint64_t* out, uint64_t n,
+                                                                uint64_t stride) {
+  in += blockIdx.x * stride;
+  out += blockIdx.x * stride;
+  uint64_t carry = 0;
+  for (uint64_t base = 0; base < n; base += (uint64_t)kScanThreads * kScanItems) {
+    const uint64_t i0 = base + (uint64_t)threadIdx.x * kScanItems;
+    uint64_t v[kScanItems], s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      v[k] = i0 + k < n ? in[i0 + k] : 0;
+      s += v[k];
+    }
+    uint64_t excl;
+    const uint64_t total = block_scan<kScanThreads>(s, excl);
+    uint64_t run = carry + excl;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      if (i0 + k < n) out[i0 + k] = run;
+      run += v[k];
+    }
+    carry += total;
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
+// ---------------------------------------------------------------- parse --
+
+// A thread's view of its line: the 16-byte chunk last loaded, in registers.
+struct LineReader {
+  const uint8_t* text;
+  uint64_t base = ~0ull;
+  uint4 v;
+
+  __device__ __forceinline__ void fetch(uint64_t i) {
+    const uint64_t b = i & ~15ull;
+    if (b != base) {
+      v = ld_chunk(text + b);
+      base = b;
+    }
+  }
+  __device__ __forceinline__ uint32_t at(uint64_t i) {
+    fetch(i);
+    const uint32_t k = (uint32_t)i & 15u;
+    const uint32_t w = k < 8 ? (k < 4 ? v.x : v.y) : (k < 12 ? v.z : v.w);
+    return (w >> ((k & 3) * 8)) & 0xffu;
+  }
+  // First byte equal to the delimiter in [i, end); `end` if there is none.
+  __device__ __forceinline__ uint64_t find(uint64_t i, uint64_t end, uint32_t pat) {
+    while (i < end) {
+      fetch(i);
+      const uint32_t m = eq_mask16(v, pat) >> (i & 15);
+      if (m) {
+        const uint64_t q = i + (__ffs(m) - 1);
+        return q < end ? q : end;
+      }
+      i = base + 16;
+    }
+    return end;
+  }
+};
+
+// Field [i, q) of a line ending at `end`, with the spaces around it trimmed
+// to [cs, ce).  Returns a reason code, 0 when the delimiter was found.
+__device__ __forceinline__ int32_t field_bounds(LineReader& rd, uint64_t i, uint64_t end, uint32_t delim,
+                                                uint32_t pat, uint64_t& q, uint64_t& cs, uint64_t& ce) {
+  q = rd.find(i, end, pat);
+  if (q >= end) return kImpTooFew;
+  cs = i;
+  ce = q;
+  while (cs < ce && rd.at(cs) == ' ') ++cs;
+  while (ce > cs && rd.at(ce - 1) == ' ') --ce;
+  (void)delim;
+  return 0;
+}
+
+// csv.h parse_signed_integer for int, throw_on_overflow (csv.h:945-995), on
+// the trimmed field.
+__device__ int32_t parse_int(LineReader& rd, uint64_t& i, uint64_t end, uint32_t delim, int32_t& out) {
+  int state = 0;  // 0: before the value, 1: in it, 2: trailing spaces
+  bool neg = false;
+  int32_t x = 0;
+  for (;; ++i) {
+    if (i >= end) return kImpTooFew;
+    const uint32_t c = rd.at(i);
+    if (c == delim) break;
+    if (c == ' ') {
+      if (state == 1) state = 2;
+      continue;
+    }
+    if (state == 2) return kImpNoDigit;  // a space inside the value
+    if (state == 0) {
+      state = 1;
+      if (c == '-') {
+        neg = true;
+        continue;
+      }
+      if (c == '+') continue;
+    }
+    if (c < '0' || c > '9') return kImpNoDigit;
+    const int32_t y = (int32_t)c - '0';
+    if (neg) {
+      if (x < (INT32_MIN + y) / 10) return kImpOverflow;
+      x = 10 * x - y;
+    } else {
+      if (x > (INT32_MAX - y) / 10) return kImpOverflow;
+      x = 10 * x + y;
+    }
+  }
+  out = x;
+  return 0;
+}
+
+// Exact fixed point: [+-]digits[(.|,)digits] scaled by 10^scale, digits past
+// `scale` dropped (the grammar of csv.h parse_float without the exponent).
+__device__ int32_t parse_decimal(LineReader& rd, uint64_t& i, uint64_t end, uint32_t delim, int scale,
+                                 int64_t& out) {
+  int state = 0;  // 0: before, 1: integer digits, 3: fraction digits, 2: trailing spaces
+  bool neg = false;
+  uint64_t m = 0;
+  int fd = 0;
+  constexpr uint64_t kMax = (uint64_t)INT64_MAX;
+  for (;; ++i) {
+    if (i >= end) return kImpTooFew;
+    const uint32_t c = rd.at(i);
+    if (c == delim) break;
+    if (c == ' ') {
+      if (state != 0) state = 2;
+      continue;
+    }
+    if (state == 2) return kImpNoDigit;
+    if (state == 0) {
+      state = 1;
+      if (c == '-' || c == '+') {
+        neg = c == '-';
+        continue;
+      }
+    }
+    if ((c == '.' || c == ',') && state == 1) {
+      state = 3;
+      continue;
+    }
+    if (c == 'e' || c == 'E') return kImpExponent;
+    if (c < '0' || c > '9') return kImpNoDigit;
+    if (state == 3) {
+      if (fd >= scale) continue;
+      ++fd;
+    }
+    const uint64_t y = c - '0';
+    if (m > (kMax - y) / 10) return kImpOverflow;
+    m = 10 * m + y;
+  }
+  for (; fd < scale; ++fd) {
+    if (m > kMax / 10) return kImpOverflow;
+    m *= 10;
+  }
+  out = neg ? -(int64_t)m : (int64_t)m;
+  return 0;
+}
+
+// csv.h parse_float for float (csv.h:1008-1069), step for step: every product,
+// quotient and sum rounded to binary32 on its own (the reference's host code
+// is compiled without contraction), the sign applied last.  Exponents beyond
+// four digits are rejected (the reference saturates them and, for the most
+// negative one, does not terminate).
+__device__ int32_t parse_float(LineReader& rd, uint64_t& i, uint64_t end, uint32_t delim, uint32_t& out) {
+  int state = 0;  // 0: before, 1: integer digits, 3: fraction digits, 4: exponent, 2: trailing spaces
+  bool neg = false, eneg = false, esign = false;
+  float x = 0.f, pos = 1.f;
+  int e = 0;
+  for (;; ++i) {
+    if (i >= end) return kImpTooFew;
+    const uint32_t c = rd.at(i);
+    if (c == delim) break;
+    if (c == ' ') {
+      if (state != 0) state = 2;
+      continue;
+    }
+    if (state == 2) return kImpNoDigit;
+    if (state == 0) {
+      state = 1;
+      if (c == '-' || c == '+') {
+        neg = c == '-';
+        continue;
+      }
+    }
+    if (state == 4) {
+      if (!esign && e == 0 && (c == '-' || c == '+')) {  // the exponent's own sign, first
+        esign = true;
+        eneg = c == '-';
+        continue;
+      }
+      esign = true;
+      if (c < '0' || c > '9') return kImpNoDigit;
+      e = e * 10 + (int)(c - '0');
+      if (e > 9999) return kImpExponent;
+      continue;
+    }
+    if ((c == '.' || c == ',') && state == 1) {
+      state = 3;
+      continue;
+    }
+    if (c == 'e' || c == 'E') {
+      state = 4;
+      continue;
+    }
+    if (c < '0' || c > '9') return kImpNoDigit;
+    const float y = (float)(int)(c - '0');
+    if (state == 1) {
+      x = __fadd_rn(__fmul_rn(x, 10.f), y);
+    } else {
+      pos = __fdiv_rn(pos, 10.f);
+      x = __fadd_rn(x, __fmul_rn(y, pos));
+    }
+  }
+  if (eneg) e = -e;
+  if (e != 0) {
+    float b = e < 0 ? 0.1f : 10.f;
+    if (e < 0) e = -e;
+    while (e != 1) {
+      if ((e & 1) == 0) {
+        b = __fmul_rn(b, b);
+        e >>= 1;
+      } else {
+        x = __fmul_rn(x, b);
+        --e;
+      }
+    }
+    x = __fmul_rn(x, b);
+  }
+  if (neg) x = -x;
+  out = __float_as_uint(x);
+  return 0;
+}
+
+__global__ void __launch_bounds__(kImpRows) imp_parse_kernel(const ImpArgs A) {
+  const uint64_t r = (uint64_t)blockIdx.x * kImpRows + threadIdx.x;
+  const bool live = r < A.nrows;
+  const uint32_t delim = A.delim;
+  const uint32_t pat = delim * 0x01010101u;
+  LineReader rd{A.text};
+  uint64_t pos = 0, end = 0;
+  int32_t bad = 0, bad_field = 0;
+  bool shape_bad = false;  // the line has too few delimiters: that outranks a bad value
+  if (live) {
+    pos = r ? A.line_end[r - 1] + 1 : 0;
+    end = r < A.nlines ? A.line_end[r] : A.nbytes;
+    if (end > pos && rd.at(end - 1) == '\r') --end;  // csv.h:479, Windows line breaks
+  }
+  for (int f = 0; f < A.nfields; ++f) {
+    if (!live || shape_bad) continue;
+    if (bad) {  // after a bad value only the delimiters are checked (csv.h splits the line first)
+      const uint64_t q = rd.find(pos, end, pat);
+      if (q >= end) {
+        bad = kImpTooFew;
+        bad_field = f;
+        shape_bad = true;
+      }
+      pos = q + 1;
+      continue;
+    }
+    const ImpField F = A.f[f];
+    uint64_t q = pos, cs = 0, ce = 0;
+    int32_t why = 0;
+    switch (F.kind) {
+      case kTxtInt: {
+        int32_t v = 0;
+        why = parse_int(rd, q, end, delim, v);
+        if (!why) static_cast<int32_t*>(F.out)[r] = v;
+        break;
+      }
+      case kTxtDecimal: {
+        int64_t v = 0;
+        why = parse_decimal(rd, q, end, delim, F.scale, v);
+        if (!why) static_cast<int64_t*>(F.out)[r] = v;
+        break;
+      }
+      case kTxtFloat: {
+        uint32_t v = 0;
+        why = parse_float(rd, q, end, delim, v);
+        if (!why) static_cast<uint32_t*>(F.out)[r] = v;
+        break;
+      }
+      case kTxtDate: {
+        why = field_bounds(rd, pos, end, delim, pat, q, cs, ce);
+        if (!why && ce - cs < 10) why = kImpShortDate;
+        if (!why) {
+          // toDate: digits at 0-3, 5-6, 8-9 weighted 10^7 .. 10^0 (query/schema/tpch.py:9-20)
+          constexpr uint32_t kW[10] = {10000000u, 1000000u, 100000u, 10000u, 0u, 1000u, 100u, 0u, 10u, 1u};
+          uint32_t d = 0;
+#pragma unroll
+          for (int k = 0; k < 10; ++k)
+            if (kW[k]) d += (rd.at(cs + k) - 48u) * kW[k];
+          static_cast<uint32_t*>(F.out)[r] = d;
+        }
+        break;
+      }
+      case kTxtChar: {
+        why = field_bounds(rd, pos, end, delim, pat, q, cs, ce);
+        if (!why && ce - cs != 1) why = kImpNotChar;  // csv.h:920-928
+        if (!why) static_cast<int8_t*>(F.out)[r] = (int8_t)rd.at(cs);
+        break;
+      }
+      case kTxtString: {
+        why = field_bounds(rd, pos, end, delim, pat, q, cs, ce);
+        if (!why) {
+          A.spos[(uint64_t)F.str * A.nrows + r] = cs;
+          A.slen[(uint64_t)F.str * A.nrows + r] = (uint32_t)(ce - cs);
+        }
+        break;
+      }
+      default: {  // kTxtSkip
+        q = rd.find(pos, end, pat);
+        if (q >= end) why = kImpTooFew;
+        break;
+      }
+    }
+    if (why && why != kImpTooFew) {
+      q = rd.find(q, end, pat);  // the field's own delimiter, past the bad byte
+      if (q >= end) why = kImpTooFew;
+    }
+    if (why) {
+      bad = why;
+      bad_field = f;
+      shape_bad = why == kImpTooFew;
+    }
+    pos = q + 1;
+  }
+  if (live && !shape_bad && rd.find(pos, end, pat) < end) {  // csv.h:864-866: one delimiter too many
+    bad = kImpTooMany;
+    bad_field = A.nfields;
+  }
+  if (bad) atomicMin(reinterpret_cast<unsigned long long*>(A.err),
+                     (unsigned long long)(r << 16 | (uint64_t)bad_field << 8 | (uint64_t)bad));
+  // string bytes of this CTA, per string column
+  for (int j = 0; j < A.nstr; ++j) {
+    uint64_t len = live && !bad ? A.slen[(uint64_t)j * A.nrows + r] : 0;
+    if (live && bad) A.slen[(uint64_t)j * A.nrows + r] = 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) len += __shfl_xor_sync(0xffffffffu, len, o);
+    __shared__ uint64_t s_sum[kImpRows / 32];
+    if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = len;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint64_t t = 0;
+      for (int w = 0; w < kImpRows / 32; ++w) t += s_sum[w];
+      A.bsum[(uint64_t)j * (A.nblocks + 1) + blockIdx.x] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Offsets from the per-CTA prefix sums, then a warp per 32 rows copies the
+// bytes (lane k moves bytes k, k + 32, ... of one row at a time).
+__global__ void __launch_bounds__(kImpRows) imp_strings_kernel(const ImpArgs A) {
+  const int j = blockIdx.y;
+  const uint64_t r = (uint64_t)blockIdx.x * kImpRows + threadIdx.x;
+  const bool live = r < A.nrows;
+  const uint64_t len = live ? A.slen[(uint64_t)j * A.nrows + r] : 0;
+  const uint64_t src = live ? A.spos[(uint64_t)j * A.nrows + r] : 0;
+  uint64_t excl;
+  block_scan<kImpRows>(len, excl);
+  const uint64_t off = A.boff[(uint64_t)j * (A.nblocks + 1) + blockIdx.x] + excl;
+  uint64_t* offs = A.soff[j];
+  uint8_t* heap = A.sheap[j];
+  if (live) {
+    offs[r] = off;
+    if (r + 1 == A.nrows) offs[r + 1] = off + len;
+  }
+  const int lane = threadIdx.x & 31;
+  for (int k = 0; k < 32; ++k) {
+    const uint64_t n = __shfl_sync(0xffffffffu, len, k);
+    const uint64_t s = __shfl_sync(0xffffffffu, src, k);
+    const uint64_t d = __shfl_sync(0xffffffffu, off, k);
+    for (uint64_t b = lane; b < n; b += 32) heap[d + b] = A.text[s + b];
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_import_lines(const uint8_t* text, uint64_t ntiles, uint64_t* tile_cnt, uint64_t* tile_off,
+                                cudaStream_t st) {
+  imp_count_kernel<<<(unsigned)ntiles, kImpThreads, 0, st>>>(text, tile_cnt);
+  imp_scan_kernel<<<1, kScanThreads, 0, st>>>(tile_cnt, tile_off, ntiles, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_import_line_ends(const uint8_t* text, uint64_t ntiles, const uint64_t* tile_off,
+                                    uint64_t* line_end, cudaStream_t st) {
+  imp_lines_kernel<<<(unsigned)ntiles, kImpThreads, 0, st>>>(text, tile_off, line_end);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_import_parse(const ImpArgs& A, cudaStream_t st) {
+  if (A.nrows == 0) return cudaSuccess;
+  imp_parse_kernel<<<(unsigned)A.nblocks, kImpRows, 0, st>>>(A);
+  if (A.nstr > 0) imp_scan_kernel<<<A.nstr, kScanThreads, 0, st>>>(A.bsum, A.boff, A.nblocks, A.nblocks + 1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_import_strings(const ImpArgs& A, cudaStream_t st) {
+  if (A.nrows == 0 || A.nstr == 0) return cudaSuccess;
+  imp_strings_kernel<<<dim3((unsigned)A.nblocks, (unsigned)A.nstr), kImpRows, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+}  // namespace dq

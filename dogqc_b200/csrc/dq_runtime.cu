@@ -46,6 +46,12 @@ cudaError_t launch_batch_reset(const BatchReset* ops, int nops, int sms, cudaStr
 cudaError_t launch_batch_scan(const BatchScanSeg* segs, int nseg, uint64_t total_blocks, uint32_t* partials,
                               cudaStream_t stream);
 cudaError_t launch_batch_pack(const BatchPack* ops, int nops, uint8_t* dst, int sms, cudaStream_t stream);
+cudaError_t launch_import_lines(const uint8_t* text, uint64_t ntiles, uint64_t* tile_cnt, uint64_t* tile_off,
+                                cudaStream_t st);
+cudaError_t launch_import_line_ends(const uint8_t* text, uint64_t ntiles, const uint64_t* tile_off,
+                                    uint64_t* line_end, cudaStream_t st);
+cudaError_t launch_import_parse(const ImpArgs& A, cudaStream_t st);
+cudaError_t launch_import_strings(const ImpArgs& A, cudaStream_t st);
 }  // namespace dq
 
 using namespace dq;
@@ -153,6 +159,7 @@ struct dq_ctx {
   std::string error;
   std::mutex mu;
   std::map<std::string, TableRec> tables;
+  dq_import_timing last_import{};
 };
 
 struct ResRec {
@@ -1443,6 +1450,244 @@ int dq_table_rows(dq_ctx* ctx, const char* name, int64_t* nrows) {
   if (it == ctx->tables.end()) return fail(ctx, DQ_ERR_NOT_FOUND, std::string("unknown table ") + name);
   *nrows = it->second.nrows;
   return DQ_OK;
+}
+
+// ---------------------------------------------------------------- import --
+
+namespace {
+
+const char* import_reason(int why) {
+  switch (why) {
+    case kImpTooFew: return "fewer delimiters than fields";
+    case kImpTooMany: return "more delimiters than fields";
+    case kImpNoDigit: return "not a number";
+    case kImpOverflow: return "number out of range";
+    case kImpNotChar: return "not a single character";
+    case kImpShortDate: return "date shorter than 10 bytes";
+    case kImpExponent: return "exponent not accepted";
+    default: return "malformed";
+  }
+}
+
+int text_ctype(int kind) {
+  switch (kind) {
+    case kTxtInt: return DQ_I32;
+    case kTxtDate: return DQ_U32;
+    case kTxtChar: return DQ_I8;
+    case kTxtDecimal: return DQ_I64;
+    case kTxtFloat: return DQ_U32;
+    case kTxtString: return DQ_STR;
+    default: return 0;
+  }
+}
+
+}  // namespace
+
+int dq_table_import_text(dq_ctx* ctx, const char* name, const char* text, uint64_t nbytes, char delim,
+                         int32_t nfields, const dq_text_field* fields, int64_t* nrows_out) {
+  if (!ctx || !name || (nbytes && !text) || nfields <= 0 || !fields || !nrows_out)
+    return fail(ctx, DQ_ERR_INVALID, "bad import arguments");
+  if (nfields > kImpMaxFields) return fail(ctx, DQ_ERR_UNSUPPORTED, "more than 64 fields a line");
+  if (delim == '\n' || delim == '\r' || delim == '\0') return fail(ctx, DQ_ERR_INVALID, "bad delimiter");
+  return guarded(ctx, [&]() {
+    if (ctx->offline) throw DqError(DQ_ERR_UNSUPPORTED, "an offline context cannot import");
+    for (int f = 0; f < nfields; ++f) {
+      const dq_text_field& F = fields[f];
+      if (F.kind < kTxtInt || F.kind > kTxtFloat) throw DqError(DQ_ERR_INVALID, "bad field kind");
+      if (F.kind == kTxtSkip) continue;
+      if (!F.name || !*F.name) throw DqError(DQ_ERR_INVALID, "field without a name");
+      if (F.kind == kTxtDecimal && (F.scale < 0 || F.scale > 18)) throw DqError(DQ_ERR_INVALID, "decimal scale not in 0..18");
+      for (int g = 0; g < f; ++g)
+        if (fields[g].kind != kTxtSkip && !strcmp(fields[g].name, F.name))
+          throw DqError(DQ_ERR_INVALID, std::string("duplicate column ") + F.name);
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DQ_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const auto t_call = std::chrono::steady_clock::now();
+    struct Events {
+      cudaEvent_t e[9] = {};
+      ~Events() {
+        for (auto& x : e)
+          if (x) cudaEventDestroy(x);
+      }
+    } ev;
+    for (auto& x : ev.e) DQ_CUDA(cudaEventCreate(&x));
+    dq_import_timing tm{};
+    tm.nbytes = nbytes;
+    DQ_CUDA(cudaEventRecord(ev.e[0], st));
+    // the text, zero-padded to whole tiles (a host or a device pointer)
+    const uint64_t ntiles = std::max<uint64_t>(1, (nbytes + kImpTile - 1) / kImpTile);
+    DevBuf tbuf, tcnt, toff;
+    tbuf.alloc(ntiles * kImpTile);
+    cudaPointerAttributes pa{};
+    const bool on_device = cudaPointerGetAttributes(&pa, text) == cudaSuccess && pa.type == cudaMemoryTypeDevice;
+    cudaGetLastError();
+    if (nbytes) DQ_CUDA(cudaMemcpyAsync(tbuf.ptr, text, nbytes, on_device ? cudaMemcpyDeviceToDevice
+                                                                          : cudaMemcpyHostToDevice, st));
+    DQ_CUDA(cudaMemsetAsync(tbuf.as<uint8_t>() + nbytes, 0, ntiles * kImpTile - nbytes + 256, st));
+    tcnt.alloc((ntiles + 1) * 8);
+    toff.alloc((ntiles + 1) * 8);
+    DQ_CUDA(cudaEventRecord(ev.e[1], st));
+    DQ_CUDA(launch_import_lines(tbuf.as<uint8_t>(), ntiles, tcnt.as<uint64_t>(), toff.as<uint64_t>(), st));
+    DQ_CUDA(cudaEventRecord(ev.e[2], st));
+    tm.kernel_launches += 2;
+    uint64_t nlines = 0;
+    uint8_t last = '\n';
+    DQ_CUDA(cudaMemcpyAsync(&nlines, toff.as<uint64_t>() + ntiles, 8, cudaMemcpyDeviceToHost, st));
+    if (nbytes) DQ_CUDA(cudaMemcpyAsync(&last, tbuf.as<uint8_t>() + nbytes - 1, 1, cudaMemcpyDeviceToHost, st));
+    DQ_CUDA(cudaStreamSynchronize(st));
+    const uint64_t nrows = nlines + (nbytes && last != '\n' ? 1 : 0);
+    DevBuf lend;
+    lend.alloc(std::max<uint64_t>(nlines, 1) * 8);
+    DQ_CUDA(cudaEventRecord(ev.e[3], st));
+    if (nlines) DQ_CUDA(launch_import_line_ends(tbuf.as<uint8_t>(), ntiles, toff.as<uint64_t>(), lend.as<uint64_t>(), st));
+    tm.kernel_launches += nlines ? 1 : 0;
+    DQ_CUDA(cudaEventRecord(ev.e[4], st));
+
+    ImpArgs A{};
+    A.text = tbuf.as<uint8_t>();
+    A.nbytes = nbytes;
+    A.nlines = nlines;
+    A.nrows = nrows;
+    A.line_end = lend.as<uint64_t>();
+    A.nblocks = (nrows + kImpRows - 1) / kImpRows;
+    A.nfields = nfields;
+    A.delim = (uint8_t)delim;
+    TableRec t;
+    t.nrows = (int64_t)nrows;
+    std::vector<int> str_col;  // string ordinal -> column index in t.cols
+    for (int f = 0; f < nfields; ++f) {
+      const dq_text_field& F = fields[f];
+      ImpField& G = A.f[f];
+      G.kind = F.kind;
+      G.scale = F.scale;
+      if (F.kind == kTxtSkip) continue;
+      ColRec rec;
+      rec.name = F.name;
+      rec.ctype = text_ctype(F.kind);
+      rec.data = std::make_shared<DevBuf>();
+      if (F.kind == kTxtString) {
+        rec.width = 0;
+        rec.offsets = std::make_shared<DevBuf>();
+        G.str = A.nstr++;
+        str_col.push_back((int)t.cols.size());
+      } else {
+        rec.width = ctype_width(rec.ctype);
+        rec.data->alloc(nrows * rec.width);
+        G.out = rec.data->ptr;
+      }
+      t.cols.push_back(std::move(rec));
+    }
+    DevBuf err, spos, slen, bsum, boff;
+    err.alloc(8);
+    DQ_CUDA(cudaMemsetAsync(err.ptr, 0xff, 8, st));
+    A.err = err.as<uint64_t>();
+    if (A.nstr) {
+      spos.alloc((uint64_t)A.nstr * std::max<uint64_t>(nrows, 1) * 8);
+      slen.alloc((uint64_t)A.nstr * std::max<uint64_t>(nrows, 1) * 4);
+      bsum.alloc((uint64_t)A.nstr * (A.nblocks + 1) * 8);
+      boff.alloc((uint64_t)A.nstr * (A.nblocks + 1) * 8);
+      A.spos = spos.as<uint64_t>();
+      A.slen = slen.as<uint32_t>();
+      A.bsum = bsum.as<uint64_t>();
+      A.boff = boff.as<uint64_t>();
+      if (nrows == 0) DQ_CUDA(cudaMemsetAsync(boff.ptr, 0, (uint64_t)A.nstr * 8, st));
+    }
+    DQ_CUDA(cudaEventRecord(ev.e[8], st));
+    DQ_CUDA(launch_import_parse(A, st));
+    DQ_CUDA(cudaEventRecord(ev.e[5], st));
+    tm.kernel_launches += nrows ? 1 + (A.nstr ? 1 : 0) : 0;
+    std::vector<uint64_t> totals(A.nstr, 0);
+    uint64_t bad = ~0ull;
+    DQ_CUDA(cudaMemcpyAsync(&bad, err.ptr, 8, cudaMemcpyDeviceToHost, st));
+    for (int j = 0; j < A.nstr; ++j)
+      DQ_CUDA(cudaMemcpyAsync(&totals[j], A.boff + (uint64_t)j * (A.nblocks + 1) + A.nblocks, 8,
+                              cudaMemcpyDeviceToHost, st));
+    DQ_CUDA(cudaStreamSynchronize(st));
+    if (bad != ~0ull) {
+      const uint64_t row = bad >> 16;
+      const int field = (int)((bad >> 8) & 0xff), why = (int)(bad & 0xff);
+      std::string where = field < nfields ? std::string(" field ") + std::to_string(field + 1) +
+                                                (fields[field].kind != kTxtSkip ? std::string(" (") + fields[field].name + ")" : "")
+                                          : std::string();
+      throw DqError(DQ_ERR_INVALID, std::string("import of ") + name + ": line " + std::to_string(row + 1) + where +
+                                        ": " + import_reason(why));
+    }
+    for (int j = 0; j < A.nstr; ++j) {
+      ColRec& c = t.cols[str_col[j]];
+      c.nchars = totals[j];
+      c.data->alloc(totals[j]);
+      c.offsets->alloc((nrows + 1) * 8);
+      A.sheap[j] = c.data->as<uint8_t>();
+      A.soff[j] = c.offsets->as<uint64_t>();
+      if (nrows == 0) DQ_CUDA(cudaMemsetAsync(c.offsets->ptr, 0, 8, st));
+    }
+    DQ_CUDA(cudaEventRecord(ev.e[6], st));
+    DQ_CUDA(launch_import_strings(A, st));
+    DQ_CUDA(cudaEventRecord(ev.e[7], st));
+    tm.kernel_launches += nrows && A.nstr ? 1 : 0;
+    DQ_CUDA(cudaStreamSynchronize(st));
+    ctx->tables[name] = std::move(t);
+    *nrows_out = (int64_t)nrows;
+    float ms = 0;
+    auto span = [&](int a, int b) {
+      DQ_CUDA(cudaEventElapsedTime(&ms, ev.e[a], ev.e[b]));
+      return (double)ms;
+    };
+    tm.copy_ms = span(0, 1);
+    tm.newline_ms = span(1, 2);
+    tm.line_end_ms = span(3, 4);
+    tm.parse_ms = span(8, 5);
+    tm.string_ms = span(6, 7);
+    tm.span_ms = span(0, 7);
+    tm.call_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_call).count();
+    ctx->last_import = tm;
+    return (int)DQ_OK;
+  });
+}
+
+int dq_table_import_timing_get(dq_ctx* ctx, dq_import_timing* out) {
+  if (!ctx || !out) return fail(ctx, DQ_ERR_INVALID, "bad arguments");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  *out = ctx->last_import;
+  return DQ_OK;
+}
+
+int dq_table_column_read(dq_ctx* ctx, const char* table, const char* column, void* data, uint64_t data_bytes,
+                         uint64_t* offsets, uint64_t* nchars) {
+  if (!ctx || !table || !column) return fail(ctx, DQ_ERR_INVALID, "bad arguments");
+  return guarded(ctx, [&]() {
+    if (ctx->offline) throw DqError(DQ_ERR_UNSUPPORTED, "an offline context holds no column data");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->tables.find(table);
+    if (it == ctx->tables.end()) throw DqError(DQ_ERR_NOT_FOUND, std::string("unknown table ") + table);
+    const ColRec* c = it->second.find(column);
+    if (!c) throw DqError(DQ_ERR_NOT_FOUND, std::string("unknown column ") + column);
+    const uint64_t nrows = (uint64_t)it->second.nrows;
+    DQ_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (c->ctype == DQ_STR) {
+      if (nchars) *nchars = c->nchars;
+      if (data) {
+        if (data_bytes < c->nchars) throw DqError(DQ_ERR_INVALID, "buffer smaller than the string heap");
+        if (c->nchars) DQ_CUDA(cudaMemcpyAsync(data, c->data->ptr, c->nchars, cudaMemcpyDeviceToHost, st));
+      }
+      if (offsets) {
+        if (c->width > 0) {
+          for (uint64_t i = 0; i <= nrows; ++i) offsets[i] = i * (uint64_t)c->width;
+        } else {
+          DQ_CUDA(cudaMemcpyAsync(offsets, c->offsets->ptr, (nrows + 1) * 8, cudaMemcpyDeviceToHost, st));
+        }
+      }
+    } else {
+      const uint64_t b = nrows * (uint64_t)ctype_width(c->ctype);
+      if (!data || data_bytes < b) throw DqError(DQ_ERR_INVALID, "buffer smaller than the column");
+      if (b) DQ_CUDA(cudaMemcpyAsync(data, c->data->ptr, b, cudaMemcpyDeviceToHost, st));
+    }
+    DQ_CUDA(cudaStreamSynchronize(st));
+    return (int)DQ_OK;
+  });
 }
 
 int dq_plan_prepare(dq_ctx* ctx, const dq_plan_desc* desc, dq_plan** out) {

@@ -238,6 +238,60 @@ class Engine(object):
         arr, n, keep = self._columns(table)
         L.check(L.lib().dq_table_update(self.ctx, table.name.encode(), n, arr, table.size, stream), self.ctx)
 
+    def import_text(self, name, text, fields, delim="|"):
+        """Parse ``.tbl`` text on the device into the table ``name``.
+
+        ``text``: bytes, or a device tensor of uint8 (``data_ptr`` is read);
+        ``fields``: (column name, kind[, scale]) per field, kind one of
+        ``L.TEXT_*`` (``None`` name for ``TEXT_SKIP``).  Returns the rows."""
+        arr = (L.dq_text_field * max(len(fields), 1))()
+        keep = []
+        for i, fd in enumerate(fields):
+            nm = fd[0].encode() if fd[0] else None
+            keep.append(nm)
+            arr[i].name = nm
+            arr[i].kind = fd[1]
+            arr[i].scale = fd[2] if len(fd) > 2 else 0
+        if hasattr(text, "data_ptr"):
+            ptr, nbytes = text.data_ptr(), int(text.numel())
+        else:
+            buf = C.create_string_buffer(bytes(text), len(text))
+            keep.append(buf)
+            ptr, nbytes = C.addressof(buf), len(text)
+        nrows = C.c_int64()
+        L.check(L.lib().dq_table_import_text(self.ctx, name.encode(), ptr, nbytes, delim.encode(), len(fields),
+                                             arr, C.byref(nrows)), self.ctx)
+        self.registered.pop(name, None)
+        return nrows.value
+
+    def import_timing(self):
+        """Phase times of the last ``import_text`` (dict; device ms from CUDA
+        events, ``call_ms`` the host time of the whole call)."""
+        t = L.dq_import_timing()
+        L.check(L.lib().dq_table_import_timing_get(self.ctx, C.byref(t)), self.ctx)
+        return {name: getattr(t, name) for name, _ in t._fields_}
+
+    def read_column(self, table, column, ctype=None):
+        """A registered column copied back to the host: a numpy array of the
+        column's type ``ctype`` (``L.I8``, ``L.I32``, ``L.U32``, ``L.I64``,
+        ``L.U64``), or for ``L.STR`` the pair (heap bytes, uint64 offsets)."""
+        nrows = C.c_int64()
+        L.check(L.lib().dq_table_rows(self.ctx, table.encode(), C.byref(nrows)), self.ctx)
+        n = nrows.value
+        if ctype == L.STR:
+            nch = C.c_uint64()
+            L.check(L.lib().dq_table_column_read(self.ctx, table.encode(), column.encode(), None, 0, None,
+                                                 C.byref(nch)), self.ctx)
+            chars = np.zeros(max(nch.value, 1), np.uint8)
+            offs = np.zeros(n + 1, np.uint64)
+            L.check(L.lib().dq_table_column_read(self.ctx, table.encode(), column.encode(), chars.ctypes.data,
+                                                 chars.nbytes, offs.ctypes.data, C.byref(nch)), self.ctx)
+            return chars[:nch.value], offs
+        out = np.zeros(max(n, 1), NP_DTYPE[ctype])
+        L.check(L.lib().dq_table_column_read(self.ctx, table.encode(), column.encode(), out.ctypes.data,
+                                             out.nbytes, None, None), self.ctx)
+        return out[:n]
+
     def prepare(self, plan, options=None, tuning=None):
         """``tuning``: dq_tuning fields as a dict (see dogqc_b200.autotune)."""
         lowering = plan if isinstance(plan, Lowering) else Lowering(plan, options)

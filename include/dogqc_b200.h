@@ -113,6 +113,60 @@ int dq_table_update(dq_ctx* ctx, const char* name, int32_t ncols, const dq_colum
 int dq_table_drop(dq_ctx* ctx, const char* name);
 int dq_table_rows(dq_ctx* ctx, const char* name, int64_t* nrows);
 
+/* ------------------------------------------------------------- import -- */
+/* A table from text in the reference's .tbl layout (replaces the generated
+ * C++ importer of dogqc/dbio.py:117-253 and the CSV reader it drives,
+ * dogqc/include/csv.h).  Lines end at '\n' (a '\r' before it is dropped; a
+ * last line without '\n' counts); every line holds exactly `nfields`
+ * delimiters, each field followed by one, and the text after the last one is
+ * ignored; spaces around a field are trimmed.  The text is copied to the
+ * device and parsed there: line ends from a per-tile newline count and its
+ * prefix sum, one thread per row for the fields, string heaps from a prefix
+ * sum of the lengths.  Kinds and column types:
+ *   INT     -> DQ_I32, [+-]digits (empty: 0), overflow is an error;
+ *   DATE    -> DQ_U32, the schema's toDate of a field of at least 10 bytes
+ *              ('YYYY-MM-DD' -> YYYYMMDD, query/schema/tpch.py:9-20);
+ *   CHAR    -> DQ_I8, a field of exactly one byte;
+ *   DECIMAL -> DQ_I64 exact, scaled by 10^scale ([+-]digits[.digits]; digits
+ *              beyond `scale` are dropped), the engine's FLOAT representation;
+ *   FLOAT   -> DQ_U32 holding the IEEE binary32 bits the reference's importer
+ *              stores (its float parse, step by step, rounded the same way);
+ *   STRING  -> DQ_STR (offsets + heap);  SKIP: not stored.
+ * A malformed row fails the call with DQ_ERR_INVALID naming its line.
+ * *nrows: the rows imported.                                                 */
+typedef enum {
+    DQ_TEXT_INT = 1, DQ_TEXT_DATE = 2, DQ_TEXT_CHAR = 3, DQ_TEXT_DECIMAL = 4, DQ_TEXT_STRING = 5, DQ_TEXT_SKIP = 6,
+    DQ_TEXT_FLOAT = 7
+} dq_text_kind;
+typedef struct {
+    const char* name;                /* column name (ignored for DQ_TEXT_SKIP)   */
+    int32_t kind;                    /* dq_text_kind                             */
+    int32_t scale;                   /* DQ_TEXT_DECIMAL: digits after the point  */
+} dq_text_field;
+int dq_table_import_text(dq_ctx* ctx, const char* name, const char* text, uint64_t nbytes, char delim,
+                         int32_t nfields, const dq_text_field* fields, int64_t* nrows);
+/* Copies a registered column back to the host: fixed width -> `data`
+ * (nrows values, `data_bytes` at most); strings -> the heap into `data`
+ * (*nchars bytes) and nrows+1 offsets into `offsets` (may be NULL to query
+ * *nchars first).                                                           */
+int dq_table_column_read(dq_ctx* ctx, const char* table, const char* column, void* data, uint64_t data_bytes,
+                         uint64_t* offsets, uint64_t* nchars);
+/* Device time of the last import's phases (CUDA events on the context
+ * stream) and the host time of the whole call.                              */
+typedef struct {
+    double copy_ms;                  /* text into the padded device buffer      */
+    double newline_ms;               /* newline count per tile + its prefix sum */
+    double line_end_ms;              /* line end positions                      */
+    double parse_ms;                 /* fields, one thread per row + string sums*/
+    double string_ms;                /* string offsets and heaps                */
+    double call_ms;                  /* host wall time of the call              */
+    double span_ms;                  /* device timeline from the first phase to */
+                                     /* the last, host waits between included   */
+    int64_t kernel_launches;
+    uint64_t nbytes;
+} dq_import_timing;
+int dq_table_import_timing_get(dq_ctx* ctx, dq_import_timing* out);
+
 /* ------------------------------------------------------------------ IR -- */
 /* A plan is a list of resources (hash tables, aggregation tables, outputs)
  * and pipelines.  Each pipeline streams one source in tiles through a list of
