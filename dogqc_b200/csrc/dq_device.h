@@ -195,8 +195,16 @@ struct ImpField {
   int32_t pad;
 };
 
+// The text as whole tiles: bytes [0, nmain) at `main`, the rest (one
+// zero-padded tile at most) at `tail`.
+struct ImpText {
+  const uint8_t* main;
+  const uint8_t* tail;
+  uint64_t nmain;         // a multiple of kImpTile
+};
+
 struct ImpArgs {
-  const uint8_t* text;    // padded with zeros to a multiple of kImpTile
+  ImpText text;
   uint64_t nbytes;
   uint64_t nlines;        // newlines in the text
   uint64_t nrows;         // nlines, plus one for a last line without a newline

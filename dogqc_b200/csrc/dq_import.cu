@@ -37,21 +37,33 @@ constexpr int kImpPerThread = kImpTile / kImpThreads;  // 64 bytes: four 16-byte
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 8;
 
-// Bytes of `w` equal to those of `pat` as a 4-bit mask (byte k -> bit k).  The
-// 0/1 byte flags sit at bits 0, 8, 16, 24; the multiply moves them to bits
-// 24..27 without overlapping partial products.
-__device__ __forceinline__ uint32_t eq_nibble(uint32_t w, uint32_t pat) {
-  const uint32_t t = __vcmpeq4(w, pat) & 0x01010101u;
-  return (t * 0x01020408u) >> 24;
+// Bit 8k+7 set exactly for the zero bytes k of x: a byte's low seven bits plus
+// 0x7F reach bit 7 unless they are all zero, and its own bit 7 rules out the
+// rest; no carry leaves a byte (the classic exact zero-byte test).  XOR with a
+// repeated byte first to find that byte.
+__device__ __forceinline__ uint32_t zero_bytes(uint32_t x) {
+  return ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);
+}
+__device__ __forceinline__ uint64_t zero_bytes64(uint64_t x) {
+  return ~(((x & 0x7F7F7F7F7F7F7F7Full) + 0x7F7F7F7F7F7F7F7Full) | x | 0x7F7F7F7F7F7F7F7Full);
 }
 
-__device__ __forceinline__ uint32_t eq_mask16(const uint4& v, uint32_t pat) {
-  return eq_nibble(v.x, pat) | (eq_nibble(v.y, pat) << 4) | (eq_nibble(v.z, pat) << 8) |
-         (eq_nibble(v.w, pat) << 12);
+// Newlines of a 16-byte chunk as a 16-bit mask (byte k -> bit k): the flags at
+// bits 7, 15, 23, 31 of each word move to bits 24..27 by one multiply whose
+// partial products do not overlap.
+__device__ __forceinline__ uint32_t nibble_of(uint32_t z) { return (((z >> 7) & 0x01010101u) * 0x01020408u) >> 24; }
+__device__ __forceinline__ uint32_t newline_mask16(const uint4& v) {
+  return nibble_of(zero_bytes(v.x ^ 0x0a0a0a0au)) | (nibble_of(zero_bytes(v.y ^ 0x0a0a0a0au)) << 4) |
+         (nibble_of(zero_bytes(v.z ^ 0x0a0a0a0au)) << 8) | (nibble_of(zero_bytes(v.w ^ 0x0a0a0a0au)) << 12);
 }
 
 __device__ __forceinline__ uint4 ld_chunk(const uint8_t* p) {
   return __ldg(reinterpret_cast<const uint4*>(p));
+}
+
+// Byte `i` of the text lives in the main part or in the padded tail tile.
+__device__ __forceinline__ const uint8_t* text_at(const ImpText& T, uint64_t i) {
+  return i < T.nmain ? T.main + i : T.tail + (i - T.nmain);
 }
 
 // Exclusive block scan of one value per thread (any power-of-two block up to
@@ -89,24 +101,29 @@ __device__ T block_scan(T x, T& excl) {
 
 // ------------------------------------------------------------ newlines --
 
-__global__ void __launch_bounds__(kImpThreads) imp_count_kernel(const uint8_t* text, uint64_t* tile_cnt) {
-  const uint8_t* p = text + (uint64_t)blockIdx.x * kImpTile + threadIdx.x * kImpPerThread;
+__global__ void __launch_bounds__(kImpThreads) imp_count_kernel(const ImpText T, uint64_t* tile_cnt) {
+  const uint8_t* p = text_at(T, (uint64_t)blockIdx.x * kImpTile) + threadIdx.x * kImpPerThread;
   uint32_t n = 0;
 #pragma unroll
-  for (int k = 0; k < kImpPerThread / 16; ++k) n += __popc(eq_mask16(ld_chunk(p + 16 * k), 0x0a0a0a0au));
+  for (int k = 0; k < kImpPerThread / 16; ++k) {
+    const uint4 v = ld_chunk(p + 16 * k);
+    n += __popc(zero_bytes(v.x ^ 0x0a0a0a0au)) + __popc(zero_bytes(v.y ^ 0x0a0a0a0au)) +
+         __popc(zero_bytes(v.z ^ 0x0a0a0a0au)) + __popc(zero_bytes(v.w ^ 0x0a0a0a0au));
+  }
   uint32_t excl;
   const uint32_t total = block_scan<kImpThreads>(n, excl);
   if (threadIdx.x == 0) tile_cnt[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(kImpThreads) imp_lines_kernel(const uint8_t* text, const uint64_t* tile_off,
+__global__ void __launch_bounds__(kImpThreads) imp_lines_kernel(const ImpText T, const uint64_t* tile_off,
                                                                 uint64_t* line_end) {
   const uint64_t first = (uint64_t)blockIdx.x * kImpTile + threadIdx.x * kImpPerThread;
-  uint32_t m[kImpPerThread / 16];
+  const uint8_t* p = text_at(T, (uint64_t)blockIdx.x * kImpTile) + threadIdx.x * kImpPerThread;
+  uint32_t m[kImpPerThread / 16];  // per 16-byte chunk: bit k for a newline at byte k
   uint32_t n = 0;
 #pragma unroll
   for (int k = 0; k < kImpPerThread / 16; ++k) {
-    m[k] = eq_mask16(ld_chunk(text + first + 16 * k), 0x0a0a0a0au);
+    m[k] = newline_mask16(ld_chunk(p + 16 * k));
     n += __popc(m[k]);
   }
   uint32_t excl;
@@ -153,14 +170,14 @@ __global__ void __launch_bounds__(kScanThreads) imp_scan_kernel(const uint64_t* 
 
 // A thread's view of its line: the 16-byte chunk last loaded, in registers.
 struct LineReader {
-  const uint8_t* text;
+  ImpText text;
   uint64_t base = ~0ull;
   uint4 v;
 
   __device__ __forceinline__ void fetch(uint64_t i) {
     const uint64_t b = i & ~15ull;
     if (b != base) {
-      v = ld_chunk(text + b);
+      v = ld_chunk(text_at(text, b));
       base = b;
     }
   }
@@ -171,12 +188,21 @@ struct LineReader {
     return (w >> ((k & 3) * 8)) & 0xffu;
   }
   // First byte equal to the delimiter in [i, end); `end` if there is none.
-  __device__ __forceinline__ uint64_t find(uint64_t i, uint64_t end, uint32_t pat) {
+  // `pat`: the delimiter in every byte of a 64-bit word.
+  __device__ __forceinline__ uint64_t find(uint64_t i, uint64_t end, uint64_t pat) {
     while (i < end) {
       fetch(i);
-      const uint32_t m = eq_mask16(v, pat) >> (i & 15);
-      if (m) {
-        const uint64_t q = i + (__ffs(m) - 1);
+      uint64_t z0 = zero_bytes64((((uint64_t)v.y << 32) | v.x) ^ pat);
+      uint64_t z1 = zero_bytes64((((uint64_t)v.w << 32) | v.z) ^ pat);
+      const uint32_t sh = (uint32_t)i & 15u;
+      if (sh >= 8) {
+        z0 = 0;
+        z1 &= ~0ull << (8 * (sh - 8));
+      } else {
+        z0 &= ~0ull << (8 * sh);
+      }
+      if (z0 | z1) {
+        const uint64_t q = base + (z0 ? (uint32_t)(__ffsll(z0) - 1) >> 3 : 8 + ((uint32_t)(__ffsll(z1) - 1) >> 3));
         return q < end ? q : end;
       }
       i = base + 16;
@@ -188,7 +214,7 @@ struct LineReader {
 // Field [i, q) of a line ending at `end`, with the spaces around it trimmed
 // to [cs, ce).  Returns a reason code, 0 when the delimiter was found.
 __device__ __forceinline__ int32_t field_bounds(LineReader& rd, uint64_t i, uint64_t end, uint32_t delim,
-                                                uint32_t pat, uint64_t& q, uint64_t& cs, uint64_t& ce) {
+                                                uint64_t pat, uint64_t& q, uint64_t& cs, uint64_t& ce) {
   q = rd.find(i, end, pat);
   if (q >= end) return kImpTooFew;
   cs = i;
@@ -197,6 +223,57 @@ __device__ __forceinline__ int32_t field_bounds(LineReader& rd, uint64_t i, uint
   while (ce > cs && rd.at(ce - 1) == ' ') --ce;
   (void)delim;
   return 0;
+}
+
+// ---------------------------------------------------------- date window --
+// A date field of 10 to 16 bytes with no spaces around it is read from a
+// 16-byte window in registers; anything else goes to the byte-at-a-time path
+// below, which gives the same value or the exact reason.  (Numbers stay on the
+// byte-at-a-time parsers: on fields of a few digits a window, a digit check
+// and a SWAR conversion cost more than one pass over the bytes.)
+
+// Bytes [i, i + 16) of the text as two little-endian halves (w0: bytes 0-7),
+// from the chunk holding i and the next one (both lie in the padded text).
+// Branch-free: the word offset selects in two steps, the byte offset is one
+// byte permute per word.
+struct Window {
+  uint64_t w0, w1;
+};
+
+__device__ __forceinline__ Window load_window(const ImpText& T, uint64_t i) {
+  const uint64_t b = i & ~15ull;
+  const uint32_t sh = (uint32_t)i & 15u;
+  const uint4 a = ld_chunk(text_at(T, b));
+  const uint4 c = ld_chunk(text_at(T, b + 16));
+  const bool s1 = sh & 4u, s2 = sh & 8u;
+  // z[j] = x[j + (sh>>2 & 1)], then y[k] = z[k + 2 * (sh>>3 & 1)] over x = a.x .. c.w
+  const uint32_t z0 = s1 ? a.y : a.x, z1 = s1 ? a.z : a.y, z2 = s1 ? a.w : a.z, z3 = s1 ? c.x : a.w,
+                 z4 = s1 ? c.y : c.x, z5 = s1 ? c.z : c.y, z6 = s1 ? c.w : c.z;
+  const uint32_t y0 = s2 ? z2 : z0, y1 = s2 ? z3 : z1, y2 = s2 ? z4 : z2, y3 = s2 ? z5 : z3, y4 = s2 ? z6 : z4;
+  const uint32_t sel = 0x3210u + 0x1111u * (sh & 3u);
+  Window W;
+  W.w0 = ((uint64_t)__byte_perm(y1, y2, sel) << 32) | __byte_perm(y0, y1, sel);
+  W.w1 = ((uint64_t)__byte_perm(y3, y4, sel) << 32) | __byte_perm(y2, y3, sel);
+  return W;
+}
+
+__device__ __forceinline__ uint32_t win_byte(const Window& W, uint32_t k) {
+  return (uint32_t)((k < 8 ? W.w0 >> (8 * k) : W.w1 >> (8 * (k - 8))) & 0xffu);
+}
+
+// DATE from the untrimmed field [i, q) of 10 to 16 bytes without spaces
+// around it (query/schema/tpch.py:9-20 over bytes 0-3, 5-6, 8-9).
+__device__ __forceinline__ bool fast_date(const ImpText& T, uint64_t i, uint64_t q, uint32_t& out) {
+  const uint32_t n = (uint32_t)(q - i);
+  if (n < 10 || n > 16) return false;
+  const Window W = load_window(T, i);
+  if ((W.w0 & 0xffu) == ' ' || win_byte(W, n - 1) == ' ') return false;
+  const uint32_t a = (uint32_t)W.w0, b = (uint32_t)(W.w0 >> 32), c = (uint32_t)W.w1;
+  out = ((a & 0xffu) - 48u) * 10000000u + (((a >> 8) & 0xffu) - 48u) * 1000000u +
+        (((a >> 16) & 0xffu) - 48u) * 100000u + ((a >> 24) - 48u) * 10000u +
+        (((b >> 8) & 0xffu) - 48u) * 1000u + (((b >> 16) & 0xffu) - 48u) * 100u +
+        ((c & 0xffu) - 48u) * 10u + (((c >> 8) & 0xffu) - 48u);
+  return true;
 }
 
 // csv.h parse_signed_integer for int, throw_on_overflow (csv.h:945-995), on
@@ -358,11 +435,11 @@ __device__ int32_t parse_float(LineReader& rd, uint64_t& i, uint64_t end, uint32
   return 0;
 }
 
-__global__ void __launch_bounds__(kImpRows) imp_parse_kernel(const ImpArgs A) {
+__global__ void __launch_bounds__(kImpRows, 6) imp_parse_kernel(const ImpArgs A) {
   const uint64_t r = (uint64_t)blockIdx.x * kImpRows + threadIdx.x;
   const bool live = r < A.nrows;
   const uint32_t delim = A.delim;
-  const uint32_t pat = delim * 0x01010101u;
+  const uint64_t pat = delim * 0x0101010101010101ull;
   LineReader rd{A.text};
   uint64_t pos = 0, end = 0;
   int32_t bad = 0, bad_field = 0;
@@ -407,6 +484,13 @@ __global__ void __launch_bounds__(kImpRows) imp_parse_kernel(const ImpArgs A) {
         break;
       }
       case kTxtDate: {
+        uint32_t v = 0;
+        const uint64_t d = rd.find(pos, end, pat);
+        if (d < end && fast_date(A.text, pos, d, v)) {
+          q = d;
+          static_cast<uint32_t*>(F.out)[r] = v;
+          break;
+        }
         why = field_bounds(rd, pos, end, delim, pat, q, cs, ce);
         if (!why && ce - cs < 10) why = kImpShortDate;
         if (!why) {
@@ -475,44 +559,62 @@ __global__ void __launch_bounds__(kImpRows) imp_parse_kernel(const ImpArgs A) {
   }
 }
 
-// Offsets from the per-CTA prefix sums, then a warp per 32 rows copies the
-// bytes (lane k moves bytes k, k + 32, ... of one row at a time).
+// Offsets from the per-CTA prefix sums, then each warp copies the bytes of
+// its 32 rows, which are contiguous in the heap: lane k moves bytes k, k + 32,
+// ... of that run, finding the row of its byte by a binary search over the
+// rows' starts (shuffles), so every lane moves a byte on every step.  One CTA
+// does every string column of its rows, so their lines are read from HBM once.
 __global__ void __launch_bounds__(kImpRows) imp_strings_kernel(const ImpArgs A) {
-  const int j = blockIdx.y;
   const uint64_t r = (uint64_t)blockIdx.x * kImpRows + threadIdx.x;
   const bool live = r < A.nrows;
-  const uint64_t len = live ? A.slen[(uint64_t)j * A.nrows + r] : 0;
-  const uint64_t src = live ? A.spos[(uint64_t)j * A.nrows + r] : 0;
-  uint64_t excl;
-  block_scan<kImpRows>(len, excl);
-  const uint64_t off = A.boff[(uint64_t)j * (A.nblocks + 1) + blockIdx.x] + excl;
-  uint64_t* offs = A.soff[j];
-  uint8_t* heap = A.sheap[j];
-  if (live) {
-    offs[r] = off;
-    if (r + 1 == A.nrows) offs[r + 1] = off + len;
-  }
   const int lane = threadIdx.x & 31;
-  for (int k = 0; k < 32; ++k) {
-    const uint64_t n = __shfl_sync(0xffffffffu, len, k);
-    const uint64_t s = __shfl_sync(0xffffffffu, src, k);
-    const uint64_t d = __shfl_sync(0xffffffffu, off, k);
-    for (uint64_t b = lane; b < n; b += 32) heap[d + b] = A.text[s + b];
+  for (int j = 0; j < A.nstr; ++j) {
+    const uint64_t len = live ? A.slen[(uint64_t)j * A.nrows + r] : 0;
+    const uint64_t src = live ? A.spos[(uint64_t)j * A.nrows + r] : 0;
+    uint64_t excl;
+    block_scan<kImpRows>(len, excl);
+    const uint64_t off = A.boff[(uint64_t)j * (A.nblocks + 1) + blockIdx.x] + excl;
+    uint64_t* offs = A.soff[j];
+    if (live) {
+      offs[r] = off;
+      if (r + 1 == A.nrows) offs[r + 1] = off + len;
+    }
+    uint64_t wincl = len;  // warp-relative run of the rows' bytes
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t y = __shfl_up_sync(0xffffffffu, wincl, o);
+      if (lane >= o) wincl += y;
+    }
+    const uint64_t wstart = wincl - len;
+    const uint64_t wtotal = __shfl_sync(0xffffffffu, wincl, 31);
+    uint8_t* dst = A.sheap[j] + __shfl_sync(0xffffffffu, off, 0);
+    for (uint64_t b0 = 0; b0 < wtotal; b0 += 32) {
+      const uint64_t b = b0 + lane;
+      int row = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const uint64_t s = __shfl_sync(0xffffffffu, wstart, row + step);
+        if (s <= b) row += step;
+      }
+      const uint64_t rs = __shfl_sync(0xffffffffu, wstart, row);
+      const uint64_t rsrc = __shfl_sync(0xffffffffu, src, row);
+      if (b < wtotal) dst[b] = *text_at(A.text, rsrc + (b - rs));
+    }
   }
 }
 
 }  // namespace
 
-cudaError_t launch_import_lines(const uint8_t* text, uint64_t ntiles, uint64_t* tile_cnt, uint64_t* tile_off,
+cudaError_t launch_import_lines(const ImpText& T, uint64_t ntiles, uint64_t* tile_cnt, uint64_t* tile_off,
                                 cudaStream_t st) {
-  imp_count_kernel<<<(unsigned)ntiles, kImpThreads, 0, st>>>(text, tile_cnt);
+  imp_count_kernel<<<(unsigned)ntiles, kImpThreads, 0, st>>>(T, tile_cnt);
   imp_scan_kernel<<<1, kScanThreads, 0, st>>>(tile_cnt, tile_off, ntiles, 0);
   return cudaGetLastError();
 }
 
-cudaError_t launch_import_line_ends(const uint8_t* text, uint64_t ntiles, const uint64_t* tile_off,
-                                    uint64_t* line_end, cudaStream_t st) {
-  imp_lines_kernel<<<(unsigned)ntiles, kImpThreads, 0, st>>>(text, tile_off, line_end);
+cudaError_t launch_import_line_ends(const ImpText& T, uint64_t ntiles, const uint64_t* tile_off, uint64_t* line_end,
+                                    cudaStream_t st) {
+  imp_lines_kernel<<<(unsigned)ntiles, kImpThreads, 0, st>>>(T, tile_off, line_end);
   return cudaGetLastError();
 }
 
@@ -525,7 +627,7 @@ cudaError_t launch_import_parse(const ImpArgs& A, cudaStream_t st) {
 
 cudaError_t launch_import_strings(const ImpArgs& A, cudaStream_t st) {
   if (A.nrows == 0 || A.nstr == 0) return cudaSuccess;
-  imp_strings_kernel<<<dim3((unsigned)A.nblocks, (unsigned)A.nstr), kImpRows, 0, st>>>(A);
+  imp_strings_kernel<<<(unsigned)A.nblocks, kImpRows, 0, st>>>(A);
   return cudaGetLastError();
 }
 

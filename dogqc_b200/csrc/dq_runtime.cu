@@ -46,10 +46,10 @@ cudaError_t launch_batch_reset(const BatchReset* ops, int nops, int sms, cudaStr
 cudaError_t launch_batch_scan(const BatchScanSeg* segs, int nseg, uint64_t total_blocks, uint32_t* partials,
                               cudaStream_t stream);
 cudaError_t launch_batch_pack(const BatchPack* ops, int nops, uint8_t* dst, int sms, cudaStream_t stream);
-cudaError_t launch_import_lines(const uint8_t* text, uint64_t ntiles, uint64_t* tile_cnt, uint64_t* tile_off,
+cudaError_t launch_import_lines(const ImpText& T, uint64_t ntiles, uint64_t* tile_cnt, uint64_t* tile_off,
                                 cudaStream_t st);
-cudaError_t launch_import_line_ends(const uint8_t* text, uint64_t ntiles, const uint64_t* tile_off,
-                                    uint64_t* line_end, cudaStream_t st);
+cudaError_t launch_import_line_ends(const ImpText& T, uint64_t ntiles, const uint64_t* tile_off, uint64_t* line_end,
+                                    cudaStream_t st);
 cudaError_t launch_import_parse(const ImpArgs& A, cudaStream_t st);
 cudaError_t launch_import_strings(const ImpArgs& A, cudaStream_t st);
 }  // namespace dq
@@ -110,6 +110,7 @@ struct OfflineScope {
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
+  std::shared_ptr<DevBuf> slab;  // set for a view into a larger buffer (freed with the last view)
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
@@ -120,10 +121,24 @@ struct DevBuf {
     if (t_offline) return;
     DQ_CUDA(cudaMalloc(&ptr, align_up(b, 256) + 256));
   }
+  // Grows (never shrinks) a reusable buffer.
+  void reserve(size_t b) {
+    if (!ptr || bytes < b) alloc(b);
+  }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr && !slab) cudaFree(ptr);
+    slab.reset();
     ptr = nullptr;
     bytes = 0;
+  }
+  // Bytes a view of `b` bytes takes in a slab (the same padding as alloc).
+  static size_t span_of(size_t b) { return align_up(b, 256) + 256; }
+  static std::shared_ptr<DevBuf> view(const std::shared_ptr<DevBuf>& slab, size_t off, size_t b) {
+    auto v = std::make_shared<DevBuf>();
+    v->slab = slab;
+    v->ptr = static_cast<uint8_t*>(slab->ptr) + off;
+    v->bytes = b;
+    return v;
   }
   template <class T>
   T* as() const { return reinterpret_cast<T*>(ptr); }
@@ -160,6 +175,9 @@ struct dq_ctx {
   std::mutex mu;
   std::map<std::string, TableRec> tables;
   dq_import_timing last_import{};
+  struct {  // text import scratch, kept for the next import
+    DevBuf text, tail, tcnt, toff, lend, err, spos, slen, bsum, boff;
+  } imp;
 };
 
 struct ResRec {
@@ -1515,48 +1533,107 @@ int dq_table_import_text(dq_ctx* ctx, const char* name, const char* text, uint64
     for (auto& x : ev.e) DQ_CUDA(cudaEventCreate(&x));
     dq_import_timing tm{};
     tm.nbytes = nbytes;
+    auto& S = ctx->imp;
     DQ_CUDA(cudaEventRecord(ev.e[0], st));
-    // the text, zero-padded to whole tiles (a host or a device pointer)
+    // The text as whole 16 KB tiles: text in this device's memory at a 16-byte
+    // boundary is read where it lies, its last partial tile from a zero-padded
+    // copy; other text is copied into a padded buffer.
     const uint64_t ntiles = std::max<uint64_t>(1, (nbytes + kImpTile - 1) / kImpTile);
-    DevBuf tbuf, tcnt, toff;
-    tbuf.alloc(ntiles * kImpTile);
     cudaPointerAttributes pa{};
-    const bool on_device = cudaPointerGetAttributes(&pa, text) == cudaSuccess && pa.type == cudaMemoryTypeDevice;
+    const bool on_device = nbytes && cudaPointerGetAttributes(&pa, text) == cudaSuccess &&
+                           pa.type == cudaMemoryTypeDevice && pa.device == ctx->device;
     cudaGetLastError();
-    if (nbytes) DQ_CUDA(cudaMemcpyAsync(tbuf.ptr, text, nbytes, on_device ? cudaMemcpyDeviceToDevice
-                                                                          : cudaMemcpyHostToDevice, st));
-    DQ_CUDA(cudaMemsetAsync(tbuf.as<uint8_t>() + nbytes, 0, ntiles * kImpTile - nbytes + 256, st));
-    tcnt.alloc((ntiles + 1) * 8);
-    toff.alloc((ntiles + 1) * 8);
+    const bool in_place = on_device && ((uintptr_t)text & 15) == 0;
+    const uint8_t* main_text;
+    uint64_t nmain;  // bytes read from main_text: whole tiles
+    S.tail.reserve(kImpTile);
+    if (in_place) {
+      nmain = nbytes / kImpTile * kImpTile;
+      main_text = reinterpret_cast<const uint8_t*>(text);
+      DQ_CUDA(cudaMemsetAsync(S.tail.ptr, 0, kImpTile + 256, st));
+      if (nbytes > nmain)
+        DQ_CUDA(cudaMemcpyAsync(S.tail.ptr, text + nmain, nbytes - nmain, cudaMemcpyDeviceToDevice, st));
+    } else {
+      nmain = ntiles * kImpTile;
+      S.text.reserve(nmain);
+      main_text = S.text.as<uint8_t>();
+      if (nbytes) DQ_CUDA(cudaMemcpyAsync(S.text.ptr, text, nbytes, on_device ? cudaMemcpyDeviceToDevice
+                                                                              : cudaMemcpyHostToDevice, st));
+      DQ_CUDA(cudaMemsetAsync(S.text.as<uint8_t>() + nbytes, 0, nmain - nbytes + 256, st));
+    }
+    S.tcnt.reserve((ntiles + 1) * 8);
+    S.toff.reserve((ntiles + 1) * 8);
+    ImpText T{main_text, S.tail.as<uint8_t>(), nmain};
     DQ_CUDA(cudaEventRecord(ev.e[1], st));
-    DQ_CUDA(launch_import_lines(tbuf.as<uint8_t>(), ntiles, tcnt.as<uint64_t>(), toff.as<uint64_t>(), st));
+    DQ_CUDA(launch_import_lines(T, ntiles, S.tcnt.as<uint64_t>(), S.toff.as<uint64_t>(), st));
     DQ_CUDA(cudaEventRecord(ev.e[2], st));
     tm.kernel_launches += 2;
     uint64_t nlines = 0;
     uint8_t last = '\n';
-    DQ_CUDA(cudaMemcpyAsync(&nlines, toff.as<uint64_t>() + ntiles, 8, cudaMemcpyDeviceToHost, st));
-    if (nbytes) DQ_CUDA(cudaMemcpyAsync(&last, tbuf.as<uint8_t>() + nbytes - 1, 1, cudaMemcpyDeviceToHost, st));
+    DQ_CUDA(cudaMemcpyAsync(&nlines, S.toff.as<uint64_t>() + ntiles, 8, cudaMemcpyDeviceToHost, st));
+    if (nbytes && on_device) DQ_CUDA(cudaMemcpyAsync(&last, text + nbytes - 1, 1, cudaMemcpyDeviceToHost, st));
+    if (nbytes && !on_device) last = (uint8_t)text[nbytes - 1];
     DQ_CUDA(cudaStreamSynchronize(st));
     const uint64_t nrows = nlines + (nbytes && last != '\n' ? 1 : 0);
-    DevBuf lend;
-    lend.alloc(std::max<uint64_t>(nlines, 1) * 8);
+    S.lend.reserve(std::max<uint64_t>(nlines, 1) * 8);
     DQ_CUDA(cudaEventRecord(ev.e[3], st));
-    if (nlines) DQ_CUDA(launch_import_line_ends(tbuf.as<uint8_t>(), ntiles, toff.as<uint64_t>(), lend.as<uint64_t>(), st));
+    if (nlines) DQ_CUDA(launch_import_line_ends(T, ntiles, S.toff.as<uint64_t>(), S.lend.as<uint64_t>(), st));
     tm.kernel_launches += nlines ? 1 : 0;
     DQ_CUDA(cudaEventRecord(ev.e[4], st));
 
     ImpArgs A{};
-    A.text = tbuf.as<uint8_t>();
+    A.text = T;
     A.nbytes = nbytes;
     A.nlines = nlines;
     A.nrows = nrows;
-    A.line_end = lend.as<uint64_t>();
+    A.line_end = S.lend.as<uint64_t>();
     A.nblocks = (nrows + kImpRows - 1) / kImpRows;
     A.nfields = nfields;
     A.delim = (uint8_t)delim;
+    // The fixed-width columns and the string offsets of the new table: one
+    // slab; the string heaps: a second one.  A table of the same name that is
+    // being replaced lends its slabs when they are large enough (a repeated
+    // load allocates nothing); if this import then fails, that table is gone.
+    std::shared_ptr<DevBuf> old_fixed, old_heap;
+    auto old = ctx->tables.find(name);
+    if (old != ctx->tables.end()) {
+      for (auto& c : old->second.cols) {
+        if (c.ctype == DQ_STR) {
+          if (c.offsets && c.offsets->slab) old_fixed = c.offsets->slab;
+          if (c.data && c.data->slab) old_heap = c.data->slab;
+        } else if (c.data && c.data->slab) {
+          old_fixed = c.data->slab;
+        }
+      }
+    }
+    bool reused = false;
+    struct DropOnFail {  // a failed import that wrote into the old table's slab removes that table
+      dq_ctx* c;
+      const char* n;
+      const bool& reused;
+      bool done;
+      ~DropOnFail() {
+        if (!done && reused) c->tables.erase(n);
+      }
+    } guard{ctx, name, reused, false};
     TableRec t;
     t.nrows = (int64_t)nrows;
     std::vector<int> str_col;  // string ordinal -> column index in t.cols
+    size_t slab_bytes = 0;
+    for (int f = 0; f < nfields; ++f) {
+      const int k = fields[f].kind;
+      if (k == kTxtSkip) continue;
+      slab_bytes += DevBuf::span_of(k == kTxtString ? (nrows + 1) * 8 : nrows * ctype_width(text_ctype(k)));
+    }
+    std::shared_ptr<DevBuf> slab;
+    if (old_fixed && old_fixed->bytes >= slab_bytes) {
+      slab = old_fixed;
+      reused = true;
+    } else {
+      slab = std::make_shared<DevBuf>();
+      slab->alloc(slab_bytes);
+    }
+    size_t at = 0;
     for (int f = 0; f < nfields; ++f) {
       const dq_text_field& F = fields[f];
       ImpField& G = A.f[f];
@@ -1566,33 +1643,33 @@ int dq_table_import_text(dq_ctx* ctx, const char* name, const char* text, uint64
       ColRec rec;
       rec.name = F.name;
       rec.ctype = text_ctype(F.kind);
-      rec.data = std::make_shared<DevBuf>();
       if (F.kind == kTxtString) {
         rec.width = 0;
-        rec.offsets = std::make_shared<DevBuf>();
+        rec.offsets = DevBuf::view(slab, at, (nrows + 1) * 8);
+        at += DevBuf::span_of((nrows + 1) * 8);
         G.str = A.nstr++;
         str_col.push_back((int)t.cols.size());
       } else {
         rec.width = ctype_width(rec.ctype);
-        rec.data->alloc(nrows * rec.width);
+        rec.data = DevBuf::view(slab, at, nrows * rec.width);
+        at += DevBuf::span_of(nrows * rec.width);
         G.out = rec.data->ptr;
       }
       t.cols.push_back(std::move(rec));
     }
-    DevBuf err, spos, slen, bsum, boff;
-    err.alloc(8);
-    DQ_CUDA(cudaMemsetAsync(err.ptr, 0xff, 8, st));
-    A.err = err.as<uint64_t>();
+    S.err.reserve(8);
+    DQ_CUDA(cudaMemsetAsync(S.err.ptr, 0xff, 8, st));
+    A.err = S.err.as<uint64_t>();
     if (A.nstr) {
-      spos.alloc((uint64_t)A.nstr * std::max<uint64_t>(nrows, 1) * 8);
-      slen.alloc((uint64_t)A.nstr * std::max<uint64_t>(nrows, 1) * 4);
-      bsum.alloc((uint64_t)A.nstr * (A.nblocks + 1) * 8);
-      boff.alloc((uint64_t)A.nstr * (A.nblocks + 1) * 8);
-      A.spos = spos.as<uint64_t>();
-      A.slen = slen.as<uint32_t>();
-      A.bsum = bsum.as<uint64_t>();
-      A.boff = boff.as<uint64_t>();
-      if (nrows == 0) DQ_CUDA(cudaMemsetAsync(boff.ptr, 0, (uint64_t)A.nstr * 8, st));
+      S.spos.reserve((uint64_t)A.nstr * std::max<uint64_t>(nrows, 1) * 8);
+      S.slen.reserve((uint64_t)A.nstr * std::max<uint64_t>(nrows, 1) * 4);
+      S.bsum.reserve((uint64_t)A.nstr * (A.nblocks + 1) * 8);
+      S.boff.reserve((uint64_t)A.nstr * (A.nblocks + 1) * 8);
+      A.spos = S.spos.as<uint64_t>();
+      A.slen = S.slen.as<uint32_t>();
+      A.bsum = S.bsum.as<uint64_t>();
+      A.boff = S.boff.as<uint64_t>();
+      if (nrows == 0) DQ_CUDA(cudaMemsetAsync(S.boff.ptr, 0, (uint64_t)A.nstr * 8, st));
     }
     DQ_CUDA(cudaEventRecord(ev.e[8], st));
     DQ_CUDA(launch_import_parse(A, st));
@@ -1600,7 +1677,7 @@ int dq_table_import_text(dq_ctx* ctx, const char* name, const char* text, uint64
     tm.kernel_launches += nrows ? 1 + (A.nstr ? 1 : 0) : 0;
     std::vector<uint64_t> totals(A.nstr, 0);
     uint64_t bad = ~0ull;
-    DQ_CUDA(cudaMemcpyAsync(&bad, err.ptr, 8, cudaMemcpyDeviceToHost, st));
+    DQ_CUDA(cudaMemcpyAsync(&bad, S.err.ptr, 8, cudaMemcpyDeviceToHost, st));
     for (int j = 0; j < A.nstr; ++j)
       DQ_CUDA(cudaMemcpyAsync(&totals[j], A.boff + (uint64_t)j * (A.nblocks + 1) + A.nblocks, 8,
                               cudaMemcpyDeviceToHost, st));
@@ -1614,11 +1691,22 @@ int dq_table_import_text(dq_ctx* ctx, const char* name, const char* text, uint64
       throw DqError(DQ_ERR_INVALID, std::string("import of ") + name + ": line " + std::to_string(row + 1) + where +
                                         ": " + import_reason(why));
     }
+    // the string heaps: a second slab
+    size_t heap_bytes = 0;
+    for (int j = 0; j < A.nstr; ++j) heap_bytes += DevBuf::span_of(totals[j]);
+    std::shared_ptr<DevBuf> heaps;
+    if (old_heap && old_heap->bytes >= heap_bytes) {
+      heaps = old_heap;
+    } else {
+      heaps = std::make_shared<DevBuf>();
+      if (A.nstr) heaps->alloc(heap_bytes);
+    }
+    at = 0;
     for (int j = 0; j < A.nstr; ++j) {
       ColRec& c = t.cols[str_col[j]];
       c.nchars = totals[j];
-      c.data->alloc(totals[j]);
-      c.offsets->alloc((nrows + 1) * 8);
+      c.data = DevBuf::view(heaps, at, totals[j]);
+      at += DevBuf::span_of(totals[j]);
       A.sheap[j] = c.data->as<uint8_t>();
       A.soff[j] = c.offsets->as<uint64_t>();
       if (nrows == 0) DQ_CUDA(cudaMemsetAsync(c.offsets->ptr, 0, 8, st));
@@ -1629,6 +1717,7 @@ int dq_table_import_text(dq_ctx* ctx, const char* name, const char* text, uint64
     tm.kernel_launches += nrows && A.nstr ? 1 : 0;
     DQ_CUDA(cudaStreamSynchronize(st));
     ctx->tables[name] = std::move(t);
+    guard.done = true;
     *nrows_out = (int64_t)nrows;
     float ms = 0;
     auto span = [&](int a, int b) {

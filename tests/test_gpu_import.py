@@ -166,10 +166,64 @@ def _random_text(n, seed):
 
 
 def test_random_text_across_tiles(engine):
+    import torch
     text = _random_text(60_000, 11)
     assert len(text) > 20 * 16384
     fields = [("k", T.INT), ("p", T.DECIMAL, 2), ("c", T.CHAR), ("s", T.STRING), ("f", T.FLOAT), ("d", T.DATE)]
     check_same(engine, text, fields)
+    want = T.parse(text, fields)
+    # device text: read in place (aligned) and copied (a view one byte in)
+    buf = torch.zeros(len(text) + 1, dtype=torch.uint8)
+    buf[1:] = torch.frombuffer(bytearray(text), dtype=torch.uint8)
+    dev = buf.cuda()
+    for view in (dev[1:].clone(), dev[1:]):
+        assert engine.import_text("t_dev", view, fields) == 60_000
+        assert read_all(engine, "t_dev", fields) == want
+
+
+def test_fast_path_boundaries(engine):
+    """Values around the 16-byte window, the int32 range and 18 decimal digits,
+    at every alignment of the field within a 16-byte chunk."""
+    ints = [b"0", b"-0", b"+7", b"-", b"+", b"2147483647", b"-2147483648", b"2147483648", b"-2147483649",
+            b"0000000000000001", b"00000000000000001", b"-000000000000042", b" 5", b"5 ", b"1 2"]
+    decs = [b"0.04", b"12345678901234.5", b"1234567890123456", b"123456789012345.6789", b".5", b"-.", b"7.",
+            b"99999999999999.99", b"999999999999999.9", b"1,25", b" 3.1", b"3.1 "]
+    dates = [b"1998-12-01", b"1998-12-01T00:00", b"1998-12-01T00:00:0", b" 1998-12-01", b"1998-12-01 "]
+    lines = []
+    for pad in range(16):
+        for v in ints:
+            for d in decs:
+                lines.append(b"%s|%s|%s|%s|\n" % (b"x" * pad, v, d, dates[(pad + len(v)) % len(dates)]))
+    text = b"".join(lines)
+    fields = [("s", T.STRING), ("k", T.INT), ("p", T.DECIMAL, 2), ("d", T.DATE)]
+    # rows whose value is out of range fail the whole import: check those one line at a time
+    good = []
+    for ln in lines:
+        try:
+            T.parse(ln, fields)
+            good.append(ln)
+        except T.TextImportError:
+            with pytest.raises(Exception):
+                engine.import_text("t_fast", ln, fields)
+    check_same(engine, b"".join(good), fields)
+
+
+def test_reimport_reuses_and_failure_drops(engine):
+    """A table replaced by a new import of the same name: smaller, larger, then
+    a failing import (which leaves no table of that name)."""
+    from dogqc_b200._lib import DqError
+    fields = [("k", T.INT), ("s", T.STRING), ("d", T.DATE)]
+    big = _random_text(3000, 5)
+    big_fields = [("k", T.INT), ("p", T.DECIMAL, 2), ("c", T.CHAR), ("s", T.STRING), ("f", T.FLOAT), ("d", T.DATE)]
+    small = b"".join(b"%d|%s|1998-01-%02d|\n" % (i, b"ab" * (i % 7), i % 28 + 1) for i in range(500))
+    for text, fl in ((big, big_fields), (small, fields), (big, big_fields), (big, big_fields)):
+        n = engine.import_text("t_re", text, fl)
+        assert n == len(T.lines_of(text))
+        assert read_all(engine, "t_re", fl) == T.parse(text, fl)
+    with pytest.raises(DqError):
+        engine.import_text("t_re", small + b"x|y|z|\n", fields)
+    with pytest.raises(DqError):
+        engine.read_column("t_re", "k", ctype_of(T.INT))
 
 
 def _import_database(engine, db):
