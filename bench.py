@@ -655,7 +655,7 @@ def run_import(args, world, rank, local):
                 "how": "dq_table_import_text from pinned host memory, host wall time of the call"},
         "roofline": {"bound": "hbm", "kernel": "imp_parse_kernel", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "algorithmic_bytes": alg, "traffic": None},
+                     "algorithmic_bytes": alg, "traffic": load_profile_traffic()},
         "gpu_launches": int(t["kernel_launches"]) * args.steps,
         "clocks": clocks.summary(),
     }

@@ -588,17 +588,38 @@ __global__ void __launch_bounds__(kImpRows) imp_strings_kernel(const ImpArgs A) 
     const uint64_t wstart = wincl - len;
     const uint64_t wtotal = __shfl_sync(0xffffffffu, wincl, 31);
     uint8_t* dst = A.sheap[j] + __shfl_sync(0xffffffffu, off, 0);
-    for (uint64_t b0 = 0; b0 < wtotal; b0 += 32) {
-      const uint64_t b = b0 + lane;
-      int row = 0;
+    // The rows of a warp are consecutive lines: with the run and the lines'
+    // span below 4 GB (always, short of multi-GB lines) the search works on
+    // 32-bit values, one shuffle a step.
+    const uint64_t src0 = __shfl_sync(0xffffffffu, src, 0);
+    const bool narrow = __all_sync(0xffffffffu, wincl < (1ull << 32) && (len == 0 || src - src0 < (1ull << 32)));
+    if (narrow) {
+      const uint32_t ws32 = (uint32_t)wstart, wt32 = (uint32_t)wtotal;
+      const uint32_t rel = len ? (uint32_t)(src - src0) - ws32 : 0u;  // source offset minus run offset
+      for (uint32_t b0 = 0; b0 < wt32; b0 += 32) {
+        const uint32_t b = b0 + lane;
+        int row = 0;
 #pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-        const uint64_t s = __shfl_sync(0xffffffffu, wstart, row + step);
-        if (s <= b) row += step;
+        for (int step = 16; step > 0; step >>= 1) {
+          const uint32_t st = __shfl_sync(0xffffffffu, ws32, row + step);
+          if (st <= b) row += step;
+        }
+        const uint32_t d = __shfl_sync(0xffffffffu, rel, row);
+        if (b < wt32) dst[b] = *text_at(A.text, src0 + (uint32_t)(b + d));
       }
-      const uint64_t rs = __shfl_sync(0xffffffffu, wstart, row);
-      const uint64_t rsrc = __shfl_sync(0xffffffffu, src, row);
-      if (b < wtotal) dst[b] = *text_at(A.text, rsrc + (b - rs));
+    } else {
+      for (uint64_t b0 = 0; b0 < wtotal; b0 += 32) {
+        const uint64_t b = b0 + lane;
+        int row = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const uint64_t st = __shfl_sync(0xffffffffu, wstart, row + step);
+          if (st <= b) row += step;
+        }
+        const uint64_t rs = __shfl_sync(0xffffffffu, wstart, row);
+        const uint64_t rsrc = __shfl_sync(0xffffffffu, src, row);
+        if (b < wtotal) dst[b] = *text_at(A.text, rsrc + (b - rs));
+      }
     }
   }
 }

@@ -12,6 +12,11 @@ size header (dogqc/include/mappedmalloc.h).
 This script writes a seeded table as ``.tbl`` text, runs the reference importer
 on it here (it needs only g++ and the reference's headers, no GPU), reads the
 column files back and stores text and values in ``tests/golden/import_ref.json``.
+It also keeps the reference's database directory for the first 200 lines
+(column files and ``dbschema.pickle``) as ``tests/golden/mmdb_ref/``, the
+fixture of the column-file reader; the pickle's ``dateformat`` entry (the
+schema's date parser as C source) is dropped so that no reference code is
+committed.
 
 Usage: ``python oracle/ref_import.py`` (reads the reference at
 $DOGQC_REFERENCE, default /root/reference).
@@ -19,6 +24,7 @@ $DOGQC_REFERENCE, default /root/reference).
 import json
 import os
 import shutil
+import subprocess
 import sys
 import tempfile
 from collections import OrderedDict
@@ -29,6 +35,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 REF = os.environ.get("DOGQC_REFERENCE", "/root/reference")
 OUT = os.path.join(REPO, "tests", "golden", "import_ref.json")
+MMDB_OUT = os.path.join(REPO, "tests", "golden", "mmdb_ref")
+MMDB_ROWS = 200
 
 
 def make_text(n=3000, seed=20261203 + 9):
@@ -97,7 +105,54 @@ def main():
         json.dump({"text": text, "rows": n, "columns": vals}, fh, separators=(",", ":"))
         fh.write("\n")
     print("wrote", OUT, n, "rows")
+    # the reference's generator keeps state between imports: the second one runs in its own process
+    subprocess.run([sys.executable, os.path.abspath(__file__), "--mmdb"], check=True)
+
+
+def write_mmdb_fixture():
+    """The reference's database directory for the first 200 lines of the text."""
+    sys.path.insert(0, REF)
+    from dogqc import dbio
+    from dogqc.types import Type
+    from query.schema.tpch import tpchSchema
+    small = "".join(make_text().splitlines(True)[:MMDB_ROWS])
+    schema = {"dateformat": tpchSchema["dateformat"],
+              "imp": {"name": "imp", "size": 0, "numColumns": 5,
+                      "attributes": OrderedDict([("k", Type.INT), ("d", Type.DATE), ("c", Type.CHAR),
+                                                 ("f", Type.FLOAT), ("s", Type.STRING)])}}
+    work = tempfile.mkdtemp(prefix="dq_mmdb_")
+    cwd = os.getcwd()
+    try:
+        csv = os.path.join(work, "csv")
+        db = os.path.join(work, "mmdb")
+        os.makedirs(csv)
+        with open(os.path.join(csv, "imp.tbl"), "w") as fh:
+            fh.write(small)
+        src = os.path.join(work, "src")
+        os.makedirs(src)
+        os.symlink(os.path.join(REF, "dogqc"), os.path.join(work, "dogqc"))
+        os.chdir(src)
+        dbio.dbAccess(schema, db, csv, doReload=True)
+        shutil.rmtree(MMDB_OUT, ignore_errors=True)
+        os.makedirs(MMDB_OUT)
+        for f in sorted(os.listdir(db)):
+            shutil.copy2(os.path.join(db, f), os.path.join(MMDB_OUT, f))
+        # the schema pickle carries the schema's date parser as C source: drop that entry
+        import pickle
+        spath = os.path.join(MMDB_OUT, "dbschema.pickle")
+        with open(spath, "rb") as fh:
+            sch = pickle.load(fh)
+        sch.pop("dateformat", None)
+        with open(spath, "wb") as fh:
+            pickle.dump(sch, fh, protocol=pickle.HIGHEST_PROTOCOL)
+    finally:
+        os.chdir(cwd)
+        shutil.rmtree(work, ignore_errors=True)
+    print("wrote", MMDB_OUT)
 
 
 if __name__ == "__main__":
-    main()
+    if "--mmdb" in sys.argv:
+        write_mmdb_fixture()
+    else:
+        main()

@@ -226,6 +226,27 @@ def test_reimport_reuses_and_failure_drops(engine):
         engine.read_column("t_re", "k", ctype_of(T.INT))
 
 
+def test_mmdb_directory_and_text_agree(engine):
+    """The reference importer's column files loaded onto the device, and the
+    same lines imported as text: equal columns."""
+    from dogqc_b200 import _lib as L
+    from dogqc_b200 import importer
+    mmdb = os.path.join(os.path.dirname(GOLDEN), "mmdb_ref")
+    e = engine
+    sizes = importer.load_mmdb(e, mmdb)
+    assert sizes == {"imp": 200}
+    with open(GOLDEN) as fh:
+        g = json.load(fh)
+    text = "".join(g["text"].splitlines(True)[:200]).encode()
+    fields = [("k", T.INT), ("d", T.DATE), ("c", T.CHAR), ("f", T.DECIMAL, 2), ("s", T.STRING)]
+    e.import_text("imp_txt", text, fields)
+    for name, kind in (("k", T.INT), ("d", T.DATE), ("c", T.CHAR)):
+        assert e.read_column("imp", name, ctype_of(kind)).tolist() == e.read_column("imp_txt", name, ctype_of(kind)).tolist()
+    assert e.read_column("imp", "f", L.U64).view(np.int64).tolist() == e.read_column("imp_txt", "f", L.I64).tolist()
+    a, b = e.read_column("imp", "s", L.STR), e.read_column("imp_txt", "s", L.STR)
+    assert a[0].tobytes() == b[0].tobytes() and a[1].tolist() == b[1].tolist()
+
+
 def _import_database(engine, db):
     from dogqc_b200 import importer
     for name, t in db.tables.items():

@@ -119,3 +119,41 @@ def test_importer_field_mapping():
     assert importer.fields_for(sch, floats="binary32")[3] == ("d", L.TEXT_FLOAT)
     assert [k for k in (T.INT, T.DATE, T.CHAR, T.DECIMAL, T.STRING, T.SKIP, T.FLOAT)] == \
         [L.TEXT_INT, L.TEXT_DATE, L.TEXT_CHAR, L.TEXT_DECIMAL, L.TEXT_STRING, L.TEXT_SKIP, L.TEXT_FLOAT]
+
+
+MMDB = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mmdb_ref")
+
+
+def test_mmdb_reader_matches_reference_directory():
+    """The reference importer's own column files (first 200 lines of the golden
+    text) read back: the same values its reader maps."""
+    from dogqc_b200 import importer
+    g = golden()
+    cols = g["columns"]
+    db = importer.read_mmdb(MMDB)
+    t = db.tables["imp"]
+    assert t.size == 200
+    assert t.columns["k"].tolist() == cols["k"][:200]
+    assert t.columns["d"].tolist() == cols["d"][:200]
+    assert t.columns["c"].tolist() == cols["c"][:200]
+    assert [t.columns["s"].get(i).decode() for i in range(200)] == cols["s"][:200]
+    text = "".join(g["text"].splitlines(True)[:200]).encode()
+    skip = (None, T.SKIP)
+    exact = T.parse(text, [skip, skip, skip, ("f", T.DECIMAL, 2), skip])["f"]
+    assert t.columns["f"].view(np.int64).tolist() == exact          # binary32 rounded back to cents
+    bits = importer.read_mmdb(MMDB, floats="bits").tables["imp"].columns["f"]
+    assert bits.view(np.float32).tolist() == np.array(cols["f"][:200], np.float32).tolist()
+
+
+def test_schema_unpickler_refuses_other_classes(tmp_path):
+    import pickle
+    from dogqc_b200 import importer
+
+    class Evil(object):
+        def __reduce__(self):
+            return (os.getcwd, ())
+    d = tmp_path / "db"
+    d.mkdir()
+    (d / "dbschema.pickle").write_bytes(pickle.dumps({"t": Evil()}))
+    with pytest.raises(pickle.UnpicklingError):
+        importer.read_schema(str(d))
