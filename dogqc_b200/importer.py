@@ -115,7 +115,7 @@ def read_mmdb(dbpath, schema=None, floats="decimal", scale=2):
     schema = schema or read_schema(dbpath)
     tables = []
     for key, t in schema.items():
-        if key == "dateformat":
+        if not isinstance(t, dict) or "attributes" not in t:
             continue
         name, n = t["name"], int(t["size"])
         cols, types = OrderedDict(), OrderedDict()
@@ -125,7 +125,9 @@ def read_mmdb(dbpath, schema=None, floats="decimal", scale=2):
             if tn == "STRING":
                 offs = _column_file(path + "_offset", np.uint64, n + 1)
                 chars = np.fromfile(path + "_char", dtype=np.uint8, offset=8)[:int(offs[-1]) if n else 0]
-                cols[attr] = StringColumn(chars, offs)
+                lens = np.diff(offs)
+                width = int(lens[0]) if n and np.all(lens == lens[0]) else 0  # fixed width: read without offsets
+                cols[attr] = StringColumn(chars, offs, width)
                 types[attr] = Type.STRING
             elif tn in ("FLOAT", "DOUBLE"):
                 v = _column_file(path, np.float32, n)
