@@ -276,15 +276,39 @@ __device__ __forceinline__ bool fast_date(const ImpText& T, uint64_t i, uint64_t
   return true;
 }
 
+// The bytes of a field in order: one aligned 4-byte load per four bytes, then
+// shifts (the padded text holds every word a line touches).
+struct ByteStream {
+  const ImpText& T;
+  uint64_t pos;
+  uint32_t w = 0, left = 0;
+  __device__ __forceinline__ ByteStream(const ImpText& t, uint64_t i) : T(t), pos(i) {}
+  __device__ __forceinline__ uint32_t next() {
+    if (left == 0) {
+      const uint32_t sh = (uint32_t)pos & 3u;
+      w = __ldg(reinterpret_cast<const uint32_t*>(text_at(T, pos - sh))) >> (8 * sh);
+      left = 4 - sh;
+    }
+    const uint32_t c = w & 0xffu;
+    w >>= 8;
+    --left;
+    ++pos;
+    return c;
+  }
+};
+
 // csv.h parse_signed_integer for int, throw_on_overflow (csv.h:945-995), on
-// the trimmed field.
-__device__ int32_t parse_int(LineReader& rd, uint64_t& i, uint64_t end, uint32_t delim, int32_t& out) {
+// the trimmed field: the magnitude is checked against the bound after every
+// digit, which is the reference's test (x > (max - y) / 10 is 10x + y > max),
+// so an overflow is reported at the same digit.
+__device__ int32_t parse_int(const ImpText& T, uint64_t& i, uint64_t end, uint32_t delim, int32_t& out) {
+  ByteStream bs(T, i);
   int state = 0;  // 0: before the value, 1: in it, 2: trailing spaces
+  uint64_t lim = 2147483647ull, u = 0;
   bool neg = false;
-  int32_t x = 0;
   for (;; ++i) {
     if (i >= end) return kImpTooFew;
-    const uint32_t c = rd.at(i);
+    const uint32_t c = bs.next();
     if (c == delim) break;
     if (c == ' ') {
       if (state == 1) state = 2;
@@ -295,36 +319,33 @@ __device__ int32_t parse_int(LineReader& rd, uint64_t& i, uint64_t end, uint32_t
       state = 1;
       if (c == '-') {
         neg = true;
+        lim = 2147483648ull;
         continue;
       }
       if (c == '+') continue;
     }
-    if (c < '0' || c > '9') return kImpNoDigit;
-    const int32_t y = (int32_t)c - '0';
-    if (neg) {
-      if (x < (INT32_MIN + y) / 10) return kImpOverflow;
-      x = 10 * x - y;
-    } else {
-      if (x > (INT32_MAX - y) / 10) return kImpOverflow;
-      x = 10 * x + y;
-    }
+    const uint32_t y = c - '0';
+    if (y > 9) return kImpNoDigit;
+    u = u * 10 + y;
+    if (u > lim) return kImpOverflow;
   }
-  out = x;
+  out = neg ? (int32_t)(0u - (uint32_t)u) : (int32_t)u;
   return 0;
 }
 
 // Exact fixed point: [+-]digits[(.|,)digits] scaled by 10^scale, digits past
 // `scale` dropped (the grammar of csv.h parse_float without the exponent).
-__device__ int32_t parse_decimal(LineReader& rd, uint64_t& i, uint64_t end, uint32_t delim, int scale,
+__device__ int32_t parse_decimal(const ImpText& T, uint64_t& i, uint64_t end, uint32_t delim, int scale,
                                  int64_t& out) {
+  ByteStream bs(T, i);
   int state = 0;  // 0: before, 1: integer digits, 3: fraction digits, 2: trailing spaces
   bool neg = false;
   uint64_t m = 0;
   int fd = 0;
-  constexpr uint64_t kMax = (uint64_t)INT64_MAX;
+  constexpr uint64_t kMax = (uint64_t)INT64_MAX, kTenth = kMax / 10, kLast = kMax % 10;
   for (;; ++i) {
     if (i >= end) return kImpTooFew;
-    const uint32_t c = rd.at(i);
+    const uint32_t c = bs.next();
     if (c == delim) break;
     if (c == ' ') {
       if (state != 0) state = 2;
@@ -343,17 +364,17 @@ __device__ int32_t parse_decimal(LineReader& rd, uint64_t& i, uint64_t end, uint
       continue;
     }
     if (c == 'e' || c == 'E') return kImpExponent;
-    if (c < '0' || c > '9') return kImpNoDigit;
+    const uint32_t y = c - '0';
+    if (y > 9) return kImpNoDigit;
     if (state == 3) {
       if (fd >= scale) continue;
       ++fd;
     }
-    const uint64_t y = c - '0';
-    if (m > (kMax - y) / 10) return kImpOverflow;
+    if (m > kTenth || (m == kTenth && y > kLast)) return kImpOverflow;
     m = 10 * m + y;
   }
   for (; fd < scale; ++fd) {
-    if (m > kMax / 10) return kImpOverflow;
+    if (m > kTenth) return kImpOverflow;
     m *= 10;
   }
   out = neg ? -(int64_t)m : (int64_t)m;
@@ -365,14 +386,15 @@ __device__ int32_t parse_decimal(LineReader& rd, uint64_t& i, uint64_t end, uint
 // is compiled without contraction), the sign applied last.  Exponents beyond
 // four digits are rejected (the reference saturates them and, for the most
 // negative one, does not terminate).
-__device__ int32_t parse_float(LineReader& rd, uint64_t& i, uint64_t end, uint32_t delim, uint32_t& out) {
+__device__ int32_t parse_float(const ImpText& T, uint64_t& i, uint64_t end, uint32_t delim, uint32_t& out) {
+  ByteStream bs(T, i);
   int state = 0;  // 0: before, 1: integer digits, 3: fraction digits, 4: exponent, 2: trailing spaces
   bool neg = false, eneg = false, esign = false;
   float x = 0.f, pos = 1.f;
   int e = 0;
   for (;; ++i) {
     if (i >= end) return kImpTooFew;
-    const uint32_t c = rd.at(i);
+    const uint32_t c = bs.next();
     if (c == delim) break;
     if (c == ' ') {
       if (state != 0) state = 2;
@@ -467,19 +489,19 @@ __global__ void __launch_bounds__(kImpRows, 6) imp_parse_kernel(const ImpArgs A)
     switch (F.kind) {
       case kTxtInt: {
         int32_t v = 0;
-        why = parse_int(rd, q, end, delim, v);
+        why = parse_int(A.text, q, end, delim, v);
         if (!why) static_cast<int32_t*>(F.out)[r] = v;
         break;
       }
       case kTxtDecimal: {
         int64_t v = 0;
-        why = parse_decimal(rd, q, end, delim, F.scale, v);
+        why = parse_decimal(A.text, q, end, delim, F.scale, v);
         if (!why) static_cast<int64_t*>(F.out)[r] = v;
         break;
       }
       case kTxtFloat: {
         uint32_t v = 0;
-        why = parse_float(rd, q, end, delim, v);
+        why = parse_float(A.text, q, end, delim, v);
         if (!why) static_cast<uint32_t*>(F.out)[r] = v;
         break;
       }
