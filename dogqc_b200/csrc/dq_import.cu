@@ -44,13 +44,10 @@ constexpr int kScanItems = 8;
 __device__ __forceinline__ uint32_t zero_bytes(uint32_t x) {
   return ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x | 0x7F7F7F7Fu);
 }
-__device__ __forceinline__ uint64_t zero_bytes64(uint64_t x) {
-  return ~(((x & 0x7F7F7F7F7F7F7F7Full) + 0x7F7F7F7F7F7F7F7Full) | x | 0x7F7F7F7F7F7F7F7Full);
-}
 
-// Newlines of a 16-byte chunk as a 16-bit mask (byte k -> bit k): the flags at
-// bits 7, 15, 23, 31 of each word move to bits 24..27 by one multiply whose
-// partial products do not overlap.
+// Zero-byte flags of a word (bits 7, 15, 23, 31) as a nibble (byte k -> bit
+// k): the flags move to bits 24..27 by one multiply whose partial products do
+// not overlap.  Four nibbles make a 16-byte chunk's mask.
 __device__ __forceinline__ uint32_t nibble_of(uint32_t z) { return (((z >> 7) & 0x01010101u) * 0x01020408u) >> 24; }
 __device__ __forceinline__ uint32_t newline_mask16(const uint4& v) {
   return nibble_of(zero_bytes(v.x ^ 0x0a0a0a0au)) | (nibble_of(zero_bytes(v.y ^ 0x0a0a0a0au)) << 4) |
@@ -168,41 +165,32 @@ __global__ void __launch_bounds__(kScanThreads) imp_scan_kernel(const uint64_t* 
 
 // ---------------------------------------------------------------- parse --
 
-// A thread's view of its line: the 16-byte chunk last loaded, in registers.
+// A thread's view of its line: the 16-byte chunk last loaded, in registers,
+// with the mask of its delimiter bytes (computed once per chunk: the fields
+// of a line share its chunks).
 struct LineReader {
   ImpText text;
+  uint32_t pat;           // the delimiter in every byte
   uint64_t base = ~0ull;
   uint4 v;
+  uint32_t dm = 0;        // bit k: byte k of the chunk is the delimiter
 
   __device__ __forceinline__ void fetch(uint64_t i) {
     const uint64_t b = i & ~15ull;
     if (b != base) {
       v = ld_chunk(text_at(text, b));
       base = b;
+      dm = nibble_of(zero_bytes(v.x ^ pat)) | (nibble_of(zero_bytes(v.y ^ pat)) << 4) |
+           (nibble_of(zero_bytes(v.z ^ pat)) << 8) | (nibble_of(zero_bytes(v.w ^ pat)) << 12);
     }
   }
-  __device__ __forceinline__ uint32_t at(uint64_t i) {
-    fetch(i);
-    const uint32_t k = (uint32_t)i & 15u;
-    const uint32_t w = k < 8 ? (k < 4 ? v.x : v.y) : (k < 12 ? v.z : v.w);
-    return (w >> ((k & 3) * 8)) & 0xffu;
-  }
   // First byte equal to the delimiter in [i, end); `end` if there is none.
-  // `pat`: the delimiter in every byte of a 64-bit word.
-  __device__ __forceinline__ uint64_t find(uint64_t i, uint64_t end, uint64_t pat) {
+  __device__ __forceinline__ uint64_t find(uint64_t i, uint64_t end) {
     while (i < end) {
       fetch(i);
-      uint64_t z0 = zero_bytes64((((uint64_t)v.y << 32) | v.x) ^ pat);
-      uint64_t z1 = zero_bytes64((((uint64_t)v.w << 32) | v.z) ^ pat);
-      const uint32_t sh = (uint32_t)i & 15u;
-      if (sh >= 8) {
-        z0 = 0;
-        z1 &= ~0ull << (8 * (sh - 8));
-      } else {
-        z0 &= ~0ull << (8 * sh);
-      }
-      if (z0 | z1) {
-        const uint64_t q = base + (z0 ? (uint32_t)(__ffsll(z0) - 1) >> 3 : 8 + ((uint32_t)(__ffsll(z1) - 1) >> 3));
+      const uint32_t m = dm >> (i & 15);
+      if (m) {
+        const uint64_t q = i + (__ffs(m) - 1);
         return q < end ? q : end;
       }
       i = base + 16;
@@ -211,17 +199,20 @@ struct LineReader {
   }
 };
 
+// One byte of the text (trimming and the line's last byte: a load that hits
+// L1, without disturbing the reader's chunk).
+__device__ __forceinline__ uint32_t byte_at(const ImpText& T, uint64_t i) { return __ldg(text_at(T, i)); }
+
 // Field [i, q) of a line ending at `end`, with the spaces around it trimmed
 // to [cs, ce).  Returns a reason code, 0 when the delimiter was found.
-__device__ __forceinline__ int32_t field_bounds(LineReader& rd, uint64_t i, uint64_t end, uint32_t delim,
-                                                uint64_t pat, uint64_t& q, uint64_t& cs, uint64_t& ce) {
-  q = rd.find(i, end, pat);
+__device__ __forceinline__ int32_t field_bounds(LineReader& rd, uint64_t i, uint64_t end, uint64_t& q,
+                                                uint64_t& cs, uint64_t& ce) {
+  q = rd.find(i, end);
   if (q >= end) return kImpTooFew;
   cs = i;
   ce = q;
-  while (cs < ce && rd.at(cs) == ' ') ++cs;
-  while (ce > cs && rd.at(ce - 1) == ' ') --ce;
-  (void)delim;
+  while (cs < ce && byte_at(rd.text, cs) == ' ') ++cs;
+  while (ce > cs && byte_at(rd.text, ce - 1) == ' ') --ce;
   return 0;
 }
 
@@ -461,20 +452,19 @@ __global__ void __launch_bounds__(kImpRows, 6) imp_parse_kernel(const ImpArgs A)
   const uint64_t r = (uint64_t)blockIdx.x * kImpRows + threadIdx.x;
   const bool live = r < A.nrows;
   const uint32_t delim = A.delim;
-  const uint64_t pat = delim * 0x0101010101010101ull;
-  LineReader rd{A.text};
+  LineReader rd{A.text, delim * 0x01010101u};
   uint64_t pos = 0, end = 0;
   int32_t bad = 0, bad_field = 0;
   bool shape_bad = false;  // the line has too few delimiters: that outranks a bad value
   if (live) {
     pos = r ? A.line_end[r - 1] + 1 : 0;
     end = r < A.nlines ? A.line_end[r] : A.nbytes;
-    if (end > pos && rd.at(end - 1) == '\r') --end;  // csv.h:479, Windows line breaks
+    if (end > pos && byte_at(A.text, end - 1) == '\r') --end;  // csv.h:479, Windows line breaks
   }
   for (int f = 0; f < A.nfields; ++f) {
     if (!live || shape_bad) continue;
     if (bad) {  // after a bad value only the delimiters are checked (csv.h splits the line first)
-      const uint64_t q = rd.find(pos, end, pat);
+      const uint64_t q = rd.find(pos, end);
       if (q >= end) {
         bad = kImpTooFew;
         bad_field = f;
@@ -507,13 +497,13 @@ __global__ void __launch_bounds__(kImpRows, 6) imp_parse_kernel(const ImpArgs A)
       }
       case kTxtDate: {
         uint32_t v = 0;
-        const uint64_t d = rd.find(pos, end, pat);
+        const uint64_t d = rd.find(pos, end);
         if (d < end && fast_date(A.text, pos, d, v)) {
           q = d;
           static_cast<uint32_t*>(F.out)[r] = v;
           break;
         }
-        why = field_bounds(rd, pos, end, delim, pat, q, cs, ce);
+        why = field_bounds(rd, pos, end, q, cs, ce);
         if (!why && ce - cs < 10) why = kImpShortDate;
         if (!why) {
           // toDate: digits at 0-3, 5-6, 8-9 weighted 10^7 .. 10^0 (query/schema/tpch.py:9-20)
@@ -521,19 +511,19 @@ __global__ void __launch_bounds__(kImpRows, 6) imp_parse_kernel(const ImpArgs A)
           uint32_t d = 0;
 #pragma unroll
           for (int k = 0; k < 10; ++k)
-            if (kW[k]) d += (rd.at(cs + k) - 48u) * kW[k];
+            if (kW[k]) d += (byte_at(A.text, cs + k) - 48u) * kW[k];
           static_cast<uint32_t*>(F.out)[r] = d;
         }
         break;
       }
       case kTxtChar: {
-        why = field_bounds(rd, pos, end, delim, pat, q, cs, ce);
+        why = field_bounds(rd, pos, end, q, cs, ce);
         if (!why && ce - cs != 1) why = kImpNotChar;  // csv.h:920-928
-        if (!why) static_cast<int8_t*>(F.out)[r] = (int8_t)rd.at(cs);
+        if (!why) static_cast<int8_t*>(F.out)[r] = (int8_t)byte_at(A.text, cs);
         break;
       }
       case kTxtString: {
-        why = field_bounds(rd, pos, end, delim, pat, q, cs, ce);
+        why = field_bounds(rd, pos, end, q, cs, ce);
         if (!why) {
           A.spos[(uint64_t)F.str * A.nrows + r] = cs;
           A.slen[(uint64_t)F.str * A.nrows + r] = (uint32_t)(ce - cs);
@@ -541,13 +531,13 @@ __global__ void __launch_bounds__(kImpRows, 6) imp_parse_kernel(const ImpArgs A)
         break;
       }
       default: {  // kTxtSkip
-        q = rd.find(pos, end, pat);
+        q = rd.find(pos, end);
         if (q >= end) why = kImpTooFew;
         break;
       }
     }
     if (why && why != kImpTooFew) {
-      q = rd.find(q, end, pat);  // the field's own delimiter, past the bad byte
+      q = rd.find(q, end);  // the field's own delimiter, past the bad byte
       if (q >= end) why = kImpTooFew;
     }
     if (why) {
@@ -557,7 +547,7 @@ __global__ void __launch_bounds__(kImpRows, 6) imp_parse_kernel(const ImpArgs A)
     }
     pos = q + 1;
   }
-  if (live && !shape_bad && rd.find(pos, end, pat) < end) {  // csv.h:864-866: one delimiter too many
+  if (live && !shape_bad && rd.find(pos, end) < end) {  // csv.h:864-866: one delimiter too many
     bad = kImpTooMany;
     bad_field = A.nfields;
   }
