@@ -28,7 +28,7 @@ WIDTH = {I8: 1, I32: 4, U32: 4, I64: 8, U64: 8}
 # dq_slot_kind
 SLOT_COL, SLOT_REG, SLOT_GATHER, SLOT_AGGKEY, SLOT_AGGVAL, SLOT_STR = 1, 2, 3, 4, 5, 6
 # dq_op_kind
-OP_ARITH, OP_CMP, OP_LOGIC, OP_CAST, OP_SELECT, OP_LIKE, OP_STREQ = 1, 2, 3, 4, 5, 6, 7
+OP_ARITH, OP_CMP, OP_LOGIC, OP_CAST, OP_SELECT, OP_LIKE, OP_STREQ, OP_STRREF = 1, 2, 3, 4, 5, 6, 7, 8
 OP_FILTER, OP_PROBE, OP_EXPAND = 10, 11, 12
 OP_AGG, OP_BUILD, OP_MM_COUNT, OP_MM_SCATTER, OP_EMIT = 20, 21, 22, 23, 24
 ADD, SUB, MUL, DIV, MOD = 1, 2, 3, 4, 5
@@ -179,6 +179,7 @@ EXPORTS = {
     "dq_result_rows": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "dq_result_ncols": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "dq_result_column": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_void_p)]),
+    "dq_result_string_heap": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
     "dq_result_free": (None, [C.c_void_p]),
     "dq_join_agg_noalloc": (C.c_int, [C.POINTER(dq_join_agg_args), C.c_void_p]),
     "dq_plan_prepare_tuned": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_desc), C.POINTER(dq_tuning),

@@ -261,6 +261,41 @@ __device__ __forceinline__ uint64_t key_tag(const DevRes& R, const uint64_t* k) 
   return fmix64(h) & 0x7fffffffffffffffull;
 }
 
+// String references (source << 48 | row): the bytes behind them, their hash
+// and equality.  Group keys of string type hash and compare the bytes, so two
+// rows with equal strings meet in one group whatever rows they came from.
+__device__ __forceinline__ void str_ref_at(const DevPipe& P, uint64_t ref, const uint8_t*& ptr, int& len) {
+  str_at(P.strsrc[ref >> kStrRefShift], (int64_t)(ref & kStrRefRow), ptr, len);
+}
+
+__device__ __forceinline__ uint64_t str_ref_hash(const DevPipe& P, uint64_t ref) {
+  const uint8_t* p;
+  int n;
+  str_ref_at(P, ref, p, n);
+  uint64_t h = 0xcbf29ce484222325ull ^ (uint64_t)n;  // FNV-1a over the bytes, then a finaliser
+  for (int j = 0; j < n; ++j) h = (h ^ p[j]) * 0x100000001b3ull;
+  return fmix64(h);
+}
+
+__device__ __forceinline__ bool str_ref_eq(const DevPipe& P, uint64_t a, uint64_t b) {
+  if (a == b) return true;
+  const uint8_t *pa, *pb;
+  int na, nb;
+  str_ref_at(P, a, pa, na);
+  str_ref_at(P, b, pb, nb);
+  return str_eq(pa, na, pb, nb);
+}
+
+// Hash tag of wide keys some of which are string references.
+__device__ __forceinline__ uint64_t key_tag_str(const DevPipe& P, const DevRes& R, const uint64_t* k) {
+  uint64_t h = 0x9e3779b97f4a7c15ull;
+  for (int i = 0; i < R.nkeys; ++i) {
+    const uint64_t v = R.key_ctype[i] == DQ_STR ? str_ref_hash(P, k[i]) : k[i];
+    h = fmix64(h ^ v) + 0x632be59bd9b4e019ull * (i + 1);
+  }
+  return fmix64(h) & 0x7fffffffffffffffull;
+}
+
 // Unique join table: returns slot index or -1.
 __device__ __forceinline__ int64_t unique_find(const DevRes& R, uint64_t tag, const uint64_t* k) {
   if (R.packed && tag == kEmpty) return R.slots[R.cap * R.words] == 0 ? (int64_t)R.cap : -1;
@@ -354,7 +389,10 @@ __device__ __noinline__ int64_t agg_slot_global(const DevPipe& P, const DevRes& 
     if (t == tag) {
       __threadfence();
       bool eq = true;
-      for (int i = 0; i < R.nkeys; ++i) eq &= ((volatile uint64_t*)s)[R.key_word + i] == k[i];
+      for (int i = 0; i < R.nkeys; ++i) {
+        const uint64_t a = ((volatile uint64_t*)s)[R.key_word + i];
+        eq &= R.key_ctype[i] == DQ_STR ? str_ref_eq(P, a, k[i]) : a == k[i];
+      }
       if (eq) return (int64_t)idx;
     }
     idx = (idx + 1 == R.cap) ? 0 : idx + 1;

@@ -35,8 +35,13 @@ struct DevStr {           // string column, read in place
   const uint8_t* chars;
   const uint64_t* offsets;
   int32_t width;          // > 0: fixed-width strings
-  int32_t pad;
+  int32_t sid;            // its index in the plan's string sources (string references)
 };
+
+// A string value carried as a 64-bit reference: the plan's string source << 48
+// | the row (group keys and output columns hold these; the bytes stay in place).
+constexpr int kStrRefShift = 48;
+constexpr uint64_t kStrRefRow = (1ull << kStrRefShift) - 1;
 
 struct DevSlot {
   int8_t kind, level, ctype, width;
@@ -138,6 +143,8 @@ struct DevPipe {
   int32_t off_flags;           // per-row probe results
   int32_t off_stash;
   int32_t smem_bytes;
+  const DevStr* strsrc;        // the plan's string sources (string references)
+  int32_t nstrsrc;
   int32_t* status;
   uint32_t* tile_counter;      // dynamic tile scheduler
   uint64_t* scratch_ll;        // misc device counters

@@ -130,6 +130,7 @@ void op_reads(const DevPipe& P, const dq_op& op, std::vector<int>& out) {
       break;
     case DQ_OP_LIKE:
     case DQ_OP_STREQ:
+    case DQ_OP_STRREF:
     case DQ_OP_FILTER:
       add(op.a);
       break;
@@ -340,6 +341,13 @@ struct Gen {
             "(sp_, sn_, " + pat + ", " + plen + ");");
           --ind;
           L("}");
+          break;
+        }
+        case DQ_OP_STRREF: {  // the string's plan-wide reference: source << 48 | row
+          const DevSlot& sl = slot(op.a);
+          if (sl.kind != DQ_SLOT_STR) throw Error("string reference of a non-string slot");
+          L(V(op.dst) + " = ((uint64_t)(uint32_t)P.strs[" + num(sl.src) + "].sid << kStrRefShift) | (uint64_t)" + row +
+            ";");
           break;
         }
         case DQ_OP_FILTER:
@@ -726,6 +734,12 @@ struct Gen {
   }
 
   // ---------------------------------------------------------------- sinks --
+  static bool has_str_key(const DevRes& R) {
+    for (int i = 0; i < R.nkeys; ++i)
+      if (R.key_ctype[i] == DQ_STR) return true;
+    return false;
+  }
+
   void sink_agg(const dq_op& op, const std::string& act) {
     const int r = op.res;
     const DevRes& R = P.res[r];
@@ -745,6 +759,7 @@ struct Gen {
     ++ind;
     std::string k = keys(op, r, op.list, op.nlist);
     if (R.packed) L("const uint64_t tag_ = " + packed_tag(r, op.list, op.nlist) + ";");
+    else if (has_str_key(R)) L("const uint64_t tag_ = key_tag_str(P, " + res(r) + ", " + k + ");");
     else L("const uint64_t tag_ = key_tag(" + res(r) + ", " + k + ");");
     auto global = [&]() {
       if (R.packed) {

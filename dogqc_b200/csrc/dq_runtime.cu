@@ -51,6 +51,10 @@ cudaError_t launch_import_lines(const ImpText& T, uint64_t ntiles, uint64_t* til
 cudaError_t launch_import_line_ends(const ImpText& T, uint64_t ntiles, const uint64_t* tile_off, uint64_t* line_end,
                                     cudaStream_t st);
 cudaError_t launch_import_parse(const ImpArgs& A, cudaStream_t st);
+cudaError_t launch_str_ref_offsets(const uint64_t* refs, uint64_t n, const DevStr* src, uint64_t* lens,
+                                   uint64_t* offs, int sms, cudaStream_t st);
+cudaError_t launch_str_ref_copy(const uint64_t* refs, uint64_t n, const DevStr* src, const uint64_t* offs,
+                                uint8_t* heap, int sms, cudaStream_t st);
 cudaError_t launch_import_strings(const ImpArgs& A, cudaStream_t st);
 }  // namespace dq
 
@@ -88,7 +92,8 @@ int ctype_width(int t) {
     case DQ_I32:
     case DQ_U32: return 4;
     case DQ_I64:
-    case DQ_U64: return 8;
+    case DQ_U64:
+    case DQ_STR: return 8;  // as a value, a string is a 64-bit reference (source << 48 | row)
     default: return 0;
   }
 }
@@ -220,7 +225,8 @@ struct PipeRec {
 struct dq_result {
   int64_t nrows = 0;
   std::vector<int> ctypes;
-  std::vector<std::vector<uint8_t>> cols;
+  std::vector<std::vector<uint8_t>> cols;   // DQ_STR: nrows + 1 uint64 offsets into heaps[j]
+  std::vector<std::vector<uint8_t>> heaps;
 };
 
 // How a plan is laid out: standalone (the default) or as one instance of a
@@ -241,6 +247,8 @@ struct dq_plan {
   DevBuf status, counters;
   dq_plan_timing timing{};
   std::vector<cudaEvent_t> events;
+  std::vector<DevStr> str_src;  // string columns the pipelines read: string references index these
+  DevBuf str_src_dev;
 };
 
 // One pipeline of a batch: a generated kernel over all instances.
@@ -339,6 +347,8 @@ void upload_column(dq_ctx* ctx, ColRec& rec, const dq_column& c, int64_t nrows, 
 }
 
 bool keys_packed(int nkeys, const int8_t* kt) {
+  for (int i = 0; i < nkeys; ++i)
+    if (kt[i] == DQ_STR) return false;  // string keys hash and compare their bytes
   if (nkeys == 0) return true;
   if (nkeys == 1) return true;
   if (nkeys == 2) return ctype_width(kt[0]) <= 4 && ctype_width(kt[1]) <= 4;
@@ -423,8 +433,7 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       R.cursor = r.cursor.as<uint64_t>();
       r.pay.clear();
       for (int j = 0; j < d.npay; ++j) {
-        if (d.pay_ctype[j] == DQ_STR) throw DqError(DQ_ERR_UNSUPPORTED, "string output columns");
-        r.pay.emplace_back(new DevBuf());
+        r.pay.emplace_back(new DevBuf());  // a string column holds references (8 bytes a row)
         r.pay.back()->alloc(cap * ctype_width(d.pay_ctype[j]));
         R.pay[j] = r.pay.back()->as<uint8_t>();
       }
@@ -462,6 +471,7 @@ void slot_reads(const dq_pipeline& d, const dq_op& op, std::vector<int>& out) {
       break;
     case DQ_OP_LIKE:
     case DQ_OP_STREQ:
+    case DQ_OP_STRREF:
     case DQ_OP_FILTER:
       add(op.a);
       break;
@@ -573,6 +583,13 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
         s.chars = c->data->as<uint8_t>();
         s.offsets = c->offsets ? c->offsets->as<uint64_t>() : nullptr;
         s.width = c->width;
+        s.sid = -1;
+        for (size_t k = 0; k < plan->str_src.size(); ++k)
+          if (plan->str_src[k].chars == s.chars && plan->str_src[k].offsets == s.offsets) s.sid = (int32_t)k;
+        if (s.sid < 0) {
+          s.sid = (int32_t)plan->str_src.size();
+          plan->str_src.push_back(s);
+        }
         col_map[i] = P.nstr++;
       } else {
         DevCol& dc = P.cols[P.ncols];
@@ -788,6 +805,11 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
 
   // generated kernel (default), else the prebuilt tile or row kernel
   p.jit = !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) && !plan->opts.batch_member;
+  if (!p.jit)
+    for (int k = 0; k < p.desc.nops; ++k)
+      if (p.desc.ops[k].kind == DQ_OP_STRREF)
+        throw DqError(DQ_ERR_UNSUPPORTED, "string group keys and string result columns run on generated plan kernels "
+                                          "only (not DQ_CFG_NO_JIT / DQ_CFG_ROW_KERNEL, batches or served batches)");
   int occ = 1;
   int64_t rows_per_cta = tile;
   if (plan->opts.batch_member) {
@@ -941,9 +963,31 @@ dq_result* read_result(dq_plan* plan, cudaStream_t st) {
   if (n > o.dev.cap) n = o.dev.cap;
   std::unique_ptr<dq_result> res(new dq_result());
   res->nrows = (int64_t)n;
+  res->heaps.resize(o.desc.npay);
   for (int j = 0; j < o.desc.npay; ++j) {
     int w = ctype_width(o.desc.pay_ctype[j]);
     res->ctypes.push_back(o.desc.pay_ctype[j]);
+    if (o.desc.pay_ctype[j] == DQ_STR) {
+      // references -> offsets and a heap, gathered on the device
+      DevBuf lens, offs, heap;
+      lens.alloc(std::max<uint64_t>(n, 1) * 8);
+      offs.alloc((n + 1) * 8);
+      const uint64_t* refs = reinterpret_cast<const uint64_t*>(o.dev.pay[j]);
+      DQ_CUDA(launch_str_ref_offsets(refs, n, plan->str_src_dev.as<DevStr>(), lens.as<uint64_t>(), offs.as<uint64_t>(),
+                                     plan->ctx->sms, st));
+      res->cols.emplace_back((size_t)(n + 1) * 8);
+      DQ_CUDA(cudaMemcpyAsync(res->cols.back().data(), offs.ptr, (n + 1) * 8, cudaMemcpyDeviceToHost, st));
+      DQ_CUDA(cudaStreamSynchronize(st));
+      uint64_t total = 0;
+      memcpy(&total, res->cols.back().data() + n * 8, 8);
+      heap.alloc(std::max<uint64_t>(total, 1));
+      DQ_CUDA(launch_str_ref_copy(refs, n, plan->str_src_dev.as<DevStr>(), offs.as<uint64_t>(), heap.as<uint8_t>(),
+                                  plan->ctx->sms, st));
+      res->heaps[j].resize(total);
+      if (total) DQ_CUDA(cudaMemcpyAsync(res->heaps[j].data(), heap.ptr, total, cudaMemcpyDeviceToHost, st));
+      DQ_CUDA(cudaStreamSynchronize(st));
+      continue;
+    }
     res->cols.emplace_back((size_t)n * w);
     if (n) DQ_CUDA(cudaMemcpyAsync(res->cols.back().data(), o.dev.pay[j], (size_t)n * w, cudaMemcpyDeviceToHost, st));
   }
@@ -969,7 +1013,18 @@ uint64_t plan_bytes(const dq_plan* plan) {
 
 // Re-derives every pipeline's copy of the resource descriptors.
 void refresh_pipelines(dq_plan* plan) {
+  plan->str_src.clear();
   for (auto& pp : plan->pipes) setup_pipeline(plan, *pp);
+  // the string sources every pipeline may resolve references against
+  const size_t n = plan->str_src.size();
+  if (plan->str_src_dev.bytes != std::max<size_t>(n, 1) * sizeof(DevStr) || (!plan->str_src_dev.ptr && !t_offline))
+    plan->str_src_dev.alloc(std::max<size_t>(n, 1) * sizeof(DevStr));
+  if (n && !plan->ctx->offline)
+    DQ_CUDA(cudaMemcpy(plan->str_src_dev.ptr, plan->str_src.data(), n * sizeof(DevStr), cudaMemcpyHostToDevice));
+  for (auto& pp : plan->pipes) {
+    pp->dev.strsrc = plan->str_src_dev.as<DevStr>();
+    pp->dev.nstrsrc = (int32_t)n;
+  }
 }
 
 // Lays out a plan's resources and pipelines (the caller holds the context lock
@@ -1880,6 +1935,14 @@ int dq_result_column(dq_result* r, int32_t col, int32_t* ctype, const void** dat
   return DQ_OK;
 }
 
+int dq_result_string_heap(dq_result* r, int32_t col, const void** chars, uint64_t* nchars) {
+  if (!r || col < 0 || col >= (int32_t)r->cols.size() || !chars || !nchars) return DQ_ERR_INVALID;
+  if (r->ctypes[col] != DQ_STR) return DQ_ERR_INVALID;
+  *chars = r->heaps[col].data();
+  *nchars = r->heaps[col].size();
+  return DQ_OK;
+}
+
 void dq_result_free(dq_result* r) { delete r; }
 
 int dq_plan_prepare_tuned(dq_ctx* ctx, const dq_plan_desc* desc, const dq_tuning* tuning, dq_plan** out) {
@@ -2087,7 +2150,7 @@ uint64_t estimate_bytes(dq_ctx* ctx, const dq_plan_desc& d) {
   for (int i = 0; i < d.nres; ++i) {
     const dq_resource& r = d.res[i];
     const uint64_t cap = (uint64_t)std::max<int64_t>(r.capacity, 16);
-    const bool packed = r.nkeys <= 1 || (r.nkeys == 2 && ctype_width(r.key_ctype[0]) <= 4 && ctype_width(r.key_ctype[1]) <= 4);
+    const bool packed = keys_packed(r.nkeys, r.key_ctype);
     const uint64_t keyw = packed ? 0 : r.nkeys;
     uint64_t widths = 0;
     for (int j = 0; j < r.npay && j < DQ_MAX_PAY; ++j) widths += ctype_width(r.pay_ctype[j]);
@@ -3096,9 +3159,18 @@ int srv_wait(dq_server* s, uint64_t ticket, dq_result** out, dq_request_info* in
 
 extern "C" {
 
+// Served results are copied back raw; string references would need the gather.
+void reject_string_results(const dq_plan_desc& d) {
+  for (int i = 0; i < d.npipes; ++i)
+    for (int k = 0; k < d.pipes[i].nops; ++k)
+      if (d.pipes[i].ops[k].kind == DQ_OP_STRREF)
+        throw DqError(DQ_ERR_UNSUPPORTED, "served requests with string group keys or string result columns");
+}
+
 int dq_server_submit(dq_server* s, const dq_plan_desc* desc, uint64_t* ticket) {
   if (!s || !desc || !ticket) return DQ_ERR_INVALID;
   return guarded(s->ctx, [&]() {
+    reject_string_results(*desc);
     std::shared_ptr<DescCopy> d = copy_desc(desc);
     uint64_t est;
     {
@@ -3117,6 +3189,7 @@ int dq_server_replay(dq_server* s, int32_t nq, const dq_plan_desc* queries, int6
   return guarded(s->ctx, [&]() {
     std::vector<std::shared_ptr<DescCopy>> descs;
     std::vector<uint64_t> est;
+    for (int q = 0; q < nq; ++q) reject_string_results(queries[q]);
     for (int q = 0; q < nq; ++q) descs.push_back(copy_desc(&queries[q]));
     {
       std::lock_guard<std::mutex> lk(s->ctx->mu);

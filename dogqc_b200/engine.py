@@ -37,7 +37,9 @@ class Result(object):
             parts = []
             for n, t, c in zip(self.names, self.ctypes, self.columns):
                 v = c[i]
-                if t == L.I8:
+                if t == L.STR:
+                    s = v.decode(errors="replace")
+                elif t == L.I8:
                     s = chr(int(v) & 0xFF)
                 elif t == L.U64:
                     s = "%10d" % int(v)
@@ -65,6 +67,17 @@ def _take_result(res, names):
             t = C.c_int32()
             ptr = C.c_void_p()
             L.check(lib.dq_result_column(res, j, C.byref(t), C.byref(ptr)))
+            if t.value == L.STR:  # offsets into a heap: the strings as bytes
+                offs = np.frombuffer((C.c_uint8 * ((n.value + 1) * 8)).from_address(ptr.value), np.uint64)
+                hp, nch = C.c_void_p(), C.c_uint64()
+                L.check(lib.dq_result_string_heap(res, j, C.byref(hp), C.byref(nch)))
+                heap = C.string_at(hp.value, nch.value) if nch.value else b""
+                col = np.empty(n.value, dtype=object)
+                for i in range(n.value):
+                    col[i] = heap[int(offs[i]):int(offs[i + 1])]
+                cols.append(col)
+                types.append(t.value)
+                continue
             dt = np.dtype(NP_DTYPE[t.value])
             if n.value:
                 buf = (C.c_uint8 * (n.value * dt.itemsize)).from_address(ptr.value)

@@ -147,6 +147,7 @@ class Pipe(object):
         self.att = {}           # attribute id -> slot index
         self.level = 0
         self.lazy = {}          # attribute id -> callable creating its slot
+        self.strref = {}        # attribute id -> register holding its string reference
 
     def slot(self, kind, level, ctype, src=0, res=-1):
         self.slots.append(dict(kind=kind, level=level, ctype=ctype, src=src, res=res))
@@ -193,6 +194,20 @@ class Pipe(object):
             else:
                 raise Unsupported("attribute %s (%d) is not available in this pipeline" % (attr.name, attr.id))
         return self.att[attr.id]
+
+    def value_slot(self, attr):
+        """The slot of ``attr`` as a value: a scanned string becomes its 64-bit
+        reference (plan string source << 48 | row), computed first thing in the
+        pipeline so refill and expansion carry it like any other value."""
+        s = self.attr_slot(attr)
+        if self.slots[s]["kind"] != L.SLOT_STR:
+            return s
+        if attr.id not in self.strref:
+            r = self.slot(L.SLOT_REG, 0, "str")
+            self.op(L.OP_STRREF, dst=r, a=s, ctype=L.STR)
+            self.ops.insert(0, self.ops.pop())
+            self.strref[attr.id] = r
+        return self.strref[attr.id]
 
     def clone_for_rebuild(self):
         """Fresh copy of the source part (used to run a build pipeline twice)."""
@@ -625,8 +640,7 @@ class Lowering(object):
         if len(groups) > L.MAX_KEYS:
             raise Unsupported("more than %d grouping attributes" % L.MAX_KEYS)
         gtypes = [lang_type(g.dataType) for g in groups]
-        if "str" in gtypes:
-            raise Unsupported("grouping by strings")
+        # string group keys: their references, hashed and compared by their bytes
         aggs = [(id, inId, _tname(red)) for id, (inId, red) in node.aggregateTuples.items()]
         # one accumulator per distinct (reduction, input): an AVG shares the SUM
         # of its input with a SUM aggregate of the same attribute and divides by
@@ -648,7 +662,7 @@ class Lowering(object):
         reds = [L.RED_COUNT if k[0] == "COUNT" else k[0] for k in accs]
         rid = self.new_res(Res(L.RES_AGG, nkeys=len(groups), key_ctype=gtypes,
                                agg_red=reds, capacity=cap, group_hint=numgroups))
-        kl, kn = pipe.list_([pipe.attr_slot(g) for g in groups])
+        kl, kn = pipe.list_([pipe.value_slot(g) for g in groups])
         inputs = []
         for red, inId in accs:
             if red == "COUNT":
@@ -681,16 +695,16 @@ class Lowering(object):
     def materialize(self, node, pipe):
         atts = list(node.outRelation.values())
         types = [lang_type(a.dataType) for a in atts]
-        if "str" in types:
-            raise Unsupported("string result columns")
         temp = _tname(node.matType) == "TEMPTABLE"
+        if "str" in types and temp:
+            raise Unsupported("string attributes in temp tables")
         cap = max(int(getattr(node, "tupleNum", 0)), 1024)
         if type(node.child).__name__ == "Aggregation":
             cap = max(cap, self.res[pipe.source_res].capacity + 1)
         rid = self.new_res(Res(L.RES_OUTPUT, pay_ctype=types, capacity=cap,
                                name=node.table["name"] if temp else None,
                                columns=[a.id for a in atts]))
-        sl, sn = pipe.list_([pipe.attr_slot(a) for a in atts])
+        sl, sn = pipe.list_([pipe.value_slot(a) for a in atts])
         pipe.op(L.OP_EMIT, res=rid, list=sl, nlist=sn)
         self.finish(pipe)
         if temp:

@@ -348,9 +348,57 @@ def plan_c8(alg, scal, Type, Reduction, flag_cut=50, nation_cut=5):
     return [tmp, dist], cfg
 
 
-GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5, "c7": gen_c5, "c8": gen_c5}
+C9_MODES = [b"REG AIR", b"AIR", b"RAIL", b"SHIP", b"TRUCK", b"MAIL", b"FOB"]
+C9_INSTRUCT = [b"DELIVER IN PERSON", b"COLLECT COD", b"NONE", b"TAKE BACK RETURN"]
+
+
+def gen_c9(scale=1.0, seed=BASE_SEED + 9):
+    """Q12-shaped: lineitem with variable-length string attributes (ship mode,
+    ship instruction), a key, a measure and a receipt date."""
+    n = _n(6_000_000, scale)
+    r = _rng(seed)
+    mode = r.integers(0, len(C9_MODES), n)
+    instr = r.integers(0, len(C9_INSTRUCT), n)
+    cols = {
+        "l_orderkey": r.integers(1, 6_000_000, n, dtype=np.int32),
+        "l_extendedprice": r.integers(90_000, 10_500_001, n, dtype=np.int64).astype(np.uint64),
+        "l_receiptdate": (EPOCH_1992 + r.integers(0, DATE_RANGE, n)).astype(np.uint32),
+        "l_shipmode": StringColumn.from_list([C9_MODES[i] for i in mode]),
+        "l_shipinstruct": StringColumn.from_list([C9_INSTRUCT[i] for i in instr]),
+    }
+    types = {"l_orderkey": Type.INT, "l_extendedprice": Type.FLOAT, "l_receiptdate": Type.DATE,
+             "l_shipmode": Type.STRING, "l_shipinstruct": Type.STRING}
+    return Database([Table("lineitem", cols, types)])
+
+
+def plan_c9(alg, scal, Type, Reduction, cutoff=EPOCH_1992 + DATE_RANGE // 2):
+    """Rows received before the cutoff, per (ship mode, ship instruction):
+    count and revenue -- grouping by two strings, both in the result."""
+    sel = alg.selection(
+        scal.SmallerExpr(scal.AttrExpr("l_receiptdate"), scal.ConstExpr(str(cutoff), Type.DATE)),
+        alg.scan("lineitem"))
+    agg = alg.aggregation(
+        ["l_shipmode", "l_shipinstruct"],
+        [(Reduction.COUNT, "", "line_count"), (Reduction.SUM, "l_extendedprice", "revenue")],
+        sel)
+    cfg = {sel.opId: {"selectivity": 0.5}, agg.opId: {"numgroups": len(C9_MODES) * len(C9_INSTRUCT)}}
+    return agg, cfg
+
+
+def plan_c9p(alg, scal, Type, Reduction, key_cut=20_000):
+    """A projection carrying strings: the rows with a small order key, their
+    key and ship mode."""
+    sel = alg.selection(
+        scal.SmallerExpr(scal.AttrExpr("l_orderkey"), scal.ConstExpr(str(key_cut), Type.INT)),
+        alg.scan("lineitem"))
+    proj = alg.projection(["l_orderkey", "l_shipmode"], sel)
+    return proj, {sel.opId: {"selectivity": key_cut / 6_000_000}}
+
+
+GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5, "c7": gen_c5, "c8": gen_c5,
+              "c9": gen_c9, "c9p": gen_c9}
 PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5, "c7": plan_c7,
-         "c8": plan_c8}
+         "c8": plan_c8, "c9": plan_c9, "c9p": plan_c9p}
 
 
 def build(name, alg, scale=1.0, **kw):

@@ -212,6 +212,9 @@ typedef enum {
     DQ_OP_SELECT = 5,    /* dst = a ? b : c (CASE arm)                         */
     DQ_OP_LIKE = 6,      /* dst = a LIKE pattern[res]                          */
     DQ_OP_STREQ = 7,     /* dst = a == pattern[res] (string constant)          */
+    DQ_OP_STRREF = 8,    /* dst = reference to string slot a's value: the     */
+                         /* plan's string source << 48 | row (a U64 value that */
+                         /* group keys and output columns carry)               */
     DQ_OP_FILTER = 10,   /* keep rows with a != 0                              */
     DQ_OP_PROBE = 11,    /* unique-HT probe (res); sub: dq_join                */
     DQ_OP_EXPAND = 12,   /* multimap probe (res) opening level+1               */
@@ -426,6 +429,9 @@ int dq_result_ncols(dq_result* r, int32_t* ncols);
 /* Host pointer to column `col` (nrows values of its C type; strings as
  * nrows (start,end) byte offsets into `dq_result_heap`).                      */
 int dq_result_column(dq_result* r, int32_t col, int32_t* ctype, const void** data);
+/* A DQ_STR result column: dq_result_column gives nrows+1 uint64 offsets into
+ * this heap of `*nchars` bytes.                                              */
+int dq_result_string_heap(dq_result* r, int32_t col, const void** chars, uint64_t* nchars);
 void dq_result_free(dq_result* r);
 
 /* ------------------------------------------------- allocation-free join -- */

@@ -7,8 +7,13 @@ widths do not enter the checksum.
 import hashlib
 
 
+def _canon(v):
+    return bytes(v) if isinstance(v, (bytes, bytearray)) else int(v)
+
+
 def canonical_rows(rows):
-    return sorted(tuple(int(v) for v in r) for r in rows)
+    """Rows as sorted tuples: integers, and strings as bytes."""
+    return sorted(tuple(_canon(v) for v in r) for r in rows)
 
 
 def canonical_checksum(rows):

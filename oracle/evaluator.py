@@ -547,10 +547,24 @@ class Oracle(object):
         groups = list(node.groupAttributes.values())
         aggs = [(id, inId, tname(red)) for id, (inId, red) in node.aggregateTuples.items()]
         partial_keys, partial_vals = [], []
+        # string keys: each distinct byte string gets a code (first seen, first code)
+        codes, strs_of = {}, []
+
+        def key_values(g, v):
+            if lang_type(g.dataType) != "str":
+                return conv(v, lang_type(g.dataType))
+            out = np.empty(len(v), np.int64)
+            for i in range(len(v)):
+                b = v.get(i)
+                if b not in codes:
+                    codes[b] = len(strs_of)
+                    strs_of.append(b)
+                out[i] = codes[b]
+            return out
         for f in self.stream(node.child):
             if f.n == 0:
                 continue
-            keys = [conv(f[g.id], lang_type(g.dataType)) for g in groups]
+            keys = [key_values(g, f[g.id]) for g in groups]
             if groups:
                 stacked = np.stack([k.astype(np.int64) for k in keys], axis=1)
                 uniq, inv = np.unique(stacked, axis=0, return_inverse=True)
@@ -605,7 +619,13 @@ class Oracle(object):
                 else:
                     cols[id] = np.zeros(ng, np.uint64)
         for j, g in enumerate(groups):
-            cols[g.id] = uniq[:, j].astype(NP[lang_type(g.dataType)])
+            if lang_type(g.dataType) == "str":
+                vals = [strs_of[int(c)] for c in uniq[:, j]]
+                heap = np.frombuffer(b"".join(vals), np.uint8) if vals else np.zeros(0, np.uint8)
+                ends = np.cumsum([len(b) for b in vals]).astype(np.int64) if vals else np.zeros(0, np.int64)
+                cols[g.id] = Strs(heap, ends - np.array([len(b) for b in vals], np.int64), ends)
+            else:
+                cols[g.id] = uniq[:, j].astype(NP[lang_type(g.dataType)])
         count_id = node.countAttr.id if hasattr(node, "countAttr") else None
         for id in node.avgAggregates:
             cnt = cols[count_id].astype(np.int64).astype(np.uint64)
