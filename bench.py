@@ -67,6 +67,10 @@ WORKLOADS = {
            {"workload": "temp_table_two_roots", "customer_rows": 150_000, "order_rows": 1_500_000,
             "orders_filter": "flag < 50 (50%)", "customers_filter": "nation < 5 (20%)",
             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c9": ("rows/s (filter + group by two variable-length strings, string result columns, input rows per second)",
+           {"workload": "string_group_by", "rows": 6_000_000, "filter": "receiptdate < middle (50%)",
+            "groups": 28, "keys": "ship mode, ship instruction (variable-length strings)",
+            "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
     "c5": ("rows/s (left outer join on a multimap + two aggregations, input rows of both tables per second)",
            {"workload": "outer_join_two_aggregations", "customer_rows": 150_000, "order_rows": 1_500_000,
             "orders_filter": "flag >= 2 (98%)", "customers_without_orders": "1/3",

@@ -371,7 +371,7 @@ def gen_c9(scale=1.0, seed=BASE_SEED + 9):
     return Database([Table("lineitem", cols, types)])
 
 
-def plan_c9(alg, scal, Type, Reduction, cutoff=EPOCH_1992 + DATE_RANGE // 2):
+def plan_c9(alg, scal, Type, Reduction, cutoff=EPOCH_1992 + DATE_RANGE // 2, groups_hint=None):
     """Rows received before the cutoff, per (ship mode, ship instruction):
     count and revenue -- grouping by two strings, both in the result."""
     sel = alg.selection(
@@ -381,7 +381,8 @@ def plan_c9(alg, scal, Type, Reduction, cutoff=EPOCH_1992 + DATE_RANGE // 2):
         ["l_shipmode", "l_shipinstruct"],
         [(Reduction.COUNT, "", "line_count"), (Reduction.SUM, "l_extendedprice", "revenue")],
         sel)
-    cfg = {sel.opId: {"selectivity": 0.5}, agg.opId: {"numgroups": len(C9_MODES) * len(C9_INSTRUCT)}}
+    cfg = {sel.opId: {"selectivity": 0.5},
+           agg.opId: {"numgroups": groups_hint or len(C9_MODES) * len(C9_INSTRUCT)}}
     return agg, cfg
 
 

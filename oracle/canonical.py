@@ -8,7 +8,9 @@ import hashlib
 
 
 def _canon(v):
-    return bytes(v) if isinstance(v, (bytes, bytearray)) else int(v)
+    if isinstance(v, (bytes, bytearray)):
+        return bytes(v)
+    return v if isinstance(v, str) else int(v)
 
 
 def canonical_rows(rows):

@@ -41,14 +41,48 @@ def write_mmdb(db, path):
                 _write(base, col)
 
 
-def parse_result(path):
-    """Return (column names, list of row tuples of ints) from a reference result file."""
+STRING_FIELD = 10  # stringPrint's default width (dogqc/include/util.h:18-30)
+
+
+def render_string(b):
+    """A string as the reference's result file shows it: right-aligned in 10
+    characters, cut to its first 10 (stringPrint, dogqc/include/util.h:18-30)."""
+    s = b.decode("latin-1") if isinstance(b, (bytes, bytearray)) else b
+    return (" " * max(0, STRING_FIELD - len(s)) + s)[:STRING_FIELD]
+
+
+def _parse_typed(line, ncols, str_cols):
+    """One result line whose string columns are fixed 10-character fields with
+    no separator after them; every other value is followed by two spaces."""
+    row, i = [], 0
+    for j in range(ncols):
+        if j in str_cols:
+            row.append(line[i:i + STRING_FIELD])
+            i += STRING_FIELD
+            continue
+        while i < len(line) and line[i] == " ":
+            i += 1
+        k = i
+        while k < len(line) and line[k] != " ":
+            k += 1
+        t = line[i:k]
+        row.append(ord(t) if len(t) == 1 and not t.isdigit() and t != "-" else int(t))
+        i = k + 2
+    return tuple(row)
+
+
+def parse_result(path, str_cols=()):
+    """Return (column names, list of row tuples) from a reference result file:
+    ints, and for the columns in ``str_cols`` the 10-character string fields."""
     with open(path, "rb") as f:
         lines = f.read().decode("latin-1").split("\n")
     names = [n.strip() for n in lines[0].split(",") if n.strip()]
     rows = []
     for line in lines[1:]:
         if not line.strip():
+            continue
+        if str_cols:
+            rows.append(_parse_typed(line, len(names), set(str_cols)))
             continue
         toks = line.split()
         if len(toks) != len(names):

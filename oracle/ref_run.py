@@ -68,7 +68,7 @@ def run_case(name, spec, outdir, scratch):
     rec["timing_ms"] = parse_timing(stdout)
     res = os.path.join(work, "queryresult.csv")
     if p.returncode == 0 and os.path.exists(res):
-        names, rows = parse_result(res)
+        names, rows = parse_result(res, spec.get("str_cols", ()))
         rec["columns"] = names
         rec["nrows"] = len(rows)
         rec["checksum"] = canonical_checksum(rows)

@@ -24,3 +24,13 @@ def make_case(spec):
     plan, cfg = workloads.build(spec["workload"], alg, **spec.get("plan_kw", {}))
     plan = alg.resolveAlgebraPlan(plan, cfg)
     return db, alg, plan
+
+
+def reference_rows(rows, spec):
+    """Rows as a golden fixture holds them: sorted lists, and the string
+    columns (``spec["str_cols"]``) as the reference's result file shows them,
+    right-aligned in 10 characters and cut to 10 (oracle/mmdb.py)."""
+    from mmdb import render_string
+    sc = set(spec.get("str_cols", ()))
+    return sorted([render_string(v) if j in sc else int(v) for j, v in enumerate(r)] for r in rows)
+
