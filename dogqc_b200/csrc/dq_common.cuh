@@ -512,6 +512,46 @@ __device__ __forceinline__ int local_group_slot(uint64_t* tags, int ns, uint64_t
   return -1;
 }
 
+// CTA-local group table for hashed keys that include strings: tags, then the
+// keys (string references) of each slot.  A claim publishes the keys before
+// the tag; a match compares the keys (strings by their bytes).  -1 when the
+// table is full or a claim stays unpublished past the wait limit: the caller
+// then aggregates into the global table, whose flush merges by key.
+__device__ __forceinline__ int local_group_slot_keys(const DevPipe& P, const DevRes& R, uint64_t* tags, uint64_t* keys,
+                                                     int ns, uint64_t tag, const uint64_t* k) {
+  uint32_t idx = slot_of(tag, (uint32_t)ns);
+  for (int n = 0; n < ns; ++n) {
+    uint64_t t = ((volatile uint64_t*)tags)[idx];
+    if (t == kEmpty) {
+      const uint64_t old = s_cas64(saddr(&tags[idx]), kEmpty, kBusy);
+      if (old == kEmpty) {
+        for (int i = 0; i < R.nkeys; ++i) ((volatile uint64_t*)keys)[idx * R.nkeys + i] = k[i];
+        __threadfence_block();
+        ((volatile uint64_t*)tags)[idx] = tag;
+        return (int)idx;
+      }
+      t = old;
+    }
+    long long spins = 0;
+    while (t == kBusy && spins < kSpinLimit) {
+      t = ((volatile uint64_t*)tags)[idx];
+      ++spins;
+    }
+    if (t == kBusy) return -1;
+    if (t == tag) {
+      __threadfence_block();
+      bool eq = true;
+      for (int i = 0; i < R.nkeys; ++i) {
+        const uint64_t a = ((volatile uint64_t*)keys)[idx * R.nkeys + i];
+        eq &= R.key_ctype[i] == DQ_STR ? str_ref_eq(P, a, k[i]) : a == k[i];
+      }
+      if (eq) return (int)idx;
+    }
+    idx = (idx + 1 == (uint32_t)ns) ? 0 : idx + 1;
+  }
+  return -1;
+}
+
 // CTA-local table of multimap buckets (the hot buckets of a skewed build side
 // land in it first): kHotSlots bucket ids, kEmpty32 when free.  Returns the
 // bucket's slot, claiming a free one in its window of kHotProbe slots, or -1.

@@ -778,7 +778,8 @@ struct Gen {
     if (agg == AGG_GLOBAL) {
       global();
     } else {
-      L("const int s_ = local_group_slot(ltags, " + num(ns) + ", tag_, " + num(R.nkeys) + ");");
+      if (R.packed) L("const int s_ = local_group_slot(ltags, " + num(ns) + ", tag_, " + num(R.nkeys) + ");");
+      else L("const int s_ = local_group_slot_keys(P, " + res(r) + ", ltags, lkeys, " + num(ns) + ", tag_, " + k + ");");
       L("if (s_ >= 0) {");
       ++ind;
       for (int j = 0; j < R.naggs; ++j) {
@@ -931,14 +932,14 @@ struct Gen {
       return;
     }
     ns = R.smem_slots;
-    if (ns <= 0 || !R.packed || batched) {  // a batched kernel's items change instance
+    if (ns <= 0 || (!R.packed && !has_str_key(R)) || batched) {  // a batched kernel's items change instance
       agg = AGG_GLOBAL;
       ns = 0;
       return;
     }
     // replicate the accumulators per lane (32 copies: lanes of a warp never
     // collide) or per half-warp (16) when the table allows, else one copy
-    const int tags = (ns + 1) * 8;
+    const int tags = (ns + 1) * 8 + (R.packed ? 0 : ns * R.nkeys * 8);  // hashed keys: their values too
     agg = AGG_LOCAL;
     copies = 1;
     for (int c : {32, 16})
@@ -1148,7 +1149,12 @@ struct Gen {
       return;
     }
     L("uint64_t* ltags = reinterpret_cast<uint64_t*>(smem);");
-    L("uint64_t* lacc = ltags + " + num(ns + 1) + ";");
+    if (R.packed) {
+      L("uint64_t* lacc = ltags + " + num(ns + 1) + ";");
+    } else {
+      L("uint64_t* lkeys = ltags + " + num(ns + 1) + ";");
+      L("uint64_t* lacc = lkeys + " + num(ns * R.nkeys) + ";");
+    }
     L("for (int i = tid; i <= " + num(ns) + "; i += " + num(block) + ") ltags[i] = kEmpty;");
     L("for (int i = tid; i < " + num((ns + 1) * R.naggs * copies) + "; i += " + num(block) + ")");
     L("  lacc[i] = ((" + lit(min_mask()) + " >> ((i / " + num(copies) + ") % " + num(R.naggs) +
@@ -1184,7 +1190,7 @@ struct Gen {
     if (copies > 1) L("for (int c_ = 1; c_ < " + num(copies) + "; ++c_) v_ = red_combine(red_, v_, lacc[i * " +
                       num(copies) + " + c_]);");
     if (R.packed) packed_claim(agg_res, "tg_");
-    else L("const int64_t g_ = agg_slot_global(P, " + rr + ", tg_, nullptr);");
+    else L("const int64_t g_ = agg_slot_global(P, " + rr + ", tg_, lkeys + s_ * " + num(R.nkeys) + ");");
     L("if (g_ >= 0) accumulate(" + rr + ".slots + (uint64_t)g_ * " + num(R.words) + " + " + num(R.val_word) +
       " + j_, red_, v_);");
     --ind;

@@ -399,11 +399,14 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       R.cap = cap;
       r.slots.alloc((cap + 1) * R.words * 8);
       R.slots = r.slots.as<uint64_t>();
-      if (d.kind == DQ_RES_AGG && R.packed) {
+      bool str_keys = false;
+      for (int i = 0; i < d.nkeys; ++i) str_keys |= d.key_ctype[i] == DQ_STR;
+      if (d.kind == DQ_RES_AGG && (R.packed || str_keys)) {
+        // CTA-local table (generated kernels only for string keys: they store the keys too)
         uint64_t want = std::max<int64_t>(d.group_hint, 1) * 2;
         uint64_t ns = 16;
         while (ns < want) ns <<= 1;
-        uint64_t bytes = (ns + 1) * (1 + d.naggs) * 8;
+        uint64_t bytes = (ns + 1) * (1 + d.naggs) * 8 + (str_keys ? ns * d.nkeys * 8 : 0);
         if (d.nkeys == 0) ns = 1, bytes = 2 * (1 + d.naggs) * 8;
         R.smem_slots = bytes <= 24 * 1024 ? (int)ns : 0;
       }
