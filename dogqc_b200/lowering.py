@@ -438,6 +438,8 @@ class Lowering(object):
                     ta, tb = tb, ta
                 if ta != "str" or tb != "strconst":
                     raise Unsupported("string equality needs an attribute and a constant")
+                if pipe.slots[a]["kind"] != L.SLOT_STR:
+                    raise Unsupported("string comparisons on strings carried through a join")
                 d = pipe.reg("i32")
                 pipe.op(L.OP_STREQ, dst=d, a=a, res=pipe.pattern(b.data))
                 return d
@@ -459,7 +461,7 @@ class Lowering(object):
         if k == "LikeExpr":
             s = self.expr(pipe, e.leftChild)
             p = self.expr(pipe, e.rightChild)
-            if not isinstance(p, Pattern) or self.ctype_of(pipe, s) != "str":
+            if not isinstance(p, Pattern) or self.ctype_of(pipe, s) != "str" or pipe.slots[s]["kind"] != L.SLOT_STR:
                 raise Unsupported("LIKE needs a string attribute and a constant pattern")
             d = pipe.reg("i32")
             pipe.op(L.OP_LIKE, dst=d, a=s, res=pipe.pattern(p.data))
@@ -561,8 +563,6 @@ class Lowering(object):
                 # the join reads need not be stored in the payload
                 build_atts = [a for a in build_atts if not (a in bk and a.lastUse <= node.opId)]
             payload = [lang_type(a.dataType) for a in build_atts]
-            if any(t == "str" for t in payload):
-                raise Unsupported("string attributes in join payloads")
             rid = self.new_res(Res(L.RES_UNIQUE, nkeys=len(bk), key_ctype=key_types, pay_ctype=payload,
                                    capacity=cap))
             info = dict(res=rid, unique=True, bk=bk, pk=pk, build_atts=build_atts, passes=["build"])
@@ -573,8 +573,6 @@ class Lowering(object):
                 if keys_in_payload[i] < 0:
                     atts.append(b)
             payload = [lang_type(a.dataType) for a in atts]
-            if any(t == "str" for t in payload):
-                raise Unsupported("string attributes in join payloads")
             if len(payload) > L.MAX_PAY:
                 raise Unsupported("more than %d payload attributes" % L.MAX_PAY)
             rid = self.new_res(Res(L.RES_MULTI, nkeys=len(bk), key_ctype=key_types, pay_ctype=payload,
@@ -592,12 +590,12 @@ class Lowering(object):
         keys = [pipe.attr_slot(a) for a in info["bk"]]
         kl, kn = pipe.list_(keys)
         if info["unique"]:
-            pl, pn = pipe.list_([pipe.attr_slot(a) for a in info["build_atts"]])
+            pl, pn = pipe.list_([pipe.value_slot(a) for a in info["build_atts"]])
             pipe.op(L.OP_BUILD, res=info["res"], list=kl, nlist=kn, list2=pl, nlist2=pn)
         elif info["pass"] == "count":
             pipe.op(L.OP_MM_COUNT, res=info["res"], list=kl, nlist=kn)
         else:
-            pl, pn = pipe.list_([pipe.attr_slot(a) for a in info["build_atts"]])
+            pl, pn = pipe.list_([pipe.value_slot(a) for a in info["build_atts"]])
             pipe.op(L.OP_MM_SCATTER, res=info["res"], list=kl, nlist=kn, list2=pl, nlist2=pn)
         self.finish(pipe)
 

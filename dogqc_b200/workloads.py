@@ -396,10 +396,49 @@ def plan_c9p(alg, scal, Type, Reduction, key_cut=20_000):
     return proj, {sel.opId: {"selectivity": key_cut / 6_000_000}}
 
 
+C10_SEGMENTS = [b"AUTOMOBILE", b"BUILDING", b"FURNITURE", b"HOUSEHOLD", b"MACHINERY"]
+
+
+def gen_c10(scale=1.0, seed=BASE_SEED + 10):
+    """Q10-shaped: customers with a name and a market segment (strings) and
+    their orders."""
+    nc = _n(150_000, scale)
+    no = _n(1_500_000, scale)
+    r = _rng(seed)
+    seg = r.integers(0, len(C10_SEGMENTS), nc)
+    cust = {"c_custkey": (r.permutation(nc) + 1).astype(np.int32),
+            "c_name": StringColumn.from_list([b"Customer#%09d" % (i + 1) for i in range(nc)]),
+            "c_mktsegment": StringColumn.from_list([C10_SEGMENTS[i] for i in seg])}
+    orders = {"o_custkey": r.integers(1, nc + 1, no, dtype=np.int32),
+              "o_totalprice": r.integers(90_000, 50_000_000, no, dtype=np.int64).astype(np.uint64)}
+    return Database([
+        Table("customer", cust, {"c_custkey": Type.INT, "c_name": Type.STRING, "c_mktsegment": Type.STRING}),
+        Table("orders", orders, {"o_custkey": Type.INT, "o_totalprice": Type.FLOAT})])
+
+
+def plan_c10(alg, scal, Type, Reduction):
+    """Orders joined to their customer (unique build), revenue and count per
+    market segment: the group key is a string carried from the build side."""
+    join = alg.join(("c_custkey", "o_custkey"), alg.scan("customer"), alg.scan("orders"))
+    agg = alg.aggregation(["c_mktsegment"],
+                          [(Reduction.SUM, "o_totalprice", "revenue"), (Reduction.COUNT, "", "cnt")], join)
+    return agg, {join.opId: {"multimatch": False, "selectivity": 1.0},
+                 agg.opId: {"numgroups": len(C10_SEGMENTS)}}
+
+
+def plan_c10p(alg, scal, Type, Reduction, price_cut=200_000):
+    """The customer name of every cheap order: a string result from the build side."""
+    sel = alg.selection(scal.SmallerExpr(scal.AttrExpr("o_totalprice"), scal.ConstExpr(str(price_cut), Type.INT)),
+                        alg.scan("orders"))
+    join = alg.join(("c_custkey", "o_custkey"), alg.scan("customer"), sel)
+    proj = alg.projection(["c_name", "o_totalprice"], join)
+    return proj, {sel.opId: {"selectivity": 0.005}, join.opId: {"multimatch": False, "selectivity": 1.0}}
+
+
 GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5, "c7": gen_c5, "c8": gen_c5,
-              "c9": gen_c9, "c9p": gen_c9}
+              "c9": gen_c9, "c9p": gen_c9, "c10": gen_c10, "c10p": gen_c10}
 PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5, "c7": plan_c7,
-         "c8": plan_c8, "c9": plan_c9, "c9p": plan_c9p}
+         "c8": plan_c8, "c9": plan_c9, "c9p": plan_c9p, "c10": plan_c10, "c10p": plan_c10p}
 
 
 def build(name, alg, scale=1.0, **kw):

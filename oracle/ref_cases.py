@@ -31,6 +31,8 @@ CASES = {
     "c8_s": dict(workload="c8", scale=0.01),
     "c9_s": dict(workload="c9", scale=0.002, str_cols=[0, 1], plan_kw={"groups_hint": 256}),
     "c9p_s": dict(workload="c9p", scale=0.002, str_cols=[1]),
+    "c10_s": dict(workload="c10", scale=0.02, str_cols=[0]),
+    "c10p_s": dict(workload="c10p", scale=0.02, str_cols=[0]),
     "c8": dict(workload="c8", scale=1.0),
     # full sizes: row counts, checksums and (small) full results are committed
     "c0": dict(workload="c0", scale=1.0),

@@ -5,7 +5,8 @@ row); group keys of string type hash and compare the bytes behind the
 references, and string result columns are gathered into offsets and a heap on
 the device after the run.  Cases: grouping by two variable-length strings
 (Q12 shape), a projection carrying strings, fixed-width strings, tables that
-came in as text, and the paths that do not take string results (batches,
+came in as text, strings carried from a join's build side (Q10 shape), and
+the paths that do not take string results (batches,
 served requests, the prebuilt kernels) refusing them."""
 import numpy as np
 import pytest
@@ -34,7 +35,8 @@ def run(engine, db, plan):
         p.free()
 
 
-@pytest.mark.parametrize("workload,scale", [("c9", 0.002), ("c9", 0.1), ("c9p", 0.002), ("c9p", 0.1)])
+@pytest.mark.parametrize("workload,scale", [("c9", 0.002), ("c9", 0.1), ("c9p", 0.002), ("c9p", 0.1),
+                                            ("c10", 0.02), ("c10", 1.0), ("c10p", 0.02), ("c10p", 1.0)])
 def test_string_keys_and_results_match_oracle(engine, workload, scale):
     db, alg, plan = make_case({"workload": workload, "scale": scale})
     names, want = run_plan(db, plan)
@@ -42,7 +44,7 @@ def test_string_keys_and_results_match_oracle(engine, workload, scale):
     assert res.names == names
     got = canonical_rows(res.rows())
     assert got == canonical_rows(want)
-    assert all(isinstance(r[0 if workload == "c9" else 1], bytes) for r in got)
+    assert all(isinstance(r[1 if workload == "c9p" else 0], bytes) for r in got)
 
 
 def test_fixed_width_string_keys(engine):
