@@ -71,6 +71,10 @@ WORKLOADS = {
            {"workload": "string_group_by", "rows": 6_000_000, "filter": "receiptdate < middle (50%)",
             "groups": 28, "keys": "ship mode, ship instruction (variable-length strings)",
             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c10": ("rows/s (FK-PK join carrying a string from the build side + group by it, input rows of both tables per second)",
+            {"workload": "join_string_payload_group_by", "customer_rows": 150_000, "order_rows": 1_500_000,
+             "groups": 5, "key": "market segment (a string of the build side)",
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
     "c5": ("rows/s (left outer join on a multimap + two aggregations, input rows of both tables per second)",
            {"workload": "outer_join_two_aggregations", "customer_rows": 150_000, "order_rows": 1_500_000,
             "orders_filter": "flag >= 2 (98%)", "customers_without_orders": "1/3",
