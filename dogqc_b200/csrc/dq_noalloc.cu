@@ -195,19 +195,59 @@ extern "C" int dq_join_agg_noalloc(const dq_join_agg_args* a, void* stream) {
   int st = scratch_on_device(&s);
   if (st != DQ_OK) return st;
   cudaStream_t cs = static_cast<cudaStream_t>(stream);
-  clear_kernel<<<512, kThreads, 0, cs>>>(s);
-  if (a->build_rows > 0)
-    build_kernel<<<(int)((a->build_rows + kThreads - 1) / kThreads < 2048 ? (a->build_rows + kThreads - 1) / kThreads : 2048),
-                   kThreads, 0, cs>>>(s, a->build_key, a->build_filter, a->filter_value, a->build_group, a->build_rows);
-  if (a->probe_rows > 0)
-    probe_kernel<<<(int)((a->probe_rows + kThreads - 1) / kThreads < 4096 ? (a->probe_rows + kThreads - 1) / kThreads : 4096),
-                   kThreads, 0, cs>>>(s, a->probe_key, a->probe_value, a->probe_rows);
-  output_kernel<<<(kGroupSlots + kThreads - 1) / kThreads, kThreads, 0, cs>>>(s, a->out_group, a->out_sum,
-                                                                             a->out_count, a->max_groups);
-  finish_kernel<<<1, 1, 0, cs>>>(s, a->out_ngroups, a->max_groups);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) {
-    dq_internal::set_global_error(std::string("dq_join_agg_noalloc: launch failed: ") + cudaGetErrorString(e));
+  // Each launch's own status comes back from cudaLaunchKernel, so an error left
+  // pending by the caller's earlier runtime calls is neither reported as ours
+  // nor cleared.
+  const char* failed = nullptr;
+  cudaError_t e = cudaSuccess;
+  auto launch = [&](const void* fn, int grid, void** args, const char* what) {
+    if (failed) return;
+    e = cudaLaunchKernel(fn, dim3(grid), dim3(kThreads), args, 0, cs);
+    if (e != cudaSuccess) failed = what;
+  };
+  {
+    void* args[] = {&s};
+    launch((const void*)clear_kernel, 512, args, "clear");
+  }
+  if (a->build_rows > 0) {
+    const int64_t blocks = (a->build_rows + kThreads - 1) / kThreads;
+    const int32_t* bk = a->build_key;
+    const int32_t* bf = a->build_filter;
+    int32_t fv = a->filter_value;
+    const int32_t* bg = a->build_group;
+    int64_t bn = a->build_rows;
+    void* args[] = {&s, &bk, &bf, &fv, &bg, &bn};
+    launch((const void*)build_kernel, (int)(blocks < 2048 ? blocks : 2048), args, "build");
+  }
+  if (a->probe_rows > 0) {
+    const int64_t blocks = (a->probe_rows + kThreads - 1) / kThreads;
+    const int32_t* pk = a->probe_key;
+    const uint64_t* pv = a->probe_value;
+    int64_t pn = a->probe_rows;
+    void* args[] = {&s, &pk, &pv, &pn};
+    launch((const void*)probe_kernel, (int)(blocks < 4096 ? blocks : 4096), args, "probe");
+  }
+  {
+    int32_t* og = a->out_group;
+    uint64_t* os = a->out_sum;
+    int32_t* oc = a->out_count;
+    int32_t mg = a->max_groups;
+    void* args[] = {&s, &og, &os, &oc, &mg};
+    launch((const void*)output_kernel, (kGroupSlots + kThreads - 1) / kThreads, args, "output");
+  }
+  {
+    const Scratch* cs_ = s;
+    int64_t* on = a->out_ngroups;
+    int32_t mg = a->max_groups;
+    void* args[] = {&cs_, &on, &mg};
+    if (!failed) {
+      e = cudaLaunchKernel((const void*)finish_kernel, dim3(1), dim3(1), args, 0, cs);
+      if (e != cudaSuccess) failed = "finish";
+    }
+  }
+  if (failed) {
+    dq_internal::set_global_error(std::string("dq_join_agg_noalloc: ") + failed + " kernel launch failed: " +
+                                  cudaGetErrorString(e));
     return DQ_ERR_CUDA;
   }
   return DQ_OK;

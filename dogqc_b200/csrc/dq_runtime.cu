@@ -1015,6 +1015,12 @@ uint64_t plan_bytes(const dq_plan* plan) {
 }
 
 // Re-derives every pipeline's copy of the resource descriptors.
+// Ordering: the string-source table is rewritten in place with a synchronous
+// copy.  Every caller runs when none of the plan's work is in flight: at
+// preparation, or when growing tables after a run whose stream the caller has
+// synchronised (dq_plan_execute's run_once, a batch execute, a completed server
+// slot).  Growing also frees the old device buffers, and cudaFree waits for the
+// device as well.
 void refresh_pipelines(dq_plan* plan) {
   plan->str_src.clear();
   for (auto& pp : plan->pipes) setup_pipeline(plan, *pp);

@@ -1,73 +1,57 @@
 """Relational-algebra plan front end.
 
-This module restates the reference plan API (dogqc/relationalAlgebra.py:57-664) so
-that plan scripts and plan configs written for DogQC build the same operator trees
-here, with the same operator ids, attribute ids, attribute pruning and cardinality
-estimates:
+Plan scripts and plan configs written for DogQC build their operator trees through
+``RelationalAlgebra`` (the builder of dogqc/relationalAlgebra.py:57-144): the same
+builder methods, operator classes, enums, per-operator hints and node fields that a
+translator reads.  The backend (``dogqc_b200.backend.Backend``) reads only those
+fields, so it takes trees built by DogQC's own classes as well.
 
-* operator ids are handed out bottom-up at construction time
-  (relationalAlgebra.py:30-32, 151-152) and ``resolveAlgebraPlan`` appends a result
-  materialisation as the root (:129-138);
-* ``resolve`` creates attributes and resolves identifiers ("name", "table.name",
-  "alias.name"; :301-314, 176-197);
-* ``prune`` keeps an attribute in an operator's output only if a later operator
-  uses it (:199-204);
-* ``configure`` propagates ``tupleNum`` and reads the per-operator hints
-  ``selectivity``, ``multimatch`` (default True), ``htSizeFactor`` (default 2.0)
-  and ``numgroups`` (default: child cardinality) from the plan config
-  (:342-349, 441-458, 564-574).
+What must agree with DogQC, because configs and results depend on it:
 
-The backend (``dogqc_b200.backend.Backend``) reads only the attributes named above,
-so it also accepts trees built with the reference's own classes.
+* operator ids count up in construction order (children before parents), and
+  ``resolveAlgebraPlan`` wraps the last root in a result materialisation
+  (relationalAlgebra.py:129-138, 151-152);
+* attribute ids count up in creation order: aggregates when the aggregation is
+  built, scanned and mapped attributes when the plan is bound
+  (relationalAlgebra.py:48-52, 301-314, 518-531);
+* an identifier is ``name``, ``table.name`` or ``alias.name``, and one that two
+  input attributes share is ambiguous (relationalAlgebra.py:174-197);
+* an operator's output keeps an attribute only if an operator above it uses it,
+  except a materialisation, which keeps all its input (relationalAlgebra.py:199-204,
+  640-642);
+* the cardinality estimates and their hints ``selectivity``, ``multimatch`` (default
+  True), ``htSizeFactor`` (default 2.0) and ``numgroups`` (default: the input's
+  estimate) (relationalAlgebra.py:342-349, 441-458, 489-500, 564-574).
+
+How it is organised here: each operator only declares what it contributes (the
+attributes it creates, the identifiers it looks up, its output, its estimate).
+The builder drives three passes over each plan root -- ``_bind`` (post-order: inputs
+first, then the operator's own lookups, which stamp each used attribute with the
+operator's id), ``_trim`` (outputs cut to what is used above) and ``_estimate``
+(post-order cardinalities) -- so no operator class walks the tree itself.
 """
-from collections import OrderedDict
+import itertools
+from collections import Counter, OrderedDict
+from collections.abc import Mapping
 from enum import Enum
 
 from dogqc_b200.types import Type
 
 
-def listWrap(elem):
-    return elem if isinstance(elem, list) else [elem]
+def _as_list(value):
+    return value if isinstance(value, list) else [value]
 
 
-class Attribute(object):
-    def __init__(self, name, id, opId):
-        self.name = name
-        self.id = id
-        self.creation = opId
-        self.numElements = None
-        self.lastUse = 0
-        self.dataType = None
-        self.identifiers = [name]
-
-
-class Context(object):
-    def __init__(self, database):
-        self.database = database
-        self.schema = dict(database.schema)
-        self.opIdNum = 0
-        self.attributeIdNum = 0
-        self.tableVersions = dict()
-
-    def opId(self):
-        self.opIdNum += 1
-        return self.opIdNum
-
-    def createTable(self, identifier):
-        table = {"name": identifier, "attributes": OrderedDict()}
-        self.schema[identifier] = table
-        return table
-
-    def resolveTable(self, identifier):
-        table = self.schema[identifier]
-        version = self.tableVersions.get(identifier, 0) + 1
-        self.tableVersions[identifier] = version
-        return version, table
-
-    def createAttribute(self, attributeName, tableName=None):
-        self.attributeIdNum += 1
-        attr = Attribute(attributeName, self.attributeIdNum, self.opIdNum)
-        return self.attributeIdNum, attr
+def _hint(cfg, op_id, key, default):
+    """Per-operator plan hint ``cfg[op_id][key]``, or ``default`` when the config
+    has no entry for the operator or the key (DogQC's configs are dicts keyed by
+    operator id; a missing config is ``None`` or ``{}``)."""
+    if not isinstance(cfg, Mapping):
+        return default
+    entry = cfg.get(op_id)
+    if isinstance(entry, Mapping) and key in entry:
+        return entry[key]
+    return default
 
 
 class Join(Enum):
@@ -91,350 +75,372 @@ class MaterializationType(Enum):
     TEMPTABLE = 2
 
 
+class Attribute(object):
+    """One column as it flows between operators.  The fields are the ones a
+    translator reads: ``id``, ``name``, ``dataType``, ``identifiers`` (names it
+    answers to), ``creation`` (operator counter when it was made), ``lastUse``
+    (id of the highest operator that reads it) and ``numElements``."""
+
+    def __init__(self, name, id, opId):
+        self.id = id
+        self.name = name
+        self.identifiers = [name]
+        self.creation = opId
+        self.lastUse = 0
+        self.dataType = None
+        self.numElements = None
+
+
+class Context(object):
+    """Id counters and the catalogue a plan is built against (the database's
+    schema plus the temp tables the plan creates)."""
+
+    def __init__(self, database):
+        self.database = database
+        self.schema = dict(database.schema)
+        self._ops = itertools.count(1)
+        self._attrs = itertools.count(1)
+        self.opIdNum = 0
+        self.attributeIdNum = 0
+        self.tableVersions = Counter()
+
+    def opId(self):
+        self.opIdNum = next(self._ops)
+        return self.opIdNum
+
+    def createTable(self, identifier):
+        self.schema[identifier] = {"name": identifier, "attributes": OrderedDict()}
+        return self.schema[identifier]
+
+    def resolveTable(self, identifier):
+        self.tableVersions[identifier] += 1
+        return self.tableVersions[identifier], self.schema[identifier]
+
+    def createAttribute(self, attributeName, tableName=None):
+        self.attributeIdNum = next(self._attrs)
+        return self.attributeIdNum, Attribute(attributeName, self.attributeIdNum, self.opIdNum)
+
+
 class AlgExpr(object):
-    def __init__(self, ctxt):
+    """An operator.  ``inputs`` holds its input operators; ``inRelation`` and
+    ``outRelation`` map attribute ids to attributes (insertion order is the
+    column order of results)."""
+
+    arity = 0
+
+    def __init__(self, ctxt, *inputs):
         self.opId = ctxt.opId()
+        self.inputs = inputs
         self.inRelation = dict()
         self.outRelation = dict()
 
-    def resolve(self, ctxt):
-        pass
-
-    def prune(self):
-        pass
-
-    def configure(self, cfg, ctxt):
-        pass
-
-    def translate(self, translator, ctxt):
-        pass
-
     def children(self):
-        return []
+        return list(self.inputs)
+
+    # -- what an operator contributes (overridden per class) --
+    def bind(self, ctxt, bound_inputs):
+        """Given its inputs' outputs (bound already), set ``inRelation``, look
+        up identifiers and create attributes; return the output relation."""
+        raise NotImplementedError
+
+    def estimate(self, cfg, input_estimates):
+        """Cardinality estimate from the inputs' estimates and the hints."""
+        return input_estimates[0]
+
+    trims_output = True
+
+    # -- name lookup (called by scalar expressions while they bind) --
+    def resolveAttribute(self, identifier):
+        owners = {}
+        for att in self.inRelation.values():
+            for ident in att.identifiers:
+                owners.setdefault(ident, []).append(att)
+        found = owners.get(identifier)
+        if not found:
+            raise NameError("%s (operator %d) has no input attribute named '%s'"
+                            % (type(self).__name__, self.opId, identifier))
+        if len(found) > 1:
+            raise SyntaxError("'%s' names %d input attributes of %s (operator %d)"
+                              % (identifier, len(found), type(self).__name__, self.opId))
+        att = found[0]
+        att.lastUse = self.opId
+        return att
 
     def touchAttribute(self, id):
         self.inRelation[id].lastUse = self.opId
 
-    def resolveAttribute(self, identifier):
-        known, ambiguous = {}, set()
-        for id, att in self.inRelation.items():
-            for ident in att.identifiers:
-                if ident in known:
-                    ambiguous.add(ident)
-                else:
-                    known[ident] = id
-        if identifier in ambiguous:
-            raise SyntaxError("Identifier %s is ambiguous in operator %s (%d)"
-                              % (identifier, type(self).__name__, self.opId))
-        if identifier not in known:
-            raise NameError("Attribute %s not found in %s operator (%d)"
-                            % (identifier, type(self).__name__, self.opId))
-        id = known[identifier]
-        self.touchAttribute(id)
-        return self.inRelation[id]
+    # -- DogQC's per-node entry points, driven by the passes below --
+    def resolve(self, ctxt):
+        return _bind(self, ctxt)
 
-    def pruneOutRelation(self):
-        self.outRelation = {id: a for id, a in self.outRelation.items()
-                            if a.lastUse > self.opId}
-
-    @staticmethod
-    def _cfg(cfg, opId, key, default):
-        try:
-            return cfg[opId][key]
-        except (KeyError, TypeError, IndexError):
-            return default
-
-
-class LiteralAlgExpr(AlgExpr):
     def prune(self):
-        self.pruneOutRelation()
+        _trim(self)
+
+    def configure(self, cfg, ctxt):
+        return _estimate(self, cfg)
 
     def translate(self, translator, ctxt):
-        return translator.translate(self)
+        return translator.translate(self, *[i.translate(translator, ctxt) for i in self.inputs])
+
+
+def _bind(node, ctxt):
+    bound = [_bind(i, ctxt) for i in node.inputs]
+    node.outRelation = node.bind(ctxt, bound)
+    return node.outRelation
+
+
+def _trim(node):
+    for i in node.inputs:
+        _trim(i)
+    if node.trims_output:
+        node.outRelation = {id: a for id, a in node.outRelation.items() if a.lastUse > node.opId}
+
+
+def _estimate(node, cfg):
+    node.tupleNum = node.estimate(cfg, [_estimate(i, cfg) for i in node.inputs])
+    return node.tupleNum
+
+
+# The arities, with the inputs under DogQC's names (translators tell unary and
+# binary operators apart by these fields).
+class LiteralAlgExpr(AlgExpr):
+    arity = 0
 
 
 class UnaryAlgExpr(AlgExpr):
-    def __init__(self, ctxt, child):
-        AlgExpr.__init__(self, ctxt)
-        self.child = child
+    arity = 1
 
-    def children(self):
-        return [self.child]
-
-    def prune(self):
-        self.child.prune()
-        self.pruneOutRelation()
-
-    def translate(self, translator, ctxt):
-        return translator.translate(self, self.child.translate(translator, ctxt))
+    @property
+    def child(self):
+        return self.inputs[0]
 
 
 class BinaryAlgExpr(AlgExpr):
-    def __init__(self, ctxt, leftChild, rightChild):
-        AlgExpr.__init__(self, ctxt)
-        self.leftChild = leftChild
-        self.rightChild = rightChild
+    arity = 2
 
-    def children(self):
-        return [self.leftChild, self.rightChild]
+    @property
+    def leftChild(self):
+        return self.inputs[0]
 
-    def prune(self):
-        self.leftChild.prune()
-        self.rightChild.prune()
-        self.pruneOutRelation()
-
-    def translate(self, translator, ctxt):
-        left = self.leftChild.translate(translator, ctxt)
-        right = self.rightChild.translate(translator, ctxt)
-        return translator.translate(self, left, right)
+    @property
+    def rightChild(self):
+        return self.inputs[1]
 
 
 class Scan(LiteralAlgExpr):
     def __init__(self, ctxt, tableName, alias=None):
-        LiteralAlgExpr.__init__(self, ctxt)
-        self.scanAttributes = dict()
+        AlgExpr.__init__(self, ctxt)
         self.scanTableId, self.table = ctxt.resolveTable(tableName)
-        self.isTempScan = "isTempTable" in self.table
         self.tableAlias = alias
+        self.isTempScan = "isTempTable" in self.table
+        self.scanAttributes = dict()
 
-    def resolve(self, ctxt):
-        for attrName, typ in self.table["attributes"].items():
-            id, attr = ctxt.createAttribute(attrName, self.table["name"])
-            attr.dataType = typ
-            attr.numElements = self.table["size"]
-            attr.identifiers.append(self.table["name"] + "." + attrName)
-            if self.tableAlias is not None:
-                attr.identifiers.append(self.tableAlias + "." + attrName)
+    def bind(self, ctxt, bound_inputs):
+        table = self.table
+        prefixes = [table["name"]] + ([self.tableAlias] if self.tableAlias is not None else [])
+        for column, ctype in table["attributes"].items():
+            id, att = ctxt.createAttribute(column, table["name"])
+            att.dataType = ctype
+            att.numElements = table["size"]
+            att.identifiers += ["%s.%s" % (p, column) for p in prefixes]
             if self.isTempScan:
-                attr.sourceId = self.table["sourceAttributes"][attrName]
-            self.scanAttributes[id] = attr
-        self.outRelation = self.scanAttributes
-        return self.outRelation
+                att.sourceId = table["sourceAttributes"][column]
+            self.scanAttributes[id] = att
+        return self.scanAttributes
 
-    def configure(self, cfg, ctxt):
-        self.tupleNum = self.table["size"]
-        return self.tupleNum
+    def estimate(self, cfg, input_estimates):
+        return self.table["size"]
 
 
 class Selection(UnaryAlgExpr):
     def __init__(self, ctxt, condition, child):
-        UnaryAlgExpr.__init__(self, ctxt, child)
+        AlgExpr.__init__(self, ctxt, child)
         self.condition = condition
 
-    def resolve(self, ctxt):
-        self.inRelation = self.child.resolve(ctxt)
+    def bind(self, ctxt, bound_inputs):
+        self.inRelation = bound_inputs[0]
         self.conditionAttributes = self.condition.resolve(self)
-        self.outRelation = self.inRelation
-        return self.outRelation
+        return self.inRelation
 
-    def configure(self, cfg, ctxt):
-        childNum = self.child.configure(cfg, ctxt)
-        self.selectivity = self._cfg(cfg, self.opId, "selectivity", 1.0)
-        self.tupleNum = int(childNum * self.selectivity)
-        return self.tupleNum
+    def estimate(self, cfg, input_estimates):
+        self.selectivity = _hint(cfg, self.opId, "selectivity", 1.0)
+        return int(input_estimates[0] * self.selectivity)
 
 
 class Map(UnaryAlgExpr):
     def __init__(self, ctxt, attrName, expression, child):
-        UnaryAlgExpr.__init__(self, ctxt, child)
-        self.expression = expression
+        AlgExpr.__init__(self, ctxt, child)
         self.attrName = attrName
+        self.expression = expression
 
-    def resolve(self, ctxt):
-        self.inRelation = self.child.resolve(ctxt)
+    def bind(self, ctxt, bound_inputs):
+        self.inRelation = bound_inputs[0]
         used = self.expression.resolve(self)
-        id, attr = ctxt.createAttribute(self.attrName)
-        attr.dataType = self.expression.type
-        self.mapAttr = attr
         self.mapStringAttributes = [a for a in used.values() if a.dataType == Type.STRING]
+        _, self.mapAttr = ctxt.createAttribute(self.attrName)
+        self.mapAttr.dataType = self.expression.type
         out = dict(self.inRelation)
-        out[attr.id] = attr
-        self.outRelation = out
+        out[self.mapAttr.id] = self.mapAttr
         return out
-
-    def configure(self, cfg, ctxt):
-        self.tupleNum = self.child.configure(cfg, ctxt)
-        return self.tupleNum
 
 
 class EquiJoin(BinaryAlgExpr):
-    def __init__(self, ctxt, joinType, equalityConditions, otherConditions, leftChild, rightChild):
-        BinaryAlgExpr.__init__(self, ctxt, leftChild, rightChild)
-        self.equalities = listWrap(equalityConditions)
-        self.conditions = otherConditions
-        self.joinType = joinType
+    """Equality join of a build side (left) and a probe side (right), with
+    optional further conditions; SEMI and ANTI output the probe side only."""
 
-    def resolve(self, ctxt):
-        inLeft = self.leftChild.resolve(ctxt)
-        self.inRelation.update(inLeft)
-        inRight = self.rightChild.resolve(ctxt)
-        self.inRelation.update(inRight)
-        condAtts = self.conditions.resolve(self) if self.conditions is not None else {}
-        self.conditionProbeAttributes = {id: a for id, a in condAtts.items() if id in inRight}
+    def __init__(self, ctxt, joinType, equalityConditions, otherConditions, leftChild, rightChild):
+        AlgExpr.__init__(self, ctxt, leftChild, rightChild)
+        self.joinType = joinType
+        self.equalities = _as_list(equalityConditions)
+        self.conditions = otherConditions
+
+    def bind(self, ctxt, bound_inputs):
+        build, probe = bound_inputs
+        self.inRelation = dict(build)
+        self.inRelation.update(probe)
+        cond = self.conditions.resolve(self) if self.conditions is not None else {}
+        self.conditionProbeAttributes = {id: a for id, a in cond.items() if id in probe}
         self.buildKeyAttributes = OrderedDict()
         self.probeKeyAttributes = OrderedDict()
-        for ident1, ident2 in self.equalities:
-            a1 = self.resolveAttribute(ident1)
-            a2 = self.resolveAttribute(ident2)
-            if a1.id in inLeft and a2.id in inRight:
-                self.buildKeyAttributes[a1.id] = a1
-                self.probeKeyAttributes[a2.id] = a2
-            elif a1.id in inRight and a2.id in inLeft:
-                self.buildKeyAttributes[a2.id] = a2
-                self.probeKeyAttributes[a1.id] = a1
+        for pair in self.equalities:
+            a, b = (self.resolveAttribute(ident) for ident in pair)
+            sides = (a.id in build, b.id in probe, b.id in build, a.id in probe)
+            if sides[0] and sides[1]:
+                bk, pk = a, b
+            elif sides[2] and sides[3]:
+                bk, pk = b, a
             else:
-                raise NameError("Attributes %s and %s come from the same relation."
-                                % (a1.name, a2.name))
-        if self.joinType in (Join.INNER, Join.OUTER):
-            self.outRelation = self.inRelation
-        else:
-            self.outRelation = inRight
-        return self.outRelation
+                raise NameError("join %d: %s and %s are not one build and one probe attribute"
+                                % (self.opId, a.name, b.name))
+            self.buildKeyAttributes[bk.id] = bk
+            self.probeKeyAttributes[pk.id] = pk
+        return self.inRelation if self.joinType in (Join.INNER, Join.OUTER) else dict(probe)
 
-    def configure(self, cfg, ctxt):
-        left = self.leftChild.configure(cfg, ctxt)
-        right = self.rightChild.configure(cfg, ctxt)
-        self.multimatch = self._cfg(cfg, self.opId, "multimatch", True)
-        self.selectivity = self._cfg(cfg, self.opId, "selectivity", 1.0)
-        self.htSizeFactor = self._cfg(cfg, self.opId, "htSizeFactor", 2.0)
-        self.tupleNum = int(max(left, right) * self.selectivity)
-        return self.tupleNum
+    def estimate(self, cfg, input_estimates):
+        self.multimatch = _hint(cfg, self.opId, "multimatch", True)
+        self.selectivity = _hint(cfg, self.opId, "selectivity", 1.0)
+        self.htSizeFactor = _hint(cfg, self.opId, "htSizeFactor", 2.0)
+        return int(max(input_estimates) * self.selectivity)
 
 
 class CrossJoin(BinaryAlgExpr):
+    """Every pair of left and right rows that satisfies ``condition``."""
+
     def __init__(self, ctxt, joinType, condition, leftChild, rightChild):
-        BinaryAlgExpr.__init__(self, ctxt, leftChild, rightChild)
-        self.condition = condition
+        AlgExpr.__init__(self, ctxt, leftChild, rightChild)
         self.joinType = joinType
+        self.condition = condition
 
-    def resolve(self, ctxt):
-        self.inRelation.update(self.leftChild.resolve(ctxt))
-        self.inRelation.update(self.rightChild.resolve(ctxt))
+    def bind(self, ctxt, bound_inputs):
+        self.inRelation = dict(bound_inputs[0])
+        self.inRelation.update(bound_inputs[1])
         self.conditionAttributes = self.condition.resolve(self)
-        self.outRelation = self.inRelation
-        return self.outRelation
+        return self.inRelation
 
-    def configure(self, cfg, ctxt):
-        left = self.leftChild.configure(cfg, ctxt)
-        right = self.rightChild.configure(cfg, ctxt)
-        self.multimatch = self._cfg(cfg, self.opId, "multimatch", True)
-        self.selectivity = self._cfg(cfg, self.opId, "selectivity", 1.0)
-        self.tupleNum = int(left * right * self.selectivity)
-        return self.tupleNum
+    def estimate(self, cfg, input_estimates):
+        self.multimatch = _hint(cfg, self.opId, "multimatch", True)
+        self.selectivity = _hint(cfg, self.opId, "selectivity", 1.0)
+        left, right = input_estimates
+        return int(left * right * self.selectivity)
 
 
 class Aggregation(UnaryAlgExpr):
+    """Group by ``groupingIdentifiers`` with ``aggregates`` given as
+    ``(Reduction, input identifier or "", alias)``.  An AVG gets a COUNT
+    beside it when the list has none (its divisor).  The aggregate attributes
+    are created here, when the operator is built."""
+
     def __init__(self, ctxt, groupingIdentifiers, aggregates, child):
-        UnaryAlgExpr.__init__(self, ctxt, child)
-        self.groupingIdentifiers = listWrap(groupingIdentifiers)
-        self.aggregates = listWrap(aggregates)
-        self.aggregateTuplesCreated = OrderedDict()
+        AlgExpr.__init__(self, ctxt, child)
+        self.groupingIdentifiers = _as_list(groupingIdentifiers)
+        specs = list(_as_list(aggregates))
+        reductions = {spec[0] for spec in specs}
+        if Reduction.AVG in reductions and Reduction.COUNT not in reductions:
+            specs.append((Reduction.COUNT, "", "count_agg"))
+        self.aggregates = specs
         self.aggregateAttributes = dict()
         self.avgAggregates = dict()
-        # AVG needs a COUNT next to it (relationalAlgebra.py:528-531)
-        if any(a[0] == Reduction.AVG for a in self.aggregates):
-            if not any(a[0] == Reduction.COUNT for a in self.aggregates):
-                self.aggregates.append((Reduction.COUNT, "", "count_agg"))
-        for reduction, inputIdentifier, alias in self.aggregates:
-            id, attr = ctxt.createAttribute(alias)
-            attr.dataType = Type.DOUBLE
+        self._specs = []
+        for reduction, source, alias in specs:
+            id, att = ctxt.createAttribute(alias)
+            att.dataType = Type.INT if reduction == Reduction.COUNT else Type.DOUBLE
             if reduction == Reduction.COUNT:
-                attr.dataType = Type.INT
-                self.countAttr = attr
-            self.aggregateAttributes[id] = attr
+                self.countAttr = att
             if reduction == Reduction.AVG:
-                self.avgAggregates[id] = attr
-            self.aggregateTuplesCreated[id] = (attr, inputIdentifier, reduction)
+                self.avgAggregates[id] = att
+            self.aggregateAttributes[id] = att
+            self._specs.append((att, source, reduction))
 
-    def resolve(self, ctxt):
-        self.inRelation = self.child.resolve(ctxt)
-        self.groupAttributes = OrderedDict()
-        for ident in self.groupingIdentifiers:
-            a = self.resolveAttribute(ident)
-            self.groupAttributes[a.id] = a
+    def bind(self, ctxt, bound_inputs):
+        self.inRelation = bound_inputs[0]
+        self.groupAttributes = OrderedDict((a.id, a) for a in map(self.resolveAttribute, self.groupingIdentifiers))
         self.aggregateInAttributes = OrderedDict()
         self.aggregateTuples = dict()
-        for id, (attr, inputIdentifier, reduction) in self.aggregateTuplesCreated.items():
-            inId = None
-            if inputIdentifier != "":
-                inAtt = self.resolveAttribute(inputIdentifier)
-                self.aggregateInAttributes[inAtt.id] = inAtt
-                inId = inAtt.id
-            self.aggregateTuples[id] = (inId, reduction)
-        self.outRelation.update(self.groupAttributes)
-        self.outRelation.update(self.aggregateAttributes)
-        return self.outRelation
+        for att, source, reduction in self._specs:
+            src = self.resolveAttribute(source) if source != "" else None
+            if src is not None:
+                self.aggregateInAttributes[src.id] = src
+            self.aggregateTuples[att.id] = (src.id if src is not None else None, reduction)
+        out = OrderedDict(self.groupAttributes)
+        out.update(self.aggregateAttributes)
+        return dict(out)
 
-    def configure(self, cfg, ctxt):
-        childNum = self.child.configure(cfg, ctxt)
-        self.doGroup = len(self.groupAttributes) > 0
-        self.numgroups = self._cfg(cfg, self.opId, "numgroups", childNum)
-        if not self.doGroup:
-            self.numgroups = 1
-        self.tupleNum = self.numgroups
-        return self.tupleNum
+    def estimate(self, cfg, input_estimates):
+        self.doGroup = bool(self.groupAttributes)
+        self.numgroups = _hint(cfg, self.opId, "numgroups", input_estimates[0]) if self.doGroup else 1
+        return self.numgroups
 
 
 class Projection(UnaryAlgExpr):
     def __init__(self, ctxt, identifiers, child):
-        UnaryAlgExpr.__init__(self, ctxt, child)
-        self.identifiers = listWrap(identifiers)
+        AlgExpr.__init__(self, ctxt, child)
+        self.identifiers = _as_list(identifiers)
 
-    def resolve(self, ctxt):
-        self.inRelation = self.child.resolve(ctxt)
-        self.projectionAttributes = dict()
-        for ident in self.identifiers:
-            a = self.resolveAttribute(ident)
-            self.projectionAttributes[a.id] = a
-        self.outRelation = self.projectionAttributes
-        return self.outRelation
-
-    def configure(self, cfg, ctxt):
-        self.tupleNum = self.child.configure(cfg, ctxt)
-        return self.tupleNum
+    def bind(self, ctxt, bound_inputs):
+        self.inRelation = bound_inputs[0]
+        self.projectionAttributes = {a.id: a for a in map(self.resolveAttribute, self.identifiers)}
+        return self.projectionAttributes
 
 
 class Materialize(UnaryAlgExpr):
+    """The plan's result, or a temp table that later plan roots scan."""
+
+    trims_output = False
+
+    def __init__(self, ctxt, child, matType=MaterializationType.RESULT, identifier=None):
+        AlgExpr.__init__(self, ctxt, child)
+        self.matType = matType
+        if matType == MaterializationType.TEMPTABLE:
+            self.table = ctxt.createTable(identifier)
+            self.table["isTempTable"] = True
+
     @staticmethod
     def result(ctxt, child):
-        m = Materialize(ctxt, child)
-        m.matType = MaterializationType.RESULT
-        return m
+        return Materialize(ctxt, child)
 
     @staticmethod
     def temp(ctxt, identifier, child):
-        m = Materialize(ctxt, child)
-        m.table = ctxt.createTable(identifier)
-        m.table["isTempTable"] = True
-        m.matType = MaterializationType.TEMPTABLE
-        return m
+        return Materialize(ctxt, child, MaterializationType.TEMPTABLE, identifier)
 
-    def resolve(self, ctxt):
-        self.inRelation = self.child.resolve(ctxt)
-        for id in self.inRelation:
-            self.touchAttribute(id)
+    def bind(self, ctxt, bound_inputs):
+        self.inRelation = bound_inputs[0]
+        for att in self.inRelation.values():
+            att.lastUse = self.opId
         if self.matType == MaterializationType.TEMPTABLE:
-            self.table["sourceAttributes"] = dict()
-            for id, a in self.inRelation.items():
-                self.table["attributes"][a.name] = a.dataType
-                self.table["sourceAttributes"][a.name] = a.id
+            self.table["sourceAttributes"] = {a.name: a.id for a in self.inRelation.values()}
+            self.table["attributes"].update((a.name, a.dataType) for a in self.inRelation.values())
             self.table["numColumns"] = len(self.inRelation)
-        self.outRelation = self.inRelation
-        return self.outRelation
+        return self.inRelation
 
-    def prune(self):
-        # the materialisation keeps everything its child delivers (:640-642)
-        self.child.prune()
-
-    def configure(self, cfg, ctxt):
-        self.tupleNum = self.child.configure(cfg, ctxt)
+    def estimate(self, cfg, input_estimates):
         if self.matType == MaterializationType.TEMPTABLE:
-            self.table["size"] = self.tupleNum
-        return self.tupleNum
+            self.table["size"] = input_estimates[0]
+        return input_estimates[0]
 
 
 class RelationalAlgebra(object):
-    """Plan builder with the reference's method names (relationalAlgebra.py:57-144)."""
+    """DogQC's plan builder (relationalAlgebra.py:57-144): the same methods,
+    keeping the selection and join nodes in the lists configs refer to."""
 
     def __init__(self, acc):
         self.ctxt = Context(acc)
@@ -443,13 +449,15 @@ class RelationalAlgebra(object):
         self.semiJoinNodes = []
         self.antiJoinNodes = []
 
+    def _kept(self, bucket, node):
+        bucket.append(node)
+        return node
+
     def scan(self, table, alias=None):
         return Scan(self.ctxt, table, alias)
 
     def selection(self, condition, child):
-        node = Selection(self.ctxt, condition, child)
-        self.selectionNodes.append(node)
-        return node
+        return self._kept(self.selectionNodes, Selection(self.ctxt, condition, child))
 
     def projection(self, attributes, child):
         return Projection(self.ctxt, attributes, child)
@@ -470,19 +478,16 @@ class RelationalAlgebra(object):
         return CrossJoin(self.ctxt, Join.CROSS, condition, leftChild, rightChild)
 
     def innerjoin(self, equalityConditions, otherConditions, leftChild, rightChild):
-        node = EquiJoin(self.ctxt, Join.INNER, equalityConditions, otherConditions, leftChild, rightChild)
-        self.joinNodes.append(node)
-        return node
+        return self._kept(self.joinNodes, EquiJoin(self.ctxt, Join.INNER, equalityConditions, otherConditions,
+                                                   leftChild, rightChild))
 
     def semijoin(self, equalityConditions, otherConditions, leftChild, rightChild):
-        node = EquiJoin(self.ctxt, Join.SEMI, equalityConditions, otherConditions, leftChild, rightChild)
-        self.semiJoinNodes.append(node)
-        return node
+        return self._kept(self.semiJoinNodes, EquiJoin(self.ctxt, Join.SEMI, equalityConditions, otherConditions,
+                                                       leftChild, rightChild))
 
     def antijoin(self, equalityConditions, otherConditions, leftChild, rightChild):
-        node = EquiJoin(self.ctxt, Join.ANTI, equalityConditions, otherConditions, leftChild, rightChild)
-        self.antiJoinNodes.append(node)
-        return node
+        return self._kept(self.antiJoinNodes, EquiJoin(self.ctxt, Join.ANTI, equalityConditions, otherConditions,
+                                                       leftChild, rightChild))
 
     def outerjoin(self, equalityConditions, otherConditions, leftChild, rightChild):
         return EquiJoin(self.ctxt, Join.OUTER, equalityConditions, otherConditions, leftChild, rightChild)
@@ -491,13 +496,15 @@ class RelationalAlgebra(object):
         return Aggregation(self.ctxt, groupAttributes, aggregates, child)
 
     def resolveAlgebraPlan(self, plan, cfg):
-        plan = listWrap(plan)
-        plan[-1] = self.result(plan[-1])
-        for node in plan:
-            node.resolve(self.ctxt)
-            node.prune()
-            node.configure(cfg, self.ctxt)
-        return plan
+        """Wraps the last root in the result and runs the passes root by root
+        (a temp table's size is known before a later root scans it)."""
+        roots = _as_list(plan)
+        roots[-1] = self.result(roots[-1])
+        for root in roots:
+            _bind(root, self.ctxt)
+            _trim(root)
+            _estimate(root, cfg)
+        return roots
 
     def translateToCompilerPlan(self, plan, translator):
-        return [node.translate(translator, self.ctxt) for node in plan]
+        return [root.translate(translator, self.ctxt) for root in plan]

@@ -454,7 +454,11 @@ void dq_result_free(dq_result* r);
  *     receives the number of groups, or -1 when they did not fit.
  *   - The first call on a device looks up the array's device address
  *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *     before any stream capture.  The address is kept for the life of the
+ *     process: after cudaDeviceReset (or anything else that replaces the
+ *     device's primary context) this entry point must not be called again.
+ *   - A launch failure returns DQ_ERR_CUDA; an error the caller left pending
+ *     on the thread is neither reported nor cleared.
  *   - Every call reuses the same array and clears what must start empty, so
  *     calls whose work overlaps on the GPU (different streams or threads)
  *     race; serialise them.

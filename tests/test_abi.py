@@ -39,3 +39,24 @@ def test_init_without_gpu_fails_cleanly():
     from dogqc_b200.engine import Engine
     with pytest.raises(_lib.DqError):
         Engine(0)
+
+
+@pytest.mark.parametrize("field,value,needle", [
+    ("max_groups", 0, b"max_groups"),
+    ("max_groups", None, b"max_groups"),   # DQ_NOALLOC_MAX_GROUPS + 1
+    ("out_ngroups", 0, b"null argument"),
+    ("build_key", 0, b"null argument"),
+    ("build_rows", -1, b"negative"),
+])
+def test_noalloc_rejects_bad_arguments_before_any_device_work(field, value, needle):
+    """Argument checks of the allocation-free join run on the host before any
+    device call, so they hold without a GPU."""
+    from dogqc_b200 import _lib as L
+    lib = L.lib()
+    a = L.dq_join_agg_args()
+    a.build_key = a.build_filter = a.build_group = 16
+    a.out_group = a.out_sum = a.out_count = a.out_ngroups = 16
+    a.build_rows, a.probe_rows, a.max_groups = 8, 0, 16
+    setattr(a, field, L.NOALLOC_MAX_GROUPS + 1 if value is None else value)
+    assert lib.dq_join_agg_noalloc(C.byref(a), None) == L.ERR_INVALID
+    assert needle in lib.dq_last_error(None)

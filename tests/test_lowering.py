@@ -48,11 +48,9 @@ def test_float_constants_rejected():
         Lowering(plan)
 
 
-def test_reference_front_end_trees_lower(tmp_path):
-    """The backend accepts trees built with the reference's own classes."""
+def _reference_front_end():
     import os
     import sys
-    import types as pytypes
     ref = os.environ.get("DOGQC_REFERENCE", "/root/reference")
     if not os.path.isdir(os.path.join(ref, "dogqc")):
         pytest.skip("reference source tree not present")
@@ -63,17 +61,47 @@ def test_reference_front_end_trees_lower(tmp_path):
         from dogqc.types import Type as RType
     finally:
         sys.path.remove(ref)
-    db = workloads.gen_c1(0.001)
+    return rscal, RAlg, RRed, RType
+
+
+def _fingerprint(roots):
+    """Operator ids, kinds, outputs (attribute ids, names, types, in order),
+    estimates and hints of every node, walked in translation order."""
+    out = []
+
+    def walk(n):
+        kids = [getattr(n, k) for k in ("child", "leftChild", "rightChild") if hasattr(n, k)]
+        for k in kids:
+            walk(k)
+        rel = [(i, a.name, a.dataType.name, a.lastUse, tuple(a.identifiers)) for i, a in n.outRelation.items()]
+        extra = tuple((k, str(getattr(n, k))) for k in ("multimatch", "htSizeFactor", "numgroups", "selectivity")
+                      if hasattr(n, k))
+        out.append((type(n).__name__, n.opId, n.tupleNum, tuple(rel), extra))
+
+    for r in roots:
+        walk(r)
+    return out
+
+
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "c3", "c5", "c7", "c8", "c9", "c9p", "c10", "c10p"])
+def test_reference_front_end_trees_lower(name):
+    """Trees built by the reference's own classes and by this package's front
+    end agree node for node (ids, outputs in order, estimates, hints) and
+    lower to the same IR."""
+    import types as pytypes
+    rscal, RAlg, RRed, RType = _reference_front_end()
+    db = workloads.GENERATORS[name](0.001)
     schema = {}
     for t, e in db.schema.items():
         e = dict(e)
         e["attributes"] = type(e["attributes"])((a, RType[ty.name]) for a, ty in e["attributes"].items())
         schema[t] = e
     alg = RAlg(pytypes.SimpleNamespace(schema=schema))
-    plan, cfg = workloads.plan_c1(alg, rscal, RType, RRed)
+    plan, cfg = workloads.PLANS[name](alg, rscal, RType, RRed)
     plan = alg.resolveAlgebraPlan(plan, cfg)
     ours = RelationalAlgebra(db)
-    p2, c2 = workloads.build("c1", ours)
+    p2, c2 = workloads.build(name, ours)
     p2 = ours.resolveAlgebraPlan(p2, c2)
+    assert _fingerprint(plan) == _fingerprint(p2)
     a, b = Lowering(plan), Lowering(p2)
     assert a.describe() == b.describe()

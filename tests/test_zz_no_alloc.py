@@ -42,7 +42,7 @@ def _plan_result(db):
     return canonical_rows(res.rows())
 
 
-def _noalloc_result(lib, dev, max_groups):
+def _noalloc_call(lib, dev, max_groups):
     import torch
     from dogqc_b200 import _lib as L
     out_group = torch.zeros(max_groups, dtype=torch.int32, device="cuda")
@@ -61,7 +61,11 @@ def _noalloc_result(lib, dev, max_groups):
     torch.cuda.synchronize()
     L.check(lib.dq_join_agg_noalloc(C.byref(a), None))
     torch.cuda.synchronize()
-    n = int(out_n.item())
+    return int(out_n.item()), out_group, out_sum, out_count
+
+
+def _noalloc_result(lib, dev, max_groups):
+    n, out_group, out_sum, out_count = _noalloc_call(lib, dev, max_groups)
     assert n >= 0
     g = out_group[:n].cpu().numpy()
     s = out_sum[:n].cpu().numpy().view(np.uint64)
@@ -69,12 +73,8 @@ def _noalloc_result(lib, dev, max_groups):
     return canonical_rows(zip(g.tolist(), s.tolist(), c.tolist()))
 
 
-def test_noalloc_join_matches_plan_execute_twice():
+def _device_columns(db):
     import torch
-    from dogqc_b200 import _lib as L
-    from dogqc_b200 import workloads
-    db = workloads.gen_c1(0.01)
-    want = _plan_result(db)
     dim, fact = db["dim"], db["fact"]
     keep = {}
     dev = {}
@@ -85,11 +85,36 @@ def test_noalloc_join_matches_plan_execute_twice():
             keep[name] = tt
             dev[name] = tt.data_ptr()
     dev["build_rows"], dev["probe_rows"] = dim.size, fact.size
+    return keep, dev
+
+
+def test_noalloc_join_matches_plan_execute_twice():
+    from dogqc_b200 import _lib as L
+    from dogqc_b200 import workloads
+    db = workloads.gen_c1(0.01)
+    want = _plan_result(db)
+    keep, dev = _device_columns(db)
     lib = L.lib()
     first = _noalloc_result(lib, dev, 64)
     second = _noalloc_result(lib, dev, 64)
     assert first == want
     assert second == want
+    del keep
+
+
+def test_noalloc_reports_groups_that_do_not_fit():
+    """25 nations into an output of 4 groups: -1, and the next call with room
+    for all groups gives the full result again."""
+    from dogqc_b200 import _lib as L
+    from dogqc_b200 import workloads
+    db = workloads.gen_c1(0.01)
+    want = _plan_result(db)
+    keep, dev = _device_columns(db)
+    lib = L.lib()
+    n, _, _, _ = _noalloc_call(lib, dev, 4)
+    assert n == -1
+    assert _noalloc_result(lib, dev, 64) == want
+    del keep
 
 
 def test_noalloc_rejects_oversized_build():
