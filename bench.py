@@ -229,30 +229,44 @@ def run_ours(args, world, rank, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     evict = torch.zeros(32 << 20, dtype=torch.int64, device="cuda")
 
-    def step():
-        flush.fill_(1)
-        evict.sum()
+    def timed(plan_, steps):
+        """Warm-up, then `steps` executions each after an L2 flush: summed
+        device time of the runs (CUDA events on the engine's stream), summed
+        per-pipeline times (zero where the run replayed a graph), launches."""
+        def step():
+            flush.fill_(1)
+            evict.sum()
+            torch.cuda.synchronize()
+            res_ = plan_.execute()
+            return res_, plan_.timing()
+        for _ in range(args.warmup):
+            res_, _ = step()
+        dist_barrier(world)
         torch.cuda.synchronize()
-        res = p.execute()
-        return res, p.timing()
-
-    for _ in range(args.warmup):
-        res, _ = step()
-    dist_barrier(world)
-    torch.cuda.synchronize()
-    total_ms, launches = 0.0, 0
-    pipe_ms = [0.0] * npipes
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            res, t = step()
-            total_ms += t["total_ms"]
+        tot, launches_ = 0.0, 0
+        pipes = [0.0] * npipes
+        for _ in range(steps):
+            res_, t = step()
+            tot += t["total_ms"]
             for i in range(npipes):
-                pipe_ms[i] += t["pipeline_ms"][i]
-            launches += t["kernel_launches"]
-    torch.cuda.synchronize()
-    dist_barrier(world)
-    total_ms = dist_max(total_ms, world)
-    pipe_ms = [dist_max(x, world) for x in pipe_ms]
+                pipes[i] += t["pipeline_ms"][i]
+            launches_ += t["kernel_launches"]
+        torch.cuda.synchronize()
+        dist_barrier(world)
+        return res_, dist_max(tot, world), [dist_max(x, world) for x in pipes], launches_
+
+    # the plan as dq_plan_execute runs it: after the first run, its launches
+    # replay from a captured CUDA graph
+    with ClockSampler(local) as clocks:
+        res, total_ms, _, launches = timed(p, args.steps)
+    # per-kernel times need events between the launches: the same plan on a
+    # second context that does not capture graphs, over as many steps
+    kengine = Engine(local, tile_rows=args.tile_rows, ctas_per_sm=args.ctas_per_sm, flags=args.engine_flags | 2)
+    kengine.register_database(db)
+    kp = kengine.prepare(plan)
+    _, k_total_ms, pipe_ms, _ = timed(kp, args.steps)
+    kp.free()
+    kengine.close()
     dom = max(range(npipes), key=lambda i: pipe_ms[i])   # the dominant pipeline kernel
     probe_ms = pipe_ms[dom]
     fact_bytes = pipeline_bytes(db, p.lowering, dom)
@@ -325,7 +339,10 @@ def run_ours(args, world, rank, local):
                      "peak_source": "%s hbm_gbs (burst copy)" % peak_kind},
         "plan": {"algorithmic_bytes": plan_bytes, "avg_ms": ms_per_step,
                  "frac": plan_bytes / (ms_per_step / 1e3) / 1e9 / peak,
-                 "pipeline_ms": [x / args.steps for x in pipe_ms]},
+                 "replayed_graph": True,
+                 "no_graph_avg_ms": k_total_ms / args.steps,
+                 "pipeline_ms": [x / args.steps for x in pipe_ms],
+                 "pipeline_ms_source": "second timed loop without graph replay (events between launches)"},
         "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clocks.summary(),
@@ -748,8 +765,8 @@ def run_served(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

@@ -77,6 +77,13 @@ __device__ __forceinline__ void ld_nc_32B(const uint64_t* p, uint64_t& a, uint64
 #endif
 }
 
+// 16 read-only bytes (two 64-bit words; p 16-byte aligned).
+__device__ __forceinline__ void ld_nc_16B(const uint64_t* p, uint64_t& a, uint64_t& b) {
+  const ulonglong2 x = __ldg(reinterpret_cast<const ulonglong2*>(p));
+  a = x.x;
+  b = x.y;
+}
+
 // MurmurHash3 64-bit finaliser (Appleby), used for every hash table.
 __device__ __forceinline__ uint64_t fmix64(uint64_t k) {
   k ^= k >> 33;
@@ -337,6 +344,27 @@ __device__ __forceinline__ int64_t unique_insert(const DevPipe& P, const DevRes&
   }
   set_status(P, kErrHtFull);
   return -1;
+}
+
+// Compact unique table (R.compact): inserts key k32 with its 32-bit payload,
+// one compare-and-swap of the whole word.  The first insert of a key wins.
+// The all-ones key cannot share the empty marker's word and is kept at slot
+// cap (0 when present), its payload at cap + 1.
+__device__ __forceinline__ void unique_insert_compact(const DevPipe& P, const DevRes& R, uint32_t k32, uint32_t pay) {
+  uint64_t* const ht = R.slots;
+  const uint32_t cap = (uint32_t)R.cap;
+  if (k32 == 0xffffffffu) {
+    if (atomicCAS((unsigned long long*)(ht + cap), kEmpty, 0ull) == kEmpty) ht[(uint64_t)cap + 1] = pay;
+    return;
+  }
+  const uint64_t w = ((uint64_t)k32 << 32) | pay;
+  uint32_t idx = slot_of((uint64_t)k32, cap);
+  for (uint32_t n = 0; n < cap; ++n) {
+    const uint64_t old = atomicCAS((unsigned long long*)(ht + idx), kEmpty, w);
+    if (old == kEmpty || (uint32_t)(old >> 32) == k32) return;
+    idx = (idx + 1u == cap) ? 0u : idx + 1u;
+  }
+  set_status(P, kErrHtFull);
 }
 
 // Aggregation table (global): find or claim the group's slot.

@@ -55,6 +55,10 @@ struct DevRes {
   int32_t nkeys;
   int8_t key_ctype[DQ_MAX_KEYS];
   int32_t packed;         // keys packed into the 64-bit tag
+  int32_t compact;        // UNIQUE, one key and one payload of at most 32 bits
+                          // each: a slot is one word, key << 32 | payload
+                          // (~0 empty); the all-ones key lives at slot cap
+                          // (0 when present) with its payload at cap + 1
   int32_t words;          // 64-bit words per slot (tag + keys + payload/aggs)
   int32_t key_word;       // first key word (hashed keys only)
   int32_t val_word;       // first payload / accumulator word
@@ -119,6 +123,9 @@ struct DevPipe {
   int32_t exp_cap;             // rows per expansion chunk
   int32_t use_tma;
   int32_t mode;                // 0: tiles, 1: heavy work units
+  int32_t clear_src;           // DQ_SRC_AGG: reset every slot read to its initial
+                               // state (the table's only scan; the next run then
+                               // needs no initialising kernel)
   int32_t ncols;
   DevCol cols[DQ_MAX_COLS];
   int32_t nstr;

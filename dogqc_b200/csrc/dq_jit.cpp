@@ -428,13 +428,23 @@ struct Gen {
       ++ind;
       L("const uint64_t* const ht_ = " + res(r) + ".slots;");
       const std::string K = num(k);
-      L("const uint32_t p_ = slot_of(" + tag + ", (uint32_t)" + res(r) + ".cap) & ~" + num(4 / R.words - 1) + "u;");
-      L("if (in_) {");
-      L("  ld_nc_32B(ht_ + (uint64_t)p_ * " + num(R.words) + ", pw" + K + "_0[u], pw" + K + "_1[u], pw" + K + "_2[u], pw" +
-        K + "_3[u]);");
-      L("} else {");
-      L("  pw" + K + "_0[u] = pw" + K + "_1[u] = pw" + K + "_2[u] = pw" + K + "_3[u] = kEmpty;");
-      L("}");
+      if (R.compact) {
+        // compact slots: the aligned 16-byte pair of the home slot
+        L("const uint32_t p_ = slot_of(" + tag + ", (uint32_t)" + res(r) + ".cap) & ~1u;");
+        L("if (in_) {");
+        L("  ld_nc_16B(ht_ + (uint64_t)p_, pw" + K + "_0[u], pw" + K + "_1[u]);");
+        L("} else {");
+        L("  pw" + K + "_0[u] = pw" + K + "_1[u] = kEmpty;");
+        L("}");
+      } else {
+        L("const uint32_t p_ = slot_of(" + tag + ", (uint32_t)" + res(r) + ".cap) & ~" + num(4 / R.words - 1) + "u;");
+        L("if (in_) {");
+        L("  ld_nc_32B(ht_ + (uint64_t)p_ * " + num(R.words) + ", pw" + K + "_0[u], pw" + K + "_1[u], pw" + K + "_2[u], pw" +
+          K + "_3[u]);");
+        L("} else {");
+        L("  pw" + K + "_0[u] = pw" + K + "_1[u] = pw" + K + "_2[u] = pw" + K + "_3[u] = kEmpty;");
+        L("}");
+      }
       --ind;
       L("}");
     }
@@ -455,8 +465,54 @@ struct Gen {
       const bool ext = tag_can_be_empty(r);
       L("const uint64_t* const ht_ = " + res(r) + ".slots;");
       L("const uint32_t hc_ = (uint32_t)" + res(r) + ".cap;");
-      if (R.words == 2 && op.sub == DQ_JOIN_INNER && op.nlist2 > 0 && P.lists[op.list2] >= 0)
+      if ((R.words == 2 || R.compact) && op.sub == DQ_JOIN_INNER && op.nlist2 > 0 && P.lists[op.list2] >= 0)
         L("uint64_t pv_ = 0;");
+      if (R.compact) {
+        // one word a slot: key << 32 | payload, read in aligned 16-byte pairs
+        // (the slot count is even).  The walk compares the keys (high words);
+        // an empty slot's key is all ones, a key the table never holds.
+        const bool pf = is_prefetched(k);
+        const bool with_pay = op.sub == DQ_JOIN_INNER && op.nlist2 > 0 && P.lists[op.list2] >= 0;
+        L("const uint32_t k_ = (uint32_t)" + tg + ";");
+        L("if (k_ == 0xffffffffu) {");
+        L("  if (ht_[(uint64_t)hc_] == 0ull) { " + s + " = (int64_t)hc_;" + (with_pay ? " pv_ = ht_[(uint64_t)hc_ + 1];" : "") +
+          " }");
+        L("} else {");
+        ++ind;
+        L("uint32_t p_ = slot_of(" + tg + ", hc_);");
+        L("uint32_t f_ = p_ & 1u;");
+        L("p_ -= f_;");
+        if (pf) {
+          L("uint64_t w0_ = pw" + num(k) + "_0[u], w1_ = pw" + num(k) + "_1[u];");
+        } else {
+          L("uint64_t w0_, w1_;");
+          L("ld_nc_16B(ht_ + (uint64_t)p_, w0_, w1_);");
+        }
+        L("for (uint32_t n_ = 0;;) {");
+        ++ind;
+        L("if ((uint32_t)(w0_ >> 32) == k_) { " + s + " = (int64_t)p_;" + (with_pay ? " pv_ = w0_;" : "") + " break; }");
+        L("if ((uint32_t)(w1_ >> 32) == k_) { " + s + " = (int64_t)p_ + 1;" + (with_pay ? " pv_ = w1_;" : "") + " break; }");
+        L("if ((f_ == 0u && w0_ == kEmpty) || w1_ == kEmpty) break;");
+        L("f_ = 0u;");
+        L("p_ = (p_ + 2u == hc_) ? 0u : p_ + 2u;");
+        L("n_ += 2u;");
+        L("if (n_ >= hc_) break;");
+        L("ld_nc_16B(ht_ + (uint64_t)p_, w0_, w1_);");
+        --ind;
+        L("}");
+        --ind;
+        L("}");
+        if (with_pay) {
+          const int d = P.lists[op.list2];
+          L("if (" + s + " >= 0) " + V(d) + " = canon(canon((uint64_t)(uint32_t)pv_, " + ct_name(R.pay_ctype[0]) + "), " +
+            ct_name(slot(d).ctype) + ");");
+        }
+        --ind;
+        L("}");
+        if (op.sub == DQ_JOIN_ANTI) L(act + " = " + act + " && " + s + " < 0;");
+        else L(act + " = " + act + " && " + s + " >= 0;");
+        return;
+      }
       if (ext) {
         L("if (" + tg + " == kEmpty) {");
         L("  if (ht_[(uint64_t)hc_ * " + W + "] == 0ull) " + s + " = (int64_t)hc_;");
@@ -805,6 +861,14 @@ struct Gen {
     const DevRes& R = P.res[r];
     L("if (" + act + ") {");
     ++ind;
+    if (R.compact) {
+      const std::string key = "canon(" + V(P.lists[op.list]) + ", " + ct_name(R.key_ctype[0]) + ")";
+      const std::string pay = op.nlist2 > 0 ? "(uint32_t)" + V(P.lists[op.list2]) : "0u";
+      L("unique_insert_compact(P, " + res(r) + ", (uint32_t)" + key + ", " + pay + ");");
+      --ind;
+      L("}");
+      return;
+    }
     std::string k = keys(op, r, op.list, op.nlist);
     L("const int64_t s_ = unique_insert(P, " + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
     if (op.nlist2 > 0) {
@@ -1295,7 +1359,8 @@ struct Gen {
     L("for (int64_t base = (int64_t)blockIdx.x * span; base < nrows; base += (int64_t)gridDim.x * span) {");
     ++ind;
     for (int k : prefetch) {
-      for (int q = 0; q < 4; ++q) L("uint64_t pw" + num(k) + "_" + num(q) + "[" + num(U) + "];");
+      const int nq = P.res[P.ops[k].res].compact ? 2 : 4;
+      for (int q = 0; q < nq; ++q) L("uint64_t pw" + num(k) + "_" + num(q) + "[" + num(U) + "];");
     }
     if (!cols.empty()) {
       // the columns of the next step are loaded before this step's rows are
@@ -1376,6 +1441,22 @@ struct Gen {
         L("}");
       }
     }
+    if (agg_src) {
+      // the table's only scan puts back each slot it read (tag and keys empty,
+      // accumulators at their initial values) when the runtime asks for it
+      const int sr = P.source_res;
+      const DevRes& R = P.res[sr];
+      L("if (P.clear_src && " + std::string(R.nkeys > 0 ? "act" : "row < nrows") + ") {");
+      ++ind;
+      L("uint64_t* const cs_ = " + res(sr) + ".slots + (uint64_t)row * " + num(R.words) + ";");
+      for (int w = 0; w < R.words; ++w) {
+        const bool acc = w >= R.val_word && w < R.val_word + R.naggs;
+        L("cs_[" + num(w) + "] = " + (acc ? std::string("red_init(") + red_name(R.agg_red[w - R.val_word]) + ")" : "kEmpty") +
+          ";");
+      }
+      --ind;
+      L("}");
+    }
     declare_regs(0);
     L("do {");
     ++ind;
@@ -1423,7 +1504,8 @@ struct Gen {
     std::vector<int> cols = source_cols();
     for (int c : cols) L("uint64_t c" + num(c) + "[" + num(U) + "];");
     for (int k : prefetch)
-      for (int q = 0; q < 4; ++q) L("uint64_t pw" + num(k) + "_" + num(q) + "[" + num(U) + "];");
+      for (int q = 0; q < (P.res[P.ops[k].res].compact ? 2 : 4); ++q)
+        L("uint64_t pw" + num(k) + "_" + num(q) + "[" + num(U) + "];");
     if (!cols.empty()) {
       col_loads(cols, "c", "base");
       if (!prefetch.empty()) {

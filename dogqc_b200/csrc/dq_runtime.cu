@@ -189,10 +189,13 @@ struct ResRec {
   dq_resource desc{};
   std::string name;
   DevRes dev{};
-  DevBuf slots, counts, offsets, cursor, scan_scratch;
+  DevBuf slots, counts, offsets, scan_scratch;
   std::vector<std::unique_ptr<DevBuf>> pay;
   uint64_t pay_rows = 0;
   int pct = 100;            // UNIQUE: slots as a percentage of the plan's capacity
+  int index = 0;            // position in the plan's resources
+  bool agg_clean = false;   // AGG: every slot is in its initial state (the last
+                            // run's scan reset what it read)
 };
 
 constexpr uint64_t kL2TableBytes = 48ull << 20;  // join tables up to this size get extra slack
@@ -217,6 +220,8 @@ struct PipeRec {
   }
   DevBuf pattern_buf, heavy_items, heavy_count, heavy_prefix;
   DevBuf heavy_gkey, heavy_glen, heavy_gcnt, heavy_glist, heavy_gstart, heavy_sorted;  // grouped deferral
+  bool clears_source = false;  // scans an aggregation table that no other pipeline
+                               // reads, and may reset its slots as it reads them
   bool mm_count = false;    // sink is a multimap count: bucket scan follows
   int mm_res = -1;
   int staged_cols = 0;
@@ -244,11 +249,41 @@ struct dq_plan {
   std::vector<std::unique_ptr<ResRec>> res;
   std::vector<std::unique_ptr<PipeRec>> pipes;
   int result_res = -1;
-  DevBuf status, counters;
+  // The words every run starts from zero, in one buffer so that one memset
+  // clears them: the status word (8 bytes), two tile counters per pipeline,
+  // then one row cursor per resource (used by OUTPUT resources).
+  DevBuf status;
+  uint32_t* counters = nullptr;
+  uint64_t* cursors = nullptr;
   dq_plan_timing timing{};
   std::vector<cudaEvent_t> events;
   std::vector<DevStr> str_src;  // string columns the pipelines read: string references index these
   DevBuf str_src_dev;
+  // Steady state of dq_plan_execute: once a run succeeded, the run's launches
+  // are captured as a CUDA graph and replayed while nothing they depend on
+  // changes (the signature: every pipeline's descriptor and launch shape and
+  // which aggregation tables start clean).  A failed run drops the graph.
+  int32_t* host_status = nullptr;   // pinned
+  cudaEvent_t graph_ev[2] = {nullptr, nullptr};  // around a graph launch (the
+                                    // events inside a graph give no times)
+  bool steady = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  std::string graph_sig;
+  int graph_launches = 0;
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    graph_exec = nullptr;
+    graph = nullptr;
+    graph_sig.clear();
+  }
+  ~dq_plan() {
+    drop_graph();
+    if (host_status) cudaFreeHost(host_status);
+    for (auto e : graph_ev)
+      if (e) cudaEventDestroy(e);
+  }
 };
 
 // One pipeline of a batch: a generated kernel over all instances.
@@ -361,6 +396,7 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
   const dq_resource& d = r.desc;
   DevRes& R = r.dev;
   memset(&R, 0, sizeof(R));
+  r.agg_clean = false;
   R.kind = d.kind;
   R.nkeys = d.nkeys;
   for (int i = 0; i < DQ_MAX_KEYS; ++i) R.key_ctype[i] = d.key_ctype[i];
@@ -382,6 +418,15 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       R.key_word = 1;
       R.val_word = 1 + (R.packed ? 0 : d.nkeys);
       R.words = R.val_word + (d.kind == DQ_RES_UNIQUE ? d.npay : d.naggs);
+      // a join table whose one key and one payload fit 32 bits each keeps both
+      // in one word (generated kernels; the prebuilt ones read wide slots)
+      if (d.kind == DQ_RES_UNIQUE && R.packed && d.nkeys == 1 && ctype_width(d.key_ctype[0]) <= 4 && d.npay == 1 &&
+          d.pay_ctype[0] != DQ_STR && ctype_width(d.pay_ctype[0]) <= 4 &&
+          !(plan->ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL))) {
+        R.compact = 1;
+        R.words = 1;
+        R.val_word = 0;
+      }
       // join tables get more slots than the plan asks for: most probes of a
       // selective join miss, a miss walks to the next empty slot, and a walk
       // past the first 32-byte slot group is a second dependent load.  Four
@@ -397,7 +442,7 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       cap = std::max<uint64_t>(cap, 16);
       if (cap >= 0xffffffffull) throw DqError(DQ_ERR_UNSUPPORTED, "hash tables hold fewer than 2^32 slots");
       R.cap = cap;
-      r.slots.alloc((cap + 1) * R.words * 8);
+      r.slots.alloc((cap + 1 + (R.compact ? 1 : 0)) * R.words * 8);
       R.slots = r.slots.as<uint64_t>();
       bool str_keys = false;
       for (int i = 0; i < d.nkeys; ++i) str_keys |= d.key_ctype[i] == DQ_STR;
@@ -432,8 +477,7 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
     }
     case DQ_RES_OUTPUT: {
       R.cap = cap;
-      r.cursor.alloc(8);
-      R.cursor = r.cursor.as<uint64_t>();
+      R.cursor = plan->cursors ? plan->cursors + r.index : nullptr;
       r.pay.clear();
       for (int j = 0; j < d.npay; ++j) {
         r.pay.emplace_back(new DevBuf());  // a string column holds references (8 bytes a row)
@@ -852,10 +896,16 @@ void free_events(dq_plan* plan) {
   plan->events.clear();
 }
 
-// One execution of all pipelines; returns the device status word.
 // Enqueues one execution of all pipelines on `st`, ending with the copy of the
 // device status word to `host_status`; returns the kernels launched.
-int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status) {
+//
+// `fast` (dq_plan_execute, where the caller reads the status after every run):
+// an aggregation table that exactly one later pipeline scans is reset by that
+// scan (each thread puts back the slots it read), so the next run needs no
+// initialising kernel; run_once records which tables a successful run left
+// clean.  Captured runs (served requests) always initialise, since a graph
+// replays the same launches whatever the previous replay left.
+int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status, bool fast = false) {
   int launches = 0;
   const size_t np = plan->pipes.size();
   if (plan->events.size() != 2 * np + 2) {
@@ -867,8 +917,8 @@ int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status) {
     }
   }
   DQ_CUDA(cudaEventRecord(plan->events[0], st));
-  DQ_CUDA(cudaMemsetAsync(plan->status.ptr, 0, 4, st));
-  DQ_CUDA(cudaMemsetAsync(plan->counters.ptr, 0, plan->counters.bytes, st));
+  // status, tile counters and output cursors: one buffer, one memset
+  DQ_CUDA(cudaMemsetAsync(plan->status.ptr, 0, plan->status.bytes, st));
   for (auto& rp : plan->res) {
     ResRec& r = *rp;
     switch (r.desc.kind) {
@@ -876,21 +926,24 @@ int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status) {
         DQ_CUDA(cudaMemsetAsync(r.slots.ptr, 0xff, r.slots.bytes, st));
         break;
       case DQ_RES_AGG:
-        DQ_CUDA(launch_agg_init(r.dev.slots, r.dev.cap + 1, r.dev.words, r.dev.val_word, r.dev.naggs, r.dev.agg_red, st));
-        ++launches;
+        if (!(fast && r.agg_clean)) {
+          DQ_CUDA(launch_agg_init(r.dev.slots, r.dev.cap + 1, r.dev.words, r.dev.val_word, r.dev.naggs, r.dev.agg_red, st));
+          ++launches;
+        }
+        r.agg_clean = false;
         break;
       case DQ_RES_MULTI:
         DQ_CUDA(cudaMemsetAsync(r.counts.ptr, 0, r.counts.bytes, st));
         break;
-      case DQ_RES_OUTPUT:
-        DQ_CUDA(cudaMemsetAsync(r.cursor.ptr, 0, 8, st));
+      default:
         break;
     }
   }
-  uint32_t* counters = plan->counters.as<uint32_t>();
+  uint32_t* counters = plan->counters;
   for (size_t i = 0; i < np; ++i) {
     PipeRec& p = *plan->pipes[i];
     p.dev.tile_counter = counters + 2 * i;
+    p.dev.clear_src = fast && p.clears_source ? 1 : 0;
     DQ_CUDA(cudaEventRecord(plan->events[1 + 2 * i], st));
     if (p.expand_op >= 0) {
       DQ_CUDA(cudaMemsetAsync(p.heavy_count.ptr, 0, 8, st));
@@ -949,11 +1002,90 @@ void collect_timing(dq_plan* plan, int launches) {
 }
 
 // One execution of all pipelines; returns the device status word.
+// What a captured run depends on besides the plan's fixed buffers.
+std::string graph_signature(const dq_plan* plan) {
+  std::string sig;
+  for (const auto& pp : plan->pipes) {
+    const PipeRec& p = *pp;
+    DevPipe d = p.dev;
+    d.clear_src = p.clears_source ? 1 : 0;  // as enqueue_run sets them in fast mode
+    sig.append(reinterpret_cast<const char*>(&d), sizeof(d));
+    const int shape[4] = {p.grid, p.grid_full, p.prog.block, p.prog.smem_bytes};
+    sig.append(reinterpret_cast<const char*>(shape), sizeof(shape));
+  }
+  for (const auto& rp : plan->res) {
+    sig.push_back(rp->agg_clean ? 1 : 0);
+    const void* bufs[3] = {rp->slots.ptr, rp->counts.ptr, rp->dev.cursor};
+    sig.append(reinterpret_cast<const char*>(bufs), sizeof(bufs));
+  }
+  const cudaEvent_t* ev = plan->events.data();
+  sig.append(reinterpret_cast<const char*>(ev), plan->events.size() * sizeof(cudaEvent_t));
+  return sig;
+}
+
+// One execution of all pipelines; returns the device status word.  After a
+// successful run the same launches replay from a captured graph (unless the
+// context has DQ_CFG_NO_GRAPH).
 int run_once(dq_plan* plan, cudaStream_t st) {
-  int32_t status = 0;
-  const int launches = enqueue_run(plan, st, &status);
+  if (!plan->host_status) DQ_CUDA(cudaMallocHost((void**)&plan->host_status, sizeof(int32_t)));
+  *plan->host_status = 0;
+  int launches = 0;
+  bool graphs = !(plan->ctx->cfg.flags & DQ_CFG_NO_GRAPH) && plan->steady;
+  if (graphs) {
+    std::string sig = graph_signature(plan);
+    if (plan->graph_exec && sig != plan->graph_sig) plan->drop_graph();
+    // a stream that cannot be captured (the legacy default stream) runs the launches directly
+    if (!plan->graph_exec && cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      graphs = false;
+    }
+  }
+  if (graphs) {
+    if (!plan->graph_exec) {
+      cudaGraph_t g = nullptr;
+      try {
+        plan->graph_launches = enqueue_run(plan, st, plan->host_status, true);
+      } catch (...) {
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      DQ_CUDA(cudaStreamEndCapture(st, &g));
+      plan->graph = g;
+      DQ_CUDA(cudaGraphInstantiate(&plan->graph_exec, plan->graph, 0));
+      plan->graph_sig = graph_signature(plan);
+    }
+    for (auto& e : plan->graph_ev)
+      if (!e) DQ_CUDA(cudaEventCreate(&e));
+    DQ_CUDA(cudaEventRecord(plan->graph_ev[0], st));
+    DQ_CUDA(cudaGraphLaunch(plan->graph_exec, st));
+    DQ_CUDA(cudaEventRecord(plan->graph_ev[1], st));
+    launches = plan->graph_launches;
+  } else {
+    launches = enqueue_run(plan, st, plan->host_status, true);
+  }
   DQ_CUDA(cudaStreamSynchronize(st));
-  collect_timing(plan, launches);
+  const int32_t status = *plan->host_status;
+  if (graphs) {
+    // the whole run from the events around the launch; no per-pipeline times
+    float ms = 0;
+    memset(&plan->timing, 0, sizeof(plan->timing));
+    cudaEventElapsedTime(&ms, plan->graph_ev[0], plan->graph_ev[1]);
+    plan->timing.total_ms = ms;
+    plan->timing.max_pipeline = -1;
+    plan->timing.kernel_launches = launches;
+  } else {
+    collect_timing(plan, launches);
+  }
+  if ((status & ~kInfoMask) == 0) {
+    // a completed run whose scans reset their aggregation tables leaves them clean
+    for (auto& pp : plan->pipes)
+      if (pp->clears_source) plan->res[pp->desc.source_res]->agg_clean = true;
+    plan->steady = true;
+  } else {
+    plan->steady = false;
+    plan->drop_graph();
+  }
   return status;
 }
 
@@ -961,7 +1093,7 @@ int run_once(dq_plan* plan, cudaStream_t st) {
 dq_result* read_result(dq_plan* plan, cudaStream_t st) {
   ResRec& o = *plan->res[plan->result_res];
   uint64_t n = 0;
-  DQ_CUDA(cudaMemcpyAsync(&n, o.cursor.ptr, 8, cudaMemcpyDeviceToHost, st));
+  DQ_CUDA(cudaMemcpyAsync(&n, o.dev.cursor, 8, cudaMemcpyDeviceToHost, st));
   DQ_CUDA(cudaStreamSynchronize(st));
   if (n > o.dev.cap) n = o.dev.cap;
   std::unique_ptr<dq_result> res(new dq_result());
@@ -1000,10 +1132,10 @@ dq_result* read_result(dq_plan* plan, cudaStream_t st) {
 
 // Device bytes a plan holds (its tables, intermediates and scratch).
 uint64_t plan_bytes(const dq_plan* plan) {
-  uint64_t b = plan->status.bytes + plan->counters.bytes;
+  uint64_t b = plan->status.bytes;
   for (auto& rp : plan->res) {
     const ResRec& r = *rp;
-    b += r.slots.bytes + r.counts.bytes + r.offsets.bytes + r.cursor.bytes + r.scan_scratch.bytes;
+    b += r.slots.bytes + r.counts.bytes + r.offsets.bytes + r.scan_scratch.bytes;
     for (auto& p : r.pay) b += p->bytes;
   }
   for (auto& pp : plan->pipes) {
@@ -1045,8 +1177,11 @@ std::unique_ptr<dq_plan> make_plan(dq_ctx* ctx, const dq_plan_desc* desc, const 
   std::unique_ptr<dq_plan> plan(new dq_plan());
   plan->ctx = ctx;
   plan->opts = opts;
-  plan->status.alloc(4);
-  plan->counters.alloc(8 * (size_t)desc->npipes);
+  plan->status.alloc(8 + 8 * (size_t)desc->npipes + 8 * (size_t)std::max(desc->nres, 0));
+  if (plan->status.ptr) {
+    plan->counters = reinterpret_cast<uint32_t*>(plan->status.as<uint8_t>() + 8);
+    plan->cursors = reinterpret_cast<uint64_t*>(plan->status.as<uint8_t>() + 8 + 8 * (size_t)desc->npipes);
+  }
   // row bound for multimap payloads: rows of the source of the pipeline that scatters into it
   std::vector<int64_t> bound(desc->nres, 1);
   for (int i = 0; i < desc->npipes; ++i) {
@@ -1066,6 +1201,7 @@ std::unique_ptr<dq_plan> make_plan(dq_ctx* ctx, const dq_plan_desc* desc, const 
   }
   for (int i = 0; i < desc->nres; ++i) {
     std::unique_ptr<ResRec> r(new ResRec());
+    r->index = i;
     r->desc = desc->res[i];
     r->name = desc->res[i].name ? desc->res[i].name : "";
     r->desc.name = nullptr;
@@ -1093,6 +1229,14 @@ std::unique_ptr<dq_plan> make_plan(dq_ctx* ctx, const dq_plan_desc* desc, const 
     for (int c = 0; c < p->desc.npatterns; ++c) p->desc.patterns[c] = p->patterns[c].c_str();
   }
   refresh_pipelines(plan.get());
+  // an aggregation table that one generated pipeline alone scans is reset by that scan
+  std::vector<int> scans(desc->nres, 0);
+  for (auto& p : plan->pipes)
+    if (p->desc.source_kind == DQ_SRC_AGG && p->desc.source_res >= 0 && p->desc.source_res < desc->nres)
+      ++scans[p->desc.source_res];
+  for (auto& p : plan->pipes)
+    p->clears_source = p->jit && p->desc.source_kind == DQ_SRC_AGG && p->desc.source_res >= 0 &&
+                       p->desc.source_res < desc->nres && scans[p->desc.source_res] == 1;
   plan->result_res = desc->result_res;
   if (plan->result_res < 0 || plan->result_res >= desc->nres || plan->res[plan->result_res]->desc.kind != DQ_RES_OUTPUT)
     throw DqError(DQ_ERR_BAD_IR, "result must be an OUTPUT resource");
@@ -1112,7 +1256,7 @@ void grow_plan(dq_plan* plan, int status) {
     }
     if ((status & kErrOverflow) && r.desc.kind == DQ_RES_OUTPUT) {
       uint64_t need = 0;
-      DQ_CUDA(cudaMemcpy(&need, r.cursor.ptr, 8, cudaMemcpyDeviceToHost));
+      DQ_CUDA(cudaMemcpy(&need, r.dev.cursor, 8, cudaMemcpyDeviceToHost));
       if (need > r.dev.cap) {
         r.desc.capacity = (int64_t)need;
         setup_resource(plan, r, 1);
@@ -2289,7 +2433,7 @@ void srv_build_graph(PoolEntry* pe, cudaStream_t st) {
   auto rec = [&](cudaError_t e) {
     if (err == cudaSuccess && e != cudaSuccess) err = e;
   };
-  rec(cudaMemcpyAsync(pe->host_out, o.cursor.ptr, 8, cudaMemcpyDeviceToHost, st));
+  rec(cudaMemcpyAsync(pe->host_out, o.dev.cursor, 8, cudaMemcpyDeviceToHost, st));
   if (!pe->count_only)
     for (int j = 0; j < o.desc.npay; ++j)
       rec(cudaMemcpyAsync(pe->host_out + pe->col_off[j], o.dev.pay[j],

@@ -316,12 +316,19 @@ int dq_plan_prepare(dq_ctx* ctx, const dq_plan_desc* desc, dq_plan** out);
  * The counterpart of the reference's generated query file.                 */
 int dq_plan_source(dq_plan* plan, int32_t pipe, char* buf, int64_t cap, int64_t* len);
 /* Runs every pipeline in order on `stream` (NULL: the context stream) and
- * returns a new result.  Resources are reset at the start of each run.       */
+ * returns a new result.  Resources start every run empty.  After a
+ * successful run the same launches are captured as a CUDA graph and replayed
+ * by later executes while the plan's tables and launch shapes stay the same
+ * (DQ_CFG_NO_GRAPH: never); an aggregation table that one pipeline alone
+ * scans is reset by that scan, so the next run needs no initialising kernel. */
 int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out);
 void dq_plan_free(dq_plan* plan);
 
 /* Device time of the last execute (CUDA events on the launching stream):
- * total, and the longest pipeline kernel with its index.                     */
+ * total, and the longest pipeline kernel with its index.  Once a plan has run
+ * successfully, dq_plan_execute replays its launches from a captured CUDA
+ * graph (unless the context has DQ_CFG_NO_GRAPH); a replayed run reports the
+ * total only (pipeline_ms zero, max_pipeline -1).                           */
 typedef struct {
     double total_ms;
     double max_pipeline_ms;
