@@ -135,6 +135,7 @@ void op_reads(const DevPipe& P, const dq_op& op, std::vector<int>& out) {
       add(op.a);
       break;
     case DQ_OP_PROBE:
+    case DQ_OP_EXISTS:
     case DQ_OP_EXPAND:
     case DQ_OP_MM_COUNT:
       add_list(op.list, op.nlist);
@@ -291,6 +292,36 @@ struct Gen {
   }
 
   // ---------------------------------------------------------------- ops --
+  // One ARITH / CMP / LOGIC / CAST / SELECT op (straight-line C).
+  void scalar_op(const dq_op& op) {
+    switch (op.kind) {
+      case DQ_OP_ARITH:
+        L(assign(op.dst, std::string("arith(") + arith_name(op.sub) + ", " + ct_name(op.ctype) + ", " +
+                             operand(op, 0) + ", " + operand(op, 1) + ")", op.ctype));
+        break;
+      case DQ_OP_CMP:
+        L(assign(op.dst, std::string("(uint64_t)compare(") + cmp_name(op.sub) + ", " + ct_name(op.ctype) + ", " +
+                             operand(op, 0) + ", " + operand(op, 1) + ")", DQ_U64));
+        break;
+      case DQ_OP_LOGIC:
+        if (op.sub == DQ_NOT) L(assign(op.dst, "(uint64_t)(" + V(op.a) + " == 0ull)", DQ_U64));
+        else
+          L(assign(op.dst, "(uint64_t)(" + V(op.a) + (op.sub == DQ_AND ? " != 0ull && " : " != 0ull || ") +
+                               V(op.b) + " != 0ull)", DQ_U64));
+        break;
+      case DQ_OP_CAST:
+        L(assign(op.dst, operand(op, 0), op.ctype));
+        break;
+      case DQ_OP_SELECT: {
+        std::string prev = V(op.c >= 0 ? op.c : op.dst);
+        L(assign(op.dst, "(" + V(op.a) + " ? " + operand(op, 1) + " : " + prev + ")", op.ctype));
+        break;
+      }
+      default:
+        throw Error("op kind " + num(op.kind) + " is not a scalar op");
+    }
+  }
+
   void ops_from(int k, int level, const std::string& act, const std::string& exit) {
     for (; k < P.nops; ++k) {
       const dq_op& op = P.ops[k];
@@ -305,27 +336,12 @@ struct Gen {
       }
       switch (op.kind) {
         case DQ_OP_ARITH:
-          L(assign(op.dst, std::string("arith(") + arith_name(op.sub) + ", " + ct_name(op.ctype) + ", " +
-                               operand(op, 0) + ", " + operand(op, 1) + ")", op.ctype));
-          break;
         case DQ_OP_CMP:
-          L(assign(op.dst, std::string("(uint64_t)compare(") + cmp_name(op.sub) + ", " + ct_name(op.ctype) + ", " +
-                               operand(op, 0) + ", " + operand(op, 1) + ")", DQ_U64));
-          break;
         case DQ_OP_LOGIC:
-          if (op.sub == DQ_NOT) L(assign(op.dst, "(uint64_t)(" + V(op.a) + " == 0ull)", DQ_U64));
-          else
-            L(assign(op.dst, "(uint64_t)(" + V(op.a) + (op.sub == DQ_AND ? " != 0ull && " : " != 0ull || ") +
-                                 V(op.b) + " != 0ull)", DQ_U64));
-          break;
         case DQ_OP_CAST:
-          L(assign(op.dst, operand(op, 0), op.ctype));
+        case DQ_OP_SELECT:
+          scalar_op(op);
           break;
-        case DQ_OP_SELECT: {
-          std::string prev = V(op.c >= 0 ? op.c : op.dst);
-          L(assign(op.dst, "(" + V(op.a) + " ? " + operand(op, 1) + " : " + prev + ")", op.ctype));
-          break;
-        }
         case DQ_OP_LIKE:
         case DQ_OP_STREQ: {
           const DevSlot& sl = slot(op.a);
@@ -365,6 +381,11 @@ struct Gen {
             refill_lanes(k, act);
             return;
           }
+          break;
+        case DQ_OP_EXISTS:
+          exists(k, level, act);
+          k += (int)op.imm;  // the condition's ops ran inside the walk
+          skip_if_idle(act, exit);
           break;
         case DQ_OP_EXPAND:
           expand(k, level, act);
@@ -677,6 +698,52 @@ struct Gen {
     }
     skip_if_idle(a, exit);
     ops_from(k + 1, lv, a, exit);
+  }
+
+  // Semi/anti join with a condition (the reference's multimatch semi/anti
+  // probe, dogqc/hashJoins.py:244-272): each lane walks its row's key range
+  // of the multimap; a build row counts when its keys equal the row's and the
+  // condition (ops k+1 .. k+imm, one level down, on the build row's gathered
+  // values and the row's own) holds; the first such row ends the walk.
+  void exists(int k, int level, const std::string& act) {
+    const dq_op& op = P.ops[k];
+    const int r = op.res;
+    const int lv = level + 1;
+    const std::string id = num(uid++);
+    const std::string fm = "xf" + id, m = "xm" + id, me = "xe" + id;
+    L("bool " + fm + " = false;");
+    L("if (" + act + ") {");
+    ++ind;
+    std::string kk = keys(op, r, op.list, op.nlist);
+    L("const uint32_t b_ = bucket_of(" + kk + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap);");
+    L("const uint32_t xc_ = " + res(r) + ".counts[b_];");
+    L("uint32_t " + m + " = xc_ ? " + res(r) + ".offsets[b_] : 0u;");
+    L("const uint32_t " + me + " = " + m + " + xc_;");
+    L("for (; " + m + " < " + me + "; ++" + m + ") {");
+    ++ind;
+    const std::vector<std::string> saved = var;
+    for (int s2 = 0; s2 < P.nslots; ++s2)
+      if (slot(s2).kind == DQ_SLOT_GATHER && slot(s2).level == lv && slot(s2).res == r) gather(s2, "true", m);
+    std::string eq = "true";
+    for (int q = 0; q < op.nlist; ++q) {
+      int t = P.res[r].key_ctype[q];
+      eq += " && canon(" + V(P.lists[op.list + q]) + ", " + ct_name(t) + ") == canon(" + V(P.lists[op.list2 + q]) + ", " +
+            ct_name(t) + ")";
+    }
+    L("if (!(" + eq + ")) continue;");
+    if (op.imm > 0) {
+      declare_regs(lv);
+      for (int j = k + 1; j <= k + (int)op.imm; ++j) scalar_op(P.ops[j]);
+      L("if (" + V(op.a) + " == 0ull) continue;");
+    }
+    L(fm + " = true;");
+    L("break;");
+    var = saved;  // the build row's values end with the walk
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+    L(act + " = " + act + " && " + (op.sub == DQ_JOIN_ANTI ? "!" : "") + fm + ";");
   }
 
   void expand(int k, int level, const std::string& act) {
@@ -1027,7 +1094,8 @@ struct Gen {
     bool heavy = false;
     for (int j = k + 1; j < P.nops; ++j) {
       const int kind = P.ops[j].kind;
-      heavy |= kind == DQ_OP_PROBE || kind == DQ_OP_EXPAND || kind == DQ_OP_LIKE || kind == DQ_OP_STREQ ||
+      heavy |= kind == DQ_OP_PROBE || kind == DQ_OP_EXPAND || kind == DQ_OP_EXISTS || kind == DQ_OP_LIKE ||
+               kind == DQ_OP_STREQ ||
                kind == DQ_OP_BUILD || kind == DQ_OP_MM_COUNT || kind == DQ_OP_MM_SCATTER || kind == DQ_OP_EMIT ||
                (kind == DQ_OP_AGG && agg != AGG_REGS);
     }

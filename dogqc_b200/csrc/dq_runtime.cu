@@ -523,6 +523,7 @@ void slot_reads(const dq_pipeline& d, const dq_op& op, std::vector<int>& out) {
       add(op.a);
       break;
     case DQ_OP_PROBE:
+    case DQ_OP_EXISTS:
     case DQ_OP_EXPAND:
     case DQ_OP_MM_COUNT:
       add_list(op.list, op.nlist);
@@ -555,11 +556,24 @@ void validate_pipeline(const dq_pipeline& d, int nres) {
       throw DqError(DQ_ERR_BAD_IR, "op list out of range");
     bool sink = op.kind >= DQ_OP_AGG;
     if (sink != (i == d.nops - 1)) throw DqError(DQ_ERR_BAD_IR, "the sink must be the last op");
-    if ((op.kind == DQ_OP_PROBE || op.kind == DQ_OP_EXPAND || sink) && (op.res < 0 || op.res >= nres))
+    if ((op.kind == DQ_OP_PROBE || op.kind == DQ_OP_EXPAND || op.kind == DQ_OP_EXISTS || sink) &&
+        (op.res < 0 || op.res >= nres))
       throw DqError(DQ_ERR_BAD_IR, "op resource out of range");
+    if (op.kind == DQ_OP_EXISTS) {
+      // the condition's ops follow it and are plain scalar ops
+      if (op.imm < 0 || i + op.imm >= d.nops - 1 || (op.imm > 0 && op.a < 0) ||
+          (op.sub != DQ_JOIN_SEMI && op.sub != DQ_JOIN_ANTI) || op.nlist != op.nlist2)
+        throw DqError(DQ_ERR_BAD_IR, "malformed EXISTS op");
+      for (int64_t j = i + 1; j <= i + op.imm; ++j) {
+        const int kj = d.ops[j].kind;
+        if (kj != DQ_OP_ARITH && kj != DQ_OP_CMP && kj != DQ_OP_LOGIC && kj != DQ_OP_CAST && kj != DQ_OP_SELECT)
+          throw DqError(DQ_ERR_BAD_IR, "an EXISTS condition holds scalar ops only");
+      }
+    }
     if ((op.kind == DQ_OP_LIKE || op.kind == DQ_OP_STREQ) && (op.res < 0 || op.res >= d.npatterns))
       throw DqError(DQ_ERR_BAD_IR, "pattern index out of range");
-    if (op.nlist > DQ_MAX_KEYS && (op.kind == DQ_OP_PROBE || op.kind == DQ_OP_EXPAND || op.kind == DQ_OP_BUILD ||
+    if (op.nlist > DQ_MAX_KEYS && (op.kind == DQ_OP_PROBE || op.kind == DQ_OP_EXPAND || op.kind == DQ_OP_EXISTS ||
+                                    op.kind == DQ_OP_BUILD ||
                                     op.kind == DQ_OP_AGG || op.kind == DQ_OP_MM_COUNT || op.kind == DQ_OP_MM_SCATTER))
       throw DqError(DQ_ERR_BAD_IR, "too many keys");
   }
@@ -852,6 +866,10 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
 
   // generated kernel (default), else the prebuilt tile or row kernel
   p.jit = !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) && !plan->opts.batch_member;
+  for (int i = 0; i < d.nops; ++i)
+    if (d.ops[i].kind == DQ_OP_EXISTS && !p.jit && !plan->opts.batch_member)
+      throw DqError(DQ_ERR_UNSUPPORTED, "semi/anti joins with conditions run on generated kernels only "
+                                        "(not DQ_CFG_NO_JIT / DQ_CFG_ROW_KERNEL)");
   if (!p.jit)
     for (int k = 0; k < p.desc.nops; ++k)
       if (p.desc.ops[k].kind == DQ_OP_STRREF)

@@ -538,8 +538,11 @@ class Lowering(object):
             if not getattr(node, "multimatch", True):
                 raise Unsupported("outer joins on unique keys (the reference's unique hash table rejects them)")
             jt = "INNER"
-        if node.conditions is not None:
-            raise Unsupported("equi-joins with extra non-equality conditions")
+        semi = jt in ("SEMI", "ANTI")
+        if node.conditions is not None and not semi:
+            # the reference evaluates a join's further conditions only in its
+            # semi and anti probes (hashJoins.py:203-204, 264-265)
+            raise Unsupported("inner and outer joins with further conditions (the reference does not evaluate them)")
         bk = list(node.buildKeyAttributes.values())
         pk = list(node.probeKeyAttributes.values())
         if len(bk) > L.MAX_KEYS:
@@ -551,10 +554,17 @@ class Lowering(object):
                 raise Unsupported("string join keys")
             key_types.append(common_type(tb, tp))
         build_atts = list(node.leftChild.outRelation.values())
-        unique = not getattr(node, "multimatch", True) or jt in ("SEMI", "ANTI")
+        # A semi or anti join asks whether a build row with equal keys exists;
+        # without a further condition only the keys matter (a unique table of
+        # keys, the reference's filter table, hashJoins.py:159-211).  With a
+        # condition every build row of the key may decide, so the build side
+        # becomes a multimap of its keys and the attributes the condition reads,
+        # walked per probe row until a row satisfies it (the reference's
+        # multimatch semi/anti probe, hashJoins.py:244-272).
+        unique = (not getattr(node, "multimatch", True) or semi) and node.conditions is None
         est = max(int(node.leftChild.tupleNum), 1)
         cap = max(int(est * float(getattr(node, "htSizeFactor", 2.0))), 16)
-        if jt in ("SEMI", "ANTI"):
+        if semi and node.conditions is None:
             build_atts = []
         if unique:
             packed = len(bk) == 1 or (len(bk) == 2 and all(t in ("i8", "i32", "u32") for t in key_types))
@@ -577,7 +587,8 @@ class Lowering(object):
                 raise Unsupported("more than %d payload attributes" % L.MAX_PAY)
             rid = self.new_res(Res(L.RES_MULTI, nkeys=len(bk), key_ctype=key_types, pay_ctype=payload,
                                    capacity=cap))
-            info = dict(res=rid, unique=False, bk=bk, pk=pk, build_atts=atts, passes=["count", "scatter"])
+            info = dict(res=rid, unique=False, bk=bk, pk=pk, build_atts=atts, passes=["count", "scatter"],
+                        exists=semi)
         self.joins[id(node)] = info
         for p in info["passes"]:
             info["pass"] = p
@@ -616,6 +627,8 @@ class Lowering(object):
             # fraction of probe rows that find a match (the plan's estimate)
             probe_rows = max(getattr(node.rightChild, "tupleNum", 0), 1)
             op.sel = min(1.0, getattr(node, "tupleNum", probe_rows) / float(probe_rows))
+        elif info.get("exists"):
+            self.exists_probe(node, pipe, info, jt, kl, kn)
         else:
             if pipe.level + 1 >= L.MAX_LEVELS:
                 raise Unsupported("more than %d nested multimatch joins in one pipeline" % (L.MAX_LEVELS - 1))
@@ -629,6 +642,48 @@ class Lowering(object):
             bl, bn = pipe.list_(bkeys)
             pipe.op(L.OP_EXPAND, res=info["res"], list=kl, nlist=kn, list2=bl, nlist2=bn)
             pipe.level = lv
+
+    def exists_probe(self, node, pipe, info, jt, kl, kn):
+        """Semi/anti join with a condition: an EXISTS op walks the probe row's
+        key range of the multimap; for each build row with equal keys the
+        condition's ops (the count that follow it, on the build row's gathered
+        attributes one level down) decide; the first build row that satisfies
+        the condition ends the walk.  The row stays (SEMI) or goes (ANTI)
+        depending on whether one did.  The build attributes are visible to the
+        condition only."""
+        if pipe.level + 1 >= L.MAX_LEVELS:
+            raise Unsupported("more than %d nested multimatch joins in one pipeline" % (L.MAX_LEVELS - 1))
+        lv = pipe.level + 1
+        gathers = []
+        for j, a in enumerate(info["build_atts"]):
+            gathers.append(pipe.slot(L.SLOT_GATHER, lv, lang_type(a.dataType), src=j, res=info["res"]))
+        bkeys = [gathers[info["build_atts"].index(b)] for b in info["bk"]]
+        bl, bn = pipe.list_(bkeys)
+        sub = L.JOIN_SEMI if jt == "SEMI" else L.JOIN_ANTI
+        op = pipe.op(L.OP_EXISTS, sub=sub, res=info["res"], list=kl, nlist=kn, list2=bl, nlist2=bn)
+        probe_rows = max(getattr(node.rightChild, "tupleNum", 0), 1)
+        op.sel = min(1.0, getattr(node, "tupleNum", probe_rows) / float(probe_rows))
+        first = len(pipe.ops)
+        saved_level = pipe.level
+        saved = {a.id: pipe.att.get(a.id) for a in info["build_atts"]}
+        pipe.level = lv
+        for a, g in zip(info["build_atts"], gathers):
+            pipe.att[a.id] = g
+        try:
+            v = self.expr(pipe, node.conditions)
+            v = self.as_slot(pipe, v)
+        finally:
+            pipe.level = saved_level
+            for aid, old in saved.items():
+                if old is None:
+                    pipe.att.pop(aid, None)
+                else:
+                    pipe.att[aid] = old
+        for o in pipe.ops[first:]:
+            if o["kind"] not in (L.OP_ARITH, L.OP_CMP, L.OP_LOGIC, L.OP_CAST, L.OP_SELECT):
+                raise Unsupported("semi/anti join conditions of this form (%d)" % o["kind"])
+        op["a"] = v
+        op["imm"] = len(pipe.ops) - first
 
     # -- aggregation -------------------------------------------------------------
     RED = {"SUM": L.RED_SUM, "AVG": L.RED_SUM, "COUNT": L.RED_COUNT, "MIN": L.RED_MIN, "MAX": L.RED_MAX}

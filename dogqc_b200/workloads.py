@@ -435,10 +435,112 @@ def plan_c10p(alg, scal, Type, Reduction, price_cut=200_000):
     return proj, {sel.opId: {"selectivity": 0.005}, join.opId: {"multimatch": False, "selectivity": 1.0}}
 
 
+# ------------------------------------------------------- c11 .. c13 -------------
+# Semi and anti joins: orders and their line items (TPC-H Q4 / Q21 shapes) and
+# customers without orders (the NOT EXISTS of Q22).
+
+def gen_c11(scale=1.0, seed=BASE_SEED + 11):
+    """Orders (keys a permutation of 1..n, a date, a status flag, a priority)
+    and line items (about four per order; orders whose key is a multiple of 7
+    have none), with a supplier, a commit and a receipt date; a line is late
+    (receipt after commit) about half the time."""
+    no = _n(1_500_000, scale, 64)
+    nl = _n(6_000_000, scale, 256)
+    ns = _n(10_000, scale, 16)
+    r = _rng(seed)
+    okeys = (r.permutation(no) + 1).astype(np.int32)
+    orders = {"o_orderkey": okeys,
+              "o_orderdate": (EPOCH_1992 + r.integers(0, DATE_RANGE, no)).astype(np.int32),
+              "o_orderstatus": np.frombuffer(b"FOP", dtype=np.int8)[r.integers(0, 3, no)],
+              "o_orderpriority": r.integers(1, 6, no, dtype=np.int32)}
+    with_lines = np.arange(1, no + 1, dtype=np.int32)
+    with_lines = with_lines[with_lines % 7 != 0]
+    commit = (EPOCH_1992 + r.integers(0, DATE_RANGE, nl)).astype(np.int32)
+    lines = {"l_orderkey": with_lines[r.integers(0, len(with_lines), nl)],
+             "l_suppkey": r.integers(1, ns + 1, nl, dtype=np.int32),
+             "l_commitdate": commit,
+             "l_receiptdate": (commit + r.integers(-30, 31, nl)).astype(np.int32)}
+    return Database([Table("orders", orders, {"o_orderkey": Type.INT, "o_orderdate": Type.INT,
+                                              "o_orderstatus": Type.CHAR, "o_orderpriority": Type.INT}),
+                     Table("lineitem", lines, {"l_orderkey": Type.INT, "l_suppkey": Type.INT,
+                                               "l_commitdate": Type.INT, "l_receiptdate": Type.INT})])
+
+
+def plan_c11(alg, scal, Type, Reduction, start=EPOCH_1992 + 546, days=92, late_slack=0):
+    """Q4 shape: orders of one quarter that have at least one late line item
+    (EXISTS, a semi join on the order key with no further condition, on a
+    unique filter table), counted per priority.  ``late_slack`` > 60 leaves no
+    late line: the semi join then rejects every order."""
+    late = alg.selection(scal.SmallerExpr(scal.AddExpr(scal.AttrExpr("l_commitdate"),
+                                                       scal.ConstExpr(str(late_slack), Type.INT)),
+                                          scal.AttrExpr("l_receiptdate")),
+                         alg.scan("lineitem"))
+    ords = alg.selection(scal.AndExpr(scal.LargerEqualExpr(scal.AttrExpr("o_orderdate"),
+                                                           scal.ConstExpr(str(start), Type.INT)),
+                                      scal.SmallerExpr(scal.AttrExpr("o_orderdate"),
+                                                       scal.ConstExpr(str(start + days), Type.INT))),
+                         alg.scan("orders"))
+    sj = alg.semijoin(("l_orderkey", "o_orderkey"), None, late, ords)
+    agg = alg.aggregation(["o_orderpriority"], [(Reduction.COUNT, "", "order_count")], sj)
+    cfg = {late.opId: {"selectivity": 0.5},
+           ords.opId: {"selectivity": days / float(DATE_RANGE)},
+           sj.opId: {"multimatch": False, "htSizeFactor": 0.5},
+           agg.opId: {"numgroups": 100}}
+    return agg, cfg
+
+
+def plan_c12(alg, scal, Type, Reduction, multimatch=True):
+    """Q21 shape: late line items (l1) of orders with status 'F' for which
+    another supplier has a line of the same order (EXISTS l2 with
+    l2.suppkey <> l1.suppkey, a semi join with a condition) and no other
+    supplier's line of the order is late (NOT EXISTS l3 ..., an anti join
+    with a condition); waiting lines counted per supplier.  The conditions
+    compare a build-side and a probe-side attribute for every key match."""
+    l1 = alg.selection(scal.LargerExpr(scal.AttrExpr("l1.l_receiptdate"), scal.AttrExpr("l1.l_commitdate")),
+                       alg.scan("lineitem", "l1"))
+    ords = alg.selection(scal.EqualsExpr(scal.AttrExpr("o_orderstatus"), scal.ConstExpr("F", Type.CHAR)),
+                         alg.scan("orders"))
+    j = alg.join(("o_orderkey", "l1.l_orderkey"), ords, l1)
+    l3 = alg.selection(scal.LargerExpr(scal.AttrExpr("l3.l_receiptdate"), scal.AttrExpr("l3.l_commitdate")),
+                       alg.scan("lineitem", "l3"))
+    aj = alg.antijoin(("l3.l_orderkey", "l1.l_orderkey"),
+                      scal.NotExpr(scal.EqualsExpr(scal.AttrExpr("l3.l_suppkey"), scal.AttrExpr("l1.l_suppkey"))),
+                      l3, j)
+    sj = alg.semijoin(("l2.l_orderkey", "l1.l_orderkey"),
+                      scal.NotExpr(scal.EqualsExpr(scal.AttrExpr("l2.l_suppkey"), scal.AttrExpr("l1.l_suppkey"))),
+                      alg.scan("lineitem", "l2"), aj)
+    agg = alg.aggregation(["l1.l_suppkey"], [(Reduction.COUNT, "", "numwait")], sj)
+    cfg = {l1.opId: {"selectivity": 0.5},
+           ords.opId: {"selectivity": 0.33},
+           j.opId: {"multimatch": False, "selectivity": 0.33},
+           l3.opId: {"selectivity": 0.5},
+           aj.opId: {"multimatch": multimatch, "htSizeFactor": 1.0, "selectivity": 0.1},
+           sj.opId: {"multimatch": multimatch, "htSizeFactor": 0.5, "selectivity": 0.1},
+           agg.opId: {"numgroups": 20_000}}
+    return agg, cfg
+
+
+def plan_c13(alg, scal, Type, Reduction, multimatch=False, flag_cut=0):
+    """NOT EXISTS without a further condition (the anti join of TPC-H Q22):
+    customers with no order whose flag is at least ``flag_cut``, counted and
+    their balances summed per nation."""
+    ords = alg.selection(scal.LargerEqualExpr(scal.AttrExpr("o_flag"), scal.ConstExpr(str(flag_cut), Type.INT)),
+                         alg.scan("orders"))
+    aj = alg.antijoin(("o_custkey", "c_custkey"), None, ords, alg.scan("customer"))
+    agg = alg.aggregation(["c_nation"], [(Reduction.COUNT, "", "numcust"), (Reduction.SUM, "c_acctbal", "totacctbal")],
+                          aj)
+    cfg = {ords.opId: {"selectivity": (100 - flag_cut) / 100.0},
+           aj.opId: {"multimatch": multimatch, "selectivity": 0.33},
+           agg.opId: {"numgroups": 25}}
+    return agg, cfg
+
+
 GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5, "c7": gen_c5, "c8": gen_c5,
-              "c9": gen_c9, "c9p": gen_c9, "c10": gen_c10, "c10p": gen_c10}
+              "c9": gen_c9, "c9p": gen_c9, "c10": gen_c10, "c10p": gen_c10, "c11": gen_c11, "c12": gen_c11,
+              "c13": gen_c5}
 PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5, "c7": plan_c7,
-         "c8": plan_c8, "c9": plan_c9, "c9p": plan_c9p, "c10": plan_c10, "c10p": plan_c10p}
+         "c8": plan_c8, "c9": plan_c9, "c9p": plan_c9p, "c10": plan_c10, "c10p": plan_c10p, "c11": plan_c11,
+         "c12": plan_c12, "c13": plan_c13}
 
 
 def build(name, alg, scale=1.0, **kw):

@@ -218,6 +218,14 @@ typedef enum {
     DQ_OP_FILTER = 10,   /* keep rows with a != 0                              */
     DQ_OP_PROBE = 11,    /* unique-HT probe (res); sub: dq_join                */
     DQ_OP_EXPAND = 12,   /* multimap probe (res) opening level+1               */
+    DQ_OP_EXISTS = 13,   /* semi/anti probe of a multimap (res); sub: dq_join  */
+                         /* (SEMI or ANTI).  list: probe keys; list2: the      */
+                         /* build keys' GATHER slots one level down; the `imm` */
+                         /* ops that follow compute slot `a` (the condition)   */
+                         /* from gathered and current values.  The row's key   */
+                         /* range is walked until a build row has equal keys   */
+                         /* and a != 0; SEMI keeps the row if one did, ANTI if */
+                         /* none did; the pipeline continues on this level     */
     DQ_OP_AGG = 20,      /* sink: aggregate into res                           */
     DQ_OP_BUILD = 21,    /* sink: insert into unique HT res                    */
     DQ_OP_MM_COUNT = 22, /* sink: multimap bucket counts                       */

@@ -34,6 +34,18 @@ CASES = {
     "c10_s": dict(workload="c10", scale=0.02, str_cols=[0]),
     "c10p_s": dict(workload="c10p", scale=0.02, str_cols=[0]),
     "c8": dict(workload="c8", scale=1.0),
+    # semi and anti joins: EXISTS without a condition on the reference's filter
+    # table (Q4 shape), EXISTS / NOT EXISTS with a condition on its multimatch
+    # table and on its filter table (Q21 shape), NOT EXISTS alone (Q22's);
+    # an empty build side rejects every probe row
+    "c11_s": dict(workload="c11", scale=0.01),
+    "c11": dict(workload="c11", scale=1.0),
+    "c11_none": dict(workload="c11", scale=0.01, plan_kw=dict(late_slack=100)),
+    "c12_s": dict(workload="c12", scale=0.01),
+    "c12": dict(workload="c12", scale=1.0),
+    "c13_s": dict(workload="c13", scale=0.05),
+    "c13_mm": dict(workload="c13", scale=0.05, plan_kw=dict(multimatch=True)),
+    "c13": dict(workload="c13", scale=1.0),
     # full sizes: row counts, checksums and (small) full results are committed
     "c0": dict(workload="c0", scale=1.0),
     "c1": dict(workload="c1", scale=1.0),

@@ -73,3 +73,20 @@ def test_batches_compile_offline(engine, shape):
     b = batch.prepare_batch(engine, insts, tuning={"rows_per_thread": 2})
     with pytest.raises(L.DqError):
         b.execute()
+
+
+@pytest.mark.parametrize("name", ["c11", "c12", "c13"])
+def test_semi_anti_joins_compile_offline(engine, name):
+    plan = engine.prepare(resolved(engine, name))
+    check_sources(plan)
+
+
+def test_conditioned_semi_join_refused_on_prebuilt_kernels():
+    """EXISTS with a condition has a generated form only."""
+    e = Engine(0, flags=L.CFG_OFFLINE | L.CFG_NO_JIT)
+    try:
+        with pytest.raises(L.DqError) as err:
+            e.prepare(resolved(e, "c12"))
+        assert err.value.status == L.ERR_UNSUPPORTED
+    finally:
+        e.close()

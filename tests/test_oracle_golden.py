@@ -12,7 +12,7 @@ from evaluator import run_plan
 from helpers import golden, golden_cases, make_case, reference_rows
 
 SMALL = [c for c in golden_cases() if golden(c)["spec"]["scale"] < 0.1]
-FULL_FAST = ["c0", "c1", "c5", "c7", "c8"]
+FULL_FAST = ["c0", "c1", "c5", "c7", "c8", "c11", "c12", "c13"]
 
 
 @pytest.mark.parametrize("case", SMALL)
