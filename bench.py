@@ -79,6 +79,17 @@ WORKLOADS = {
            {"workload": "outer_join_two_aggregations", "customer_rows": 150_000, "order_rows": 1_500_000,
             "orders_filter": "flag >= 2 (98%)", "customers_without_orders": "1/3",
             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c11": ("rows/s (EXISTS on a unique key filter table + group by, input rows of both tables per second)",
+            {"workload": "semi_join_exists", "order_rows": 1_500_000, "lineitem_rows": 6_000_000,
+             "orders_filter": "one quarter (3.6%)", "lineitem_filter": "commit < receipt (~48%)", "groups": 5,
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c12": ("rows/s (EXISTS and NOT EXISTS with <> conditions walked over multimaps, input rows per second)",
+            {"workload": "semi_anti_join_conditions", "order_rows": 1_500_000, "lineitem_rows": "3 x 6,000,000",
+             "groups": "~10,000",
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c13": ("rows/s (NOT EXISTS on a unique key filter table + group by, input rows of both tables per second)",
+            {"workload": "anti_join_not_exists", "customer_rows": 150_000, "order_rows": 1_500_000, "groups": 25,
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
 }
 
 
@@ -352,105 +363,120 @@ def run_ours(args, world, rank, local):
         out["join_pairs"] = {"pairs": pairs, "pairs_per_s": pairs * world / (ms_per_step / 1e3)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(db, plan)
+        out["ref_gpu_baseline"] = ref_gpu_baseline(db)
     engine.close()
     return out
 
 
 # ------------------------------------------------------------ CPU baselines --
 
-_WORKER_DB = {}
-
-
-def _oracle_partition(args):
-    """Worker: evaluate the plan over one slice of the fact table."""
-    lo, hi = args
+def _cpu_eval():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from evaluator import run_plan
+    import cpu_eval
+    return cpu_eval
+
+
+def _sized_for(db, plan, seconds, runs):
+    """The workload, or a smaller seeded instance of the same shape, such that
+    `runs` evaluations on all cores take about `seconds` (one run is timed
+    first, after a warm-up run)."""
     from dogqc_b200 import workloads
-    from dogqc_b200.database import Database, Table
-    if "db" not in _WORKER_DB:
-        _WORKER_DB["db"] = workloads.GENERATORS[WORKLOAD](SCALE)
-    db = _WORKER_DB["db"]
-    fact = db["fact"]
-    part = Table("fact", {c: v[lo:hi] for c, v in fact.columns.items()}, fact.types)
-    db2 = Database([db["dim"], part])
-    plan = build_plan(db2)
-    t0 = time.perf_counter()
-    names, rows = run_plan(db2, plan)
-    return names, rows, time.perf_counter() - t0
-
-
-def merge_partials(rows):
-    """Merge per-partition (nation, sum, count) rows: wrapping 64/32-bit adds."""
-    acc = {}
-    for key, s, c in rows:
-        a = acc.setdefault(key, [0, 0])
-        a[0] = (a[0] + s) % (1 << 64)
-        a[1] = (a[1] + c) % (1 << 32)
-    out = []
-    for k, (s, c) in acc.items():
-        out.append((k, s, c - (1 << 32) if c >= 1 << 31 else c))
-    return out
-
-
-def cpu_baseline(db, plan, repeats=2, max_rows=8_000_000):
-    """Single-threaded oracle over the workload (bounded: a few seconds per run;
-    workloads above `max_rows` input rows run on a proportionally smaller seeded
-    instance of the same shape)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from evaluator import run_plan
-    from dogqc_b200 import workloads
-    rows = input_rows(db)
-    what = "full runs of the workload"
-    if rows > max_rows:
-        scale = SCALE * max_rows / rows
+    cpu = _cpu_eval()
+    prep = cpu.Prepared(db, plan)
+    prep.run()                       # warm-up: first touches of fresh memory
+    one = prep.run()[2]
+    scale, what = SCALE, "the full workload"
+    if one * runs > seconds:
+        scale = SCALE * seconds / (one * runs)
         db = workloads.GENERATORS[WORKLOAD](scale)
         plan = build_plan(db)
-        rows = input_rows(db)
-        what = "runs of the same workload at scale %.3f" % scale
-    t0 = time.perf_counter()
-    for _ in range(repeats):
-        run_plan(db, plan)
-    dt = time.perf_counter() - t0
-    return {"value": rows * repeats / dt, "unit": "rows/s", "cores": 1, "kind": "port",
-            "sample": "%d %s (%d input rows each) through the numpy oracle" % (repeats, what, rows)}
+        prep = cpu.Prepared(db, plan)
+        prep.run()
+        what = "the same workload at scale %.4f" % scale
+    return db, plan, prep, what
+
+
+def cpu_baseline(db, plan, seconds=15.0, repeats=5):
+    """The multithreaded C++ evaluation of the same plan IR (oracle/cpu_eval.cpp)
+    on all host cores: the median of `repeats` warm runs, on the full workload
+    or, above about `seconds` of CPU time, a smaller seeded instance of it."""
+    cpu = _cpu_eval()
+    db, plan, prep, what = _sized_for(db, plan, seconds, repeats)
+    times = sorted(prep.run()[2] for _ in range(repeats))
+    dt = times[len(times) // 2]
+    rows = input_rows(db)
+    return {"value": rows / dt, "unit": "rows/s", "cores": prep.threads, "kind": "port",
+            "sample": "median of %d warm runs of %s (%d input rows) through the C++ evaluator of the plan IR "
+                      "(oracle/cpu_eval.cpp), %d threads" % (repeats, what, rows, prep.threads),
+            "ms_per_run": dt * 1e3}
+
+
+def ref_gpu_baseline(db, runs=5):
+    """The reference's own generated pipeline for this workload (its CUDA
+    source from its translator, compiled for sm_100a into oracle/_ref/bin by
+    oracle/ref_harness.py) run on the same seeded tables in this bench run:
+    medians of its own <timing> block (std::clock around each synchronised
+    launch) over `runs` runs."""
+    import shutil
+    import subprocess
+    import tempfile
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from mmdb import write_mmdb
+    from ref_run import parse_timing
+    exe = os.path.join(ROOT, "oracle", "_ref", "bin", WORKLOAD)
+    if SCALE != 1.0 or not os.path.exists(exe):
+        return {"unavailable": "no reference binary for %s at scale %g" % (WORKLOAD, SCALE)}
+    work = tempfile.mkdtemp(prefix="dq_refgpu_")
+    try:
+        write_mmdb(db, os.path.join(work, "mmdb"))
+        timings = []
+        for _ in range(runs):
+            p = subprocess.run([exe], cwd=work, capture_output=True, timeout=300)
+            if p.returncode != 0:
+                return {"unavailable": "reference binary exited with %d" % p.returncode}
+            timings.append(parse_timing(p.stdout.decode("latin-1")))
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    med = {}
+    for k in timings[0]:
+        vals = sorted(t.get(k, 0.0) for t in timings)
+        med[k] = vals[len(vals) // 2]
+    total = med.get("totalKernelTime", 0.0)
+    rows = input_rows(db)
+    return {"binary": "oracle/_ref/bin/%s (the reference's generated pipeline, sm_100a)" % WORKLOAD,
+            "runs": runs, "kernel_ms": {k: v for k, v in med.items() if k.startswith("krnl_")},
+            "total_kernel_ms": total, "rows_per_s": rows / (total / 1e3) if total else None,
+            "timer": "the program's own <timing>: std::clock around each launch and its synchronisation, "
+                     "0.1 ms resolution"}
 
 
 def run_reference(args, world, rank):
-    """The CPU oracle over all host cores: the fact table is split into one slice
-    per core, each worker evaluates the plan on its slice, partial aggregates
-    are merged."""
-    import multiprocessing as mp
+    """The CPU reference arm: the C++ evaluator of the same plan IR on all host
+    cores, one evaluation per step (of a smaller seeded instance of the same
+    workload when `steps` full evaluations would take more than two minutes)."""
     if rank != 0:
         return None
     from dogqc_b200 import workloads
     db = workloads.GENERATORS[WORKLOAD](SCALE)
-    nfact, ndim = db["fact"].size, db["dim"].size
-    cores = os.cpu_count() or 1
-    bounds = [(nfact * i // cores, nfact * (i + 1) // cores) for i in range(cores)]
-    ctx = mp.get_context("spawn")
+    plan = build_plan(db)
+    db, plan, prep, what = _sized_for(db, plan, 120.0, args.warmup + args.steps)
+    rows = input_rows(db)
     times = []
-    with ctx.Pool(cores) as pool:
-        for i in range(args.warmup + args.steps):
-            t0 = time.perf_counter()
-            parts = pool.map(_oracle_partition, bounds)
-            merged = merge_partials([r for _, rows, _ in parts for r in rows])
-            dt = time.perf_counter() - t0
-            worker = max(w for _, _, w in parts)
-            if i >= args.warmup:
-                times.append(worker)
-    # each step: every worker generates its tables, then evaluates; the timed part
-    # is the evaluation (the slowest worker)
+    for i in range(args.warmup + args.steps):
+        dt = prep.run()[2]
+        if i >= args.warmup:
+            times.append(dt)
     step_s = sum(times) / len(times)
-    value = (nfact + ndim) / step_s
+    value = rows / step_s
+    metric, config = WORKLOADS[WORKLOAD]
     return {
-        "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic (seeded)",
-        "config": CONFIG, "impl": "reference",
-        "cpu_baseline": {"kind": "port", "cores": cores, "value": value, "unit": "rows/s",
-                         "sample": "full workload per step; fact table split over %d processes, "
-                                   "dimension built by each; %d groups merged" % (cores, len(merged))},
+        "config": config, "impl": "reference",
+        "cpu_baseline": {"kind": "port", "cores": prep.threads, "value": value, "unit": "rows/s",
+                         "sample": "one evaluation of %s (%d input rows) per step through the C++ evaluator "
+                                   "of the plan IR (oracle/cpu_eval.cpp), %d threads" % (what, rows, prep.threads)},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -797,9 +823,10 @@ def main():
         out = run_served(args, world, rank, local)
     elif args.impl == "ours" and WORKLOAD == "tbl":
         out = run_import(args, world, rank, local)
-    elif args.impl == "reference" and WORKLOAD != "c1":
-        out = {"impl": "reference", "unavailable": "the partitioned CPU reference arm covers the c1 workload; "
-                                                   "the others report cpu_baseline in the ours line"}
+    elif args.impl == "reference" and WORKLOAD not in WORKLOADS:
+        out = {"impl": "reference", "unavailable": "the CPU reference arm evaluates plan workloads (c0-c13); "
+                                                   "the batched, served and import forms report their own "
+                                                   "one-by-one and CPU baselines in the ours line"}
         out = out if rank == 0 else None
     elif args.impl == "reference":
         out = run_reference(args, world, rank)
