@@ -29,7 +29,7 @@ WIDTH = {I8: 1, I32: 4, U32: 4, I64: 8, U64: 8}
 SLOT_COL, SLOT_REG, SLOT_GATHER, SLOT_AGGKEY, SLOT_AGGVAL, SLOT_STR = 1, 2, 3, 4, 5, 6
 # dq_op_kind
 OP_ARITH, OP_CMP, OP_LOGIC, OP_CAST, OP_SELECT, OP_LIKE, OP_STREQ, OP_STRREF = 1, 2, 3, 4, 5, 6, 7, 8
-OP_FILTER, OP_PROBE, OP_EXPAND, OP_EXISTS = 10, 11, 12, 13
+OP_PROFILE, OP_FILTER, OP_PROBE, OP_EXPAND, OP_EXISTS = 9, 10, 11, 12, 13
 OP_AGG, OP_BUILD, OP_MM_COUNT, OP_MM_SCATTER, OP_EMIT = 20, 21, 22, 23, 24
 ADD, SUB, MUL, DIV, MOD = 1, 2, 3, 4, 5
 EQ, NE, LT, LE, GT, GE = 1, 2, 3, 4, 5, 6
@@ -107,7 +107,8 @@ class dq_plan_timing(C.Structure):
 
 class dq_tuning(C.Structure):
     _fields_ = [("rows_per_thread", C.c_int32), ("block_threads", C.c_int32), ("refill", C.c_int32),
-                ("unique_slots_pct", C.c_int32), ("multi_buckets_pct", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("unique_slots_pct", C.c_int32), ("multi_buckets_pct", C.c_int32), ("refill_threshold", C.c_int32),
+                ("defer_threshold", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class dq_server_config(C.Structure):
@@ -175,6 +176,7 @@ EXPORTS = {
     "dq_plan_execute": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dq_plan_free": (None, [C.c_void_p]),
     "dq_plan_source": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
+    "dq_plan_profile": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_uint64)]),
     "dq_plan_timing_get": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_timing)]),
     "dq_result_rows": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "dq_result_ncols": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),

@@ -1,22 +1,31 @@
-"""Autotuner for launch shape and table sizing (dq_tuning).
+"""Autotuner for launch shape, table sizing and divergence handling (dq_tuning).
 
 The reference fixes these choices in its generator: grid 920-1024 CTAs of 128
 threads (dogqc/kernel.py:10-11), hash tables at twice the estimated rows
 (dogqc/hashJoins.py:43) and a lane-refill threshold of 28 of 32 lanes
-(dogqc/cudaDivergenceBuffer.py:15).  Here they are measured: a coordinate
+(dogqc/cudaDivergenceBuffer.py:15, 216).  Here they are measured: a coordinate
 search over the knobs below, each candidate prepared (its kernels generated and
 compiled, its tables sized) and timed on the device with CUDA events, the
-fastest kept.  Results are cached per plan shape for the life of the process.
+fastest kept.  Results are cached per plan shape, in the process and in a JSON
+file (``DOGQC_B200_TUNING_CACHE``, default ``~/.cache/dogqc_b200/tuning.json``)
+keyed by the plan shape, the device name and the library's ABI version, so a
+later process starts from the tuned values.
 
 Knobs (the dq_tuning fields):
   rows_per_thread    consecutive rows one thread loads and processes per step
   block_threads      threads per CTA of the generated kernels
   refill             -1 turns the plan's lane refill off
+  refill_threshold   buffered rows that make a warp process them (the
+                     reference's 28 of 32; 0: 32, full warps only)
+  defer_threshold    expansion ranges longer than this are deferred and
+                     grouped (the expansion granularity; 0: adaptive)
   unique_slots_pct   join-table slots as % of the plan's estimate (load factor;
                      0 is the backend's size-dependent default)
   multi_buckets_pct  multimap buckets as % of the plan's estimate
 """
 import hashlib
+import json
+import os
 
 import numpy as np
 
@@ -24,11 +33,51 @@ KNOBS = [
     ("rows_per_thread", [1, 2, 4]),
     ("block_threads", [128, 256, 512]),
     ("refill", [0, -1]),
+    ("refill_threshold", [0, 28, 24, 16]),
+    ("defer_threshold", [0, 8, 32, 128, 512]),
     ("unique_slots_pct", [0, 200, 400, 800]),
     ("multi_buckets_pct", [100, 50, 25, 200]),
 ]
 
 _cache = {}
+
+
+def cache_path():
+    return os.environ.get("DOGQC_B200_TUNING_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "dogqc_b200", "tuning.json"))
+
+
+def _disk_load():
+    try:
+        with open(cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _disk_store(key, tuning, seconds):
+    """Adds one entry (atomic rename; a concurrent writer loses at worst its own entry)."""
+    path = cache_path()
+    data = _disk_load()
+    data[key] = {"tuning": tuning, "seconds": seconds}
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = "%s.%d.tmp" % (path, os.getpid())
+        with open(tmp, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+
+
+def _device_tag(engine):
+    try:
+        import torch
+        name = torch.cuda.get_device_name(getattr(engine, "device", 0))
+    except Exception:
+        name = "device"
+    from dogqc_b200 import _lib
+    return "%s|abi%d" % (name, _lib.ABI_VERSION)
 
 
 def shape_key(lowering):
@@ -100,15 +149,28 @@ def plan_measure(engine, lowering, reps=3, warmup=1):
     return measure
 
 
-def tune_batch(engine, lowerings, knobs=KNOBS, reps=3):
-    key = ("batch", shape_key(lowerings[0]), len(lowerings))
-    if key not in _cache:
-        _cache[key] = coordinate_search(batch_measure(engine, lowerings, reps), knobs)
+def _tuned(key, engine, search):
+    """(best tuning, its seconds, search log): from this process's cache, the
+    file cache (no log: not searched here), or a new search that is stored."""
+    if key in _cache:
+        return _cache[key]
+    disk_key = "%s|%s" % (key, _device_tag(engine))
+    hit = _disk_load().get(disk_key)
+    if hit is not None:
+        _cache[key] = (hit["tuning"], hit["seconds"], [])
+        return _cache[key]
+    best, t, log = search()
+    _cache[key] = (best, t, log)
+    if t is not None:
+        _disk_store(disk_key, best, t)
     return _cache[key]
+
+
+def tune_batch(engine, lowerings, knobs=KNOBS, reps=3):
+    key = "batch|%s|%d" % (shape_key(lowerings[0]), len(lowerings))
+    return _tuned(key, engine, lambda: coordinate_search(batch_measure(engine, lowerings, reps), knobs))
 
 
 def tune_plan(engine, lowering, knobs=KNOBS, reps=3):
-    key = ("plan", shape_key(lowering))
-    if key not in _cache:
-        _cache[key] = coordinate_search(plan_measure(engine, lowering, reps), knobs)
-    return _cache[key]
+    key = "plan|%s" % shape_key(lowering)
+    return _tuned(key, engine, lambda: coordinate_search(plan_measure(engine, lowering, reps), knobs))

@@ -13,11 +13,16 @@ is invoked bottom-up by ``translateToCompilerPlan`` and returns light plan
 nodes; ``gencode`` lowers the plan into the pipeline IR; ``compile`` prepares it
 on the device through the C ABI (no nvcc at query time); ``execute`` runs it,
 prints the reference's ``Result: N tuples`` summary and ``<timing>`` block, and
-returns the ``Result``.  ``setBuffers`` and ``setProfilers`` are accepted.  The
-knobs the reference reads from class attributes (``KernelCall.default*``,
+returns the ``Result``.  ``setBuffers`` places the lane refill after the given
+selections and joins, as the reference places its ``LaneRefill`` (without it,
+one refill per pipeline follows its first selective filter or probe);
+``setProfilers`` adds lane-activity histograms where the given operators hand
+their rows on, printed after the ``<timing>`` block.  The knobs the reference
+reads from class attributes (``KernelCall.default*``,
 ``EquiJoinTranslator.usePushDownJoin``) do not apply: launch shapes come from
-the device, lane refill is done by compacting the tile after every filter or
-probe, and expansion is always pushed down to the CTA.
+the device (or ``dq_tuning``), and multimatch probes always walk their match
+ranges warp-cooperatively, the reference's push-down, with long ranges deferred
+and grouped by range.
 
 Tables are read from the database behind the plan context: a
 ``dogqc_b200.database.Database`` (host columns), or the reference's accessor
@@ -50,6 +55,7 @@ class Backend(object):
         self.decimalRepr = decimalRepr
         self.debug = debug
         self.bufferPositions = []
+        self._buffers_set = False
         self.profilerPositions = []
         self.engine = engine
         self.device = device
@@ -63,14 +69,29 @@ class Backend(object):
         return TranslatedNode(algebraExpr, [c for c in (child1, child2) if c is not None])
 
     def setBuffers(self, positions):
+        """Lane refill after these operators (selection or join ids) and
+        nowhere else, where the reference places its LaneRefill
+        (dogqc/cudaTranslator.py:59-63, 84-86); without a call the backend
+        places one refill per pipeline after its first selective filter or
+        probe."""
         self.bufferPositions = list(positions)
+        self._buffers_set = True
 
     def setProfilers(self, positions):
+        """Lane-activity histograms (warp steps by active lanes) where these
+        operators hand their rows to their parents, as the reference's
+        LaneActivityProfiler counts them (dogqc/cudaLaneActivityProfile.py);
+        printed by execute() and returned by profiles()."""
         self.profilerPositions = list(positions)
 
     def gencode(self, translationPlan):
         roots = [t.algExpr if isinstance(t, TranslatedNode) else t for t in translationPlan]
-        self.lowering = Lowering(roots, {"buffers": self.bufferPositions})
+        options = {}
+        if self._buffers_set:
+            options["buffers"] = list(self.bufferPositions)
+        if self.profilerPositions:
+            options["profilers"] = list(self.profilerPositions)
+        self.lowering = Lowering(roots, options)
         return self.lowering
 
     def _database(self):
@@ -105,8 +126,20 @@ class Backend(object):
                 sys.stdout.write("%32s: %6.3f ms\n" % ("pipeline%d" % i, ms))
             sys.stdout.write("%32s: %6.3f ms\n" % ("totalKernelTime", t["total_ms"]))
             sys.stdout.write("</timing>\n")
+            for op_id, counts in self.profiles().items():
+                sys.stdout.write("<p%d>\n" % op_id)
+                sys.stdout.write("".join("%d, %d\n" % (i, c) for i, c in enumerate(counts)))
+                sys.stdout.write("</p%d>\n\n" % op_id)
             sys.stdout.flush()
         return self.result
+
+    def profiles(self):
+        """Operator id -> lane-activity histogram of the last execute (33
+        counts: warp steps with 0..32 active lanes as the operator handed its
+        rows on), for the operators given to setProfilers."""
+        if self.plan is None or self.lowering is None:
+            return {}
+        return {op_id: self.plan.profile(i) for i, op_id in enumerate(self.lowering.profile_points)}
 
     def showGraph(self, plan):
         raise NotImplementedError("plan graphs need graphviz, which this image does not ship")

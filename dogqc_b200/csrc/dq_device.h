@@ -155,6 +155,7 @@ struct DevPipe {
   int32_t* status;
   uint32_t* tile_counter;      // dynamic tile scheduler
   uint64_t* scratch_ll;        // misc device counters
+  uint64_t* profile;           // lane-activity histograms, 33 bins a profile point
 };
 
 // ---------------------------------------------------------------- batches --

@@ -174,6 +174,7 @@ struct Gen {
   std::map<int, std::string> pending;  // gathered slots not loaded yet -> match index
   int min_blocks = 0;            // __launch_bounds__ minimum CTAs per SM (0: none)
   int refill = -1;               // op after which lanes are refilled (-1: none)
+  int refill_threshold = 32;     // buffered rows that make the warp process them
   int nbuf = 0;                  // values per row in the warp buffers
   int buf_off = 0;               // shared-memory offset of the warp buffers
   int hot = 0;                   // multimap sink through the CTA's hot-bucket table:
@@ -366,6 +367,12 @@ struct Gen {
             ";");
           break;
         }
+        case DQ_OP_PROFILE:
+          L("{");
+          L("  const unsigned pm_ = __ballot_sync(kFull, " + act + ");");
+          L("  if (lane == 0) atomicAdd((unsigned long long*)(P.profile + " + num(op.res * 33) + " + __popc(pm_)), 1ull);");
+          L("}");
+          break;
         case DQ_OP_FILTER:
           L(act + " = " + act + " && (" + V(op.a) + " != 0ull);");
           skip_if_idle(act, exit);
@@ -1232,7 +1239,7 @@ struct Gen {
     L("} while (0);");
     L("__syncwarp();");
     L("const bool last_ = " + last_step + " && u == " + num(U - 1) + ";");
-    L("while (wn >= 32 || (last_ && wn > 0)) {");
+    L("while (wn >= " + num(refill_threshold) + " || (last_ && wn > 0)) {");
     ++ind;
     L("bool ra = lane < wn;");
     j = 0;
@@ -1767,6 +1774,7 @@ Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t
   if (const char* e = getenv("DQ_JIT_ROWS")) rows = atoi(e);
   if (rows > 0 && !has_expand && P.source_kind != DQ_SRC_AGG) g.U = rows >= 4 ? 4 : rows >= 2 ? 2 : 1;
   if (t.refill < 0) refill_op = -1;
+  if (t.refill_threshold >= 1 && t.refill_threshold <= 32) g.refill_threshold = t.refill_threshold;
   if (const char* e = getenv("DQ_JIT_MIN_BLOCKS")) g.min_blocks = std::min(8, std::max(0, atoi(e)));
   if (const char* e = getenv("DQ_JIT_LOAD")) {
     std::string s(e);

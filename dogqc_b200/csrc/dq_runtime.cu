@@ -240,6 +240,7 @@ struct PlanOpts {
   bool batch_member = false;  // no standalone kernels, no deferred expansion
   int unique_pct = 0;         // join-table slots, % of the plan's capacity (0: by size)
   int multi_pct = 100;        // multimap buckets, % of the plan's capacity
+  int defer_threshold = 0;    // expansion ranges longer than this are deferred (0: adaptive)
   jit::Tuning tuning;
 };
 
@@ -251,10 +252,13 @@ struct dq_plan {
   int result_res = -1;
   // The words every run starts from zero, in one buffer so that one memset
   // clears them: the status word (8 bytes), two tile counters per pipeline,
-  // then one row cursor per resource (used by OUTPUT resources).
+  // then one row cursor per resource (used by OUTPUT resources), then the
+  // lane-activity histograms of the plan's profile points (33 bins each).
   DevBuf status;
   uint32_t* counters = nullptr;
   uint64_t* cursors = nullptr;
+  uint64_t* profile = nullptr;
+  int nprofile = 0;
   dq_plan_timing timing{};
   std::vector<cudaEvent_t> events;
   std::vector<DevStr> str_src;  // string columns the pipelines read: string references index these
@@ -606,6 +610,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   P.source_kind = d.source_kind;
   P.source_res = d.source_res;
   P.status = plan->status.as<int32_t>();
+  P.profile = plan->profile;
 
   // resources: the pipeline sees the plan's resources under the same indices
   if (plan->res.size() > (size_t)kMaxRes) throw DqError(DQ_ERR_UNSUPPORTED, "more than 8 resources in a plan");
@@ -777,7 +782,9 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     H.grouped = plan->opts.batch_member || !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) ? 1 : 0;
     const uint64_t dflt = H.grouped ? (p.heavy_threshold ? p.heavy_threshold : (uint64_t)kGroupThreshold)
                                     : (uint64_t)tile * 8;
-    H.threshold = ctx->cfg.defer_threshold > 0 ? (uint64_t)ctx->cfg.defer_threshold : dflt;
+    H.threshold = ctx->cfg.defer_threshold > 0    ? (uint64_t)ctx->cfg.defer_threshold
+                  : plan->opts.defer_threshold > 0 ? (uint64_t)plan->opts.defer_threshold
+                                                   : dflt;
     if (H.grouped && !p.heavy_stats && !ctx->offline && !plan->opts.batch_member)
       DQ_CUDA(cudaMallocHost((void**)&p.heavy_stats, 8));
     if (plan->opts.batch_member) break;  // the batch holds the buffers, shared by its instances
@@ -867,9 +874,9 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   // generated kernel (default), else the prebuilt tile or row kernel
   p.jit = !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) && !plan->opts.batch_member;
   for (int i = 0; i < d.nops; ++i)
-    if (d.ops[i].kind == DQ_OP_EXISTS && !p.jit && !plan->opts.batch_member)
-      throw DqError(DQ_ERR_UNSUPPORTED, "semi/anti joins with conditions run on generated kernels only "
-                                        "(not DQ_CFG_NO_JIT / DQ_CFG_ROW_KERNEL)");
+    if ((d.ops[i].kind == DQ_OP_EXISTS || d.ops[i].kind == DQ_OP_PROFILE) && !p.jit && !plan->opts.batch_member)
+      throw DqError(DQ_ERR_UNSUPPORTED, "semi/anti joins with conditions and lane-activity profiles run on "
+                                        "generated kernels only (not DQ_CFG_NO_JIT / DQ_CFG_ROW_KERNEL)");
   if (!p.jit)
     for (int k = 0; k < p.desc.nops; ++k)
       if (p.desc.ops[k].kind == DQ_OP_STRREF)
@@ -1195,10 +1202,19 @@ std::unique_ptr<dq_plan> make_plan(dq_ctx* ctx, const dq_plan_desc* desc, const 
   std::unique_ptr<dq_plan> plan(new dq_plan());
   plan->ctx = ctx;
   plan->opts = opts;
-  plan->status.alloc(8 + 8 * (size_t)desc->npipes + 8 * (size_t)std::max(desc->nres, 0));
+  for (int i = 0; i < desc->npipes; ++i)
+    for (int k = 0; k < desc->pipes[i].nops && k < DQ_MAX_OPS; ++k)
+      if (desc->pipes[i].ops[k].kind == DQ_OP_PROFILE) {
+        const int r = desc->pipes[i].ops[k].res;
+        if (r < 0 || r >= 1024) throw DqError(DQ_ERR_BAD_IR, "profile point out of range");
+        plan->nprofile = std::max(plan->nprofile, r + 1);
+      }
+  const size_t ctrl = 8 + 8 * (size_t)desc->npipes + 8 * (size_t)std::max(desc->nres, 0);
+  plan->status.alloc(ctrl + 33 * 8 * (size_t)plan->nprofile);
   if (plan->status.ptr) {
     plan->counters = reinterpret_cast<uint32_t*>(plan->status.as<uint8_t>() + 8);
     plan->cursors = reinterpret_cast<uint64_t*>(plan->status.as<uint8_t>() + 8 + 8 * (size_t)desc->npipes);
+    if (plan->nprofile) plan->profile = reinterpret_cast<uint64_t*>(plan->status.as<uint8_t>() + ctrl);
   }
   // row bound for multimap payloads: rows of the source of the pipeline that scatters into it
   std::vector<int64_t> bound(desc->nres, 1);
@@ -1310,7 +1326,7 @@ bool grow_heavy(dq_plan* plan) {
 // threshold to kGroupThresholdLow for the runs that follow, fewer than 2 raise
 // it back (the runs' results do not depend on it).
 void adapt_threshold(dq_plan* plan) {
-  if (plan->ctx->cfg.defer_threshold > 0) return;
+  if (plan->ctx->cfg.defer_threshold > 0 || plan->opts.defer_threshold > 0) return;
   for (auto& pp : plan->pipes) {
     PipeRec& p = *pp;
     if (p.expand_op < 0 || !p.heavy_stats || !p.dev.heavy.grouped) continue;
@@ -1337,6 +1353,7 @@ jit::Tuning tuning_of(const dq_tuning* t) {
     j.rows_per_thread = t->rows_per_thread;
     j.block = t->block_threads;
     j.refill = t->refill;
+    j.refill_threshold = t->refill_threshold;
   }
   return j;
 }
@@ -1346,6 +1363,7 @@ PlanOpts opts_of(const dq_tuning* t) {
   o.tuning = tuning_of(t);
   if (t && t->unique_slots_pct > 0) o.unique_pct = t->unique_slots_pct;
   if (t && t->multi_buckets_pct > 0) o.multi_pct = t->multi_buckets_pct;
+  if (t && t->defer_threshold > 0) o.defer_threshold = t->defer_threshold;
   return o;
 }
 
@@ -1378,7 +1396,10 @@ void setup_batch_heavy(dq_batch* b, size_t p, BatchStage& S) {
   H.cap = (uint32_t)std::min<int64_t>(std::max<int64_t>(rows, 1),
                                       std::max<int64_t>(1 << 20, (int64_t)b->heavy_cap));
   const uint64_t groups = std::min<uint64_t>(
-      H.cap, build_rows / (std::max<uint64_t>(H.threshold, kBatchGroupThreshold) + 1) + (uint64_t)b->ninst);
+      H.cap, build_rows / ((b->inst[0]->opts.defer_threshold > 0 ? H.threshold
+                                                                   : std::max<uint64_t>(H.threshold, kBatchGroupThreshold)) +
+                           1) +
+                 (uint64_t)b->ninst);
   H.gcap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(64, 2 * groups), 0xfffffff0ull);
   S.h_items.alloc((size_t)H.cap * H.words * 8);
   S.h_count.alloc(8);
@@ -1433,7 +1454,9 @@ void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
       descs[i] = pl.pipes[p]->dev;
       descs[i].status = b->status.as<int32_t>();
       if (p0.expand_op >= 0) {
-        const uint64_t threshold = std::max<uint64_t>(descs[i].heavy.threshold, kBatchGroupThreshold);
+        const uint64_t threshold = pl.opts.defer_threshold > 0
+                                       ? (uint64_t)pl.opts.defer_threshold
+                                       : std::max<uint64_t>(descs[i].heavy.threshold, kBatchGroupThreshold);
         descs[i].heavy = S.heavy;
         descs[i].heavy.threshold = threshold;
         descs[i].tile_counter = S.h_units.as<uint32_t>();
@@ -2063,6 +2086,18 @@ void dq_plan_free(dq_plan* plan) {
   cudaSetDevice(plan->ctx->device);
   free_events(plan);
   delete plan;
+}
+
+int dq_plan_profile(dq_plan* plan, int32_t point, uint64_t* counts) {
+  if (!plan || !counts) return DQ_ERR_INVALID;
+  if (point < 0 || point >= plan->nprofile) return fail(plan->ctx, DQ_ERR_NOT_FOUND, "no such profile point");
+  return guarded(plan->ctx, [&]() {
+    if (plan->ctx->offline) throw DqError(DQ_ERR_UNSUPPORTED, "an offline context has no profiles");
+    std::lock_guard<std::mutex> lk(plan->ctx->mu);
+    DQ_CUDA(cudaSetDevice(plan->ctx->device));
+    DQ_CUDA(cudaMemcpy(counts, plan->profile + (size_t)point * 33, 33 * 8, cudaMemcpyDeviceToHost));
+    return (int)DQ_OK;
+  });
 }
 
 int dq_plan_source(dq_plan* plan, int32_t pipe, char* buf, int64_t cap, int64_t* len) {

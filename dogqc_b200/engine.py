@@ -133,6 +133,13 @@ class Plan(object):
         L.check(lib.dq_plan_source(self.handle, pipe, buf, n.value + 1, C.byref(n)), self.engine.ctx)
         return buf.value.decode()
 
+    def profile(self, point):
+        """Lane-activity histogram of profile point ``point`` in the last
+        execute: 33 counts, warp steps with 0..32 active lanes."""
+        counts = (C.c_uint64 * 33)()
+        L.check(L.lib().dq_plan_profile(self.handle, point, counts), self.engine.ctx)
+        return list(counts)
+
     def timing(self):
         t = L.dq_plan_timing()
         L.check(L.lib().dq_plan_timing_get(self.handle, C.byref(t)))
@@ -179,6 +186,13 @@ class Batch(object):
         L.check(L.lib().dq_batch_execute(self.handle, stream, out), self.engine.ctx)
         return [_take_result(C.c_void_p(out[i]), self.lowerings[i].result_names) for i in range(n)]
 
+    def profile(self, point):
+        """Lane-activity histogram of profile point ``point`` in the last
+        execute: 33 counts, warp steps with 0..32 active lanes."""
+        counts = (C.c_uint64 * 33)()
+        L.check(L.lib().dq_plan_profile(self.handle, point, counts), self.engine.ctx)
+        return list(counts)
+
     def timing(self):
         t = L.dq_plan_timing()
         L.check(L.lib().dq_batch_timing_get(self.handle, C.byref(t)))
@@ -210,6 +224,7 @@ class Engine(object):
         handle = C.c_void_p()
         L.check(L.lib().dq_init(C.byref(cfg), C.byref(handle)))
         self.ctx = handle
+        self.device = device
         self.registered = {}
 
     @staticmethod

@@ -45,8 +45,10 @@ NP_DTYPE = {L.I8: "int8", L.I32: "int32", L.U32: "uint32", L.I64: "int64", L.U64
 
 class _Op(dict):
     """One IR op (its fields), plus the plan's estimate of the fraction of rows
-    that pass it (filters and probes), which places the lane refill."""
+    that pass it (filters and probes) and the id of the algebra operator it
+    came from, which place the lane refill."""
     sel = 1.0
+    origin = None
 
 
 # A filter or probe whose estimated pass fraction is at most this refills the
@@ -56,13 +58,25 @@ L2_TABLE_BYTES = 48 << 20   # join tables the runtime gives 4x slots (they stay 
 NARROW = ("i8", "i32", "u32")
 
 
-def refill_point(ops):
-    """1 + index of the first level-0 filter/probe that passes at most
-    REFILL_SELECTIVITY of its rows (the ``compact`` field of dq_pipeline), or 0."""
+def refill_point(ops, buffers=None):
+    """The ``compact`` field of dq_pipeline: 1 + the index of the level-0
+    filter or probe after which the lanes are refilled, or 0.
+
+    ``buffers`` (``Backend.setBuffers``): the operator ids the reference wraps
+    in its ``LaneRefill`` (dogqc/cudaTranslator.py:84-86) -- the refill goes
+    after the filter of such a selection or the probe of such a join, the first
+    of them in the pipeline; a pipeline with none has no refill, as in the
+    reference.  Without positions: after the first filter or probe estimated to
+    pass at most REFILL_SELECTIVITY of its rows."""
     for k, o in enumerate(ops):
         if o["kind"] == L.OP_EXPAND:
             break
-        if o["kind"] in (L.OP_FILTER, L.OP_PROBE) and getattr(o, "sel", 1.0) <= REFILL_SELECTIVITY:
+        if o["kind"] not in (L.OP_FILTER, L.OP_PROBE):
+            continue
+        if buffers is not None:
+            if getattr(o, "origin", None) in buffers:
+                return k + 1
+        elif getattr(o, "sel", 1.0) <= REFILL_SELECTIVITY:
             return k + 1
     return 0
 
@@ -228,6 +242,7 @@ class Lowering(object):
         self.temp = {}
         self.parent = {}
         self.joins = {}   # id(EquiJoin node) -> build information
+        self.profile_points = []   # operator ids with a lane-activity profile, by point
         for r in self.roots:
             self._link(r, None)
         for r in self.roots:
@@ -297,7 +312,7 @@ class Lowering(object):
         """Continue ``pipe`` (which delivers ``child``'s rows) at ``node``."""
         k = type(node).__name__
         if k == "Selection":
-            self.filter(pipe, node.condition, getattr(node, "selectivity", 1.0))
+            self.filter(pipe, node.condition, getattr(node, "selectivity", 1.0), origin=node.opId)
             self.consume_parent(node, pipe)
         elif k == "Map":
             v = self.expr(pipe, node.expression)
@@ -317,7 +332,7 @@ class Lowering(object):
                 self.join_build_sink(node, pipe)
             else:
                 self.join_probe(node, pipe)
-                self.filter(pipe, node.condition, getattr(node, "selectivity", 1.0))
+                self.filter(pipe, node.condition, getattr(node, "selectivity", 1.0), origin=node.opId)
                 self.consume_parent(node, pipe)
         elif k == "Aggregation":
             self.aggregate(node, pipe)
@@ -327,6 +342,13 @@ class Lowering(object):
             raise Unsupported("operator %s" % k)
 
     def consume_parent(self, node, pipe):
+        if node.opId in self.options.get("profilers", ()):
+            # the reference's LaneActivityProfiler sits between the operator
+            # and its parent (dogqc/cudaTranslator.py:87-88): count the lanes
+            # still active as the operator hands its rows on
+            if node.opId not in self.profile_points:
+                self.profile_points.append(node.opId)
+            pipe.op(L.OP_PROFILE, res=self.profile_points.index(node.opId))
         parent = self.parent[id(node)]
         if parent is None:
             raise Unsupported("plan root %s is not a materialisation" % type(node).__name__)
@@ -513,13 +535,15 @@ class Lowering(object):
             raise Unsupported("string constant used as a value")
         return v
 
-    def filter(self, pipe, condition, selectivity=1.0):
+    def filter(self, pipe, condition, selectivity=1.0, origin=None):
         v = self.expr(pipe, condition)
         if isinstance(v, Imm):
             if v.value != 0:
                 return
             v = self.materialize_value(pipe, v, "i32")
-        pipe.op(L.OP_FILTER, a=v).sel = selectivity
+        op = pipe.op(L.OP_FILTER, a=v)
+        op.sel = selectivity
+        op.origin = origin
 
     # -- joins -------------------------------------------------------------------
     def produce_join(self, node):
@@ -624,6 +648,7 @@ class Lowering(object):
             pl, pn = pipe.list_(dsts)
             sub = {"INNER": L.JOIN_INNER, "SEMI": L.JOIN_SEMI, "ANTI": L.JOIN_ANTI}[jt]
             op = pipe.op(L.OP_PROBE, sub=sub, res=info["res"], list=kl, nlist=kn, list2=pl, nlist2=pn)
+            op.origin = node.opId
             # fraction of probe rows that find a match (the plan's estimate)
             probe_rows = max(getattr(node.rightChild, "tupleNum", 0), 1)
             op.sel = min(1.0, getattr(node, "tupleNum", probe_rows) / float(probe_rows))
@@ -863,7 +888,7 @@ class Lowering(object):
             for j, pat in enumerate(p.patterns):
                 keep.append(pat)
                 d.patterns[j] = pat
-            d.compact = refill_point(p.ops)
+            d.compact = refill_point(p.ops, self.options.get("buffers"))
         desc = L.dq_plan_desc()
         desc.abi_version = L.ABI_VERSION
         desc.nres = len(self.res)

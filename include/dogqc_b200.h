@@ -215,6 +215,9 @@ typedef enum {
     DQ_OP_STRREF = 8,    /* dst = reference to string slot a's value: the     */
                          /* plan's string source << 48 | row (a U64 value that */
                          /* group keys and output columns carry)               */
+    DQ_OP_PROFILE = 9,   /* lane-activity counter `res`: each warp step that   */
+                         /* passes adds 1 to bin (active lanes, 0..32) of the  */
+                         /* point's histogram (dq_plan_profile)                */
     DQ_OP_FILTER = 10,   /* keep rows with a != 0                              */
     DQ_OP_PROBE = 11,    /* unique-HT probe (res); sub: dq_join                */
     DQ_OP_EXPAND = 12,   /* multimap probe (res) opening level+1               */
@@ -331,6 +334,12 @@ int dq_plan_source(dq_plan* plan, int32_t pipe, char* buf, int64_t cap, int64_t*
  * scans is reset by that scan, so the next run needs no initialising kernel. */
 int dq_plan_execute(dq_plan* plan, void* stream, dq_result** out);
 void dq_plan_free(dq_plan* plan);
+/* Lane-activity histogram of profile point `point` (DQ_OP_PROFILE res) over
+ * the last execute: counts[i] = warp steps that reached the point with i of
+ * their 32 lanes active (33 bins).  The reference's LaneActivityProfiler,
+ * placed by CudaCompiler.setProfilers (dogqc/cudaLaneActivityProfile.py:10-35,
+ * dogqc/cudaTranslator.py:65-89).  DQ_ERR_NOT_FOUND: no such point.         */
+int dq_plan_profile(dq_plan* plan, int32_t point, uint64_t* counts);
 
 /* Device time of the last execute (CUDA events on the launching stream):
  * total, and the longest pipeline kernel with its index.  Once a plan has run
@@ -359,7 +368,12 @@ typedef struct {
                                      /* capacity (default 400 for tables of     */
                                      /* up to 48 MB there, else 200)            */
     int32_t multi_buckets_pct;       /* multimap buckets, % (default 100)       */
-    int32_t reserved[3];
+    int32_t refill_threshold;        /* lane refill: buffered rows that make a  */
+                                     /* warp process them, 1..32 (default 32;   */
+                                     /* the reference's 0.9 x 32 = 28)          */
+    int32_t defer_threshold;         /* expansion ranges longer than this are   */
+                                     /* deferred (0: adaptive, 128 or 8)        */
+    int32_t reserved[1];
 } dq_tuning;
 int dq_plan_prepare_tuned(dq_ctx* ctx, const dq_plan_desc* desc, const dq_tuning* tuning, dq_plan** out);
 

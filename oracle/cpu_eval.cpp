@@ -699,6 +699,8 @@ struct Plan {
           for (int j = 0; j < L.nsel; ++j) dst[L.sel[j]] = base | (uint64_t)L.srow[L.sel[j]];
           break;
         }
+        case DQ_OP_PROFILE:  // lane-activity counters are a device measurement
+          break;
         case DQ_OP_FILTER: {
           const uint64_t* x = L.slot(op.a);
           int m = 0;

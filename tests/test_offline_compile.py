@@ -90,3 +90,46 @@ def test_conditioned_semi_join_refused_on_prebuilt_kernels():
         assert err.value.status == L.ERR_UNSUPPORTED
     finally:
         e.close()
+
+
+def test_set_buffers_places_the_refill_where_the_reference_does(engine):
+    """Without setBuffers the c0 filter (96% pass) gets no refill; with the
+    selection's id the generated kernel refills after it, as the reference's
+    LaneRefill does (ref_c0_lr pins its results)."""
+    from dogqc_b200.backend import Backend
+    db = W.GENERATORS["c0"](SCALE)
+    engine.register_database(db)
+    srcs = []
+    for positions in (None, "selection"):
+        alg = RelationalAlgebra(db)
+        plan, cfg = W.build("c0", alg)
+        plan = alg.resolveAlgebraPlan(plan, cfg)
+        b = Backend(alg, engine=engine)
+        if positions:
+            b.setBuffers([alg.selectionNodes[0].opId])
+        b.gencode(alg.translateToCompilerPlan(plan, b))
+        b.compile("c0")
+        srcs.append(b.plan.source(0))
+    assert "refill buffer" not in srcs[0]
+    assert "refill buffer" in srcs[1]
+
+
+def test_refill_threshold_knob(engine):
+    p = engine.prepare(resolved(engine, "c1"), tuning={"refill_threshold": 28})
+    assert "while (wn >= 28" in p.source(1)
+    p = engine.prepare(resolved(engine, "c1"))
+    assert "while (wn >= 32" in p.source(1)
+
+
+def test_tuning_cache_on_disk(tmp_path, monkeypatch):
+    from dogqc_b200 import autotune
+    monkeypatch.setenv("DOGQC_B200_TUNING_CACHE", str(tmp_path / "t.json"))
+    monkeypatch.setattr(autotune, "_cache", {})
+    got = autotune._tuned("plan|x", None, lambda: ({"rows_per_thread": 2, "refill_threshold": 28}, 0.5, [1, 2]))
+    assert got[0]["refill_threshold"] == 28
+    monkeypatch.setattr(autotune, "_cache", {})
+
+    def again():
+        raise AssertionError("searched although the file holds the result")
+    got = autotune._tuned("plan|x", None, again)
+    assert got[0] == {"rows_per_thread": 2, "refill_threshold": 28} and got[1] == 0.5
