@@ -113,7 +113,7 @@ class dq_tuning(C.Structure):
 
 class dq_server_config(C.Structure):
     _fields_ = [("slots", C.c_int32), ("pool_per_query", C.c_int32), ("memory_budget", C.c_uint64),
-                ("batch_max", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("batch_max", C.c_int32), ("batch_rows_max", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class dq_request_info(C.Structure):

@@ -2010,14 +2010,25 @@ void build(Entry& e, const std::string& src) {
 }  // namespace
 
 Kernels compile(const Program& prog, bool load) {
-  std::lock_guard<std::mutex> lk(g_mu);
-  std::unique_ptr<Entry>& slot = g_cache[prog.source];
-  if (!slot) {
-    std::unique_ptr<Entry> e(new Entry());
-    build(*e, prog.source);
-    slot = std::move(e);
+  // the cache is looked up and filled under the lock, the compiler runs
+  // outside it: a thread compiling a new shape does not hold up threads whose
+  // kernels are cached already (a server's request loop)
+  Entry* found = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_cache.find(prog.source);
+    if (it != g_cache.end()) found = it->second.get();
   }
-  Entry& e = *slot;
+  if (!found) {
+    std::unique_ptr<Entry> built(new Entry());
+    build(*built, prog.source);
+    std::lock_guard<std::mutex> lk(g_mu);
+    std::unique_ptr<Entry>& slot = g_cache[prog.source];
+    if (!slot) slot = std::move(built);  // else another thread built it first
+    found = slot.get();
+  }
+  std::lock_guard<std::mutex> lk(g_mu);
+  Entry& e = *found;
   if (load && !e.lib) {
     cudaError_t err = cudaLibraryLoadData(&e.lib, e.cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (err != cudaSuccess) {

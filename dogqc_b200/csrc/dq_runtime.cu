@@ -23,6 +23,7 @@
 #include <string>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "../../include/dogqc_b200.h"
@@ -108,6 +109,16 @@ struct OfflineScope {
   bool prev;
   explicit OfflineScope(bool on) : prev(t_offline) { t_offline = on; }
   ~OfflineScope() { t_offline = prev; }
+};
+
+// Generation only: with a list set, preparing a plan (under an OfflineScope)
+// appends each pipeline's generated program to it instead of compiling it.
+thread_local std::vector<jit::Program>* t_collect = nullptr;
+
+struct CollectScope {
+  std::vector<jit::Program>* prev;
+  explicit CollectScope(std::vector<jit::Program>* to) : prev(t_collect) { t_collect = to; }
+  ~CollectScope() { t_collect = prev; }
 };
 
 // Device buffer with 256 bytes of tail padding: tile copies round their size up
@@ -740,7 +751,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   P.pat_off[d.npatterns] = (int32_t)cat.size();
   if (!cat.empty()) {
     p.pattern_buf.alloc(cat.size());
-    if (!ctx->offline) DQ_CUDA(cudaMemcpy(p.pattern_buf.ptr, cat.data(), cat.size(), cudaMemcpyHostToDevice));
+    if (!ctx->offline && !t_offline) DQ_CUDA(cudaMemcpy(p.pattern_buf.ptr, cat.data(), cat.size(), cudaMemcpyHostToDevice));
     P.patterns = p.pattern_buf.as<uint8_t>();
   }
   const dq_op& sink = d.ops[d.nops - 1];
@@ -785,7 +796,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     H.threshold = ctx->cfg.defer_threshold > 0    ? (uint64_t)ctx->cfg.defer_threshold
                   : plan->opts.defer_threshold > 0 ? (uint64_t)plan->opts.defer_threshold
                                                    : dflt;
-    if (H.grouped && !p.heavy_stats && !ctx->offline && !plan->opts.batch_member)
+    if (H.grouped && !p.heavy_stats && !ctx->offline && !t_offline && !plan->opts.batch_member)
       DQ_CUDA(cudaMallocHost((void**)&p.heavy_stats, 8));
     if (plan->opts.batch_member) break;  // the batch holds the buffers, shared by its instances
     p.heavy_items.alloc((size_t)H.cap * H.words * 8);
@@ -888,9 +899,10 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     // the batch launches its own many-instance kernels
   } else if (p.jit) {
     p.prog = jit::generate(P, p.expand_op, d.compact - 1, plan->opts.tuning);
-    p.kernels = jit::compile(p.prog, !ctx->offline);
+    if (t_collect) t_collect->push_back(p.prog);
+    else p.kernels = jit::compile(p.prog, !ctx->offline);
     rows_per_cta = (int64_t)p.prog.block * p.prog.rows_per_thread;
-    if (!ctx->offline) {
+    if (!ctx->offline && !t_offline) {
       const void* fn = (const void*)p.kernels.main;
       DQ_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, p.prog.smem_bytes));
       DQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, p.prog.block, p.prog.smem_bytes));
@@ -1185,7 +1197,7 @@ void refresh_pipelines(dq_plan* plan) {
   const size_t n = plan->str_src.size();
   if (plan->str_src_dev.bytes != std::max<size_t>(n, 1) * sizeof(DevStr) || (!plan->str_src_dev.ptr && !t_offline))
     plan->str_src_dev.alloc(std::max<size_t>(n, 1) * sizeof(DevStr));
-  if (n && !plan->ctx->offline)
+  if (n && !plan->ctx->offline && !t_offline)
     DQ_CUDA(cudaMemcpy(plan->str_src_dev.ptr, plan->str_src.data(), n * sizeof(DevStr), cudaMemcpyHostToDevice));
   for (auto& pp : plan->pipes) {
     pp->dev.strsrc = plan->str_src_dev.as<DevStr>();
@@ -2299,6 +2311,7 @@ struct DescCopy {
   std::deque<std::string> strs;
   dq_plan_desc d{};
   std::string key;
+  uint64_t rows = 0;                // input rows of the tables it scans (set at submit)
   const char* keep(const char* s) {
     if (!s) return nullptr;
     strs.emplace_back(s);
@@ -2350,6 +2363,19 @@ std::shared_ptr<DescCopy> copy_desc(const dq_plan_desc* in) {
 }
 
 // Device bytes a request's plan will hold, from its IR (before preparing it).
+// Rows of the registered tables a plan scans (each table once).
+uint64_t scanned_rows(dq_ctx* ctx, const dq_plan_desc& d) {
+  std::unordered_set<std::string> seen;
+  uint64_t rows = 0;
+  for (int i = 0; i < d.npipes; ++i) {
+    const dq_pipeline& p = d.pipes[i];
+    if (p.source_kind != DQ_SRC_TABLE || !p.table || !seen.insert(p.table).second) continue;
+    auto it = ctx->tables.find(p.table);
+    if (it != ctx->tables.end()) rows += (uint64_t)std::max<int64_t>(it->second.nrows, 0);
+  }
+  return rows;
+}
+
 uint64_t estimate_bytes(dq_ctx* ctx, const dq_plan_desc& d) {
   uint64_t b = 4096;
   std::vector<uint64_t> multi_rows(std::max(d.nres, 0), 0);
@@ -2624,6 +2650,7 @@ struct dq_server {
   std::vector<SrvSlot> slots;
   cudaStream_t prep = nullptr;      // captures and uploads of pooled plans' graphs
   uint64_t mem = 0;
+  std::unordered_set<std::string> compiled;  // request keys whose kernels a submitter compiled (under ctx->mu)
   // statistics (under mu)
   uint64_t submitted = 0, completed = 0, failed = 0, mem_peak = 0, mem_now = 0;
   std::vector<double> lat;
@@ -2988,8 +3015,12 @@ std::vector<std::pair<SrvReq*, PoolEntry*>> srv_take_batch(dq_server* s, SrvShap
   std::vector<std::pair<SrvReq*, PoolEntry*>> out;
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->pending.empty() || s->cfg.batch_max <= 1) return out;
+  // large requests run alone: the many-instance kernels pay off for requests
+  // whose launches, not their rows, dominate (their aggregates go to global
+  // tables, without a plain kernel's CTA-local pre-aggregation)
+  const uint64_t rows_max = s->cfg.batch_rows_max > 0 ? (uint64_t)s->cfg.batch_rows_max : (1ull << 18);
   SrvReq* head = s->pending.front();
-  if (head->solo) return out;
+  if (head->solo || head->desc->rows > rows_max) return out;
   auto sit = s->shape_of.find(head->desc->key);
   if (sit == s->shape_of.end() || !sit->second) return out;
   SrvShape* sh = sit->second;
@@ -2999,7 +3030,7 @@ std::vector<std::pair<SrvReq*, PoolEntry*>> srv_take_batch(dq_server* s, SrvShap
     SrvReq* r = *it;
     auto q = s->shape_of.find(r->desc->key);
     PoolEntry* pe = nullptr;
-    if (!r->solo && q != s->shape_of.end() && q->second == sh) {
+    if (!r->solo && r->desc->rows <= rows_max && q != s->shape_of.end() && q->second == sh) {
       auto& v = s->pool[r->desc->key];
       for (auto& e : v)
         if (!e->busy) {
@@ -3361,6 +3392,40 @@ int srv_wait(dq_server* s, uint64_t ticket, dq_result** out, dq_request_info* in
   return status;
 }
 
+// A request of a shape this server has not seen: its kernels (the plan's and
+// the many-instance ones its batches use) are generated under the context lock
+// with no device work, then compiled in the submitting thread without any lock
+// held.  The request loop's preparation of it then finds them in the compiled
+// kernel cache instead of compiling on the loop, where it would hold up every
+// request in flight.
+void precompile(dq_server* s, const DescCopy& d) {
+  std::vector<jit::Program> progs;
+  {
+    std::lock_guard<std::mutex> lk(s->ctx->mu);
+    if (!s->compiled.insert(d.key).second) return;
+    try {
+      OfflineScope off(true);
+      CollectScope cs(&progs);
+      std::unique_ptr<dq_plan> plan = make_plan(s->ctx, &d.d, PlanOpts());
+      if (s->cfg.batch_max != 1)
+        for (auto& pp : plan->pipes) {
+          if (!pp->jit) continue;
+          jit::Tuning t = plan->opts.tuning;
+          t.batched = true;
+          progs.push_back(jit::generate(pp->dev, pp->expand_op, pp->desc.compact - 1, t));
+        }
+    } catch (const std::exception&) {
+      return;  // the loop's own preparation reports what is wrong with the request
+    }
+  }
+  for (auto& pr : progs) {
+    try {
+      jit::compile(pr, false);
+    } catch (const std::exception&) {
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -3378,10 +3443,12 @@ int dq_server_submit(dq_server* s, const dq_plan_desc* desc, uint64_t* ticket) {
   return guarded(s->ctx, [&]() {
     reject_string_results(*desc);
     std::shared_ptr<DescCopy> d = copy_desc(desc);
+    precompile(s, *d);
     uint64_t est;
     {
       std::lock_guard<std::mutex> lk(s->ctx->mu);
       est = estimate_bytes(s->ctx, d->d);
+      d->rows = scanned_rows(s->ctx, d->d);
     }
     *ticket = srv_submit(s, d, est);
     return (int)DQ_OK;
@@ -3397,9 +3464,15 @@ int dq_server_replay(dq_server* s, int32_t nq, const dq_plan_desc* queries, int6
     std::vector<uint64_t> est;
     for (int q = 0; q < nq; ++q) reject_string_results(queries[q]);
     for (int q = 0; q < nq; ++q) descs.push_back(copy_desc(&queries[q]));
+    // the driver holds every query before the first arrival: unseen shapes are
+    // compiled now, as their submitters would have compiled them
+    for (auto& d : descs) precompile(s, *d);
     {
       std::lock_guard<std::mutex> lk(s->ctx->mu);
-      for (auto& d : descs) est.push_back(estimate_bytes(s->ctx, d->d));
+      for (auto& d : descs) {
+        est.push_back(estimate_bytes(s->ctx, d->d));
+        d->rows = scanned_rows(s->ctx, d->d);
+      }
     }
     for (int64_t i = 0; i < nreq; ++i)
       if (query_of[i] < 0 || query_of[i] >= nq) throw DqError(DQ_ERR_INVALID, "request names no query");

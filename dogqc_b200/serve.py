@@ -21,15 +21,17 @@ from dogqc_b200.engine import _take_result
 
 
 class Server(object):
-    def __init__(self, engine, slots=4, memory_budget=0, pool_per_query=0, batch_max=0):
+    def __init__(self, engine, slots=4, memory_budget=0, pool_per_query=0, batch_max=0, batch_rows_max=0):
         """``batch_max``: requests of one shape run as one launch (0: 16, 1:
-        every request alone); ``pool_per_query`` 0: twice ``slots``."""
+        every request alone); ``batch_rows_max``: requests scanning more input
+        rows run alone (0: 2^18); ``pool_per_query`` 0: twice ``slots``."""
         self.engine = engine
         cfg = L.dq_server_config()
         cfg.slots = slots
         cfg.memory_budget = int(memory_budget)
         cfg.pool_per_query = pool_per_query
         cfg.batch_max = batch_max
+        cfg.batch_rows_max = batch_rows_max
         h = C.c_void_p()
         L.check(L.lib().dq_server_start(engine.ctx, C.byref(cfg), C.byref(h)), engine.ctx)
         self.handle = h
@@ -86,6 +88,29 @@ def make_queries(shapes=("c0", "c1", "c2", "c3"), sizes=(0.01, 0.1, 1.0), max_ro
             if max_rows:
                 rows = min(rows, max_rows)
             out.append(Instance(shape, 100 * si + zi, max(rows, 1024)))
+    return out
+
+
+def c4_sizes(per_shape=6, lo=0.01, hi=5.0, seed=20261203 + 4):
+    """Table sizes of the served configuration, as fractions of the shapes'
+    full configurations: per shape, `per_shape` - 1 sizes drawn log-uniform in
+    [lo, hi] (seeded) and the largest size itself."""
+    r = np.random.Generator(np.random.Philox(seed))
+    out = {}
+    for shape in ("c0", "c1", "c2", "c3"):
+        draws = np.exp(r.uniform(math.log(lo), math.log(hi), per_shape - 1))
+        out[shape] = sorted([float(x) for x in draws] + [hi])
+    return out
+
+
+def make_c4_queries(per_shape=6, lo=0.01, hi=5.0):
+    """The served configuration's queries: each shape of c0-c3 at its
+    `c4_sizes`, on its own seeded tables (the largest, 5x c3: 300,000,000 fact
+    rows)."""
+    out = []
+    for si, (shape, sizes) in enumerate(sorted(c4_sizes(per_shape, lo, hi).items())):
+        for zi, size in enumerate(sizes):
+            out.append(Instance(shape, 100 * si + zi, max(int(round(FULL_ROWS[shape] * size)), 1024)))
     return out
 
 

@@ -414,7 +414,10 @@ typedef struct {
     int32_t pool_per_query;          /* plans kept per request; 0: twice slots  */
     uint64_t memory_budget;          /* bytes; 0: 150 GB                         */
     int32_t batch_max;               /* requests per launch; 0: 16, 1: alone    */
-    int32_t reserved[3];
+    int32_t batch_rows_max;          /* requests scanning more input rows than  */
+                                     /* this run alone (their plain plan's      */
+                                     /* graph); 0: 2^18                         */
+    int32_t reserved[2];
 } dq_server_config;
 typedef struct {
     double queue_ms;                 /* submitted -> dispatched to a stream      */

@@ -121,3 +121,65 @@ def test_continuous_batching_results(engine, queries, batch_max):
             assert st["batches"] == 0
     finally:
         srv.stop()
+
+
+def test_large_request_same_alone_and_in_mix(engine, queries):
+    """A large request (the c3 shape at half its configuration: 30,000,000
+    fact rows, ~500,000 groups) gives the same rows alone and while small
+    requests run beside it, and the C++ evaluator of the plan agrees."""
+    import cpu_eval
+    from dogqc_b200 import serve
+    from dogqc_b200.batch import Instance
+    big = Instance("c3", 990, 30_000_000)
+    engine.register_database(big.db)
+    p = engine.prepare(big.lowering)
+    try:
+        alone = canonical_rows(p.execute().rows())
+    finally:
+        p.free()
+    assert canonical_rows(cpu_eval.run_plan(big.base_db, big.plan)[1]) == alone
+    small = {}
+    for i, q in enumerate(queries):
+        ps = engine.prepare(q.lowering)
+        try:
+            small[i] = canonical_rows(ps.execute().rows())
+        finally:
+            ps.free()
+    qs = list(queries) + [big]
+    sched = serve.arrivals(24, None, queries, seed=13)
+    sched = sched[:8] + [(0.0, len(qs) - 1)] + sched[8:]
+    srv = serve.Server(engine, slots=4)
+    try:
+        results, infos, wall, errors = serve.mixed_stream(srv, qs, sched)
+        assert not errors
+        for (at, qi), res in zip(sched, results):
+            assert canonical_rows(res.rows()) == (alone if qi == len(qs) - 1 else small[qi])
+    finally:
+        srv.stop()
+
+
+def test_unseen_shape_compiles_in_the_submitter(engine, queries):
+    """A request of a shape the server has not seen compiles its kernels in
+    the submitting thread (dq_server_submit), so the request loop serves the
+    others meanwhile; its result is right."""
+    from dogqc_b200 import serve
+    from dogqc_b200 import workloads
+    from dogqc_b200.database import Database, Table
+    from dogqc_b200.lowering import Lowering
+    from dogqc_b200.relational import RelationalAlgebra
+    db = workloads.gen_c11(0.01)
+    alg = RelationalAlgebra(db)
+    plan, cfg = workloads.build("c11", alg)
+    plan = alg.resolveAlgebraPlan(plan, cfg)
+    low = Lowering(plan)
+    for p in low.pipes:
+        if p.table:
+            p.table = p.table + "@unseen"
+    engine.register_database(Database([Table(t.name + "@unseen", t.columns, t.types) for t in db.tables.values()]))
+    srv = serve.Server(engine, slots=2)
+    try:
+        t = srv.submit(low)
+        res, info = srv.wait(t)
+        assert canonical_rows(res.rows()) == canonical_rows(run_plan(db, plan)[1])
+    finally:
+        srv.stop()
