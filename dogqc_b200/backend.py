@@ -27,7 +27,7 @@ and grouped by range.
 Tables are read from the database behind the plan context: a
 ``dogqc_b200.database.Database`` (host columns), or the reference's accessor
 whose ``dbpath`` holds ``<table>_<attr>`` column files
-(``dogqc_b200.storage.load_mmdb``).
+(``dogqc_b200.importer.read_mmdb``).
 """
 import sys
 
@@ -98,8 +98,8 @@ class Backend(object):
         ctxt = getattr(self.algebraContext, "ctxt", self.algebraContext)
         db = getattr(ctxt, "database", None)
         if db is not None and not hasattr(db, "tables") and hasattr(db, "dbpath"):
-            from dogqc_b200.storage import load_mmdb
-            db = load_mmdb(db.schema, db.dbpath)
+            from dogqc_b200.importer import read_mmdb
+            db = read_mmdb(db.dbpath, schema=db.schema)
         return db
 
     def compile(self, filename=None):

