@@ -29,7 +29,7 @@ WIDTH = {I8: 1, I32: 4, U32: 4, I64: 8, U64: 8}
 SLOT_COL, SLOT_REG, SLOT_GATHER, SLOT_AGGKEY, SLOT_AGGVAL, SLOT_STR = 1, 2, 3, 4, 5, 6
 # dq_op_kind
 OP_ARITH, OP_CMP, OP_LOGIC, OP_CAST, OP_SELECT, OP_LIKE, OP_STREQ, OP_STRREF = 1, 2, 3, 4, 5, 6, 7, 8
-OP_PROFILE, OP_FILTER, OP_PROBE, OP_EXPAND, OP_EXISTS = 9, 10, 11, 12, 13
+OP_PROFILE, OP_FILTER, OP_PROBE, OP_EXPAND, OP_EXISTS, OP_SUBSTR = 9, 10, 11, 12, 13, 14
 OP_AGG, OP_BUILD, OP_MM_COUNT, OP_MM_SCATTER, OP_EMIT = 20, 21, 22, 23, 24
 ADD, SUB, MUL, DIV, MOD = 1, 2, 3, 4, 5
 EQ, NE, LT, LE, GT, GE = 1, 2, 3, 4, 5, 6

@@ -268,11 +268,32 @@ __device__ __forceinline__ uint64_t key_tag(const DevRes& R, const uint64_t* k) 
   return fmix64(h) & 0x7fffffffffffffffull;
 }
 
-// String references (source << 48 | row): the bytes behind them, their hash
-// and equality.  Group keys of string type hash and compare the bytes, so two
-// rows with equal strings meet in one group whatever rows they came from.
+// String references (source, substring window, row): the bytes behind them,
+// their hash and equality.  Join and group keys of string type hash and
+// compare the bytes, so two rows with equal strings meet whatever rows they
+// came from.
 __device__ __forceinline__ void str_ref_at(const DevPipe& P, uint64_t ref, const uint8_t*& ptr, int& len) {
-  str_at(P.strsrc[ref >> kStrRefShift], (int64_t)(ref & kStrRefRow), ptr, len);
+  str_ref_bytes(P.strsrc, ref, ptr, len);
+}
+
+// SUBSTRING(s, from, for) of a reference, the reference's stringSubstring
+// (include/util.cuh:132-142): first byte from - 1, `for` bytes, the window
+// clamped to the string (a window past its end is empty).  Offsets are within
+// the string's first kStrRefMaxOffset bytes (the lowering checks constants).
+__device__ __forceinline__ uint64_t str_ref_substring(uint64_t ref, int from, int len) {
+  int s0 = 0, e0 = 1 << 30;
+  if (ref & kStrRefSub) {
+    s0 = (int)((ref >> kStrRefStartShift) & 0xff);
+    e0 = (int)((ref >> kStrRefEndShift) & 0xff);
+  }
+  int st = s0 + from - 1;
+  int en = st + len;
+  if (st < s0) st = s0;
+  if (en > e0) en = e0;
+  st = st < 0 ? 0 : (st > kStrRefMaxOffset ? kStrRefMaxOffset : st);
+  en = en < st ? st : (en > kStrRefMaxOffset ? kStrRefMaxOffset : en);
+  return (ref & ~((1ull << kStrRefShift) - 1 - kStrRefRow)) | kStrRefSub | ((uint64_t)st << kStrRefStartShift) |
+         ((uint64_t)en << kStrRefEndShift);
 }
 
 __device__ __forceinline__ uint64_t str_ref_hash(const DevPipe& P, uint64_t ref) {
@@ -303,6 +324,23 @@ __device__ __forceinline__ uint64_t key_tag_str(const DevPipe& P, const DevRes& 
   return fmix64(h) & 0x7fffffffffffffffull;
 }
 
+// Bucket of a multimap key some of whose values are string references: their
+// bytes' hashes stand in for them (bucket_of otherwise).
+__device__ __forceinline__ uint32_t bucket_of_str(const DevPipe& P, const DevRes& R, const uint64_t* k, int n,
+                                                  uint32_t cap) {
+  uint64_t h = 0;
+  for (int i = 0; i < n; ++i) {
+    const uint64_t v = R.key_ctype[i] == DQ_STR ? str_ref_hash(P, k[i]) : k[i];
+    h = i == 0 ? v : (h ^ (h >> 29)) * 0xbf58476d1ce4e5b9ull + v;
+  }
+  return slot_of(h, cap);
+}
+
+// Key equality of a stored key word and a probe key word of ctype t.
+__device__ __forceinline__ bool key_word_eq(const DevPipe& P, int t, uint64_t a, uint64_t b) {
+  return t == DQ_STR ? str_ref_eq(P, a, b) : a == b;
+}
+
 // Unique join table: returns slot index or -1.
 __device__ __forceinline__ int64_t unique_find(const DevRes& R, uint64_t tag, const uint64_t* k) {
   if (R.packed && tag == kEmpty) return R.slots[R.cap * R.words] == 0 ? (int64_t)R.cap : -1;
@@ -319,6 +357,68 @@ __device__ __forceinline__ int64_t unique_find(const DevRes& R, uint64_t tag, co
     }
     idx = (idx + 1 == R.cap) ? 0 : idx + 1;
   }
+  return -1;
+}
+
+// Unique join table with string keys (tags are byte hashes): the keys of a
+// slot with the probe's tag are compared by their bytes.
+__device__ __forceinline__ int64_t unique_find_str(const DevPipe& P, const DevRes& R, uint64_t tag,
+                                                   const uint64_t* k) {
+  uint64_t idx = slot_of(tag, (uint32_t)R.cap);
+  for (uint64_t n = 0; n < R.cap; ++n) {
+    const uint64_t* s = R.slots + idx * R.words;
+    const uint64_t t = s[0];
+    if (t == kEmpty) return -1;
+    if (t == tag) {
+      bool eq = true;
+      for (int i = 0; i < R.nkeys && eq; ++i) eq = key_word_eq(P, R.key_ctype[i], s[R.key_word + i], k[i]);
+      if (eq) return (int64_t)idx;
+    }
+    idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+  }
+  return -1;
+}
+
+// Inserts string keys: a slot is claimed with a busy marker, its keys written,
+// then its tag published, so an insert of equal bytes (another row holding the
+// same string) finds the keys and stops there: each distinct key takes one
+// slot, however often the build side repeats it.  Returns the claimed slot,
+// or -1 when the key was present (the first insert wins) or the table is full.
+__device__ __forceinline__ int64_t unique_insert_str(const DevPipe& P, const DevRes& R, uint64_t tag,
+                                                     const uint64_t* k) {
+  uint64_t idx = slot_of(tag, (uint32_t)R.cap);
+  for (uint64_t n = 0; n < R.cap; ++n) {
+    uint64_t* s = R.slots + idx * R.words;
+    uint64_t t = *(volatile uint64_t*)s;
+    if (t == kEmpty) {
+      const uint64_t old = atomicCAS((unsigned long long*)s, kEmpty, kBusy);
+      if (old == kEmpty) {
+        for (int i = 0; i < R.nkeys; ++i) s[R.key_word + i] = k[i];
+        __threadfence();
+        atomicExch((unsigned long long*)s, tag);
+        return (int64_t)idx;
+      }
+      t = old;
+    }
+    long long spins = 0;
+    while (t == kBusy && spins < kSpinLimit) {
+      t = *(volatile uint64_t*)s;
+      ++spins;
+    }
+    if (t == kBusy) {
+      set_status(P, kErrTimeout);
+      return -1;
+    }
+    if (t == tag) {
+      __threadfence();
+      bool eq = true;
+      for (int i = 0; i < R.nkeys && eq; ++i)
+        eq = key_word_eq(P, R.key_ctype[i], ((volatile uint64_t*)s)[R.key_word + i], k[i]);
+      if (eq) return -1;
+    }
+    idx = (idx + 1 == R.cap) ? 0 : idx + 1;
+  }
+  set_status(P, kErrHtFull);
   return -1;
 }
 

@@ -38,10 +38,41 @@ struct DevStr {           // string column, read in place
   int32_t sid;            // its index in the plan's string sources (string references)
 };
 
-// A string value carried as a 64-bit reference: the plan's string source << 48
-// | the row (group keys and output columns hold these; the bytes stay in place).
-constexpr int kStrRefShift = 48;
-constexpr uint64_t kStrRefRow = (1ull << kStrRefShift) - 1;
+// A string value carried as a 64-bit reference (group keys, join payloads and
+// output columns hold these; the bytes stay in place): the plan's string source
+// (bits 63..52), a substring flag (bit 51) with the substring's first and end
+// byte offsets in the string (bits 50..43 and 42..35) and the row (bits 34..0).
+constexpr int kStrRefShift = 52;
+constexpr uint64_t kStrRefSub = 1ull << 51;
+constexpr int kStrRefStartShift = 43;
+constexpr int kStrRefEndShift = 35;
+constexpr uint64_t kStrRefRow = (1ull << kStrRefEndShift) - 1;
+constexpr int kStrRefMaxSources = 1 << 12;
+constexpr int kStrRefMaxOffset = 255;
+
+#ifdef __CUDACC__
+// The bytes a reference names: its source's row, cut to the substring window
+// when the flag is set (offsets past the string's end give the empty string).
+__device__ __forceinline__ void str_ref_bytes(const DevStr* src, uint64_t ref, const uint8_t*& p, int& n) {
+  const DevStr& d = src[ref >> kStrRefShift];
+  const uint64_t row = ref & kStrRefRow;
+  if (d.width > 0) {
+    p = d.chars + row * (uint64_t)d.width;
+    n = d.width;
+  } else {
+    p = d.chars + d.offsets[row];
+    n = (int)(d.offsets[row + 1] - d.offsets[row]);
+  }
+  if (ref & kStrRefSub) {
+    int st = (int)((ref >> kStrRefStartShift) & 0xff), en = (int)((ref >> kStrRefEndShift) & 0xff);
+    st = st < n ? st : n;
+    en = en < n ? en : n;
+    if (en < st) en = st;
+    p += st;
+    n = en - st;
+  }
+}
+#endif
 
 struct DevSlot {
   int8_t kind, level, ctype, width;

@@ -637,16 +637,16 @@ __global__ void __launch_bounds__(kImpRows) imp_strings_kernel(const ImpArgs A) 
 }
 
 // ------------------------------------------------------- string results --
-// Result columns of string type hold references (source << 48 | row); these
+// Result columns of string type hold references (source, substring window, row); these
 // turn them into offsets and a heap: the lengths, their prefix sum (the scan
 // above), then one warp per row copies its bytes.
 
 __global__ void str_ref_len_kernel(const uint64_t* refs, uint64_t n, const DevStr* src, uint64_t* lens) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t ref = refs[i];
-    const DevStr& d = src[ref >> kStrRefShift];
-    const uint64_t row = ref & kStrRefRow;
-    lens[i] = d.width > 0 ? (uint64_t)d.width : d.offsets[row + 1] - d.offsets[row];
+    const uint8_t* p;
+    int n;
+    str_ref_bytes(src, refs[i], p, n);
+    lens[i] = (uint64_t)n;
   }
 }
 
@@ -655,10 +655,9 @@ __global__ void str_ref_copy_kernel(const uint64_t* refs, uint64_t n, const DevS
   const int lane = threadIdx.x & 31;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
   for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; i < n; i += warps) {
-    const uint64_t ref = refs[i];
-    const DevStr& d = src[ref >> kStrRefShift];
-    const uint64_t row = ref & kStrRefRow;
-    const uint8_t* from = d.width > 0 ? d.chars + row * (uint64_t)d.width : d.chars + d.offsets[row];
+    const uint8_t* from;
+    int n;
+    str_ref_bytes(src, refs[i], from, n);
     const uint64_t len = offs[i + 1] - offs[i];
     for (uint64_t b = lane; b < len; b += 32) heap[offs[i] + b] = from[b];
   }

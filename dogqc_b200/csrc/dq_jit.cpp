@@ -128,9 +128,13 @@ void op_reads(const DevPipe& P, const dq_op& op, std::vector<int>& out) {
       if (!(op.flags & DQ_OPF_B_IMM)) add(op.b);
       add(op.c >= 0 ? op.c : op.dst);
       break;
-    case DQ_OP_LIKE:
     case DQ_OP_STREQ:
+      add(op.a);
+      if (op.res < 0) add(op.b);
+      break;
+    case DQ_OP_LIKE:
     case DQ_OP_STRREF:
+    case DQ_OP_SUBSTR:
     case DQ_OP_FILTER:
       add(op.a);
       break;
@@ -271,6 +275,29 @@ struct Gen {
   }
 
   // keys of a resource from a slot list, canonicalised to the key types
+  // Declares nothing; sets p/n to the bytes of string slot s (a string
+  // column read at `row`, or a reference held in a value).
+  void str_bytes(int s, const std::string& row, const std::string& p, const std::string& n) {
+    const DevSlot& sl = slot(s);
+    if (sl.ctype != DQ_STR) throw Error("string op on a non-string slot");
+    if (sl.kind == DQ_SLOT_STR) L("str_at(P.strs[" + num(sl.src) + "], " + row + ", " + p + ", " + n + ");");
+    else L("str_ref_at(P, " + V(s) + ", " + p + ", " + n + ");");
+  }
+
+  // Bucket of a multimap key held in array kk.
+  std::string bucket(const dq_op& op, int r, const std::string& kk) {
+    if (has_str_key(P.res[r]))
+      return "bucket_of_str(P, " + res(r) + ", " + kk + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap)";
+    return "bucket_of(" + kk + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap)";
+  }
+
+  // Equality of a probe key slot and a build key slot of resource r's key q.
+  std::string key_eq(int r, int q, int a, int b) {
+    const int t = P.res[r].key_ctype[q];
+    if (t == DQ_STR) return "str_ref_eq(P, " + V(a) + ", " + V(b) + ")";
+    return "canon(" + V(a) + ", " + ct_name(t) + ") == canon(" + V(b) + ", " + ct_name(t) + ")";
+  }
+
   std::string keys(const dq_op& op, int r, int list, int n) {
     std::string k = fresh("kk");
     L("uint64_t " + k + "[" + num(std::max(n, 1)) + "];");
@@ -345,22 +372,33 @@ struct Gen {
           break;
         case DQ_OP_LIKE:
         case DQ_OP_STREQ: {
-          const DevSlot& sl = slot(op.a);
-          if (sl.kind != DQ_SLOT_STR) throw Error("string op on a non-string slot");
           L(V(op.dst) + " = 0;");
           L("if (" + act + ") {");
           ++ind;
           L("const uint8_t* sp_; int sn_;");
-          L("str_at(P.strs[" + num(sl.src) + "], " + row + ", sp_, sn_);");
-          std::string pat = "P.patterns + P.pat_off[" + num(op.res) + "]";
-          std::string plen = "P.pat_off[" + num(op.res + 1) + "] - P.pat_off[" + num(op.res) + "]";
-          L(V(op.dst) + std::string(" = (uint64_t)") + (op.kind == DQ_OP_LIKE ? "like_match" : "str_eq") +
-            "(sp_, sn_, " + pat + ", " + plen + ");");
+          str_bytes(op.a, row, "sp_", "sn_");
+          if (op.kind == DQ_OP_STREQ && op.res < 0) {
+            L("const uint8_t* sq_; int sm_;");
+            str_bytes(op.b, row, "sq_", "sm_");
+            L(V(op.dst) + " = (uint64_t)str_eq(sp_, sn_, sq_, sm_);");
+          } else {
+            std::string pat = "P.patterns + P.pat_off[" + num(op.res) + "]";
+            std::string plen = "P.pat_off[" + num(op.res + 1) + "] - P.pat_off[" + num(op.res) + "]";
+            L(V(op.dst) + std::string(" = (uint64_t)") + (op.kind == DQ_OP_LIKE ? "like_match" : "str_eq") +
+              "(sp_, sn_, " + pat + ", " + plen + ");");
+          }
           --ind;
           L("}");
           break;
         }
-        case DQ_OP_STRREF: {  // the string's plan-wide reference: source << 48 | row
+        case DQ_OP_SUBSTR: {
+          if (slot(op.a).ctype != DQ_STR || slot(op.a).kind == DQ_SLOT_STR)
+            throw Error("SUBSTR reads a string reference");
+          L(V(op.dst) + " = str_ref_substring(" + V(op.a) + ", " + num((int32_t)(uint32_t)op.imm) + ", " +
+            num((int32_t)(uint32_t)((uint64_t)op.imm >> 32)) + ");");
+          break;
+        }
+        case DQ_OP_STRREF: {  // the string's plan-wide reference: source, no window, row
           const DevSlot& sl = slot(op.a);
           if (sl.kind != DQ_SLOT_STR) throw Error("string reference of a non-string slot");
           L(V(op.dst) + " = ((uint64_t)(uint32_t)P.strs[" + num(sl.src) + "].sid << kStrRefShift) | (uint64_t)" + row +
@@ -604,7 +642,10 @@ struct Gen {
       }
     } else {
       std::string k = keys(op, r, op.list, op.nlist);
-      L(s + " = unique_find(" + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
+      if (has_str_key(R))
+        L(s + " = unique_find_str(P, " + res(r) + ", key_tag_str(P, " + res(r) + ", " + k + "), " + k + ");");
+      else
+        L(s + " = unique_find(" + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
     }
     if (!pay_reg.empty()) {
       // the payload came with the tag (the all-ones key's slot is read here)
@@ -698,11 +739,8 @@ struct Gen {
   void match_ops(int k, int lv, const std::string& a, const std::string& exit) {
     const dq_op& op = P.ops[k];
     declare_regs(lv);
-    for (int q = 0; q < op.nlist; ++q) {
-      int t = P.res[op.res].key_ctype[q];
-      L(a + " = " + a + " && canon(" + V(P.lists[op.list + q]) + ", " + ct_name(t) + ") == canon(" +
-        V(P.lists[op.list2 + q]) + ", " + ct_name(t) + ");");
-    }
+    for (int q = 0; q < op.nlist; ++q)
+      L(a + " = " + a + " && " + key_eq(op.res, q, P.lists[op.list + q], P.lists[op.list2 + q]) + ";");
     skip_if_idle(a, exit);
     ops_from(k + 1, lv, a, exit);
   }
@@ -722,7 +760,7 @@ struct Gen {
     L("if (" + act + ") {");
     ++ind;
     std::string kk = keys(op, r, op.list, op.nlist);
-    L("const uint32_t b_ = bucket_of(" + kk + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap);");
+    L("const uint32_t b_ = " + bucket(op, r, kk) + ";");
     L("const uint32_t xc_ = " + res(r) + ".counts[b_];");
     L("uint32_t " + m + " = xc_ ? " + res(r) + ".offsets[b_] : 0u;");
     L("const uint32_t " + me + " = " + m + " + xc_;");
@@ -732,11 +770,7 @@ struct Gen {
     for (int s2 = 0; s2 < P.nslots; ++s2)
       if (slot(s2).kind == DQ_SLOT_GATHER && slot(s2).level == lv && slot(s2).res == r) gather(s2, "true", m);
     std::string eq = "true";
-    for (int q = 0; q < op.nlist; ++q) {
-      int t = P.res[r].key_ctype[q];
-      eq += " && canon(" + V(P.lists[op.list + q]) + ", " + ct_name(t) + ") == canon(" + V(P.lists[op.list2 + q]) + ", " +
-            ct_name(t) + ")";
-    }
+    for (int q = 0; q < op.nlist; ++q) eq += " && " + key_eq(r, q, P.lists[op.list + q], P.lists[op.list2 + q]);
     L("if (!(" + eq + ")) continue;");
     if (op.imm > 0) {
       declare_regs(lv);
@@ -765,7 +799,7 @@ struct Gen {
     L("if (" + act + ") {");
     ++ind;
     std::string kk = keys(op, r, op.list, op.nlist);
-    L("const uint32_t b_ = bucket_of(" + kk + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap);");
+    L("const uint32_t b_ = " + bucket(op, r, kk) + ";");
     L(ec + " = " + res(r) + ".counts[b_];");
     L(eo + " = " + ec + " ? " + res(r) + ".offsets[b_] : 0u;");
     --ind;
@@ -944,7 +978,10 @@ struct Gen {
       return;
     }
     std::string k = keys(op, r, op.list, op.nlist);
-    L("const int64_t s_ = unique_insert(P, " + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
+    if (has_str_key(R))
+      L("const int64_t s_ = unique_insert_str(P, " + res(r) + ", key_tag_str(P, " + res(r) + ", " + k + "), " + k + ");");
+    else
+      L("const int64_t s_ = unique_insert(P, " + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
     if (op.nlist2 > 0) {
       L("if (s_ >= 0) {");
       ++ind;
@@ -967,7 +1004,7 @@ struct Gen {
     L("if (" + act + ") {");
     ++ind;
     std::string k = keys(op, r, op.list, op.nlist);
-    L("b_ = bucket_of(" + k + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap);");
+    L("b_ = " + bucket(op, r, k) + ";");
     --ind;
     L("}");
     L("const unsigned peers_ = __match_any_sync(kFull, b_);");
@@ -1102,7 +1139,7 @@ struct Gen {
     for (int j = k + 1; j < P.nops; ++j) {
       const int kind = P.ops[j].kind;
       heavy |= kind == DQ_OP_PROBE || kind == DQ_OP_EXPAND || kind == DQ_OP_EXISTS || kind == DQ_OP_LIKE ||
-               kind == DQ_OP_STREQ ||
+               kind == DQ_OP_STREQ || kind == DQ_OP_SUBSTR ||
                kind == DQ_OP_BUILD || kind == DQ_OP_MM_COUNT || kind == DQ_OP_MM_SCATTER || kind == DQ_OP_EMIT ||
                (kind == DQ_OP_AGG && agg != AGG_REGS);
     }

@@ -94,7 +94,7 @@ int ctype_width(int t) {
     case DQ_U32: return 4;
     case DQ_I64:
     case DQ_U64:
-    case DQ_STR: return 8;  // as a value, a string is a 64-bit reference (source << 48 | row)
+    case DQ_STR: return 8;  // as a value, a string is a 64-bit reference (source, window, row)
     default: return 0;
   }
 }
@@ -531,9 +531,13 @@ void slot_reads(const dq_pipeline& d, const dq_op& op, std::vector<int>& out) {
       if (!(op.flags & DQ_OPF_B_IMM)) add(op.b);
       add(op.c >= 0 ? op.c : op.dst);
       break;
-    case DQ_OP_LIKE:
     case DQ_OP_STREQ:
+      add(op.a);
+      if (op.res < 0) add(op.b);
+      break;
+    case DQ_OP_LIKE:
     case DQ_OP_STRREF:
+    case DQ_OP_SUBSTR:
     case DQ_OP_FILTER:
       add(op.a);
       break;
@@ -585,8 +589,19 @@ void validate_pipeline(const dq_pipeline& d, int nres) {
           throw DqError(DQ_ERR_BAD_IR, "an EXISTS condition holds scalar ops only");
       }
     }
-    if ((op.kind == DQ_OP_LIKE || op.kind == DQ_OP_STREQ) && (op.res < 0 || op.res >= d.npatterns))
+    const bool two_strings = op.kind == DQ_OP_STREQ && op.res == -1;
+    if ((op.kind == DQ_OP_LIKE || op.kind == DQ_OP_STREQ) && !two_strings && (op.res < 0 || op.res >= d.npatterns))
       throw DqError(DQ_ERR_BAD_IR, "pattern index out of range");
+    auto is_str = [&](int s) { return s >= 0 && d.slots[s].ctype == DQ_STR; };
+    if ((op.kind == DQ_OP_LIKE || op.kind == DQ_OP_STREQ) && (!is_str(op.a) || (two_strings && !is_str(op.b))))
+      throw DqError(DQ_ERR_BAD_IR, "string comparison of a non-string slot");
+    if (op.kind == DQ_OP_SUBSTR) {
+      const int32_t from = (int32_t)(uint32_t)op.imm, len = (int32_t)(uint32_t)((uint64_t)op.imm >> 32);
+      if (!is_str(op.a) || d.slots[op.a].kind == DQ_SLOT_STR || op.dst < 0 || d.slots[op.dst].ctype != DQ_STR)
+        throw DqError(DQ_ERR_BAD_IR, "SUBSTR takes and gives string references");
+      if ((int64_t)from - 1 + (int64_t)len > 255 || (int64_t)from - 1 > 255)
+        throw DqError(DQ_ERR_UNSUPPORTED, "substring windows end within the first 255 bytes of a string");
+    }
     if (op.nlist > DQ_MAX_KEYS && (op.kind == DQ_OP_PROBE || op.kind == DQ_OP_EXPAND || op.kind == DQ_OP_EXISTS ||
                                     op.kind == DQ_OP_BUILD ||
                                     op.kind == DQ_OP_AGG || op.kind == DQ_OP_MM_COUNT || op.kind == DQ_OP_MM_SCATTER))
@@ -664,6 +679,8 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
         for (size_t k = 0; k < plan->str_src.size(); ++k)
           if (plan->str_src[k].chars == s.chars && plan->str_src[k].offsets == s.offsets) s.sid = (int32_t)k;
         if (s.sid < 0) {
+          if (plan->str_src.size() >= (size_t)kStrRefMaxSources)
+            throw DqError(DQ_ERR_UNSUPPORTED, "a plan reads at most 4096 string columns");
           s.sid = (int32_t)plan->str_src.size();
           plan->str_src.push_back(s);
         }
@@ -738,11 +755,11 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
         throw DqError(DQ_ERR_BAD_IR, "bad slot kind");
     }
   }
-  // ops, lists, patterns
+  // ops, lists, patterns (d.patterns point into p.patterns, which outlives
+  // every re-derivation of the pipeline)
   P.nops = d.nops;
   for (int i = 0; i < d.nops; ++i) P.ops[i] = d.ops[i];
   for (int i = 0; i < d.nlist; ++i) P.lists[i] = d.lists[i];
-  p.patterns.clear();
   std::string cat;
   for (int i = 0; i < d.npatterns; ++i) {
     P.pat_off[i] = (int32_t)cat.size();
@@ -889,10 +906,18 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
       throw DqError(DQ_ERR_UNSUPPORTED, "semi/anti joins with conditions and lane-activity profiles run on "
                                         "generated kernels only (not DQ_CFG_NO_JIT / DQ_CFG_ROW_KERNEL)");
   if (!p.jit)
-    for (int k = 0; k < p.desc.nops; ++k)
-      if (p.desc.ops[k].kind == DQ_OP_STRREF)
-        throw DqError(DQ_ERR_UNSUPPORTED, "string group keys and string result columns run on generated plan kernels "
-                                          "only (not DQ_CFG_NO_JIT / DQ_CFG_ROW_KERNEL, batches or served batches)");
+    for (int k = 0; k < p.desc.nops; ++k) {
+      const dq_op& op = p.desc.ops[k];
+      // the prebuilt kernels read strings in place only: references (string
+      // keys, payloads, results, substrings) need generated kernels
+      const bool refs = op.kind == DQ_OP_STRREF || op.kind == DQ_OP_SUBSTR ||
+                        ((op.kind == DQ_OP_LIKE || op.kind == DQ_OP_STREQ) &&
+                         (op.res < 0 || p.desc.slots[op.a].kind != DQ_SLOT_STR));
+      if (refs)
+        throw DqError(DQ_ERR_UNSUPPORTED, "string join keys, string group keys, substrings and string result columns "
+                                          "run on generated plan kernels only (not DQ_CFG_NO_JIT / "
+                                          "DQ_CFG_ROW_KERNEL, batches or served batches)");
+    }
   int occ = 1;
   int64_t rows_per_cta = tile;
   if (plan->opts.batch_member) {

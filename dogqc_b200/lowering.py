@@ -161,7 +161,7 @@ class Pipe(object):
         self.att = {}           # attribute id -> slot index
         self.level = 0
         self.lazy = {}          # attribute id -> callable creating its slot
-        self.strref = {}        # attribute id -> register holding its string reference
+        self.strref = {}        # string column slot -> register holding its reference
 
     def slot(self, kind, level, ctype, src=0, res=-1):
         self.slots.append(dict(kind=kind, level=level, ctype=ctype, src=src, res=res))
@@ -210,18 +210,21 @@ class Pipe(object):
         return self.att[attr.id]
 
     def value_slot(self, attr):
-        """The slot of ``attr`` as a value: a scanned string becomes its 64-bit
-        reference (plan string source << 48 | row), computed first thing in the
-        pipeline so refill and expansion carry it like any other value."""
-        s = self.attr_slot(attr)
+        """The slot of ``attr`` as a value (see ``ref_of``)."""
+        return self.ref_of(self.attr_slot(attr))
+
+    def ref_of(self, s):
+        """Slot ``s`` as a value: a scanned string becomes its 64-bit reference
+        (plan string source, substring window, row), computed first thing in
+        the pipeline so refill and expansion carry it like any other value."""
         if self.slots[s]["kind"] != L.SLOT_STR:
             return s
-        if attr.id not in self.strref:
+        if s not in self.strref:
             r = self.slot(L.SLOT_REG, 0, "str")
             self.op(L.OP_STRREF, dst=r, a=s, ctype=L.STR)
             self.ops.insert(0, self.ops.pop())
-            self.strref[attr.id] = r
-        return self.strref[attr.id]
+            self.strref[s] = r
+        return self.strref[s]
 
     def clone_for_rebuild(self):
         """Fresh copy of the source part (used to run a build pipeline twice)."""
@@ -403,13 +406,13 @@ class Lowering(object):
         return pipe.slots[v]["ctype"]
 
     def materialize_value(self, pipe, v, ctype):
-        """A slot holding v converted to ctype."""
+        """A slot holding v converted to ctype (a string as its reference)."""
         if isinstance(v, Pattern):
-            raise Unsupported("string values as map results")
+            raise Unsupported("string constants as map results")
         if not isinstance(v, Imm) and pipe.slots[v]["ctype"] == ctype:
-            return v
-        if ctype == "str":
-            raise Unsupported("string-valued maps")
+            return pipe.ref_of(v) if ctype == "str" else v
+        if ctype == "str" or (not isinstance(v, Imm) and pipe.slots[v]["ctype"] == "str"):
+            raise Unsupported("conversions between strings and numbers")
         d = pipe.reg(ctype)
         if isinstance(v, Imm):
             pipe.op(L.OP_CAST, dst=d, ctype=CT[ctype], flags=L.OPF_A_IMM, imm=_imm64(_wrap(v.value, ctype)))
@@ -453,17 +456,22 @@ class Lowering(object):
             b = self.expr(pipe, e.rightChild)
             ta, tb = self.ctype_of(pipe, a), self.ctype_of(pipe, b)
             if "str" in (ta, tb) or "strconst" in (ta, tb):
+                # the reference's stringEquals (util.cuh:86-102, scalarAlgebra.py:167-188);
+                # it has no ordering of strings
                 if k != "EqualsExpr":
                     raise Unsupported("ordering comparisons on strings")
                 if ta == "strconst":
                     a, b = b, a
                     ta, tb = tb, ta
-                if ta != "str" or tb != "strconst":
-                    raise Unsupported("string equality needs an attribute and a constant")
-                if pipe.slots[a]["kind"] != L.SLOT_STR:
-                    raise Unsupported("string comparisons on strings carried through a join")
+                if ta == "strconst":
+                    return Imm(int(a.data == b.data), "i32")
+                if ta != "str" or tb not in ("str", "strconst"):
+                    raise Unsupported("comparisons of strings with numbers")
                 d = pipe.reg("i32")
-                pipe.op(L.OP_STREQ, dst=d, a=a, res=pipe.pattern(b.data))
+                if tb == "strconst":
+                    pipe.op(L.OP_STREQ, dst=d, a=self.str_operand(pipe, a), res=pipe.pattern(b.data))
+                else:
+                    pipe.op(L.OP_STREQ, dst=d, a=self.str_operand(pipe, a), b=self.str_operand(pipe, b), res=-1)
                 return d
             t = common_type(ta, tb)
             d = pipe.reg("i32")
@@ -483,11 +491,13 @@ class Lowering(object):
         if k == "LikeExpr":
             s = self.expr(pipe, e.leftChild)
             p = self.expr(pipe, e.rightChild)
-            if not isinstance(p, Pattern) or self.ctype_of(pipe, s) != "str" or pipe.slots[s]["kind"] != L.SLOT_STR:
-                raise Unsupported("LIKE needs a string attribute and a constant pattern")
+            if not isinstance(p, Pattern) or isinstance(s, (Imm, Pattern)) or self.ctype_of(pipe, s) != "str":
+                raise Unsupported("LIKE needs a string value and a constant pattern")
             d = pipe.reg("i32")
-            pipe.op(L.OP_LIKE, dst=d, a=s, res=pipe.pattern(p.data))
+            pipe.op(L.OP_LIKE, dst=d, a=self.str_operand(pipe, s), res=pipe.pattern(p.data))
             return d
+        if k == "SubstringExpr":
+            return self.substring(pipe, e)
         if k == "ExtractExpr":
             a = self.expr(pipe, e.child)
             t = common_type(self.ctype_of(pipe, a), "i32")
@@ -521,6 +531,33 @@ class Lowering(object):
                 pipe.op(L.OP_SELECT, **kw)
             return d
         raise Unsupported("scalar expression %s" % k)
+
+    @staticmethod
+    def str_operand(pipe, s):
+        """A string operand: a scanned column is read in place at level 0; below
+        an expansion its reference is used, a value that deferred expansion
+        ranges carry like any other."""
+        return pipe.ref_of(s) if pipe.level > 0 else s
+
+    def substring(self, pipe, e):
+        """SUBSTRING(s, from, for) with constant bounds (the reference's
+        stringSubstring, util.cuh:132-142): a reference to the same bytes with a
+        window; nested substrings narrow it.  The window ends within the
+        string's first 255 bytes."""
+        s = self.expr(pipe, e.exprString)
+        f = self.expr(pipe, e.exprFrom)
+        n = self.expr(pipe, e.exprFor)
+        if isinstance(s, (Imm, Pattern)) or self.ctype_of(pipe, s) != "str":
+            raise Unsupported("SUBSTRING of a string constant")
+        if not isinstance(f, Imm) or not isinstance(n, Imm):
+            raise Unsupported("SUBSTRING bounds that are not constants")
+        fv, nv = _wrap(f.value, "i32"), _wrap(n.value, "i32")
+        if fv - 1 > 255 or fv - 1 + nv > 255:
+            raise Unsupported("SUBSTRING windows ending past byte 255")
+        d = pipe.reg("str")
+        pipe.op(L.OP_SUBSTR, dst=d, a=pipe.ref_of(s), ctype=L.STR,
+                imm=_imm64((fv & 0xffffffff) | ((nv & 0xffffffff) << 32)))
+        return d
 
     def _cast_into(self, pipe, d, v, t):
         if isinstance(v, Imm):
@@ -575,8 +612,13 @@ class Lowering(object):
         for b, p in zip(bk, pk):
             tb, tp = lang_type(b.dataType), lang_type(p.dataType)
             if "str" in (tb, tp):
-                raise Unsupported("string join keys")
-            key_types.append(common_type(tb, tp))
+                # string keys: references, hashed and compared by their bytes
+                # (the reference's stringHash / stringEquals, hashTableUtil.py:15-35)
+                if tb != tp:
+                    raise Unsupported("join keys comparing a string with a number")
+                key_types.append("str")
+            else:
+                key_types.append(common_type(tb, tp))
         build_atts = list(node.leftChild.outRelation.values())
         # A semi or anti join asks whether a build row with equal keys exists;
         # without a further condition only the keys matter (a unique table of
@@ -591,7 +633,8 @@ class Lowering(object):
         if semi and node.conditions is None:
             build_atts = []
         if unique:
-            packed = len(bk) == 1 or (len(bk) == 2 and all(t in ("i8", "i32", "u32") for t in key_types))
+            packed = "str" not in key_types and (
+                len(bk) == 1 or (len(bk) == 2 and all(t in ("i8", "i32", "u32") for t in key_types)))
             if packed:
                 # the packed tag is the exact key: build keys that no operator above
                 # the join reads need not be stored in the payload
@@ -622,7 +665,7 @@ class Lowering(object):
 
     def join_build_sink(self, node, pipe):
         info = self.joins[id(node)]
-        keys = [pipe.attr_slot(a) for a in info["bk"]]
+        keys = [pipe.value_slot(a) for a in info["bk"]]
         kl, kn = pipe.list_(keys)
         if info["unique"]:
             pl, pn = pipe.list_([pipe.value_slot(a) for a in info["build_atts"]])
@@ -637,7 +680,7 @@ class Lowering(object):
     def join_probe(self, node, pipe):
         info = self.joins[id(node)]
         jt = _tname(node.joinType)
-        keys = [pipe.attr_slot(a) for a in info["pk"]]
+        keys = [pipe.value_slot(a) for a in info["pk"]]
         kl, kn = pipe.list_(keys)
         if info["unique"]:
             dsts = []
@@ -800,7 +843,7 @@ class Lowering(object):
         """Relative cost of one probe of a join table: 1 for a table that stays
         L2-resident (the runtime's 4x slots fit L2_TABLE_BYTES), 2 otherwise."""
         r = self.res[op["res"]]
-        packed = r.nkeys <= 1 or (r.nkeys == 2 and all(t in NARROW for t in r.key_ctype))
+        packed = "str" not in r.key_ctype and (r.nkeys <= 1 or (r.nkeys == 2 and all(t in NARROW for t in r.key_ctype)))
         words = 1 + len(r.pay_ctype) + (0 if packed else r.nkeys)
         return 1.0 if r.capacity * 4 * words * 8 <= L2_TABLE_BYTES else 2.0
 

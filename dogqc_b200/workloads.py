@@ -535,12 +535,234 @@ def plan_c13(alg, scal, Type, Reduction, multimatch=False, flag_cut=0):
     return agg, cfg
 
 
+# ------------------------------------------------------- c14 .. c16 -------------
+# Strings beyond the scan: predicates on strings carried through a join and
+# group keys of strings from aggregation tables (TPC-H Q16 shape), joins on
+# string keys (unique, multimatch, semi and anti), and substrings as map
+# results, IN lists and group keys (TPC-H Q22 shape).
+
+C14_TYPE1 = [b"STANDARD", b"SMALL", b"MEDIUM", b"LARGE", b"ECONOMY", b"PROMO"]
+C14_TYPE2 = [b"ANODIZED", b"BURNISHED", b"PLATED", b"POLISHED", b"BRUSHED"]
+C14_TYPE3 = [b"TIN", b"NICKEL", b"BRASS", b"STEEL", b"COPPER"]
+C14_WORDS = [b"carefully", b"final", b"deposits", b"sleep", b"furiously", b"regular", b"accounts", b"haggle",
+             b"quickly", b"ironic", b"packages", b"among", b"the", b"blithely", b"pending", b"requests", b"wake",
+             b"slyly", b"express", b"theodolites", b"above", b"bold", b"foxes", b"instructions", b"nag"]
+C14_SIZES = [49, 14, 23, 45, 19, 3, 36, 9]
+
+
+def _comments(r, n, plant=None, plant_rate=0.0):
+    """n variable-length comments of 3..12 words; with ``plant`` (a pair of
+    words) about ``plant_rate`` of them hold the first word, later the second."""
+    nw = r.integers(3, 13, n)
+    words = r.integers(0, len(C14_WORDS), int(nw.sum()))
+    planted = r.random(n) < plant_rate if plant else np.zeros(n, bool)
+    out, k = [], 0
+    for i in range(n):
+        w = [C14_WORDS[j] for j in words[k:k + nw[i]]]
+        k += nw[i]
+        if planted[i]:
+            w.insert(1, plant[0])
+            w.insert(len(w), plant[1])
+        out.append(b" ".join(w))
+    return StringColumn.from_list(out)
+
+
+def gen_c14(scale=1.0, seed=BASE_SEED + 14):
+    """Q16-shaped: parts with a brand ("Brand#MN"), a three-word type and a
+    size, four supplier rows per part, and suppliers with comments (1% of them
+    hold "Customer ... Complaints")."""
+    np_ = _n(200_000, scale, 64)
+    ns = _n(10_000, scale, 16)
+    r = _rng(seed)
+    pk = (r.permutation(np_) + 1).astype(np.int32)
+    brand = r.integers(1, 6, (np_, 2))
+    t = r.integers(0, [len(C14_TYPE1), len(C14_TYPE2), len(C14_TYPE3)], (np_, 3))
+    part = {"p_partkey": pk,
+            "p_brand": StringColumn.from_list([b"Brand#%d%d" % (a, b) for a, b in brand]),
+            "p_type": StringColumn.from_list([b" ".join((C14_TYPE1[a], C14_TYPE2[b], C14_TYPE3[c])) for a, b, c in t]),
+            "p_size": r.integers(1, 51, np_, dtype=np.int32)}
+    base = np.repeat(np.arange(1, np_ + 1, dtype=np.int64), 4)
+    i = np.tile(np.arange(4, dtype=np.int64), np_)
+    partsupp = {"ps_partkey": base.astype(np.int32),
+                "ps_suppkey": ((base + i * (ns // 4 + (base - 1) // ns)) % ns + 1).astype(np.int32)}
+    supplier = {"s_suppkey": (r.permutation(ns) + 1).astype(np.int32),
+                "s_comment": _comments(r, ns, (b"Customer", b"Complaints"), 0.01)}
+    return Database([
+        Table("part", part, {"p_partkey": Type.INT, "p_brand": Type.STRING, "p_type": Type.STRING, "p_size": Type.INT}),
+        Table("partsupp", partsupp, {"ps_partkey": Type.INT, "ps_suppkey": Type.INT}),
+        Table("supplier", supplier, {"s_suppkey": Type.INT, "s_comment": Type.STRING})])
+
+
+def plan_c14(alg, scal, Type, Reduction, late_filter=False):
+    """TPC-H Q16: the parts not of one brand, not of a type prefix and of eight
+    sizes, joined to their supplier rows, without the suppliers with complaints
+    (an anti join), counted per supplier and then per (brand, type, size).
+    With ``late_filter`` the brand and type predicates run above the join, on
+    the strings the join carries from its build side."""
+    brand_ok = scal.NotExpr(scal.EqualsExpr(scal.AttrExpr("p_brand"), scal.ConstExpr("Brand#45", Type.STRING)))
+    type_ok = scal.NotExpr(scal.LikeExpr(scal.AttrExpr("p_type"), scal.ConstExpr("MEDIUM POLISHED%", Type.STRING)))
+    sizes = scal.InExpr(scal.AttrExpr("p_size"), [scal.ConstExpr(str(v), Type.INT) for v in C14_SIZES])
+    complaints = alg.selection(
+        scal.LikeExpr(scal.AttrExpr("s_comment"), scal.ConstExpr("%Customer%Complaints%", Type.STRING)),
+        alg.scan("supplier"))
+    if late_filter:
+        parts = alg.selection(sizes, alg.scan("part"))
+        join = alg.join(("p_partkey", "ps_partkey"), parts, alg.scan("partsupp"))
+        late = alg.selection(scal.AndExpr(brand_ok, type_ok), join)
+        top = late
+    else:
+        parts = alg.selection(scal.AndExpr(scal.AndExpr(brand_ok, type_ok), sizes), alg.scan("part"))
+        join = alg.join(("p_partkey", "ps_partkey"), parts, alg.scan("partsupp"))
+        late = None
+        top = join
+    anti = alg.antijoin(("ps_suppkey", "s_suppkey"), None, complaints, top)
+    per_supp = alg.aggregation(["p_brand", "p_type", "p_size", "ps_suppkey"],
+                               [(Reduction.COUNT, "", "supp_count_resolvedistinct")], anti)
+    agg = alg.aggregation(["p_brand", "p_type", "p_size"], [(Reduction.COUNT, "", "supp_count")], per_supp)
+    proj = alg.projection(["p_brand", "p_type", "p_size", "supp_count"], agg)
+    cfg = {parts.opId: {"selectivity": 0.15}, complaints.opId: {"selectivity": 0.01},
+           join.opId: {"multimatch": False},
+           per_supp.opId: {"numgroups": 120_000}, agg.opId: {"numgroups": 20_000}}
+    if late is not None:
+        cfg[late.opId] = {"selectivity": 0.8}
+    return proj, cfg
+
+
+C15_NATIONS = [b"ALGERIA", b"ARGENTINA", b"BRAZIL", b"CANADA", b"EGYPT", b"ETHIOPIA", b"FRANCE", b"GERMANY",
+               b"INDIA", b"INDONESIA", b"IRAN", b"IRAQ", b"JAPAN", b"JORDAN", b"KENYA", b"MOROCCO",
+               b"MOZAMBIQUE", b"PERU", b"CHINA", b"ROMANIA", b"SAUDI ARABIA", b"VIETNAM", b"RUSSIA",
+               b"UNITED KINGDOM", b"UNITED STATES"]
+C15_MODES = [b"REG AIR", b"AIR", b"RAIL", b"SHIP", b"TRUCK", b"MAIL", b"FOB"]
+
+
+def gen_c15(scale=1.0, seed=BASE_SEED + 15):
+    """Joins on strings: nations keyed by name (25, with a region), suppliers
+    naming their nation (1% name one that is not in the table), shipping modes
+    with one to three carriers each (a string key with duplicates) and line
+    items naming their mode (one mode of eight is not in the table)."""
+    ns = _n(100_000, scale, 64)
+    nl = _n(6_000_000, scale, 256)
+    r = _rng(seed)
+    nation = {"n_name": StringColumn.from_list(C15_NATIONS),
+              "n_regionkey": (np.arange(len(C15_NATIONS)) % 5).astype(np.int32)}
+    names = C15_NATIONS + [b"ATLANTIS"]
+    pick = np.where(r.random(ns) < 0.01, len(C15_NATIONS), r.integers(0, len(C15_NATIONS), ns))
+    supplier = {"s_suppkey": (r.permutation(ns) + 1).astype(np.int32),
+                "s_nation": StringColumn.from_list([names[i] for i in pick]),
+                "s_acctbal": r.integers(0, 1_000_000, ns, dtype=np.int32)}
+    reps = r.integers(1, 4, len(C15_MODES))
+    modes = {"m_mode": StringColumn.from_list([m for m, k in zip(C15_MODES, reps) for _ in range(k)]),
+             "m_carrier": np.arange(int(reps.sum()), dtype=np.int32) + 1,
+             "m_maxqty": r.integers(10, 51, int(reps.sum()), dtype=np.int32)}
+    lmodes = C15_MODES + [b"BARGE"]
+    lineitem = {"l_shipmode": StringColumn.from_list([lmodes[i] for i in r.integers(0, len(lmodes), nl)]),
+                "l_quantity": r.integers(1, 51, nl, dtype=np.int32)}
+    return Database([
+        Table("nation", nation, {"n_name": Type.STRING, "n_regionkey": Type.INT}),
+        Table("supplier", supplier, {"s_suppkey": Type.INT, "s_nation": Type.STRING, "s_acctbal": Type.INT}),
+        Table("modes", modes, {"m_mode": Type.STRING, "m_carrier": Type.INT, "m_maxqty": Type.INT}),
+        Table("lineitem", lineitem, {"l_shipmode": Type.STRING, "l_quantity": Type.INT})])
+
+
+def plan_c15(alg, scal, Type, Reduction, variant="unique", region_cut=3):
+    """One join on a string key.
+
+    * ``unique``: suppliers joined to their nation by name (a unique table of
+      the nation names), count and balance per region;
+    * ``multi``: line items joined to every carrier of their shipping mode (a
+      multimap keyed by the mode), count and quantity per carrier;
+    * ``semi`` / ``anti``: the suppliers whose nation is (not) among the
+      nations of the first regions, counted per nation name;
+    * ``exists``: the line items of a mode with a carrier that takes their
+      quantity (a semi join with a further condition on a string key), count
+      and quantity per mode;
+    * ``dup``: the carriers whose mode some line item ships by (a semi join
+      whose build side repeats each of its eight keys many times)."""
+    if variant == "dup":
+        j = alg.semijoin(("l_shipmode", "m_mode"), None, alg.scan("lineitem"), alg.scan("modes"))
+        agg = alg.aggregation(["m_carrier"], [(Reduction.COUNT, "", "carriers"),
+                                              (Reduction.SUM, "m_maxqty", "maxqty")], j)
+        return agg, {agg.opId: {"numgroups": 32}}
+    if variant == "unique":
+        j = alg.join(("n_name", "s_nation"), alg.scan("nation"), alg.scan("supplier"))
+        agg = alg.aggregation(["n_regionkey"], [(Reduction.COUNT, "", "suppliers"),
+                                                (Reduction.SUM, "s_acctbal", "balance")], j)
+        return agg, {j.opId: {"multimatch": False}, agg.opId: {"numgroups": 5}}
+    if variant == "multi":
+        j = alg.join(("m_mode", "l_shipmode"), alg.scan("modes"), alg.scan("lineitem"))
+        agg = alg.aggregation(["m_carrier"], [(Reduction.COUNT, "", "lines"),
+                                              (Reduction.SUM, "l_quantity", "quantity")], j)
+        return agg, {j.opId: {"multimatch": True}, agg.opId: {"numgroups": 32}}
+    if variant in ("semi", "anti"):
+        nat = alg.selection(scal.SmallerExpr(scal.AttrExpr("n_regionkey"), scal.ConstExpr(str(region_cut), Type.INT)),
+                            alg.scan("nation"))
+        make = alg.semijoin if variant == "semi" else alg.antijoin
+        j = make(("n_name", "s_nation"), None, nat, alg.scan("supplier"))
+        agg = alg.aggregation(["s_nation"], [(Reduction.COUNT, "", "suppliers")], j)
+        return agg, {nat.opId: {"selectivity": region_cut / 5.0}, agg.opId: {"numgroups": 32}}
+    cond = scal.LargerEqualExpr(scal.AttrExpr("m_maxqty"), scal.AttrExpr("l_quantity"))
+    j = alg.semijoin(("m_mode", "l_shipmode"), cond, alg.scan("modes"), alg.scan("lineitem"))
+    agg = alg.aggregation(["l_shipmode"], [(Reduction.COUNT, "", "lines"),
+                                           (Reduction.SUM, "l_quantity", "quantity")], j)
+    return agg, {j.opId: {"multimatch": True}, agg.opId: {"numgroups": 16}}
+
+
+C16_CODES = ["13", "31", "23", "29", "30", "18", "17"]
+
+
+def gen_c16(scale=1.0, seed=BASE_SEED + 16):
+    """Q22-shaped: customers with a phone number "CC-AAA-BBB-CCCC" (country
+    codes 10..34), an account balance (5% zero) and orders (every customer
+    whose key is a multiple of 3 has none)."""
+    nc = _n(150_000, scale, 64)
+    no = _n(1_500_000, scale, 64)
+    r = _rng(seed)
+    cc = r.integers(10, 35, nc)
+    rest = r.integers(0, [1000, 1000, 10000], (nc, 3))
+    cust = {"c_custkey": (r.permutation(nc) + 1).astype(np.int32),
+            "c_phone": StringColumn.from_list([b"%02d-%03d-%03d-%04d" % (c, a, b, d)
+                                               for c, (a, b, d) in zip(cc, rest)]),
+            "c_acctbal": np.where(r.random(nc) < 0.05, 0, r.integers(1, 1_000_000, nc)).astype(np.int32)}
+    with_orders = np.arange(1, nc + 1, dtype=np.int32)
+    with_orders = with_orders[with_orders % 3 != 0]
+    orders = {"o_custkey": with_orders[r.integers(0, len(with_orders), no)]}
+    return Database([
+        Table("customer", cust, {"c_custkey": Type.INT, "c_phone": Type.STRING, "c_acctbal": Type.INT}),
+        Table("orders", orders, {"o_custkey": Type.INT})])
+
+
+def plan_c16(alg, scal, Type, Reduction):
+    """TPC-H Q22: the customers of seven country codes (the phone number's
+    first two characters) with a balance above those codes' average positive
+    balance and no orders, counted and summed per country code (a substring as
+    a map result and group key)."""
+    def code(alias):
+        return scal.SubstringExpr(scal.AttrExpr(alias + ".c_phone"), scal.ConstExpr("1", Type.INT),
+                                  scal.ConstExpr("2", Type.INT))
+
+    def in_codes(alias):
+        return scal.InExpr(code(alias), [scal.ConstExpr(c, Type.STRING) for c in C16_CODES])
+
+    c1 = alg.selection(scal.AndExpr(scal.LargerExpr(scal.AttrExpr("c1.c_acctbal"), scal.ConstExpr("0", Type.INT)),
+                                    in_codes("c1")), alg.scan("customer", "c1"))
+    avg = alg.aggregation([], [(Reduction.AVG, "c1.c_acctbal", "avg")], c1)
+    c2 = alg.selection(in_codes("c2"), alg.scan("customer", "c2"))
+    cj = alg.crossjoin(scal.LargerExpr(scal.AttrExpr("c2.c_acctbal"), scal.AttrExpr("avg")), avg, c2)
+    anti = alg.antijoin([("o_custkey", "c_custkey")], None, alg.scan("orders"), cj)
+    m = alg.map("cntrycode", code("c2"), anti)
+    agg = alg.aggregation(["cntrycode"], [(Reduction.COUNT, "", "numcust"),
+                                          (Reduction.SUM, "c_acctbal", "totacctbal")], m)
+    cfg = {c1.opId: {"selectivity": 0.27}, c2.opId: {"selectivity": 0.28}, cj.opId: {"selectivity": 0.5},
+           anti.opId: {"multimatch": False}, agg.opId: {"numgroups": 7}}
+    return agg, cfg
+
+
 GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5, "c7": gen_c5, "c8": gen_c5,
               "c9": gen_c9, "c9p": gen_c9, "c10": gen_c10, "c10p": gen_c10, "c11": gen_c11, "c12": gen_c11,
-              "c13": gen_c5}
+              "c13": gen_c5, "c14": gen_c14, "c15": gen_c15, "c16": gen_c16}
 PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5, "c7": plan_c7,
          "c8": plan_c8, "c9": plan_c9, "c9p": plan_c9p, "c10": plan_c10, "c10p": plan_c10p, "c11": plan_c11,
-         "c12": plan_c12, "c13": plan_c13}
+         "c12": plan_c12, "c13": plan_c13, "c14": plan_c14, "c15": plan_c15, "c16": plan_c16}
 
 
 def build(name, alg, scale=1.0, **kw):

@@ -210,15 +210,22 @@ typedef enum {
     DQ_OP_LOGIC = 3,     /* sub: dq_logic                                      */
     DQ_OP_CAST = 4,      /* dst = (dst type) a                                 */
     DQ_OP_SELECT = 5,    /* dst = a ? b : c (CASE arm)                         */
-    DQ_OP_LIKE = 6,      /* dst = a LIKE pattern[res]                          */
-    DQ_OP_STREQ = 7,     /* dst = a == pattern[res] (string constant)          */
+    DQ_OP_LIKE = 6,      /* dst = a LIKE pattern[res]; a is a string column    */
+                         /* slot or a slot holding a string reference          */
+    DQ_OP_STREQ = 7,     /* dst = a == pattern[res] (string constant); with    */
+                         /* res = -1, dst = a == b (two string values)         */
     DQ_OP_STRREF = 8,    /* dst = reference to string slot a's value: the     */
-                         /* plan's string source << 48 | row (a U64 value that */
-                         /* group keys and output columns carry)               */
+                         /* plan's string source, a substring window and the  */
+                         /* row in one 64-bit value that join keys, payloads,  */
+                         /* group keys and output columns carry               */
     DQ_OP_PROFILE = 9,   /* lane-activity counter `res`: each warp step that   */
                          /* passes adds 1 to bin (active lanes, 0..32) of the  */
                          /* point's histogram (dq_plan_profile)                */
     DQ_OP_FILTER = 10,   /* keep rows with a != 0                              */
+    DQ_OP_SUBSTR = 14,   /* dst = SUBSTRING(a FROM f FOR n) of reference a:    */
+                         /* f = (int32_t)imm, n = (int32_t)(imm >> 32); the    */
+                         /* window (f - 1 .. f - 1 + n, clamped to the string) */
+                         /* must end within the string's first 255 bytes       */
     DQ_OP_PROBE = 11,    /* unique-HT probe (res); sub: dq_join                */
     DQ_OP_EXPAND = 12,   /* multimap probe (res) opening level+1               */
     DQ_OP_EXISTS = 13,   /* semi/anti probe of a multimap (res); sub: dq_join  */

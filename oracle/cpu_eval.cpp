@@ -183,10 +183,14 @@ struct Table {
   std::unordered_map<std::string, Column> cols;
 };
 
-// A string value is a reference: its string source (a column of a table) and
-// its row.
-constexpr int kRefShift = 48;
-constexpr uint64_t kRefRow = (1ull << kRefShift) - 1;
+// A string value is a reference: its string source (a column of a table,
+// bits 63..52), a substring flag (bit 51) with the window's first and end byte
+// offsets (bits 50..43, 42..35) and its row (bits 34..0), the device's layout.
+constexpr int kRefShift = 52;
+constexpr uint64_t kRefSub = 1ull << 51;
+constexpr int kRefStartShift = 43;
+constexpr int kRefEndShift = 35;
+constexpr uint64_t kRefRow = (1ull << kRefEndShift) - 1;
 
 struct Strings {
   std::vector<const Column*> src;
@@ -200,8 +204,33 @@ struct Strings {
       p = c.data + c.offsets[row];
       n = (int)(c.offsets[row + 1] - c.offsets[row]);
     }
+    if (ref & kRefSub) {
+      const int st = std::min((int)((ref >> kRefStartShift) & 0xff), n);
+      const int en = std::max(std::min((int)((ref >> kRefEndShift) & 0xff), n), st);
+      p += st;
+      n = en - st;
+    }
   }
 };
+
+// SUBSTRING(s, from, len) as a window on the reference: the first byte from - 1,
+// len bytes, within the parent window (the reference's stringSubstring,
+// include/util.cuh:132-142); a window past the string's end is empty.
+uint64_t substring_ref(uint64_t ref, int from, int len) {
+  int s0 = 0, e0 = 1 << 30;
+  if (ref & kRefSub) {
+    s0 = (int)((ref >> kRefStartShift) & 0xff);
+    e0 = (int)((ref >> kRefEndShift) & 0xff);
+  }
+  int st = s0 + from - 1;
+  int en = st + len;
+  st = std::max(st, s0);
+  en = std::min(en, e0);
+  st = std::min(std::max(st, 0), 255);
+  en = std::min(std::max(en, st), 255);
+  return (ref & ((~0ull << kRefShift) | kRefRow)) | kRefSub | ((uint64_t)st << kRefStartShift) |
+         ((uint64_t)en << kRefEndShift);
+}
 
 // ------------------------------------------------------------ resources --
 
@@ -239,6 +268,21 @@ struct KeyHash {
       if (na != nb || memcmp(pa, pb, (size_t)na) != 0) return false;
     }
     return true;
+  }
+  // A total order of keys that agrees with eq (strings by their bytes).
+  int cmp(const uint64_t* a, const uint64_t* b) const {
+    for (int i = 0; i < r->nkeys; ++i) {
+      if (a[i] == b[i]) continue;
+      if (r->key_ctype[i] != DQ_STR) return a[i] < b[i] ? -1 : 1;
+      const uint8_t *pa, *pb;
+      int na, nb;
+      strs->at(a[i], pa, na);
+      strs->at(b[i], pb, nb);
+      const int c = memcmp(pa, pb, (size_t)std::min(na, nb));
+      if (c != 0) return c;
+      if (na != nb) return na < nb ? -1 : 1;
+    }
+    return 0;
   }
 };
 
@@ -287,9 +331,11 @@ struct UniqueTable {
   int nk = 0;
   std::vector<uint64_t> slots;   // (1 + W) words a slot; word 0: 1 if used
   uint64_t mask = 0;
+  const KeyHash* keq = nullptr;  // key equality (string keys by their bytes)
   void build(const Rows& rows, int nkeys, const KeyHash& kh) {
     W = rows.width;
     nk = nkeys;
+    keq = &kh;
     uint64_t cap = 16;
     while (cap < (uint64_t)rows.n() * 2) cap <<= 1;
     mask = cap - 1;
@@ -304,7 +350,7 @@ struct UniqueTable {
           std::copy(row, row + W, sl + 1);
           break;
         }
-        if (std::equal(row, row + nk, sl + 1)) break;
+        if (kh.eq(row, sl + 1)) break;
         h = (h + 1) & mask;
       }
     }
@@ -316,7 +362,7 @@ struct UniqueTable {
     for (;;) {
       const uint64_t* sl = &slots[h * (W + 1)];
       if (!sl[0]) return nullptr;
-      if (std::equal(k, k + nk, sl + 1)) return sl + 1;
+      if (keq->eq(k, sl + 1)) return sl + 1;
       h = (h + 1) & mask;
     }
   }
@@ -662,6 +708,13 @@ struct Plan {
     if (C.nsel) emit();
   }
 
+  // The reference of string slot s for row i: a string column's value is its
+  // source row's, anything else holds a reference already.
+  uint64_t str_value(const Pipeline& p, const Level& L, int s, uint32_t i) const {
+    if (p.d->slots[s].kind == DQ_SLOT_STR) return ((uint64_t)p.sid[s] << kRefShift) | (uint64_t)L.srow[i];
+    return L.slot(s)[i];
+  }
+
   // Ops k.. over the active rows of batch L at `level`.
   void eval(const Pipeline& p, int k, int level, Worker& w) const {
     const dq_pipeline& d = *p.d;
@@ -679,18 +732,32 @@ struct Plan {
         case DQ_OP_LIKE:
         case DQ_OP_STREQ: {
           uint64_t* dst = L.slot(op.dst);
-          const std::string& pat = p.patterns[op.res];
-          if (d.slots[op.a].kind != DQ_SLOT_STR) throw Fail("string op on a non-string slot");
-          const uint64_t base = (uint64_t)p.sid[op.a] << kRefShift;
+          const bool two = op.kind == DQ_OP_STREQ && op.res < 0;
+          static const std::string none;
+          const std::string& pat = two ? none : p.patterns[op.res];
           for (int j = 0; j < L.nsel; ++j) {
             const uint32_t i = L.sel[j];
             const uint8_t* s;
             int n;
-            strs.at(base | (uint64_t)L.srow[i], s, n);
-            dst[i] = op.kind == DQ_OP_LIKE
-                         ? like_match(s, n, reinterpret_cast<const uint8_t*>(pat.data()), (int)pat.size())
-                         : (n == (int)pat.size() && memcmp(s, pat.data(), (size_t)n) == 0);
+            strs.at(str_value(p, L, op.a, i), s, n);
+            if (two) {
+              const uint8_t* t;
+              int m;
+              strs.at(str_value(p, L, op.b, i), t, m);
+              dst[i] = n == m && memcmp(s, t, (size_t)n) == 0;
+            } else {
+              dst[i] = op.kind == DQ_OP_LIKE
+                           ? like_match(s, n, reinterpret_cast<const uint8_t*>(pat.data()), (int)pat.size())
+                           : (n == (int)pat.size() && memcmp(s, pat.data(), (size_t)n) == 0);
+            }
           }
+          break;
+        }
+        case DQ_OP_SUBSTR: {
+          uint64_t* dst = L.slot(op.dst);
+          const uint64_t* a = L.slot(op.a);
+          const int from = (int32_t)(uint32_t)op.imm, len = (int32_t)(uint32_t)((uint64_t)op.imm >> 32);
+          for (int j = 0; j < L.nsel; ++j) dst[L.sel[j]] = substring_ref(a[L.sel[j]], from, len);
           break;
         }
         case DQ_OP_STRREF: {
@@ -916,8 +983,7 @@ struct Plan {
     };
     const int W = r.rows.width;
     const int nk = r.d->nkeys;
-    for (int i = 0; i < nk; ++i)
-      if (r.d->key_ctype[i] == DQ_STR) throw Fail("string multimap keys");
+    const KeyHash& kh = r.agg.kh;   // string keys compare by their bytes
     const int P = threads;
     const int nw = (int)workers.size();
     std::vector<std::vector<uint64_t>> hashes(nw);
@@ -966,18 +1032,15 @@ struct Plan {
       for (int64_t i = lo; i < hi; ++i) idx[i - lo] = {phash[i], i};
       std::sort(idx.begin(), idx.end());
       auto key_less = [&](const std::pair<uint64_t, int64_t>& a, const std::pair<uint64_t, int64_t>& b) {
-        for (int k = 0; k < nk; ++k)
-          if (part[(size_t)a.second * W + k] != part[(size_t)b.second * W + k])
-            return part[(size_t)a.second * W + k] < part[(size_t)b.second * W + k];
-        return a.second < b.second;
+        const int c = kh.cmp(&part[(size_t)a.second * W], &part[(size_t)b.second * W]);
+        return c != 0 ? c < 0 : a.second < b.second;
       };
       for (size_t a = 0; a < idx.size();) {
         size_t b = a + 1;
         while (b < idx.size() && idx[b].first == idx[a].first) ++b;
         bool mixed = false;
         for (size_t c = a + 1; c < b && !mixed; ++c)
-          mixed = !std::equal(&part[(size_t)idx[c].second * W], &part[(size_t)idx[c].second * W + nk],
-                              &part[(size_t)idx[a].second * W]);
+          mixed = !kh.eq(&part[(size_t)idx[c].second * W], &part[(size_t)idx[a].second * W]);
         if (mixed) std::sort(idx.begin() + a, idx.begin() + b, key_less);
         a = b;
       }
@@ -985,8 +1048,7 @@ struct Plan {
       for (int64_t i = lo; i < hi; ++i) {
         const int64_t src = idx[i - lo].second;
         std::copy(&part[(size_t)src * W], &part[(size_t)(src + 1) * W], &sorted.v[(size_t)i * W]);
-        if (i > lo && !std::equal(&sorted.v[(size_t)i * W], &sorted.v[(size_t)i * W + nk],
-                                  &sorted.v[(size_t)(i - 1) * W])) {
+        if (i > lo && !kh.eq(&sorted.v[(size_t)i * W], &sorted.v[(size_t)(i - 1) * W])) {
           run[start] = i - start;
           start = i;
         }

@@ -308,6 +308,11 @@ def evaluate(e, frame, n):
         end = start + c.astype(np.int64)
         start = np.maximum(start, s.start)
         end = np.minimum(end, s.end)
+        # a window that starts past the string's end (or a negative length)
+        # gives the reference a string of negative length, equal to nothing
+        # and hashed over no bytes; here it is the empty string
+        start = np.minimum(start, s.end)
+        end = np.maximum(end, start)
         return Strs(s.heap, start, end), "str"
     raise NotImplementedError("scalar expression %s" % k)
 
@@ -363,6 +368,7 @@ class Oracle(object):
     def __init__(self, db):
         self.db = db
         self.temps = {}
+        self._string_ids = {}
 
     def run(self, plan):
         out = None
@@ -433,17 +439,40 @@ class Oracle(object):
         return f
 
     # -- joins ----------------------------------------------------------------
-    @staticmethod
-    def _keys(frame, atts_a, atts_b):
-        """Keys of frame for attributes ``atts_a`` compared against ``atts_b``."""
+    def _keys(self, frame, atts_a, atts_b):
+        """Keys of frame for attributes ``atts_a`` compared against ``atts_b``.
+        A string key becomes the number of its bytes in a dictionary shared
+        by both sides of every join (the reference hashes and compares the
+        bytes, hashTableUtil.py:15-35)."""
         cols = []
         for a, b in zip(atts_a, atts_b):
             ta, tb = lang_type(a.dataType), lang_type(b.dataType)
             v = frame[a.id]
-            if ta == "str":
-                raise NotImplementedError("string join keys")
+            if ta == "str" or tb == "str":
+                if ta != tb:
+                    raise NotImplementedError("join keys comparing a string with a number")
+                cols.append(self._string_key_ids(v))
+                continue
             cols.append(conv(v, common(ta, tb)).astype(np.uint64).view(np.int64))
         return cols
+
+    def _string_key_ids(self, v):
+        """Dictionary numbers of the strings of ``v``: the distinct byte strings
+        are found over a zero-padded matrix (with the length as a last column),
+        then numbered through the shared dictionary."""
+        n = len(v)
+        if n == 0:
+            return np.zeros(0, dtype=np.int64)
+        lens = v.end - v.start
+        width = int(lens.max())
+        pos = v.start[:, None] + np.arange(max(width, 1))[None, :]
+        inside = np.arange(max(width, 1))[None, :] < lens[:, None]
+        mat = np.where(inside, v.heap[np.minimum(pos, max(len(v.heap) - 1, 0))] if len(v.heap) else 0, 0)
+        mat = np.concatenate([mat.astype(np.int64), lens[:, None].astype(np.int64)], axis=1)
+        uniq, inv = np.unique(mat, axis=0, return_inverse=True)
+        ids = self._string_ids
+        local = np.array([ids.setdefault(bytes(u[:u[-1]].astype(np.uint8)), len(ids)) for u in uniq], dtype=np.int64)
+        return local[inv.reshape(-1)]
 
     def equijoin(self, node):
         jt = tname(node.joinType)

@@ -46,6 +46,24 @@ CASES = {
     "c13_s": dict(workload="c13", scale=0.05),
     "c13_mm": dict(workload="c13", scale=0.05, plan_kw=dict(multimatch=True)),
     "c13": dict(workload="c13", scale=1.0),
+    # strings beyond the scan: Q16 (string predicates before / after the join,
+    # string group keys of an aggregation over an aggregation), joins on string
+    # keys (unique, multimatch, semi, anti, semi with a condition), Q22
+    # (substrings in an IN list, as a map result and a group key)
+    "c14_s": dict(workload="c14", scale=0.05, str_cols=[0, 1]),
+    "c14_late_s": dict(workload="c14", scale=0.05, str_cols=[0, 1], plan_kw=dict(late_filter=True)),
+    "c14": dict(workload="c14", scale=1.0, str_cols=[0, 1]),
+    "c15_u_s": dict(workload="c15", scale=0.02, plan_kw=dict(variant="unique")),
+    "c15_m_s": dict(workload="c15", scale=0.02, plan_kw=dict(variant="multi")),
+    "c15_semi_s": dict(workload="c15", scale=0.02, str_cols=[0], plan_kw=dict(variant="semi")),
+    "c15_anti_s": dict(workload="c15", scale=0.02, str_cols=[0], plan_kw=dict(variant="anti")),
+    "c15_x_s": dict(workload="c15", scale=0.02, str_cols=[0], plan_kw=dict(variant="exists")),
+    # the reference's filter table stores every repeat of a build key in a slot
+    # of its own, so an insert walks all earlier repeats: kept small
+    "c15_dup_s": dict(workload="c15", scale=0.005, plan_kw=dict(variant="dup")),
+    "c15_m": dict(workload="c15", scale=1.0, plan_kw=dict(variant="multi")),
+    "c16_s": dict(workload="c16", scale=0.05, str_cols=[0]),
+    "c16": dict(workload="c16", scale=1.0, str_cols=[0]),
     # full sizes: row counts, checksums and (small) full results are committed
     "c0": dict(workload="c0", scale=1.0),
     "c1": dict(workload="c1", scale=1.0),

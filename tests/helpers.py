@@ -34,3 +34,12 @@ def reference_rows(rows, spec):
     sc = set(spec.get("str_cols", ()))
     return sorted([render_string(v) if j in sc else int(v) for j, v in enumerate(r)] for r in rows)
 
+
+
+def result_checksum(rows, spec):
+    """Checksum of result rows as the fixtures hold it: string columns as the
+    reference's result file shows them."""
+    from canonical import canonical_checksum
+    if spec.get("str_cols"):
+        return canonical_checksum(reference_rows(rows, spec))
+    return canonical_checksum(rows)

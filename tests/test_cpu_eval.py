@@ -6,10 +6,10 @@ change a result)."""
 import pytest
 
 from canonical import canonical_checksum
-from helpers import golden, golden_cases, make_case, reference_rows
+from helpers import golden, golden_cases, make_case, reference_rows, result_checksum
 
 SMALL = [c for c in golden_cases() if golden(c)["spec"]["scale"] < 0.1]
-FULL = ["c0", "c1", "c5", "c7", "c8", "c11", "c13"]
+FULL = ["c0", "c1", "c5", "c7", "c8", "c11", "c13", "c14", "c15_m", "c16"]
 
 
 def _run(case, threads):
@@ -32,7 +32,7 @@ def test_small_cases_match_reference(case, threads):
 def test_full_size_matches_reference(case):
     g, names, rows = _run(case, 4)
     assert len(rows) == g["nrows"]
-    assert canonical_checksum(rows) == g["checksum"]
+    assert result_checksum(rows, g["spec"]) == g["checksum"]
 
 
 def test_evaluates_the_ir_the_device_prepares():
