@@ -1,6 +1,7 @@
 """Batched form: many independent instances of one plan shape in one launch.
 
-An instance is a workload shape (c0..c3) at its own size, on its own tables.
+An instance is a workload shape (c0..c3, or the string shapes c9, c14, c16) at
+its own size, on its own tables.
 Its tables are registered under instance names (``<table>@<i>``) and its lowered
 plan is rewritten to scan them, so every instance has the same pipelines and
 ops and the C ABI's batch (dq_batch_*) runs them all through one generated
@@ -19,8 +20,10 @@ from dogqc_b200.database import Database, Table
 from dogqc_b200.lowering import Lowering
 from dogqc_b200.relational import RelationalAlgebra
 
-# rows of the largest table of each shape at scale 1 (instance sizes scale it)
-FULL_ROWS = {"c0": 6_000_000, "c1": 6_000_000, "c2": 16_777_216, "c3": 60_000_000}
+# rows of the largest table of each shape at scale 1 (instance sizes scale it);
+# c9, c14 and c16 carry strings (group keys, predicates, substrings, results)
+FULL_ROWS = {"c0": 6_000_000, "c1": 6_000_000, "c2": 16_777_216, "c3": 60_000_000, "c9": 6_000_000,
+             "c14": 800_000, "c16": 1_500_000}
 SEED = workloads.BASE_SEED + 7000
 
 

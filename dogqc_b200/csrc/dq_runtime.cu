@@ -905,7 +905,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     if ((d.ops[i].kind == DQ_OP_EXISTS || d.ops[i].kind == DQ_OP_PROFILE) && !p.jit && !plan->opts.batch_member)
       throw DqError(DQ_ERR_UNSUPPORTED, "semi/anti joins with conditions and lane-activity profiles run on "
                                         "generated kernels only (not DQ_CFG_NO_JIT / DQ_CFG_ROW_KERNEL)");
-  if (!p.jit)
+  if (!p.jit && !plan->opts.batch_member)
     for (int k = 0; k < p.desc.nops; ++k) {
       const dq_op& op = p.desc.ops[k];
       // the prebuilt kernels read strings in place only: references (string
@@ -915,8 +915,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
                          (op.res < 0 || p.desc.slots[op.a].kind != DQ_SLOT_STR));
       if (refs)
         throw DqError(DQ_ERR_UNSUPPORTED, "string join keys, string group keys, substrings and string result columns "
-                                          "run on generated plan kernels only (not DQ_CFG_NO_JIT / "
-                                          "DQ_CFG_ROW_KERNEL, batches or served batches)");
+                                          "run on generated kernels only (not DQ_CFG_NO_JIT / DQ_CFG_ROW_KERNEL)");
     }
   int occ = 1;
   int64_t rows_per_cta = tile;
@@ -1151,6 +1150,53 @@ int run_once(dq_plan* plan, cudaStream_t st) {
   return status;
 }
 
+// A result's string column: the n references a run left in device memory,
+// gathered on the device through the plan's string sources into nrows + 1
+// offsets and a heap, then copied to the host.
+void gather_string_column(const dq_plan* plan, const uint64_t* refs, uint64_t n, cudaStream_t st,
+                          std::vector<uint8_t>& offsets, std::vector<uint8_t>& heap_out) {
+  DevBuf lens, offs, heap;
+  lens.alloc(std::max<uint64_t>(n, 1) * 8);
+  offs.alloc((n + 1) * 8);
+  DQ_CUDA(launch_str_ref_offsets(refs, n, plan->str_src_dev.as<DevStr>(), lens.as<uint64_t>(), offs.as<uint64_t>(),
+                                 plan->ctx->sms, st));
+  offsets.resize((size_t)(n + 1) * 8);
+  DQ_CUDA(cudaMemcpyAsync(offsets.data(), offs.ptr, (n + 1) * 8, cudaMemcpyDeviceToHost, st));
+  DQ_CUDA(cudaStreamSynchronize(st));
+  uint64_t total = 0;
+  memcpy(&total, offsets.data() + n * 8, 8);
+  heap.alloc(std::max<uint64_t>(total, 1));
+  DQ_CUDA(launch_str_ref_copy(refs, n, plan->str_src_dev.as<DevStr>(), offs.as<uint64_t>(), heap.as<uint8_t>(),
+                              plan->ctx->sms, st));
+  heap_out.resize(total);
+  if (total) DQ_CUDA(cudaMemcpyAsync(heap_out.data(), heap.ptr, total, cudaMemcpyDeviceToHost, st));
+  DQ_CUDA(cudaStreamSynchronize(st));
+}
+
+// Result columns of a plan's OUTPUT resource whose n rows were copied to the
+// host at `packed` + col_off[j] (fixed-width columns); string columns are
+// gathered from the device references instead.
+dq_result* packed_result(const dq_plan* plan, const uint8_t* packed, const std::vector<uint64_t>& col_off, uint64_t n,
+                         cudaStream_t st) {
+  const ResRec& o = *plan->res[plan->result_res];
+  std::unique_ptr<dq_result> res(new dq_result());
+  res->nrows = (int64_t)n;
+  res->heaps.resize(o.desc.npay);
+  for (int j = 0; j < o.desc.npay; ++j) {
+    const int w = ctype_width(o.desc.pay_ctype[j]);
+    res->ctypes.push_back(o.desc.pay_ctype[j]);
+    if (o.desc.pay_ctype[j] == DQ_STR) {
+      res->cols.emplace_back();
+      gather_string_column(plan, reinterpret_cast<const uint64_t*>(o.dev.pay[j]), n, st, res->cols.back(),
+                           res->heaps[j]);
+      continue;
+    }
+    const uint8_t* src = packed + col_off[j];
+    res->cols.emplace_back(src, src + (size_t)n * w);
+  }
+  return res.release();
+}
+
 // Copies a completed execution's result (OUTPUT resource) to the host.
 dq_result* read_result(dq_plan* plan, cudaStream_t st) {
   ResRec& o = *plan->res[plan->result_res];
@@ -1165,24 +1211,9 @@ dq_result* read_result(dq_plan* plan, cudaStream_t st) {
     int w = ctype_width(o.desc.pay_ctype[j]);
     res->ctypes.push_back(o.desc.pay_ctype[j]);
     if (o.desc.pay_ctype[j] == DQ_STR) {
-      // references -> offsets and a heap, gathered on the device
-      DevBuf lens, offs, heap;
-      lens.alloc(std::max<uint64_t>(n, 1) * 8);
-      offs.alloc((n + 1) * 8);
-      const uint64_t* refs = reinterpret_cast<const uint64_t*>(o.dev.pay[j]);
-      DQ_CUDA(launch_str_ref_offsets(refs, n, plan->str_src_dev.as<DevStr>(), lens.as<uint64_t>(), offs.as<uint64_t>(),
-                                     plan->ctx->sms, st));
-      res->cols.emplace_back((size_t)(n + 1) * 8);
-      DQ_CUDA(cudaMemcpyAsync(res->cols.back().data(), offs.ptr, (n + 1) * 8, cudaMemcpyDeviceToHost, st));
-      DQ_CUDA(cudaStreamSynchronize(st));
-      uint64_t total = 0;
-      memcpy(&total, res->cols.back().data() + n * 8, 8);
-      heap.alloc(std::max<uint64_t>(total, 1));
-      DQ_CUDA(launch_str_ref_copy(refs, n, plan->str_src_dev.as<DevStr>(), offs.as<uint64_t>(), heap.as<uint8_t>(),
-                                  plan->ctx->sms, st));
-      res->heaps[j].resize(total);
-      if (total) DQ_CUDA(cudaMemcpyAsync(res->heaps[j].data(), heap.ptr, total, cudaMemcpyDeviceToHost, st));
-      DQ_CUDA(cudaStreamSynchronize(st));
+      res->cols.emplace_back();
+      gather_string_column(plan, reinterpret_cast<const uint64_t*>(o.dev.pay[j]), n, st, res->cols.back(),
+                           res->heaps[j]);
       continue;
     }
     res->cols.emplace_back((size_t)n * w);
@@ -2273,17 +2304,15 @@ int dq_batch_execute(dq_batch* b, void* stream, dq_result** results) {
     b->timing.max_pipeline = -1;
     b->timing.kernel_launches = b->launches;
     const uint64_t* rows = reinterpret_cast<const uint64_t*>(b->host + b->packed_bytes);
-    for (int i = 0; i < b->ninst; ++i) {
-      const ResRec& o = *b->inst[i]->res[b->inst[i]->result_res];
-      std::unique_ptr<dq_result> res(new dq_result());
-      res->nrows = (int64_t)rows[i];
-      for (int j = 0; j < o.desc.npay; ++j) {
-        const int w = ctype_width(o.desc.pay_ctype[j]);
-        res->ctypes.push_back(o.desc.pay_ctype[j]);
-        const uint8_t* src = b->host + b->col_off[i][j];
-        res->cols.emplace_back(src, src + (size_t)rows[i] * w);
+    for (int i = 0; i < b->ninst; ++i) results[i] = nullptr;
+    try {
+      for (int i = 0; i < b->ninst; ++i) results[i] = packed_result(b->inst[i].get(), b->host, b->col_off[i], rows[i], st);
+    } catch (...) {
+      for (int i = 0; i < b->ninst; ++i) {
+        delete results[i];
+        results[i] = nullptr;
       }
-      results[i] = res.release();
+      throw;
     }
     return (int)DQ_OK;
   });
@@ -2556,20 +2585,23 @@ dq_result* srv_graph_result(PoolEntry* pe, cudaStream_t st) {
   uint64_t n = 0;
   memcpy(&n, pe->host_out, 8);
   if (n > o.dev.cap) n = o.dev.cap;
+  if (!pe->count_only) return packed_result(pe->plan.get(), pe->host_out, pe->col_off, n, st);
   std::unique_ptr<dq_result> res(new dq_result());
   res->nrows = (int64_t)n;
+  res->heaps.resize(o.desc.npay);
   for (int j = 0; j < o.desc.npay; ++j) {
     const int w = ctype_width(o.desc.pay_ctype[j]);
     res->ctypes.push_back(o.desc.pay_ctype[j]);
-    if (pe->count_only) {
+    if (o.desc.pay_ctype[j] == DQ_STR) {
+      res->cols.emplace_back();
+      gather_string_column(pe->plan.get(), reinterpret_cast<const uint64_t*>(o.dev.pay[j]), n, st, res->cols.back(),
+                           res->heaps[j]);
+    } else {
       res->cols.emplace_back((size_t)n * w);
       if (n) DQ_CUDA(cudaMemcpyAsync(res->cols.back().data(), o.dev.pay[j], (size_t)n * w, cudaMemcpyDeviceToHost, st));
-    } else {
-      const uint8_t* src = pe->host_out + pe->col_off[j];
-      res->cols.emplace_back(src, src + (size_t)n * w);
     }
   }
-  if (pe->count_only && n) DQ_CUDA(cudaStreamSynchronize(st));
+  if (n) DQ_CUDA(cudaStreamSynchronize(st));
   return res.release();
 }
 
@@ -3018,18 +3050,17 @@ void srv_complete_batch(dq_server* s, SrvSlot& slot) {
   for (int i = 0; i < K; ++i) {
     SrvReq* r = members[i].first;
     PoolEntry* pe = members[i].second;
-    const ResRec& o = *pe->plan->res[pe->plan->result_res];
-    std::unique_ptr<dq_result> res(new dq_result());
-    res->nrows = (int64_t)rows[i];
-    for (int j = 0; j < o.desc.npay; ++j) {
-      const int w = ctype_width(o.desc.pay_ctype[j]);
-      res->ctypes.push_back(o.desc.pay_ctype[j]);
-      const uint8_t* src = B.host_out + B.col_off[i][j];
-      res->cols.emplace_back(src, src + (size_t)rows[i] * w);
+    dq_result* res = nullptr;
+    try {
+      res = packed_result(pe->plan.get(), B.host_out, B.col_off[i], rows[i], slot.st);
+    } catch (const DqError& e) {
+      srv_release(s, r, pe);
+      srv_finish(s, r, e.code, e.what(), nullptr);
+      continue;
     }
     r->info.kernel_launches += B.launches;
     srv_release(s, r, pe);
-    srv_finish(s, r, DQ_OK, "", res.release());
+    srv_finish(s, r, DQ_OK, "", res);
   }
 }
 
@@ -3455,18 +3486,9 @@ void precompile(dq_server* s, const DescCopy& d) {
 
 extern "C" {
 
-// Served results are copied back raw; string references would need the gather.
-void reject_string_results(const dq_plan_desc& d) {
-  for (int i = 0; i < d.npipes; ++i)
-    for (int k = 0; k < d.pipes[i].nops; ++k)
-      if (d.pipes[i].ops[k].kind == DQ_OP_STRREF)
-        throw DqError(DQ_ERR_UNSUPPORTED, "served requests with string group keys or string result columns");
-}
-
 int dq_server_submit(dq_server* s, const dq_plan_desc* desc, uint64_t* ticket) {
   if (!s || !desc || !ticket) return DQ_ERR_INVALID;
   return guarded(s->ctx, [&]() {
-    reject_string_results(*desc);
     std::shared_ptr<DescCopy> d = copy_desc(desc);
     precompile(s, *d);
     uint64_t est;
@@ -3487,7 +3509,6 @@ int dq_server_replay(dq_server* s, int32_t nq, const dq_plan_desc* queries, int6
   return guarded(s->ctx, [&]() {
     std::vector<std::shared_ptr<DescCopy>> descs;
     std::vector<uint64_t> est;
-    for (int q = 0; q < nq; ++q) reject_string_results(queries[q]);
     for (int q = 0; q < nq; ++q) descs.push_back(copy_desc(&queries[q]));
     // the driver holds every query before the first arrival: unseen shapes are
     // compiled now, as their submitters would have compiled them

@@ -43,6 +43,15 @@ def test_batch_matches_oracle(engine, shape, n, lo, hi):
     _check(engine, _instances(shape, n, lo, hi))
 
 
+@pytest.mark.parametrize("shape,n,lo,hi", [("c9", 5, 1 << 10, 1 << 15), ("c14", 4, 1 << 12, 1 << 15),
+                                            ("c16", 4, 1 << 11, 1 << 15)])
+def test_batch_with_strings_matches_oracle(engine, shape, n, lo, hi):
+    """String group keys and result columns (c9), string predicates, string
+    keys of an aggregation over an aggregation (c14) and substrings (c16):
+    each instance's references resolve against its own tables."""
+    _check(engine, _instances(shape, n, lo, hi))
+
+
 @pytest.mark.parametrize("tuning", [{"rows_per_thread": 1}, {"rows_per_thread": 4, "block_threads": 128},
                                     {"block_threads": 512, "refill": -1}, {"multi_buckets_pct": 50},
                                     {"unique_slots_pct": 400}])

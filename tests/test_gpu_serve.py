@@ -183,3 +183,26 @@ def test_unseen_shape_compiles_in_the_submitter(engine, queries):
         assert canonical_rows(res.rows()) == canonical_rows(run_plan(db, plan)[1])
     finally:
         srv.stop()
+
+
+def test_string_requests_alone_and_batched(engine):
+    """Requests with string group keys, predicates, substrings and string
+    result columns, alone and as continuous batches: their results are the
+    oracle's, strings gathered per request."""
+    from dogqc_b200 import serve
+    qs = serve.make_queries(shapes=("c9", "c14", "c16"), sizes=(0.0005, 0.002, 0.01))
+    serve.register(engine, qs)
+    want = [canonical_rows(run_plan(q.base_db, q.plan)[1]) for q in qs]
+    for batch_max in (8, 1):
+        srv = serve.Server(engine, slots=2, batch_max=batch_max)
+        try:
+            serve.warm(srv, qs, 2, rounds=1)
+            sched = serve.arrivals(48, None, qs, seed=21)
+            results, infos, wall, errors = serve.mixed_stream(srv, qs, sched)
+            assert not errors
+            for (at, qi), res in zip(sched, results):
+                assert canonical_rows(res.rows()) == want[qi]
+            if batch_max > 1:
+                assert srv.stats()["batches"] > 0
+        finally:
+            srv.stop()

@@ -11,8 +11,7 @@ string group keys of an aggregation over an aggregation (Q16 shape), joins on
 string keys (unique, multimatch, semi, anti, semi with a condition, a build
 side repeating its keys), substrings in IN lists, as map results and group
 keys (Q22 shape), substring windows at and past the string's ends, and the
-paths that do not take string references (batches, served requests, the
-prebuilt kernels) refusing them."""
+prebuilt kernels refusing string references."""
 import numpy as np
 import pytest
 
@@ -136,29 +135,21 @@ def test_imported_text_string_keys(engine):
     assert got == canonical_rows(run_plan(db, plan)[1])
 
 
-def test_paths_without_string_results_refuse_them(engine):
+def test_prebuilt_kernels_refuse_string_references(engine):
+    """The prebuilt kernels read strings in place only: plans whose strings
+    travel as references (group keys, results, join keys, substrings) are
+    refused there; batches and served requests take them (test_gpu_batch,
+    test_gpu_serve)."""
     from dogqc_b200 import _lib as L
     from dogqc_b200.engine import Engine
-    from dogqc_b200.lowering import Lowering
-    db, alg, plan = make_case({"workload": "c9", "scale": 0.002})
-    engine.register_database(db, force=True)
-    lw = Lowering(plan)
-    with pytest.raises(L.DqError) as e:
-        engine.prepare_batch([lw, Lowering(plan)])
-    assert e.value.status == L.ERR_UNSUPPORTED
     prebuilt = Engine(0, flags=L.CFG_NO_JIT)
     try:
-        prebuilt.register_database(db)
-        with pytest.raises(L.DqError) as e:
-            prebuilt.prepare(plan)
-        assert e.value.status == L.ERR_UNSUPPORTED
+        for case in ({"workload": "c9", "scale": 0.002}, {"workload": "c16", "scale": 0.002},
+                     {"workload": "c15", "scale": 0.002, "plan_kw": {"variant": "unique"}}):
+            db, alg, plan = make_case(case)
+            prebuilt.register_database(db, force=True)
+            with pytest.raises(L.DqError) as e:
+                prebuilt.prepare(plan)
+            assert e.value.status == L.ERR_UNSUPPORTED
     finally:
         prebuilt.close()
-    from dogqc_b200 import serve
-    srv = serve.Server(engine, slots=2)
-    try:
-        with pytest.raises(L.DqError) as e:
-            srv.submit(lw)
-        assert e.value.status == L.ERR_UNSUPPORTED
-    finally:
-        srv.stop()
