@@ -296,13 +296,37 @@ __device__ __forceinline__ uint64_t str_ref_substring(uint64_t ref, int from, in
          ((uint64_t)en << kStrRefEndShift);
 }
 
+// String hash: the string's 8-byte little-endian words (the last one
+// zero-padded), each mixed with its index, summed, and the sum finalised with
+// the length.  A sum of independent word terms lets a warp hash one string a
+// word per lane (str_ref_hash_warp) and reach the value one lane computes
+// alone, so either may hash the keys of one table.
+__device__ __forceinline__ uint64_t str_word(const uint8_t* p, int n, int i) {
+  const int b = 8 * i, e = b + 8 < n ? b + 8 : n;
+  uint64_t w = 0;
+  for (int j = b; j < e; ++j) w |= (uint64_t)p[j] << (8 * (j - b));
+  return w;
+}
+
+__device__ __forceinline__ uint64_t str_word_term(uint64_t w, int i) {
+  return fmix64(w ^ (0x9e3779b97f4a7c15ull * (uint64_t)(i + 1)));
+}
+
+__device__ __forceinline__ uint64_t str_hash_final(uint64_t sum, int n) {
+  return fmix64(sum + (uint64_t)n * 0xc2b2ae3d27d4eb4full);
+}
+
+__device__ __forceinline__ uint64_t str_hash(const uint8_t* p, int n) {
+  uint64_t sum = 0;
+  for (int i = 0; 8 * i < n; ++i) sum += str_word_term(str_word(p, n, i), i);
+  return str_hash_final(sum, n);
+}
+
 __device__ __forceinline__ uint64_t str_ref_hash(const DevPipe& P, uint64_t ref) {
   const uint8_t* p;
   int n;
   str_ref_at(P, ref, p, n);
-  uint64_t h = 0xcbf29ce484222325ull ^ (uint64_t)n;  // FNV-1a over the bytes, then a finaliser
-  for (int j = 0; j < n; ++j) h = (h ^ p[j]) * 0x100000001b3ull;
-  return fmix64(h);
+  return str_hash(p, n);
 }
 
 __device__ __forceinline__ bool str_ref_eq(const DevPipe& P, uint64_t a, uint64_t b) {
@@ -314,23 +338,93 @@ __device__ __forceinline__ bool str_ref_eq(const DevPipe& P, uint64_t a, uint64_
   return str_eq(pa, na, pb, nb);
 }
 
-// Hash tag of wide keys some of which are string references.
-__device__ __forceinline__ uint64_t key_tag_str(const DevPipe& P, const DevRes& R, const uint64_t* k) {
+constexpr int kStrCoopMin = 32;  // strings longer than this are hashed and compared by the whole warp
+
+__device__ __forceinline__ uint64_t warp_sum64(uint64_t v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// Hash of each active lane's string reference, called by every lane of the
+// warp (the reference's push-down string hash, include/hashing.cuh:39-62):
+// strings longer than kStrCoopMin bytes are hashed one after another by all
+// 32 lanes, a word per lane with coalesced reads, the shorter ones by their
+// own lane; every lane gets str_ref_hash's value (inactive lanes 0).
+__device__ __noinline__ uint64_t str_ref_hash_warp(const DevPipe& P, bool active, uint64_t ref) {
+  const uint8_t* p = nullptr;
+  int n = 0;
+  if (active) str_ref_at(P, ref, p, n);
+  const bool wide = active && n > kStrCoopMin;
+  uint64_t h = (active && !wide) ? str_hash(p, n) : 0ull;
+  const int lane = (int)(threadIdx.x & 31);
+  unsigned todo = __ballot_sync(kFull, wide);
+  while (todo) {
+    const int src = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const uint8_t* q = reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, (unsigned long long)p, src));
+    const int m = __shfl_sync(kFull, n, src);
+    uint64_t part = 0;
+    for (int i = lane; 8 * i < m; i += 32) part += str_word_term(str_word(q, m, i), i);
+    part = warp_sum64(part);
+    if (lane == src) h = str_hash_final(part, m);
+  }
+  return h;
+}
+
+// Equality of two active lanes' string references, called by every lane of
+// the warp (the reference's stringEqualsPushdown, include/util.cuh:104-130):
+// pairs of equal length longer than kStrCoopMin bytes are compared by all 32
+// lanes a byte each, the shorter ones by their own lane.
+__device__ __noinline__ bool str_ref_eq_warp(const DevPipe& P, bool active, uint64_t a, uint64_t b) {
+  const uint8_t *pa = nullptr, *pb = nullptr;
+  int na = 0, nb = 0;
+  if (active && a != b) {
+    str_ref_at(P, a, pa, na);
+    str_ref_at(P, b, pb, nb);
+  }
+  const bool wide = active && a != b && na == nb && na > kStrCoopMin;
+  bool eq = active && (a == b || (!wide && str_eq(pa, na, pb, nb)));
+  const int lane = (int)(threadIdx.x & 31);
+  unsigned todo = __ballot_sync(kFull, wide);
+  while (todo) {
+    const int src = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const uint8_t* x = reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, (unsigned long long)pa, src));
+    const uint8_t* y = reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, (unsigned long long)pb, src));
+    const int m = __shfl_sync(kFull, na, src);
+    bool same = true;
+    for (int j = lane; j < m; j += 32) same &= x[j] == y[j];
+    same = __all_sync(kFull, same);
+    if (lane == src) eq = same;
+  }
+  return eq;
+}
+
+// Hash tag of wide keys some of which are string references, given the
+// strings' hashes `sh` (entries of non-string keys unused).
+__device__ __forceinline__ uint64_t key_tag_strh(const DevRes& R, const uint64_t* k, const uint64_t* sh) {
   uint64_t h = 0x9e3779b97f4a7c15ull;
   for (int i = 0; i < R.nkeys; ++i) {
-    const uint64_t v = R.key_ctype[i] == DQ_STR ? str_ref_hash(P, k[i]) : k[i];
+    const uint64_t v = R.key_ctype[i] == DQ_STR ? sh[i] : k[i];
     h = fmix64(h ^ v) + 0x632be59bd9b4e019ull * (i + 1);
   }
   return fmix64(h) & 0x7fffffffffffffffull;
 }
 
+__device__ __forceinline__ uint64_t key_tag_str(const DevPipe& P, const DevRes& R, const uint64_t* k) {
+  uint64_t sh[DQ_MAX_KEYS];
+  for (int i = 0; i < R.nkeys; ++i) sh[i] = R.key_ctype[i] == DQ_STR ? str_ref_hash(P, k[i]) : 0ull;
+  return key_tag_strh(R, k, sh);
+}
+
 // Bucket of a multimap key some of whose values are string references: their
-// bytes' hashes stand in for them (bucket_of otherwise).
-__device__ __forceinline__ uint32_t bucket_of_str(const DevPipe& P, const DevRes& R, const uint64_t* k, int n,
-                                                  uint32_t cap) {
+// bytes' hashes `sh` stand in for them (bucket_of otherwise).
+__device__ __forceinline__ uint32_t bucket_of_strh(const DevRes& R, const uint64_t* k, const uint64_t* sh, int n,
+                                                   uint32_t cap) {
   uint64_t h = 0;
   for (int i = 0; i < n; ++i) {
-    const uint64_t v = R.key_ctype[i] == DQ_STR ? str_ref_hash(P, k[i]) : k[i];
+    const uint64_t v = R.key_ctype[i] == DQ_STR ? sh[i] : k[i];
     h = i == 0 ? v : (h ^ (h >> 29)) * 0xbf58476d1ce4e5b9ull + v;
   }
   return slot_of(h, cap);

@@ -284,11 +284,26 @@ struct Gen {
     else L("str_ref_at(P, " + V(s) + ", " + p + ", " + n + ");");
   }
 
-  // Bucket of a multimap key held in array kk.
-  std::string bucket(const dq_op& op, int r, const std::string& kk) {
+  // Bucket of a multimap key held in array kk (string keys: their hashes in sh).
+  std::string bucket(const dq_op& op, int r, const std::string& kk, const std::string& sh) {
     if (has_str_key(P.res[r]))
-      return "bucket_of_str(P, " + res(r) + ", " + kk + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap)";
+      return "bucket_of_strh(" + res(r) + ", " + kk + ", " + sh + ", " + num(op.nlist) + ", (uint32_t)" + res(r) +
+             ".cap)";
     return "bucket_of(" + kk + ", " + num(op.nlist) + ", (uint32_t)" + res(r) + ".cap)";
+  }
+
+  // Hashes of the string values among a key list, computed by the whole warp
+  // where its lanes have not branched (long strings cooperatively, a word per
+  // lane); the array's other entries stay 0.  Empty when resource r has no
+  // string keys.
+  std::string str_key_hashes(int r, int list, int n, const std::string& act) {
+    if (!has_str_key(P.res[r])) return std::string();
+    const std::string h = fresh("sh");
+    L("uint64_t " + h + "[" + num(std::max(n, 1)) + "] = {};");
+    for (int i = 0; i < n; ++i)
+      if (P.res[r].key_ctype[i] == DQ_STR)
+        L(h + "[" + num(i) + "] = str_ref_hash_warp(P, " + act + ", " + V(P.lists[list + i]) + ");");
+    return h;
   }
 
   // Equality of a probe key slot and a build key slot of resource r's key q.
@@ -521,6 +536,7 @@ struct Gen {
     const int r = op.res;
     const DevRes& R = P.res[r];
     std::string s = fresh("ps");
+    const std::string sh = str_key_hashes(r, op.list, op.nlist, act);
     L("int64_t " + s + " = -1;");
     L("if (" + act + ") {");
     ++ind;
@@ -643,7 +659,7 @@ struct Gen {
     } else {
       std::string k = keys(op, r, op.list, op.nlist);
       if (has_str_key(R))
-        L(s + " = unique_find_str(P, " + res(r) + ", key_tag_str(P, " + res(r) + ", " + k + "), " + k + ");");
+        L(s + " = unique_find_str(P, " + res(r) + ", key_tag_strh(" + res(r) + ", " + k + ", " + sh + "), " + k + ");");
       else
         L(s + " = unique_find(" + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
     }
@@ -739,8 +755,13 @@ struct Gen {
   void match_ops(int k, int lv, const std::string& a, const std::string& exit) {
     const dq_op& op = P.ops[k];
     declare_regs(lv);
-    for (int q = 0; q < op.nlist; ++q)
-      L(a + " = " + a + " && " + key_eq(op.res, q, P.lists[op.list + q], P.lists[op.list2 + q]) + ";");
+    for (int q = 0; q < op.nlist; ++q) {
+      const int x = P.lists[op.list + q], y = P.lists[op.list2 + q];
+      if (P.res[op.res].key_ctype[q] == DQ_STR)  // long strings compared by the whole warp
+        L(a + " = str_ref_eq_warp(P, " + a + ", " + V(x) + ", " + V(y) + ");");
+      else
+        L(a + " = " + a + " && " + key_eq(op.res, q, x, y) + ";");
+    }
     skip_if_idle(a, exit);
     ops_from(k + 1, lv, a, exit);
   }
@@ -756,11 +777,12 @@ struct Gen {
     const int lv = level + 1;
     const std::string id = num(uid++);
     const std::string fm = "xf" + id, m = "xm" + id, me = "xe" + id;
+    const std::string sh = str_key_hashes(r, op.list, op.nlist, act);
     L("bool " + fm + " = false;");
     L("if (" + act + ") {");
     ++ind;
     std::string kk = keys(op, r, op.list, op.nlist);
-    L("const uint32_t b_ = " + bucket(op, r, kk) + ";");
+    L("const uint32_t b_ = " + bucket(op, r, kk, sh) + ";");
     L("const uint32_t xc_ = " + res(r) + ".counts[b_];");
     L("uint32_t " + m + " = xc_ ? " + res(r) + ".offsets[b_] : 0u;");
     L("const uint32_t " + me + " = " + m + " + xc_;");
@@ -795,11 +817,12 @@ struct Gen {
                       q = "eq" + id, sl = "es" + id, m = "em" + id, a = "ea" + id;
     L("{");
     ++ind;
+    const std::string sh = str_key_hashes(r, op.list, op.nlist, act);
     L("uint32_t " + eo + " = 0u, " + ec + " = 0u;");
     L("if (" + act + ") {");
     ++ind;
     std::string kk = keys(op, r, op.list, op.nlist);
-    L("const uint32_t b_ = " + bucket(op, r, kk) + ";");
+    L("const uint32_t b_ = " + bucket(op, r, kk, sh) + ";");
     L(ec + " = " + res(r) + ".counts[b_];");
     L(eo + " = " + ec + " ? " + res(r) + ".offsets[b_] : 0u;");
     --ind;
@@ -919,11 +942,12 @@ struct Gen {
       L("}");
       return;
     }
+    const std::string sh = str_key_hashes(r, op.list, op.nlist, act);
     L("if (" + act + ") {");
     ++ind;
     std::string k = keys(op, r, op.list, op.nlist);
     if (R.packed) L("const uint64_t tag_ = " + packed_tag(r, op.list, op.nlist) + ";");
-    else if (has_str_key(R)) L("const uint64_t tag_ = key_tag_str(P, " + res(r) + ", " + k + ");");
+    else if (has_str_key(R)) L("const uint64_t tag_ = key_tag_strh(" + res(r) + ", " + k + ", " + sh + ");");
     else L("const uint64_t tag_ = key_tag(" + res(r) + ", " + k + ");");
     auto global = [&]() {
       if (R.packed) {
@@ -967,6 +991,7 @@ struct Gen {
   void sink_build(const dq_op& op, const std::string& act) {
     const int r = op.res;
     const DevRes& R = P.res[r];
+    const std::string sh = str_key_hashes(r, op.list, op.nlist, act);
     L("if (" + act + ") {");
     ++ind;
     if (R.compact) {
@@ -979,7 +1004,8 @@ struct Gen {
     }
     std::string k = keys(op, r, op.list, op.nlist);
     if (has_str_key(R))
-      L("const int64_t s_ = unique_insert_str(P, " + res(r) + ", key_tag_str(P, " + res(r) + ", " + k + "), " + k + ");");
+      L("const int64_t s_ = unique_insert_str(P, " + res(r) + ", key_tag_strh(" + res(r) + ", " + k + ", " + sh + "), " + k +
+        ");");
     else
       L("const int64_t s_ = unique_insert(P, " + res(r) + ", key_tag(" + res(r) + ", " + k + "), " + k + ");");
     if (op.nlist2 > 0) {
@@ -1000,11 +1026,12 @@ struct Gen {
     // size, the others their rank within the group
     const int r = op.res;
     const DevRes& R = P.res[r];
+    const std::string sh = str_key_hashes(r, op.list, op.nlist, act);
     L("uint32_t b_ = 0xffffffffu;");
     L("if (" + act + ") {");
     ++ind;
     std::string k = keys(op, r, op.list, op.nlist);
-    L("b_ = " + bucket(op, r, k) + ";");
+    L("b_ = " + bucket(op, r, k, sh) + ";");
     --ind;
     L("}");
     L("const unsigned peers_ = __match_any_sync(kFull, b_);");

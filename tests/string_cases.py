@@ -2,7 +2,8 @@
 cases: empty, one-byte and 286-byte strings, substring windows that start
 before the string, end past it, lie wholly past it or have no length, nested
 substrings, equality of two string columns, of a scanned string and one a join
-carries, and a substring of a joined string as a group key."""
+carries, and a substring of a joined string as a group key; long strings (up
+to 300 bytes, hashed and compared by whole warps) as group and join keys."""
 import numpy as np
 
 import dogqc_b200.scalar as scal
@@ -77,4 +78,44 @@ def like_joined_plan(db):
         sel = alg.selection(scal.LikeExpr(scal.AttrExpr("s"), scal.ConstExpr("%l%o%", Type.STRING)), j)
         agg = alg.aggregation(["ds"], [(Reduction.COUNT, "", "cnt")], sel)
         return agg, {j.opId: {"multimatch": True}, sel.opId: {"selectivity": 0.2}, agg.opId: {"numgroups": 16}}
+    return _resolve(db, build)
+
+
+def long_db(n=4000, distinct=60, seed=11):
+    """Strings of 0 to 300 bytes (``distinct`` of them, many sharing long
+    prefixes) as keys: a fact table naming them, a dimension with each once
+    and a multimap side with each one to three times."""
+    r = np.random.Generator(np.random.Philox(seed))
+    base = bytes(range(33, 127)) * 4
+    words = [base[:int(x)] + b"#%d" % i for i, x in enumerate(r.integers(0, 297, distinct))]
+    words[0] = b""
+    f = {"fk": StringColumn.from_list([words[i] for i in r.integers(0, distinct, n)]),
+         "fv": r.integers(0, 1000, n, dtype=np.int32)}
+    dim = {"dk": StringColumn.from_list(words[1:]), "dv": np.arange(1, distinct, dtype=np.int32)}
+    reps = r.integers(1, 4, distinct)
+    mm = {"mk": StringColumn.from_list([w for w, k in zip(words, reps) for _ in range(k)]),
+          "mv": np.arange(int(reps.sum()), dtype=np.int32)}
+    return Database([Table("f", f, {"fk": Type.STRING, "fv": Type.INT}),
+                     Table("dim", dim, {"dk": Type.STRING, "dv": Type.INT}),
+                     Table("mm", mm, {"mk": Type.STRING, "mv": Type.INT})])
+
+
+def long_key_plan(db, kind):
+    """``group``: count and sum per long string; ``unique`` / ``multi``: the
+    fact rows joined to the dimension / multimap by the long string;
+    ``semi`` / ``anti``: the fact rows whose string the dimension holds (not)."""
+    def build(alg):
+        if kind == "group":
+            agg = alg.aggregation(["fk"], [(Reduction.COUNT, "", "c"), (Reduction.SUM, "fv", "s")], alg.scan("f"))
+            return agg, {agg.opId: {"numgroups": 64}}
+        if kind in ("unique", "multi"):
+            build_side, key = ("dim", "dk") if kind == "unique" else ("mm", "mk")
+            j = alg.join((key, "fk"), alg.scan(build_side), alg.scan("f"))
+            agg = alg.aggregation(["dv" if kind == "unique" else "mv"], [(Reduction.COUNT, "", "c"),
+                                                                         (Reduction.SUM, "fv", "s")], j)
+            return agg, {j.opId: {"multimatch": kind == "multi"}, agg.opId: {"numgroups": 256}}
+        make = alg.semijoin if kind == "semi" else alg.antijoin
+        j = make(("dk", "fk"), None, alg.scan("dim"), alg.scan("f"))
+        agg = alg.aggregation(["fk"], [(Reduction.COUNT, "", "c")], j)
+        return agg, {agg.opId: {"numgroups": 64}}
     return _resolve(db, build)

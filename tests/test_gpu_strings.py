@@ -83,6 +83,16 @@ def test_string_comparisons_through_joins_match_oracle(engine, make):
     assert canonical_rows(run(engine, db, plan).rows()) == canonical_rows(run_plan(db, plan)[1])
 
 
+@pytest.mark.parametrize("kind", ["group", "unique", "multi", "semi", "anti"])
+def test_long_string_keys_match_oracle(engine, kind):
+    """Keys of up to 300 bytes: hashed (and, after a multimatch expansion,
+    compared) by whole warps, a word or a byte per lane, giving the values a
+    lane computes alone for the short ones."""
+    db = string_cases.long_db()
+    plan = string_cases.long_key_plan(db, kind)
+    assert canonical_rows(run(engine, db, plan).rows()) == canonical_rows(run_plan(db, plan)[1])
+
+
 @pytest.mark.parametrize("pattern", ["%ABCDEFGHIJKLMNOP%", "xxxxxxxxxxxxxxxxxxxx%", "%JKLMNOPQRSTUVWXYZABC%",
                                      "hello world%"])
 def test_long_like_patterns_match_oracle(engine, pattern):

@@ -92,3 +92,11 @@ def test_cpu_evaluator_string_join_keys_match_oracle(variant):
     import cpu_eval
     db, alg, plan = make_case({"workload": "c15", "scale": 0.02, "plan_kw": {"variant": variant}})
     assert canonical_rows(cpu_eval.Prepared(db, plan, 4).run()[1]) == canonical_rows(run_plan(db, plan)[1])
+
+
+@pytest.mark.parametrize("kind", ["group", "unique", "multi", "semi", "anti"])
+def test_cpu_evaluator_long_string_keys_match_oracle(kind):
+    import cpu_eval
+    db = string_cases.long_db()
+    plan = string_cases.long_key_plan(db, kind)
+    assert canonical_rows(cpu_eval.Prepared(db, plan, 3).run()[1]) == canonical_rows(run_plan(db, plan)[1])
