@@ -9,8 +9,8 @@ namespace dq {
 
 constexpr int kThreads = 256;          // pipeline kernel block size
 constexpr int kMaxStages = 4;          // tile staging depth
-constexpr int kMaxRes = 8;             // resources one pipeline touches
-constexpr int kMaxStr = 4;             // string columns per pipeline
+constexpr int kMaxRes = 16;            // resources of a plan (every pipeline sees them all)
+constexpr int kMaxStr = 8;             // string columns per pipeline
 constexpr int kMaxStash = 24;          // values carried by one heavy work item
 constexpr uint64_t kEmpty = ~0ull;     // empty tag of every hash table
 

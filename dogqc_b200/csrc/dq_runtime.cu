@@ -639,7 +639,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   P.profile = plan->profile;
 
   // resources: the pipeline sees the plan's resources under the same indices
-  if (plan->res.size() > (size_t)kMaxRes) throw DqError(DQ_ERR_UNSUPPORTED, "more than 8 resources in a plan");
+  if (plan->res.size() > (size_t)kMaxRes) throw DqError(DQ_ERR_UNSUPPORTED, "more than " + std::to_string(kMaxRes) + " resources in a plan");
   P.nres = (int)plan->res.size();
   for (size_t i = 0; i < plan->res.size(); ++i) P.res[i] = plan->res[i]->dev;
 

@@ -757,12 +757,168 @@ def plan_c16(alg, scal, Type, Reduction):
     return agg, cfg
 
 
+# ------------------------------------------------------- c17 .. c19 -------------
+# TPC-H Q13, Q20 and Q2 over one TPC-H-like schema with its strings (names,
+# addresses, phone numbers, comments, part names and types).
+
+TPCH_REGIONS = [b"AFRICA", b"AMERICA", b"ASIA", b"EUROPE", b"MIDDLE EAST"]
+TPCH_COLORS = [b"almond", b"antique", b"aquamarine", b"azure", b"beige", b"bisque", b"black", b"blanched",
+               b"blue", b"blush", b"brown", b"burlywood", b"chartreuse", b"chiffon", b"chocolate", b"coral",
+               b"cornflower", b"cornsilk", b"cream", b"cyan", b"dark", b"deep", b"dim", b"dodger", b"drab",
+               b"firebrick", b"floral", b"forest", b"frosted", b"gainsboro", b"ghost", b"goldenrod", b"green",
+               b"grey", b"honeydew", b"hot", b"indian", b"ivory", b"khaki", b"lace", b"lavender", b"lawn",
+               b"lemon", b"light", b"lime", b"linen", b"magenta", b"maroon", b"medium", b"metallic"]
+ALNUM = np.frombuffer(b"abcdefghijklmnopqrstuvwxyzABCDEFGHIJKLMNOPQRSTUVWXYZ0123456789 ,.", dtype=np.uint8)
+
+
+def _text(r, n, lo, hi):
+    """n strings of lo..hi random characters (addresses)."""
+    lens = r.integers(lo, hi + 1, n)
+    chars = ALNUM[r.integers(0, len(ALNUM), int(lens.sum()))]
+    offsets = np.zeros(n + 1, dtype=np.uint64)
+    np.cumsum(lens, out=offsets[1:])
+    return StringColumn(chars, offsets, 0)
+
+
+def gen_tpch(scale=1.0, seed=BASE_SEED + 17):
+    """TPC-H-like tables at scale factor ``scale`` (lineitem 6,000,000 rows at
+    1.0): region, nation, supplier, customer, part, partsupp (four suppliers a
+    part), orders (a third of the customers have none; 1% of the comments hold
+    "special ... requests") and lineitem (lines of the partsupp pairs)."""
+    ns = _n(10_000, scale, 16)
+    nc = _n(150_000, scale, 16)
+    np_ = _n(200_000, scale, 16)
+    no = _n(1_500_000, scale, 16)
+    nl = _n(6_000_000, scale, 64)
+    r = _rng(seed)
+    region = {"r_regionkey": np.arange(5, dtype=np.int32), "r_name": StringColumn.from_list(TPCH_REGIONS)}
+    nation = {"n_nationkey": np.arange(25, dtype=np.int32), "n_name": StringColumn.from_list(C15_NATIONS),
+              "n_regionkey": (np.arange(25) % 5).astype(np.int32)}
+    supplier = {"s_suppkey": np.arange(1, ns + 1, dtype=np.int32),
+                "s_name": StringColumn.from_list([b"Supplier#%09d" % (i + 1) for i in range(ns)]),
+                "s_address": _text(r, ns, 10, 40),
+                "s_nationkey": r.integers(0, 25, ns, dtype=np.int32),
+                "s_phone": StringColumn.from_list([b"%02d-%03d-%03d-%04d" % (10 + a, b, c, d) for a, b, c, d in
+                                                   r.integers(0, [25, 1000, 1000, 10000], (ns, 4))]),
+                "s_acctbal": r.integers(0, 1_100_000, ns, dtype=np.int64).astype(np.uint64),
+                "s_comment": _comments(r, ns)}
+    customer = {"c_custkey": np.arange(1, nc + 1, dtype=np.int32)}
+    names = r.integers(0, len(TPCH_COLORS), (np_, 5))
+    t = r.integers(0, [len(C14_TYPE1), len(C14_TYPE2), len(C14_TYPE3)], (np_, 3))
+    part = {"p_partkey": np.arange(1, np_ + 1, dtype=np.int32),
+            "p_name": StringColumn.from_list([b" ".join(TPCH_COLORS[j] for j in row) for row in names]),
+            "p_mfgr": StringColumn.from_list([b"Manufacturer#%d" % m for m in r.integers(1, 6, np_)]),
+            "p_type": StringColumn.from_list([b" ".join((C14_TYPE1[a], C14_TYPE2[b], C14_TYPE3[c])) for a, b, c in t]),
+            "p_size": r.integers(1, 51, np_, dtype=np.int32)}
+    pk = np.repeat(np.arange(1, np_ + 1, dtype=np.int64), 4)
+    i = np.tile(np.arange(4, dtype=np.int64), np_)
+    partsupp = {"ps_partkey": pk.astype(np.int32),
+                "ps_suppkey": ((pk + i * (ns // 4 + (pk - 1) // ns)) % ns + 1).astype(np.int32),
+                "ps_availqty": r.integers(1, 10_000, 4 * np_, dtype=np.int32),
+                "ps_supplycost": r.integers(100, 100_001, 4 * np_, dtype=np.int64).astype(np.uint64)}
+    with_orders = np.arange(1, nc + 1, dtype=np.int32)
+    with_orders = with_orders[with_orders % 3 != 0]
+    orders = {"o_orderkey": np.arange(1, no + 1, dtype=np.int32),
+              "o_custkey": with_orders[r.integers(0, len(with_orders), no)],
+              "o_comment": _comments(r, no, (b"special", b"requests"), 0.01)}
+    ps = r.integers(0, 4 * np_, nl)
+    lineitem = {"l_partkey": partsupp["ps_partkey"][ps], "l_suppkey": partsupp["ps_suppkey"][ps],
+                "l_quantity": r.integers(1, 51, nl, dtype=np.int32),
+                "l_shipdate": (EPOCH_1992 + r.integers(0, DATE_RANGE, nl)).astype(np.int32)}
+    I, S, F, D = Type.INT, Type.STRING, Type.FLOAT, Type.DATE
+    return Database([
+        Table("region", region, {"r_regionkey": I, "r_name": S}),
+        Table("nation", nation, {"n_nationkey": I, "n_name": S, "n_regionkey": I}),
+        Table("supplier", supplier, {"s_suppkey": I, "s_name": S, "s_address": S, "s_nationkey": I, "s_phone": S,
+                                     "s_acctbal": F, "s_comment": S}),
+        Table("customer", customer, {"c_custkey": I}),
+        Table("part", part, {"p_partkey": I, "p_name": S, "p_mfgr": S, "p_type": S, "p_size": I}),
+        Table("partsupp", partsupp, {"ps_partkey": I, "ps_suppkey": I, "ps_availqty": I, "ps_supplycost": F}),
+        Table("orders", orders, {"o_orderkey": I, "o_custkey": I, "o_comment": S}),
+        Table("lineitem", lineitem, {"l_partkey": I, "l_suppkey": I, "l_quantity": I, "l_shipdate": I})])
+
+
+def plan_c17(alg, scal, Type, Reduction, numgroups=150_000):
+    """TPC-H Q13: customers left outer join their orders whose comment does
+    not mention special requests (NOT LIKE '%special%requests%' on
+    variable-length comments), orders per customer, then customers per order
+    count."""
+    ords = alg.selection(scal.NotExpr(scal.LikeExpr(scal.AttrExpr("o_comment"),
+                                                    scal.ConstExpr("%special%requests%", Type.STRING))),
+                         alg.scan("orders"))
+    j = alg.outerjoin([("c_custkey", "o_custkey")], None, ords, alg.scan("customer"))
+    per = alg.aggregation(["c_custkey"], [(Reduction.COUNT, "o_orderkey", "c_count")], j)
+    dist = alg.aggregation(["c_count"], [(Reduction.COUNT, "", "custdist")], per)
+    return dist, {ords.opId: {"selectivity": 0.99}, j.opId: {"multimatch": True},
+                  per.opId: {"numgroups": numgroups}, dist.opId: {"numgroups": 64}}
+
+
+def plan_c18(alg, scal, Type, Reduction, start=EPOCH_1992 + 731, nation="CANADA", prefix="forest%"):
+    """TPC-H Q20: suppliers of one nation (n_name = constant, joined by key)
+    holding a part whose name starts with a word (LIKE 'forest%') in excess:
+    twice the available quantity above the quantity the supplier shipped of
+    that part in one year (a unique table keyed by two attributes, built from
+    an aggregation); their names and addresses."""
+    forest = alg.selection(scal.LikeExpr(scal.AttrExpr("p_name"), scal.ConstExpr(prefix, Type.STRING)),
+                           alg.scan("part"))
+    ps = alg.semijoin(("ps_partkey", "p_partkey"), None, forest, alg.scan("partsupp"))
+    year = alg.selection(scal.AndExpr(
+        scal.LargerEqualExpr(scal.AttrExpr("l_shipdate"), scal.ConstExpr(str(start), Type.DATE)),
+        scal.SmallerExpr(scal.AttrExpr("l_shipdate"), scal.ConstExpr(str(start + 365), Type.DATE))),
+        alg.scan("lineitem"))
+    shipped = alg.aggregation(["l_partkey", "l_suppkey"], [(Reduction.SUM, "l_quantity", "sum_qty")], year)
+    j = alg.join([("l_partkey", "ps_partkey"), ("l_suppkey", "ps_suppkey")], shipped, ps)
+    excess = alg.selection(scal.LargerExpr(scal.MulExpr(scal.ConstExpr("2", Type.INT), scal.AttrExpr("ps_availqty")),
+                                           scal.AttrExpr("sum_qty")), j)
+    nat = alg.selection(scal.EqualsExpr(scal.AttrExpr("n_name"), scal.ConstExpr(nation, Type.STRING)),
+                        alg.scan("nation"))
+    supp = alg.join(("s_nationkey", "n_nationkey"), nat, alg.scan("supplier"))
+    semi = alg.semijoin(("s_suppkey", "ps_suppkey"), None, excess, supp)
+    proj = alg.projection(["s_name", "s_address"], semi)
+    cfg = {forest.opId: {"selectivity": 0.1}, year.opId: {"selectivity": 0.15},
+           shipped.opId: {"numgroups": 800_000}, j.opId: {"multimatch": False, "selectivity": 0.08},
+           excess.opId: {"selectivity": 0.5}, nat.opId: {"selectivity": 0.04}, supp.opId: {"multimatch": False}}
+    return proj, cfg
+
+
+def plan_c19(alg, scal, Type, Reduction, region="EUROPE", size=15, suffix="%BRASS"):
+    """TPC-H Q2: the parts of one size and type suffix (LIKE '%BRASS') with
+    the supplier of one region (r_name = constant) offering the minimum supply
+    cost (an aggregation's MIN joined back, equality of two attributes), with
+    the supplier's and nation's strings in the result."""
+    def europe(sup_alias):
+        reg = alg.selection(scal.EqualsExpr(scal.AttrExpr("r_name"), scal.ConstExpr(region, Type.STRING)),
+                            alg.scan("region"))
+        nat = alg.join(("r_regionkey", "n_regionkey"), reg, alg.scan("nation"))
+        return alg.join(("s_nationkey", "n_nationkey"), nat, alg.scan("supplier", sup_alias))
+
+    def parts(alias):
+        pref = (alias + ".") if alias else ""
+        return alg.selection(scal.AndExpr(
+            scal.LikeExpr(scal.AttrExpr(pref + "p_type"), scal.ConstExpr(suffix, Type.STRING)),
+            scal.EqualsExpr(scal.AttrExpr(pref + "p_size"), scal.ConstExpr(str(size), Type.INT))),
+            alg.scan("part", alias) if alias else alg.scan("part"))
+
+    early = alg.semijoin(("ps_partkey", "earlyp.p_partkey"), None, parts("earlyp"), alg.scan("partsupp", "ps1"))
+    cost = alg.join(("s_suppkey", "ps_suppkey"), europe(None), early)
+    mins = alg.aggregation(["ps_partkey"], [(Reduction.MIN, "ps_supplycost", "min_supplycost")], cost)
+    withp = alg.join(("p_partkey", "ps_partkey"), mins, parts(None))
+    best = alg.join([("ps2.ps_partkey", "ps1.ps_partkey")], withp, alg.scan("partsupp", "ps2"))
+    best = alg.selection(scal.EqualsExpr(scal.AttrExpr("min_supplycost"), scal.AttrExpr("ps2.ps_supplycost")), best)
+    out = alg.join(("s2.s_suppkey", "ps2.ps_suppkey"), europe("s2"), best)
+    proj = alg.projection(["s_acctbal", "s_name", "n_name", "p_partkey", "p_mfgr", "s_address", "s_phone",
+                           "s_comment"], out)
+    return proj, {mins.opId: {"numgroups": 4_000}}
+
+
 GENERATORS = {"c0": gen_c0, "c1": gen_c1, "c2": gen_c2, "c3": gen_c3, "c5": gen_c5, "c7": gen_c5, "c8": gen_c5,
               "c9": gen_c9, "c9p": gen_c9, "c10": gen_c10, "c10p": gen_c10, "c11": gen_c11, "c12": gen_c11,
-              "c13": gen_c5, "c14": gen_c14, "c15": gen_c15, "c16": gen_c16}
+              "c13": gen_c5, "c14": gen_c14, "c15": gen_c15, "c16": gen_c16, "c17": gen_tpch, "c18": gen_tpch,
+              "c19": gen_tpch}
 PLANS = {"c0": plan_c0, "c1": plan_c1, "c2": plan_c2, "c3": plan_c3, "c5": plan_c5, "c7": plan_c7,
          "c8": plan_c8, "c9": plan_c9, "c9p": plan_c9p, "c10": plan_c10, "c10p": plan_c10p, "c11": plan_c11,
-         "c12": plan_c12, "c13": plan_c13, "c14": plan_c14, "c15": plan_c15, "c16": plan_c16}
+         "c12": plan_c12, "c13": plan_c13, "c14": plan_c14, "c15": plan_c15, "c16": plan_c16, "c17": plan_c17,
+         "c18": plan_c18, "c19": plan_c19}
 
 
 def build(name, alg, scale=1.0, **kw):

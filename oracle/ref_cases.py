@@ -64,6 +64,16 @@ CASES = {
     "c15_m": dict(workload="c15", scale=1.0, plan_kw=dict(variant="multi")),
     "c16_s": dict(workload="c16", scale=0.05, str_cols=[0]),
     "c16": dict(workload="c16", scale=1.0, str_cols=[0]),
+    # TPC-H Q13 (NOT LIKE on variable-length comments under an outer join),
+    # Q20 (LIKE prefix, string equality on the nation, a two-attribute unique
+    # table built from an aggregation, string results) and Q2 (LIKE suffix,
+    # MIN joined back, eight result columns of which six are strings)
+    "c17_s": dict(workload="c17", scale=0.01),
+    "c17": dict(workload="c17", scale=1.0),
+    "c18_s": dict(workload="c18", scale=0.05, str_cols=[0, 1]),
+    "c18": dict(workload="c18", scale=1.0, str_cols=[0, 1]),
+    "c19_s": dict(workload="c19", scale=0.05, str_cols=[1, 2, 4, 5, 6, 7]),
+    "c19": dict(workload="c19", scale=1.0, str_cols=[1, 2, 4, 5, 6, 7]),
     # full sizes: row counts, checksums and (small) full results are committed
     "c0": dict(workload="c0", scale=1.0),
     "c1": dict(workload="c1", scale=1.0),

@@ -9,7 +9,7 @@ from canonical import canonical_checksum
 from helpers import golden, golden_cases, make_case, reference_rows, result_checksum
 
 SMALL = [c for c in golden_cases() if golden(c)["spec"]["scale"] < 0.1]
-FULL = ["c0", "c1", "c5", "c7", "c8", "c11", "c13", "c14", "c15_m", "c16"]
+FULL = ["c0", "c1", "c5", "c7", "c8", "c11", "c13", "c14", "c15_m", "c16", "c17", "c18", "c19"]
 
 
 def _run(case, threads):

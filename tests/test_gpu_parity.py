@@ -16,7 +16,7 @@ from helpers import golden, golden_cases, make_case, reference_rows, result_chec
 pytestmark = pytest.mark.gpu
 
 SMALL = [c for c in golden_cases() if golden(c)["spec"]["scale"] < 0.1]
-FULL = ["c0", "c1", "c2", "c3", "c5", "c7", "c8", "c11", "c12", "c13", "c14", "c15_m", "c16"]
+FULL = ["c0", "c1", "c2", "c3", "c5", "c7", "c8", "c11", "c12", "c13", "c14", "c15_m", "c16", "c17", "c18", "c19"]
 
 
 @pytest.fixture(scope="module")

@@ -45,7 +45,7 @@ def check_sources(plan, max_spill=0):
 
 
 @pytest.mark.parametrize("name", ["c0", "c1", "c2", "c3", "c5", "c7", "c8", "c9", "c9p", "c10", "c10p", "c14", "c15",
-                                  "c16"])
+                                  "c16", "c17", "c18", "c19"])
 def test_every_workload_compiles_offline(engine, name):
     plan = engine.prepare(resolved(engine, name))
     check_sources(plan)

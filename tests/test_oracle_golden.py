@@ -12,7 +12,7 @@ from evaluator import run_plan
 from helpers import golden, golden_cases, make_case, reference_rows, result_checksum
 
 SMALL = [c for c in golden_cases() if golden(c)["spec"]["scale"] < 0.1]
-FULL_FAST = ["c0", "c1", "c5", "c7", "c8", "c11", "c12", "c13", "c14", "c16"]
+FULL_FAST = ["c0", "c1", "c5", "c7", "c8", "c11", "c12", "c13", "c14", "c16", "c18", "c19"]
 
 
 @pytest.mark.parametrize("case", SMALL)
