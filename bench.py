@@ -233,20 +233,37 @@ def run_ours(args, world, rank, local):
     rows_per_step = input_rows(db)
     engine = Engine(local, tile_rows=args.tile_rows, ctas_per_sm=args.ctas_per_sm, flags=args.engine_flags)
     engine.register_database(db)
-    p = engine.prepare(plan)
-    npipes = len(p.lowering.pipes)
     # L2 flush between steps: write 256 MB (evicts the inputs), then read another
     # 256 MB, which writes the dirty flush lines back before the timed region
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     evict = torch.zeros(32 << 20, dtype=torch.int64, device="cuda")
+
+    def flush_l2():
+        flush.fill_(1)
+        evict.sum()
+
+    # the plan's launch shapes and table sizing, picked by measurement on this
+    # GPU (each candidate run after an L2 flush) before anything is timed
+    tuning, tuned = None, None
+    if args.tuning:
+        tuning = json.loads(args.tuning)
+        tuned = {"tuning": tuning, "given": True}
+    elif not args.no_autotune:
+        from dogqc_b200 import autotune
+        from dogqc_b200.lowering import Lowering
+        t0 = time.perf_counter()
+        tuning, t_best, log = autotune.tune_plan(engine, Lowering(plan), reps=5, between=flush_l2)
+        tuned = {"tuning": tuning, "candidates": len(log), "best_ms": t_best * 1e3 if t_best else None,
+                 "search_s": round(time.perf_counter() - t0, 1)}
+    p = engine.prepare(plan, tuning=tuning)
+    npipes = len(p.lowering.pipes)
 
     def timed(plan_, steps):
         """Warm-up, then `steps` executions each after an L2 flush: summed
         device time of the runs (CUDA events on the engine's stream), summed
         per-pipeline times (zero where the run replayed a graph), launches."""
         def step():
-            flush.fill_(1)
-            evict.sum()
+            flush_l2()
             torch.cuda.synchronize()
             res_ = plan_.execute()
             return res_, plan_.timing()
@@ -255,11 +272,11 @@ def run_ours(args, world, rank, local):
         dist_barrier(world)
         torch.cuda.synchronize()
         tot, launches_ = 0.0, 0
-        pipes = [0.0] * npipes
+        pipes = [0.0] * len(plan_.lowering.pipes)
         for _ in range(steps):
             res_, t = step()
             tot += t["total_ms"]
-            for i in range(npipes):
+            for i in range(len(pipes)):
                 pipes[i] += t["pipeline_ms"][i]
             launches_ += t["kernel_launches"]
         torch.cuda.synchronize()
@@ -274,12 +291,27 @@ def run_ours(args, world, rank, local):
     # second context that does not capture graphs, over as many steps
     kengine = Engine(local, tile_rows=args.tile_rows, ctas_per_sm=args.ctas_per_sm, flags=args.engine_flags | 2)
     kengine.register_database(db)
-    kp = kengine.prepare(plan)
+    kp = kengine.prepare(plan, tuning=tuning)
     _, k_total_ms, pipe_ms, _ = timed(kp, args.steps)
     kp.free()
-    kengine.close()
     dom = max(range(npipes), key=lambda i: pipe_ms[i])   # the dominant pipeline kernel
     probe_ms = pipe_ms[dom]
+    # the same launch's streaming bound: one generated kernel that reads the
+    # dominant pipeline's columns (same table, same bytes) and only sums them
+    stream_ms = None
+    dp = p.lowering.pipes[dom]
+    if dp.table and not args.no_stream_bound:
+        from dogqc_b200.database import StringColumn
+        from dogqc_b200.relational import RelationalAlgebra, Reduction
+        cols = [c for c in dp.cols if not isinstance(db.tables[dp.table].columns[c], StringColumn)]
+        if cols:
+            salg = RelationalAlgebra(db)
+            sagg = salg.aggregation([], [(Reduction.SUM, c, "sum_%d" % i) for i, c in enumerate(cols)], salg.scan(dp.table))
+            sp = kengine.prepare(salg.resolveAlgebraPlan(sagg, {}))
+            _, _, s_pipe_ms, _ = timed(sp, args.steps)
+            sp.free()
+            stream_ms = s_pipe_ms[0] / args.steps
+    kengine.close()
     fact_bytes = pipeline_bytes(db, p.lowering, dom)
     ms_per_step = total_ms / args.steps
     value = rows_per_step * world / (ms_per_step / 1e3)
@@ -347,7 +379,11 @@ def run_ours(args, world, rank, local):
                      "frac": achieved / peak, "traffic": load_profile_traffic(),
                      "kernel": kernel,
                      "algorithmic_bytes": fact_bytes, "avg_ms": probe_avg_s * 1e3,
-                     "peak_source": "%s hbm_gbs (burst copy)" % peak_kind},
+                     "peak_source": "%s hbm_gbs (burst copy)" % peak_kind,
+                     "stream_ms": stream_ms,
+                     "frac_of_stream": stream_ms / (probe_avg_s * 1e3) if stream_ms else None,
+                     "stream_source": "one generated kernel summing the same columns of the same table "
+                                      "(the kernel's reads without its probes, groups or refill)"},
         "plan": {"algorithmic_bytes": plan_bytes, "avg_ms": ms_per_step,
                  "frac": plan_bytes / (ms_per_step / 1e3) / 1e9 / peak,
                  "replayed_graph": True,
@@ -355,6 +391,7 @@ def run_ours(args, world, rank, local):
                  "pipeline_ms": [x / args.steps for x in pipe_ms],
                  "pipeline_ms_source": "second timed loop without graph replay (events between launches)"},
         "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "autotune": tuned,
         "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
@@ -857,6 +894,10 @@ def main():
                          "the other configurations, for the per-pipeline table; c2x256: the batched form; "
                          "c4: the served mixed stream")
     ap.add_argument("--autotune", action="store_true", help="c2x256: pick the batch's tuning by measurement")
+    ap.add_argument("--no-stream-bound", action="store_true", help="skip timing the dominant kernel's stream bound")
+    ap.add_argument("--tuning", default="", help='plain workloads: a dq_tuning as JSON, e.g. {"rows_per_thread": 2}')
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="plain workloads: time the plan with the default launch shapes instead of tuning it first")
     ap.add_argument("--slots", type=int, default=4, help="c4: launches in flight on the device (streams)")
     ap.add_argument("--batch-max", type=int, default=0,
                     help="c4: requests of one shape per launch (0: 16; 1: every request alone)")

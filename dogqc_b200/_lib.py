@@ -108,7 +108,7 @@ class dq_plan_timing(C.Structure):
 class dq_tuning(C.Structure):
     _fields_ = [("rows_per_thread", C.c_int32), ("block_threads", C.c_int32), ("refill", C.c_int32),
                 ("unique_slots_pct", C.c_int32), ("multi_buckets_pct", C.c_int32), ("refill_threshold", C.c_int32),
-                ("defer_threshold", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("defer_threshold", C.c_int32), ("ctas_per_sm", C.c_int32)]
 
 
 class dq_server_config(C.Structure):

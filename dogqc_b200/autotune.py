@@ -37,6 +37,7 @@ KNOBS = [
     ("defer_threshold", [0, 8, 32, 128, 512]),
     ("unique_slots_pct", [0, 200, 400, 800]),
     ("multi_buckets_pct", [100, 50, 25, 200]),
+    ("ctas_per_sm", [0, 3, 4, 2]),
 ]
 
 _cache = {}
@@ -129,8 +130,10 @@ def batch_measure(engine, lowerings, reps=3, warmup=1):
     return measure
 
 
-def plan_measure(engine, lowering, reps=3, warmup=1):
-    """Median device time of a plan prepared with the candidate tuning."""
+def plan_measure(engine, lowering, reps=3, warmup=1, between=None):
+    """Median device time of a plan prepared with the candidate tuning;
+    ``between()`` runs before every execution (an L2 flush, so that inputs
+    that would fit L2 are read from HBM as in a timed run)."""
     def measure(tuning):
         try:
             p = engine.prepare(lowering, tuning=tuning)
@@ -138,15 +141,37 @@ def plan_measure(engine, lowering, reps=3, warmup=1):
             return None
         try:
             for _ in range(warmup):
+                if between:
+                    between()
                 p.execute()
             ts = []
             for _ in range(reps):
+                if between:
+                    between()
                 p.execute()
                 ts.append(p.timing()["total_ms"])
             return float(np.median(ts)) / 1e3
         finally:
             p.free()
     return measure
+
+
+def relevant_knobs(lowering, knobs=KNOBS):
+    """The knobs that can change a plan's kernels: table sizing only with
+    such tables, expansion deferral only with an expansion."""
+    kinds = {r.kind for r in lowering.res}
+    from dogqc_b200 import _lib as L
+    ops = {o["kind"] for p in lowering.pipes for o in p.ops}
+    out = []
+    for knob, values in knobs:
+        if knob == "unique_slots_pct" and L.RES_UNIQUE not in kinds:
+            continue
+        if knob == "multi_buckets_pct" and L.RES_MULTI not in kinds:
+            continue
+        if knob == "defer_threshold" and L.OP_EXPAND not in ops:
+            continue
+        out.append((knob, values))
+    return out
 
 
 def _tuned(key, engine, search):
@@ -171,6 +196,7 @@ def tune_batch(engine, lowerings, knobs=KNOBS, reps=3):
     return _tuned(key, engine, lambda: coordinate_search(batch_measure(engine, lowerings, reps), knobs))
 
 
-def tune_plan(engine, lowering, knobs=KNOBS, reps=3):
+def tune_plan(engine, lowering, knobs=None, reps=3, between=None):
     key = "plan|%s" % shape_key(lowering)
-    return _tuned(key, engine, lambda: coordinate_search(plan_measure(engine, lowering, reps), knobs))
+    knobs = relevant_knobs(lowering) if knobs is None else knobs
+    return _tuned(key, engine, lambda: coordinate_search(plan_measure(engine, lowering, reps, between=between), knobs))

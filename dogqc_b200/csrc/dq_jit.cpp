@@ -43,7 +43,7 @@ namespace dq {
 namespace jit {
 namespace {
 
-constexpr int kStripedMax = 48 * 1024;      // shared memory the striped local table may take
+constexpr int kStripedMax = 12 * 1024;      // shared memory a replicated CTA-local aggregation table may take
 constexpr int kBlock = kThreads;
 constexpr int kWarpBuf = 64;                // rows one warp's divergence buffer holds
 
@@ -1140,11 +1140,15 @@ struct Gen {
       return;
     }
     // replicate the accumulators per lane (32 copies: lanes of a warp never
-    // collide) or per half-warp (16) when the table allows, else one copy
+    // collide), per half-warp (16) or per eighth (8, 4) when the table stays
+    // within kStripedMax, else one copy.  A large table costs more than the
+    // collisions it avoids: shared memory taken from the SM's L1 leaves fewer
+    // lines for the loads in flight (a 33 KB table made the C1 probe kernel
+    // twice as slow at five CTAs per SM as an 8.8 KB one)
     const int tags = (ns + 1) * 8 + (R.packed ? 0 : ns * R.nkeys * 8);  // hashed keys: their values too
     agg = AGG_LOCAL;
     copies = 1;
-    for (int c : {32, 16})
+    for (int c : {32, 16, 8, 4})
       if (tags + (ns + 1) * R.naggs * 8 * c <= kStripedMax) {
         agg = AGG_STRIPED;
         copies = c;

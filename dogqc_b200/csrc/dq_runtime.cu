@@ -252,6 +252,7 @@ struct PlanOpts {
   int unique_pct = 0;         // join-table slots, % of the plan's capacity (0: by size)
   int multi_pct = 100;        // multimap buckets, % of the plan's capacity
   int defer_threshold = 0;    // expansion ranges longer than this are deferred (0: adaptive)
+  int ctas_per_sm = 0;        // resident CTAs per SM of pipeline kernels (0: occupancy)
   jit::Tuning tuning;
 };
 
@@ -938,7 +939,8 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
     occ = p.row ? row_occupancy(P.smem_bytes) : pipeline_occupancy(P.smem_bytes);
   }
   if (occ < 1) throw DqError(DQ_ERR_UNSUPPORTED, "pipeline kernel cannot be resident with this shared memory");
-  int want = ctx->cfg.ctas_per_sm > 0 ? std::min(ctx->cfg.ctas_per_sm, occ) : occ;
+  const int asked = plan->opts.ctas_per_sm > 0 ? plan->opts.ctas_per_sm : ctx->cfg.ctas_per_sm;
+  int want = asked > 0 ? std::min(asked, occ) : occ;
   p.grid_full = ctx->sms * want;
   p.grid = p.grid_full;
   if (!P.nrows_dev) {  // no more CTAs than row blocks
@@ -1432,6 +1434,7 @@ PlanOpts opts_of(const dq_tuning* t) {
   if (t && t->unique_slots_pct > 0) o.unique_pct = t->unique_slots_pct;
   if (t && t->multi_buckets_pct > 0) o.multi_pct = t->multi_buckets_pct;
   if (t && t->defer_threshold > 0) o.defer_threshold = t->defer_threshold;
+  if (t && t->ctas_per_sm > 0) o.ctas_per_sm = t->ctas_per_sm;
   return o;
 }
 

@@ -380,7 +380,8 @@ typedef struct {
                                      /* the reference's 0.9 x 32 = 28)          */
     int32_t defer_threshold;         /* expansion ranges longer than this are   */
                                      /* deferred (0: adaptive, 128 or 8)        */
-    int32_t reserved[1];
+    int32_t ctas_per_sm;             /* resident CTAs per SM of each generated  */
+                                     /* pipeline kernel (0: as many as fit)     */
 } dq_tuning;
 int dq_plan_prepare_tuned(dq_ctx* ctx, const dq_plan_desc* desc, const dq_tuning* tuning, dq_plan** out);
 
