@@ -184,7 +184,10 @@ struct DevPipe {
   const DevStr* strsrc;        // the plan's string sources (string references)
   int32_t nstrsrc;
   int32_t* status;
-  uint32_t* tile_counter;      // dynamic tile scheduler
+  uint32_t* tile_counter;      // dynamic tile scheduler; [1]: CTAs done (fused tail)
+  const DevPipe* tail;         // the next pipeline's descriptor when this kernel's
+                               // last CTA runs it (a scan of this pipeline's small
+                               // aggregation table into the result)
   uint64_t* scratch_ll;        // misc device counters
   uint64_t* profile;           // lane-activity histograms, 33 bins a profile point
 };

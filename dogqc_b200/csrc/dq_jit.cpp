@@ -186,6 +186,8 @@ struct Gen {
   int hot_off = 0;               // shared-memory offset of that table
   std::string inst_expr = "0u";  // the instance a deferred item belongs to (batches)
   std::string ldfn = "__ldcs";   // load function of streamed source columns
+  bool single_cta = false;       // the tail function: one CTA scans the whole source
+  bool tail_call = false;        // the main kernel's last CTA calls dq_tail
   int block = kBlock;            // threads per CTA
   bool batched = false;          // kernel over many instances of the plan
   // whether the current step is the lane's last (the refill buffer drains then)
@@ -1416,10 +1418,51 @@ struct Gen {
     agg_init();
   }
 
+  // A word of the aggregation table the pipeline scans.  The fused tail reads
+  // it past L1 (__ldcg): the other CTAs' atomics wrote it at L2.
+  std::string src_ld(const std::string& ptr) const {
+    return single_cta ? "__ldcg(reinterpret_cast<const unsigned long long*>(" + ptr + "))" : "*(" + ptr + ")";
+  }
+
   void epilogue() {
     agg_flush();
+    if (tail_call) {
+      // every CTA's aggregates are merged (its atomics fenced) before it
+      // counts itself done; the last one scans the table into the result
+      L("{");
+      L("  __shared__ int dq_last_;");
+      L("  __threadfence();");
+      L("  __syncthreads();");
+      L("  if (tid == 0) dq_last_ = atomicAdd(P.tile_counter + 1, 1u) == gridDim.x - 1u;");
+      L("  __syncthreads();");
+      L("  if (dq_last_) {");
+      L("    __threadfence();");
+      L("    dq_tail(*P.tail);");
+      L("  }");
+      L("}");
+    }
     --ind;
     L("}");
+  }
+
+  // The next pipeline as a device function one CTA runs over its whole source
+  // (the fused tail): the row loop of dq_main without the grid stride.
+  void tail_function() {
+    L("__device__ __noinline__ void dq_tail(const DevPipe& P) {");
+    ++ind;
+    L("if (*(volatile int32_t*)P.status & (kErrHtFull | kErrTimeout)) return;");
+    L("const int tid = threadIdx.x, lane = tid & 31;");
+    L("(void)lane;");
+    L("const int64_t nrows = source_rows(P);");
+    L("const int64_t span = (int64_t)blockDim.x * " + num(U) + ";");
+    L("for (int64_t base = 0; base < nrows; base += span) {");
+    ++ind;
+    row_loop();
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+    L("");
   }
 
   // <dst><col>[0..U) for the thread's U consecutive rows of the step starting
@@ -1556,7 +1599,8 @@ struct Gen {
     if (agg_src) {
       const int sr = P.source_res;
       const DevRes& R = P.res[sr];
-      if (R.nkeys > 0) L("if (act) act = " + res(sr) + ".slots[(uint64_t)row * " + num(R.words) + "] != kEmpty;");
+      if (R.nkeys > 0)
+        L("if (act) act = " + src_ld(res(sr) + ".slots + (uint64_t)row * " + num(R.words)) + " != kEmpty;");
     }
     for (int s = 0; s < P.nslots; ++s) {
       const DevSlot& sl = slot(s);
@@ -1571,14 +1615,14 @@ struct Gen {
         ++ind;
         L("const uint64_t* as_ = " + res(sl.res) + ".slots + (uint64_t)row * " + num(R.words) + ";");
         if (sl.kind == DQ_SLOT_AGGVAL) {
-          L(var[s] + " = canon(as_[" + num(R.val_word + sl.src) + "], " + ct_name(sl.ctype) + ");");
+          L(var[s] + " = canon(" + src_ld("as_ + " + num(R.val_word + sl.src)) + ", " + ct_name(sl.ctype) + ");");
         } else if (R.packed) {
-          L("const uint64_t t_ = (uint64_t)row == " + res(sl.res) + ".cap ? kEmpty : as_[0];");
+          L("const uint64_t t_ = (uint64_t)row == " + res(sl.res) + ".cap ? kEmpty : " + src_ld("as_") + ";");
           bool wide = R.nkeys == 1 && (R.key_ctype[0] == DQ_I64 || R.key_ctype[0] == DQ_U64);
           L(var[s] + " = canon(" + (wide ? std::string("t_") : "(t_ >> " + num(32 * sl.src) + ") & 0xffffffffull") +
             ", " + ct_name(sl.ctype) + ");");
         } else {
-          L(var[s] + " = canon(as_[" + num(R.key_word + sl.src) + "], " + ct_name(sl.ctype) + ");");
+          L(var[s] + " = canon(" + src_ld("as_ + " + num(R.key_word + sl.src)) + ", " + ct_name(sl.ctype) + ");");
         }
         --ind;
         L("}");
@@ -1830,7 +1874,7 @@ struct Gen {
 
 }  // namespace
 
-Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t) {
+Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t, const DevPipe* tail) {
   Gen g(P, expand_op);
   g.batched = t.batched;
   if (t.block == 128 || t.block == 256 || t.block == 512) g.block = t.block;
@@ -1838,24 +1882,14 @@ Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t
   for (int i = 0; i < P.nops; ++i) has_expand |= P.ops[i].kind == DQ_OP_EXPAND;
   g.U = (has_expand || P.source_kind == DQ_SRC_AGG) ? 1 : 4;
   // tuning knobs: rows per thread and step (1, 2 or 4), minimum resident CTAs per SM
-  int rows = t.rows_per_thread;
-  if (const char* e = getenv("DQ_JIT_ROWS")) rows = atoi(e);
+  const int rows = t.rows_per_thread;
   if (rows > 0 && !has_expand && P.source_kind != DQ_SRC_AGG) g.U = rows >= 4 ? 4 : rows >= 2 ? 2 : 1;
   if (t.refill < 0) refill_op = -1;
   if (t.refill_threshold >= 1 && t.refill_threshold <= 32) g.refill_threshold = t.refill_threshold;
-  if (const char* e = getenv("DQ_JIT_MIN_BLOCKS")) g.min_blocks = std::min(8, std::max(0, atoi(e)));
-  if (const char* e = getenv("DQ_JIT_LOAD")) {
-    std::string s(e);
-    g.ldfn = s == "nc" ? "__ldg" : s == "plain" ? "ld_plain" : s == "lu" ? "__ldlu" : "__ldcs";
-  }
   g.choose_agg();
-  const char* no_refill = getenv("DQ_JIT_REFILL");
-  g.choose_refill(no_refill && atoi(no_refill) == 0 ? -1 : refill_op);
-  const char* no_hot = getenv("DQ_JIT_HOT");
-  if (!(no_hot && atoi(no_hot) == 0)) g.choose_hot();
+  g.choose_refill(refill_op);
+  g.choose_hot();
   g.choose_prefetch();
-  const char* no_pf = getenv("DQ_JIT_PREFETCH");
-  if (no_pf && atoi(no_pf) == 0) g.prefetch.clear();
   if (g.U == 4 && rows <= 0) {
     // four rows per thread keep enough loads in flight for narrow pipelines;
     // wide ones (many columns or several early probes) run out of registers
@@ -1866,6 +1900,17 @@ Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t
     if (cols.size() > 3 || g.prefetch.size() > 1) g.U = 2;
   }
   g.o = "// generated pipeline kernel (dogqc_b200)\n#include \"dq_common.cuh\"\nusing namespace dq;\n\n";
+  if (tail && !t.batched && expand_op < 0) {
+    Gen tg(*tail, -1);
+    tg.single_cta = true;
+    tg.U = 1;
+    tg.choose_agg();
+    tg.choose_refill(-1);
+    if (tg.agg != AGG_NONE || tg.smem > 0) throw Error("a fused tail takes no shared memory");
+    tg.tail_function();
+    g.o += tg.o;
+    g.tail_call = true;
+  }
   Program prog;
   prog.block = g.block;
   if (t.batched) {

@@ -53,7 +53,11 @@ struct Tuning {
 // stash indices); `expand_op` is the expansion whose wide ranges are deferred
 // to the second kernel (-1: none); `refill_op` is the selective filter or
 // probe after which the warps refill their lanes from a buffer (-1: none).
-Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t = Tuning());
+// With `tail` (the next pipeline: a scan of this pipeline's aggregation table
+// with scalar ops and an emit sink), the kernel's last CTA runs that pipeline
+// after every CTA has merged its aggregates, and the tail needs no launch.
+Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t = Tuning(),
+                 const DevPipe* tail = nullptr);
 
 // Compiles the program (cached by source text) and, with `load`, loads it.
 Kernels compile(const Program& prog, bool load);

@@ -236,6 +236,9 @@ struct PipeRec {
   bool mm_count = false;    // sink is a multimap count: bucket scan follows
   int mm_res = -1;
   int staged_cols = 0;
+  int tail = -1;            // the pipeline this kernel's last CTA runs (fused tail)
+  int fused_into = -1;      // runs inside that pipeline's kernel, not launched
+  DevBuf tail_buf;          // device copy of the fused tail's descriptor
 };
 
 struct dq_result {
@@ -922,8 +925,12 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   int64_t rows_per_cta = tile;
   if (plan->opts.batch_member) {
     // the batch launches its own many-instance kernels
+  } else if (p.jit && p.fused_into >= 0) {
+    // runs inside the kernel of pipeline `fused_into`: no kernel of its own
   } else if (p.jit) {
-    p.prog = jit::generate(P, p.expand_op, d.compact - 1, plan->opts.tuning);
+    const DevPipe* tail = p.tail >= 0 && p.expand_op < 0 ? &plan->pipes[p.tail]->dev : nullptr;
+    if (p.tail >= 0 && !tail) throw DqError(DQ_ERR_BAD_IR, "a pipeline with deferred expansion cannot run a fused tail");
+    p.prog = jit::generate(P, p.expand_op, d.compact - 1, plan->opts.tuning, tail);
     if (t_collect) t_collect->push_back(p.prog);
     else p.kernels = jit::compile(p.prog, !ctx->offline);
     rows_per_cta = (int64_t)p.prog.block * p.prog.rows_per_thread;
@@ -1015,9 +1022,15 @@ int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status, bool fast 
         DQ_CUDA(cudaMemsetAsync(p.heavy_gcnt.ptr, 0, p.heavy_gcnt.bytes, st));
       }
     }
-    if (p.jit) DQ_CUDA(launch_generated(p.kernels.main, p.dev, p.grid, p.prog.block, p.prog.smem_bytes, st));
-    else DQ_CUDA(p.row ? launch_row(p.dev, p.grid, st) : launch_pipeline(p.dev, p.grid, st));
-    ++launches;
+    if (p.fused_into >= 0) {
+      // ran in the last CTA of pipeline fused_into's kernel
+    } else if (p.jit) {
+      DQ_CUDA(launch_generated(p.kernels.main, p.dev, p.grid, p.prog.block, p.prog.smem_bytes, st));
+      ++launches;
+    } else {
+      DQ_CUDA(p.row ? launch_row(p.dev, p.grid, st) : launch_pipeline(p.dev, p.grid, st));
+      ++launches;
+    }
     if (p.expand_op >= 0) {
       if (p.dev.heavy.grouped) {
         DQ_CUDA(launch_heavy_group(p.dev.heavy, p.dev.status, plan->ctx->sms, st));
@@ -1250,7 +1263,9 @@ uint64_t plan_bytes(const dq_plan* plan) {
 // device as well.
 void refresh_pipelines(dq_plan* plan) {
   plan->str_src.clear();
-  for (auto& pp : plan->pipes) setup_pipeline(plan, *pp);
+  // last pipeline first: a fused tail's descriptor is laid out before the
+  // kernel that runs it is generated
+  for (size_t i = plan->pipes.size(); i-- > 0;) setup_pipeline(plan, *plan->pipes[i]);
   // the string sources every pipeline may resolve references against
   const size_t n = plan->str_src.size();
   if (plan->str_src_dev.bytes != std::max<size_t>(n, 1) * sizeof(DevStr) || (!plan->str_src_dev.ptr && !t_offline))
@@ -1261,6 +1276,42 @@ void refresh_pipelines(dq_plan* plan) {
     pp->dev.strsrc = plan->str_src_dev.as<DevStr>();
     pp->dev.nstrsrc = (int32_t)n;
   }
+  // fused tails: their descriptors where the kernels that run them read them
+  // (they always reset the aggregation table they scan: they are its only scan)
+  for (size_t i = 0; i < plan->pipes.size(); ++i) {
+    PipeRec& p = *plan->pipes[i];
+    if (p.tail < 0) continue;
+    PipeRec& t = *plan->pipes[p.tail];
+    t.dev.clear_src = 1;
+    t.dev.tile_counter = plan->counters + 2 * p.tail;
+    if (!p.tail_buf.ptr || p.tail_buf.bytes != sizeof(DevPipe)) p.tail_buf.alloc(sizeof(DevPipe));
+    if (!plan->ctx->offline && !t_offline)
+      DQ_CUDA(cudaMemcpy(p.tail_buf.ptr, &t.dev, sizeof(DevPipe), cudaMemcpyHostToDevice));
+    p.dev.tail = p.tail_buf.as<DevPipe>();
+  }
+}
+
+// Whether pipeline k's kernel can run pipeline k + 1 in its last CTA: k
+// aggregates into a table of at most 65,536 slots that k + 1 alone scans,
+// with scalar ops and filters into an emit sink, and k defers no expansion.
+bool fusable_tail(const dq_plan_desc* desc, const std::vector<std::unique_ptr<ResRec>>& res, int k) {
+  const dq_pipeline& a = desc->pipes[k];
+  const dq_pipeline& b = desc->pipes[k + 1];
+  if (a.nops <= 0 || b.nops <= 0) return false;
+  const dq_op& sink = a.ops[a.nops - 1];
+  if (sink.kind != DQ_OP_AGG || b.source_kind != DQ_SRC_AGG || b.source_res != sink.res) return false;
+  if (sink.res < 0 || sink.res >= (int)res.size() || res[sink.res]->dev.cap + 1 > 65536) return false;
+  for (int i = 0; i < a.nops; ++i)
+    if (a.ops[i].kind == DQ_OP_EXPAND) return false;
+  for (int i = 0; i < b.nops; ++i) {
+    const int kd = b.ops[i].kind;
+    const bool ok = kd == DQ_OP_ARITH || kd == DQ_OP_CMP || kd == DQ_OP_LOGIC || kd == DQ_OP_CAST ||
+                    kd == DQ_OP_SELECT || kd == DQ_OP_FILTER || (kd == DQ_OP_EMIT && i == b.nops - 1);
+    if (!ok) return false;
+  }
+  for (int i = 0; i < desc->npipes; ++i)
+    if (i != k + 1 && desc->pipes[i].source_kind == DQ_SRC_AGG && desc->pipes[i].source_res == sink.res) return false;
+  return true;
 }
 
 // Lays out a plan's resources and pipelines (the caller holds the context lock
@@ -1332,6 +1383,14 @@ std::unique_ptr<dq_plan> make_plan(dq_ctx* ctx, const dq_plan_desc* desc, const 
     p->desc.table = p->col_names.back().c_str();
     for (int c = 0; c < p->desc.npatterns; ++c) p->desc.patterns[c] = p->patterns[c].c_str();
   }
+  // the last CTA of an aggregating kernel runs the small scan that follows it
+  const bool generated = !(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) && !opts.batch_member;
+  if (generated)
+    for (int k = 0; k + 1 < desc->npipes; ++k)
+      if (plan->pipes[k]->fused_into < 0 && fusable_tail(desc, plan->res, k)) {
+        plan->pipes[k]->tail = k + 1;
+        plan->pipes[k + 1]->fused_into = k;
+      }
   refresh_pipelines(plan.get());
   // an aggregation table that one generated pipeline alone scans is reset by that scan
   std::vector<int> scans(desc->nres, 0);
@@ -2174,9 +2233,17 @@ int dq_plan_profile(dq_plan* plan, int32_t point, uint64_t* counts) {
 int dq_plan_source(dq_plan* plan, int32_t pipe, char* buf, int64_t cap, int64_t* len) {
   if (!plan || !len || cap < 0 || (cap > 0 && !buf)) return DQ_ERR_INVALID;
   if (pipe < 0 || pipe >= (int32_t)plan->pipes.size()) return fail(plan->ctx, DQ_ERR_INVALID, "no such pipeline");
-  const PipeRec& p = *plan->pipes[pipe];
+  const PipeRec* pp = plan->pipes[pipe].get();
+  std::string text;
+  if (pp->fused_into >= 0) {
+    // a fused tail: the kernel that runs it (its code is dq_tail there)
+    text = "// pipeline " + std::to_string(pipe) + " runs as dq_tail in the last CTA of pipeline " +
+           std::to_string(pp->fused_into) + "'s kernel\n";
+    pp = plan->pipes[pp->fused_into].get();
+  }
+  const PipeRec& p = *pp;
   if (!p.jit) return fail(plan->ctx, DQ_ERR_NOT_FOUND, "pipeline runs on a prebuilt kernel");
-  std::string text = p.prog.source;
+  text += p.prog.source;
   if (!p.kernels.log.empty()) text += "\n/* compiler report:\n" + p.kernels.log + "\n*/\n";
   *len = (int64_t)text.size();
   if (cap > 0) {

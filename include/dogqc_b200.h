@@ -331,6 +331,9 @@ int dq_plan_prepare(dq_ctx* ctx, const dq_plan_desc* desc, dq_plan** out);
 /* Generated CUDA source of pipeline `pipe` followed by the compiler's
  * register report, NUL-terminated into buf (at most cap bytes); *len is the
  * full length.  DQ_ERR_NOT_FOUND when the pipeline runs on a prebuilt kernel.
+ * A small scan of an aggregation table that follows the pipeline filling it
+ * runs in the last CTA of that pipeline's kernel (no launch of its own): its
+ * source is that kernel's, where it is the function dq_tail.
  * The counterpart of the reference's generated query file.                 */
 int dq_plan_source(dq_plan* plan, int32_t pipe, char* buf, int64_t cap, int64_t* len);
 /* Runs every pipeline in order on `stream` (NULL: the context stream) and
