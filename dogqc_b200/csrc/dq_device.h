@@ -20,6 +20,8 @@ enum : int32_t {
   kErrTimeout = 2,
   kErrOverflow = 4,
   kErrBadOp = 8,
+  kErrKeyRange = 16,     // a key outside a key-domain bitmap's range: the host
+                         // turns the table back into a hash table and re-runs
   kInfoHeavyFull = 32,   // informational: deferred expansion items exceeded their
                          // capacity; the rest ran in place (results stay exact)
 };
@@ -106,6 +108,10 @@ struct DevRes {
   uint64_t* cursor;       // OUTPUT row cursor
   int32_t smem_slots;     // AGG: CTA-local table slots (0: global only)
   int32_t smem_off;       // AGG: offset of the CTA-local table
+  int32_t bitmap;         // UNIQUE without payload over a small key domain:
+                          // slots hold one bit per key in [bmin, bmin + brange)
+  int64_t bmin;
+  uint64_t brange;
 };
 
 struct DevHeavy {         // deferred wide expansion ranges

@@ -27,6 +27,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <climits>
+
 #include "dq_device.h"
 
 namespace dq {
@@ -695,6 +697,40 @@ cudaError_t launch_import_parse(const ImpArgs& A, cudaStream_t st) {
   if (A.nrows == 0) return cudaSuccess;
   imp_parse_kernel<<<(unsigned)A.nblocks, kImpRows, 0, st>>>(A);
   if (A.nstr > 0) imp_scan_kernel<<<A.nstr, kScanThreads, 0, st>>>(A.bsum, A.boff, A.nblocks, A.nblocks + 1);
+  return cudaGetLastError();
+}
+
+// Smallest and largest value of an integer column (`width` bytes a value,
+// sign-extended when `is_signed`) into out[0], out[1] (initialised by the caller
+// to INT64_MAX, INT64_MIN).
+__global__ void col_minmax_kernel(const uint8_t* col, uint64_t n, int width, int is_signed, long long* out) {
+  long long lo = LLONG_MAX, hi = LLONG_MIN;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    long long v;
+    if (width == 1) v = is_signed ? (long long)(int8_t)col[i] : (long long)col[i];
+    else if (width == 4) {
+      const uint32_t u = reinterpret_cast<const uint32_t*>(col)[i];
+      v = is_signed ? (long long)(int32_t)u : (long long)u;
+    } else {
+      v = (long long)reinterpret_cast<const uint64_t*>(col)[i];
+    }
+    lo = v < lo ? v : lo;
+    hi = v > hi ? v : hi;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const long long a = __shfl_xor_sync(0xffffffffu, lo, o), b = __shfl_xor_sync(0xffffffffu, hi, o);
+    lo = a < lo ? a : lo;
+    hi = b > hi ? b : hi;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(out, lo);
+    atomicMax(out + 1, hi);
+  }
+}
+
+cudaError_t launch_col_minmax(const uint8_t* col, uint64_t n, int width, bool is_signed, long long* out, int sms,
+                              cudaStream_t st) {
+  if (n) col_minmax_kernel<<<sms * 4, 256, 0, st>>>(col, n, width, is_signed ? 1 : 0, out);
   return cudaGetLastError();
 }
 

@@ -186,6 +186,7 @@ struct Gen {
   int hot_off = 0;               // shared-memory offset of that table
   std::string inst_expr = "0u";  // the instance a deferred item belongs to (batches)
   std::string ldfn = "__ldcs";   // load function of streamed source columns
+  std::vector<std::pair<int, int>> bitmaps;  // key-domain bitmaps probed: (resource, smem offset)
   bool single_cta = false;       // the tail function: one CTA scans the whole source
   bool tail_call = false;        // the main kernel's last CTA calls dq_tail
   int block = kBlock;            // threads per CTA
@@ -486,7 +487,7 @@ struct Gen {
       if (op.kind == DQ_OP_EXPAND || (refill >= 0 && k > refill)) break;
       if (op.kind != DQ_OP_PROBE) continue;
       const DevRes& R = P.res[op.res];
-      if (!R.packed || R.nkeys == 0 || R.words > 2 || tag_can_be_empty(op.res)) continue;
+      if (R.bitmap || !R.packed || R.nkeys == 0 || R.words > 2 || tag_can_be_empty(op.res)) continue;
       bool cols = true;
       for (int i = 0; i < op.nlist; ++i) cols &= slot(P.lists[op.list + i]).kind == DQ_SLOT_COL;
       if (cols) prefetch.push_back(k);
@@ -538,6 +539,18 @@ struct Gen {
     const int r = op.res;
     const DevRes& R = P.res[r];
     std::string s = fresh("ps");
+    if (R.bitmap) {
+      // a bit per key of the build column's domain
+      const std::string key = "canon(" + V(P.lists[op.list]) + ", " + ct_name(R.key_ctype[0]) + ")";
+      L("int64_t " + s + " = -1;");
+      L("if (" + act + ") {");
+      L("  const uint64_t o_ = (uint64_t)((int64_t)" + key + " - " + res(r) + ".bmin);");
+      L("  if (o_ < " + res(r) + ".brange && ((" + bitmap_words(r) + "[o_ >> 5] >> (o_ & 31u)) & 1u)) " + s + " = 0;");
+      L("}");
+      if (op.sub == DQ_JOIN_ANTI) L(act + " = " + act + " && " + s + " < 0;");
+      else L(act + " = " + act + " && " + s + " >= 0;");
+      return;
+    }
     const std::string sh = str_key_hashes(r, op.list, op.nlist, act);
     L("int64_t " + s + " = -1;");
     L("if (" + act + ") {");
@@ -993,6 +1006,18 @@ struct Gen {
   void sink_build(const dq_op& op, const std::string& act) {
     const int r = op.res;
     const DevRes& R = P.res[r];
+    if (R.bitmap) {
+      // keys outside the domain measured at preparation: the table's data
+      // changed; the host re-runs the plan with a hash table
+      const std::string key = "canon(" + V(P.lists[op.list]) + ", " + ct_name(R.key_ctype[0]) + ")";
+      L("if (" + act + ") {");
+      L("  const uint64_t o_ = (uint64_t)((int64_t)" + key + " - " + res(r) + ".bmin);");
+      L("  if (o_ < " + res(r) + ".brange) atomicOr(reinterpret_cast<unsigned int*>(" + res(r) +
+        ".slots) + (o_ >> 5), 1u << (o_ & 31u));");
+      L("  else set_status(P, kErrKeyRange);");
+      L("}");
+      return;
+    }
     const std::string sh = str_key_hashes(r, op.list, op.nlist, act);
     L("if (" + act + ") {");
     ++ind;
@@ -1416,6 +1441,42 @@ struct Gen {
     L("(void)smem;");
     L("(void)lane;");
     agg_init();
+    bitmap_init();
+  }
+
+  // The key-domain bitmaps this kernel probes, one word per thread into
+  // shared memory (a probe is then a bank access, not an L2 access).
+  void choose_bitmaps() {
+    bitmaps.clear();
+    if (batched) return;  // a batched kernel's items change instance: its probes read the bits in place
+    for (int k = 0; k < P.nops; ++k) {
+      const dq_op& op = P.ops[k];
+      if (op.kind != DQ_OP_PROBE || !P.res[op.res].bitmap) continue;
+      bool seen = false;
+      for (auto& b : bitmaps) seen |= b.first == op.res;
+      if (seen) continue;
+      const int off = (smem + 15) / 16 * 16;
+      bitmaps.emplace_back(op.res, off);
+      smem = off + (int)P.res[op.res].cap * 4;
+    }
+  }
+
+  void bitmap_init() {
+    for (auto& b : bitmaps) {
+      L("{");
+      L("  const uint32_t* g_ = reinterpret_cast<const uint32_t*>(" + res(b.first) + ".slots);");
+      L("  uint32_t* s_ = reinterpret_cast<uint32_t*>(smem + " + num(b.second) + ");");
+      L("  for (uint32_t i = tid; i < (uint32_t)" + res(b.first) + ".cap; i += " + num(block) + "u) s_[i] = __ldcg(g_ + i);");
+      L("}");
+    }
+    if (!bitmaps.empty()) L("__syncthreads();");
+  }
+
+  // Bits of resource r as the probe reads them: shared memory or in place.
+  std::string bitmap_words(int r) const {
+    for (auto& b : bitmaps)
+      if (b.first == r) return "reinterpret_cast<const uint32_t*>(smem + " + num(b.second) + ")";
+    return "reinterpret_cast<const uint32_t*>(" + res(r) + ".slots)";
   }
 
   // A word of the aggregation table the pipeline scans.  The fused tail reads
@@ -1890,6 +1951,7 @@ Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t
   g.choose_refill(refill_op);
   g.choose_hot();
   g.choose_prefetch();
+  g.choose_bitmaps();
   if (g.U == 4 && rows <= 0) {
     // four rows per thread keep enough loads in flight for narrow pipelines;
     // wide ones (many columns or several early probes) run out of registers

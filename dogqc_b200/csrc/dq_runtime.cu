@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <condition_variable>
 #include <cstdio>
@@ -57,6 +58,8 @@ cudaError_t launch_str_ref_offsets(const uint64_t* refs, uint64_t n, const DevSt
 cudaError_t launch_str_ref_copy(const uint64_t* refs, uint64_t n, const DevStr* src, const uint64_t* offs,
                                 uint8_t* heap, int sms, cudaStream_t st);
 cudaError_t launch_import_strings(const ImpArgs& A, cudaStream_t st);
+cudaError_t launch_col_minmax(const uint8_t* col, uint64_t n, int width, bool is_signed, long long* out, int sms,
+                              cudaStream_t st);
 }  // namespace dq
 
 using namespace dq;
@@ -207,6 +210,10 @@ struct ResRec {
   int index = 0;            // position in the plan's resources
   bool agg_clean = false;   // AGG: every slot is in its initial state (the last
                             // run's scan reset what it read)
+  bool bitmap = false;      // UNIQUE: a bit per key of the build column's domain
+  int64_t bmin = 0;         //   [bmin, bmin + brange) instead of a hash table
+  uint64_t brange = 0;
+  bool no_bitmap = false;   // a run met a key outside the domain: hash table from then on
 };
 
 constexpr uint64_t kL2TableBytes = 48ull << 20;  // join tables up to this size get extra slack
@@ -430,6 +437,17 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
       d.naggs > DQ_MAX_AGGS)
     throw DqError(DQ_ERR_BAD_IR, "resource sizes out of range");
   uint64_t cap = (uint64_t)std::max<int64_t>(d.capacity, 1);
+  if (d.kind == DQ_RES_UNIQUE && r.bitmap && !r.no_bitmap) {
+    // one bit per key of the build column's domain, cleared every run
+    R.bitmap = 1;
+    R.bmin = r.bmin;
+    R.brange = r.brange;
+    R.cap = (r.brange + 31) / 32;
+    R.words = 0;
+    r.slots.alloc(R.cap * 4 + 16);
+    R.slots = r.slots.as<uint64_t>();
+    return;
+  }
   switch (d.kind) {
     case DQ_RES_UNIQUE:
     case DQ_RES_AGG: {
@@ -993,7 +1011,7 @@ int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status, bool fast 
     ResRec& r = *rp;
     switch (r.desc.kind) {
       case DQ_RES_UNIQUE:
-        DQ_CUDA(cudaMemsetAsync(r.slots.ptr, 0xff, r.slots.bytes, st));
+        DQ_CUDA(cudaMemsetAsync(r.slots.ptr, r.dev.bitmap ? 0 : 0xff, r.slots.bytes, st));
         break;
       case DQ_RES_AGG:
         if (!(fast && r.agg_clean)) {
@@ -1314,6 +1332,63 @@ bool fusable_tail(const dq_plan_desc* desc, const std::vector<std::unique_ptr<Re
   return true;
 }
 
+// Unique tables whose key domain is small become a bit per key: one key, no
+// payload, read straight from a column of a registered table by the one
+// pipeline that builds the table, and at most kBitmapKeys values between the
+// column's smallest and largest (measured on the device at preparation).  A
+// probe is then one bit test (in shared memory for the generated kernels).
+constexpr uint64_t kBitmapKeys = 1ull << 18;  // 32 KB of bits
+
+void choose_bitmap(dq_ctx* ctx, const dq_plan_desc* desc, int i, ResRec& r) {
+  const dq_resource& d = desc->res[i];
+  if (d.kind != DQ_RES_UNIQUE || d.nkeys != 1 || d.npay != 0 || r.no_bitmap) return;
+  const int kt = d.key_ctype[0];
+  if (kt != DQ_I8 && kt != DQ_I32 && kt != DQ_U32 && kt != DQ_I64) return;
+  const dq_pipeline* build = nullptr;
+  for (int p = 0; p < desc->npipes; ++p) {
+    const dq_pipeline& pd = desc->pipes[p];
+    if (pd.nops <= 0 || pd.nops > DQ_MAX_OPS) return;
+    for (int k = 0; k < pd.nops; ++k) {
+      const dq_op& op = pd.ops[k];
+      // ops whose `res` names a resource (LIKE, STREQ and PROFILE use it otherwise)
+      const bool uses_res = op.kind == DQ_OP_PROBE || op.kind == DQ_OP_EXPAND || op.kind == DQ_OP_EXISTS ||
+                            op.kind >= DQ_OP_AGG;
+      if (!uses_res || op.res != i) continue;
+      if (op.kind == DQ_OP_BUILD && k == pd.nops - 1) {
+        if (build) return;
+        build = &pd;
+      } else if (op.kind != DQ_OP_PROBE || op.nlist != 1) {
+        return;
+      }
+    }
+  }
+  if (!build || build->source_kind != DQ_SRC_TABLE || !build->table) return;
+  const dq_op& sink = build->ops[build->nops - 1];
+  if (sink.nlist != 1 || sink.nlist2 != 0 || sink.list < 0 || sink.list >= build->nlist) return;
+  const int ks = build->lists[sink.list];
+  if (ks < 0 || ks >= build->nslots || build->slots[ks].kind != DQ_SLOT_COL) return;
+  const int ci = build->slots[ks].src;
+  if (ci < 0 || ci >= build->ncols || !build->cols[ci]) return;
+  auto t = ctx->tables.find(build->table);
+  if (t == ctx->tables.end() || t->second.nrows <= 0) return;
+  const ColRec* c = t->second.find(build->cols[ci]);
+  // the key is the column's value unchanged: same type in the slot and the table
+  if (!c || c->ctype != kt || build->slots[ks].ctype != kt || !c->data || !c->data->ptr) return;
+  DevBuf mm;
+  mm.alloc(16);
+  const long long init[2] = {LLONG_MAX, LLONG_MIN};
+  DQ_CUDA(cudaMemcpy(mm.ptr, init, 16, cudaMemcpyHostToDevice));
+  DQ_CUDA(launch_col_minmax(c->data->as<uint8_t>(), (uint64_t)t->second.nrows, ctype_width(c->ctype),
+                            kt != DQ_U32, mm.as<long long>(), ctx->sms, ctx->stream));
+  long long got[2];
+  DQ_CUDA(cudaMemcpyAsync(got, mm.ptr, 16, cudaMemcpyDeviceToHost, ctx->stream));
+  DQ_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (got[0] > got[1] || (unsigned long long)(got[1] - got[0]) >= kBitmapKeys) return;
+  r.bitmap = true;
+  r.bmin = got[0];
+  r.brange = (uint64_t)(got[1] - got[0]) + 1;
+}
+
 // Lays out a plan's resources and pipelines (the caller holds the context lock
 // and has made the device current).
 std::unique_ptr<dq_plan> make_plan(dq_ctx* ctx, const dq_plan_desc* desc, const PlanOpts& opts) {
@@ -1360,6 +1435,8 @@ std::unique_ptr<dq_plan> make_plan(dq_ctx* ctx, const dq_plan_desc* desc, const 
     r->desc = desc->res[i];
     r->name = desc->res[i].name ? desc->res[i].name : "";
     r->desc.name = nullptr;
+    if (!(ctx->cfg.flags & (DQ_CFG_NO_JIT | DQ_CFG_ROW_KERNEL)) && !ctx->offline && !t_offline)
+      choose_bitmap(ctx, desc, i, *r);
     setup_resource(plan.get(), *r, bound[i]);
     plan->res.push_back(std::move(r));
   }
@@ -1411,6 +1488,12 @@ std::unique_ptr<dq_plan> make_plan(dq_ctx* ctx, const dq_plan_desc* desc, const 
 void grow_plan(dq_plan* plan, int status) {
   for (auto& rp : plan->res) {
     ResRec& r = *rp;
+    if ((status & kErrKeyRange) && r.bitmap && !r.no_bitmap) {
+      // the table's data changed since preparation: a hash table from now on
+      r.no_bitmap = true;
+      setup_resource(plan, r, 1);
+      continue;
+    }
     if ((status & kErrHtFull) && (r.desc.kind == DQ_RES_UNIQUE || r.desc.kind == DQ_RES_AGG)) {
       // four times the slots (join tables are sized at unique_pct of the capacity)
       const int64_t pct = r.desc.kind == DQ_RES_UNIQUE ? r.pct : 100;
@@ -1638,7 +1721,8 @@ void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
       BatchReset op{};
       switch (r.desc.kind) {
         case DQ_RES_UNIQUE:
-          op.ptr = r.dev.slots, op.n = (r.dev.cap + 1) * r.dev.words, op.value = kEmpty, op.kind = 0;
+          if (r.dev.bitmap) op.ptr = r.dev.slots, op.n = (r.dev.cap * 4 + 7) / 8, op.value = 0, op.kind = 0;
+          else op.ptr = r.dev.slots, op.n = (r.dev.cap + 1) * r.dev.words, op.value = kEmpty, op.kind = 0;
           break;
         case DQ_RES_AGG:
           op.ptr = r.dev.slots, op.n = r.dev.cap + 1, op.kind = 2, op.words = r.dev.words;
@@ -2991,7 +3075,8 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
       BatchReset op{};
       switch (r.desc.kind) {
         case DQ_RES_UNIQUE:
-          op.ptr = r.dev.slots, op.n = (r.dev.cap + 1) * r.dev.words, op.value = kEmpty, op.kind = 0;
+          if (r.dev.bitmap) op.ptr = r.dev.slots, op.n = (r.dev.cap * 4 + 7) / 8, op.value = 0, op.kind = 0;
+          else op.ptr = r.dev.slots, op.n = (r.dev.cap + 1) * r.dev.words, op.value = kEmpty, op.kind = 0;
           break;
         case DQ_RES_AGG:
           op.ptr = r.dev.slots, op.n = r.dev.cap + 1, op.kind = 2, op.words = r.dev.words;
