@@ -108,8 +108,10 @@ struct DevRes {
   uint64_t* cursor;       // OUTPUT row cursor
   int32_t smem_slots;     // AGG: CTA-local table slots (0: global only)
   int32_t smem_off;       // AGG: offset of the CTA-local table
-  int32_t bitmap;         // UNIQUE without payload over a small key domain:
-                          // slots hold one bit per key in [bmin, bmin + brange)
+  int32_t bitmap;         // UNIQUE over a small key domain [bmin, bmin + brange):
+                          // 1: no payload, slots hold one bit per key;
+                          // 2: one 32-bit payload, slots hold a word per key,
+                          //    (1 << 32) | payload, 0 when the key is absent
   int64_t bmin;
   uint64_t brange;
 };

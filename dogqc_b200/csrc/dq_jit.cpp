@@ -487,7 +487,8 @@ struct Gen {
       if (op.kind == DQ_OP_EXPAND || (refill >= 0 && k > refill)) break;
       if (op.kind != DQ_OP_PROBE) continue;
       const DevRes& R = P.res[op.res];
-      if (R.bitmap || !R.packed || R.nkeys == 0 || R.words > 2 || tag_can_be_empty(op.res)) continue;
+      if (R.bitmap == 1) continue;
+      if (R.bitmap != 2 && (!R.packed || R.nkeys == 0 || R.words > 2 || tag_can_be_empty(op.res))) continue;
       bool cols = true;
       for (int i = 0; i < op.nlist; ++i) cols &= slot(P.lists[op.list + i]).kind == DQ_SLOT_COL;
       if (cols) prefetch.push_back(k);
@@ -512,6 +513,14 @@ struct Gen {
       ++ind;
       L("const uint64_t* const ht_ = " + res(r) + ".slots;");
       const std::string K = num(k);
+      if (R.bitmap == 2) {
+        // the key's word of a dense table
+        L("const uint64_t o_ = (uint64_t)" + key[0] + " - (uint64_t)" + res(r) + ".bmin;");
+        L("pw" + K + "_0[u] = in_ && o_ < " + res(r) + ".brange ? __ldg(reinterpret_cast<const unsigned long long*>(ht_) + o_) : 0ull;");
+        --ind;
+        L("}");
+        continue;
+      }
       if (R.compact) {
         // compact slots: the aligned 16-byte pair of the home slot
         L("const uint32_t p_ = slot_of(" + tag + ", (uint32_t)" + res(r) + ".cap) & ~1u;");
@@ -539,12 +548,40 @@ struct Gen {
     const int r = op.res;
     const DevRes& R = P.res[r];
     std::string s = fresh("ps");
+    if (R.bitmap == 2) {
+      // a payload word per key of the build column's domain
+      const std::string key = "canon(" + V(P.lists[op.list]) + ", " + ct_name(R.key_ctype[0]) + ")";
+      const bool with_pay = op.sub == DQ_JOIN_INNER && op.nlist2 > 0 && P.lists[op.list2] >= 0;
+      L("int64_t " + s + " = -1;");
+      L("if (" + act + ") {");
+      ++ind;
+      if (is_prefetched(k)) {
+        L("const uint64_t w_ = pw" + num(k) + "_0[u];");
+      } else {
+        L("const uint64_t o_ = (uint64_t)" + key + " - (uint64_t)" + res(r) + ".bmin;");
+        L("const uint64_t w_ = o_ < " + res(r) + ".brange ? __ldg(reinterpret_cast<const unsigned long long*>(" + res(r) +
+          ".slots) + o_) : 0ull;");
+      }
+      L("if (w_) {");
+      L("  " + s + " = 0;");
+      if (with_pay) {
+        const int d = P.lists[op.list2];
+        L("  " + V(d) + " = canon(canon((uint64_t)(uint32_t)w_, " + ct_name(R.pay_ctype[0]) + "), " +
+          ct_name(slot(d).ctype) + ");");
+      }
+      L("}");
+      --ind;
+      L("}");
+      if (op.sub == DQ_JOIN_ANTI) L(act + " = " + act + " && " + s + " < 0;");
+      else L(act + " = " + act + " && " + s + " >= 0;");
+      return;
+    }
     if (R.bitmap) {
       // a bit per key of the build column's domain
       const std::string key = "canon(" + V(P.lists[op.list]) + ", " + ct_name(R.key_ctype[0]) + ")";
       L("int64_t " + s + " = -1;");
       L("if (" + act + ") {");
-      L("  const uint64_t o_ = (uint64_t)((int64_t)" + key + " - " + res(r) + ".bmin);");
+      L("  const uint64_t o_ = (uint64_t)" + key + " - (uint64_t)" + res(r) + ".bmin;");
       L("  if (o_ < " + res(r) + ".brange && ((" + bitmap_words(r) + "[o_ >> 5] >> (o_ & 31u)) & 1u)) " + s + " = 0;");
       L("}");
       if (op.sub == DQ_JOIN_ANTI) L(act + " = " + act + " && " + s + " < 0;");
@@ -1011,9 +1048,16 @@ struct Gen {
       // changed; the host re-runs the plan with a hash table
       const std::string key = "canon(" + V(P.lists[op.list]) + ", " + ct_name(R.key_ctype[0]) + ")";
       L("if (" + act + ") {");
-      L("  const uint64_t o_ = (uint64_t)((int64_t)" + key + " - " + res(r) + ".bmin);");
-      L("  if (o_ < " + res(r) + ".brange) atomicOr(reinterpret_cast<unsigned int*>(" + res(r) +
-        ".slots) + (o_ >> 5), 1u << (o_ & 31u));");
+      L("  const uint64_t o_ = (uint64_t)" + key + " - (uint64_t)" + res(r) + ".bmin;");
+      if (R.bitmap == 2) {
+        // the first row of a key wins, as in the hash table
+        const std::string pay = op.nlist2 > 0 ? "(uint64_t)(uint32_t)" + V(P.lists[op.list2]) : "0ull";
+        L("  if (o_ < " + res(r) + ".brange) atomicCAS(reinterpret_cast<unsigned long long*>(" + res(r) +
+          ".slots) + o_, 0ull, (1ull << 32) | " + pay + ");");
+      } else {
+        L("  if (o_ < " + res(r) + ".brange) atomicOr(reinterpret_cast<unsigned int*>(" + res(r) +
+          ".slots) + (o_ >> 5), 1u << (o_ & 31u));");
+      }
       L("  else set_status(P, kErrKeyRange);");
       L("}");
       return;
@@ -1451,7 +1495,7 @@ struct Gen {
     if (batched) return;  // a batched kernel's items change instance: its probes read the bits in place
     for (int k = 0; k < P.nops; ++k) {
       const dq_op& op = P.ops[k];
-      if (op.kind != DQ_OP_PROBE || !P.res[op.res].bitmap) continue;
+      if (op.kind != DQ_OP_PROBE || P.res[op.res].bitmap != 1) continue;
       bool seen = false;
       for (auto& b : bitmaps) seen |= b.first == op.res;
       if (seen) continue;
@@ -1606,7 +1650,8 @@ struct Gen {
     L("for (int64_t base = (int64_t)blockIdx.x * span; base < nrows; base += (int64_t)gridDim.x * span) {");
     ++ind;
     for (int k : prefetch) {
-      const int nq = P.res[P.ops[k].res].compact ? 2 : 4;
+      const DevRes& Rk = P.res[P.ops[k].res];
+      const int nq = Rk.bitmap == 2 ? 1 : Rk.compact ? 2 : 4;
       for (int q = 0; q < nq; ++q) L("uint64_t pw" + num(k) + "_" + num(q) + "[" + num(U) + "];");
     }
     if (!cols.empty()) {
@@ -1752,7 +1797,7 @@ struct Gen {
     std::vector<int> cols = source_cols();
     for (int c : cols) L("uint64_t c" + num(c) + "[" + num(U) + "];");
     for (int k : prefetch)
-      for (int q = 0; q < (P.res[P.ops[k].res].compact ? 2 : 4); ++q)
+      for (int q = 0; q < (P.res[P.ops[k].res].bitmap == 2 ? 1 : P.res[P.ops[k].res].compact ? 2 : 4); ++q)
         L("uint64_t pw" + num(k) + "_" + num(q) + "[" + num(U) + "];");
     if (!cols.empty()) {
       col_loads(cols, "c", "base");

@@ -210,8 +210,8 @@ struct ResRec {
   int index = 0;            // position in the plan's resources
   bool agg_clean = false;   // AGG: every slot is in its initial state (the last
                             // run's scan reset what it read)
-  bool bitmap = false;      // UNIQUE: a bit per key of the build column's domain
-  int64_t bmin = 0;         //   [bmin, bmin + brange) instead of a hash table
+  int bitmap = 0;           // UNIQUE: a bit (1) or a payload word (2) per key of the
+  int64_t bmin = 0;         //   build column's domain [bmin, bmin + brange), no hash table
   uint64_t brange = 0;
   bool no_bitmap = false;   // a run met a key outside the domain: hash table from then on
 };
@@ -438,13 +438,14 @@ void setup_resource(dq_plan* plan, ResRec& r, int64_t build_rows_bound) {
     throw DqError(DQ_ERR_BAD_IR, "resource sizes out of range");
   uint64_t cap = (uint64_t)std::max<int64_t>(d.capacity, 1);
   if (d.kind == DQ_RES_UNIQUE && r.bitmap && !r.no_bitmap) {
-    // one bit per key of the build column's domain, cleared every run
-    R.bitmap = 1;
+    // one bit (no payload) or one word (a payload) per key of the build
+    // column's domain, cleared every run; cap counts 32- or 64-bit words
+    R.bitmap = r.bitmap;
     R.bmin = r.bmin;
     R.brange = r.brange;
-    R.cap = (r.brange + 31) / 32;
+    R.cap = r.bitmap == 1 ? (r.brange + 31) / 32 : r.brange;
     R.words = 0;
-    r.slots.alloc(R.cap * 4 + 16);
+    r.slots.alloc(R.cap * (r.bitmap == 1 ? 4 : 8) + 16);
     R.slots = r.slots.as<uint64_t>();
     return;
   }
@@ -1332,16 +1333,21 @@ bool fusable_tail(const dq_plan_desc* desc, const std::vector<std::unique_ptr<Re
   return true;
 }
 
-// Unique tables whose key domain is small become a bit per key: one key, no
-// payload, read straight from a column of a registered table by the one
-// pipeline that builds the table, and at most kBitmapKeys values between the
-// column's smallest and largest (measured on the device at preparation).  A
-// probe is then one bit test (in shared memory for the generated kernels).
+// Unique tables over a small key domain need no hashing: one key, read
+// straight from a column of a registered table by the one pipeline that builds
+// the table, whose smallest and largest values (measured on the device at
+// preparation) span few keys.
+// - No payload, at most kBitmapKeys keys: a bit per key.  A probe is one bit
+//   test (in shared memory for the generated kernels).
+// - One payload of at most 32 bits, at most kDenseKeys keys and at most four
+//   per row of the build table: a word per key.  A probe is one 8-byte load.
 constexpr uint64_t kBitmapKeys = 1ull << 18;  // 32 KB of bits
+constexpr uint64_t kDenseKeys = 1ull << 24;   // 128 MB of words
 
 void choose_bitmap(dq_ctx* ctx, const dq_plan_desc* desc, int i, ResRec& r) {
   const dq_resource& d = desc->res[i];
-  if (d.kind != DQ_RES_UNIQUE || d.nkeys != 1 || d.npay != 0 || r.no_bitmap) return;
+  if (d.kind != DQ_RES_UNIQUE || d.nkeys != 1 || d.npay > 1 || r.no_bitmap) return;
+  if (d.npay == 1 && (d.pay_ctype[0] == DQ_STR || ctype_width(d.pay_ctype[0]) > 4)) return;
   const int kt = d.key_ctype[0];
   if (kt != DQ_I8 && kt != DQ_I32 && kt != DQ_U32 && kt != DQ_I64) return;
   const dq_pipeline* build = nullptr;
@@ -1364,7 +1370,7 @@ void choose_bitmap(dq_ctx* ctx, const dq_plan_desc* desc, int i, ResRec& r) {
   }
   if (!build || build->source_kind != DQ_SRC_TABLE || !build->table) return;
   const dq_op& sink = build->ops[build->nops - 1];
-  if (sink.nlist != 1 || sink.nlist2 != 0 || sink.list < 0 || sink.list >= build->nlist) return;
+  if (sink.nlist != 1 || sink.nlist2 != d.npay || sink.list < 0 || sink.list >= build->nlist) return;
   const int ks = build->lists[sink.list];
   if (ks < 0 || ks >= build->nslots || build->slots[ks].kind != DQ_SLOT_COL) return;
   const int ci = build->slots[ks].src;
@@ -1383,10 +1389,13 @@ void choose_bitmap(dq_ctx* ctx, const dq_plan_desc* desc, int i, ResRec& r) {
   long long got[2];
   DQ_CUDA(cudaMemcpyAsync(got, mm.ptr, 16, cudaMemcpyDeviceToHost, ctx->stream));
   DQ_CUDA(cudaStreamSynchronize(ctx->stream));
-  if (got[0] > got[1] || (unsigned long long)(got[1] - got[0]) >= kBitmapKeys) return;
-  r.bitmap = true;
+  if (got[0] > got[1]) return;
+  const uint64_t span = (uint64_t)got[1] - (uint64_t)got[0] + 1;  // 0: all 2^64 values
+  if (span == 0 || (d.npay == 0 ? span > kBitmapKeys : span > kDenseKeys || span > 4 * (uint64_t)t->second.nrows))
+    return;
+  r.bitmap = d.npay == 0 ? 1 : 2;
   r.bmin = got[0];
-  r.brange = (uint64_t)(got[1] - got[0]) + 1;
+  r.brange = span;
 }
 
 // Lays out a plan's resources and pipelines (the caller holds the context lock
@@ -1721,7 +1730,8 @@ void build_batch(dq_batch* b, const jit::Tuning& tuning, cudaStream_t st) {
       BatchReset op{};
       switch (r.desc.kind) {
         case DQ_RES_UNIQUE:
-          if (r.dev.bitmap) op.ptr = r.dev.slots, op.n = (r.dev.cap * 4 + 7) / 8, op.value = 0, op.kind = 0;
+          if (r.dev.bitmap) op.ptr = r.dev.slots, op.n = r.dev.bitmap == 1 ? (r.dev.cap * 4 + 7) / 8 : r.dev.cap,
+                            op.value = 0, op.kind = 0;
           else op.ptr = r.dev.slots, op.n = (r.dev.cap + 1) * r.dev.words, op.value = kEmpty, op.kind = 0;
           break;
         case DQ_RES_AGG:
@@ -3075,7 +3085,8 @@ void srv_dispatch_batch(dq_server* s, SrvSlot& slot, SrvShape* sh) {
       BatchReset op{};
       switch (r.desc.kind) {
         case DQ_RES_UNIQUE:
-          if (r.dev.bitmap) op.ptr = r.dev.slots, op.n = (r.dev.cap * 4 + 7) / 8, op.value = 0, op.kind = 0;
+          if (r.dev.bitmap) op.ptr = r.dev.slots, op.n = r.dev.bitmap == 1 ? (r.dev.cap * 4 + 7) / 8 : r.dev.cap,
+                            op.value = 0, op.kind = 0;
           else op.ptr = r.dev.slots, op.n = (r.dev.cap + 1) * r.dev.words, op.value = kEmpty, op.kind = 0;
           break;
         case DQ_RES_AGG:
