@@ -90,6 +90,29 @@ WORKLOADS = {
     "c13": ("rows/s (NOT EXISTS on a unique key filter table + group by, input rows of both tables per second)",
             {"workload": "anti_join_not_exists", "customer_rows": 150_000, "order_rows": 1_500_000, "groups": 25,
              "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c14": ("rows/s (TPC-H Q16 shape: string predicates, FK-PK join, anti join, two aggregations with string keys, "
+            "input rows of the tables read per second)",
+            {"workload": "q16_strings", "part_rows": 200_000, "partsupp_rows": 800_000, "supplier_rows": 10_000,
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c15": ("rows/s (FK-PK join on a string key + group by, input rows of both tables per second)",
+            {"workload": "string_key_join", "nation_rows": 25, "supplier_rows": 100_000,
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c16": ("rows/s (TPC-H Q22 shape: substrings in an IN list and as a group key, nested-loop join with an "
+            "average, NOT EXISTS, input rows of the tables read per second)",
+            {"workload": "q22_substrings", "customer_rows": "2 x 150,000", "order_rows": 1_500_000,
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c17": ("rows/s (TPC-H Q13 shape: NOT LIKE on comments, outer join, two aggregations, input rows per second)",
+            {"workload": "q13_comments", "customer_rows": 150_000, "order_rows": 1_500_000,
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c18": ("rows/s (TPC-H Q20 shape: LIKE prefix, aggregation into a two-key join table, semi joins, string "
+            "results, input rows of the tables read per second)",
+            {"workload": "q20_strings", "lineitem_rows": 6_000_000, "partsupp_rows": 800_000, "part_rows": 200_000,
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
+    "c19": ("rows/s (TPC-H Q2 shape: LIKE suffix, MIN joined back, string results, input rows of the tables read "
+            "per second)",
+            {"workload": "q2_strings", "partsupp_rows": "2 x 800,000", "part_rows": "2 x 200,000",
+             "supplier_rows": "2 x 10,000",
+             "l2": "256 MB write + 256 MB read between steps (inputs evicted)", "parallelism": "replicas"}),
 }
 
 
