@@ -220,6 +220,74 @@ __device__ __noinline__ bool like_match(const uint8_t* s, int ls, const uint8_t*
   return l_pos >= l_in_end;
 }
 
+// Prefetches into L1 the 128-byte lines (at most four) that n bytes at p
+// cover: a warp that works through its lanes' long strings one after another
+// then waits for their memory once, not once per string.  The lines lie in the
+// string's own allocation (heaps start 256-byte aligned).
+__device__ __forceinline__ void prefetch_bytes(const uint8_t* p, int n) {
+  const unsigned long long a = (unsigned long long)p & ~127ull, e = (unsigned long long)p + (unsigned long long)n;
+  for (int i = 0; i < 4 && a + 128ull * (unsigned long long)i < e; ++i)
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(a + 128ull * (unsigned long long)i));
+}
+
+// LIKE of each active lane's string, called by every lane of the warp.  For a
+// pattern '%L1%...%Ln%' (at most 8 literals, none empty, no '_') the matcher
+// above finds each literal at its leftmost occurrence after the previous one's
+// end.  Strings over 32 bytes are then searched by the whole warp, 32 start
+// positions a step (lane j tries base + j) with neighbouring reads; shorter
+// strings and other patterns run like_match in their own lane.
+__device__ __noinline__ bool like_match_warp(bool active, const uint8_t* s, int ls, const uint8_t* p, int lp) {
+  int lo[8], ln[8], nl = 0;  // the literals (the pattern is the same in every lane)
+  bool simple = lp >= 3 && p[0] == '%' && p[lp - 1] == '%';
+  for (int i = 1, start = 1; simple && i < lp; ++i) {
+    if (p[i] == '_') {
+      simple = false;
+    } else if (p[i] == '%') {
+      if (i == start || nl == 8) {
+        simple = false;
+      } else {
+        lo[nl] = start;
+        ln[nl] = i - start;
+        ++nl;
+        start = i + 1;
+      }
+    }
+  }
+  if (!simple) return active && like_match(s, ls, p, lp);
+  const bool wide = active && ls > 32;
+  if (wide) prefetch_bytes(s, ls);
+  bool r = active && !wide && like_match(s, ls, p, lp);
+  const int lane = (int)(threadIdx.x & 31);
+  unsigned todo = __ballot_sync(kFull, wide);
+  while (todo) {
+    const int src = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const uint8_t* q = reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, (unsigned long long)s, src));
+    const int n = __shfl_sync(kFull, ls, src);
+    int pos = 0;
+    bool ok = true;
+    for (int k = 0; k < nl && ok; ++k) {
+      const uint8_t* L = p + lo[k];
+      const int m = ln[k];
+      bool found = false;
+      for (int base = pos; base + m <= n; base += 32) {
+        const int c = base + lane;
+        bool hit = c + m <= n;
+        for (int j = 0; hit && j < m; ++j) hit = q[c + j] == L[j];
+        const unsigned hm = __ballot_sync(kFull, hit);
+        if (hm) {
+          pos = base + __ffs(hm) - 1 + m;
+          found = true;
+          break;
+        }
+      }
+      ok = found;
+    }
+    if (lane == src) r = ok;
+  }
+  return r;
+}
+
 // String value of row g of a string column.
 __device__ __forceinline__ void str_at(const DevStr& d, int64_t g, const uint8_t*& ptr, int& len) {
   if (d.width > 0) {
@@ -356,6 +424,7 @@ __device__ __noinline__ uint64_t str_ref_hash_warp(const DevPipe& P, bool active
   int n = 0;
   if (active) str_ref_at(P, ref, p, n);
   const bool wide = active && n > kStrCoopMin;
+  if (wide) prefetch_bytes(p, n);
   uint64_t h = (active && !wide) ? str_hash(p, n) : 0ull;
   const int lane = (int)(threadIdx.x & 31);
   unsigned todo = __ballot_sync(kFull, wide);
@@ -384,6 +453,10 @@ __device__ __noinline__ bool str_ref_eq_warp(const DevPipe& P, bool active, uint
     str_ref_at(P, b, pb, nb);
   }
   const bool wide = active && a != b && na == nb && na > kStrCoopMin;
+  if (wide) {
+    prefetch_bytes(pa, na);
+    prefetch_bytes(pb, nb);
+  }
   bool eq = active && (a == b || (!wide && str_eq(pa, na, pb, nb)));
   const int lane = (int)(threadIdx.x & 31);
   unsigned todo = __ballot_sync(kFull, wide);

@@ -388,7 +388,22 @@ struct Gen {
         case DQ_OP_SELECT:
           scalar_op(op);
           break;
-        case DQ_OP_LIKE:
+        case DQ_OP_LIKE: {
+          // every lane calls the matcher: long strings are searched by the whole warp
+          L("{");
+          ++ind;
+          L("const uint8_t* sp_ = nullptr; int sn_ = 0;");
+          L("if (" + act + ") {");
+          ++ind;
+          str_bytes(op.a, row, "sp_", "sn_");
+          --ind;
+          L("}");
+          L(V(op.dst) + " = (uint64_t)like_match_warp(" + act + ", sp_, sn_, P.patterns + P.pat_off[" + num(op.res) +
+            "], P.pat_off[" + num(op.res + 1) + "] - P.pat_off[" + num(op.res) + "]);");
+          --ind;
+          L("}");
+          break;
+        }
         case DQ_OP_STREQ: {
           L(V(op.dst) + " = 0;");
           L("if (" + act + ") {");

@@ -93,6 +93,24 @@ def test_long_string_keys_match_oracle(engine, kind):
     assert canonical_rows(run(engine, db, plan).rows()) == canonical_rows(run_plan(db, plan)[1])
 
 
+@pytest.mark.parametrize("pattern", ["%#1%", "%ABC%xyz%", "%!\"#%#4%", "%pqrs%PQRS%#%", "%~!%", "%abc%abc%abc%abc%",
+                                     "%a%b%c%d%e%f%g%h%", "%a%b%c%d%e%f%g%h%i%", "%AB_D%", "A%", "%#59"])
+def test_like_on_long_strings_matches_oracle(engine, pattern):
+    """Strings of up to 300 bytes: patterns of '%'-separated literals are
+    searched by whole warps (32 start positions a step); patterns with '_', a
+    missing leading or trailing '%' or more than eight literals run in each
+    lane.  Both give the reference matcher's answers."""
+    import dogqc_b200.scalar as scal
+    from dogqc_b200.relational import RelationalAlgebra
+    from dogqc_b200.types import Type
+    db = string_cases.long_db()
+    alg = RelationalAlgebra(db)
+    sel = alg.selection(scal.LikeExpr(scal.AttrExpr("fk"), scal.ConstExpr(pattern, Type.STRING)), alg.scan("f"))
+    plan = alg.resolveAlgebraPlan(alg.projection(["fv", "fk"], sel), {})
+    want = canonical_rows(run_plan(db, plan)[1])
+    assert canonical_rows(run(engine, db, plan).rows()) == want
+
+
 @pytest.mark.parametrize("pattern", ["%ABCDEFGHIJKLMNOP%", "xxxxxxxxxxxxxxxxxxxx%", "%JKLMNOPQRSTUVWXYZABC%",
                                      "hello world%"])
 def test_long_like_patterns_match_oracle(engine, pattern):
