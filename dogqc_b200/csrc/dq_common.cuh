@@ -230,62 +230,47 @@ __device__ __forceinline__ void prefetch_bytes(const uint8_t* p, int n) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(a + 128ull * (unsigned long long)i));
 }
 
-// LIKE of each active lane's string, called by every lane of the warp.  For a
-// pattern '%L1%...%Ln%' (at most 8 literals, none empty, no '_') the matcher
-// above finds each literal at its leftmost occurrence after the previous one's
-// end.  Strings over 32 bytes are then searched by the whole warp, 32 start
-// positions a step (lane j tries base + j) with neighbouring reads; shorter
-// strings and other patterns run like_match in their own lane.
-__device__ __noinline__ bool like_match_warp(bool active, const uint8_t* s, int ls, const uint8_t* p, int lp) {
-  int lo[8], ln[8], nl = 0;  // the literals (the pattern is the same in every lane)
-  bool simple = lp >= 3 && p[0] == '%' && p[lp - 1] == '%';
-  for (int i = 1, start = 1; simple && i < lp; ++i) {
-    if (p[i] == '_') {
-      simple = false;
-    } else if (p[i] == '%') {
-      if (i == start || nl == 8) {
-        simple = false;
-      } else {
-        lo[nl] = start;
-        ln[nl] = i - start;
-        ++nl;
-        start = i + 1;
-      }
+// First index in [from, to) of byte c in s, or -1.  Tests eight bytes at a
+// time in the aligned words that cover the range (a zero-byte test on
+// w ^ c repeated, Mycroft's method); bytes before `from` are set to 0xff first
+// so that no borrow from them can flag a later byte.  String heaps start
+// 256-byte aligned and are padded at the end, so every such word lies in the
+// heap's allocation.
+__device__ __forceinline__ int find_byte(const uint8_t* s, int from, int to, uint8_t c) {
+  if (from >= to) return -1;
+  const unsigned long long ones = 0x0101010101010101ull, pat = ones * c;
+  const unsigned long long first = (unsigned long long)(s + from), end = (unsigned long long)(s + to);
+  unsigned long long a = first & ~7ull;
+  int skip = (int)(first - a);
+  for (; a < end; a += 8, skip = 0) {
+    unsigned long long t = __ldg(reinterpret_cast<const unsigned long long*>(a)) ^ pat;
+    if (skip) t |= (1ull << (8 * skip)) - 1;
+    const unsigned long long z = (t - ones) & ~t & 0x8080808080808080ull;
+    if (z) {
+      const int i = (int)(a - (unsigned long long)s) + (__ffsll((long long)z) - 1) / 8;
+      return i < to ? i : -1;
     }
   }
-  if (!simple) return active && like_match(s, ls, p, lp);
-  const bool wide = active && ls > 32;
-  if (wide) prefetch_bytes(s, ls);
-  bool r = active && !wide && like_match(s, ls, p, lp);
-  const int lane = (int)(threadIdx.x & 31);
-  unsigned todo = __ballot_sync(kFull, wide);
-  while (todo) {
-    const int src = __ffs(todo) - 1;
-    todo &= todo - 1;
-    const uint8_t* q = reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, (unsigned long long)s, src));
-    const int n = __shfl_sync(kFull, ls, src);
-    int pos = 0;
-    bool ok = true;
-    for (int k = 0; k < nl && ok; ++k) {
-      const uint8_t* L = p + lo[k];
-      const int m = ln[k];
-      bool found = false;
-      for (int base = pos; base + m <= n; base += 32) {
-        const int c = base + lane;
-        bool hit = c + m <= n;
-        for (int j = 0; hit && j < m; ++j) hit = q[c + j] == L[j];
-        const unsigned hm = __ballot_sync(kFull, hit);
-        if (hm) {
-          pos = base + __ffs(hm) - 1 + m;
-          found = true;
-          break;
-        }
-      }
-      ok = found;
+  return -1;
+}
+
+// One literal of a LIKE pattern '%L1%...%Ln%': its leftmost occurrence in
+// s[pos, n); on success pos moves past it.  For such patterns (no '_', no
+// empty literal) like_match's outcome is that of finding L1, ..., Ln this way
+// one after another.
+__device__ __forceinline__ bool like_find(const uint8_t* s, int n, int& pos, const uint8_t* L, int m) {
+  while (pos + m <= n) {
+    const int c = find_byte(s, pos, n - m + 1, L[0]);
+    if (c < 0) return false;
+    int j = 1;
+    while (j < m && s[c + j] == L[j]) ++j;
+    if (j == m) {
+      pos = c + m;
+      return true;
     }
-    if (lane == src) r = ok;
+    pos = c + 1;
   }
-  return r;
+  return false;
 }
 
 // String value of row g of a string column.

@@ -187,6 +187,7 @@ struct Gen {
   std::string inst_expr = "0u";  // the instance a deferred item belongs to (batches)
   std::string ldfn = "__ldcs";   // load function of streamed source columns
   std::vector<std::pair<int, int>> bitmaps;  // key-domain bitmaps probed: (resource, smem offset)
+  const std::string* patterns = nullptr;     // host copy of the pattern bytes (P.pat_off into it)
   bool single_cta = false;       // the tail function: one CTA scans the whole source
   bool tail_call = false;        // the main kernel's last CTA calls dq_tail
   int block = kBlock;            // threads per CTA
@@ -389,17 +390,38 @@ struct Gen {
           scalar_op(op);
           break;
         case DQ_OP_LIKE: {
-          // every lane calls the matcher: long strings are searched by the whole warp
-          L("{");
-          ++ind;
-          L("const uint8_t* sp_ = nullptr; int sn_ = 0;");
+          // a pattern '%L1%...%Ln%' (no '_', no empty literal) finds its
+          // literals one after another, eight bytes a step; others run the
+          // reference matcher's algorithm (like_match)
+          std::vector<std::pair<int, int>> lits;  // (offset in the pattern buffer, length)
+          bool simple = false;
+          if (patterns) {
+            const int o = P.pat_off[op.res], lp = P.pat_off[op.res + 1] - o;
+            const std::string pat = patterns->substr((size_t)o, (size_t)lp);
+            simple = lp >= 3 && pat.front() == '%' && pat.back() == '%' && pat.find('_') == std::string::npos;
+            for (int i = 1, start = 1; simple && i < lp; ++i)
+              if (pat[(size_t)i] == '%') {
+                if (i == start) simple = false;
+                else lits.emplace_back(o + start, i - start);
+                start = i + 1;
+              }
+          }
+          L(V(op.dst) + " = 0;");
           L("if (" + act + ") {");
           ++ind;
+          L("const uint8_t* sp_; int sn_;");
           str_bytes(op.a, row, "sp_", "sn_");
-          --ind;
-          L("}");
-          L(V(op.dst) + " = (uint64_t)like_match_warp(" + act + ", sp_, sn_, P.patterns + P.pat_off[" + num(op.res) +
-            "], P.pat_off[" + num(op.res + 1) + "] - P.pat_off[" + num(op.res) + "]);");
+          if (simple) {
+            L("int lp_ = 0;");
+            std::string cond;
+            for (auto& l : lits)
+              cond += (cond.empty() ? "" : " && ") + std::string("like_find(sp_, sn_, lp_, P.patterns + ") + num(l.first) +
+                      ", " + num(l.second) + ")";
+            L(V(op.dst) + " = (uint64_t)(" + cond + ");");
+          } else {
+            L(V(op.dst) + " = (uint64_t)like_match(sp_, sn_, P.patterns + P.pat_off[" + num(op.res) + "], P.pat_off[" +
+              num(op.res + 1) + "] - P.pat_off[" + num(op.res) + "]);");
+          }
           --ind;
           L("}");
           break;
@@ -1995,8 +2017,10 @@ struct Gen {
 
 }  // namespace
 
-Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t, const DevPipe* tail) {
+Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t, const DevPipe* tail,
+                 const std::string* patterns) {
   Gen g(P, expand_op);
+  g.patterns = patterns;
   g.batched = t.batched;
   if (t.block == 128 || t.block == 256 || t.block == 512) g.block = t.block;
   bool has_expand = false;

@@ -56,8 +56,11 @@ struct Tuning {
 // With `tail` (the next pipeline: a scan of this pipeline's aggregation table
 // with scalar ops and an emit sink), the kernel's last CTA runs that pipeline
 // after every CTA has merged its aggregates, and the tail needs no launch.
+// `patterns`: the host copy of the bytes P.patterns points to (the LIKE
+// patterns and string constants, P.pat_off into them); with it, a LIKE
+// pattern of '%'-separated literals compiles into a search for each literal.
 Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t = Tuning(),
-                 const DevPipe* tail = nullptr);
+                 const DevPipe* tail = nullptr, const std::string* patterns = nullptr);
 
 // Compiles the program (cached by source text) and, with `load`, loads it.
 Kernels compile(const Program& prog, bool load);

@@ -237,6 +237,7 @@ struct PipeRec {
     if (heavy_stats) cudaFreeHost(heavy_stats);
   }
   DevBuf pattern_buf, heavy_items, heavy_count, heavy_prefix;
+  std::string pattern_text;  // the concatenated patterns pattern_buf holds (P.pat_off into it)
   DevBuf heavy_gkey, heavy_glen, heavy_gcnt, heavy_glist, heavy_gstart, heavy_sorted;  // grouped deferral
   bool clears_source = false;  // scans an aggregation table that no other pipeline
                                // reads, and may reset its slots as it reads them
@@ -783,7 +784,8 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   P.nops = d.nops;
   for (int i = 0; i < d.nops; ++i) P.ops[i] = d.ops[i];
   for (int i = 0; i < d.nlist; ++i) P.lists[i] = d.lists[i];
-  std::string cat;
+  std::string& cat = p.pattern_text;
+  cat.clear();
   for (int i = 0; i < d.npatterns; ++i) {
     P.pat_off[i] = (int32_t)cat.size();
     cat += d.patterns[i] ? d.patterns[i] : "";
@@ -949,7 +951,7 @@ void setup_pipeline(dq_plan* plan, PipeRec& p) {
   } else if (p.jit) {
     const DevPipe* tail = p.tail >= 0 && p.expand_op < 0 ? &plan->pipes[p.tail]->dev : nullptr;
     if (p.tail >= 0 && !tail) throw DqError(DQ_ERR_BAD_IR, "a pipeline with deferred expansion cannot run a fused tail");
-    p.prog = jit::generate(P, p.expand_op, d.compact - 1, plan->opts.tuning, tail);
+    p.prog = jit::generate(P, p.expand_op, d.compact - 1, plan->opts.tuning, tail, &p.pattern_text);
     if (t_collect) t_collect->push_back(p.prog);
     else p.kernels = jit::compile(p.prog, !ctx->offline);
     rows_per_cta = (int64_t)p.prog.block * p.prog.rows_per_thread;

@@ -94,12 +94,13 @@ def test_long_string_keys_match_oracle(engine, kind):
 
 
 @pytest.mark.parametrize("pattern", ["%#1%", "%ABC%xyz%", "%!\"#%#4%", "%pqrs%PQRS%#%", "%~!%", "%abc%abc%abc%abc%",
-                                     "%a%b%c%d%e%f%g%h%", "%a%b%c%d%e%f%g%h%i%", "%AB_D%", "A%", "%#59"])
+                                     "%a%b%c%d%e%f%g%h%", "%a%b%c%d%e%f%g%h%i%", "%AB_D%", "A%", "%#59", "%",
+                                     "%%", "%#%%1%", "%~", "%}~!\"#$%&'()*+,-./0123456789:;<=>?@ABCDEFG%"])
 def test_like_on_long_strings_matches_oracle(engine, pattern):
-    """Strings of up to 300 bytes: patterns of '%'-separated literals are
-    searched by whole warps (32 start positions a step); patterns with '_', a
-    missing leading or trailing '%' or more than eight literals run in each
-    lane.  Both give the reference matcher's answers."""
+    """Strings of up to 300 bytes: patterns '%L1%...%Ln%' find their literals
+    one after another, eight bytes a step; patterns with '_', an empty literal
+    or a missing leading or trailing '%' run the reference matcher's algorithm.
+    Both give its answers."""
     import dogqc_b200.scalar as scal
     from dogqc_b200.relational import RelationalAlgebra
     from dogqc_b200.types import Type
