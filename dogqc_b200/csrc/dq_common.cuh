@@ -230,6 +230,19 @@ __device__ __forceinline__ void prefetch_bytes(const uint8_t* p, int n) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(a + 128ull * (unsigned long long)i));
 }
 
+// Bytes p[0, m) (1 <= m <= 8) as a little-endian word, zero above byte m:
+// one or two loads of the aligned words that hold them, shifted together.
+// Every such word holds at least one of the bytes, so it lies in the same
+// allocation (string heaps start 256-byte aligned and are padded at the end).
+__device__ __forceinline__ uint64_t load_bytes(const uint8_t* p, int m) {
+  const unsigned long long at = (unsigned long long)p;
+  const unsigned long long* a = reinterpret_cast<const unsigned long long*>(at & ~7ull);
+  const int sh = (int)(at & 7);
+  uint64_t w = __ldg(a) >> (8 * sh);
+  if (sh + m > 8) w |= __ldg(a + 1) << (64 - 8 * sh);
+  return m >= 8 ? w : (w & ((1ull << (8 * m)) - 1));
+}
+
 // First index in [from, to) of byte c in s, or -1.  Tests eight bytes at a
 // time in the aligned words that cover the range (a zero-byte test on
 // w ^ c repeated, Mycroft's method); bytes before `from` are set to 0xff first
@@ -286,9 +299,12 @@ __device__ __forceinline__ void str_at(const DevStr& d, int64_t g, const uint8_t
 }
 
 __device__ __forceinline__ bool str_eq(const uint8_t* s, int ls, const uint8_t* p, int lp) {
-  bool eq = ls == lp;
-  for (int j = 0; eq && j < ls; ++j) eq = s[j] == p[j];
-  return eq;
+  if (ls != lp) return false;
+  for (int b = 0; b < ls; b += 8) {
+    const int m = ls - b < 8 ? ls - b : 8;
+    if (load_bytes(s + b, m) != load_bytes(p + b, m)) return false;
+  }
+  return true;
 }
 
 // ------------------------------------------------------------ pipelines --
@@ -355,10 +371,8 @@ __device__ __forceinline__ uint64_t str_ref_substring(uint64_t ref, int from, in
 // word per lane (str_ref_hash_warp) and reach the value one lane computes
 // alone, so either may hash the keys of one table.
 __device__ __forceinline__ uint64_t str_word(const uint8_t* p, int n, int i) {
-  const int b = 8 * i, e = b + 8 < n ? b + 8 : n;
-  uint64_t w = 0;
-  for (int j = b; j < e; ++j) w |= (uint64_t)p[j] << (8 * (j - b));
-  return w;
+  const int b = 8 * i;
+  return load_bytes(p + b, n - b < 8 ? n - b : 8);
 }
 
 __device__ __forceinline__ uint64_t str_word_term(uint64_t w, int i) {

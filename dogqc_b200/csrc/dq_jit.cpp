@@ -1525,14 +1525,15 @@ struct Gen {
     bitmap_init();
   }
 
-  // The key-domain bitmaps this kernel probes, one word per thread into
-  // shared memory (a probe is then a bank access, not an L2 access).
+  // The key-domain bitmaps of at most 32 KB this kernel probes, one word per
+  // thread into shared memory (a probe is then a bank access, not an L2
+  // access); larger ones are probed in place.
   void choose_bitmaps() {
     bitmaps.clear();
     if (batched) return;  // a batched kernel's items change instance: its probes read the bits in place
     for (int k = 0; k < P.nops; ++k) {
       const dq_op& op = P.ops[k];
-      if (op.kind != DQ_OP_PROBE || P.res[op.res].bitmap != 1) continue;
+      if (op.kind != DQ_OP_PROBE || P.res[op.res].bitmap != 1 || P.res[op.res].cap > 8192) continue;
       bool seen = false;
       for (auto& b : bitmaps) seen |= b.first == op.res;
       if (seen) continue;

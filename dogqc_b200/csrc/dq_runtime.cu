@@ -1339,12 +1339,14 @@ bool fusable_tail(const dq_plan_desc* desc, const std::vector<std::unique_ptr<Re
 // straight from a column of a registered table by the one pipeline that builds
 // the table, whose smallest and largest values (measured on the device at
 // preparation) span few keys.
-// - No payload, at most kBitmapKeys keys: a bit per key.  A probe is one bit
-//   test (in shared memory for the generated kernels).
+// - No payload: a bit per key, for at most kBitmapKeys keys, or at most
+//   kDenseKeys keys and at most 64 per row of the build table.  A probe is one
+//   bit test (in shared memory for the generated kernels when the bits fit
+//   kBitmapKeys, else a 4-byte load of a table of at most 2 MB).
 // - One payload of at most 32 bits, at most kDenseKeys keys and at most four
 //   per row of the build table: a word per key.  A probe is one 8-byte load.
 constexpr uint64_t kBitmapKeys = 1ull << 18;  // 32 KB of bits
-constexpr uint64_t kDenseKeys = 1ull << 24;   // 128 MB of words
+constexpr uint64_t kDenseKeys = 1ull << 24;   // 128 MB of words, 2 MB of bits
 
 void choose_bitmap(dq_ctx* ctx, const dq_plan_desc* desc, int i, ResRec& r) {
   const dq_resource& d = desc->res[i];
@@ -1393,7 +1395,8 @@ void choose_bitmap(dq_ctx* ctx, const dq_plan_desc* desc, int i, ResRec& r) {
   DQ_CUDA(cudaStreamSynchronize(ctx->stream));
   if (got[0] > got[1]) return;
   const uint64_t span = (uint64_t)got[1] - (uint64_t)got[0] + 1;  // 0: all 2^64 values
-  if (span == 0 || (d.npay == 0 ? span > kBitmapKeys : span > kDenseKeys || span > 4 * (uint64_t)t->second.nrows))
+  const uint64_t rows = (uint64_t)t->second.nrows;
+  if (span == 0 || span > kDenseKeys || (d.npay == 0 ? span > kBitmapKeys && span > 64 * rows : span > 4 * rows))
     return;
   r.bitmap = d.npay == 0 ? 1 : 2;
   r.bmin = got[0];

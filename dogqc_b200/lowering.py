@@ -635,14 +635,21 @@ class Lowering(object):
         if unique:
             packed = "str" not in key_types and (
                 len(bk) == 1 or (len(bk) == 2 and all(t in ("i8", "i32", "u32") for t in key_types)))
+            alias = {}
             if packed:
                 # the packed tag is the exact key: build keys that no operator above
-                # the join reads need not be stored in the payload
-                build_atts = [a for a in build_atts if not (a in bk and a.lastUse <= node.opId)]
+                # the join reads need not be stored in the payload, and above an
+                # inner join a build key equals its probe key, so one of the same
+                # type is read from the probe side
+                for b, p in zip(bk, pk):
+                    if jt == "INNER" and b.dataType == p.dataType and lang_type(b.dataType) == lang_type(p.dataType):
+                        alias[b.id] = p
+                build_atts = [a for a in build_atts
+                              if not (a in bk and (a.lastUse <= node.opId or a.id in alias))]
             payload = [lang_type(a.dataType) for a in build_atts]
             rid = self.new_res(Res(L.RES_UNIQUE, nkeys=len(bk), key_ctype=key_types, pay_ctype=payload,
                                    capacity=cap))
-            info = dict(res=rid, unique=True, bk=bk, pk=pk, build_atts=build_atts, passes=["build"])
+            info = dict(res=rid, unique=True, bk=bk, pk=pk, build_atts=build_atts, passes=["build"], alias=alias)
         else:
             keys_in_payload = [build_atts.index(b) if b in build_atts else -1 for b in bk]
             atts = list(build_atts)
@@ -688,6 +695,9 @@ class Lowering(object):
                 s = pipe.reg(lang_type(a.dataType))
                 pipe.att[a.id] = s
                 dsts.append(s)
+            for b, ks in zip(info["bk"], keys):
+                if b.id in info["alias"]:
+                    pipe.att[b.id] = ks
             pl, pn = pipe.list_(dsts)
             sub = {"INNER": L.JOIN_INNER, "SEMI": L.JOIN_SEMI, "ANTI": L.JOIN_ANTI}[jt]
             op = pipe.op(L.OP_PROBE, sub=sub, res=info["res"], list=kl, nlist=kn, list2=pl, nlist2=pn)

@@ -272,7 +272,8 @@ def plan_c3(alg, scal, Type, Reduction, patterns=None, d1_cut=50, d3_cut=100, nu
            s3.opId: {"selectivity": d3_cut / 100.0},
            j3.opId: {"multimatch": False, "selectivity": 1.0},
            j2.opId: {"multimatch": False, "selectivity": sel_like},
-           j1.opId: {"multimatch": False, "selectivity": sel_like * d1_cut / 100.0},
+           # a join's selectivity scales its larger input: the rows reaching j1
+           j1.opId: {"multimatch": False, "selectivity": d1_cut / 100.0},
            agg.opId: {"numgroups": numgroups}}
     return agg, cfg
 

@@ -2,14 +2,15 @@
 
 A unique join table with one integer key, built straight from a column whose
 values span few keys (measured on the device when the plan is prepared),
-needs no hashing: without a payload and over at most 2^18 keys it is a bit per
-key, probed in shared memory; with one payload of at most 32 bits and at most
-four keys per build row it is a word per key, one load a probe.  Cases: the C3
-star join's two small dimensions (inner joins whose payload no operator
-reads), semi and anti filters (Q4 / Q22 shapes), the C1 dimension (the nation
-as payload), and a table whose keys move out of the measured domain after
-preparation: the build reports it, and the plan re-runs with a hash table and
-stays exact.
+needs no hashing: without a payload it is a bit per key, probed in shared
+memory up to 2^18 keys and in place above (C3 at scale 0.3: 300,000 keys of
+the first dimension); with one payload of at most 32 bits and at most four
+keys per build row it is a word per key, one load a probe.  Cases: the C3 star
+join's three dimensions (inner joins whose build key, the one attribute read
+above them, is read from the probe side), semi and anti filters (Q4 / Q22
+shapes), the C1 dimension (the nation as payload), and a table whose keys move
+out of the measured domain after preparation: the build reports it, and the
+plan re-runs with a hash table and stays exact.
 """
 import numpy as np
 import pytest
@@ -33,7 +34,8 @@ def _bitmap_pipelines(p):
     return [i for i in range(len(p.lowering.pipes)) if ".bmin" in p.source(i)]
 
 
-@pytest.mark.parametrize("workload,scale", [("c3", 0.05), ("c11", 0.05), ("c13", 0.05), ("c1", 0.05), ("c1", 1.0)])
+@pytest.mark.parametrize("workload,scale", [("c3", 0.05), ("c3", 0.3), ("c11", 0.05), ("c13", 0.05), ("c1", 0.05),
+                                            ("c1", 1.0)])
 def test_bitmap_probes_match_oracle(engine, workload, scale):
     db, alg, plan = make_case({"workload": workload, "scale": scale})
     engine.register_database(db, force=True)
