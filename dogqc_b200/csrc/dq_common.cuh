@@ -366,17 +366,18 @@ __device__ __forceinline__ uint64_t str_ref_substring(uint64_t ref, int from, in
 }
 
 // String hash: the string's 8-byte little-endian words (the last one
-// zero-padded), each mixed with its index, summed, and the sum finalised with
-// the length.  A sum of independent word terms lets a warp hash one string a
-// word per lane (str_ref_hash_warp) and reach the value one lane computes
-// alone, so either may hash the keys of one table.
+// zero-padded), each offset by an index constant and multiplied by an odd
+// index-dependent constant (a multilinear hash), summed, and the sum mixed
+// with the length.  A sum of independent word terms lets a warp hash one
+// string a word per lane (str_ref_hash_warp) and reach the value one lane
+// computes alone, so either may hash the keys of one table.
 __device__ __forceinline__ uint64_t str_word(const uint8_t* p, int n, int i) {
   const int b = 8 * i;
   return load_bytes(p + b, n - b < 8 ? n - b : 8);
 }
 
 __device__ __forceinline__ uint64_t str_word_term(uint64_t w, int i) {
-  return fmix64(w ^ (0x9e3779b97f4a7c15ull * (uint64_t)(i + 1)));
+  return (w + 0x632be59bd9b4e019ull * (uint64_t)(i + 1)) * (0x9e3779b97f4a7c15ull * (uint64_t)(2 * i + 1));
 }
 
 __device__ __forceinline__ uint64_t str_hash_final(uint64_t sum, int n) {
@@ -413,15 +414,13 @@ __device__ __forceinline__ uint64_t warp_sum64(uint64_t v) {
   return v;
 }
 
-// Hash of each active lane's string reference, called by every lane of the
-// warp (the reference's push-down string hash, include/hashing.cuh:39-62):
+// Hash of each active lane's string (bytes p[0, n)), called by every lane of
+// the warp (the reference's push-down string hash, include/hashing.cuh:39-62):
 // strings longer than kStrCoopMin bytes are hashed one after another by all
 // 32 lanes, a word per lane with coalesced reads, the shorter ones by their
-// own lane; every lane gets str_ref_hash's value (inactive lanes 0).
-__device__ __noinline__ uint64_t str_ref_hash_warp(const DevPipe& P, bool active, uint64_t ref) {
-  const uint8_t* p = nullptr;
-  int n = 0;
-  if (active) str_ref_at(P, ref, p, n);
+// own lane; every lane gets str_hash's value (inactive lanes 0).
+// str_ref_hash_warp hashes the bytes behind a reference.
+__device__ __noinline__ uint64_t str_hash_warp(bool active, const uint8_t* p, int n) {
   const bool wide = active && n > kStrCoopMin;
   if (wide) prefetch_bytes(p, n);
   uint64_t h = (active && !wide) ? str_hash(p, n) : 0ull;
@@ -438,6 +437,51 @@ __device__ __noinline__ uint64_t str_ref_hash_warp(const DevPipe& P, bool active
     if (lane == src) h = str_hash_final(part, m);
   }
   return h;
+}
+
+// The words of a string of at most kStrCoopMin bytes, loaded independently
+// of one another (zero past the end), and its str_hash from them.  Two such
+// strings are equal exactly when their lengths and words are.
+constexpr int kStrShortWords = kStrCoopMin / 8;
+
+__device__ __forceinline__ void str_words_short(const uint8_t* p, int n, uint64_t* w) {
+#pragma unroll
+  for (int i = 0; i < kStrShortWords; ++i) w[i] = 8 * i < n ? load_bytes(p + 8 * i, n - 8 * i < 8 ? n - 8 * i : 8) : 0ull;
+}
+
+__device__ __forceinline__ uint64_t str_hash_words(const uint64_t* w, int n) {
+  uint64_t sum = 0;
+#pragma unroll
+  for (int i = 0; i < kStrShortWords; ++i)
+    if (8 * i < n) sum += str_word_term(w[i], i);
+  return str_hash_final(sum, n);
+}
+
+// The warp's strings longer than kStrCoopMin bytes (lanes with `wide` set)
+// hashed one after another by all 32 lanes, a word per lane; other lanes keep
+// h.  Called by every lane of the warp.
+__device__ __noinline__ uint64_t str_hash_wide(bool wide, const uint8_t* p, int n, uint64_t h) {
+  const int lane = (int)(threadIdx.x & 31);
+  if (wide) prefetch_bytes(p, n);
+  unsigned todo = __ballot_sync(kFull, wide);
+  while (todo) {
+    const int src = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const uint8_t* q = reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, (unsigned long long)p, src));
+    const int m = __shfl_sync(kFull, n, src);
+    uint64_t part = 0;
+    for (int i = lane; 8 * i < m; i += 32) part += str_word_term(str_word(q, m, i), i);
+    part = warp_sum64(part);
+    if (lane == src) h = str_hash_final(part, m);
+  }
+  return h;
+}
+
+__device__ __forceinline__ uint64_t str_ref_hash_warp(const DevPipe& P, bool active, uint64_t ref) {
+  const uint8_t* p = nullptr;
+  int n = 0;
+  if (active) str_ref_at(P, ref, p, n);
+  return str_hash_warp(active, p, n);
 }
 
 // Equality of two active lanes' string references, called by every lane of

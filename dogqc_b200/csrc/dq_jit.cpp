@@ -46,6 +46,7 @@ namespace {
 constexpr int kStripedMax = 12 * 1024;      // shared memory a replicated CTA-local aggregation table may take
 constexpr int kBlock = kThreads;
 constexpr int kWarpBuf = 64;                // rows one warp's divergence buffer holds
+constexpr int kStrSlotWords = 6;            // a CTA-local group slot's string: location, length, 4 words
 
 const char* ct_name(int t) {
   switch (t) {
@@ -188,6 +189,8 @@ struct Gen {
   std::string ldfn = "__ldcs";   // load function of streamed source columns
   std::vector<std::pair<int, int>> bitmaps;  // key-domain bitmaps probed: (resource, smem offset)
   const std::string* patterns = nullptr;     // host copy of the pattern bytes (P.pat_off into it)
+  std::vector<std::string> str_ptr, str_len;  // located string keys of the last str_key_hashes
+  std::vector<std::string> str_words;         // and their words (strings of at most kStrCoopMin bytes)
   bool single_cta = false;       // the tail function: one CTA scans the whole source
   bool tail_call = false;        // the main kernel's last CTA calls dq_tail
   int block = kBlock;            // threads per CTA
@@ -285,7 +288,29 @@ struct Gen {
     const DevSlot& sl = slot(s);
     if (sl.ctype != DQ_STR) throw Error("string op on a non-string slot");
     if (sl.kind == DQ_SLOT_STR) L("str_at(P.strs[" + num(sl.src) + "], " + row + ", " + p + ", " + n + ");");
-    else L("str_ref_at(P, " + V(s) + ", " + p + ", " + n + ");");
+    else L(locate_ref(s, p, n) + ";");
+  }
+
+  // The pipeline string a reference slot holds when one STRREF op writes it
+  // (no window; its source known here), else -1.
+  int ref_source(int s) const {
+    int src = -1, writers = 0;
+    for (int k = 0; k < P.nops; ++k) {
+      const dq_op& op = P.ops[k];
+      if (op.dst != s) continue;
+      ++writers;
+      if (op.kind == DQ_OP_STRREF && slot(op.a).kind == DQ_SLOT_STR) src = slot(op.a).src;
+    }
+    return writers == 1 ? src : -1;
+  }
+
+  // Locating the bytes behind reference slot s: straight from the pipeline's
+  // string column when its source is known, else through the plan's sources.
+  std::string locate_ref(int s, const std::string& p, const std::string& n) const {
+    const int src = ref_source(s);
+    if (src >= 0)
+      return "str_at(P.strs[" + num(src) + "], (int64_t)(" + V(s) + " & kStrRefRow), " + p + ", " + n + ")";
+    return "str_ref_at(P, " + V(s) + ", " + p + ", " + n + ")";
   }
 
   // Bucket of a multimap key held in array kk (string keys: their hashes in sh).
@@ -300,14 +325,125 @@ struct Gen {
   // where its lanes have not branched (long strings cooperatively, a word per
   // lane); the array's other entries stay 0.  Empty when resource r has no
   // string keys.
+  // The bytes behind each string key are located once (str_ptr / str_len
+  // name them, per key index) for the comparisons that follow.  All keys are
+  // located first and the short ones hashed by their lanes with independent
+  // loads, so the loads of several keys overlap; long ones go to the warp.
   std::string str_key_hashes(int r, int list, int n, const std::string& act) {
+    str_ptr.assign((size_t)std::max(n, 0), std::string());
+    str_len.assign((size_t)std::max(n, 0), std::string());
+    str_words.assign((size_t)std::max(n, 0), std::string());
     if (!has_str_key(P.res[r])) return std::string();
     const std::string h = fresh("sh");
     L("uint64_t " + h + "[" + num(std::max(n, 1)) + "] = {};");
     for (int i = 0; i < n; ++i)
-      if (P.res[r].key_ctype[i] == DQ_STR)
-        L(h + "[" + num(i) + "] = str_ref_hash_warp(P, " + act + ", " + V(P.lists[list + i]) + ");");
+      if (P.res[r].key_ctype[i] == DQ_STR) {
+        const std::string sp = fresh("skp"), sn = fresh("skn");
+        L("const uint8_t* " + sp + " = nullptr;");
+        L("int " + sn + " = 0;");
+        L("if (" + act + ") " + locate_ref(P.lists[list + i], sp, sn) + ";");
+        str_ptr[(size_t)i] = sp;
+        str_len[(size_t)i] = sn;
+      }
+    for (int i = 0; i < n; ++i)
+      if (P.res[r].key_ctype[i] == DQ_STR) {
+        const std::string w = fresh("skw");
+        L("uint64_t " + w + "[kStrShortWords] = {};");
+        L("if (" + act + " && " + str_len[(size_t)i] + " <= kStrCoopMin) {");
+        L("  str_words_short(" + str_ptr[(size_t)i] + ", " + str_len[(size_t)i] + ", " + w + ");");
+        L("  " + h + "[" + num(i) + "] = str_hash_words(" + w + ", " + str_len[(size_t)i] + ");");
+        L("}");
+        str_words[(size_t)i] = w;
+      }
+    for (int i = 0; i < n; ++i)
+      if (P.res[r].key_ctype[i] == DQ_STR) {
+        const std::string wide = "(" + act + " && " + str_len[(size_t)i] + " > kStrCoopMin)";
+        L("if (__any_sync(kFull, " + wide + ")) " + h + "[" + num(i) + "] = str_hash_wide(" + wide + ", " +
+          str_ptr[(size_t)i] + ", " + str_len[(size_t)i] + ", " + h + "[" + num(i) + "]);");
+      }
     return h;
+  }
+
+  // CTA-local group slot of a key with strings: linear probing over ns slots
+  // of ltags; a claim publishes the key values (lkeys, for the flush) and,
+  // per string, its location, length and words (lstr: kStrSlotWords words)
+  // before the tag.  A row whose tag matches compares lengths and words (a
+  // string of at most kStrCoopMin bytes) or its bytes with the slot string's
+  // (a longer one), without locating the slot's string again.  s_ stays -1
+  // when the table is full or a claim stays unpublished past the wait limit
+  // (the caller aggregates into the global table).
+  void local_str_slot(int r, const std::string& k) {
+    const DevRes& R = P.res[r];
+    const std::string NK = num(R.nkeys), NS = num(ns), NSTR = num(nstr_keys(R));
+    L("int s_ = -1;");
+    L("{");
+    ++ind;
+    L("uint32_t i_ = slot_of(tag_, " + NS + "u);");
+    L("for (int n_ = 0; n_ < " + NS + "; ++n_) {");
+    ++ind;
+    L("uint64_t t_ = ((volatile uint64_t*)ltags)[i_];");
+    L("if (t_ == kEmpty) {");
+    ++ind;
+    L("const uint64_t o_ = s_cas64(saddr(&ltags[i_]), kEmpty, kBusy);");
+    L("if (o_ == kEmpty) {");
+    ++ind;
+    for (int q = 0, j = 0; q < R.nkeys; ++q) {
+      L("((volatile uint64_t*)lkeys)[i_ * " + NK + " + " + num(q) + "] = " + k + "[" + num(q) + "];");
+      if (R.key_ctype[q] != DQ_STR) continue;
+      const std::string at = "((volatile uint64_t*)lstr)[(i_ * " + NSTR + " + " + num(j) + ") * " + num(kStrSlotWords);
+      L(at + "] = (uint64_t)" + str_ptr[(size_t)q] + ";");
+      L(at + " + 1] = (uint64_t)" + str_len[(size_t)q] + ";");
+      for (int w = 0; w < kStrSlotWords - 2; ++w)
+        L(at + " + " + num(2 + w) + "] = " + str_words[(size_t)q] + "[" + num(w) + "];");
+      ++j;
+    }
+    L("__threadfence_block();");
+    L("((volatile uint64_t*)ltags)[i_] = tag_;");
+    L("s_ = (int)i_;");
+    L("break;");
+    --ind;
+    L("}");
+    L("t_ = o_;");
+    --ind;
+    L("}");
+    L("for (long long w_ = 0; t_ == kBusy && w_ < kSpinLimit; ++w_) t_ = ((volatile uint64_t*)ltags)[i_];");
+    L("if (t_ == kBusy) break;");
+    L("if (t_ == tag_) {");
+    ++ind;
+    L("__threadfence_block();");
+    std::string eq;
+    for (int q = 0, j = 0; q < R.nkeys; ++q) {
+      if (!eq.empty()) eq += " && ";
+      if (R.key_ctype[q] != DQ_STR) {
+        eq += "((volatile uint64_t*)lkeys)[i_ * " + NK + " + " + num(q) + "] == " + k + "[" + num(q) + "]";
+        continue;
+      }
+      const std::string at = "((volatile uint64_t*)lstr)[(i_ * " + NSTR + " + " + num(j) + ") * " + num(kStrSlotWords);
+      const std::string& n = str_len[(size_t)q];
+      std::string words;
+      for (int w = 0; w < kStrSlotWords - 2; ++w)
+        words += (w ? " && " : "") + at + " + " + num(2 + w) + "] == " + str_words[(size_t)q] + "[" + num(w) + "]";
+      eq += "(int)" + at + " + 1] == " + n + " && (" + n + " <= kStrCoopMin ? (" + words +
+            ") : str_eq((const uint8_t*)" + at + "], " + n + ", " + str_ptr[(size_t)q] + ", " + n + "))";
+      ++j;
+    }
+    L("if (" + eq + ") {");
+    L("  s_ = (int)i_;");
+    L("  break;");
+    L("}");
+    --ind;
+    L("}");
+    L("i_ = i_ + 1 == " + NS + "u ? 0u : i_ + 1;");
+    --ind;
+    L("}");
+    --ind;
+    L("}");
+  }
+
+  static int nstr_keys(const DevRes& R) {
+    int n = 0;
+    for (int q = 0; q < R.nkeys; ++q) n += R.key_ctype[q] == DQ_STR;
+    return n;
   }
 
   // Equality of a probe key slot and a build key slot of resource r's key q.
@@ -1036,8 +1172,16 @@ struct Gen {
     ++ind;
     std::string k = keys(op, r, op.list, op.nlist);
     if (R.packed) L("const uint64_t tag_ = " + packed_tag(r, op.list, op.nlist) + ";");
-    else if (has_str_key(R)) L("const uint64_t tag_ = key_tag_strh(" + res(r) + ", " + k + ", " + sh + ");");
-    else L("const uint64_t tag_ = key_tag(" + res(r) + ", " + k + ");");
+    else if (has_str_key(R)) {
+      // key_tag_strh unrolled over the resource's keys
+      L("uint64_t th_ = 0x9e3779b97f4a7c15ull;");
+      for (int q = 0; q < R.nkeys; ++q)
+        L("th_ = fmix64(th_ ^ " + (R.key_ctype[q] == DQ_STR ? sh : k) + "[" + num(q) + "]) + 0x632be59bd9b4e019ull * " +
+          num(q + 1) + "ull;");
+      L("const uint64_t tag_ = fmix64(th_) & 0x7fffffffffffffffull;");
+    } else {
+      L("const uint64_t tag_ = key_tag(" + res(r) + ", " + k + ");");
+    }
     auto global = [&]() {
       if (R.packed) {
         packed_claim(r, "tag_");
@@ -1056,6 +1200,7 @@ struct Gen {
       global();
     } else {
       if (R.packed) L("const int s_ = local_group_slot(ltags, " + num(ns) + ", tag_, " + num(R.nkeys) + ");");
+      else if (has_str_key(R)) local_str_slot(r, k);
       else L("const int s_ = local_group_slot_keys(P, " + res(r) + ", ltags, lkeys, " + num(ns) + ", tag_, " + k + ");");
       L("if (s_ >= 0) {");
       ++ind;
@@ -1253,7 +1398,8 @@ struct Gen {
     // collisions it avoids: shared memory taken from the SM's L1 leaves fewer
     // lines for the loads in flight (a 33 KB table made the C1 probe kernel
     // twice as slow at five CTAs per SM as an 8.8 KB one)
-    const int tags = (ns + 1) * 8 + (R.packed ? 0 : ns * R.nkeys * 8);  // hashed keys: their values too
+    // hashed keys: their values too, and each string's location
+    const int tags = (ns + 1) * 8 + (R.packed ? 0 : ns * (R.nkeys + kStrSlotWords * nstr_keys(R)) * 8);
     agg = AGG_LOCAL;
     copies = 1;
     for (int c : {32, 16, 8, 4})
@@ -1468,7 +1614,12 @@ struct Gen {
       L("uint64_t* lacc = ltags + " + num(ns + 1) + ";");
     } else {
       L("uint64_t* lkeys = ltags + " + num(ns + 1) + ";");
-      L("uint64_t* lacc = lkeys + " + num(ns * R.nkeys) + ";");
+      if (has_str_key(R)) {
+        L("uint64_t* lstr = lkeys + " + num(ns * R.nkeys) + ";");
+        L("uint64_t* lacc = lstr + " + num(ns * kStrSlotWords * nstr_keys(R)) + ";");
+      } else {
+        L("uint64_t* lacc = lkeys + " + num(ns * R.nkeys) + ";");
+      }
     }
     L("for (int i = tid; i <= " + num(ns) + "; i += " + num(block) + ") ltags[i] = kEmpty;");
     L("for (int i = tid; i < " + num((ns + 1) * R.naggs * copies) + "; i += " + num(block) + ")");
