@@ -298,6 +298,10 @@ struct dq_plan {
   cudaGraphExec_t graph_exec = nullptr;
   std::string graph_sig;
   int graph_launches = 0;
+  // Side streams a captured run forks its independent pipelines onto (the
+  // graph then holds them as parallel branches), and the fork event.
+  std::vector<cudaStream_t> lanes;
+  cudaEvent_t fork_ev = nullptr;
   void drop_graph() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
@@ -310,6 +314,8 @@ struct dq_plan {
     if (host_status) cudaFreeHost(host_status);
     for (auto e : graph_ev)
       if (e) cudaEventDestroy(e);
+    for (auto l : lanes) cudaStreamDestroy(l);
+    if (fork_ev) cudaEventDestroy(fork_ev);
   }
 };
 
@@ -987,8 +993,69 @@ void free_events(dq_plan* plan) {
   plan->events.clear();
 }
 
+// Resources pipeline i's kernel reads and writes, its fused tail's included.
+// A scanned temp table or aggregation table counts as written as well (a scan
+// may reset the slots it reads).
+void pipe_access(const dq_plan* plan, size_t i, std::vector<int>& rd, std::vector<int>& wr) {
+  rd.clear();
+  wr.clear();
+  for (size_t j = 0; j < plan->pipes.size(); ++j) {
+    const PipeRec& p = *plan->pipes[j];
+    if (j != i && p.fused_into != (int)i) continue;
+    const dq_pipeline& d = p.desc;
+    if (d.source_kind == DQ_SRC_OUTPUT || d.source_kind == DQ_SRC_AGG) {
+      rd.push_back(d.source_res);
+      wr.push_back(d.source_res);
+    }
+    for (int k = 0; k < d.nops && k < DQ_MAX_OPS; ++k) {
+      const dq_op& op = d.ops[k];
+      switch (op.kind) {
+        case DQ_OP_PROBE:
+        case DQ_OP_EXPAND:
+        case DQ_OP_EXISTS:
+          rd.push_back(op.res);
+          break;
+        case DQ_OP_AGG:
+        case DQ_OP_BUILD:
+        case DQ_OP_MM_COUNT:
+        case DQ_OP_MM_SCATTER:
+        case DQ_OP_EMIT:
+          wr.push_back(op.res);
+          break;
+        default:
+          break;
+      }
+    }
+  }
+}
+
+// For each launched pipeline, the earlier launched pipelines it must follow:
+// those that write a resource it reads or writes, or read one it writes.
+std::vector<std::vector<int>> pipe_deps(const dq_plan* plan) {
+  const size_t np = plan->pipes.size();
+  std::vector<std::vector<int>> rd(np), wr(np), deps(np);
+  for (size_t i = 0; i < np; ++i) pipe_access(plan, i, rd[i], wr[i]);
+  auto meets = [](const std::vector<int>& a, const std::vector<int>& b) {
+    for (int x : a)
+      for (int y : b)
+        if (x == y) return true;
+    return false;
+  };
+  for (size_t j = 0; j < np; ++j) {
+    if (plan->pipes[j]->fused_into >= 0) continue;
+    for (size_t i = 0; i < j; ++i) {
+      if (plan->pipes[i]->fused_into >= 0) continue;
+      if (meets(wr[i], rd[j]) || meets(wr[i], wr[j]) || meets(rd[i], wr[j])) deps[j].push_back((int)i);
+    }
+  }
+  return deps;
+}
+
 // Enqueues one execution of all pipelines on `st`, ending with the copy of the
 // device status word to `host_status`; returns the kernels launched.
+// `dag` (a captured run): a pipeline that follows no unfinished pipeline of
+// `st` starts on a side stream, so independent pipelines become parallel
+// branches of the graph; each waits for the pipelines it depends on.
 //
 // `fast` (dq_plan_execute, where the caller reads the status after every run):
 // an aggregation table that exactly one later pipeline scans is reset by that
@@ -996,9 +1063,50 @@ void free_events(dq_plan* plan) {
 // initialising kernel; run_once records which tables a successful run left
 // clean.  Captured runs (served requests) always initialise, since a graph
 // replays the same launches whatever the previous replay left.
-int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status, bool fast = false) {
+constexpr int kLanes = 4;  // streams a captured run spreads its pipelines over
+
+// The side streams and fork event of a captured run (made before the capture).
+void ensure_lanes(dq_plan* plan) {
+  while ((int)plan->lanes.size() < kLanes - 1) {
+    cudaStream_t l;
+    DQ_CUDA(cudaStreamCreateWithFlags(&l, cudaStreamNonBlocking));
+    plan->lanes.push_back(l);
+  }
+  if (!plan->fork_ev) DQ_CUDA(cudaEventCreateWithFlags(&plan->fork_ev, cudaEventDisableTiming));
+}
+
+int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status, bool fast = false, bool dag = false) {
   int launches = 0;
   const size_t np = plan->pipes.size();
+  std::vector<std::vector<int>> deps;
+  std::vector<int> lane_of(np, 0), lane_last(kLanes, -1);
+  std::vector<bool> lane_forked(kLanes, false);
+  bool forks = false;
+  if (dag) {
+    if ((int)plan->lanes.size() < kLanes - 1 || !plan->fork_ev) throw DqError(DQ_ERR_INVALID, "side streams missing");
+    deps = pipe_deps(plan);
+    // lanes: a fused tail runs with its kernel, a pipeline with dependencies
+    // continues the chain of the latest one, the others take the least
+    // recently used lane
+    std::vector<int> last(kLanes, -1);
+    for (size_t i = 0; i < np; ++i) {
+      const PipeRec& p = *plan->pipes[i];
+      int lane = 0;
+      if (p.fused_into >= 0) {
+        lane = lane_of[(size_t)p.fused_into];
+      } else if (!deps[i].empty()) {
+        lane = lane_of[(size_t)deps[i].back()];
+      } else {
+        for (int l = 1; l < kLanes; ++l)
+          if (last[(size_t)l] < last[(size_t)lane]) lane = l;
+      }
+      lane_of[i] = lane;
+      last[(size_t)lane] = (int)i;
+      forks |= lane != 0;
+    }
+    dag = forks;
+  }
+  auto lane_stream = [&](int l) { return l == 0 ? st : plan->lanes[(size_t)l - 1]; };
   if (plan->events.size() != 2 * np + 2) {
     free_events(plan);
     for (size_t i = 0; i < 2 * np + 2; ++i) {
@@ -1030,11 +1138,25 @@ int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status, bool fast 
         break;
     }
   }
+  if (dag) DQ_CUDA(cudaEventRecord(plan->fork_ev, st));
+  const cudaStream_t origin = st;
   uint32_t* counters = plan->counters;
   for (size_t i = 0; i < np; ++i) {
     PipeRec& p = *plan->pipes[i];
     p.dev.tile_counter = counters + 2 * i;
     p.dev.clear_src = fast && p.clears_source ? 1 : 0;
+    if (dag) {
+      const int lane = lane_of[i];
+      st = lane_stream(lane);
+      if (lane && !lane_forked[(size_t)lane]) {
+        DQ_CUDA(cudaStreamWaitEvent(st, plan->fork_ev, 0));
+        lane_forked[(size_t)lane] = true;
+      }
+      if (p.fused_into < 0)
+        for (int d : deps[i])
+          if (lane_of[(size_t)d] != lane) DQ_CUDA(cudaStreamWaitEvent(st, plan->events[2 + 2 * (size_t)d], 0));
+      lane_last[(size_t)lane] = (int)i;
+    }
     DQ_CUDA(cudaEventRecord(plan->events[1 + 2 * i], st));
     if (p.expand_op >= 0) {
       DQ_CUDA(cudaMemsetAsync(p.heavy_count.ptr, 0, 8, st));
@@ -1073,6 +1195,10 @@ int enqueue_run(dq_plan* plan, cudaStream_t st, int32_t* host_status, bool fast 
     }
     DQ_CUDA(cudaEventRecord(plan->events[2 + 2 * i], st));
   }
+  st = origin;
+  if (dag)
+    for (int l = 1; l < kLanes; ++l)
+      if (lane_last[(size_t)l] >= 0) DQ_CUDA(cudaStreamWaitEvent(st, plan->events[2 + 2 * (size_t)lane_last[(size_t)l]], 0));
   DQ_CUDA(cudaEventRecord(plan->events[2 * np + 1], st));
   DQ_CUDA(cudaMemcpyAsync(host_status, plan->status.ptr, 4, cudaMemcpyDeviceToHost, st));
   return launches;
@@ -1131,6 +1257,7 @@ int run_once(dq_plan* plan, cudaStream_t st) {
   if (graphs) {
     std::string sig = graph_signature(plan);
     if (plan->graph_exec && sig != plan->graph_sig) plan->drop_graph();
+    if (!plan->graph_exec) ensure_lanes(plan);
     // a stream that cannot be captured (the legacy default stream) runs the launches directly
     if (!plan->graph_exec && cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       cudaGetLastError();
@@ -1141,7 +1268,7 @@ int run_once(dq_plan* plan, cudaStream_t st) {
     if (!plan->graph_exec) {
       cudaGraph_t g = nullptr;
       try {
-        plan->graph_launches = enqueue_run(plan, st, plan->host_status, true);
+        plan->graph_launches = enqueue_run(plan, st, plan->host_status, true, true);
       } catch (...) {
         cudaStreamEndCapture(st, &g);
         if (g) cudaGraphDestroy(g);
