@@ -1232,10 +1232,11 @@ struct Gen {
       L("if (" + act + ") {");
       L("  const uint64_t o_ = (uint64_t)" + key + " - (uint64_t)" + res(r) + ".bmin;");
       if (R.bitmap == 2) {
-        // the first row of a key wins, as in the hash table
+        // one row of a key wins (an 8-byte store is atomic), as one claim
+        // wins in the hash table; a store needs no round trip to L2
         const std::string pay = op.nlist2 > 0 ? "(uint64_t)(uint32_t)" + V(P.lists[op.list2]) : "0ull";
-        L("  if (o_ < " + res(r) + ".brange) atomicCAS(reinterpret_cast<unsigned long long*>(" + res(r) +
-          ".slots) + o_, 0ull, (1ull << 32) | " + pay + ");");
+        L("  if (o_ < " + res(r) + ".brange) reinterpret_cast<unsigned long long*>(" + res(r) +
+          ".slots)[o_] = (1ull << 32) | " + pay + ";");
       } else {
         L("  if (o_ < " + res(r) + ".brange) atomicOr(reinterpret_cast<unsigned int*>(" + res(r) +
           ".slots) + (o_ >> 5), 1u << (o_ & 31u));");
