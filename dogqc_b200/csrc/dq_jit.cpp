@@ -1400,11 +1400,14 @@ struct Gen {
     // lines for the loads in flight (a 33 KB table made the C1 probe kernel
     // twice as slow at five CTAs per SM as an 8.8 KB one)
     // hashed keys: their values too, and each string's location
+    // (32 lane-private copies in a pipeline without probes, C0 at 26 KB, ran
+    // 8 % slower than 8 copies at 6.5 KB)
+    const int limit = kStripedMax;
     const int tags = (ns + 1) * 8 + (R.packed ? 0 : ns * (R.nkeys + kStrSlotWords * nstr_keys(R)) * 8);
     agg = AGG_LOCAL;
     copies = 1;
     for (int c : {32, 16, 8, 4})
-      if (tags + (ns + 1) * R.naggs * 8 * c <= kStripedMax) {
+      if (tags + (ns + 1) * R.naggs * 8 * c <= limit) {
         agg = AGG_STRIPED;
         copies = c;
         break;

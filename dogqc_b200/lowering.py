@@ -146,6 +146,26 @@ class Res(object):
         self.columns = kw.get("columns", [])
 
 
+def _costly_rows(node):
+    """Whether producing ``node``'s rows does costly per-row work: a join, or
+    a LIKE or SUBSTRING in a selection or map."""
+    def costly_expr(e):
+        if e is None:
+            return False
+        if type(e).__name__ in ("LikeExpr", "SubstringExpr"):
+            return True
+        return any(costly_expr(getattr(e, a, None)) for a in ("leftChild", "rightChild", "child"))
+    k = type(node).__name__
+    if k in ("EquiJoin", "CrossJoin", "Aggregation"):
+        return True
+    if k == "Selection" and costly_expr(node.condition):
+        return True
+    if k == "Map" and costly_expr(node.expression):
+        return True
+    child = getattr(node, "child", None)
+    return child is not None and _costly_rows(child)
+
+
 class Pipe(object):
     """One pipeline under construction."""
 
@@ -663,15 +683,37 @@ class Lowering(object):
                                    capacity=cap))
             info = dict(res=rid, unique=False, bk=bk, pk=pk, build_atts=atts, passes=["count", "scatter"],
                         exists=semi)
+            if "str" not in payload and _costly_rows(node.leftChild):
+                # the multimap's two passes would each redo the build side's
+                # costly per-row work (string predicates, joins): one pass
+                # writes its rows' keys and payload to a temp table that the
+                # count and scatter passes scan instead
+                info["stage"] = self.new_res(Res(L.RES_OUTPUT, pay_ctype=payload, capacity=max(est, 1024),
+                                                 columns=[a.id for a in atts]))
         self.joins[id(node)] = info
-        for p in info["passes"]:
-            info["pass"] = p
+        if "stage" in info:
+            info["pass"] = "stage"
             self.produce(node.leftChild)
+            for p in info["passes"]:
+                info["pass"] = p
+                pipe = Pipe(L.SRC_OUTPUT, source_res=info["stage"])
+                for j, a in enumerate(info["build_atts"]):
+                    pipe.lazy[a.id] = self._lazy_col(pipe, str(j), lang_type(a.dataType))
+                self.join_build_sink(node, pipe)
+        else:
+            for p in info["passes"]:
+                info["pass"] = p
+                self.produce(node.leftChild)
         info["built"] = True
         self.produce(node.rightChild)
 
     def join_build_sink(self, node, pipe):
         info = self.joins[id(node)]
+        if info.get("pass") == "stage":
+            sl, sn = pipe.list_([pipe.value_slot(a) for a in info["build_atts"]])
+            pipe.op(L.OP_EMIT, res=info["stage"], list=sl, nlist=sn)
+            self.finish(pipe)
+            return
         keys = [pipe.value_slot(a) for a in info["bk"]]
         kl, kn = pipe.list_(keys)
         if info["unique"]:
