@@ -1398,16 +1398,14 @@ struct Gen {
     // within kStripedMax, else one copy.  A large table costs more than the
     // collisions it avoids: shared memory taken from the SM's L1 leaves fewer
     // lines for the loads in flight (a 33 KB table made the C1 probe kernel
-    // twice as slow at five CTAs per SM as an 8.8 KB one)
+    // twice as slow at five CTAs per SM as an 8.8 KB one), and even without
+    // probes 32 copies of C0's table (26 KB) ran 8 % slower than 8 (6.5 KB)
     // hashed keys: their values too, and each string's location
-    // (32 lane-private copies in a pipeline without probes, C0 at 26 KB, ran
-    // 8 % slower than 8 copies at 6.5 KB)
-    const int limit = kStripedMax;
     const int tags = (ns + 1) * 8 + (R.packed ? 0 : ns * (R.nkeys + kStrSlotWords * nstr_keys(R)) * 8);
     agg = AGG_LOCAL;
     copies = 1;
     for (int c : {32, 16, 8, 4})
-      if (tags + (ns + 1) * R.naggs * 8 * c <= limit) {
+      if (tags + (ns + 1) * R.naggs * 8 * c <= kStripedMax) {
         agg = AGG_STRIPED;
         copies = c;
         break;
