@@ -105,3 +105,49 @@ def test_reference_front_end_trees_lower(name):
     assert _fingerprint(plan) == _fingerprint(p2)
     a, b = Lowering(plan), Lowering(p2)
     assert a.describe() == b.describe()
+
+
+def _lowered(name, scale=0.001):
+    db = workloads.GENERATORS[name](scale)
+    alg = RelationalAlgebra(db)
+    plan, cfg = workloads.build(name, alg)
+    return Lowering(alg.resolveAlgebraPlan(plan, cfg))
+
+
+def test_inner_join_build_key_read_from_probe_side():
+    """C3 groups by its first dimension's key: above the inner join that key
+    equals the fact row's foreign key (same type), so the join table keeps no
+    payload and the aggregation reads the fact column."""
+    lw = _lowered("c3", 0.0002)
+    fact = lw.pipes[3]
+    probes = [o for o in fact.ops if o["kind"] == L.OP_PROBE]
+    assert len(probes) == 3
+    assert all(len(lw.res[o["res"]].pay_ctype) == 0 for o in probes)
+    agg = fact.ops[-1]
+    assert agg["kind"] == L.OP_AGG
+    key = fact.lists[agg["list"]]
+    assert fact.slots[key]["kind"] == L.SLOT_COL
+    assert fact.cols[fact.slots[key]["src"]] == "f_fk1"
+
+
+def test_costly_multimap_build_side_is_staged_once():
+    """Q13: the orders behind the outer join pass a NOT LIKE on their
+    comments.  One pipeline evaluates it and writes the surviving rows' keys
+    and payload to a temp table; the multimap's count and scatter passes scan
+    that table instead of the comments."""
+    lw = _lowered("c17")
+    sinks = [p.ops[-1]["kind"] for p in lw.pipes]
+    assert sinks[:3] == [L.OP_EMIT, L.OP_MM_COUNT, L.OP_MM_SCATTER]
+    stage = lw.pipes[0].ops[-1]["res"]
+    assert lw.res[stage].kind == L.RES_OUTPUT
+    assert [p.source_kind for p in lw.pipes[1:3]] == [L.SRC_OUTPUT, L.SRC_OUTPUT]
+    assert all(p.source_res == stage for p in lw.pipes[1:3])
+    assert any(o["kind"] == L.OP_LIKE for o in lw.pipes[0].ops)
+    assert not any(o["kind"] == L.OP_LIKE for p in lw.pipes[1:3] for o in p.ops)
+
+
+def test_plain_multimap_build_side_is_scanned_per_pass():
+    """C2's build side is a plain scan: both passes read the table."""
+    lw = _lowered("c2", 0.0005)
+    assert [p.ops[-1]["kind"] for p in lw.pipes[:2]] == [L.OP_MM_COUNT, L.OP_MM_SCATTER]
+    assert [p.source_kind for p in lw.pipes[:2]] == [L.SRC_TABLE, L.SRC_TABLE]
