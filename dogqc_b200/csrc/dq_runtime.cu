@@ -1440,15 +1440,18 @@ void refresh_pipelines(dq_plan* plan) {
 }
 
 // Whether pipeline k's kernel can run pipeline k + 1 in its last CTA: k
-// aggregates into a table of at most 65,536 slots that k + 1 alone scans,
+// aggregates into a table of at most kTailSlots slots that k + 1 alone scans,
 // with scalar ops and filters into an emit sink, and k defers no expansion.
+// One CTA scans the table: at 40,000 slots (the Q16- and Q21-shaped results)
+// that took 0.08-0.18 ms, far more than the launch it saves.
+constexpr uint64_t kTailSlots = 8192;
 bool fusable_tail(const dq_plan_desc* desc, const std::vector<std::unique_ptr<ResRec>>& res, int k) {
   const dq_pipeline& a = desc->pipes[k];
   const dq_pipeline& b = desc->pipes[k + 1];
   if (a.nops <= 0 || b.nops <= 0) return false;
   const dq_op& sink = a.ops[a.nops - 1];
   if (sink.kind != DQ_OP_AGG || b.source_kind != DQ_SRC_AGG || b.source_res != sink.res) return false;
-  if (sink.res < 0 || sink.res >= (int)res.size() || res[sink.res]->dev.cap + 1 > 65536) return false;
+  if (sink.res < 0 || sink.res >= (int)res.size() || res[sink.res]->dev.cap + 1 > kTailSlots) return false;
   for (int i = 0; i < a.nops; ++i)
     if (a.ops[i].kind == DQ_OP_EXPAND) return false;
   for (int i = 0; i < b.nops; ++i) {
