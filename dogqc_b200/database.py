@@ -70,6 +70,18 @@ class StringColumn(object):
     def get(self, i):
         return bytes(self.chars[int(self.offsets[i]):int(self.offsets[i + 1])])
 
+    def __getitem__(self, i):
+        if not -len(self) <= i < len(self):
+            raise IndexError(i)
+        return self.get(i % len(self))
+
+    def __iter__(self):
+        return iter(self.tolist())
+
+    def tolist(self):
+        heap, offs = self.chars.tobytes(), self.offsets.tolist()
+        return [heap[offs[i]:offs[i + 1]] for i in range(len(offs) - 1)]
+
     def take(self, idx):
         idx = np.asarray(idx, dtype=np.int64)
         return [self.get(i) for i in idx]

@@ -14,7 +14,8 @@ from dogqc_b200.lowering import NP_DTYPE, Lowering, lang_type
 
 
 class Result(object):
-    """A materialised result: column names, C types and numpy arrays."""
+    """A materialised result: column names, C types and columns (numpy arrays;
+    strings as a StringColumn, whose rows become bytes on demand)."""
 
     def __init__(self, names, ctypes_, columns, nrows):
         self.names = list(names)
@@ -67,15 +68,12 @@ def _take_result(res, names):
             t = C.c_int32()
             ptr = C.c_void_p()
             L.check(lib.dq_result_column(res, j, C.byref(t), C.byref(ptr)))
-            if t.value == L.STR:  # offsets into a heap: the strings as bytes
-                offs = np.frombuffer((C.c_uint8 * ((n.value + 1) * 8)).from_address(ptr.value), np.uint64)
+            if t.value == L.STR:  # offsets into a heap, kept as a StringColumn (bytes per row on demand)
+                offs = np.frombuffer((C.c_uint8 * ((n.value + 1) * 8)).from_address(ptr.value), np.uint64).copy()
                 hp, nch = C.c_void_p(), C.c_uint64()
                 L.check(lib.dq_result_string_heap(res, j, C.byref(hp), C.byref(nch)))
                 heap = C.string_at(hp.value, nch.value) if nch.value else b""
-                col = np.empty(n.value, dtype=object)
-                for i in range(n.value):
-                    col[i] = heap[int(offs[i]):int(offs[i + 1])]
-                cols.append(col)
+                cols.append(StringColumn(np.frombuffer(heap, dtype=np.uint8), offs))
                 types.append(t.value)
                 continue
             dt = np.dtype(NP_DTYPE[t.value])
