@@ -2177,6 +2177,7 @@ Program generate(const DevPipe& P, int expand_op, int refill_op, const Tuning& t
   g.patterns = patterns;
   g.batched = t.batched;
   if (t.block == 128 || t.block == 256 || t.block == 512) g.block = t.block;
+  if (t.min_blocks > 0 && t.min_blocks * g.block <= 2048) g.min_blocks = t.min_blocks;
   bool has_expand = false;
   for (int i = 0; i < P.nops; ++i) has_expand |= P.ops[i].kind == DQ_OP_EXPAND;
   g.U = (has_expand || P.source_kind == DQ_SRC_AGG) ? 1 : 4;
@@ -2384,15 +2385,17 @@ bool spills(const std::string& log) {
   return false;
 }
 
-// The source with every `__launch_bounds__(N)` made `__launch_bounds__(N, 1)`.
+// The source with every `__launch_bounds__(N)` or `__launch_bounds__(N, M)`
+// made `__launch_bounds__(N, 1)`.
 std::string one_block_bounds(const std::string& src) {
   std::string out;
   const std::string tag = "__launch_bounds__(";
   size_t pos = 0;
   for (size_t i = src.find(tag); i != std::string::npos; i = src.find(tag, pos)) {
     const size_t close = src.find(')', i);
-    out += src.substr(pos, close - pos);
-    if (src.substr(i, close - i).find(',') == std::string::npos) out += ", 1";
+    const size_t comma = src.find(',', i);
+    out += src.substr(pos, (comma < close ? comma : close) - pos);
+    out += ", 1";
     pos = close;
   }
   return out + src.substr(pos);

@@ -46,6 +46,7 @@ struct Tuning {
   int block = 0;             // 128, 256 or 512 threads per CTA
   int refill = 0;            // -1: no lane refill; 0: the plan's refill point
   int refill_threshold = 0;  // buffered rows that make a warp process them (0: 32)
+  int min_blocks = 0;        // CTAs per SM the launch bounds ask registers for (0: none)
 };
 
 // Source of the kernels for one pipeline.  `P` is the launch descriptor the

@@ -1710,6 +1710,8 @@ jit::Tuning tuning_of(const dq_tuning* t) {
     j.block = t->block_threads;
     j.refill = t->refill;
     j.refill_threshold = t->refill_threshold;
+    // resident CTAs asked for: the kernels' register budget must let them fit
+    if (t->ctas_per_sm > 0 && t->ctas_per_sm <= 8) j.min_blocks = t->ctas_per_sm;
   }
   return j;
 }

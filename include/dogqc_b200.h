@@ -384,7 +384,9 @@ typedef struct {
     int32_t defer_threshold;         /* expansion ranges longer than this are   */
                                      /* deferred (0: adaptive, 128 or 8)        */
     int32_t ctas_per_sm;             /* resident CTAs per SM of each generated  */
-                                     /* pipeline kernel (0: as many as fit)     */
+                                     /* pipeline kernel (0: as many as fit);    */
+                                     /* 1..8 also bound its registers so that   */
+                                     /* they fit (unless that spills)           */
 } dq_tuning;
 int dq_plan_prepare_tuned(dq_ctx* ctx, const dq_plan_desc* desc, const dq_tuning* tuning, dq_plan** out);
 
