@@ -176,6 +176,8 @@ EXPORTS = {
     "dq_plan_execute": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
     "dq_plan_free": (None, [C.c_void_p]),
     "dq_plan_source": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]),
+    "dq_plan_dependencies": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32,
+                                       C.POINTER(C.c_int32)]),
     "dq_plan_profile": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_uint64)]),
     "dq_plan_timing_get": (C.c_int, [C.c_void_p, C.POINTER(dq_plan_timing)]),
     "dq_result_rows": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),

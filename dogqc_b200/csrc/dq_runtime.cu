@@ -2485,6 +2485,16 @@ int dq_plan_source(dq_plan* plan, int32_t pipe, char* buf, int64_t cap, int64_t*
   return DQ_OK;
 }
 
+int dq_plan_dependencies(dq_plan* plan, int32_t pipe, int32_t* out, int32_t cap, int32_t* n) {
+  if (!plan || !n || cap < 0 || (cap > 0 && !out)) return DQ_ERR_INVALID;
+  if (pipe < 0 || pipe >= (int32_t)plan->pipes.size()) return fail(plan->ctx, DQ_ERR_INVALID, "no such pipeline");
+  const std::vector<std::vector<int>> deps = pipe_deps(plan);
+  const std::vector<int>& d = deps[(size_t)pipe];
+  *n = (int32_t)d.size();
+  for (int32_t i = 0; i < cap && i < *n; ++i) out[i] = d[(size_t)i];
+  return DQ_OK;
+}
+
 int dq_plan_timing_get(dq_plan* plan, dq_plan_timing* out) {
   if (!plan || !out) return DQ_ERR_INVALID;
   *out = plan->timing;

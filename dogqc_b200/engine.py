@@ -131,6 +131,14 @@ class Plan(object):
         L.check(lib.dq_plan_source(self.handle, pipe, buf, n.value + 1, C.byref(n)), self.engine.ctx)
         return buf.value.decode()
 
+    def dependencies(self, pipe):
+        """The earlier pipelines ``pipe`` waits for in a replayed run (the
+        others may run beside it)."""
+        out = (C.c_int32 * len(self.lowering.pipes))()
+        n = C.c_int32()
+        L.check(L.lib().dq_plan_dependencies(self.handle, pipe, out, len(out), C.byref(n)), self.engine.ctx)
+        return list(out[:n.value])
+
     def profile(self, point):
         """Lane-activity histogram of profile point ``point`` in the last
         execute: 33 counts, warp steps with 0..32 active lanes."""

@@ -336,6 +336,14 @@ int dq_plan_prepare(dq_ctx* ctx, const dq_plan_desc* desc, dq_plan** out);
  * source is that kernel's, where it is the function dq_tail.
  * The counterpart of the reference's generated query file.                 */
 int dq_plan_source(dq_plan* plan, int32_t pipe, char* buf, int64_t cap, int64_t* len);
+/* The earlier pipelines pipeline `pipe` waits for when a run is replayed as a
+ * CUDA graph: those that write a table it reads or writes, or read a table it
+ * writes (a scanned temp or aggregation table counts as written).  The others
+ * may run beside it, on other streams of the graph.  At most cap indices into
+ * out, ascending; *n is their count.  A result scan fused into the kernel of
+ * the pipeline before it has none (it runs in that kernel).  No device work:
+ * offline contexts answer too.                                              */
+int dq_plan_dependencies(dq_plan* plan, int32_t pipe, int32_t* out, int32_t cap, int32_t* n);
 /* Runs every pipeline in order on `stream` (NULL: the context stream) and
  * returns a new result.  Resources start every run empty.  After a
  * successful run the same launches are captured as a CUDA graph and replayed

@@ -57,6 +57,7 @@ def test_every_workload_compiles_offline(engine, name):
     {"rows_per_thread": 1, "block_threads": 128},
     {"rows_per_thread": 2, "block_threads": 512, "refill": -1},
     {"rows_per_thread": 4, "block_threads": 256, "unique_slots_pct": 400, "multi_buckets_pct": 50},
+    {"rows_per_thread": 2, "block_threads": 256, "ctas_per_sm": 4},
 ])
 @pytest.mark.parametrize("name", ["c1", "c2"])
 def test_tuned_launch_shapes_compile(engine, name, tuning):
@@ -134,3 +135,20 @@ def test_tuning_cache_on_disk(tmp_path, monkeypatch):
         raise AssertionError("searched although the file holds the result")
     got = autotune._tuned("plan|x", None, again)
     assert got[0] == {"rows_per_thread": 2, "refill_threshold": 28} and got[1] == 0.5
+
+
+def test_replayed_runs_overlap_independent_pipelines(engine):
+    """A replayed run waits only where pipelines share a table.  C3: the three
+    dimension builds share none and may run side by side; the fact pipeline
+    waits for all three, the result scan for the fact pipeline.  Q13 (C17):
+    the staged build side, then the multimap's count and scatter passes over
+    it, the probe after both passes, its aggregation's scan, and a fused
+    result scan (it runs in its predecessor's kernel) with none."""
+    plan = engine.prepare(resolved(engine, "c3"))
+    assert [plan.dependencies(i) for i in range(5)] == [[], [], [], [0, 1, 2], [3]]
+    plan = engine.prepare(resolved(engine, "c17"))
+    assert [plan.dependencies(i) for i in range(6)] == [[], [0], [0, 1], [1, 2], [3], []]
+    plan = engine.prepare(resolved(engine, "c1"))
+    assert [plan.dependencies(i) for i in range(3)] == [[], [0], []]
+    with pytest.raises(L.DqError):
+        plan.dependencies(3)
