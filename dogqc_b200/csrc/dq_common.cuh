@@ -369,7 +369,7 @@ __device__ __forceinline__ uint64_t str_ref_substring(uint64_t ref, int from, in
 // zero-padded), each offset by an index constant and multiplied by an odd
 // index-dependent constant (a multilinear hash), summed, and the sum mixed
 // with the length.  A sum of independent word terms lets a warp hash one
-// string a word per lane (str_ref_hash_warp) and reach the value one lane
+// string a word per lane (str_hash_wide) and reach the value one lane
 // computes alone, so either may hash the keys of one table.
 __device__ __forceinline__ uint64_t str_word(const uint8_t* p, int n, int i) {
   const int b = 8 * i;
@@ -414,31 +414,6 @@ __device__ __forceinline__ uint64_t warp_sum64(uint64_t v) {
   return v;
 }
 
-// Hash of each active lane's string (bytes p[0, n)), called by every lane of
-// the warp (the reference's push-down string hash, include/hashing.cuh:39-62):
-// strings longer than kStrCoopMin bytes are hashed one after another by all
-// 32 lanes, a word per lane with coalesced reads, the shorter ones by their
-// own lane; every lane gets str_hash's value (inactive lanes 0).
-// str_ref_hash_warp hashes the bytes behind a reference.
-__device__ __noinline__ uint64_t str_hash_warp(bool active, const uint8_t* p, int n) {
-  const bool wide = active && n > kStrCoopMin;
-  if (wide) prefetch_bytes(p, n);
-  uint64_t h = (active && !wide) ? str_hash(p, n) : 0ull;
-  const int lane = (int)(threadIdx.x & 31);
-  unsigned todo = __ballot_sync(kFull, wide);
-  while (todo) {
-    const int src = __ffs(todo) - 1;
-    todo &= todo - 1;
-    const uint8_t* q = reinterpret_cast<const uint8_t*>(__shfl_sync(kFull, (unsigned long long)p, src));
-    const int m = __shfl_sync(kFull, n, src);
-    uint64_t part = 0;
-    for (int i = lane; 8 * i < m; i += 32) part += str_word_term(str_word(q, m, i), i);
-    part = warp_sum64(part);
-    if (lane == src) h = str_hash_final(part, m);
-  }
-  return h;
-}
-
 // The words of a string of at most kStrCoopMin bytes, loaded independently
 // of one another (zero past the end), and its str_hash from them.  Two such
 // strings are equal exactly when their lengths and words are.
@@ -458,8 +433,10 @@ __device__ __forceinline__ uint64_t str_hash_words(const uint64_t* w, int n) {
 }
 
 // The warp's strings longer than kStrCoopMin bytes (lanes with `wide` set)
-// hashed one after another by all 32 lanes, a word per lane; other lanes keep
-// h.  Called by every lane of the warp.
+// hashed one after another by all 32 lanes, a word per lane with coalesced
+// reads (the reference's push-down string hash, include/hashing.cuh:39-62);
+// each gets str_hash's value, and the other lanes keep h.  Called by every
+// lane of the warp, before its lanes branch.
 __device__ __noinline__ uint64_t str_hash_wide(bool wide, const uint8_t* p, int n, uint64_t h) {
   const int lane = (int)(threadIdx.x & 31);
   if (wide) prefetch_bytes(p, n);
@@ -475,13 +452,6 @@ __device__ __noinline__ uint64_t str_hash_wide(bool wide, const uint8_t* p, int 
     if (lane == src) h = str_hash_final(part, m);
   }
   return h;
-}
-
-__device__ __forceinline__ uint64_t str_ref_hash_warp(const DevPipe& P, bool active, uint64_t ref) {
-  const uint8_t* p = nullptr;
-  int n = 0;
-  if (active) str_ref_at(P, ref, p, n);
-  return str_hash_warp(active, p, n);
 }
 
 // Equality of two active lanes' string references, called by every lane of
