@@ -100,3 +100,25 @@ def test_cpu_evaluator_long_string_keys_match_oracle(kind):
     db = string_cases.long_db()
     plan = string_cases.long_key_plan(db, kind)
     assert canonical_rows(cpu_eval.Prepared(db, plan, 3).run()[1]) == canonical_rows(run_plan(db, plan)[1])
+
+
+def test_string_column_reads_as_bytes():
+    """A string result column stays a heap and offsets; reading it gives the
+    rows' bytes (by index, negative too, by iteration and as a list)."""
+    import numpy as np
+    from dogqc_b200.database import StringColumn
+    from dogqc_b200.engine import Result
+    words = [b"", b"a", b"hello world", b"x" * 40, b"AB-12"]
+    col = StringColumn.from_list(words)
+    assert len(col) == 5
+    assert col.tolist() == words
+    assert list(col) == words
+    assert [col[i] for i in range(5)] == words
+    assert col[-1] == b"AB-12" and col[-5] == b""
+    with pytest.raises(IndexError):
+        col[5]
+    with pytest.raises(IndexError):
+        col[-6]
+    res = Result(["s", "k"], [L.STR, L.I32], [col, np.arange(5, dtype=np.int32)], 5)
+    assert res.rows() == list(zip(words, range(5)))
+    assert "hello world" in res.format_sample()
