@@ -152,3 +152,24 @@ def test_replayed_runs_overlap_independent_pipelines(engine):
     assert [plan.dependencies(i) for i in range(3)] == [[], [0], []]
     with pytest.raises(L.DqError):
         plan.dependencies(3)
+
+
+@pytest.mark.parametrize("pattern,search", [("%#1%", True), ("%ABC%xyz%", True), ("%a%b%c%d%e%f%g%h%i%", True),
+                                            ("%", False), ("%%", False), ("%a%%b%", False), ("A%", False),
+                                            ("%#59", False), ("%AB_D%", False), ("abc", False)])
+def test_like_patterns_of_percent_separated_literals_compile_to_searches(engine, pattern, search):
+    """'%L1%...%Ln%' (no '_', no empty literal) becomes one literal search
+    after another (like_find); every other pattern runs the reference
+    matcher's algorithm (like_match)."""
+    import string_cases
+    import dogqc_b200.scalar as scal
+    from dogqc_b200.types import Type
+    db = string_cases.long_db(200)
+    engine.register_database(db, force=True)
+    alg = RelationalAlgebra(db)
+    sel = alg.selection(scal.LikeExpr(scal.AttrExpr("fk"), scal.ConstExpr(pattern, Type.STRING)), alg.scan("f"))
+    plan = engine.prepare(alg.resolveAlgebraPlan(alg.projection(["fv", "fk"], sel), {}))
+    src = plan.source(0)
+    body = src[src.index("dq_main"):]
+    assert ("like_find(" in body) == search
+    assert ("like_match(" in body) == (not search)
